@@ -1,0 +1,380 @@
+#!/usr/bin/env python
+"""Throughput of PSI's phase-space-sheet voxelization on B200.
+
+Workload: 128^3 Lagrangian particles (seeded Zel'dovich lattice, P(k) ~ k^-2,
+rms displacement 2 cells, velocities 10 psi through float32) in a periodic box
+of side 100, cut into 6 tets per cube and deposited with moments to order 2
+(m, x, v, xx, xv, vv) on a 256^3 float64 grid.  One step = one full voxels()
+call over the workload.  The headline is the mixed-precision kernel's tets/s;
+the FP64 kernel is timed beside it and the mixed result is checked against it.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun every rank deposits its own lattice (seed + rank) on its own
+GPU (weak scaling, no collective on the data path); the step time is the max
+over ranks of CUDA-event time.  `--impl reference` times the reference's own C
+implementation (oracle/_ref, compiled from its sources) on all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [ROOT]
+
+METRIC = "tets/s @128³→256³: mixed vs FP64 GPU at ≤1e-5 voxel err; fwd+bwd / fwd time"
+N_PART = 128
+N_GRID = 256
+RMS = 2.0
+BOX = ((0.0, 0.0, 0.0), (100.0, 100.0, 100.0))
+FIELDS = ["x", "v", "xx", "xv", "vv"]
+WORKLOAD = "128^3 particles -> 256^3 grid, Zel'dovich rms 2 cells, fields m,x,v,xx,xv,vv"
+DATA = "synthetic: seeded Zel'dovich-displaced particle lattice (P(k)~k^-2), element mass 1"
+TETS_PER_STEP = 6 * N_PART ** 3
+FP64_FMA_PER_CLK_PER_SM = 64
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def env_rank():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+# ---------------------------------------------------------------- clocks
+class Clocks:
+    """nvidia-smi samples taken while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self):
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.count(",") >= 8]
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if "Active" in v and "Not" not in v})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": float(rows[0][2]),
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------- reference arm
+def _ref_init(seed):
+    global _W
+    sys.path[:0] = [ROOT, os.path.join(ROOT, "oracle")]
+    import numpy as np
+
+    from pypsi_b200.synth import zeldovich
+
+    pos, vel = zeldovich(N_PART, RMS, seed)
+    _W = (np.ascontiguousarray(pos.reshape(-1, 3)), np.ascontiguousarray(vel.reshape(-1, 3)))
+
+
+def sample_blocks(edge=16):
+    """Lagrangian sub-blocks of the lattice (origin triples) whose tets do not
+    wrap the periodic box; the sample units of the CPU runs."""
+    nb = N_PART // edge
+    return [(i * edge, j * edge, k * edge) for i in range(1, nb - 1) for j in range(1, nb - 1)
+            for k in range(1, nb - 1)]
+
+
+def _ref_block(args):
+    """Deposit one sub-block with the reference's psi_voxels on a window that
+    covers it at the workload's voxel size; returns (tets, seconds)."""
+    origin, edge, kind = args
+    import numpy as np
+
+    import oracle as O
+
+    pos, vel = _W
+    n = N_PART
+    i, j, k = np.meshgrid(*(np.arange(o, o + edge) for o in origin), indexing="ij")
+    conn = np.empty(i.shape + (8,), np.int32)
+    for ii in range(2):
+        for jj in range(2):
+            for kk in range(2):
+                conn[..., 4 * ii + 2 * jj + kk] = (n * n * ((i + ii) % n) + n * ((j + jj) % n) + (k + kk) % n)
+    conn = conn.reshape(-1, 8)
+    p = pos[np.unique(conn)]
+    d = BOX[1][0] / N_GRID
+    lo = np.floor(p.min(axis=0) / d) - 1
+    hi = np.ceil(p.max(axis=0) / d) + 1
+    bounds = (tuple(lo * d), tuple(hi * d))
+    ng = tuple(int(v) for v in (hi - lo))
+    t0 = time.perf_counter()
+    O.voxelize(kind, n=ng, bounds=bounds, pos=pos, vel=vel, conn=conn, periodic_box=None, fields=FIELDS)
+    return 6 * conn.shape[0], time.perf_counter() - t0
+
+
+def run_reference(args):
+    rank, world, _ = env_rank()
+    if rank != 0:
+        return
+    import multiprocessing as mp
+
+    sys.path[:0] = [os.path.join(ROOT, "oracle")]
+    import oracle as O
+
+    kind = "reference" if O.available("reference") else "restatement"
+    cores = len(os.sched_getaffinity(0))
+    blocks = sample_blocks()
+    per_step = blocks[: max(1, min(len(blocks), cores))]
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores, initializer=_ref_init, initargs=(1234,)) as pool:
+        def step():
+            t0 = time.perf_counter()
+            res = pool.map(_ref_block, [(b, 16, kind) for b in per_step], chunksize=1)
+            return sum(r[0] for r in res), time.perf_counter() - t0
+
+        for _ in range(args.warmup):
+            step()
+        tets, secs = 0, 0.0
+        for _ in range(args.steps):
+            t, s = step()
+            tets += t
+            secs += s
+    value = tets / secs
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "tets/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * secs / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": DATA,
+            "config": {"workload": WORKLOAD, "precision": "fp64 (reference C)"},
+            "cpu_baseline": {"value": value, "unit": "tets/s", "cores": cores,
+                             "kind": "reference" if kind == "reference" else "port",
+                             "sample": f"{len(per_step)} Lagrangian 16^3-element sub-blocks of the workload per step, "
+                                       f"one per process, each on a window covering it at the 256^3 voxel size"},
+            "e2e": {"value": value, "unit": "tets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline_single(seconds=12.0):
+    """The reference's C path on one host core over a bounded sample."""
+    sys.path[:0] = [os.path.join(ROOT, "oracle")]
+    import oracle as O
+
+    kind = "reference" if O.available("reference") else "restatement"
+    _ref_init(1234)
+    tets, secs, nb = 0, 0.0, 0
+    for b in sample_blocks():
+        t, s = _ref_block((b, 16, kind))
+        tets += t
+        secs += s
+        nb += 1
+        if secs > seconds:
+            break
+    return {"value": tets / secs, "unit": "tets/s", "cores": 1, "kind": "reference" if kind == "reference" else "port",
+            "sample": f"{nb} Lagrangian 16^3-element sub-blocks of the workload ({tets} tets, {secs:.1f} s), "
+                      f"each on a window covering it at the 256^3 voxel size"}
+
+
+# ---------------------------------------------------------------- our arm
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    rank, world, local = env_rank()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    from pypsi_b200 import PSI, capi
+    from pypsi_b200.metrics import field_errors, mass_error
+    from pypsi_b200.synth import zeldovich
+
+    pos, vel = zeldovich(N_PART, RMS, 1234 + rank)
+    dev = torch.device("cuda", local)
+    dpos = torch.from_numpy(pos.reshape(-1, 3)).to(dev)
+    dvel = torch.from_numpy(vel.reshape(-1, 3)).to(dev)
+    shapes = {"m": (N_GRID,) * 3, "x": (N_GRID,) * 3 + (3,), "v": (N_GRID,) * 3 + (3,)}
+    for f in ("xx", "xv", "vv"):
+        shapes[f] = (N_GRID,) * 3 + (3, 3)
+
+    def fresh():
+        return {f: torch.zeros(s, dtype=torch.float64, device=dev) for f, s in shapes.items()}
+
+    stream = torch.cuda.current_stream()
+
+    def step(fields, prec):
+        return capi.voxels_device(fields, (N_GRID,) * 3, BOX, dpos, dvel, block_dims=(N_PART,) * 3,
+                                  periodic_box=BOX, precision=prec, stream=stream)
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    def timed(prec, fields, clocks=False):
+        for _ in range(args.warmup):
+            step(fields, prec)
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        stats = []
+        ck = Clocks(local) if clocks else None
+        if ck:
+            ck.__enter__()
+        e0.record(stream)
+        for _ in range(args.steps):
+            stats.append(step(fields, prec))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if ck:
+            ck.__exit__()
+        barrier()
+        ms = e0.elapsed_time(e1)
+        if dist:
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms / args.steps, stats, (ck.summary() if ck else None)
+
+    fields = fresh()
+    ms_mixed, st_mixed, clocks = timed("mixed", fields, clocks=True)
+    ms_fp64, st_fp64, _ = timed("fp64", fields)
+    del fields
+
+    # accuracy of the headline (mixed) against FP64 on the same input, and mass
+    errs, merr = {}, {}
+    outs = {}
+    for prec in ("fp64", "mixed"):
+        f = fresh()
+        step(f, prec)
+        torch.cuda.synchronize()
+        outs[prec] = {k: v.cpu().numpy() for k, v in f.items()}
+        merr[prec] = mass_error(outs[prec]["m"], N_PART ** 3)
+        del f
+    errs = field_errors(outs["mixed"], outs["fp64"])
+    del outs
+    torch.cuda.empty_cache()
+
+    # end to end through the drop-in module: host numpy in, host numpy out
+    mesh = PSI.Mesh(loader="block", pos=pos, vel=vel, periodic_box=BOX)
+    grid = PSI.Grid(n=(N_GRID,) * 3, bounds=BOX, fields=FIELDS)
+    PSI.voxels(grid=grid, mesh=mesh, precision="mixed")
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        PSI.voxels(grid=grid, mesh=mesh, precision="mixed")
+    e2e_s = (time.perf_counter() - t0) / args.e2e_steps
+    if dist:
+        t = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    field_bytes = sum(a.nbytes for a in grid.fields.values())
+    h2d = pos.nbytes + vel.nbytes + mesh.mass.nbytes + field_bytes
+    d2h = field_bytes
+    del grid
+    capi.lib.psib_release_device_memory()
+
+    if dist:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+
+    # roofline of the clip kernels (the dominant work): algorithmic FP64 flops
+    # per fragment F_k = 20 V + t_k (2V - 4) + P_k (V = mean vertices/fragment),
+    # k = 1 on the first clip pass and 2 on the second.
+    s = st_mixed[-1]
+    frags = s["fragments"] / s["passes"]
+    vbar = s["frag_verts"] / max(1, s["fragments"])
+    f1 = 20 * vbar + 33 * (2 * vbar - 4) + 50
+    f2 = 20 * vbar + 132 * (2 * vbar - 4) + 520
+    flops = frags * (f1 + f2)
+    clip_ms = statistics.mean(x["ms_clip"] for x in st_mixed)
+    launches = s["clip_launches"]
+    achieved = flops / (clip_ms * 1e-3) / 1e12
+    peak = 148 * FP64_FMA_PER_CLK_PER_SM * 2 * 1965e6 / 1e12
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        peaks = {}
+    value = world * TETS_PER_STEP / (ms_mixed * 1e-3)
+    line = {
+        "metric": METRIC, "value": value, "unit": "tets/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64", "data": DATA,
+        "config": {"workload": WORKLOAD, "precision": "mixed (FP32 clip, FP64 moments/accumulation)",
+                   "l2": "inputs larger than L2 (4.6 GB of grid fields, 3 GB of tet images per step)",
+                   "per_rank": "each rank deposits its own lattice (seed 1234+rank) on its own GPU"},
+        "fp64": {"value": world * TETS_PER_STEP / (ms_fp64 * 1e-3), "unit": "tets/s", "ms_per_step": ms_fp64},
+        "mixed_over_fp64": ms_fp64 / ms_mixed,
+        "voxel_clips_per_s": world * frags / (ms_mixed * 1e-3),
+        "mixed_vs_fp64_err": {f: e["norm"] for f, e in errs.items() if f != "dead_m"},
+        "mixed_vs_fp64_err_m_rel": errs["m"]["rel"],
+        "mass_err": merr,
+        "fwd_bwd_over_fwd": None,
+        "work": {"tets": TETS_PER_STEP, "tet_images": s["tet_images"], "fragments_per_pass": frags,
+                 "verts_per_fragment": vbar, "passes": s["passes"], "splits_per_pass": s["splits"] / s["passes"]},
+        "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                     "traffic": None, "kernel": "clip-and-deposit (both passes)",
+                     "achieved_def": "sum over fragments of F_1 + F_2 algorithmic FP64 flops / clip-kernel event time",
+                     "peak_source": "FP64 FMA issue rate 64/clk/SM x 148 SMs x 2 flop at 1965 MHz; "
+                                    "MEASURED_PEAKS.json has no FP64 figure",
+                     "clip_ms_per_step": clip_ms, "clip_launches_per_step": launches,
+                     "hbm_peak_gbs_measured": peaks.get("hbm_gbs")},
+        "e2e": {"value": world * TETS_PER_STEP / e2e_s, "unit": "tets/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "api": "PSI.voxels(grid, mesh, precision='mixed') on host numpy arrays",
+                "ms_per_step": e2e_s * 1e3},
+        "gpu_launches": int(sum(x["kernel_launches"] for x in st_mixed)),
+        "clocks": clocks,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_single()
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,141 @@
+/*
+ * psi_b200.h -- C ABI of the B200 phase-space-sheet voxelizer (libpsi_b200.so).
+ *
+ * Plain C types only: pointers, sizes and status codes.  No CUDA, C++ or
+ * PyTorch type appears in a signature; the stream is passed as void*.
+ *
+ * The library replaces the density path of PyPSI:
+ *   void psi_voxels(psi_grid* grid, psi_mesh* mesh, psi_rtree* rtree,
+ *                   psi_int mode, psi_real reftol, psi_int max_ref_lvl);
+ * declared at src/PSI.c:39, defined at src/cpsi.c:41, and called only from
+ * PSI_voxels at src/PSI.c:1015.  psib_grid and psib_mesh carry the same data
+ * as psi_grid (include/grid.h:46-53) and psi_mesh (include/mesh.h:42-52),
+ * with the same array layouts (src/PSI.c:124-186, :399-656).
+ *
+ * Every entry point returns PSIB_OK (0) or a PSIB_ERR_* code; none exits or
+ * aborts.  psib_last_error() gives a message for the last failure on the
+ * calling thread.
+ */
+#ifndef PSI_B200_H
+#define PSI_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PSIB_ABI_VERSION 1
+
+/* status codes */
+#define PSIB_OK 0
+#define PSIB_ERR_ARG 1         /* invalid argument (shape, type, value) */
+#define PSIB_ERR_CUDA 2        /* a CUDA runtime call failed */
+#define PSIB_ERR_NOMEM 3       /* device or pinned host allocation failed */
+#define PSIB_ERR_OVERFLOW 4    /* a polyhedron outgrew its vertex buffer */
+#define PSIB_ERR_INDEX 5       /* connectivity or voxel index out of range */
+#define PSIB_ERR_UNSUPPORTED 6 /* a mode the library does not implement */
+#define PSIB_ERR_NODEVICE 7    /* no CUDA device is visible */
+
+/* grid field tags, as include/grid.h:37-42 */
+#define PSIB_M 0
+#define PSIB_X 1
+#define PSIB_V 2
+#define PSIB_XX 3
+#define PSIB_XV 4
+#define PSIB_VV 5
+
+/* deposit mode, as include/psi.h:69-70 */
+#define PSIB_MODE_DENSITY 0
+#define PSIB_MODE_ANNIHILATION 1 /* not implemented: returns PSIB_ERR_UNSUPPORTED */
+
+/* arithmetic of the clip kernel */
+#define PSIB_FP64 0  /* the reference's double-precision operation order, no FMA */
+#define PSIB_MIXED 1 /* FP32 clipping on tile-recentred tets, FP64 moments and sums */
+
+/* where the pointers of psib_grid / psib_mesh live */
+#define PSIB_HOST 0   /* host memory; the library copies in and out */
+#define PSIB_DEVICE 1 /* device memory of the current CUDA device */
+
+/* Cartesian grid.  fields[t] points to nx*ny*nz*{1,3,9} doubles in C order
+ * (m: (nx,ny,nz); x,v: (...,3); xx,xv,vv: (...,3,3)) or is NULL when the field
+ * is not requested.  fields[PSIB_M] is required.  As in the reference the call
+ * ACCUMULATES into the fields: m is a mass sum, x and v mass-weighted means,
+ * xx, xv, vv mass-weighted (co)variances (src/geometry.c:164-186). */
+typedef struct {
+    int n[3];
+    double window[2][3];
+    double d[3]; /* (window[1]-window[0])/n, as src/PSI.c:111-113 computes it */
+    double *fields[6];
+} psib_grid;
+
+/* Lagrangian mesh.  pos and vel are npart x 3 doubles (vel may be NULL:
+ * zeros), mass is one double per element (NULL: ones).  connectivity is
+ * nelem x elemtype ints (elemtype 4 or 8).  With connectivity == NULL and
+ * block_dims set, the trilinear block connectivity of src/PSI.c:636-656 is
+ * implied (periodic wrap when periodic != 0), and is never materialised. */
+typedef struct {
+    int elemtype;
+    long long npart;
+    long long nelem;
+    const double *pos;
+    const double *vel;
+    const double *mass;
+    const int *connectivity;
+    int block_dims[3];
+    int periodic;
+    double box[2][3];
+} psib_mesh;
+
+/* Work counters and timings of one call (all optional outputs). */
+typedef struct {
+    long long elements_kept; /* elements surviving the window cull */
+    long long tets;          /* tets after refinement, without periodic images */
+    long long tet_images;    /* tets including periodic images (work items) */
+    long long fragments;     /* (tet image, voxel) pieces with m0 > 0, summed over passes */
+    long long frag_verts;    /* sum of fragment vertex counts, summed over passes */
+    long long splits;        /* axis-aligned splits, summed over passes */
+    int passes;              /* clip passes over the tets (2 for second-order fields) */
+    int chunks;              /* element chunks the tets were streamed in */
+    float ms_total;          /* device time of the whole call, host copies included */
+    float ms_clip;           /* device time of the clip-and-deposit kernels */
+    float ms_tess;           /* device time of tessellation and ordering */
+    float ms_final;          /* device time of the finalisation kernels */
+    long long clip_launches; /* launches of the clip-and-deposit kernels */
+    long long kernel_launches; /* launches of this library's own kernels (library scans/sorts excluded) */
+} psib_stats;
+
+typedef struct {
+    int precision;     /* PSIB_FP64 or PSIB_MIXED */
+    int deterministic; /* 1: sort-and-segmented-update mode, bit-reproducible (FP64 only) */
+    int memory;        /* PSIB_HOST or PSIB_DEVICE */
+    int device;        /* CUDA device ordinal for PSIB_HOST calls (-1: current) */
+    void *stream;      /* cudaStream_t for PSIB_DEVICE calls; NULL: legacy default stream */
+    psib_stats *stats; /* optional */
+} psib_options;
+
+/* Deposit the mesh's tets on the grid: the density branch of psi_voxels
+ * (src/cpsi.c:41-112) with refinement as src/refine.c:58-289.
+ * refine_max_lvl is capped at 6 like src/refine.c:89-92. */
+int psib_voxels(const psib_grid *grid, const psib_mesh *mesh, int mode, double refine_tolerance,
+                int refine_max_lvl, const psib_options *opt);
+
+/* Message for the last failure on this thread ("" if none). */
+const char *psib_last_error(void);
+
+/* ABI version (PSIB_ABI_VERSION) and the number of visible CUDA devices
+ * (0 when none or the driver is absent). */
+int psib_abi_version(void);
+int psib_device_count(void);
+
+/* Page-locked host memory for grid fields, so that host<->device copies run
+ * at full link speed.  Returns NULL on failure (e.g. no device); release with
+ * psib_host_free. */
+void *psib_host_alloc(unsigned long long bytes);
+void psib_host_free(void *p);
+
+/* Release the library's cached device buffers on the current device. */
+int psib_release_device_memory(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PSI_B200_H */

@@ -1,0 +1,209 @@
+"""ctypes front end of the test oracle.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, ``__graft_entry__.smoke()`` and
+bench.py's CPU-baseline / reference legs as the checker.  The product package
+``pypsi_b200`` never imports it.
+
+Two back ends with one interface:
+
+* ``restatement`` -- ``_build/liboracle.so`` from ``psi_oracle.c``, a step by
+  step C restatement of the reference density path with work counters;
+* ``reference``   -- ``_ref/libpsiref.so``, the reference's own sources
+  (src/cpsi.c, src/geometry.c, src/refine.c, ...) compiled unchanged; its entry
+  ``psi_voxels`` is declared at src/PSI.c:39 and defined at src/cpsi.c:41.
+
+``voxelize`` returns the grid fields in the reference's layout
+(src/PSI.c:124-186): ``m`` (nx,ny,nz), ``x``/``v`` (...,3), ``xx``/``xv``/``vv``
+(...,3,3), all float64.
+"""
+from __future__ import annotations
+
+import contextlib
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_ORACLE = os.path.join(HERE, "_build", "liboracle.so")
+LIB_REF = os.path.join(HERE, "_ref", "libpsiref.so")
+FIELD_NAMES = ("m", "x", "v", "xx", "xv", "vv")
+
+
+def build(ref_root: str = "/root/reference", quiet: bool = True) -> None:
+    """Compile the restatement, and the reference when its tree is present."""
+    targets = ["oracle"]
+    if os.path.isdir(os.path.join(ref_root, "src")):
+        targets.append("ref")
+    out = subprocess.run(["make", "-C", HERE, f"REF={ref_root}", *targets],
+                         capture_output=True, text=True)
+    if out.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
+
+
+# ---- restatement structs (psi_oracle.c) ----
+class _OgGrid(C.Structure):
+    _fields_ = [("n", C.c_int * 3), ("win", (C.c_double * 3) * 2), ("d", C.c_double * 3),
+                ("f", C.POINTER(C.c_double) * 6)]
+
+
+class _OgMesh(C.Structure):
+    _fields_ = [("elemtype", C.c_int), ("npart", C.c_int), ("nelem", C.c_int),
+                ("pos", C.POINTER(C.c_double)), ("vel", C.POINTER(C.c_double)),
+                ("mass", C.POINTER(C.c_double)), ("conn", C.POINTER(C.c_int)),
+                ("periodic", C.c_int), ("box", (C.c_double * 3) * 2)]
+
+
+class Counters(C.Structure):
+    _fields_ = [("elements_kept", C.c_longlong), ("tets", C.c_longlong),
+                ("tet_images", C.c_longlong), ("fragments", C.c_longlong),
+                ("splits", C.c_longlong), ("frag_verts", C.c_longlong),
+                ("max_verts", C.c_longlong), ("errors", C.c_longlong)]
+
+    def as_dict(self):
+        return {k: int(getattr(self, k)) for k, _ in self._fields_}
+
+
+# ---- reference structs (include/grid.h:46-53, include/mesh.h:42-52) ----
+class _PsiGrid(C.Structure):
+    _fields_ = [("type", C.c_int), ("dim", C.c_int), ("fields", C.POINTER(C.c_double) * 16),
+                ("window", (C.c_double * 3) * 2), ("n", C.c_int * 3), ("d", C.c_double * 3)]
+
+
+class _PsiMesh(C.Structure):
+    _fields_ = [("elemtype", C.c_int), ("dim", C.c_int), ("pos", C.POINTER(C.c_double)),
+                ("vel", C.POINTER(C.c_double)), ("mass", C.POINTER(C.c_double)),
+                ("npart", C.c_int), ("nelem", C.c_int), ("connectivity", C.POINTER(C.c_int)),
+                ("box", (C.c_double * 3) * 2), ("periodic", C.c_int)]
+
+
+_libs: dict[str, C.CDLL] = {}
+
+
+def _lib(kind: str) -> C.CDLL:
+    if kind not in _libs:
+        path = LIB_ORACLE if kind == "restatement" else LIB_REF
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} not built (run oracle.build())")
+        lib = C.CDLL(path)
+        if kind == "restatement":
+            lib.oracle_voxels.argtypes = [C.POINTER(_OgGrid), C.POINTER(_OgMesh), C.c_double,
+                                          C.c_int, C.POINTER(Counters)]
+            lib.oracle_voxels.restype = C.c_int
+        else:
+            lib.psi_voxels.argtypes = [C.POINTER(_PsiGrid), C.POINTER(_PsiMesh), C.c_void_p,
+                                       C.c_int, C.c_double, C.c_int]
+            lib.psi_voxels.restype = None
+        _libs[kind] = lib
+    return _libs[kind]
+
+
+def available(kind: str) -> bool:
+    return os.path.exists(LIB_ORACLE if kind == "restatement" else LIB_REF)
+
+
+@contextlib.contextmanager
+def _quiet_stdout():
+    """The reference prints a progress line per 1024 elements (src/cpsi.c:82-83)."""
+    import sys
+    sys.stdout.flush()
+    saved = os.dup(1)
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    try:
+        os.dup2(devnull, 1)
+        yield
+    finally:
+        libc = C.CDLL(None)
+        libc.fflush(None)
+        os.dup2(saved, 1)
+        os.close(saved)
+        os.close(devnull)
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double)) if a is not None else None
+
+
+def new_fields(n, fields):
+    n = tuple(int(v) for v in n)
+    shapes = {"m": n, "x": n + (3,), "v": n + (3,), "xx": n + (3, 3), "xv": n + (3, 3), "vv": n + (3, 3)}
+    out = {"m": np.zeros(shapes["m"])}
+    for f in fields:
+        f = "xv" if f == "vx" else f
+        out[f] = np.zeros(shapes[f])
+    return out
+
+
+def voxelize(kind, n, bounds, pos, conn, vel=None, mass=None, periodic_box=None, fields=(),
+             reftol=1.0, maxlvl=0, out=None, counters=False):
+    """Run the density path of the chosen back end.
+
+    pos (npart,3) f64, conn (nelem, 4|8) i32, vel like pos (zeros if None),
+    mass (nelem,) (ones if None).  ``out`` (a dict of field arrays) is
+    accumulated into, as the reference accumulates into grid.fields.
+    """
+    lib = _lib(kind)
+    pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
+    conn = np.ascontiguousarray(conn, dtype=np.int32)
+    conn = conn.reshape(conn.shape[0], -1)
+    npart, nelem, et = pos.shape[0], conn.shape[0], conn.shape[1]
+    vel = np.zeros_like(pos) if vel is None else np.ascontiguousarray(vel, dtype=np.float64).reshape(-1, 3)
+    mass = np.ones(nelem) if mass is None else np.ascontiguousarray(mass, dtype=np.float64).reshape(-1)
+    if out is None:
+        out = new_fields(n, fields)
+    n = [int(v) for v in n]
+    lo = [float(v) for v in bounds[0]]
+    hi = [float(v) for v in bounds[1]]
+    d = [(hi[i] - lo[i]) / n[i] for i in range(3)]  # src/PSI.c:111-113
+    box = periodic_box if periodic_box is not None else ((0.0,) * 3, (0.0,) * 3)
+    for f, a in out.items():
+        assert a.dtype == np.float64 and a.flags.c_contiguous, f
+    ptrs = [_dp(out.get(f)) for f in FIELD_NAMES]
+    if kind == "restatement":
+        g = _OgGrid()
+        g.n[:] = n
+        g.win[0][:] = lo
+        g.win[1][:] = hi
+        g.d[:] = d
+        for i, p in enumerate(ptrs):
+            g.f[i] = p
+        m = _OgMesh(elemtype=et, npart=npart, nelem=nelem, pos=_dp(pos), vel=_dp(vel), mass=_dp(mass),
+                    conn=conn.ctypes.data_as(C.POINTER(C.c_int)), periodic=int(periodic_box is not None))
+        m.box[0][:] = [float(v) for v in box[0]]
+        m.box[1][:] = [float(v) for v in box[1]]
+        cnt = Counters()
+        rc = lib.oracle_voxels(C.byref(g), C.byref(m), float(reftol), int(maxlvl), C.byref(cnt))
+        if rc != 0:
+            raise RuntimeError("oracle_voxels failed")
+        return (out, cnt.as_dict()) if counters else out
+    g = _PsiGrid(type=0, dim=3)
+    g.n[:] = n
+    g.window[0][:] = lo
+    g.window[1][:] = hi
+    g.d[:] = d
+    for i, p in enumerate(ptrs):
+        if p is not None:
+            g.fields[i] = p
+    m = _PsiMesh(elemtype=et, dim=3, pos=_dp(pos), vel=_dp(vel), mass=_dp(mass), npart=npart, nelem=nelem,
+                 connectivity=conn.ctypes.data_as(C.POINTER(C.c_int)), periodic=int(periodic_box is not None))
+    m.box[0][:] = [float(v) for v in box[0]]
+    m.box[1][:] = [float(v) for v in box[1]]
+    with _quiet_stdout():
+        lib.psi_voxels(C.byref(g), C.byref(m), None, 0, float(reftol), int(maxlvl))
+    return (out, None) if counters else out
+
+
+def block_connectivity(nside, periodic):
+    """Trilinear connectivity of a block mesh, as PSI.Mesh(loader='block') builds it
+    (src/PSI.c:553-560, :636-656): element (i,j,k) -> vertices 4ii+2jj+kk."""
+    nx, ny, nz = (int(v) for v in nside)
+    ne = (nx, ny, nz) if periodic else (nx - 1, ny - 1, nz - 1)
+    i, j, k = np.meshgrid(np.arange(ne[0]), np.arange(ne[1]), np.arange(ne[2]), indexing="ij")
+    conn = np.empty(ne + (8,), dtype=np.int32)
+    for ii in range(2):
+        for jj in range(2):
+            for kk in range(2):
+                conn[..., 4 * ii + 2 * jj + kk] = (ny * nz * ((i + ii) % nx) + nz * ((j + jj) % ny)
+                                                   + ((k + kk) % nz))
+    return conn.reshape(-1, 8)

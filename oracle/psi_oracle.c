@@ -1,0 +1,682 @@
+/*
+ * psi_oracle.c -- CPU restatement of PSI.voxels(grid, mesh) in density mode.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker for the CUDA path.  Only
+ * tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg load it; the
+ * product library (pypsi_b200) never links, imports or calls anything here.
+ *
+ * It restates the reference algorithm of devonmpowell/PyPSI (files cited as
+ * path:line inside that project) one step at a time, keeping every
+ * floating-point operation in the reference's order so that, compiled with
+ * -ffp-contract=off and no FMA, it reproduces the reference bit for bit.  That
+ * claim is pinned by tests/test_oracle_pin.py against the reference's own
+ * sources compiled into oracle/_ref/ (oracle/Makefile).
+ *
+ * Beyond the reference it keeps work counters (tets, tet images, fragments,
+ * splits, fragment vertices) which give the algorithmic work units of a run.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define OV_MAXV 64        /* vertex buffer of one polyhedron (include/geometry.h:23) */
+#define OV_STACK 64       /* bisection stack depth (src/geometry.c:41-46) */
+#define OV_WALK_CAP 4096  /* bound on a face walk; the reference has none */
+
+/* ---- public structs (mirrored by oracle/oracle.py with ctypes) ---- */
+
+typedef struct {
+    int n[3];
+    double win[2][3];
+    double d[3];
+    double *f[6]; /* m, x, v, xx, xv, vv (include/grid.h:37-42); NULL when absent */
+} og_grid;
+
+typedef struct {
+    int elemtype;            /* 4, 8 (27 is rejected by this oracle) */
+    int npart, nelem;
+    const double *pos, *vel; /* npart x 3 */
+    const double *mass;      /* nelem */
+    const int *conn;         /* nelem x elemtype */
+    int periodic;
+    double box[2][3];
+} og_mesh;
+
+typedef struct {
+    long long elements_kept; /* elements that survive the window cull */
+    long long tets;          /* tets after refinement, without periodic images */
+    long long tet_images;    /* tets including periodic images */
+    long long fragments;     /* (tet image, voxel) pieces with m0 > 0 */
+    long long splits;        /* calls of the axis-aligned split */
+    long long frag_verts;    /* sum of vertex counts over emitted fragments */
+    long long max_verts;     /* largest vertex count of any polyhedron seen */
+    long long errors;        /* vertex-buffer overflow or a face walk that did not close */
+} og_counters;
+
+/* ---- polyhedron: r3d vertex graph with barycentric mass coordinates q ---- */
+
+typedef struct {
+    double pos[3];
+    double q[3];
+    int nbr[3];
+} ov_vert;
+
+typedef struct {
+    int nv;
+    int lo[3], hi[3]; /* voxel index box (src/geometry.c:838-841) */
+    ov_vert v[OV_MAXV];
+} ov_poly;
+
+static og_counters *g_cnt;
+
+static void note_nv(int nv)
+{
+    if (nv > g_cnt->max_verts) g_cnt->max_verts = nv;
+}
+
+/* Link each vertex created by a cut to its two neighbours on the cut face by
+ * walking around the face it opens (src/geometry.c:459-482, :646-669). */
+static int link_new_vertices(ov_poly *P, int onv, int nv)
+{
+    for (int vs = onv; vs < nv; ++vs) {
+        int vc = vs, vn = P->v[vs].nbr[0], k = 0, steps = 0;
+        do {
+            for (k = 0; k < 3; ++k)
+                if (P->v[vn].nbr[k] == vc) break;
+            if (k == 3 || ++steps > OV_WALK_CAP) return -1;
+            vc = vn;
+            vn = P->v[vc].nbr[(k + 1) % 3];
+        } while (vc < onv);
+        P->v[vs].nbr[2] = vc;
+        P->v[vc].nbr[1] = vs;
+    }
+    return 0;
+}
+
+/* Clip by half-spaces n.x + d >= 0 (src/geometry.c:391-501). */
+static void ov_clip(ov_poly *P, const double (*pn)[3], const double *pd, int nplanes)
+{
+    if (P->nv <= 0) return;
+    for (int p = 0; p < nplanes; ++p) {
+        int onv = P->nv;
+        double s[OV_MAXV];
+        int map[OV_MAXV];
+        double smin = 1.0e30, smax = -1.0e30;
+        memset(map, 0, sizeof(map));
+        for (int v = 0; v < onv; ++v) {
+            s[v] = pd[p];
+            for (int i = 0; i < 3; ++i) s[v] += P->v[v].pos[i] * pn[p][i];
+            if (s[v] < smin) smin = s[v];
+            if (s[v] > smax) smax = s[v];
+            if (s[v] < 0.0) map[v] = 1;
+        }
+        if (smin >= 0.0) continue;
+        if (smax <= 0.0) {
+            P->nv = 0;
+            return;
+        }
+        int nv = onv;
+        for (int vc = 0; vc < onv; ++vc) {
+            if (map[vc]) continue;
+            for (int k = 0; k < 3; ++k) {
+                int vn = P->v[vc].nbr[k];
+                if (!map[vn]) continue;
+                if (nv >= OV_MAXV) { g_cnt->errors++; P->nv = 0; return; }
+                double w = 1.0 / (s[vc] - s[vn]);
+                ov_vert *a = &P->v[vc], *b = &P->v[vn], *c = &P->v[nv];
+                for (int i = 0; i < 3; ++i) c->pos[i] = w * (b->pos[i] * s[vc] - a->pos[i] * s[vn]);
+                for (int i = 0; i < 3; ++i) c->q[i] = w * (b->q[i] * s[vc] - a->q[i] * s[vn]);
+                c->nbr[0] = vc;
+                a->nbr[k] = nv;
+                nv++;
+            }
+        }
+        if (link_new_vertices(P, onv, nv)) { g_cnt->errors++; P->nv = 0; return; }
+        note_nv(nv);
+        int cnt = 0;
+        for (int v = 0; v < nv; ++v) {
+            if (!map[v]) {
+                P->v[cnt] = P->v[v];
+                map[v] = cnt++;
+            }
+        }
+        P->nv = cnt;
+        for (int v = 0; v < cnt; ++v)
+            for (int k = 0; k < 3; ++k) P->v[v].nbr[k] = map[P->v[v].nbr[k]];
+    }
+}
+
+/* Split by the plane x[ax] = coord into out[0] (x <= coord) and out[1]
+ * (src/geometry.c:560-690).  `in` is used as scratch. */
+static void ov_split(ov_poly *in, ov_poly *out, double coord, int ax)
+{
+    double s[OV_MAXV];
+    int side[OV_MAXV];
+    int nright = 0, onv = in->nv;
+    memset(side, 0, sizeof(side));
+    g_cnt->splits++;
+    for (int v = 0; v < onv; ++v) {
+        s[v] = coord - in->v[v].pos[ax];
+        if (s[v] < 0.0) {
+            side[v] = 1;
+            nright++;
+        }
+    }
+    if (nright == 0) {
+        out[0] = *in;
+        out[1].nv = 0;
+        return;
+    }
+    if (nright == onv) {
+        out[1] = *in;
+        out[0].nv = 0;
+        return;
+    }
+    int nv = onv;
+    for (int vc = 0; vc < onv; ++vc) {
+        if (side[vc]) continue;
+        for (int k = 0; k < 3; ++k) {
+            int vn = in->v[vc].nbr[k];
+            if (!side[vn]) continue;
+            if (nv + 2 > OV_MAXV) { g_cnt->errors++; out[0].nv = out[1].nv = 0; return; }
+            double w = 1.0 / (s[vc] - s[vn]);
+            ov_vert *a = &in->v[vc], *b = &in->v[vn];
+            double np_[3], nq[3];
+            for (int i = 0; i < 3; ++i) {
+                np_[i] = w * (b->pos[i] * s[vc] - a->pos[i] * s[vn]);
+                nq[i] = w * (b->q[i] * s[vc] - a->q[i] * s[vn]);
+            }
+            ov_vert *l = &in->v[nv], *r = &in->v[nv + 1];
+            memcpy(l->pos, np_, sizeof(np_));
+            memcpy(l->q, nq, sizeof(nq));
+            l->nbr[0] = vc;
+            a->nbr[k] = nv;
+            memcpy(r->pos, np_, sizeof(np_));
+            memcpy(r->q, nq, sizeof(nq));
+            side[nv + 1] = 1;
+            r->nbr[0] = vn;
+            int kb;
+            for (kb = 0; kb < 3; ++kb)
+                if (b->nbr[kb] == vc) break;
+            if (kb == 3) { g_cnt->errors++; out[0].nv = out[1].nv = 0; return; }
+            b->nbr[kb] = nv + 1;
+            nv += 2;
+        }
+    }
+    if (link_new_vertices(in, onv, nv)) { g_cnt->errors++; out[0].nv = out[1].nv = 0; return; }
+    note_nv(nv);
+    out[0].nv = 0;
+    out[1].nv = 0;
+    for (int v = 0; v < nv; ++v) {
+        ov_poly *o = &out[side[v]];
+        o->v[o->nv] = in->v[v];
+        side[v] = o->nv++;
+    }
+    for (int h = 0; h < 2; ++h)
+        for (int v = 0; v < out[h].nv; ++v)
+            for (int k = 0; k < 3; ++k) out[h].v[v].nbr[k] = side[out[h].v[v].nbr[k]];
+}
+
+/* Moments of the polyhedron in q-space, orders 0..2 (1, 4 or 10 values), by
+ * fan-triangulating every face (src/geometry.c:692-767). */
+static void ov_reduce(const ov_poly *P, double *mom, int order)
+{
+    static const int nmom[3] = {1, 4, 10};
+    unsigned char done[OV_MAXV][3];
+    memset(mom, 0, nmom[order] * sizeof(double));
+    memset(done, 0, sizeof(done));
+    for (int vs = 0; vs < P->nv; ++vs)
+        for (int ks = 0; ks < 3; ++ks) {
+            if (done[vs][ks]) continue;
+            int vc = vs, kn = ks, k;
+            done[vc][kn] = 1;
+            int vn = P->v[vc].nbr[kn];
+            const double *q0 = P->v[vc].q;
+            for (k = 0; k < 3; ++k)
+                if (P->v[vn].nbr[k] == vc) break;
+            vc = vn;
+            kn = (k + 1) % 3;
+            done[vc][kn] = 1;
+            vn = P->v[vc].nbr[kn];
+            int steps = 0;
+            while (vn != vs) {
+                if (++steps > OV_WALK_CAP) { g_cnt->errors++; return; }
+                const double *q1 = P->v[vn].q;
+                const double *q2 = P->v[vc].q;
+                /* 6 x signed volume of the cone (0, q0, q1, q2) */
+                double m = (-q2[0] * q1[1] * q0[2] + q1[0] * q2[1] * q0[2] + q2[0] * q0[1] * q1[2]
+                            - q0[0] * q2[1] * q1[2] - q1[0] * q0[1] * q2[2] + q0[0] * q1[1] * q2[2]);
+                mom[0] += m;
+                if (order > 0) {
+                    mom[1] += 0.25 * m * (q0[0] + q1[0] + q2[0]);
+                    mom[2] += 0.25 * m * (q0[1] + q1[1] + q2[1]);
+                    mom[3] += 0.25 * m * (q0[2] + q1[2] + q2[2]);
+                }
+                if (order > 1) {
+                    mom[4] += 0.1 * m * (q0[0] * q0[0] + q1[0] * q1[0] + q2[0] * q2[0] + q1[0] * q2[0] + q0[0] * (q1[0] + q2[0]));
+                    mom[5] += 0.05 * m * (q2[0] * q0[1] + q2[0] * q1[1] + 2 * q2[0] * q2[1] + q0[0] * (2 * q0[1] + q1[1] + q2[1]) + q1[0] * (q0[1] + 2 * q1[1] + q2[1]));
+                    mom[6] += 0.05 * m * (q2[0] * q0[2] + q2[0] * q1[2] + 2 * q2[0] * q2[2] + q0[0] * (2 * q0[2] + q1[2] + q2[2]) + q1[0] * (q0[2] + 2 * q1[2] + q2[2]));
+                    mom[7] += 0.1 * m * (q0[1] * q0[1] + q1[1] * q1[1] + q2[1] * q2[1] + q1[1] * q2[1] + q0[1] * (q1[1] + q2[1]));
+                    mom[8] += 0.05 * m * (q2[1] * q0[2] + q2[1] * q1[2] + 2 * q2[1] * q2[2] + q0[1] * (2 * q0[2] + q1[2] + q2[2]) + q1[1] * (q0[2] + 2 * q1[2] + q2[2]));
+                    mom[9] += 0.1 * m * (q0[2] * q0[2] + q1[2] * q1[2] + q2[2] * q2[2] + q1[2] * q2[2] + q0[2] * (q1[2] + q2[2]));
+                }
+                for (k = 0; k < 3; ++k)
+                    if (P->v[vn].nbr[k] == vc) break;
+                vc = vn;
+                kn = (k + 1) % 3;
+                done[vc][kn] = 1;
+                vn = P->v[vc].nbr[kn];
+            }
+        }
+}
+
+/* The tet as a vertex graph with q = (0, e_x, e_y, e_z) (src/geometry.c:769-804). */
+static void ov_init_tet(ov_poly *P, const double (*pos)[3])
+{
+    static const int nb[4][3] = {{1, 3, 2}, {2, 3, 0}, {0, 3, 1}, {1, 2, 0}};
+    memset(P, 0, sizeof(*P));
+    P->nv = 4;
+    for (int v = 0; v < 4; ++v) {
+        for (int k = 0; k < 3; ++k) P->v[v].nbr[k] = nb[v][k];
+        for (int i = 0; i < 3; ++i) P->v[v].pos[i] = pos[v][i];
+    }
+    P->v[1].q[0] = 1.0;
+    P->v[2].q[1] = 1.0;
+    P->v[3].q[2] = 1.0;
+}
+
+/* Deposit one tet image on the grid: window clip, index box, bisection to
+ * single voxels, moment projection and the online field update
+ * (src/geometry.c:60-188, :806-896). */
+static void ov_voxelize_tet(const double (*pos)[3], const double (*vel)[3], double mass,
+                            const double (*rbox)[3], const og_grid *g, ov_poly *stack)
+{
+    static const int qi[3][3] = {{4, 5, 6}, {5, 7, 8}, {6, 8, 9}};
+    double DX[3][3], DV[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            DX[i][j] = pos[j + 1][i] - pos[0][i];
+            DV[i][j] = vel[j + 1][i] - vel[0][i];
+        }
+    int order = 0;
+    if (g->f[1] || g->f[2]) order = 1;
+    if (g->f[3] || g->f[4] || g->f[5]) order = 2;
+
+    ov_poly *P = &stack[0];
+    ov_init_tet(P, pos);
+
+    /* window planes and index box (src/geometry.c:806-843) */
+    double pn[6][3], pd[6];
+    int npl = 0;
+    memset(pn, 0, sizeof(pn));
+    memset(pd, 0, sizeof(pd));
+    for (int i = 0; i < 3; ++i) {
+        double cmin = rbox[0][i], cmax = rbox[1][i];
+        int clo = 0, chi = 0;
+        if (g->win[0][i] > cmin) { cmin = g->win[0][i]; clo = 1; }
+        if (g->win[1][i] < cmax) { cmax = g->win[1][i]; chi = 1; }
+        if (clo) { pn[npl][i] = 1.0; pd[npl] = -cmin; npl++; }
+        if (chi) { pn[npl][i] = -1.0; pd[npl] = cmax; npl++; }
+        P->lo[i] = (int)floor((cmin - g->win[0][i]) / g->d[i]);
+        P->hi[i] = (int)ceil((cmax - g->win[0][i]) / g->d[i]);
+        if (P->lo[i] < 0) P->lo[i] = 0;
+        if (P->hi[i] > g->n[i]) P->hi[i] = g->n[i];
+    }
+    note_nv(P->nv);
+    ov_clip(P, (const double(*)[3])pn, pd, npl);
+
+    int top = 1;
+    ov_poly cur;
+    double mom[10];
+    while (top > 0) {
+        cur = stack[--top];
+        if (cur.nv <= 0) continue;
+        int dmax = 0, ax = 0;
+        for (int i = 0; i < 3; ++i) {
+            int sz = cur.hi[i] - cur.lo[i];
+            if (sz > dmax) { dmax = sz; ax = i; }
+        }
+        if (dmax <= 1) {
+            /* dmax == 0 only for a tet image collapsed onto grid planes in every
+             * axis; the reference loops forever there, this oracle reduces it. */
+            ov_reduce(&cur, mom, order);
+            if (mom[0] <= 0.0) continue;
+            if (cur.lo[0] >= g->n[0] || cur.lo[1] >= g->n[1] || cur.lo[2] >= g->n[2]) {
+                g_cnt->errors++;
+                continue;
+            }
+            long long gi = (long long)g->n[1] * g->n[2] * cur.lo[0] + (long long)g->n[2] * cur.lo[1] + cur.lo[2];
+            g_cnt->fragments++;
+            g_cnt->frag_verts += cur.nv;
+
+            double cm[3], cv[3], sxx[3][3], sxv[3][3], svv[3][3];
+            if (g->f[1])
+                for (int i = 0; i < 3; ++i) {
+                    cm[i] = mom[0] * pos[0][i];
+                    for (int j = 0; j < 3; ++j) cm[i] += mom[j + 1] * DX[i][j];
+                    cm[i] /= mom[0];
+                }
+            if (g->f[2])
+                for (int i = 0; i < 3; ++i) {
+                    cv[i] = mom[0] * vel[0][i];
+                    for (int j = 0; j < 3; ++j) cv[i] += mom[j + 1] * DV[i][j];
+                    cv[i] /= mom[0];
+                }
+            if (g->f[3])
+                for (int i = 0; i < 3; ++i)
+                    for (int j = 0; j < 3; ++j) {
+                        sxx[i][j] = mom[0] * (pos[0][i] - cm[i]) * (pos[0][j] - cm[j]);
+                        for (int a = 0; a < 3; ++a) {
+                            sxx[i][j] += DX[i][a] * mom[1 + a] * (pos[0][j] - cm[j]);
+                            sxx[i][j] += DX[j][a] * mom[1 + a] * (pos[0][i] - cm[i]);
+                        }
+                        for (int a = 0; a < 3; ++a)
+                            for (int b = 0; b < 3; ++b) sxx[i][j] += DX[i][a] * DX[j][b] * mom[qi[a][b]];
+                        sxx[i][j] /= mom[0];
+                    }
+            if (g->f[4])
+                /* the reference pairs DX with (x0 - cm) and DV with (v0 - cv)
+                 * in the two cross terms (src/geometry.c:139-140); kept as is */
+                for (int i = 0; i < 3; ++i)
+                    for (int j = 0; j < 3; ++j) {
+                        sxv[i][j] = mom[0] * (pos[0][i] - cm[i]) * (vel[0][j] - cv[j]);
+                        for (int a = 0; a < 3; ++a) {
+                            sxv[i][j] += DX[i][a] * mom[1 + a] * (pos[0][j] - cm[j]);
+                            sxv[i][j] += DV[j][a] * mom[1 + a] * (vel[0][i] - cv[i]);
+                        }
+                        for (int a = 0; a < 3; ++a)
+                            for (int b = 0; b < 3; ++b) sxv[i][j] += DX[i][a] * DV[j][b] * mom[qi[a][b]];
+                        sxv[i][j] /= mom[0];
+                    }
+            if (g->f[5])
+                for (int i = 0; i < 3; ++i)
+                    for (int j = 0; j < 3; ++j) {
+                        svv[i][j] = mom[0] * (vel[0][i] - cv[i]) * (vel[0][j] - cv[j]);
+                        for (int a = 0; a < 3; ++a) {
+                            svv[i][j] += DV[i][a] * mom[1 + a] * (vel[0][j] - cv[j]);
+                            svv[i][j] += DV[j][a] * mom[1 + a] * (vel[0][i] - cv[i]);
+                        }
+                        for (int a = 0; a < 3; ++a)
+                            for (int b = 0; b < 3; ++b) svv[i][j] += DV[i][a] * DV[j][b] * mom[qi[a][b]];
+                        svv[i][j] /= mom[0];
+                    }
+
+            /* online weighted update (src/geometry.c:164-186) */
+            double *M = g->f[0], *X = g->f[1], *V = g->f[2];
+            double cw = mass * mom[0] / (M[gi] + mass * mom[0]);
+            double dw = M[gi] / (M[gi] + mass * mom[0]);
+            if (g->f[3])
+                for (int i = 0; i < 3; ++i)
+                    for (int j = 0; j < 3; ++j) {
+                        double *t = &g->f[3][9 * gi + 3 * i + j];
+                        *t = dw * *t + cw * sxx[i][j] + cw * dw * (cm[i] - X[3 * gi + i]) * (cm[j] - X[3 * gi + j]);
+                    }
+            if (g->f[4])
+                for (int i = 0; i < 3; ++i)
+                    for (int j = 0; j < 3; ++j) {
+                        double *t = &g->f[4][9 * gi + 3 * i + j];
+                        *t = dw * *t + cw * sxv[i][j] + cw * dw * (cm[i] - X[3 * gi + i]) * (cv[j] - V[3 * gi + j]);
+                    }
+            if (g->f[5])
+                for (int i = 0; i < 3; ++i)
+                    for (int j = 0; j < 3; ++j) {
+                        double *t = &g->f[5][9 * gi + 3 * i + j];
+                        *t = dw * *t + cw * svv[i][j] + cw * dw * (cv[i] - V[3 * gi + i]) * (cv[j] - V[3 * gi + j]);
+                    }
+            if (X)
+                for (int i = 0; i < 3; ++i) X[3 * gi + i] += cw * (cm[i] - X[3 * gi + i]);
+            if (V)
+                for (int i = 0; i < 3; ++i) V[3 * gi + i] += cw * (cv[i] - V[3 * gi + i]);
+            M[gi] += mass * mom[0];
+            continue;
+        }
+        if (top + 2 > OV_STACK) { g_cnt->errors++; continue; }
+        double coord = g->d[ax] * (cur.lo[ax] + dmax / 2) + g->win[0][ax];
+        ov_split(&cur, &stack[top], coord, ax);
+        memcpy(stack[top].lo, cur.lo, sizeof(cur.lo));
+        memcpy(stack[top].hi, cur.hi, sizeof(cur.hi));
+        stack[top].hi[ax] -= dmax - dmax / 2;
+        memcpy(stack[top + 1].lo, cur.lo, sizeof(cur.lo));
+        memcpy(stack[top + 1].hi, cur.hi, sizeof(cur.hi));
+        stack[top + 1].lo[ax] += dmax / 2;
+        top += 2;
+    }
+}
+
+/* ---- element -> tets (src/refine.c) ---- */
+
+typedef struct {
+    double (*pos)[3]; /* 4 per tet */
+    double (*vel)[3];
+    double *mass;
+    int num, cap;
+    int max_lvl;
+    double ptol2;
+} ov_tetbuf;
+
+static const int TET_CORNERS[6][4] = {{2, 0, 6, 18}, {8, 2, 6, 18}, {8, 20, 2, 18},
+                                      {8, 24, 20, 18}, {8, 6, 24, 18}, {8, 26, 20, 24}}; /* src/refine.c:39-41 */
+#define I2(a, b, c) (4 * (a) + 2 * (b) + (c))
+#define I3(a, b, c) (9 * (a) + 3 * (b) + (c))
+
+static int tetbuf_reserve(ov_tetbuf *tb, int extra)
+{
+    if (tb->num + extra > tb->cap) {
+        int nc = tb->cap ? 2 * tb->cap : 64;
+        while (nc < tb->num + extra) nc *= 2;
+        void *a = realloc(tb->pos, (size_t)nc * 4 * sizeof(*tb->pos));
+        if (!a) return -1;
+        tb->pos = a;
+        a = realloc(tb->vel, (size_t)nc * 4 * sizeof(*tb->vel));
+        if (!a) return -1;
+        tb->vel = a;
+        a = realloc(tb->mass, (size_t)nc * sizeof(double));
+        if (!a) return -1;
+        tb->mass = a;
+        tb->cap = nc;
+    }
+    return 0;
+}
+
+static int tetbuf_push6(ov_tetbuf *tb, const double (*p)[3], const double (*u)[3], double mass)
+{
+    if (tetbuf_reserve(tb, 6)) return -1;
+    for (int t = 0; t < 6; ++t) {
+        for (int v = 0; v < 4; ++v) {
+            int c = TET_CORNERS[t][v];
+            memcpy(tb->pos[4 * tb->num + v], p[c], 3 * sizeof(double));
+            memcpy(tb->vel[4 * tb->num + v], u[c], 3 * sizeof(double));
+        }
+        tb->mass[tb->num] = mass * (1.0 / 6); /* M_PER_TET, src/refine.c:49,147 */
+        tb->num++;
+    }
+    return 0;
+}
+
+/* 8 cube corners -> 27 nodes by repeated midpoints (src/refine.c:292-319). */
+static void interp_trilinear(const double (*in)[3], double (*out)[3])
+{
+    for (int ax = 0; ax < 3; ++ax) {
+        for (int i = 0; i < 2; ++i)
+            for (int j = 0; j < 2; ++j)
+                for (int k = 0; k < 2; ++k) out[I3(2 * i, 2 * j, 2 * k)][ax] = in[I2(i, j, k)][ax];
+        for (int j = 0; j < 3; j += 2)
+            for (int k = 0; k < 3; k += 2)
+                out[I3(1, j, k)][ax] = 0.5 * (out[I3(0, j, k)][ax] + out[I3(2, j, k)][ax]);
+        for (int i = 0; i < 3; ++i)
+            for (int k = 0; k < 3; k += 2)
+                out[I3(i, 1, k)][ax] = 0.5 * (out[I3(i, 0, k)][ax] + out[I3(i, 2, k)][ax]);
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j)
+                out[I3(i, j, 1)][ax] = 0.5 * (out[I3(i, j, 0)][ax] + out[I3(i, j, 2)][ax]);
+    }
+}
+
+/* Adaptive octree refinement of a trilinear element (src/refine.c:223-289). */
+static int refine_trilinear(ov_tetbuf *tb, const double (*p)[3], const double (*u)[3], double mass, int lvl)
+{
+    static const int edges[7][3] = {{2, 4, 6}, {2, 10, 18}, {6, 12, 18}, {8, 13, 18},
+                                    {8, 14, 20}, {8, 16, 24}, {20, 22, 24}};
+    if (lvl < tb->max_lvl)
+        for (int e = 0; e < 7; ++e) {
+            double err2 = 0.0;
+            for (int i = 0; i < 3; ++i) {
+                double mt = 0.5 * (p[edges[e][0]][i] + p[edges[e][2]][i]);
+                double ml = p[edges[e][1]][i];
+                err2 += (mt - ml) * (mt - ml);
+            }
+            if (err2 > tb->ptol2) {
+                double cp[8][3], cu[8][3], np_[27][3], nu[27][3];
+                for (int i = 0; i < 2; ++i)
+                    for (int j = 0; j < 2; ++j)
+                        for (int k = 0; k < 2; ++k) {
+                            for (int a = 0; a < 2; ++a)
+                                for (int b = 0; b < 2; ++b)
+                                    for (int c = 0; c < 2; ++c) {
+                                        memcpy(cp[I2(a, b, c)], p[I3(a + i, b + j, c + k)], sizeof(cp[0]));
+                                        memcpy(cu[I2(a, b, c)], u[I3(a + i, b + j, c + k)], sizeof(cu[0]));
+                                    }
+                            interp_trilinear((const double(*)[3])cp, np_);
+                            interp_trilinear((const double(*)[3])cu, nu);
+                            if (refine_trilinear(tb, (const double(*)[3])np_, (const double(*)[3])nu, 0.125 * mass, lvl + 1))
+                                return -1;
+                        }
+                return 0;
+            }
+        }
+    return tetbuf_push6(tb, p, u, mass);
+}
+
+/* ---- element loop helpers (src/cpsi.c:277-373) ---- */
+
+static void aabb(const double (*p)[3], int n, double (*rb)[3])
+{
+    for (int i = 0; i < 3; ++i) {
+        rb[0][i] = 1.0e30;
+        rb[1][i] = -1.0e30;
+    }
+    for (int v = 0; v < n; ++v)
+        for (int i = 0; i < 3; ++i) {
+            if (p[v][i] < rb[0][i]) rb[0][i] = p[v][i];
+            if (p[v][i] > rb[1][i]) rb[1][i] = p[v][i];
+        }
+}
+
+static int aabb_periodic(double (*p)[3], int n, double (*rb)[3], const og_grid *g, const og_mesh *m)
+{
+    aabb((const double(*)[3])p, n, rb);
+    if (m->periodic) {
+        for (int i = 0; i < 3; ++i) {
+            double span = m->box[1][i] - m->box[0][i];
+            if (rb[1][i] - rb[0][i] > 0.5 * span) {
+                rb[0][i] = 1.0e30;
+                rb[1][i] = -1.0e30;
+                for (int v = 0; v < n; ++v) {
+                    if (p[v][i] > m->box[0][i] + 0.5 * span) p[v][i] -= span;
+                    if (p[v][i] < rb[0][i]) rb[0][i] = p[v][i];
+                    if (p[v][i] > rb[1][i]) rb[1][i] = p[v][i];
+                }
+            }
+            if (rb[0][i] > g->win[1][i]) return 0;
+            if (rb[1][i] < g->win[0][i] && rb[0][i] + span > g->win[1][i]) return 0;
+        }
+    } else {
+        for (int i = 0; i < 3; ++i) {
+            if (rb[0][i] > g->win[1][i]) return 0;
+            if (rb[1][i] < g->win[0][i]) return 0;
+        }
+    }
+    return 1;
+}
+
+/* Up to 8 periodic images of a tet (src/cpsi.c:343-373). */
+static int make_images(double (*p)[3], double (*rb)[3], const og_grid *g, const og_mesh *m)
+{
+    int num = 1, flags = 0;
+    double span[3];
+    if (!m->periodic) return 1;
+    for (int i = 0; i < 3; ++i) {
+        span[i] = m->box[1][i] - m->box[0][i];
+        if (rb[0][i] < m->box[0][i]) flags |= 1 << i;
+    }
+    for (int s = 1; s < 8; ++s) {
+        if ((flags & s) != s) continue;
+        int ok = 1;
+        for (int i = 0; i < 3 && ok; ++i) {
+            double sh = span[i] * (1 & (s >> i));
+            rb[2 * num + 0][i] = rb[0][i] + sh;
+            rb[2 * num + 1][i] = rb[1][i] + sh;
+            if (rb[2 * num + 0][i] > g->win[1][i] || rb[2 * num + 1][i] < g->win[0][i]) {
+                ok = 0;
+                break;
+            }
+            for (int v = 0; v < 4; ++v) p[4 * num + v][i] = p[v][i] + sh;
+        }
+        if (ok) num++;
+    }
+    return num;
+}
+
+/* The density branch of psi_voxels (src/cpsi.c:41-112).  Returns 0, or -1 on
+ * an unsupported element type / allocation failure. */
+int oracle_voxels(og_grid *g, const og_mesh *m, double reftol, int max_lvl, og_counters *cnt)
+{
+    og_counters dummy;
+    memset(&dummy, 0, sizeof(dummy));
+    g_cnt = cnt ? cnt : &dummy;
+    if (m->elemtype != 4 && m->elemtype != 8) return -1;
+    double dxmin = 1.0e30;
+    for (int i = 0; i < 3; ++i)
+        if (g->d[i] < dxmin) dxmin = g->d[i];
+    ov_tetbuf tb;
+    memset(&tb, 0, sizeof(tb));
+    if (max_lvl > 6) max_lvl = 6; /* src/refine.c:89-92 */
+    tb.max_lvl = max_lvl;
+    tb.ptol2 = (reftol * dxmin) * (reftol * dxmin);
+    ov_poly *stack = malloc(OV_STACK * sizeof(ov_poly));
+    if (!stack) return -1;
+    int vpe = m->elemtype;
+    int rc = 0;
+    for (int e = 0; e < m->nelem; ++e) {
+        double tp[8][3], tu[8][3], rb[2][3];
+        for (int v = 0; v < vpe; ++v) {
+            int id = m->conn[e * vpe + v];
+            memcpy(tp[v], &m->pos[3 * (size_t)id], sizeof(tp[v]));
+            memcpy(tu[v], &m->vel[3 * (size_t)id], sizeof(tu[v]));
+        }
+        if (!aabb_periodic(tp, vpe, rb, g, m)) continue;
+        g_cnt->elements_kept++;
+        tb.num = 0;
+        if (vpe == 4) {
+            if (tetbuf_reserve(&tb, 1)) { rc = -1; break; }
+            /* a simplex element is one tet of the element's own mass (src/refine.c:60-66) */
+            memcpy(tb.pos[0], tp, sizeof(double) * 12);
+            memcpy(tb.vel[0], tu, sizeof(double) * 12);
+            tb.mass[0] = m->mass[e];
+            tb.num = 1;
+        } else {
+            double np_[27][3], nu[27][3];
+            interp_trilinear((const double(*)[3])tp, np_);
+            interp_trilinear((const double(*)[3])tu, nu);
+            if (refine_trilinear(&tb, (const double(*)[3])np_, (const double(*)[3])nu, m->mass[e], 0)) { rc = -1; break; }
+        }
+        for (int t = 0; t < tb.num; ++t) {
+            double gp[32][3], grb[16][3];
+            memcpy(gp, tb.pos[4 * t], sizeof(double) * 12);
+            aabb((const double(*)[3])gp, 4, grb);
+            int ng = make_images(gp, grb, g, m);
+            g_cnt->tets++;
+            for (int k = 0; k < ng; ++k) {
+                g_cnt->tet_images++;
+                ov_voxelize_tet((const double(*)[3])&gp[4 * k], (const double(*)[3])tb.vel[4 * t], tb.mass[t],
+                                (const double(*)[3])&grb[2 * k], g, stack);
+            }
+        }
+    }
+    free(stack);
+    free(tb.pos);
+    free(tb.vel);
+    free(tb.mass);
+    return rc;
+}

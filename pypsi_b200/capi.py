@@ -1,0 +1,125 @@
+"""ctypes binding of include/psi_b200.h for callers that hold device memory.
+
+``voxels_device`` runs psib_voxels in PSIB_DEVICE mode on buffers that already
+live on the GPU (torch CUDA tensors here, raw device pointers in general) and on
+the caller's CUDA stream.  It is also the template of the binding a maintainer
+of the reference would add to call the library from Python without the PSI
+extension.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+from . import lib
+
+PSIB_FP64, PSIB_MIXED = 0, 1
+PSIB_HOST, PSIB_DEVICE = 0, 1
+FIELDS = ("m", "x", "v", "xx", "xv", "vv")
+COMPONENTS = {"m": 1, "x": 3, "v": 3, "xx": 9, "xv": 9, "vv": 9}
+
+
+class Grid(C.Structure):
+    _fields_ = [("n", C.c_int * 3), ("window", (C.c_double * 3) * 2), ("d", C.c_double * 3),
+                ("fields", C.c_void_p * 6)]
+
+
+class Mesh(C.Structure):
+    _fields_ = [("elemtype", C.c_int), ("npart", C.c_longlong), ("nelem", C.c_longlong), ("pos", C.c_void_p),
+                ("vel", C.c_void_p), ("mass", C.c_void_p), ("connectivity", C.c_void_p),
+                ("block_dims", C.c_int * 3), ("periodic", C.c_int), ("box", (C.c_double * 3) * 2)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("elements_kept", C.c_longlong), ("tets", C.c_longlong), ("tet_images", C.c_longlong),
+                ("fragments", C.c_longlong), ("frag_verts", C.c_longlong), ("splits", C.c_longlong),
+                ("passes", C.c_int), ("chunks", C.c_int), ("ms_total", C.c_float), ("ms_clip", C.c_float),
+                ("ms_tess", C.c_float), ("ms_final", C.c_float), ("clip_launches", C.c_longlong),
+                ("kernel_launches", C.c_longlong)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Options(C.Structure):
+    _fields_ = [("precision", C.c_int), ("deterministic", C.c_int), ("memory", C.c_int), ("device", C.c_int),
+                ("stream", C.c_void_p), ("stats", C.POINTER(Stats))]
+
+
+lib.psib_voxels.argtypes = [C.POINTER(Grid), C.POINTER(Mesh), C.c_int, C.c_double, C.c_int, C.POINTER(Options)]
+lib.psib_voxels.restype = C.c_int
+lib.psib_last_error.restype = C.c_char_p
+lib.psib_release_device_memory.restype = C.c_int
+
+
+class PsibError(RuntimeError):
+    def __init__(self, code: int):
+        self.code = code
+        super().__init__(f"psib_voxels failed (code {code}): {lib.psib_last_error().decode()}")
+
+
+def make_grid(n, bounds, field_ptrs: dict) -> Grid:
+    g = Grid()
+    g.n[:] = [int(v) for v in n]
+    for i in range(3):
+        g.window[0][i] = float(bounds[0][i])
+        g.window[1][i] = float(bounds[1][i])
+        g.d[i] = (g.window[1][i] - g.window[0][i]) / g.n[i]  # as src/PSI.c:111-113
+    for i, f in enumerate(FIELDS):
+        g.fields[i] = field_ptrs.get(f)
+    return g
+
+
+def make_mesh(npart, nelem, pos_ptr, vel_ptr=None, mass_ptr=None, conn_ptr=None, elemtype=8, block_dims=None,
+              periodic_box=None) -> Mesh:
+    m = Mesh(elemtype=elemtype, npart=int(npart), nelem=int(nelem), pos=pos_ptr, vel=vel_ptr, mass=mass_ptr,
+             connectivity=conn_ptr)
+    if block_dims is not None:
+        m.block_dims[:] = [int(v) for v in block_dims]
+    if periodic_box is not None:
+        m.periodic = 1
+        for i in range(3):
+            m.box[0][i] = float(periodic_box[0][i])
+            m.box[1][i] = float(periodic_box[1][i])
+    return m
+
+
+def voxels(grid: Grid, mesh: Mesh, precision=PSIB_FP64, deterministic=False, memory=PSIB_DEVICE, stream=None,
+           refine_tolerance=1.0, refine_max_lvl=0) -> dict:
+    st = Stats()
+    o = Options(precision=precision, deterministic=int(bool(deterministic)), memory=memory, device=-1,
+                stream=stream, stats=C.pointer(st))
+    rc = lib.psib_voxels(C.byref(grid), C.byref(mesh), 0, float(refine_tolerance), int(refine_max_lvl), C.byref(o))
+    if rc != 0:
+        raise PsibError(rc)
+    return st.as_dict()
+
+
+def voxels_device(fields: dict, n, bounds, pos, vel=None, mass=None, connectivity=None, block_dims=None,
+                  periodic_box=None, precision="fp64", deterministic=False, refine_tolerance=1.0, refine_max_lvl=0,
+                  stream=None) -> dict:
+    """Deposit on device-resident torch tensors.
+
+    fields: {"m": (nx,ny,nz) float64 CUDA tensor, "x": (...,3), ...}; pos/vel:
+    (npart,3) float64; mass: (nelem,) float64; connectivity: (nelem, 4|8) int32
+    or None with block_dims for a block lattice.  Runs on `stream` (a
+    torch.cuda.Stream; default: the current stream)."""
+    import torch
+
+    for f, t in fields.items():
+        assert t.is_cuda and t.dtype == torch.float64 and t.is_contiguous(), f
+    ptr = {f: t.data_ptr() for f, t in fields.items()}
+    g = make_grid(n, bounds, ptr)
+    npart = pos.numel() // 3
+    if connectivity is not None:
+        elemtype, nelem = connectivity.shape[-1], connectivity.numel() // connectivity.shape[-1]
+    else:
+        elemtype = 8
+        nelem = 1
+        for b in block_dims:
+            nelem *= b if periodic_box is not None else b - 1
+    m = make_mesh(npart, nelem, pos.data_ptr(), vel.data_ptr() if vel is not None else None,
+                  mass.data_ptr() if mass is not None else None,
+                  connectivity.data_ptr() if connectivity is not None else None, elemtype, block_dims, periodic_box)
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return voxels(g, m, PSIB_MIXED if precision == "mixed" else PSIB_FP64, deterministic, PSIB_DEVICE,
+                  C.c_void_p(s.cuda_stream), refine_tolerance, refine_max_lvl)

@@ -1,0 +1,729 @@
+// pipeline.cu -- the C ABI (include/psi_b200.h) and the host orchestration of
+// one PSI.voxels call on the GPU:
+//
+//   count   elements -> tet images per element          (tess.cu)
+//   scan    per-element offsets (CUB)
+//   emit    tet images in the reference's visiting order (tess.cu)
+//   order   images sorted by footprint key (CUB radix sort)
+//   clip    persistent clip-and-deposit kernels          (clip_fp64.cu / clip_mixed.cu)
+//   final   voxel means / covariances merged into the fields (tess.cu)
+//
+// Second-order fields take two clip passes (means first, then centred second
+// moments).  Meshes whose tet images exceed the item budget are streamed in
+// element chunks.  Deterministic mode records fragments, sorts them by
+// (voxel, item) and applies the reference's online update per voxel.
+#include <cub/cub.cuh>
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "psi_b200.h"
+#include "psib_device.cuh"
+#include "psib_kernels.h"
+
+using namespace psib;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CK(x)                                                                                  \
+    do {                                                                                       \
+        cudaError_t _e = (x);                                                                  \
+        if (_e != cudaSuccess)                                                                 \
+            return fail(_e == cudaErrorMemoryAllocation ? PSIB_ERR_NOMEM : PSIB_ERR_CUDA,      \
+                        "%s failed: %s (%s:%d)", #x, cudaGetErrorString(_e), __FILE__, __LINE__); \
+    } while (0)
+
+#define RET(x)                         \
+    do {                               \
+        int _r = (x);                  \
+        if (_r != PSIB_OK) return _r;  \
+    } while (0)
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t n = 0;
+    template <class T> T* as() const { return (T*)p; }
+};
+
+int ensure(DevBuf& b, size_t bytes)
+{
+    if (bytes == 0) bytes = 16;
+    if (b.n >= bytes) return PSIB_OK;
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.n = 0;
+    cudaError_t e = cudaMalloc(&b.p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        b.p = nullptr;
+        return fail(PSIB_ERR_NOMEM, "cudaMalloc of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+    }
+    b.n = bytes;
+    return PSIB_OK;
+}
+
+struct Ctx {
+    int device = -1;
+    int num_sms = 0;
+    cudaStream_t own = nullptr; // stream of host-memory calls
+    cudaEvent_t ev[8] = {};
+    // host-mode copies
+    DevBuf hpos, hvel, hmass, hconn, hfield[6];
+    // accumulators
+    DevBuf W, SX, SV, XX, XV, VV, MX, MV;
+    // items
+    DevBuf ip, iu, imass, ielem, ipid, ikey;
+    DevBuf key_sorted, order_in, order;
+    DevBuf counts, offsets;
+    DevBuf cub_tmp, scratch;
+    DevBuf small; // status, counters, heads
+    // records
+    DevBuf rkey, rmom, rkey_sorted, rperm_in, rperm;
+    std::vector<DevBuf*> all()
+    {
+        return {&hpos, &hpos, &hvel, &hmass, &hconn, &hfield[0], &hfield[1], &hfield[2], &hfield[3], &hfield[4],
+                &hfield[5], &W, &SX, &SV, &XX, &XV, &VV, &MX, &MV, &ip, &iu, &imass, &ielem, &ipid, &ikey,
+                &key_sorted, &order_in, &order, &counts, &offsets, &cub_tmp, &scratch, &small, &rkey, &rmom,
+                &rkey_sorted, &rperm_in, &rperm};
+    }
+};
+
+std::mutex g_mu;
+Ctx* g_ctx[64];
+
+int get_ctx(int dev, Ctx** out)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (dev < 0 || dev >= 64) return fail(PSIB_ERR_ARG, "device ordinal %d out of range", dev);
+    if (!g_ctx[dev]) {
+        Ctx* c = new Ctx();
+        c->device = dev;
+        CK(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, dev));
+        CK(cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking));
+        for (auto& e : c->ev) CK(cudaEventCreate(&e));
+        g_ctx[dev] = c;
+    }
+    *out = g_ctx[dev];
+    return PSIB_OK;
+}
+
+// small device block layout (unsigned long long words)
+enum { S_STATUS = 0, S_CNT = 1 /* 3 words */, S_TESS = 4 /* 2 */, S_HEAD = 8 /* 4 */, S_RECN = 12, S_NDEEP = 13,
+       S_ANY = 14, S_WORDS = 16 };
+
+__global__ void k_count_deep(const uint16_t* key, long long n, unsigned long long* out)
+{
+    unsigned long long c = 0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        c += (key[i] == 0xFFFF);
+    c = __reduce_add_sync(0xFFFFFFFFu, (unsigned)c);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, c);
+}
+
+__global__ void k_iota(int* o, long long n)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        o[i] = (int)i;
+}
+
+__global__ void k_iota_u(unsigned* o, long long n)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        o[i] = (unsigned)i;
+}
+
+long long env_ll(const char* name, long long dflt)
+{
+    const char* s = getenv(name);
+    if (!s || !*s) return dflt;
+    return atoll(s);
+}
+
+struct Call {
+    const psib_grid* grid;
+    const psib_mesh* mesh;
+    double reftol;
+    int maxlvl;
+    int precision;
+    int deterministic;
+    cudaStream_t st;
+    Ctx* C;
+    psib_stats* stats;
+    // device views
+    double* F[6];
+    const double *pos, *vel, *mass;
+    const int* conn;
+};
+
+int check_status(Call& c, unsigned long long* small_host)
+{
+    unsigned st = (unsigned)small_host[S_STATUS];
+    if (!st) return PSIB_OK;
+    if (st & ST_INDEX) return fail(PSIB_ERR_INDEX, "connectivity or voxel index out of range (status 0x%x)", st);
+    if (st & (ST_OVERFLOW | ST_DEPTH))
+        return fail(PSIB_ERR_OVERFLOW, "a polyhedron outgrew the vertex buffer or slot pool (status 0x%x)", st);
+    if (st & ST_GRAPH) return fail(PSIB_ERR_OVERFLOW, "a polyhedron graph walk did not close (status 0x%x)", st);
+    return fail(PSIB_ERR_CUDA, "kernel status 0x%x", st);
+}
+
+int run_device(Call& c)
+{
+    Ctx& C = *c.C;
+    const psib_grid& g = *c.grid;
+    const psib_mesh& m = *c.mesh;
+    cudaStream_t st = c.st;
+    const long long nvox = (long long)g.n[0] * g.n[1] * g.n[2];
+
+    unsigned flags = 0;
+    if (c.F[1]) flags |= F_X;
+    if (c.F[2]) flags |= F_V;
+    if (c.F[3]) flags |= F_XX;
+    if (c.F[4]) flags |= F_XV;
+    if (c.F[5]) flags |= F_VV;
+    const int order = (flags & (F_XX | F_XV | F_VV)) ? 2 : (flags & (F_X | F_V)) ? 1 : 0;
+    const bool det = c.deterministic != 0;
+    const int passes = (!det && order == 2) ? 2 : 1;
+
+    GridDev gd;
+    for (int i = 0; i < 3; ++i) {
+        gd.n[i] = g.n[i];
+        gd.w0[i] = g.window[0][i];
+        gd.w1[i] = g.window[1][i];
+        gd.d[i] = g.d[i];
+    }
+
+    MeshDev md;
+    md.elemtype = m.elemtype;
+    md.npart = m.npart;
+    md.nelem = m.nelem;
+    md.pos = c.pos;
+    md.vel = c.vel;
+    md.mass = c.mass;
+    md.conn = c.conn;
+    md.periodic = m.periodic ? 1 : 0;
+    for (int i = 0; i < 3; ++i) {
+        md.bdim[i] = m.block_dims[i];
+        md.edim[i] = m.periodic ? m.block_dims[i] : m.block_dims[i] - 1;
+        md.box0[i] = m.box[0][i];
+        md.box1[i] = m.box[1][i];
+    }
+    double dxmin = 1.0e30;
+    for (int i = 0; i < 3; ++i)
+        if (g.d[i] < dxmin) dxmin = g.d[i];
+    const double tol = c.reftol * dxmin;
+
+    // accumulators
+    const size_t v8 = (size_t)nvox * sizeof(double);
+    AccDev acc = {};
+    acc.flags = flags;
+    if (!det) {
+        RET(ensure(C.W, v8));
+        acc.W = C.W.as<double>();
+        CK(cudaMemsetAsync(acc.W, 0, v8, st));
+        if (flags & F_X) { RET(ensure(C.SX, 3 * v8)); acc.SX = C.SX.as<double>(); CK(cudaMemsetAsync(acc.SX, 0, 3 * v8, st)); }
+        if (flags & F_V) { RET(ensure(C.SV, 3 * v8)); acc.SV = C.SV.as<double>(); CK(cudaMemsetAsync(acc.SV, 0, 3 * v8, st)); }
+        if (flags & F_XX) { RET(ensure(C.XX, 9 * v8)); acc.XX = C.XX.as<double>(); CK(cudaMemsetAsync(acc.XX, 0, 9 * v8, st)); }
+        if (flags & F_XV) { RET(ensure(C.XV, 9 * v8)); acc.XV = C.XV.as<double>(); CK(cudaMemsetAsync(acc.XV, 0, 9 * v8, st)); }
+        if (flags & F_VV) { RET(ensure(C.VV, 9 * v8)); acc.VV = C.VV.as<double>(); CK(cudaMemsetAsync(acc.VV, 0, 9 * v8, st)); }
+        if (passes == 2) {
+            if (flags & (F_XX | F_XV)) { RET(ensure(C.MX, 3 * v8)); acc.MX = C.MX.as<double>(); }
+            if (flags & (F_XV | F_VV)) { RET(ensure(C.MV, 3 * v8)); acc.MV = C.MV.as<double>(); }
+        }
+    }
+
+    RET(ensure(C.small, S_WORDS * 8));
+    unsigned long long* sm = C.small.as<unsigned long long>();
+    CK(cudaMemsetAsync(sm, 0, S_WORDS * 8, st));
+
+    CK(cudaEventRecord(C.ev[1], st));
+    // ---- count tet images per element ----
+    const long long ne = m.nelem;
+    RET(ensure(C.counts, (size_t)(ne + 1) * sizeof(long long)));
+    RET(ensure(C.offsets, (size_t)(ne + 1) * sizeof(long long)));
+    TessArgs ta = {};
+    ta.m = md;
+    ta.g = gd;
+    ta.max_lvl = c.maxlvl;
+    ta.ptol2 = tol * tol;
+    ta.status = (unsigned*)&sm[S_STATUS];
+    ta.counters = &sm[S_TESS];
+    std::vector<long long> offs_host;
+    long long total = 0;
+    {
+        // counts are written as int into the long long buffer's first half; widen via scan input
+        ta.e0 = 0;
+        ta.e1 = ne;
+        ta.count = (int*)C.counts.p;
+        CK(launch_tess_count(ta, st));
+        size_t tb = 0;
+        const int* cin = (const int*)C.counts.p;
+        long long* cout = C.offsets.as<long long>();
+        CK(cub::DeviceScan::ExclusiveScan(nullptr, tb, cin, cout, cub::Sum(), (long long)0, (int)(ne + 1), st));
+        RET(ensure(C.cub_tmp, tb));
+        // the (ne+1)-th count must be zero for the total to land in offsets[ne]
+        CK(cudaMemsetAsync((int*)C.counts.p + ne, 0, sizeof(int), st));
+        CK(cub::DeviceScan::ExclusiveScan(C.cub_tmp.p, tb, cin, cout, cub::Sum(), (long long)0, (int)(ne + 1), st));
+        CK(cudaMemcpyAsync(&total, cout + ne, sizeof(long long), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+    }
+    {
+        unsigned long long h[S_WORDS];
+        CK(cudaMemcpy(h, sm, sizeof(h), cudaMemcpyDeviceToHost));
+        RET(check_status(c, h));
+    }
+
+    // ---- chunking ----
+    const long long budget = env_ll("PSIB_ITEM_BUDGET", 24ll << 20);
+    std::vector<long long> cb; // element boundaries
+    cb.push_back(0);
+    if (total > budget) {
+        offs_host.resize(ne + 1);
+        CK(cudaMemcpy(offs_host.data(), C.offsets.p, (ne + 1) * sizeof(long long), cudaMemcpyDeviceToHost));
+        long long e = 0;
+        while (e < ne) {
+            long long e1 = e;
+            while (e1 < ne && offs_host[e1 + 1] - offs_host[e] <= budget) ++e1;
+            if (e1 == e) e1 = e + 1; // one element larger than the budget
+            cb.push_back(e1);
+            e = e1;
+        }
+    } else {
+        cb.push_back(ne);
+    }
+    const int nchunks = (int)cb.size() - 1;
+    long long cap = 0;
+    if (nchunks == 1) cap = total;
+    else
+        for (int k = 0; k < nchunks; ++k) cap = std::max(cap, offs_host[cb[k + 1]] - offs_host[cb[k]]);
+    if (cap < 1) cap = 1;
+
+    RET(ensure(C.ip, (size_t)cap * 12 * sizeof(double)));
+    RET(ensure(C.iu, (size_t)cap * 12 * sizeof(double)));
+    RET(ensure(C.imass, (size_t)cap * sizeof(double)));
+    RET(ensure(C.ielem, (size_t)cap * sizeof(int)));
+    RET(ensure(C.ipid, (size_t)cap * 4 * sizeof(int)));
+    RET(ensure(C.ikey, (size_t)cap * sizeof(uint16_t)));
+    RET(ensure(C.key_sorted, (size_t)cap * sizeof(uint16_t)));
+    RET(ensure(C.order_in, (size_t)cap * sizeof(int)));
+    RET(ensure(C.order, (size_t)cap * sizeof(int)));
+    ItemArrays it;
+    it.p = C.ip.as<double>();
+    it.u = C.iu.as<double>();
+    it.mass = C.imass.as<double>();
+    it.elem = C.ielem.as<int>();
+    it.pid = C.ipid.as<int>();
+    it.key = C.ikey.as<uint16_t>();
+    it.cap = cap;
+    ta.it = it;
+    ta.offset = C.offsets.as<long long>();
+
+    // occupancy of the persistent clip kernels
+    int clip_block = 128;
+    int clip_grid = C.num_sms * 4;
+    const int big_block = 64;
+    const size_t big_bytes = (c.precision == PSIB_MIXED && !det) ? scratch_bytes_mixed_big() : scratch_bytes_fp64_big();
+
+    ClipArgs ca = {};
+    ca.it = it;
+    ca.order = C.order.as<int>();
+    ca.g = gd;
+    ca.acc = acc;
+    ca.mom_order = order;
+    ca.status = (unsigned*)&sm[S_STATUS];
+    ca.counters = &sm[S_CNT];
+
+    float ms_clip = 0.f, ms_tess = 0.f;
+    long long launches = 0, klaunch = 1; // the count kernel
+    double* MXw = acc.MX ? (double*)acc.MX : nullptr;
+    double* MVw = acc.MV ? (double*)acc.MV : nullptr;
+
+    for (int pass = 1; pass <= passes; ++pass) {
+        for (int k = 0; k < nchunks; ++k) {
+            const long long e0 = cb[k], e1 = cb[k + 1];
+            long long obase = 0, nitems = 0;
+            if (nchunks == 1) {
+                obase = 0;
+                nitems = total;
+            } else {
+                obase = offs_host[e0];
+                nitems = offs_host[e1] - obase;
+            }
+            if (nitems == 0) continue;
+            const bool reuse = (nchunks == 1 && pass > 1);
+            long long nmain = nitems, ndeep = 0;
+            CK(cudaEventRecord(C.ev[2], st));
+            if (!reuse) {
+                ta.e0 = e0;
+                ta.e1 = e1;
+                ta.offset = C.offsets.as<long long>() + e0;
+                ta.offset_base = obase;
+                ta.counters = (pass == 1) ? &sm[S_TESS] : nullptr;
+                CK(launch_tess_emit(ta, st));
+                klaunch += 3; // emit, iota, count_deep
+                // order by footprint key
+                CK(cudaMemsetAsync(&sm[S_NDEEP], 0, 8, st));
+                k_iota<<<C.num_sms * 8, 256, 0, st>>>(C.order_in.as<int>(), nitems);
+                CK(cudaGetLastError());
+                k_count_deep<<<C.num_sms * 8, 256, 0, st>>>(it.key, nitems, &sm[S_NDEEP]);
+                CK(cudaGetLastError());
+                size_t tb = 0;
+                CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, it.key, C.key_sorted.as<uint16_t>(),
+                                                   C.order_in.as<int>(), C.order.as<int>(), (int)nitems, 0, 16, st));
+                RET(ensure(C.cub_tmp, tb));
+                CK(cub::DeviceRadixSort::SortPairs(C.cub_tmp.p, tb, it.key, C.key_sorted.as<uint16_t>(),
+                                                   C.order_in.as<int>(), C.order.as<int>(), (int)nitems, 0, 16, st));
+            }
+            unsigned long long hd = 0;
+            CK(cudaMemcpyAsync(&hd, &sm[S_NDEEP], 8, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            ndeep = (long long)hd;
+            nmain = nitems - ndeep;
+            CK(cudaEventRecord(C.ev[3], st));
+            {
+                float t = 0.f;
+                CK(cudaEventElapsedTime(&t, C.ev[2], C.ev[3]));
+                ms_tess += t;
+            }
+
+            ca.pass = pass;
+            ca.acc = acc;
+            if (pass == 2) {
+                ca.acc.MX = MXw;
+                ca.acc.MV = MVw;
+            }
+            bool redo = true;
+            while (redo) {
+                redo = false;
+                if (det) {
+                    const unsigned long long want = (unsigned long long)std::max<long long>(nitems * 40, 1 << 16);
+                    const int nm = order == 2 ? 10 : order == 1 ? 4 : 1;
+                    const unsigned long long have = std::max<unsigned long long>(C.rkey.n / 8, want);
+                    RET(ensure(C.rkey, have * 8));
+                    RET(ensure(C.rmom, have * 8 * nm));
+                    ca.rec_key = C.rkey.as<unsigned long long>();
+                    ca.rec_mom = C.rmom.as<double>();
+                    ca.rec_cap = std::min<unsigned long long>(C.rkey.n / 8, C.rmom.n / (8 * nm));
+                    ca.rec_nmom = order == 2 ? 10 : order == 1 ? 4 : 1;
+                    ca.rec_n = &sm[S_RECN];
+                    ca.rec_item_base = 0;
+                    CK(cudaMemsetAsync(&sm[S_RECN], 0, 8, st));
+                }
+                CK(cudaEventRecord(C.ev[4], st));
+                CK(cudaMemsetAsync(&sm[S_HEAD], 0, 16, st));
+                if (nmain > 0) {
+                    ca.order_base = 0;
+                    ca.n = nmain;
+                    ca.head = &sm[S_HEAD];
+                    if (c.precision == PSIB_MIXED && !det) CK(launch_clip_mixed(ca, false, clip_grid, clip_block, st));
+                    else CK(launch_clip_fp64(ca, false, det, clip_grid, clip_block, st));
+                    launches++;
+                }
+                if (ndeep > 0) {
+                    const int big_grid = (int)std::min<long long>(C.num_sms * 2, (ndeep + big_block - 1) / big_block);
+                    RET(ensure(C.scratch, big_bytes * (size_t)big_grid * big_block));
+                    ca.scratch = C.scratch.p;
+                    ca.order_base = nmain;
+                    ca.n = ndeep;
+                    ca.head = &sm[S_HEAD + 1];
+                    if (c.precision == PSIB_MIXED && !det) CK(launch_clip_mixed(ca, true, big_grid, big_block, st));
+                    else CK(launch_clip_fp64(ca, true, det, big_grid, big_block, st));
+                    launches++;
+                }
+                CK(cudaEventRecord(C.ev[5], st));
+                {
+                    CK(cudaEventSynchronize(C.ev[5]));
+                    float t = 0.f;
+                    CK(cudaEventElapsedTime(&t, C.ev[4], C.ev[5]));
+                    ms_clip += t;
+                }
+                if (det) {
+                    unsigned long long h[S_WORDS];
+                    CK(cudaMemcpy(h, sm, sizeof(h), cudaMemcpyDeviceToHost));
+                    const unsigned long long nrec = h[S_RECN];
+                    if (nrec > ca.rec_cap) {
+                        // the buffer was too small: grow to the exact need and redo the chunk
+                        RET(ensure(C.rkey, nrec * 8));
+                        RET(ensure(C.rmom, nrec * 8 * ca.rec_nmom));
+                        unsigned clr = 0;
+                        CK(cudaMemcpy(&sm[S_STATUS], &clr, sizeof(clr), cudaMemcpyHostToDevice));
+                        redo = true;
+                        continue;
+                    }
+                    RET(check_status(c, h));
+                    if (nrec > 0xFFFFFFFFull) return fail(PSIB_ERR_OVERFLOW, "too many fragments in one chunk");
+                    RET(ensure(C.rkey_sorted, nrec * 8));
+                    RET(ensure(C.rperm_in, nrec * 4));
+                    RET(ensure(C.rperm, nrec * 4));
+                    k_iota_u<<<C.num_sms * 8, 256, 0, st>>>(C.rperm_in.as<unsigned>(), (long long)nrec);
+                    CK(cudaGetLastError());
+                    int vbits = 1;
+                    while ((1ll << vbits) < nvox) ++vbits;
+                    size_t tb = 0;
+                    CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, C.rkey.as<unsigned long long>(),
+                                                       C.rkey_sorted.as<unsigned long long>(), C.rperm_in.as<unsigned>(),
+                                                       C.rperm.as<unsigned>(), (int)nrec, 0, 32 + vbits, st));
+                    RET(ensure(C.cub_tmp, tb));
+                    CK(cub::DeviceRadixSort::SortPairs(C.cub_tmp.p, tb, C.rkey.as<unsigned long long>(),
+                                                       C.rkey_sorted.as<unsigned long long>(), C.rperm_in.as<unsigned>(),
+                                                       C.rperm.as<unsigned>(), (int)nrec, 0, 32 + vbits, st));
+                    ApplyArgs aa = {};
+                    aa.key = C.rkey_sorted.as<unsigned long long>();
+                    aa.mom = C.rmom.as<double>();
+                    aa.perm = C.rperm.as<unsigned>();
+                    aa.nrec = (long long)nrec;
+                    aa.nmom = ca.rec_nmom;
+                    aa.it = it;
+                    aa.item_base = 0;
+                    aa.M = c.F[0]; aa.X = c.F[1]; aa.V = c.F[2]; aa.XX = c.F[3]; aa.XV = c.F[4]; aa.VV = c.F[5];
+                    CK(launch_apply_records(aa, st));
+                    klaunch += 2; // iota, apply
+                }
+            }
+        }
+        if (pass == 1 && passes == 2) {
+            FinalArgs f = {};
+            f.g = gd;
+            f.acc = acc;
+            f.MX = MXw;
+            f.MV = MVw;
+            f.nvox = nvox;
+            CK(launch_finalize_means(f, st));
+            klaunch++;
+        }
+    }
+    CK(cudaEventRecord(C.ev[6], st));
+    if (!det) {
+        FinalArgs f = {};
+        f.g = gd;
+        f.acc = acc;
+        f.M = c.F[0]; f.X = c.F[1]; f.V = c.F[2]; f.XX = c.F[3]; f.XV = c.F[4]; f.VV = c.F[5];
+        f.nvox = nvox;
+        CK(launch_finalize_merge(f, st));
+        klaunch++;
+    }
+    CK(cudaEventRecord(C.ev[7], st));
+    unsigned long long h[S_WORDS];
+    CK(cudaMemcpyAsync(h, sm, sizeof(h), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    RET(check_status(c, h));
+    if (c.stats) {
+        psib_stats& s = *c.stats;
+        s.elements_kept = (long long)h[S_TESS];
+        s.tets = (long long)h[S_TESS + 1];
+        s.tet_images = total;
+        s.fragments = (long long)h[S_CNT];
+        s.frag_verts = (long long)h[S_CNT + 1];
+        s.splits = (long long)h[S_CNT + 2];
+        s.passes = passes;
+        s.chunks = nchunks;
+        s.ms_clip = ms_clip;
+        s.ms_tess = ms_tess;
+        float t = 0.f;
+        CK(cudaEventElapsedTime(&t, C.ev[6], C.ev[7]));
+        s.ms_final = t;
+        s.clip_launches = launches;
+        s.kernel_launches = klaunch + launches;
+    }
+    return PSIB_OK;
+}
+
+int validate(const psib_grid* g, const psib_mesh* m, int mode, const psib_options* o)
+{
+    if (!g || !m) return fail(PSIB_ERR_ARG, "grid and mesh are required");
+    if (mode == PSIB_MODE_ANNIHILATION)
+        return fail(PSIB_ERR_UNSUPPORTED, "annihilation mode is not implemented by this library");
+    if (mode != PSIB_MODE_DENSITY) return fail(PSIB_ERR_ARG, "invalid mode %d", mode);
+    for (int i = 0; i < 3; ++i) {
+        if (g->n[i] <= 0) return fail(PSIB_ERR_ARG, "grid n must be positive");
+        if (!(g->d[i] > 0.0)) return fail(PSIB_ERR_ARG, "grid cell size d must be positive");
+    }
+    if ((long long)g->n[0] * g->n[1] * g->n[2] >= (1ll << 32))
+        return fail(PSIB_ERR_ARG, "grids of 2^32 voxels or more are not supported");
+    if (!g->fields[PSIB_M]) return fail(PSIB_ERR_ARG, "field m is required");
+    if (g->fields[PSIB_XX] && !g->fields[PSIB_X]) return fail(PSIB_ERR_ARG, "field 'xx' requires field 'x'");
+    if (g->fields[PSIB_XV] && !(g->fields[PSIB_X] && g->fields[PSIB_V]))
+        return fail(PSIB_ERR_ARG, "field 'xv' requires fields 'x' and 'v'");
+    if (g->fields[PSIB_VV] && !g->fields[PSIB_V]) return fail(PSIB_ERR_ARG, "field 'vv' requires field 'v'");
+    if (m->elemtype == 27) return fail(PSIB_ERR_UNSUPPORTED, "triquadratic elements are not implemented");
+    if (m->elemtype != 4 && m->elemtype != 8) return fail(PSIB_ERR_ARG, "elemtype must be 4 or 8");
+    if (m->nelem < 0 || m->npart < 0) return fail(PSIB_ERR_ARG, "negative mesh size");
+    if (m->nelem >= (1ll << 31) || m->npart >= (1ll << 31))
+        return fail(PSIB_ERR_ARG, "meshes of 2^31 elements or particles are not supported");
+    if (m->nelem > 0 && !m->pos) return fail(PSIB_ERR_ARG, "pos is required");
+    if (!m->connectivity) {
+        if (m->elemtype != 8) return fail(PSIB_ERR_ARG, "implicit connectivity needs elemtype 8");
+        long long np = 1, nel = 1;
+        for (int i = 0; i < 3; ++i) {
+            if (m->block_dims[i] <= 0) return fail(PSIB_ERR_ARG, "connectivity or block_dims is required");
+            np *= m->block_dims[i];
+            nel *= m->periodic ? m->block_dims[i] : m->block_dims[i] - 1;
+        }
+        if (np != m->npart || nel != m->nelem) return fail(PSIB_ERR_ARG, "block_dims disagree with npart/nelem");
+    }
+    if (o && o->precision != PSIB_FP64 && o->precision != PSIB_MIXED)
+        return fail(PSIB_ERR_ARG, "invalid precision %d", o->precision);
+    if (o && o->deterministic && o->precision == PSIB_MIXED)
+        return fail(PSIB_ERR_ARG, "deterministic mode runs in FP64 only");
+    return PSIB_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+const char* psib_last_error(void) { return g_err.c_str(); }
+
+int psib_abi_version(void) { return PSIB_ABI_VERSION; }
+
+int psib_device_count(void)
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+void* psib_host_alloc(unsigned long long bytes)
+{
+    void* p = nullptr;
+    if (psib_device_count() <= 0) return nullptr;
+    if (cudaHostAlloc(&p, bytes ? bytes : 16, cudaHostAllocPortable) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return p;
+}
+
+void psib_host_free(void* p)
+{
+    if (p) cudaFreeHost(p);
+}
+
+int psib_release_device_memory(void)
+{
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (dev >= 0 && dev < 64 && g_ctx[dev]) {
+        CK(cudaDeviceSynchronize());
+        for (DevBuf* b : g_ctx[dev]->all()) {
+            if (b->p) cudaFree(b->p);
+            b->p = nullptr;
+            b->n = 0;
+        }
+    }
+    return PSIB_OK;
+}
+
+int psib_voxels(const psib_grid* grid, const psib_mesh* mesh, int mode, double refine_tolerance, int refine_max_lvl,
+                const psib_options* opt)
+{
+    g_err.clear();
+    psib_options o = {};
+    o.precision = PSIB_FP64;
+    o.memory = PSIB_HOST;
+    o.device = -1;
+    if (opt) o = *opt;
+    RET(validate(grid, mesh, mode, &o));
+    if (psib_device_count() <= 0) return fail(PSIB_ERR_NODEVICE, "no CUDA device is visible");
+    int dev = o.device;
+    if (o.memory == PSIB_DEVICE || dev < 0) CK(cudaGetDevice(&dev));
+    CK(cudaSetDevice(dev));
+    Ctx* C = nullptr;
+    RET(get_ctx(dev, &C));
+
+    Call c = {};
+    c.grid = grid;
+    c.mesh = mesh;
+    c.reftol = refine_tolerance;
+    c.maxlvl = refine_max_lvl > 6 ? 6 : (refine_max_lvl < 0 ? 0 : refine_max_lvl);
+    c.precision = o.precision;
+    c.deterministic = o.deterministic;
+    c.C = C;
+    c.stats = o.stats;
+    if (o.stats) *o.stats = psib_stats{};
+
+    const long long nvox = (long long)grid->n[0] * grid->n[1] * grid->n[2];
+    static const int comps[6] = {1, 3, 3, 9, 9, 9};
+    if (o.memory == PSIB_DEVICE) {
+        c.st = (cudaStream_t)o.stream;
+        for (int f = 0; f < 6; ++f) c.F[f] = grid->fields[f];
+        c.pos = mesh->pos;
+        c.vel = mesh->vel;
+        c.mass = mesh->mass;
+        c.conn = mesh->connectivity;
+        CK(cudaEventRecord(C->ev[0], c.st));
+        RET(run_device(c));
+        if (o.stats) {
+            CK(cudaEventRecord(C->ev[7], c.st));
+            CK(cudaEventSynchronize(C->ev[7]));
+            CK(cudaEventElapsedTime(&o.stats->ms_total, C->ev[0], C->ev[7]));
+        }
+        return PSIB_OK;
+    }
+    // host memory: copy in, run, copy out
+    cudaStream_t st = C->own;
+    c.st = st;
+    CK(cudaEventRecord(C->ev[0], st));
+    const size_t np3 = (size_t)mesh->npart * 3 * sizeof(double);
+    if (mesh->nelem > 0) {
+        RET(ensure(C->hpos, np3));
+        CK(cudaMemcpyAsync(C->hpos.p, mesh->pos, np3, cudaMemcpyHostToDevice, st));
+        c.pos = C->hpos.as<double>();
+        if (mesh->vel) {
+            RET(ensure(C->hvel, np3));
+            CK(cudaMemcpyAsync(C->hvel.p, mesh->vel, np3, cudaMemcpyHostToDevice, st));
+            c.vel = C->hvel.as<double>();
+        }
+        if (mesh->mass) {
+            RET(ensure(C->hmass, (size_t)mesh->nelem * sizeof(double)));
+            CK(cudaMemcpyAsync(C->hmass.p, mesh->mass, (size_t)mesh->nelem * sizeof(double), cudaMemcpyHostToDevice, st));
+            c.mass = C->hmass.as<double>();
+        }
+        if (mesh->connectivity) {
+            const size_t cb = (size_t)mesh->nelem * mesh->elemtype * sizeof(int);
+            RET(ensure(C->hconn, cb));
+            CK(cudaMemcpyAsync(C->hconn.p, mesh->connectivity, cb, cudaMemcpyHostToDevice, st));
+            c.conn = C->hconn.as<int>();
+        }
+    }
+    for (int f = 0; f < 6; ++f) {
+        if (!grid->fields[f]) continue;
+        const size_t b = (size_t)nvox * comps[f] * sizeof(double);
+        RET(ensure(C->hfield[f], b));
+        CK(cudaMemcpyAsync(C->hfield[f].p, grid->fields[f], b, cudaMemcpyHostToDevice, st));
+        c.F[f] = C->hfield[f].as<double>();
+    }
+    if (mesh->nelem > 0) RET(run_device(c));
+    for (int f = 0; f < 6; ++f) {
+        if (!grid->fields[f]) continue;
+        const size_t b = (size_t)nvox * comps[f] * sizeof(double);
+        CK(cudaMemcpyAsync(grid->fields[f], c.F[f], b, cudaMemcpyDeviceToHost, st));
+    }
+    CK(cudaEventRecord(C->ev[7], st));
+    CK(cudaEventSynchronize(C->ev[7]));
+    if (o.stats) CK(cudaEventElapsedTime(&o.stats->ms_total, C->ev[0], C->ev[7]));
+    return PSIB_OK;
+}
+
+} // extern "C"

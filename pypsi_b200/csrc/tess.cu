@@ -1,0 +1,500 @@
+// tess.cu -- elements to tet images, and the per-voxel finalisation.
+//
+// Built with --fmad=false: the element unwrap, the trilinear refinement and
+// the online field update below repeat the reference's double-precision
+// operations in the reference's order.
+#include "psib_device.cuh"
+#include "psib_kernels.h"
+
+namespace psib {
+
+// The 6-tet split of a 27-node cube, node indices 9i+3j+k (src/refine.c:39-41).
+__constant__ int c_tet_nodes[6][4] = {{2, 0, 6, 18}, {8, 2, 6, 18}, {8, 20, 2, 18},
+                                      {8, 24, 20, 18}, {8, 6, 24, 18}, {8, 26, 20, 24}};
+// The same split on the 8 corner vertices 4i+2j+k of an unrefined element.
+__constant__ int c_tet_corners[6][4] = {{1, 0, 2, 4}, {3, 1, 2, 4}, {3, 5, 1, 4},
+                                        {3, 6, 5, 4}, {3, 2, 6, 4}, {3, 7, 5, 6}};
+// Edges (end, midpoint, end) whose midpoint deviation drives refinement (src/refine.c:228-230).
+__constant__ int c_ref_edges[7][3] = {{2, 4, 6}, {2, 10, 18}, {6, 12, 18}, {8, 13, 18},
+                                      {8, 14, 20}, {8, 16, 24}, {20, 22, 24}};
+
+constexpr int MAX_REFINE = 6; // src/refine.c:89-92
+
+__device__ __forceinline__ int I2(int a, int b, int c) { return 4 * a + 2 * b + c; }
+__device__ __forceinline__ int I3(int a, int b, int c) { return 9 * a + 3 * b + c; }
+
+// 8 corners -> 27 nodes by repeated midpoints (src/refine.c:292-319).
+__device__ void interp_trilinear(const double (*in)[3], double (*out)[3])
+{
+    for (int ax = 0; ax < 3; ++ax) {
+        for (int i = 0; i < 2; ++i)
+            for (int j = 0; j < 2; ++j)
+                for (int k = 0; k < 2; ++k) out[I3(2 * i, 2 * j, 2 * k)][ax] = in[I2(i, j, k)][ax];
+        for (int j = 0; j < 3; j += 2)
+            for (int k = 0; k < 3; k += 2) out[I3(1, j, k)][ax] = 0.5 * (out[I3(0, j, k)][ax] + out[I3(2, j, k)][ax]);
+        for (int i = 0; i < 3; ++i)
+            for (int k = 0; k < 3; k += 2) out[I3(i, 1, k)][ax] = 0.5 * (out[I3(i, 0, k)][ax] + out[I3(i, 2, k)][ax]);
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) out[I3(i, j, 1)][ax] = 0.5 * (out[I3(i, j, 0)][ax] + out[I3(i, j, 2)][ax]);
+    }
+}
+
+// Gather an element's vertices; false if an id is out of range.
+__device__ bool gather(const MeshDev& m, long long e, double (*p)[3], double (*u)[3], int* ids)
+{
+    const int et = m.elemtype;
+    if (m.conn) {
+        for (int v = 0; v < et; ++v) {
+            const int id = m.conn[e * et + v];
+            if (id < 0 || id >= m.npart) return false;
+            ids[v] = id;
+        }
+    } else {
+        // implicit block connectivity (src/PSI.c:644-656)
+        const long long nyz = (long long)m.edim[1] * m.edim[2];
+        const int i = (int)(e / nyz), j = (int)((e / m.edim[2]) % m.edim[1]), k = (int)(e % m.edim[2]);
+        for (int ii = 0; ii < 2; ++ii)
+            for (int jj = 0; jj < 2; ++jj)
+                for (int kk = 0; kk < 2; ++kk)
+                    ids[I2(ii, jj, kk)] = (int)((long long)m.bdim[1] * m.bdim[2] * ((i + ii) % m.bdim[0])
+                                                + (long long)m.bdim[2] * ((j + jj) % m.bdim[1]) + ((k + kk) % m.bdim[2]));
+    }
+    for (int v = 0; v < et; ++v)
+        for (int i = 0; i < 3; ++i) {
+            p[v][i] = m.pos[3 * (long long)ids[v] + i];
+            u[v][i] = m.vel ? m.vel[3 * (long long)ids[v] + i] : 0.0;
+        }
+    return true;
+}
+
+__device__ void aabb_n(const double (*p)[3], int n, double (*rb)[3])
+{
+    for (int i = 0; i < 3; ++i) {
+        rb[0][i] = 1.0e30;
+        rb[1][i] = -1.0e30;
+    }
+    for (int v = 0; v < n; ++v)
+        for (int i = 0; i < 3; ++i) {
+            if (p[v][i] < rb[0][i]) rb[0][i] = p[v][i];
+            if (p[v][i] > rb[1][i]) rb[1][i] = p[v][i];
+        }
+}
+
+// Unwrap an element that spans more than half the periodic box and cull it
+// against the window (src/cpsi.c:309-341).
+__device__ bool aabb_periodic(double (*p)[3], int n, const MeshDev& m, const GridDev& g)
+{
+    double rb[2][3];
+    aabb_n(p, n, rb);
+    if (m.periodic) {
+        for (int i = 0; i < 3; ++i) {
+            const double span = m.box1[i] - m.box0[i];
+            if (rb[1][i] - rb[0][i] > 0.5 * span) {
+                rb[0][i] = 1.0e30;
+                rb[1][i] = -1.0e30;
+                for (int v = 0; v < n; ++v) {
+                    if (p[v][i] > m.box0[i] + 0.5 * span) p[v][i] -= span;
+                    if (p[v][i] < rb[0][i]) rb[0][i] = p[v][i];
+                    if (p[v][i] > rb[1][i]) rb[1][i] = p[v][i];
+                }
+            }
+            if (rb[0][i] > g.w1[i]) return false;
+            if (rb[1][i] < g.w0[i] && rb[0][i] + span > g.w1[i]) return false;
+        }
+    } else {
+        for (int i = 0; i < 3; ++i) {
+            if (rb[0][i] > g.w1[i]) return false;
+            if (rb[1][i] < g.w0[i]) return false;
+        }
+    }
+    return true;
+}
+
+// Periodic images of one tet (src/cpsi.c:343-373): image 0 is the tet itself,
+// image s (bit i set = shifted by +span_i) exists when the tet reaches below
+// box0 on every axis of s and the shifted box meets the window.  Images whose
+// box lies outside the window are dropped here: the window clip would empty
+// them (smax <= 0 at src/geometry.c:430).  Returns a mask of kept images.
+__device__ unsigned tet_images(const double (*p)[3], const MeshDev& m, const GridDev& g, double (*rb)[3])
+{
+    aabb_n(p, 4, rb);
+    unsigned flags = 0, keep = 0;
+    if (m.periodic)
+        for (int i = 0; i < 3; ++i)
+            if (rb[0][i] < m.box0[i]) flags |= 1u << i;
+    for (int s = 0; s < 8; ++s) {
+        if ((flags & s) != (unsigned)s) continue;
+        bool ok = true;
+        for (int i = 0; i < 3; ++i) {
+            const double sh = (m.box1[i] - m.box0[i]) * (1 & (s >> i));
+            const double a = (s ? rb[0][i] + sh : rb[0][i]), b = (s ? rb[1][i] + sh : rb[1][i]);
+            if (s && (a > g.w1[i] || b < g.w0[i])) ok = false;  // the reference's own image test
+            if (b <= g.w0[i] || a >= g.w1[i]) ok = false;        // nothing inside the window
+        }
+        if (ok) keep |= 1u << s;
+    }
+    return keep;
+}
+
+// Ordering key of an image from its voxel index box (src/geometry.c:838-841):
+// 0xFFFF for trees deeper than the main clip kernel serves, otherwise larger
+// boxes first.
+__device__ uint16_t footprint_key(const double (*rb)[3], const GridDev& g)
+{
+    int depth = 0;
+    long long vol = 1;
+    for (int i = 0; i < 3; ++i) {
+        double cmin = rb[0][i], cmax = rb[1][i];
+        if (g.w0[i] > cmin) cmin = g.w0[i];
+        if (g.w1[i] < cmax) cmax = g.w1[i];
+        int lo = (int)floor((cmin - g.w0[i]) / g.d[i]);
+        int hi = (int)ceil((cmax - g.w0[i]) / g.d[i]);
+        if (lo < 0) lo = 0;
+        if (hi > g.n[i]) hi = g.n[i];
+        const int sz = hi - lo;
+        if (sz > 1) depth += 32 - __clz(sz - 1);
+        if (vol < 0xFFFF) vol *= (sz > 1 ? sz : 1);
+    }
+    if (depth > DMAX_MAIN) return 0xFFFF;
+    return (uint16_t)(0xFFFE - (vol < 0xFFFE ? vol : 0xFFFE));
+}
+
+struct Emitter {
+    const TessArgs& a;
+    bool write;      // false: count only
+    long long pos;   // next item index (emit)
+    int n;           // items so far
+    unsigned long long tets;
+    __device__ void tet(const double (*p)[3], const double (*u)[3], double mass, long long e, const int* pid)
+    {
+        double rb[2][3];
+        const unsigned keep = tet_images(p, a.m, a.g, rb);
+        tets++;
+        for (int s = 0; s < 8; ++s) {
+            if (!((keep >> s) & 1u)) continue;
+            if (write) {
+                const long long t = pos++;
+                const long long cap = a.it.cap;
+                double q[4][3], rq[2][3];
+                for (int v = 0; v < 4; ++v)
+                    for (int i = 0; i < 3; ++i) {
+                        const double sh = (a.m.box1[i] - a.m.box0[i]) * (1 & (s >> i));
+                        q[v][i] = s ? p[v][i] + sh : p[v][i];
+                        a.it.p[(3 * v + i) * cap + t] = q[v][i];
+                        a.it.u[(3 * v + i) * cap + t] = u[v][i];
+                    }
+                for (int i = 0; i < 3; ++i) {
+                    const double sh = (a.m.box1[i] - a.m.box0[i]) * (1 & (s >> i));
+                    rq[0][i] = s ? rb[0][i] + sh : rb[0][i];
+                    rq[1][i] = s ? rb[1][i] + sh : rb[1][i];
+                }
+                a.it.mass[t] = mass;
+                a.it.elem[t] = (int)e;
+                for (int v = 0; v < 4; ++v) a.it.pid[v * cap + t] = pid ? pid[v] : -1;
+                a.it.key[t] = footprint_key(rq, a.g);
+            }
+            n++;
+        }
+    }
+};
+
+struct RefNode {
+    double p[27][3];
+    double u[27][3];
+    double mass;
+    int child;
+};
+
+// Adaptive refinement of a trilinear element, depth first in the reference's
+// child order (src/refine.c:223-289).
+__device__ void refine_element(Emitter& em, const double (*cp)[3], const double (*cu)[3], double mass, long long e,
+                               int max_lvl, double ptol2, RefNode* L)
+{
+    interp_trilinear(cp, L[0].p);
+    interp_trilinear(cu, L[0].u);
+    L[0].mass = mass;
+    L[0].child = -1;
+    int d = 0;
+    while (d >= 0) {
+        RefNode& N = L[d];
+        if (N.child < 0) {
+            bool refine = false;
+            if (d < max_lvl)
+                for (int k = 0; k < 7 && !refine; ++k) {
+                    double err2 = 0.0;
+                    for (int i = 0; i < 3; ++i) {
+                        const double mt = 0.5 * (N.p[c_ref_edges[k][0]][i] + N.p[c_ref_edges[k][2]][i]);
+                        const double ml = N.p[c_ref_edges[k][1]][i];
+                        err2 += (mt - ml) * (mt - ml);
+                    }
+                    refine = err2 > ptol2;
+                }
+            if (!refine) {
+                for (int t = 0; t < 6; ++t) {
+                    double tp[4][3], tu[4][3];
+                    for (int v = 0; v < 4; ++v)
+                        for (int i = 0; i < 3; ++i) {
+                            tp[v][i] = N.p[c_tet_nodes[t][v]][i];
+                            tu[v][i] = N.u[c_tet_nodes[t][v]][i];
+                        }
+                    em.tet(tp, tu, N.mass * (1.0 / 6), e, nullptr);
+                }
+                d--;
+                continue;
+            }
+            N.child = 0;
+        }
+        if (N.child < 8) {
+            const int c = N.child++;
+            const int ci = c >> 2, cj = (c >> 1) & 1, ck = c & 1;
+            double kp[8][3], ku[8][3];
+            for (int a = 0; a < 2; ++a)
+                for (int b = 0; b < 2; ++b)
+                    for (int cc = 0; cc < 2; ++cc)
+                        for (int i = 0; i < 3; ++i) {
+                            kp[I2(a, b, cc)][i] = N.p[I3(a + ci, b + cj, cc + ck)][i];
+                            ku[I2(a, b, cc)][i] = N.u[I3(a + ci, b + cj, cc + ck)][i];
+                        }
+            interp_trilinear(kp, L[d + 1].p);
+            interp_trilinear(ku, L[d + 1].u);
+            L[d + 1].mass = 0.125 * N.mass;
+            L[d + 1].child = -1;
+            d++;
+        } else {
+            d--;
+        }
+    }
+}
+
+template <bool REFINE>
+__device__ int element_items(const TessArgs& a, bool write, long long e, long long pos, unsigned long long& tets,
+                             RefNode* L)
+{
+    double p[8][3], u[8][3];
+    int ids[8];
+    if (!gather(a.m, e, p, u, ids)) {
+        atomicOr(a.status, ST_INDEX);
+        return 0;
+    }
+    const int et = a.m.elemtype;
+    if (!aabb_periodic(p, et, a.m, a.g)) return 0;
+    const double me = a.m.mass ? a.m.mass[e] : 1.0;
+    Emitter em{a, write, pos, 0, 0};
+    if (et == 4) {
+        em.tet(p, u, me, e, ids); // a simplex element is one tet (src/refine.c:60-66)
+    } else if (!REFINE) {
+        for (int t = 0; t < 6; ++t) {
+            double tp[4][3], tu[4][3];
+            int pid[4];
+            for (int v = 0; v < 4; ++v) {
+                const int c = c_tet_corners[t][v];
+                pid[v] = ids[c];
+                for (int i = 0; i < 3; ++i) {
+                    tp[v][i] = p[c][i];
+                    tu[v][i] = u[c][i];
+                }
+            }
+            em.tet(tp, tu, me * (1.0 / 6), e, pid);
+        }
+    } else {
+        if constexpr (REFINE) refine_element(em, p, u, me, e, a.max_lvl, a.ptol2, L);
+    }
+    tets += em.tets;
+    return em.n;
+}
+
+template <bool REFINE, bool EMIT>
+__global__ void __launch_bounds__(128) k_tess(TessArgs a)
+{
+    RefNode* L = nullptr;
+    RefNode Lbuf[REFINE ? MAX_REFINE + 1 : 1];
+    if constexpr (REFINE) L = Lbuf;
+    unsigned long long kept = 0, tets = 0;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long e = a.e0 + blockIdx.x * (long long)blockDim.x + threadIdx.x; e < a.e1; e += stride) {
+        const long long pos = EMIT ? a.offset[e - a.e0] - a.offset_base : 0;
+        const int n = element_items<REFINE>(a, EMIT, e, pos, tets, L);
+        if (!EMIT) a.count[e - a.e0] = n;
+        kept += (n > 0);
+    }
+    if (a.counters && EMIT) {
+        atomicAdd(&a.counters[0], kept);
+        atomicAdd(&a.counters[1], tets);
+    }
+}
+
+static int tess_grid(long long n)
+{
+    long long b = (n + 127) / 128;
+    return (int)(b < 148 * 16 ? (b < 1 ? 1 : b) : 148 * 16);
+}
+
+cudaError_t launch_tess_count(const TessArgs& a, cudaStream_t s)
+{
+    const int g = tess_grid(a.e1 - a.e0);
+    if (a.max_lvl > 0 && a.m.elemtype == 8)
+        k_tess<true, false><<<g, 128, 0, s>>>(a);
+    else
+        k_tess<false, false><<<g, 128, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tess_emit(const TessArgs& a, cudaStream_t s)
+{
+    const int g = tess_grid(a.e1 - a.e0);
+    if (a.max_lvl > 0 && a.m.elemtype == 8)
+        k_tess<true, true><<<g, 128, 0, s>>>(a);
+    else
+        k_tess<false, true><<<g, 128, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+// ---- finalisation ----
+
+__global__ void k_finalize_means(FinalArgs f)
+{
+    const long long gi = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (gi >= f.nvox) return;
+    const double W = f.acc.W[gi];
+    const int vz = (int)(gi % f.g.n[2]), vy = (int)((gi / f.g.n[2]) % f.g.n[1]), vx = (int)(gi / ((long long)f.g.n[1] * f.g.n[2]));
+    const int vox[3] = {vx, vy, vz};
+    for (int i = 0; i < 3; ++i) {
+        if (f.MX) f.MX[3 * gi + i] = W > 0.0 ? f.g.w0[i] + f.g.d[i] * (vox[i] + 0.5) + f.acc.SX[3 * gi + i] / W : 0.0;
+        if (f.MV) f.MV[3 * gi + i] = W > 0.0 ? f.acc.SV[3 * gi + i] / W : 0.0;
+    }
+}
+
+// Merge the new deposit (mass W, means, covariances) into the existing fields
+// with the parallel-axis rule of the reference's online update
+// (src/geometry.c:164-186).
+__global__ void k_finalize_merge(FinalArgs f)
+{
+    const long long gi = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (gi >= f.nvox) return;
+    const double W = f.acc.W[gi];
+    if (W == 0.0) return;
+    const unsigned fl = f.acc.flags;
+    const int vz = (int)(gi % f.g.n[2]), vy = (int)((gi / f.g.n[2]) % f.g.n[1]), vx = (int)(gi / ((long long)f.g.n[1] * f.g.n[2]));
+    const int vox[3] = {vx, vy, vz};
+    double mx[3], mv[3];
+    for (int i = 0; i < 3; ++i) {
+        mx[i] = (fl & F_X) ? f.g.w0[i] + f.g.d[i] * (vox[i] + 0.5) + f.acc.SX[3 * gi + i] / W : 0.0;
+        mv[i] = (fl & F_V) ? f.acc.SV[3 * gi + i] / W : 0.0;
+    }
+    const double M0 = f.M[gi];
+    if (M0 == 0.0) {
+        f.M[gi] = W;
+        for (int i = 0; i < 3; ++i) {
+            if (fl & F_X) f.X[3 * gi + i] = mx[i];
+            if (fl & F_V) f.V[3 * gi + i] = mv[i];
+        }
+        for (int k = 0; k < 9; ++k) {
+            if (fl & F_XX) f.XX[9 * gi + k] = f.acc.XX[9 * gi + k] / W;
+            if (fl & F_XV) f.XV[9 * gi + k] = f.acc.XV[9 * gi + k] / W;
+            if (fl & F_VV) f.VV[9 * gi + k] = f.acc.VV[9 * gi + k] / W;
+        }
+        return;
+    }
+    const double Mt = M0 + W;
+    const double b = W / Mt, a = M0 / Mt;
+    double dx[3] = {0, 0, 0}, dv[3] = {0, 0, 0};
+    for (int i = 0; i < 3; ++i) {
+        if (fl & F_X) dx[i] = mx[i] - f.X[3 * gi + i];
+        if (fl & F_V) dv[i] = mv[i] - f.V[3 * gi + i];
+    }
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            const int k = 3 * i + j;
+            if (fl & F_XX) f.XX[9 * gi + k] = a * f.XX[9 * gi + k] + b * (f.acc.XX[9 * gi + k] / W) + a * b * dx[i] * dx[j];
+            if (fl & F_XV) f.XV[9 * gi + k] = a * f.XV[9 * gi + k] + b * (f.acc.XV[9 * gi + k] / W) + a * b * dx[i] * dv[j];
+            if (fl & F_VV) f.VV[9 * gi + k] = a * f.VV[9 * gi + k] + b * (f.acc.VV[9 * gi + k] / W) + a * b * dv[i] * dv[j];
+        }
+    for (int i = 0; i < 3; ++i) {
+        if (fl & F_X) f.X[3 * gi + i] += b * dx[i];
+        if (fl & F_V) f.V[3 * gi + i] += b * dv[i];
+    }
+    f.M[gi] = Mt;
+}
+
+cudaError_t launch_finalize_means(const FinalArgs& f, cudaStream_t s)
+{
+    if (f.nvox == 0) return cudaSuccess;
+    k_finalize_means<<<(unsigned)((f.nvox + 255) / 256), 256, 0, s>>>(f);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_finalize_merge(const FinalArgs& f, cudaStream_t s)
+{
+    if (f.nvox == 0) return cudaSuccess;
+    k_finalize_merge<<<(unsigned)((f.nvox + 255) / 256), 256, 0, s>>>(f);
+    return cudaGetLastError();
+}
+
+// ---- deterministic mode: the reference's online update, voxel by voxel ----
+
+// One thread per run of equal voxel keys walks the run in item order and
+// applies src/geometry.c:106-186 exactly as the reference does.
+__global__ void k_apply_records(ApplyArgs a)
+{
+    const long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (r >= a.nrec) return;
+    const unsigned long long vox = a.key[r] >> 32;
+    if (r > 0 && (a.key[r - 1] >> 32) == vox) return;
+    const long long gi = (long long)vox;
+    const long long cap = a.it.cap;
+    for (long long j = r; j < a.nrec && (a.key[j] >> 32) == vox; ++j) {
+        const long long t = a.item_base + (long long)(a.key[j] & 0xFFFFFFFFull);
+        const double* mom = a.mom + (long long)a.perm[j] * a.nmom;
+        double p0[3], v0[3], DX[3][3], DV[3][3];
+        for (int i = 0; i < 3; ++i) {
+            p0[i] = a.it.p[(i)*cap + t];
+            v0[i] = a.it.u[(i)*cap + t];
+            for (int k = 0; k < 3; ++k) {
+                DX[i][k] = a.it.p[(3 * (k + 1) + i) * cap + t] - p0[i];
+                DV[i][k] = a.it.u[(3 * (k + 1) + i) * cap + t] - v0[i];
+            }
+        }
+        const double mass = a.it.mass[t];
+        double cm[3], cv[3], sxx[3][3], sxv[3][3], svv[3][3];
+        if (a.X) centroid(mom, p0, DX, cm);
+        if (a.V) centroid(mom, v0, DV, cv);
+        if (a.XX) second_moment(mom, p0, cm, DX, p0, cm, DX, p0, cm, p0, cm, sxx);
+        if (a.XV) second_moment(mom, p0, cm, DX, v0, cv, DV, p0, cm, v0, cv, sxv);
+        if (a.VV) second_moment(mom, v0, cv, DV, v0, cv, DV, v0, cv, v0, cv, svv);
+        double* M = a.M;
+        const double cw = mass * mom[0] / (M[gi] + mass * mom[0]);
+        const double dw = M[gi] / (M[gi] + mass * mom[0]);
+        if (a.XX)
+            for (int i = 0; i < 3; ++i)
+                for (int j2 = 0; j2 < 3; ++j2) {
+                    double* o = &a.XX[9 * gi + 3 * i + j2];
+                    *o = dw * *o + cw * sxx[i][j2] + cw * dw * (cm[i] - a.X[3 * gi + i]) * (cm[j2] - a.X[3 * gi + j2]);
+                }
+        if (a.XV)
+            for (int i = 0; i < 3; ++i)
+                for (int j2 = 0; j2 < 3; ++j2) {
+                    double* o = &a.XV[9 * gi + 3 * i + j2];
+                    *o = dw * *o + cw * sxv[i][j2] + cw * dw * (cm[i] - a.X[3 * gi + i]) * (cv[j2] - a.V[3 * gi + j2]);
+                }
+        if (a.VV)
+            for (int i = 0; i < 3; ++i)
+                for (int j2 = 0; j2 < 3; ++j2) {
+                    double* o = &a.VV[9 * gi + 3 * i + j2];
+                    *o = dw * *o + cw * svv[i][j2] + cw * dw * (cv[i] - a.V[3 * gi + i]) * (cv[j2] - a.V[3 * gi + j2]);
+                }
+        if (a.X)
+            for (int i = 0; i < 3; ++i) a.X[3 * gi + i] += cw * (cm[i] - a.X[3 * gi + i]);
+        if (a.V)
+            for (int i = 0; i < 3; ++i) a.V[3 * gi + i] += cw * (cv[i] - a.V[3 * gi + i]);
+        M[gi] += mass * mom[0];
+    }
+}
+
+cudaError_t launch_apply_records(const ApplyArgs& a, cudaStream_t s)
+{
+    if (a.nrec == 0) return cudaSuccess;
+    k_apply_records<<<(unsigned)((a.nrec + 255) / 256), 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+} // namespace psib
