@@ -37,7 +37,6 @@ BOX = ((0.0, 0.0, 0.0), (100.0, 100.0, 100.0))
 FIELDS = ["x", "v", "xx", "xv", "vv"]
 WORKLOAD = "128^3 particles -> 256^3 grid, Zel'dovich rms 2 cells, fields m,x,v,xx,xv,vv"
 DATA = "synthetic: seeded Zel'dovich-displaced particle lattice (P(k)~k^-2), element mass 1"
-TETS_PER_STEP = 6 * N_PART ** 3
 FP64_FMA_PER_CLK_PER_SM = 64
 
 
@@ -49,7 +48,15 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    return ap.parse_args()
+    # smaller cases for profiling runs (the headline workload is the default)
+    ap.add_argument("--n-part", type=int, default=N_PART)
+    ap.add_argument("--n-grid", type=int, default=N_GRID)
+    ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"])
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if (args.n_part, args.n_grid) != (N_PART, N_GRID) or args.precision != "both":
+        args.no_cpu_baseline = True
+    return args
 
 
 def env_rank():
@@ -227,13 +234,15 @@ def run_ours(args):
     from pypsi_b200.metrics import field_errors, mass_error
     from pypsi_b200.synth import zeldovich
 
-    pos, vel = zeldovich(N_PART, RMS, 1234 + rank)
+    n_part, n_grid = args.n_part, args.n_grid
+    tets_per_step = 6 * n_part ** 3
+    pos, vel = zeldovich(n_part, RMS, 1234 + rank)
     dev = torch.device("cuda", local)
     dpos = torch.from_numpy(pos.reshape(-1, 3)).to(dev)
     dvel = torch.from_numpy(vel.reshape(-1, 3)).to(dev)
-    shapes = {"m": (N_GRID,) * 3, "x": (N_GRID,) * 3 + (3,), "v": (N_GRID,) * 3 + (3,)}
+    shapes = {"m": (n_grid,) * 3, "x": (n_grid,) * 3 + (3,), "v": (n_grid,) * 3 + (3,)}
     for f in ("xx", "xv", "vv"):
-        shapes[f] = (N_GRID,) * 3 + (3, 3)
+        shapes[f] = (n_grid,) * 3 + (3, 3)
 
     def fresh():
         return {f: torch.zeros(s, dtype=torch.float64, device=dev) for f, s in shapes.items()}
@@ -241,7 +250,7 @@ def run_ours(args):
     stream = torch.cuda.current_stream()
 
     def step(fields, prec):
-        return capi.voxels_device(fields, (N_GRID,) * 3, BOX, dpos, dvel, block_dims=(N_PART,) * 3,
+        return capi.voxels_device(fields, (n_grid,) * 3, BOX, dpos, dvel, block_dims=(n_part,) * 3,
                                   periodic_box=BOX, precision=prec, stream=stream)
 
     def barrier():
@@ -274,41 +283,50 @@ def run_ours(args):
         return ms / args.steps, stats, (ck.summary() if ck else None)
 
     fields = fresh()
-    ms_mixed, st_mixed, clocks = timed("mixed", fields, clocks=True)
-    ms_fp64, st_fp64, _ = timed("fp64", fields)
+    head = "fp64" if args.precision == "fp64" else "mixed"
+    ms_mixed, st_mixed, clocks = timed(head, fields, clocks=True)
+    ms_fp64, st_fp64 = ms_mixed, st_mixed
+    if args.precision == "both":
+        ms_fp64, st_fp64, _ = timed("fp64", fields)
     del fields
 
     # accuracy of the headline (mixed) against FP64 on the same input, and mass
     errs, merr = {}, {}
-    outs = {}
-    for prec in ("fp64", "mixed"):
-        f = fresh()
-        step(f, prec)
-        torch.cuda.synchronize()
-        outs[prec] = {k: v.cpu().numpy() for k, v in f.items()}
-        merr[prec] = mass_error(outs[prec]["m"], N_PART ** 3)
-        del f
-    errs = field_errors(outs["mixed"], outs["fp64"])
-    del outs
+    if args.precision == "both":
+        outs = {}
+        for prec in ("fp64", "mixed"):
+            f = fresh()
+            step(f, prec)
+            torch.cuda.synchronize()
+            outs[prec] = {k: v.cpu().numpy() for k, v in f.items()}
+            merr[prec] = mass_error(outs[prec]["m"], n_part ** 3)
+            del f
+        errs = field_errors(outs["mixed"], outs["fp64"])
+        del outs
     torch.cuda.empty_cache()
 
     # end to end through the drop-in module: host numpy in, host numpy out
-    mesh = PSI.Mesh(loader="block", pos=pos, vel=vel, periodic_box=BOX)
-    grid = PSI.Grid(n=(N_GRID,) * 3, bounds=BOX, fields=FIELDS)
-    PSI.voxels(grid=grid, mesh=mesh, precision="mixed")
-    barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.e2e_steps):
-        PSI.voxels(grid=grid, mesh=mesh, precision="mixed")
-    e2e_s = (time.perf_counter() - t0) / args.e2e_steps
-    if dist:
-        t = torch.tensor([e2e_s], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    field_bytes = sum(a.nbytes for a in grid.fields.values())
-    h2d = pos.nbytes + vel.nbytes + mesh.mass.nbytes + field_bytes
-    d2h = field_bytes
-    del grid
+    e2e = None
+    if not args.no_e2e:
+        mesh = PSI.Mesh(loader="block", pos=pos, vel=vel, periodic_box=BOX)
+        grid = PSI.Grid(n=(n_grid,) * 3, bounds=BOX, fields=FIELDS)
+        PSI.voxels(grid=grid, mesh=mesh, precision=head)
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            PSI.voxels(grid=grid, mesh=mesh, precision=head)
+        e2e_s = (time.perf_counter() - t0) / args.e2e_steps
+        if dist:
+            t = torch.tensor([e2e_s], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        field_bytes = sum(a.nbytes for a in grid.fields.values())
+        e2e = {"value": world * tets_per_step / e2e_s, "unit": "tets/s",
+               "h2d_bytes_per_step": pos.nbytes + vel.nbytes + mesh.mass.nbytes + field_bytes,
+               "d2h_bytes_per_step": field_bytes,
+               "api": f"PSI.voxels(grid, mesh, precision='{head}') on host numpy arrays",
+               "ms_per_step": e2e_s * 1e3}
+        del grid
     capi.lib.psib_release_device_memory()
 
     if dist:
@@ -316,15 +334,13 @@ def run_ours(args):
     if rank != 0:
         return
 
-    # roofline of the clip kernels (the dominant work): algorithmic FP64 flops
-    # per fragment F_k = 20 V + t_k (2V - 4) + P_k (V = mean vertices/fragment),
-    # k = 1 on the first clip pass and 2 on the second.
+    # roofline of the clip kernels: algorithmic FP64 flops per fragment
+    # F_2 = 20 V + 132 (2V - 4) + 520 (V = mean vertices per fragment; clip,
+    # order-2 reduce, projection and update)
     s = st_mixed[-1]
     frags = s["fragments"] / s["passes"]
     vbar = s["frag_verts"] / max(1, s["fragments"])
-    f1 = 20 * vbar + 33 * (2 * vbar - 4) + 50
-    f2 = 20 * vbar + 132 * (2 * vbar - 4) + 520
-    flops = frags * (f1 + f2)
+    flops = frags * (20 * vbar + 132 * (2 * vbar - 4) + 520)
     clip_ms = statistics.mean(x["ms_clip"] for x in st_mixed)
     launches = s["clip_launches"]
     achieved = flops / (clip_ms * 1e-3) / 1e12
@@ -333,33 +349,37 @@ def run_ours(args):
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except OSError:
         peaks = {}
-    value = world * TETS_PER_STEP / (ms_mixed * 1e-3)
+    value = world * tets_per_step / (ms_mixed * 1e-3)
     line = {
         "metric": METRIC, "value": value, "unit": "tets/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32+f64", "data": DATA,
-        "config": {"workload": WORKLOAD, "precision": "mixed (FP32 clip, FP64 moments/accumulation)",
+        "vs_baseline": None, "dtype": "f64" if head == "fp64" else "f32+f64", "data": DATA,
+        "config": {"workload": WORKLOAD if (n_part, n_grid) == (N_PART, N_GRID) else
+                   f"{n_part}^3 particles -> {n_grid}^3 grid, Zel'dovich rms 2 cells, fields m,x,v,xx,xv,vv",
+                   "precision": "fp64 (reference operation order)" if head == "fp64" else
+                   "mixed (FP32 clip, FP64 moments/accumulation)",
                    "l2": "inputs larger than L2 (4.6 GB of grid fields, 3 GB of tet images per step)",
                    "per_rank": "each rank deposits its own lattice (seed 1234+rank) on its own GPU"},
-        "fp64": {"value": world * TETS_PER_STEP / (ms_fp64 * 1e-3), "unit": "tets/s", "ms_per_step": ms_fp64},
+        "fp64": {"value": world * tets_per_step / (ms_fp64 * 1e-3), "unit": "tets/s", "ms_per_step": ms_fp64},
         "mixed_over_fp64": ms_fp64 / ms_mixed,
         "voxel_clips_per_s": world * frags / (ms_mixed * 1e-3),
-        "mixed_vs_fp64_err": {f: e["norm"] for f, e in errs.items() if f != "dead_m"},
-        "mixed_vs_fp64_err_m_rel": errs["m"]["rel"],
+        "mixed_vs_fp64_err": {f: e["norm"] for f, e in errs.items() if f != "dead_m"} if errs else None,
+        "mixed_vs_fp64_err_m_rel": errs["m"]["rel"] if errs else None,
         "mass_err": merr,
         "fwd_bwd_over_fwd": None,
-        "work": {"tets": TETS_PER_STEP, "tet_images": s["tet_images"], "fragments_per_pass": frags,
+        "stage_ms": {"tessellate_and_order": statistics.mean(x["ms_tess"] for x in st_mixed),
+                     "clip": statistics.mean(x["ms_clip"] for x in st_mixed),
+                     "sort_and_apply": statistics.mean(x["ms_final"] for x in st_mixed)},
+        "work": {"tets": tets_per_step, "tet_images": s["tet_images"], "fragments_per_pass": frags,
                  "verts_per_fragment": vbar, "passes": s["passes"], "splits_per_pass": s["splits"] / s["passes"]},
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                     "traffic": None, "kernel": "clip-and-deposit (both passes)",
-                     "achieved_def": "sum over fragments of F_1 + F_2 algorithmic FP64 flops / clip-kernel event time",
+                     "traffic": None, "kernel": "clip (records)",
+                     "achieved_def": "sum over fragments of F_2 algorithmic FP64 flops / clip-kernel event time",
                      "peak_source": "FP64 FMA issue rate 64/clk/SM x 148 SMs x 2 flop at 1965 MHz; "
                                     "MEASURED_PEAKS.json has no FP64 figure",
                      "clip_ms_per_step": clip_ms, "clip_launches_per_step": launches,
                      "hbm_peak_gbs_measured": peaks.get("hbm_gbs")},
-        "e2e": {"value": world * TETS_PER_STEP / e2e_s, "unit": "tets/s", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h, "api": "PSI.voxels(grid, mesh, precision='mixed') on host numpy arrays",
-                "ms_per_step": e2e_s * 1e3},
+        "e2e": e2e,
         "gpu_launches": int(sum(x["kernel_launches"] for x in st_mixed)),
         "clocks": clocks,
     }

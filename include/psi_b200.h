@@ -90,22 +90,23 @@ typedef struct {
     long long elements_kept; /* elements surviving the window cull */
     long long tets;          /* tets after refinement, without periodic images */
     long long tet_images;    /* tets including periodic images (work items) */
-    long long fragments;     /* (tet image, voxel) pieces with m0 > 0, summed over passes */
-    long long frag_verts;    /* sum of fragment vertex counts, summed over passes */
-    long long splits;        /* axis-aligned splits, summed over passes */
-    int passes;              /* clip passes over the tets (2 for second-order fields) */
+    long long fragments;     /* (tet image, voxel) pieces with m0 > 0 */
+    long long frag_verts;    /* sum of fragment vertex counts */
+    long long splits;        /* axis-aligned splits of the bisection */
+    int passes;              /* clip passes over the tets (1) */
     int chunks;              /* element chunks the tets were streamed in */
     float ms_total;          /* device time of the whole call, host copies included */
-    float ms_clip;           /* device time of the clip-and-deposit kernels */
+    float ms_clip;           /* device time of the clip kernels */
     float ms_tess;           /* device time of tessellation and ordering */
-    float ms_final;          /* device time of the finalisation kernels */
-    long long clip_launches; /* launches of the clip-and-deposit kernels */
+    float ms_final;          /* device time of the record sort and the field update */
+    long long clip_launches; /* launches of the clip kernels */
     long long kernel_launches; /* launches of this library's own kernels (library scans/sorts excluded) */
 } psib_stats;
 
 typedef struct {
     int precision;     /* PSIB_FP64 or PSIB_MIXED */
-    int deterministic; /* 1: sort-and-segmented-update mode, bit-reproducible (FP64 only) */
+    int deterministic; /* accepted for compatibility: every call is deterministic (fragments are sorted
+                          by voxel and applied in the reference's order; FP64 equals the reference bit for bit) */
     int memory;        /* PSIB_HOST or PSIB_DEVICE */
     int device;        /* CUDA device ordinal for PSIB_HOST calls (-1: current) */
     void *stream;      /* cudaStream_t for PSIB_DEVICE calls; NULL: legacy default stream */

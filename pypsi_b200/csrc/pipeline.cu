@@ -1,17 +1,19 @@
 // pipeline.cu -- the C ABI (include/psi_b200.h) and the host orchestration of
 // one PSI.voxels call on the GPU:
 //
-//   count   elements -> tet images per element          (tess.cu)
+//   count   elements -> tet images per element             (tess.cu)
 //   scan    per-element offsets (CUB)
-//   emit    tet images in the reference's visiting order (tess.cu)
-//   order   images sorted by footprint key (CUB radix sort)
-//   clip    persistent clip-and-deposit kernels          (clip_fp64.cu / clip_mixed.cu)
-//   final   voxel means / covariances merged into the fields (tess.cu)
+//   emit    tet images in the reference's visiting order    (tess.cu)
+//   order   images sorted by footprint key (CUB radix sort) for load balance
+//   clip    persistent clip kernels: one record per fragment (clip_fp64.cu / clip_mixed.cu)
+//   sort    records by (voxel, image) (CUB radix sort)
+//   apply   each voxel's records, in image order, with the reference's
+//           online field update (tess.cu)
 //
-// Second-order fields take two clip passes (means first, then centred second
-// moments).  Meshes whose tet images exceed the item budget are streamed in
-// element chunks.  Deterministic mode records fragments, sorts them by
-// (voxel, item) and applies the reference's online update per voxel.
+// Images are numbered in the reference's visiting order, so each voxel sees
+// its fragments in the reference's order and the FP64 path reproduces the
+// reference's fields bit for bit.  Meshes whose tet images exceed the item
+// budget are streamed in element chunks, in order.
 #include <cub/cub.cuh>
 #include <cuda_runtime.h>
 
@@ -87,22 +89,20 @@ struct Ctx {
     cudaEvent_t ev[8] = {};
     // host-mode copies
     DevBuf hpos, hvel, hmass, hconn, hfield[6];
-    // accumulators
-    DevBuf W, SX, SV, XX, XV, VV, MX, MV;
     // items
-    DevBuf ip, iu, imass, ielem, ipid, ikey;
+    DevBuf iframe, ielem, ipid, ikey;
     DevBuf key_sorted, order_in, order;
     DevBuf counts, offsets;
-    DevBuf cub_tmp, scratch;
-    DevBuf small; // status, counters, heads
+    DevBuf cub_tmp, scratch, scratch_big, iscale;
+    DevBuf small; // status, counters, queue heads
     // records
-    DevBuf rkey, rmom, rkey_sorted, rperm_in, rperm;
+    DevBuf rkey, rmom, rkey_sorted, rperm_in, rperm, rvox, ritem, rmom_sorted, run_vox, run_cnt, run_off;
     std::vector<DevBuf*> all()
     {
         return {&hpos, &hpos, &hvel, &hmass, &hconn, &hfield[0], &hfield[1], &hfield[2], &hfield[3], &hfield[4],
-                &hfield[5], &W, &SX, &SV, &XX, &XV, &VV, &MX, &MV, &ip, &iu, &imass, &ielem, &ipid, &ikey,
-                &key_sorted, &order_in, &order, &counts, &offsets, &cub_tmp, &scratch, &small, &rkey, &rmom,
-                &rkey_sorted, &rperm_in, &rperm};
+                &hfield[5], &iframe, &ielem, &ipid, &ikey,
+                &key_sorted, &order_in, &order, &counts, &offsets, &cub_tmp, &scratch, &scratch_big, &iscale, &small, &rkey, &rmom,
+                &rkey_sorted, &rperm_in, &rperm, &rvox, &ritem, &rmom_sorted, &run_vox, &run_cnt, &run_off};
     }
 };
 
@@ -127,7 +127,7 @@ int get_ctx(int dev, Ctx** out)
 
 // small device block layout (unsigned long long words)
 enum { S_STATUS = 0, S_CNT = 1 /* 3 words */, S_TESS = 4 /* 2 */, S_HEAD = 8 /* 4 */, S_RECN = 12, S_NDEEP = 13,
-       S_ANY = 14, S_WORDS = 16 };
+       S_WORDS = 16 };
 
 __global__ void k_count_deep(const uint16_t* key, long long n, unsigned long long* out)
 {
@@ -199,8 +199,9 @@ int run_device(Call& c)
     if (c.F[4]) flags |= F_XV;
     if (c.F[5]) flags |= F_VV;
     const int order = (flags & (F_XX | F_XV | F_VV)) ? 2 : (flags & (F_X | F_V)) ? 1 : 0;
-    const bool det = c.deterministic != 0;
-    const int passes = (!det && order == 2) ? 2 : 1;
+    const bool mixed = c.precision == PSIB_MIXED;
+    // 1, 4 or 10 moments per record (FP32 kernel: m0, q-centroid, central second moment)
+    const int nmom = order == 2 ? 10 : order == 1 ? 4 : 1;
 
     GridDev gd;
     for (int i = 0; i < 3; ++i) {
@@ -230,25 +231,6 @@ int run_device(Call& c)
         if (g.d[i] < dxmin) dxmin = g.d[i];
     const double tol = c.reftol * dxmin;
 
-    // accumulators
-    const size_t v8 = (size_t)nvox * sizeof(double);
-    AccDev acc = {};
-    acc.flags = flags;
-    if (!det) {
-        RET(ensure(C.W, v8));
-        acc.W = C.W.as<double>();
-        CK(cudaMemsetAsync(acc.W, 0, v8, st));
-        if (flags & F_X) { RET(ensure(C.SX, 3 * v8)); acc.SX = C.SX.as<double>(); CK(cudaMemsetAsync(acc.SX, 0, 3 * v8, st)); }
-        if (flags & F_V) { RET(ensure(C.SV, 3 * v8)); acc.SV = C.SV.as<double>(); CK(cudaMemsetAsync(acc.SV, 0, 3 * v8, st)); }
-        if (flags & F_XX) { RET(ensure(C.XX, 9 * v8)); acc.XX = C.XX.as<double>(); CK(cudaMemsetAsync(acc.XX, 0, 9 * v8, st)); }
-        if (flags & F_XV) { RET(ensure(C.XV, 9 * v8)); acc.XV = C.XV.as<double>(); CK(cudaMemsetAsync(acc.XV, 0, 9 * v8, st)); }
-        if (flags & F_VV) { RET(ensure(C.VV, 9 * v8)); acc.VV = C.VV.as<double>(); CK(cudaMemsetAsync(acc.VV, 0, 9 * v8, st)); }
-        if (passes == 2) {
-            if (flags & (F_XX | F_XV)) { RET(ensure(C.MX, 3 * v8)); acc.MX = C.MX.as<double>(); }
-            if (flags & (F_XV | F_VV)) { RET(ensure(C.MV, 3 * v8)); acc.MV = C.MV.as<double>(); }
-        }
-    }
-
     RET(ensure(C.small, S_WORDS * 8));
     unsigned long long* sm = C.small.as<unsigned long long>();
     CK(cudaMemsetAsync(sm, 0, S_WORDS * 8, st));
@@ -267,19 +249,20 @@ int run_device(Call& c)
     ta.counters = &sm[S_TESS];
     std::vector<long long> offs_host;
     long long total = 0;
+    long long klaunch = 0; // this library's own kernel launches
     {
-        // counts are written as int into the long long buffer's first half; widen via scan input
+        // counts are written as int into the first half of the buffer
         ta.e0 = 0;
         ta.e1 = ne;
         ta.count = (int*)C.counts.p;
         CK(launch_tess_count(ta, st));
+        klaunch++;
         size_t tb = 0;
         const int* cin = (const int*)C.counts.p;
         long long* cout = C.offsets.as<long long>();
+        CK(cudaMemsetAsync((int*)C.counts.p + ne, 0, sizeof(int), st));
         CK(cub::DeviceScan::ExclusiveScan(nullptr, tb, cin, cout, cub::Sum(), (long long)0, (int)(ne + 1), st));
         RET(ensure(C.cub_tmp, tb));
-        // the (ne+1)-th count must be zero for the total to land in offsets[ne]
-        CK(cudaMemsetAsync((int*)C.counts.p + ne, 0, sizeof(int), st));
         CK(cub::DeviceScan::ExclusiveScan(C.cub_tmp.p, tb, cin, cout, cub::Sum(), (long long)0, (int)(ne + 1), st));
         CK(cudaMemcpyAsync(&total, cout + ne, sizeof(long long), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
@@ -290,8 +273,8 @@ int run_device(Call& c)
         RET(check_status(c, h));
     }
 
-    // ---- chunking ----
-    const long long budget = env_ll("PSIB_ITEM_BUDGET", 24ll << 20);
+    // ---- chunking: images are streamed in element chunks of at most `budget` ----
+    const long long budget = env_ll("PSIB_ITEM_BUDGET", 16ll << 20);
     std::vector<long long> cb; // element boundaries
     cb.push_back(0);
     if (total > budget) {
@@ -315,211 +298,214 @@ int run_device(Call& c)
         for (int k = 0; k < nchunks; ++k) cap = std::max(cap, offs_host[cb[k + 1]] - offs_host[cb[k]]);
     if (cap < 1) cap = 1;
 
-    RET(ensure(C.ip, (size_t)cap * 12 * sizeof(double)));
-    RET(ensure(C.iu, (size_t)cap * 12 * sizeof(double)));
-    RET(ensure(C.imass, (size_t)cap * sizeof(double)));
+    RET(ensure(C.iframe, (size_t)cap * FRAME * sizeof(double)));
     RET(ensure(C.ielem, (size_t)cap * sizeof(int)));
     RET(ensure(C.ipid, (size_t)cap * 4 * sizeof(int)));
     RET(ensure(C.ikey, (size_t)cap * sizeof(uint16_t)));
     RET(ensure(C.key_sorted, (size_t)cap * sizeof(uint16_t)));
     RET(ensure(C.order_in, (size_t)cap * sizeof(int)));
     RET(ensure(C.order, (size_t)cap * sizeof(int)));
+    if (mixed) RET(ensure(C.iscale, (size_t)cap * sizeof(double)));
     ItemArrays it;
-    it.p = C.ip.as<double>();
-    it.u = C.iu.as<double>();
-    it.mass = C.imass.as<double>();
+    it.frame = C.iframe.as<double>();
     it.elem = C.ielem.as<int>();
     it.pid = C.ipid.as<int>();
     it.key = C.ikey.as<uint16_t>();
     it.cap = cap;
     ta.it = it;
-    ta.offset = C.offsets.as<long long>();
 
-    // occupancy of the persistent clip kernels
-    int clip_block = 128;
-    int clip_grid = C.num_sms * 4;
-    const int big_block = 64;
-    const size_t big_bytes = (c.precision == PSIB_MIXED && !det) ? scratch_bytes_mixed_big() : scratch_bytes_fp64_big();
+    // persistent clip kernels: one resident wave, each thread with its own scratch region
+    const int clip_block = 128, big_block = 64;
+    const int clip_grid =
+        C.num_sms * (mixed ? clip_blocks_per_sm_mixed(false, clip_block) : clip_blocks_per_sm_fp64(false, clip_block));
+    const size_t main_bytes = mixed ? scratch_bytes_mixed(false) : scratch_bytes_fp64(false);
+    const size_t big_bytes = mixed ? scratch_bytes_mixed(true) : scratch_bytes_fp64(true);
+    RET(ensure(C.scratch, main_bytes * (size_t)clip_grid * clip_block));
 
     ClipArgs ca = {};
     ca.it = it;
     ca.order = C.order.as<int>();
     ca.g = gd;
-    ca.acc = acc;
     ca.mom_order = order;
     ca.status = (unsigned*)&sm[S_STATUS];
     ca.counters = &sm[S_CNT];
+    ca.rec_nmom = nmom;
+    ca.rec_n = &sm[S_RECN];
+    ca.rec_item_base = 0;
+    ca.scale = mixed ? C.iscale.as<double>() : nullptr;
 
-    float ms_clip = 0.f, ms_tess = 0.f;
-    long long launches = 0, klaunch = 1; // the count kernel
-    double* MXw = acc.MX ? (double*)acc.MX : nullptr;
-    double* MVw = acc.MV ? (double*)acc.MV : nullptr;
+    float ms_clip = 0.f, ms_tess = 0.f, ms_final = 0.f;
+    unsigned long long clip_counts[3] = {0, 0, 0}; // fragments, fragment vertices, splits
+    long long launches = 0;
+    for (int k = 0; k < nchunks; ++k) {
+        const long long e0 = cb[k], e1 = cb[k + 1];
+        const long long obase = nchunks == 1 ? 0 : offs_host[e0];
+        const long long nitems = nchunks == 1 ? total : offs_host[e1] - obase;
+        if (nitems == 0) continue;
+        if (nitems >= (1ll << 32)) return fail(PSIB_ERR_OVERFLOW, "too many tet images in one chunk");
+        // ---- emit images, order them by footprint ----
+        CK(cudaEventRecord(C.ev[2], st));
+        ta.e0 = e0;
+        ta.e1 = e1;
+        ta.offset = C.offsets.as<long long>() + e0;
+        ta.offset_base = obase;
+        CK(launch_tess_emit(ta, st));
+        CK(cudaMemsetAsync(&sm[S_NDEEP], 0, 8, st));
+        k_iota<<<C.num_sms * 8, 256, 0, st>>>(C.order_in.as<int>(), nitems);
+        CK(cudaGetLastError());
+        k_count_deep<<<C.num_sms * 8, 256, 0, st>>>(it.key, nitems, &sm[S_NDEEP]);
+        CK(cudaGetLastError());
+        klaunch += 3;
+        size_t tb = 0;
+        CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, it.key, C.key_sorted.as<uint16_t>(), C.order_in.as<int>(),
+                                           C.order.as<int>(), (int)nitems, 0, 16, st));
+        RET(ensure(C.cub_tmp, tb));
+        CK(cub::DeviceRadixSort::SortPairs(C.cub_tmp.p, tb, it.key, C.key_sorted.as<uint16_t>(), C.order_in.as<int>(),
+                                           C.order.as<int>(), (int)nitems, 0, 16, st));
+        unsigned long long hd = 0;
+        CK(cudaEventRecord(C.ev[3], st));
+        CK(cudaMemcpyAsync(&hd, &sm[S_NDEEP], 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        const long long ndeep = (long long)hd, nmain = nitems - ndeep;
+        {
+            float t = 0.f;
+            CK(cudaEventElapsedTime(&t, C.ev[2], C.ev[3]));
+            ms_tess += t;
+        }
 
-    for (int pass = 1; pass <= passes; ++pass) {
-        for (int k = 0; k < nchunks; ++k) {
-            const long long e0 = cb[k], e1 = cb[k + 1];
-            long long obase = 0, nitems = 0;
-            if (nchunks == 1) {
-                obase = 0;
-                nitems = total;
-            } else {
-                obase = offs_host[e0];
-                nitems = offs_host[e1] - obase;
+        // ---- clip to fragment records; grow the record buffer and redo if it overflowed ----
+        int ibits = 1, vbits = 1;
+        while ((1ll << ibits) < nitems) ++ibits;
+        while ((1ll << vbits) < nvox) ++vbits;
+        if (ibits + vbits > 64) return fail(PSIB_ERR_OVERFLOW, "grid and chunk too large for a 64-bit record key");
+        ca.rec_ibits = ibits;
+        for (int attempt = 0;; ++attempt) {
+            const unsigned long long want = (unsigned long long)std::max<long long>(nitems * 20, 1 << 16);
+            const unsigned long long have = std::max<unsigned long long>(C.rkey.n / 8, want);
+            RET(ensure(C.rkey, have * 8));
+            RET(ensure(C.rmom, have * 8 * nmom));
+            ca.rec_key = C.rkey.as<unsigned long long>();
+            ca.rec_mom = C.rmom.as<double>();
+            ca.rec_cap = std::min<unsigned long long>(C.rkey.n / 8, C.rmom.n / (8 * nmom));
+            CK(cudaMemsetAsync(&sm[S_RECN], 0, 8, st));
+            CK(cudaMemsetAsync(&sm[S_CNT], 0, 24, st)); // this attempt's counters
+            CK(cudaMemsetAsync(&sm[S_HEAD], 0, 16, st));
+            CK(cudaEventRecord(C.ev[4], st));
+            if (nmain > 0) {
+                ca.scratch = C.scratch.p;
+                ca.order_base = 0;
+                ca.n = nmain;
+                ca.head = &sm[S_HEAD];
+                if (mixed) CK(launch_clip_mixed(ca, false, clip_grid, clip_block, st));
+                else CK(launch_clip_fp64(ca, false, clip_grid, clip_block, st));
+                launches++;
             }
-            if (nitems == 0) continue;
-            const bool reuse = (nchunks == 1 && pass > 1);
-            long long nmain = nitems, ndeep = 0;
-            CK(cudaEventRecord(C.ev[2], st));
-            if (!reuse) {
-                ta.e0 = e0;
-                ta.e1 = e1;
-                ta.offset = C.offsets.as<long long>() + e0;
-                ta.offset_base = obase;
-                ta.counters = (pass == 1) ? &sm[S_TESS] : nullptr;
-                CK(launch_tess_emit(ta, st));
-                klaunch += 3; // emit, iota, count_deep
-                // order by footprint key
-                CK(cudaMemsetAsync(&sm[S_NDEEP], 0, 8, st));
-                k_iota<<<C.num_sms * 8, 256, 0, st>>>(C.order_in.as<int>(), nitems);
-                CK(cudaGetLastError());
-                k_count_deep<<<C.num_sms * 8, 256, 0, st>>>(it.key, nitems, &sm[S_NDEEP]);
-                CK(cudaGetLastError());
-                size_t tb = 0;
-                CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, it.key, C.key_sorted.as<uint16_t>(),
-                                                   C.order_in.as<int>(), C.order.as<int>(), (int)nitems, 0, 16, st));
-                RET(ensure(C.cub_tmp, tb));
-                CK(cub::DeviceRadixSort::SortPairs(C.cub_tmp.p, tb, it.key, C.key_sorted.as<uint16_t>(),
-                                                   C.order_in.as<int>(), C.order.as<int>(), (int)nitems, 0, 16, st));
+            if (ndeep > 0) {
+                const int big_grid = (int)std::min<long long>(C.num_sms * 2, (ndeep + big_block - 1) / big_block);
+                RET(ensure(C.scratch_big, big_bytes * (size_t)big_grid * big_block));
+                ca.scratch = C.scratch_big.p;
+                ca.order_base = nmain;
+                ca.n = ndeep;
+                ca.head = &sm[S_HEAD + 1];
+                if (mixed) CK(launch_clip_mixed(ca, true, big_grid, big_block, st));
+                else CK(launch_clip_fp64(ca, true, big_grid, big_block, st));
+                launches++;
             }
-            unsigned long long hd = 0;
-            CK(cudaMemcpyAsync(&hd, &sm[S_NDEEP], 8, cudaMemcpyDeviceToHost, st));
+            CK(cudaEventRecord(C.ev[5], st));
+            unsigned long long h[S_WORDS];
+            CK(cudaMemcpyAsync(h, sm, sizeof(h), cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
-            ndeep = (long long)hd;
-            nmain = nitems - ndeep;
-            CK(cudaEventRecord(C.ev[3], st));
             {
                 float t = 0.f;
-                CK(cudaEventElapsedTime(&t, C.ev[2], C.ev[3]));
-                ms_tess += t;
+                CK(cudaEventElapsedTime(&t, C.ev[4], C.ev[5]));
+                ms_clip += t;
             }
-
-            ca.pass = pass;
-            ca.acc = acc;
-            if (pass == 2) {
-                ca.acc.MX = MXw;
-                ca.acc.MV = MVw;
+            const unsigned long long nrec = h[S_RECN];
+            if (nrec > ca.rec_cap && attempt == 0) {
+                // the buffer was too small: grow to the exact need and redo the chunk
+                RET(ensure(C.rkey, nrec * 8));
+                RET(ensure(C.rmom, nrec * 8 * nmom));
+                unsigned clr = 0;
+                CK(cudaMemcpy(&sm[S_STATUS], &clr, sizeof(clr), cudaMemcpyHostToDevice));
+                continue;
             }
-            bool redo = true;
-            while (redo) {
-                redo = false;
-                if (det) {
-                    const unsigned long long want = (unsigned long long)std::max<long long>(nitems * 40, 1 << 16);
-                    const int nm = order == 2 ? 10 : order == 1 ? 4 : 1;
-                    const unsigned long long have = std::max<unsigned long long>(C.rkey.n / 8, want);
-                    RET(ensure(C.rkey, have * 8));
-                    RET(ensure(C.rmom, have * 8 * nm));
-                    ca.rec_key = C.rkey.as<unsigned long long>();
-                    ca.rec_mom = C.rmom.as<double>();
-                    ca.rec_cap = std::min<unsigned long long>(C.rkey.n / 8, C.rmom.n / (8 * nm));
-                    ca.rec_nmom = order == 2 ? 10 : order == 1 ? 4 : 1;
-                    ca.rec_n = &sm[S_RECN];
-                    ca.rec_item_base = 0;
-                    CK(cudaMemsetAsync(&sm[S_RECN], 0, 8, st));
-                }
-                CK(cudaEventRecord(C.ev[4], st));
-                CK(cudaMemsetAsync(&sm[S_HEAD], 0, 16, st));
-                if (nmain > 0) {
-                    ca.order_base = 0;
-                    ca.n = nmain;
-                    ca.head = &sm[S_HEAD];
-                    if (c.precision == PSIB_MIXED && !det) CK(launch_clip_mixed(ca, false, clip_grid, clip_block, st));
-                    else CK(launch_clip_fp64(ca, false, det, clip_grid, clip_block, st));
-                    launches++;
-                }
-                if (ndeep > 0) {
-                    const int big_grid = (int)std::min<long long>(C.num_sms * 2, (ndeep + big_block - 1) / big_block);
-                    RET(ensure(C.scratch, big_bytes * (size_t)big_grid * big_block));
-                    ca.scratch = C.scratch.p;
-                    ca.order_base = nmain;
-                    ca.n = ndeep;
-                    ca.head = &sm[S_HEAD + 1];
-                    if (c.precision == PSIB_MIXED && !det) CK(launch_clip_mixed(ca, true, big_grid, big_block, st));
-                    else CK(launch_clip_fp64(ca, true, det, big_grid, big_block, st));
-                    launches++;
-                }
-                CK(cudaEventRecord(C.ev[5], st));
-                {
-                    CK(cudaEventSynchronize(C.ev[5]));
-                    float t = 0.f;
-                    CK(cudaEventElapsedTime(&t, C.ev[4], C.ev[5]));
-                    ms_clip += t;
-                }
-                if (det) {
-                    unsigned long long h[S_WORDS];
-                    CK(cudaMemcpy(h, sm, sizeof(h), cudaMemcpyDeviceToHost));
-                    const unsigned long long nrec = h[S_RECN];
-                    if (nrec > ca.rec_cap) {
-                        // the buffer was too small: grow to the exact need and redo the chunk
-                        RET(ensure(C.rkey, nrec * 8));
-                        RET(ensure(C.rmom, nrec * 8 * ca.rec_nmom));
-                        unsigned clr = 0;
-                        CK(cudaMemcpy(&sm[S_STATUS], &clr, sizeof(clr), cudaMemcpyHostToDevice));
-                        redo = true;
-                        continue;
-                    }
-                    RET(check_status(c, h));
-                    if (nrec > 0xFFFFFFFFull) return fail(PSIB_ERR_OVERFLOW, "too many fragments in one chunk");
-                    RET(ensure(C.rkey_sorted, nrec * 8));
-                    RET(ensure(C.rperm_in, nrec * 4));
-                    RET(ensure(C.rperm, nrec * 4));
-                    k_iota_u<<<C.num_sms * 8, 256, 0, st>>>(C.rperm_in.as<unsigned>(), (long long)nrec);
-                    CK(cudaGetLastError());
-                    int vbits = 1;
-                    while ((1ll << vbits) < nvox) ++vbits;
-                    size_t tb = 0;
-                    CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, C.rkey.as<unsigned long long>(),
-                                                       C.rkey_sorted.as<unsigned long long>(), C.rperm_in.as<unsigned>(),
-                                                       C.rperm.as<unsigned>(), (int)nrec, 0, 32 + vbits, st));
-                    RET(ensure(C.cub_tmp, tb));
-                    CK(cub::DeviceRadixSort::SortPairs(C.cub_tmp.p, tb, C.rkey.as<unsigned long long>(),
-                                                       C.rkey_sorted.as<unsigned long long>(), C.rperm_in.as<unsigned>(),
-                                                       C.rperm.as<unsigned>(), (int)nrec, 0, 32 + vbits, st));
-                    ApplyArgs aa = {};
-                    aa.key = C.rkey_sorted.as<unsigned long long>();
-                    aa.mom = C.rmom.as<double>();
-                    aa.perm = C.rperm.as<unsigned>();
-                    aa.nrec = (long long)nrec;
-                    aa.nmom = ca.rec_nmom;
-                    aa.it = it;
-                    aa.item_base = 0;
-                    aa.M = c.F[0]; aa.X = c.F[1]; aa.V = c.F[2]; aa.XX = c.F[3]; aa.XV = c.F[4]; aa.VV = c.F[5];
-                    CK(launch_apply_records(aa, st));
-                    klaunch += 2; // iota, apply
-                }
-            }
-        }
-        if (pass == 1 && passes == 2) {
-            FinalArgs f = {};
-            f.g = gd;
-            f.acc = acc;
-            f.MX = MXw;
-            f.MV = MVw;
-            f.nvox = nvox;
-            CK(launch_finalize_means(f, st));
-            klaunch++;
+            RET(check_status(c, h));
+            for (int w = 0; w < 3; ++w) clip_counts[w] += h[S_CNT + w];
+            if (nrec >= (1ull << 32)) return fail(PSIB_ERR_OVERFLOW, "too many fragments in one chunk");
+            if (nrec == 0) break;
+            // ---- sort records by (voxel, image), gather them in that order, apply each voxel's run ----
+            CK(cudaEventRecord(C.ev[6], st));
+            RET(ensure(C.rkey_sorted, nrec * 8));
+            RET(ensure(C.rperm_in, nrec * 4));
+            RET(ensure(C.rperm, nrec * 4));
+            RET(ensure(C.rvox, nrec * 4));
+            RET(ensure(C.ritem, nrec * 4));
+            RET(ensure(C.rmom_sorted, nrec * 8 * nmom));
+            const long long maxruns = std::min<long long>((long long)nrec, nvox);
+            RET(ensure(C.run_vox, (size_t)maxruns * 4));
+            RET(ensure(C.run_cnt, (size_t)maxruns * 4 + 8));
+            RET(ensure(C.run_off, (size_t)maxruns * 8));
+            k_iota_u<<<C.num_sms * 8, 256, 0, st>>>(C.rperm_in.as<unsigned>(), (long long)nrec);
+            CK(cudaGetLastError());
+            tb = 0;
+            CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, C.rkey.as<unsigned long long>(),
+                                               C.rkey_sorted.as<unsigned long long>(), C.rperm_in.as<unsigned>(),
+                                               C.rperm.as<unsigned>(), (int)nrec, 0, ibits + vbits, st));
+            RET(ensure(C.cub_tmp, tb));
+            CK(cub::DeviceRadixSort::SortPairs(C.cub_tmp.p, tb, C.rkey.as<unsigned long long>(),
+                                               C.rkey_sorted.as<unsigned long long>(), C.rperm_in.as<unsigned>(),
+                                               C.rperm.as<unsigned>(), (int)nrec, 0, ibits + vbits, st));
+            GatherArgs ga = {};
+            ga.key = C.rkey_sorted.as<unsigned long long>();
+            ga.perm = C.rperm.as<unsigned>();
+            ga.mom = C.rmom.as<double>();
+            ga.nrec = (long long)nrec;
+            ga.nmom = nmom;
+            ga.ibits = ibits;
+            ga.vox = C.rvox.as<unsigned>();
+            ga.item = C.ritem.as<unsigned>();
+            ga.mom_sorted = C.rmom_sorted.as<double>();
+            CK(launch_gather_records(ga, st));
+            // voxel runs: (voxel, count) pairs, then their offsets
+            int* d_nruns = (int*)(C.run_cnt.as<char>() + (size_t)maxruns * 4);
+            tb = 0;
+            CK(cub::DeviceRunLengthEncode::Encode(nullptr, tb, C.rvox.as<unsigned>(), C.run_vox.as<unsigned>(),
+                                                  C.run_cnt.as<int>(), d_nruns, (int)nrec, st));
+            RET(ensure(C.cub_tmp, tb));
+            CK(cub::DeviceRunLengthEncode::Encode(C.cub_tmp.p, tb, C.rvox.as<unsigned>(), C.run_vox.as<unsigned>(),
+                                                  C.run_cnt.as<int>(), d_nruns, (int)nrec, st));
+            int nruns = 0;
+            CK(cudaMemcpyAsync(&nruns, d_nruns, sizeof(int), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            tb = 0;
+            CK(cub::DeviceScan::ExclusiveScan(nullptr, tb, C.run_cnt.as<int>(), C.run_off.as<long long>(), cub::Sum(),
+                                              (long long)0, nruns, st));
+            RET(ensure(C.cub_tmp, tb));
+            CK(cub::DeviceScan::ExclusiveScan(C.cub_tmp.p, tb, C.run_cnt.as<int>(), C.run_off.as<long long>(),
+                                              cub::Sum(), (long long)0, nruns, st));
+            ApplyArgs aa = {};
+            aa.run_vox = C.run_vox.as<unsigned>();
+            aa.run_cnt = C.run_cnt.as<int>();
+            aa.run_off = C.run_off.as<long long>();
+            aa.nruns = nruns;
+            aa.item = C.ritem.as<unsigned>();
+            aa.mom = C.rmom_sorted.as<double>();
+            aa.nmom = nmom;
+            aa.central = mixed;
+            aa.scale = ca.scale;
+            aa.it = it;
+            aa.item_base = 0;
+            aa.M = c.F[0]; aa.X = c.F[1]; aa.V = c.F[2]; aa.XX = c.F[3]; aa.XV = c.F[4]; aa.VV = c.F[5];
+            CK(launch_apply_records(aa, st));
+            klaunch += 3; // iota, gather, apply
+            CK(cudaEventRecord(C.ev[7], st));
+            CK(cudaEventSynchronize(C.ev[7]));
+            float t = 0.f;
+            CK(cudaEventElapsedTime(&t, C.ev[6], C.ev[7]));
+            ms_final += t;
+            break;
         }
     }
-    CK(cudaEventRecord(C.ev[6], st));
-    if (!det) {
-        FinalArgs f = {};
-        f.g = gd;
-        f.acc = acc;
-        f.M = c.F[0]; f.X = c.F[1]; f.V = c.F[2]; f.XX = c.F[3]; f.XV = c.F[4]; f.VV = c.F[5];
-        f.nvox = nvox;
-        CK(launch_finalize_merge(f, st));
-        klaunch++;
-    }
-    CK(cudaEventRecord(C.ev[7], st));
     unsigned long long h[S_WORDS];
     CK(cudaMemcpyAsync(h, sm, sizeof(h), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
@@ -529,19 +515,18 @@ int run_device(Call& c)
         s.elements_kept = (long long)h[S_TESS];
         s.tets = (long long)h[S_TESS + 1];
         s.tet_images = total;
-        s.fragments = (long long)h[S_CNT];
-        s.frag_verts = (long long)h[S_CNT + 1];
-        s.splits = (long long)h[S_CNT + 2];
-        s.passes = passes;
+        s.fragments = (long long)clip_counts[0];
+        s.frag_verts = (long long)clip_counts[1];
+        s.splits = (long long)clip_counts[2];
+        s.passes = 1;
         s.chunks = nchunks;
         s.ms_clip = ms_clip;
         s.ms_tess = ms_tess;
-        float t = 0.f;
-        CK(cudaEventElapsedTime(&t, C.ev[6], C.ev[7]));
-        s.ms_final = t;
+        s.ms_final = ms_final;
         s.clip_launches = launches;
         s.kernel_launches = klaunch + launches;
     }
+    (void)nvox;
     return PSIB_OK;
 }
 
@@ -580,8 +565,6 @@ int validate(const psib_grid* g, const psib_mesh* m, int mode, const psib_option
     }
     if (o && o->precision != PSIB_FP64 && o->precision != PSIB_MIXED)
         return fail(PSIB_ERR_ARG, "invalid precision %d", o->precision);
-    if (o && o->deterministic && o->precision == PSIB_MIXED)
-        return fail(PSIB_ERR_ARG, "deterministic mode runs in FP64 only");
     return PSIB_OK;
 }
 

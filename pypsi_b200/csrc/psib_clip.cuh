@@ -1,26 +1,46 @@
-// psib_clip.cuh -- the clip-and-deposit kernels (included by clip_fp64.cu and
-// clip_mixed.cu, which compile it with and without FMA contraction).
+// psib_clip.cuh -- the clip kernels (included by clip_fp64.cu and
+// clip_mixed.cu, which compile it without and with FMA contraction).
 //
 // One thread voxelizes one tet image (psi_voxelize_tet, src/geometry.c:60-188):
-// window clip and index box (src/geometry.c:806-843), bisection to voxels,
-// moments, projection with the tet's deformation matrices, deposit.
+// window clip and index box (src/geometry.c:806-843), depth-first bisection to
+// single voxels (:852-896), q-space moments of each fragment (:692-767).  Each
+// fragment becomes a record -- key (voxel, image) and up to ten moments --
+// and nothing is accumulated here.  The records are then sorted by key and
+// each voxel's run is applied to the grid fields in the reference's order by
+// one thread (apply kernels in tess.cu), which reproduces the reference's
+// online field update (src/geometry.c:164-186) exactly: no atomics, one clip
+// pass for every field order.
 //
-// The grid fields of the reference are mass-weighted means and covariances
-// built by a sequential online update (src/geometry.c:164-186), which atomics
-// cannot reproduce.  The kernels therefore accumulate sums that merge exactly:
-//   pass 1: W = sum w, SX = sum w (c_f - c_vox), SV = sum w v_f
-//   pass 2: XX = sum w (S_f + (c_f - mu)(c_f - mu)^T), likewise XV, VV,
-// with w = mass * m0 of a fragment, c_f its centroid, S_f its central second
-// moment and mu the voxel mean from pass 1.  Centring on the voxel mean keeps
-// the covariances free of cancellation; the finalize kernel merges them into
-// the existing fields with the same parallel-axis rule as the online update.
-// In record mode (deterministic, FP64) each fragment's raw q-moments are
-// written out instead, to be applied per voxel in the reference's order.
+// Records of the FP64 kernel hold the reference's raw moments m0..m9 about
+// q = 0.  Records of the FP32 kernel hold m0, the fragment's q-centroid and its
+// central q-space second moment (moments taken about a vertex of the fragment,
+// reduce_about), which keep FP32 vertex errors from being amplified; its
+// threads also store each image's mass-correction factor (exact FP64 volume of
+// the window-clipped tet over the sum of its FP32 fragment volumes).
+//
+// Each thread owns a contiguous region of a global scratch buffer for its
+// polyhedron slots: contiguous per-thread storage keeps every 32-byte sector a
+// thread touches full of its own data, where the compiler's local memory would
+// interleave threads word by word and waste most of each sector as soon as
+// threads index different slots.
 #pragma once
 #include "psib_device.cuh"
 #include "psib_kernels.h"
 
 namespace psib {
+
+// Per-thread scratch region: NS polyhedron slots, then (FP32 kernels) two
+// FP64 polyhedra for the window clip.  Both parts start on 16-byte boundaries.
+__host__ __device__ constexpr size_t round16(size_t b) { return (b + 15) & ~(size_t)15; }
+
+template <class R, int NS>
+__host__ __device__ constexpr size_t wclip_offset() { return round16(sizeof(Poly<R>) * NS); }
+
+template <class R, int NS>
+__host__ __device__ constexpr size_t region_bytes()
+{
+    return wclip_offset<R, NS>() + (sizeof(R) == 4 ? round16(2 * sizeof(Poly<double>)) : 0);
+}
 
 __device__ __forceinline__ void aabb4(const double (*p)[3], double (*rb)[3])
 {
@@ -35,76 +55,35 @@ __device__ __forceinline__ void aabb4(const double (*p)[3], double (*rb)[3])
         }
 }
 
-__device__ __forceinline__ void deposit(const ClipArgs& a, const TetFrame& F, double mass, const double* mom,
-                                        long long gi, const int* vox)
-{
-    const AccDev& A = a.acc;
-    const double w = mass * mom[0];
-    double cm[3], cv[3];
-    if (A.flags & (F_X | F_XX | F_XV)) centroid(mom, F.x0, F.DX, cm);
-    if (A.flags & (F_V | F_XV | F_VV)) centroid(mom, F.v0, F.DV, cv);
-    if (a.pass == 1) {
-        atomicAdd(&A.W[gi], w);
-        if (A.flags & F_X)
-            for (int i = 0; i < 3; ++i) {
-                const double c = a.g.w0[i] + a.g.d[i] * (vox[i] + 0.5);
-                atomicAdd(&A.SX[3 * gi + i], w * (cm[i] - c));
-            }
-        if (A.flags & F_V)
-            for (int i = 0; i < 3; ++i) atomicAdd(&A.SV[3 * gi + i], w * cv[i]);
-        return;
-    }
-    double dx[3] = {0, 0, 0}, dv[3] = {0, 0, 0};
-    if (A.flags & (F_XX | F_XV))
-        for (int i = 0; i < 3; ++i) dx[i] = cm[i] - A.MX[3 * gi + i];
-    if (A.flags & (F_XV | F_VV))
-        for (int i = 0; i < 3; ++i) dv[i] = cv[i] - A.MV[3 * gi + i];
-    double S[3][3];
-    if (A.flags & F_XX) {
-        second_moment(mom, F.x0, cm, F.DX, F.x0, cm, F.DX, F.x0, cm, F.x0, cm, S);
-        for (int i = 0; i < 3; ++i)
-            for (int j = 0; j < 3; ++j) atomicAdd(&A.XX[9 * gi + 3 * i + j], w * (S[i][j] + dx[i] * dx[j]));
-    }
-    if (A.flags & F_XV) {
-        second_moment(mom, F.x0, cm, F.DX, F.v0, cv, F.DV, F.x0, cm, F.v0, cv, S);
-        for (int i = 0; i < 3; ++i)
-            for (int j = 0; j < 3; ++j) atomicAdd(&A.XV[9 * gi + 3 * i + j], w * (S[i][j] + dx[i] * dv[j]));
-    }
-    if (A.flags & F_VV) {
-        second_moment(mom, F.v0, cv, F.DV, F.v0, cv, F.DV, F.v0, cv, F.v0, cv, S);
-        for (int i = 0; i < 3; ++i)
-            for (int j = 0; j < 3; ++j) atomicAdd(&A.VV[9 * gi + 3 * i + j], w * (S[i][j] + dv[i] * dv[j]));
-    }
-}
-
 // Per-thread counters, folded into the global ones once per thread.
 struct Tally {
     unsigned long long frags = 0, verts = 0, splits = 0;
 };
 
-// Voxelize item t.  S points to NS polyhedron slots owned by this thread.
-template <class R, int NS, bool RECORD>
-__device__ void clip_item(const ClipArgs& a, long long t, Poly<R>* S, unsigned& st, Tally& tally)
+__device__ __forceinline__ void write_record(const ClipArgs& a, long long gi, long long t, const double* mom,
+                                             unsigned& st)
 {
-    const long long cap = a.it.cap;
+    const unsigned long long r = atomicAdd(a.rec_n, 1ull);
+    if (r < a.rec_cap) {
+        a.rec_key[r] = ((unsigned long long)gi << a.rec_ibits) | (unsigned long long)(t - a.rec_item_base);
+        double* dst = a.rec_mom + r * a.rec_nmom;
+        for (int k = 0; k < a.rec_nmom; ++k) dst[k] = mom[k];
+    } else {
+        st |= ST_RECORDS;
+    }
+}
+
+// Voxelize item t.  S points to NS polyhedron slots owned by this thread,
+// WC to two FP64 polyhedra (FP32 kernel only).  CENTRAL: write centroid-form
+// records (always so in the FP32 kernel; the FP64 kernel does it when it
+// serves the mixed-precision mode).
+template <class R, int NS, bool CENTRAL>
+__device__ void clip_item(const ClipArgs& a, long long t, Poly<R>* S, Poly<double>* WC, unsigned& st, Tally& tally)
+{
+    const double* fr = a.it.frame + t * FRAME;
     double p[4][3];
     for (int v = 0; v < 4; ++v)
-        for (int i = 0; i < 3; ++i) p[v][i] = a.it.p[(3 * v + i) * cap + t];
-    const double mass = a.it.mass[t];
-    TetFrame F;
-    for (int i = 0; i < 3; ++i) {
-        F.x0[i] = p[0][i];
-        for (int j = 0; j < 3; ++j) F.DX[i][j] = p[j + 1][i] - p[0][i];
-    }
-    if (a.acc.flags & (F_V | F_XV | F_VV)) {
-        double u[4][3];
-        for (int v = 0; v < 4; ++v)
-            for (int i = 0; i < 3; ++i) u[v][i] = a.it.u[(3 * v + i) * cap + t];
-        for (int i = 0; i < 3; ++i) {
-            F.v0[i] = u[0][i];
-            for (int j = 0; j < 3; ++j) F.DV[i][j] = u[j + 1][i] - u[0][i];
-        }
-    }
+        for (int i = 0; i < 3; ++i) p[v][i] = fr[3 * v + i];
     double rb[2][3];
     aabb4(p, rb);
 
@@ -138,55 +117,55 @@ __device__ void clip_item(const ClipArgs& a, long long t, Poly<R>* S, unsigned& 
     }
 #define PSIB_FREE(i) (freem |= 1ull << (i))
 
-    // Recentring for the FP32 kernel: coordinates relative to the index box's
-    // lower corner, so FP32 keeps its precision at grid-cell scale.
+    // Recentring for the FP32 kernel: coordinates relative to the tet's first
+    // vertex, so FP32 keeps its precision at the scale of the tet (which can be
+    // far smaller than a voxel once refined).
     double org[3];
-    for (int i = 0; i < 3; ++i) org[i] = (sizeof(R) == 8) ? 0.0 : a.g.w0[i] + a.g.d[i] * lo[i];
+    for (int i = 0; i < 3; ++i) org[i] = (sizeof(R) == 8) ? 0.0 : p[0][i];
 
     int c;
     PSIB_ALLOC(c);
     R s[MAXV];
-    // q-volume the fragments must add up to: 1 for a tet inside the window.
-    double target = 1.0, msum = 0.0, mbest = -1.0;
-    long long gbest = -1;
+    double target = 1.0, vsum = 0.0; // exact and FP32 q-volume of the image (FP32 kernel)
     if constexpr (sizeof(R) == 4) {
         if (npl > 0) {
             // The FP32 kernel clips against the window in FP64, so that a tet
             // split across periodic images still deposits exactly its mass.
-            Poly<double> W[2];
-            init_tet(W[0], p);
+            Poly<double>* W[2] = {&WC[0], &WC[1]};
+            init_tet(*W[0], p);
             double sd[MAXV];
             int cw = 0;
-            for (int pl = 0; pl < npl && W[cw].nv > 0; ++pl) {
+            for (int pl = 0; pl < npl && W[cw]->nv > 0; ++pl) {
                 const int ax = pax[pl];
                 double smin = 1.0e30, smax = -1.0e30;
                 uint32_t um = 0;
-                for (int v = 0; v < W[cw].nv; ++v) {
+                for (int v = 0; v < W[cw]->nv; ++v) {
                     double t0 = pdd[pl];
-                    for (int i = 0; i < 3; ++i) t0 += W[cw].x[v][i] * (i == ax ? (double)psg[pl] : 0.0);
+                    for (int i = 0; i < 3; ++i) t0 += W[cw]->x[v][i] * (i == ax ? (double)psg[pl] : 0.0);
                     sd[v] = t0;
                     if (t0 < smin) smin = t0;
                     if (t0 > smax) smax = t0;
                     if (t0 < 0.0) um |= 1u << v;
                 }
                 if (smin >= 0.0) continue;
-                if (smax <= 0.0) { W[cw].nv = 0; break; }
-                const unsigned e = cut_poly<double, false>(W[cw], sd, um, W[1 - cw], W[1 - cw]);
+                if (smax <= 0.0) { W[cw]->nv = 0; break; }
+                const unsigned e = cut_poly<double, false>(*W[cw], sd, um, *W[1 - cw], *W[1 - cw]);
                 if (e) { st |= e; return; }
                 cw = 1 - cw;
             }
-            if (W[cw].nv == 0) return;
+            if (W[cw]->nv == 0) { a.scale[t] = 1.0; return; }
             double m0[10];
-            const unsigned e = reduce_poly(W[cw], m0, 0);
+            const unsigned e = reduce_poly(*W[cw], m0, 0);
             if (e) { st |= e; return; }
             target = m0[0];
             Poly<R>& P = S[c];
-            P.nv = W[cw].nv;
+            const Poly<double>& Q = *W[cw];
+            P.nv = Q.nv;
             for (int v = 0; v < P.nv; ++v) {
-                P.nb[v] = W[cw].nb[v];
+                P.nb[v] = Q.nb[v];
                 for (int i = 0; i < 3; ++i) {
-                    P.x[v][i] = (R)(W[cw].x[v][i] - org[i]);
-                    P.q[v][i] = (R)W[cw].q[v][i];
+                    P.x[v][i] = (R)(Q.x[v][i] - org[i]);
+                    P.q[v][i] = (R)Q.q[v][i];
                 }
             }
         }
@@ -203,7 +182,7 @@ __device__ void clip_item(const ClipArgs& a, long long t, Poly<R>* S, unsigned& 
         Poly<R>& P = S[c];
         const int ax = pax[pl];
         const R sg = (R)psg[pl];
-        const R dd = (sizeof(R) == 8) ? (R)pdd[pl] : (R)(pdd[pl] + psg[pl] * org[ax]);
+        const R dd = (R)pdd[pl];
         R smin = (R)1.0e30, smax = (R)-1.0e30;
         uint32_t um = 0;
         for (int v = 0; v < P.nv; ++v) {
@@ -238,8 +217,11 @@ __device__ void clip_item(const ClipArgs& a, long long t, Poly<R>* S, unsigned& 
                 if (sz > dmax) { dmax = sz; ax = i; }
             }
             if (dmax <= 1) {
-                // a single voxel: reduce and deposit (src/geometry.c:873-884)
-                const unsigned e = reduce_poly(P, mom, order);
+                // a single voxel (src/geometry.c:873-884)
+                double o[3] = {0.0, 0.0, 0.0};
+                if constexpr (CENTRAL)
+                    for (int i = 0; i < 3; ++i) o[i] = (double)P.q[0][i];
+                const unsigned e = CENTRAL ? reduce_about(P, o, mom, order) : reduce_poly(P, mom, order);
                 if (e) { st |= e; return; }
                 if (mom[0] > 0.0) {
                     if (P.lo[0] >= a.g.n[0] || P.lo[1] >= a.g.n[1] || P.lo[2] >= a.g.n[2]) {
@@ -248,20 +230,24 @@ __device__ void clip_item(const ClipArgs& a, long long t, Poly<R>* S, unsigned& 
                         const long long gi = ((long long)a.g.n[1] * P.lo[0] + P.lo[1]) * a.g.n[2] + P.lo[2];
                         tally.frags++;
                         tally.verts += P.nv;
-                        if constexpr (sizeof(R) == 4) {
-                            msum += mom[0];
-                            if (mom[0] > mbest) { mbest = mom[0]; gbest = gi; }
-                        }
-                        if (RECORD) {
-                            const unsigned long long r = atomicAdd(a.rec_n, 1ull);
-                            if (r < a.rec_cap) {
-                                a.rec_key[r] = ((unsigned long long)gi << 32) | (unsigned long long)(t - a.rec_item_base);
-                                for (int k = 0; k < a.rec_nmom; ++k) a.rec_mom[r * a.rec_nmom + k] = mom[k];
-                            } else {
-                                st |= ST_RECORDS;
-                            }
+                        if constexpr (CENTRAL) {
+                            // m0, q-centroid, central q second moment (xx xy xz yy yz zz)
+                            vsum += mom[0];
+                            double rec[10];
+                            const double m0 = mom[0];
+                            double u[3];
+                            for (int i = 0; i < 3; ++i) u[i] = mom[1 + i] / m0;
+                            rec[0] = m0;
+                            for (int i = 0; i < 3; ++i) rec[1 + i] = o[i] + u[i];
+                            rec[4] = mom[4] / m0 - u[0] * u[0];
+                            rec[5] = mom[5] / m0 - u[0] * u[1];
+                            rec[6] = mom[6] / m0 - u[0] * u[2];
+                            rec[7] = mom[7] / m0 - u[1] * u[1];
+                            rec[8] = mom[8] / m0 - u[1] * u[2];
+                            rec[9] = mom[9] / m0 - u[2] * u[2];
+                            write_record(a, gi, t, rec, st);
                         } else {
-                            deposit(a, F, mass, mom, gi, P.lo);
+                            write_record(a, gi, t, mom, st);
                         }
                     }
                 }
@@ -308,19 +294,25 @@ __device__ void clip_item(const ClipArgs& a, long long t, Poly<R>* S, unsigned& 
         c = stk[--top];
     }
     if constexpr (sizeof(R) == 4) {
-        // FP32 fragments miss the exact q-volume by O(1e-7); book the residual
-        // on the largest fragment's voxel so the tet deposits exactly its mass.
-        if (!RECORD && a.pass == 1 && gbest >= 0) atomicAdd(&a.acc.W[gbest], mass * (target - msum));
+        // FP32 fragments miss the exact q-volume by O(1e-7): the apply kernel
+        // scales this image's fragment masses by target / vsum.
+        a.scale[t] = vsum > 0.0 ? target / vsum : 1.0;
+    } else if constexpr (CENTRAL) {
+        a.scale[t] = 1.0;
     }
 #undef PSIB_ALLOC
 #undef PSIB_FREE
 }
 
-// Persistent kernel: warps take 32 consecutive queue entries at a time.
-template <class R, int NS, bool RECORD, bool SCRATCH>
-__device__ __forceinline__ void clip_loop(const ClipArgs& a, Poly<R>* S)
+// Persistent kernel body: warps take 32 consecutive queue entries at a time.
+template <class R, int NS, bool CENTRAL>
+__device__ __forceinline__ void clip_loop(const ClipArgs& a)
 {
     const int lane = threadIdx.x & 31;
+    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    char* region = (char*)a.scratch + tid * region_bytes<R, NS>();
+    Poly<R>* S = (Poly<R>*)region;
+    Poly<double>* WC = (Poly<double>*)(region + wclip_offset<R, NS>());
     unsigned st = 0;
     Tally tally;
     for (;;) {
@@ -331,7 +323,7 @@ __device__ __forceinline__ void clip_loop(const ClipArgs& a, Poly<R>* S)
         const long long i = (long long)base + lane;
         if (i < a.n) {
             const long long t = a.order ? (long long)a.order[a.order_base + i] : a.order_base + i;
-            clip_item<R, NS, RECORD>(a, t, S, st, tally);
+            clip_item<R, NS, CENTRAL>(a, t, S, WC, st, tally);
         }
     }
     if (st) atomicOr(a.status, st);

@@ -28,6 +28,7 @@ constexpr int MAXV = 20;       // vertices of one polyhedron; <= 10 faces bound 
 constexpr int DMAX_MAIN = 8;   // bisection depth served by the main clip kernel
 constexpr int NS_MAIN = DMAX_MAIN + 3;
 constexpr int DMAX_BIG = 40;   // deeper trees go to the big-tet kernel
+constexpr int SPAN_MAX = 16;   // longer index boxes also go to it (FP64 in both precisions)
 constexpr int NS_BIG = DMAX_BIG + 3;
 constexpr int WALK_CAP = 64;   // a face has < MAXV edges; longer walks mean a broken graph
 
@@ -152,8 +153,8 @@ __device__ __forceinline__ unsigned cut_poly(const Poly<R>& in, const R* s, uint
 }
 
 // The tet as a vertex graph with q = (0, e_x, e_y, e_z) (src/geometry.c:769-804).
-template <class R>
-__device__ __forceinline__ void init_tet(Poly<R>& P, const R (*x)[3])
+template <class PT, class T>
+__device__ __forceinline__ void init_tet(PT& P, const T (*x)[3])
 {
     P.nb[0] = 1u | (3u << 8) | (2u << 16);
     P.nb[1] = 2u | (3u << 8) | (0u << 16);
@@ -162,7 +163,7 @@ __device__ __forceinline__ void init_tet(Poly<R>& P, const R (*x)[3])
     for (int v = 0; v < 4; ++v)
         for (int i = 0; i < 3; ++i) {
             P.x[v][i] = x[v][i];
-            P.q[v][i] = (v == i + 1) ? R(1) : R(0);
+            P.q[v][i] = (v == i + 1) ? 1 : 0;
         }
     P.nv = 4;
 }
@@ -170,16 +171,17 @@ __device__ __forceinline__ void init_tet(Poly<R>& P, const R (*x)[3])
 // Fragment moments in q-space: order 0 (1 value), 1 (4) or 2 (10), by fan
 // triangles of every face, accumulated in the reference's order
 // (src/geometry.c:692-767).  Always FP64.
-template <class R>
-__device__ __forceinline__ unsigned reduce_poly(const Poly<R>& P, double* mom, int order)
+template <class PT>
+__device__ __forceinline__ unsigned reduce_poly(const PT& P, double* mom, int order)
 {
     for (int i = 0; i < 10; ++i) mom[i] = 0.0;
-    uint64_t done = 0;
+    uint64_t done[2] = {0ull, 0ull};
     for (int vs = 0; vs < P.nv; ++vs)
         for (int ks = 0; ks < 3; ++ks) {
-            if ((done >> (3 * vs + ks)) & 1ull) continue;
+            const int b0 = 3 * vs + ks;
+            if ((done[b0 >> 6] >> (b0 & 63)) & 1ull) continue;
             int vc = vs, kn = ks;
-            done |= 1ull << (3 * vc + kn);
+            done[b0 >> 6] |= 1ull << (b0 & 63);
             int vn = nbget(P.nb[vc], kn);
             if (vn >= P.nv) return ST_GRAPH;
             const double q0x = (double)P.q[vc][0], q0y = (double)P.q[vc][1], q0z = (double)P.q[vc][2];
@@ -187,7 +189,8 @@ __device__ __forceinline__ unsigned reduce_poly(const Poly<R>& P, double* mom, i
             int k = (nbget(w, 0) == vc) ? 0 : (nbget(w, 1) == vc) ? 1 : (nbget(w, 2) == vc) ? 2 : 3;
             vc = vn;
             kn = (k + 1) % 3;
-            done |= 1ull << (3 * vc + kn);
+            int b = 3 * vc + kn;
+            done[b >> 6] |= 1ull << (b & 63);
             vn = nbget(P.nb[vc], kn);
             int steps = 0;
             while (vn != vs) {
@@ -215,7 +218,8 @@ __device__ __forceinline__ unsigned reduce_poly(const Poly<R>& P, double* mom, i
                 vc = vn;
                 kn = (k + 1) % 3;
                 if (k == 3) return ST_GRAPH;
-                done |= 1ull << (3 * vc + kn);
+                b = 3 * vc + kn;
+                done[b >> 6] |= 1ull << (b & 63);
                 vn = nbget(P.nb[vc], kn);
             }
         }
@@ -259,6 +263,165 @@ __device__ __forceinline__ void second_moment(const double* mom, const double* o
                 for (int b = 0; b < 3; ++b) t += Da[i][a] * Db[j][b] * mom[qi[a][b]];
             S[i][j] = t / mom[0];
         }
+}
+
+} // namespace psib
+
+namespace psib {
+
+// ---- one-sided cuts for the per-voxel path kernels ----
+//
+// A lane follows the bisection path from the tet's index box down to its own
+// voxel and keeps only the side of each split that contains that voxel.  The
+// kept half of a split is the same polyhedron, vertex for vertex, that the
+// reference's two-sided split produces for that child, so the fragment at the
+// end of the path equals the reference's bit for bit.
+
+constexpr int CAPV = 32; // vertex buffer of an in-place cut: kept vertices + cut vertices
+
+template <class R>
+struct Buf {
+    R x[CAPV][3];
+    R q[CAPV][3];
+    uint32_t nb[CAPV];
+    int nv;
+};
+
+__device__ __forceinline__ uint32_t low_mask(int n) { return n >= 32 ? 0xFFFFFFFFu : ((1u << n) - 1u); }
+
+// Keep the lower side (s >= 0, keep_upper == false) or the upper side (s < 0)
+// of a cut, in place.  The result lists the kept old vertices in order, then
+// the cut vertices in the reference's creation order (lower vertex ascending,
+// link ascending), exactly like the corresponding output of the two-sided
+// split (src/geometry.c:593-690) or of the window clip (:436-500).
+template <class R>
+__device__ __forceinline__ unsigned half_cut(Buf<R>& P, const R* s, uint32_t umask, bool keep_upper)
+{
+    const int n = P.nv;
+    const uint32_t lmask = low_mask(n) & ~umask;
+    const uint32_t kmask = keep_upper ? umask : lmask;
+    int nv = n;
+    for (int vc = 0; vc < n; ++vc) {
+        if (!((lmask >> vc) & 1u)) continue;
+        for (int np = 0; np < 3; ++np) {
+            const int vn = nbget(P.nb[vc], np);
+            if (vn >= n) return ST_GRAPH; // lower-vertex links are only rewritten after they are read
+            if (!((umask >> vn) & 1u)) continue;
+            if (nv >= CAPV) return ST_OVERFLOW;
+            const R sc = s[vc], sn = s[vn];
+            const R iw = R(1) / (sc - sn);
+            for (int i = 0; i < 3; ++i) {
+                P.x[nv][i] = iw * (P.x[vn][i] * sc - P.x[vc][i] * sn);
+                P.q[nv][i] = iw * (P.q[vn][i] * sc - P.q[vc][i] * sn);
+            }
+            if (!keep_upper) {
+                P.nb[nv] = 0xFFFF00u | (uint32_t)vc;
+                P.nb[vc] = nbset(P.nb[vc], np, nv);
+            } else {
+                P.nb[nv] = 0xFFFF00u | (uint32_t)vn;
+                const uint32_t wn = P.nb[vn];
+                const int kb = (nbget(wn, 0) == vc) ? 0 : (nbget(wn, 1) == vc) ? 1 : (nbget(wn, 2) == vc) ? 2 : 3;
+                if (kb == 3) return ST_GRAPH;
+                P.nb[vn] = nbset(wn, kb, nv);
+            }
+            ++nv;
+        }
+    }
+    // close the cut face, walking the kept side (src/geometry.c:459-482)
+    for (int vs = n; vs < nv; ++vs) {
+        int vc = vs, vn = nbget(P.nb[vs], 0);
+        int steps = 0;
+        do {
+            if (vn >= nv) return ST_GRAPH;
+            const uint32_t w = P.nb[vn];
+            const int k = (nbget(w, 0) == vc) ? 0 : (nbget(w, 1) == vc) ? 1 : (nbget(w, 2) == vc) ? 2 : 3;
+            if (k == 3 || ++steps > WALK_CAP) return ST_GRAPH;
+            vc = vn;
+            vn = nbget(P.nb[vc], (k + 1) % 3);
+        } while (vc < n);
+        P.nb[vs] = nbset(P.nb[vs], 2, vc);
+        P.nb[vc] = nbset(P.nb[vc], 1, vs);
+    }
+    // compact: kept old vertices, then the cut vertices, with links renumbered
+    const int nk = __popc(kmask);
+    for (int v = 0; v < nv; ++v) {
+        const bool keep = v >= n || ((kmask >> v) & 1u);
+        if (!keep) continue;
+        const int dst = v < n ? rank_in(kmask, v) : nk + (v - n);
+        uint32_t w = P.nb[v], ow = 0;
+        for (int k = 0; k < 3; ++k) {
+            const int t = nbget(w, k);
+            const int tt = t < n ? rank_in(kmask, t) : nk + (t - n);
+            ow |= (uint32_t)tt << (8 * k);
+        }
+        for (int i = 0; i < 3; ++i) {
+            P.x[dst][i] = P.x[v][i];
+            P.q[dst][i] = P.q[v][i];
+        }
+        P.nb[dst] = ow;
+    }
+    P.nv = nk + (nv - n);
+    return 0;
+}
+
+// Moments of a polyhedron about the q-space point o (order 0, 1 or 2): the
+// same fan triangles as reduce_poly, with every vertex taken relative to o.
+// With o on the polyhedron the cone volumes do not cancel and the first and
+// second moments are fragment-sized, so central moments follow without
+// cancellation.  Used by the mixed-precision kernel.
+template <class PT>
+__device__ __forceinline__ unsigned reduce_about(const PT& P, const double* o, double* mom, int order)
+{
+    for (int i = 0; i < 10; ++i) mom[i] = 0.0;
+    uint64_t done[2] = {0ull, 0ull};
+    for (int vs = 0; vs < P.nv; ++vs)
+        for (int ks = 0; ks < 3; ++ks) {
+            const int b0 = 3 * vs + ks;
+            if ((done[b0 >> 6] >> (b0 & 63)) & 1ull) continue;
+            int vc = vs, kn = ks;
+            done[b0 >> 6] |= 1ull << (b0 & 63);
+            int vn = nbget(P.nb[vc], kn);
+            if (vn >= P.nv) return ST_GRAPH;
+            const double q0x = (double)P.q[vc][0] - o[0], q0y = (double)P.q[vc][1] - o[1], q0z = (double)P.q[vc][2] - o[2];
+            uint32_t w = P.nb[vn];
+            int k = (nbget(w, 0) == vc) ? 0 : (nbget(w, 1) == vc) ? 1 : (nbget(w, 2) == vc) ? 2 : 3;
+            vc = vn;
+            kn = (k + 1) % 3;
+            int b = 3 * vc + kn;
+            done[b >> 6] |= 1ull << (b & 63);
+            vn = nbget(P.nb[vc], kn);
+            int steps = 0;
+            while (vn != vs) {
+                if (++steps > WALK_CAP || vn >= P.nv || k == 3) return ST_GRAPH;
+                const double q1x = (double)P.q[vn][0] - o[0], q1y = (double)P.q[vn][1] - o[1], q1z = (double)P.q[vn][2] - o[2];
+                const double q2x = (double)P.q[vc][0] - o[0], q2y = (double)P.q[vc][1] - o[1], q2z = (double)P.q[vc][2] - o[2];
+                const double m = (-q2x * q1y * q0z + q1x * q2y * q0z + q2x * q0y * q1z
+                                  - q0x * q2y * q1z - q1x * q0y * q2z + q0x * q1y * q2z);
+                mom[0] += m;
+                if (order > 0) {
+                    mom[1] += 0.25 * m * (q0x + q1x + q2x);
+                    mom[2] += 0.25 * m * (q0y + q1y + q2y);
+                    mom[3] += 0.25 * m * (q0z + q1z + q2z);
+                }
+                if (order > 1) {
+                    mom[4] += 0.1 * m * (q0x * q0x + q1x * q1x + q2x * q2x + q1x * q2x + q0x * (q1x + q2x));
+                    mom[5] += 0.05 * m * (q2x * q0y + q2x * q1y + 2 * q2x * q2y + q0x * (2 * q0y + q1y + q2y) + q1x * (q0y + 2 * q1y + q2y));
+                    mom[6] += 0.05 * m * (q2x * q0z + q2x * q1z + 2 * q2x * q2z + q0x * (2 * q0z + q1z + q2z) + q1x * (q0z + 2 * q1z + q2z));
+                    mom[7] += 0.1 * m * (q0y * q0y + q1y * q1y + q2y * q2y + q1y * q2y + q0y * (q1y + q2y));
+                    mom[8] += 0.05 * m * (q2y * q0z + q2y * q1z + 2 * q2y * q2z + q0y * (2 * q0z + q1z + q2z) + q1y * (q0z + 2 * q1z + q2z));
+                    mom[9] += 0.1 * m * (q0z * q0z + q1z * q1z + q2z * q2z + q1z * q2z + q0z * (q1z + q2z));
+                }
+                w = P.nb[vn];
+                k = (nbget(w, 0) == vc) ? 0 : (nbget(w, 1) == vc) ? 1 : (nbget(w, 2) == vc) ? 2 : 3;
+                if (k == 3) return ST_GRAPH;
+                vc = vn;
+                kn = (k + 1) % 3;
+                b = 3 * vc + kn;
+                done[b >> 6] |= 1ull << (b & 63);
+                vn = nbget(P.nb[vc], kn);
+            }
+        }
+    return 0;
 }
 
 } // namespace psib

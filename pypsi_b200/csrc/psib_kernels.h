@@ -10,28 +10,26 @@ namespace psib {
 // field presence flags
 enum : unsigned { F_X = 1u, F_V = 2u, F_XX = 4u, F_XV = 8u, F_VV = 16u };
 
-// Tet images ("items"), structure of arrays with capacity `cap`:
-// vertex v, axis i of item t at p[(3v+i)*cap + t].  Items are written in the
-// reference's visiting order (element, refinement path, tet, periodic image).
+// Tet images ("items").  Each image's frame is one contiguous record of
+// FRAME doubles -- the 4 vertex positions (vertex-major, periodic image
+// applied), the 4 vertex velocities, the tet mass and one pad -- because the
+// clip and apply kernels visit images in footprint and voxel order, not in
+// index order, and a contiguous frame costs them 7 sectors instead of 25.
+// Images are numbered in the reference's visiting order (element,
+// refinement path, tet, periodic image).
+constexpr int FRAME = 26;
+constexpr int FR_U = 12, FR_MASS = 24;
 struct ItemArrays {
-    double *p;       // 12 x cap positions (periodic image applied)
-    double *u;       // 12 x cap velocities
-    double *mass;    // cap
+    double *frame;   // FRAME x cap
     int *elem;       // cap: element index
-    int *pid;        // 4 x cap: particle ids of the 4 vertices (unrefined meshes), else unused
-    uint16_t *key;   // cap: ordering key (0 = largest footprint first; 0xFFFF = deep tree)
+    int *pid;        // 4 x cap: particle ids of the 4 vertices (unrefined meshes), else -1
+    uint16_t *key;   // cap: 0xFFFF for images the deep-tree kernel takes, else larger boxes first
     long long cap;
 };
 
 struct GridDev {
     int n[3];
     double w0[3], w1[3], d[3];
-};
-
-struct AccDev {
-    double *W, *SX, *SV, *XX, *XV, *VV; // sums, see psib_clip.cuh
-    const double *MX, *MV;              // pass-1 voxel means (pass 2)
-    unsigned flags;                     // F_* of the requested fields
 };
 
 struct ClipArgs {
@@ -41,19 +39,19 @@ struct ClipArgs {
     long long n;             // queue entries of this launch
     unsigned long long *head;
     GridDev g;
-    AccDev acc;
-    int pass;                // 1 or 2
     int mom_order;           // polynomial order of the moments (0, 1, 2)
     unsigned *status;
     unsigned long long *counters; // fragments, fragment vertices, splits
-    // fragment records (deterministic mode)
-    unsigned long long *rec_key;
-    double *rec_mom;
+    // fragment records
+    unsigned long long *rec_key; // voxel << rec_ibits | item
+    double *rec_mom;             // rec_nmom doubles per record
     unsigned long long *rec_n;
     unsigned long long rec_cap;
     int rec_nmom;
     long long rec_item_base;
-    void *scratch;           // big-tet kernel: NS_BIG slots per thread
+    int rec_ibits;           // bits of the item field of a record key
+    double *scale;           // FP32 kernel: per item, exact / FP32 q-volume
+    void *scratch;           // per-thread scratch regions (grid x block of them)
 };
 
 struct MeshDev {
@@ -82,30 +80,44 @@ struct TessArgs {
 };
 
 // ---- launchers (return cudaError_t of the launch) ----
-cudaError_t launch_clip_fp64(const ClipArgs &a, bool big, bool record, int grid, int block, cudaStream_t s);
+// big: the kernel for images whose bisection tree is deeper than DMAX_MAIN
+cudaError_t launch_clip_fp64(const ClipArgs &a, bool big, int grid, int block, cudaStream_t s);
+// mixed precision: FP32 main kernel; big -> the FP64 deep-tree kernel writing centroid-form records
 cudaError_t launch_clip_mixed(const ClipArgs &a, bool big, int grid, int block, cudaStream_t s);
-size_t scratch_bytes_fp64_big();
-size_t scratch_bytes_mixed_big();
+// bytes of one thread's scratch region
+size_t scratch_bytes_fp64(bool big);
+size_t scratch_bytes_mixed(bool big);
+// resident blocks per SM of a clip kernel at this block size
+int clip_blocks_per_sm_fp64(bool big, int block);
+int clip_blocks_per_sm_mixed(bool big, int block);
 
 cudaError_t launch_tess_count(const TessArgs &a, cudaStream_t s);
 cudaError_t launch_tess_emit(const TessArgs &a, cudaStream_t s);
 
-struct FinalArgs {
-    GridDev g;
-    AccDev acc;
-    double *M, *X, *V, *XX, *XV, *VV; // the grid fields (reference layout)
-    double *MX, *MV;                  // pass-1 means (written by finalize_means)
-    long long nvox;
-};
-cudaError_t launch_finalize_means(const FinalArgs &f, cudaStream_t s);
-cudaError_t launch_finalize_merge(const FinalArgs &f, cudaStream_t s);
-
-struct ApplyArgs {
-    const unsigned long long *key; // sorted fragment keys (voxel << 32 | item)
-    const double *mom;             // moments, rec_nmom per record, in sorted order
+// Sorted fragment records gathered into key order: voxel, item and moments.
+struct GatherArgs {
+    const unsigned long long *key; // sorted keys
     const unsigned *perm;          // sorted position -> record
+    const double *mom;             // record moments, record order
     long long nrec;
+    int nmom, ibits;
+    unsigned *vox;                 // out: voxel of each sorted record
+    unsigned *item;                // out: item of each sorted record
+    double *mom_sorted;            // out: moments in key order
+};
+cudaError_t launch_gather_records(const GatherArgs &a, cudaStream_t s);
+
+// One thread per voxel run of the sorted records.
+struct ApplyArgs {
+    const unsigned *run_vox;       // voxel of each run
+    const int *run_cnt;            // records of each run
+    const long long *run_off;      // first sorted record of each run
+    long long nruns;
+    const unsigned *item;          // item of each sorted record
+    const double *mom;             // moments of each sorted record
     int nmom;
+    int central;                   // records hold m0, q-centroid, central second moment
+    const double *scale;           // per item mass correction (central records)
     ItemArrays it;
     long long item_base;
     double *M, *X, *V, *XX, *XV, *VV;

@@ -137,11 +137,13 @@ __device__ unsigned tet_images(const double (*p)[3], const MeshDev& m, const Gri
 }
 
 // Ordering key of an image from its voxel index box (src/geometry.c:838-841):
-// 0xFFFF for trees deeper than the main clip kernel serves, otherwise larger
-// boxes first.
+// 0xFFFF for images the deep-tree kernel takes -- bisection trees deeper than
+// the main kernel serves (DMAX_MAIN), or boxes longer than SPAN_MAX voxels on
+// an axis, where FP32 coordinates would lose too much precision inside a voxel
+// -- otherwise larger boxes first.
 __device__ uint16_t footprint_key(const double (*rb)[3], const GridDev& g)
 {
-    int depth = 0;
+    int depth = 0, span = 0;
     long long vol = 1;
     for (int i = 0; i < 3; ++i) {
         double cmin = rb[0][i], cmax = rb[1][i];
@@ -153,9 +155,10 @@ __device__ uint16_t footprint_key(const double (*rb)[3], const GridDev& g)
         if (hi > g.n[i]) hi = g.n[i];
         const int sz = hi - lo;
         if (sz > 1) depth += 32 - __clz(sz - 1);
+        if (sz > span) span = sz;
         if (vol < 0xFFFF) vol *= (sz > 1 ? sz : 1);
     }
-    if (depth > DMAX_MAIN) return 0xFFFF;
+    if (depth > DMAX_MAIN || span > SPAN_MAX) return 0xFFFF;
     return (uint16_t)(0xFFFE - (vol < 0xFFFE ? vol : 0xFFFE));
 }
 
@@ -176,19 +179,21 @@ struct Emitter {
                 const long long t = pos++;
                 const long long cap = a.it.cap;
                 double q[4][3], rq[2][3];
+                double* fr = a.it.frame + t * FRAME;
                 for (int v = 0; v < 4; ++v)
                     for (int i = 0; i < 3; ++i) {
                         const double sh = (a.m.box1[i] - a.m.box0[i]) * (1 & (s >> i));
                         q[v][i] = s ? p[v][i] + sh : p[v][i];
-                        a.it.p[(3 * v + i) * cap + t] = q[v][i];
-                        a.it.u[(3 * v + i) * cap + t] = u[v][i];
+                        fr[3 * v + i] = q[v][i];
+                        fr[FR_U + 3 * v + i] = u[v][i];
                     }
                 for (int i = 0; i < 3; ++i) {
                     const double sh = (a.m.box1[i] - a.m.box0[i]) * (1 & (s >> i));
                     rq[0][i] = s ? rb[0][i] + sh : rb[0][i];
                     rq[1][i] = s ? rb[1][i] + sh : rb[1][i];
                 }
-                a.it.mass[t] = mass;
+                fr[FR_MASS] = mass;
+                fr[FR_MASS + 1] = 0.0;
                 a.it.elem[t] = (int)e;
                 for (int v = 0; v < 4; ++v) a.it.pid[v * cap + t] = pid ? pid[v] : -1;
                 a.it.key[t] = footprint_key(rq, a.g);
@@ -349,151 +354,147 @@ cudaError_t launch_tess_emit(const TessArgs& a, cudaStream_t s)
     return cudaGetLastError();
 }
 
-// ---- finalisation ----
+// ---- fragment records applied to the fields, voxel by voxel ----
 
-__global__ void k_finalize_means(FinalArgs f)
+// Physical moments of one FP32-kernel fragment from its record (m0, q-centroid,
+// central q second moment): centroid c = x0 + D cq, central moment D C D^T.
+// The x-v moment is brought to the reference's pairing of its cross terms
+// (src/geometry.c:137-146), which equals cov_xv + 2 a b^T - a a^T - b b^T with
+// a = x0 - c_x and b = v0 - c_v.
+__device__ void mixed_fragment(const double* rec, const double* p0, const double (*DX)[3], const double* v0,
+                               const double (*DV)[3], bool x, bool v, bool xx, bool xv, bool vv, double* cm,
+                               double* cv, double (*sxx)[3], double (*sxv)[3], double (*svv)[3])
 {
-    const long long gi = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (gi >= f.nvox) return;
-    const double W = f.acc.W[gi];
-    const int vz = (int)(gi % f.g.n[2]), vy = (int)((gi / f.g.n[2]) % f.g.n[1]), vx = (int)(gi / ((long long)f.g.n[1] * f.g.n[2]));
-    const int vox[3] = {vx, vy, vz};
-    for (int i = 0; i < 3; ++i) {
-        if (f.MX) f.MX[3 * gi + i] = W > 0.0 ? f.g.w0[i] + f.g.d[i] * (vox[i] + 0.5) + f.acc.SX[3 * gi + i] / W : 0.0;
-        if (f.MV) f.MV[3 * gi + i] = W > 0.0 ? f.acc.SV[3 * gi + i] / W : 0.0;
-    }
-}
-
-// Merge the new deposit (mass W, means, covariances) into the existing fields
-// with the parallel-axis rule of the reference's online update
-// (src/geometry.c:164-186).
-__global__ void k_finalize_merge(FinalArgs f)
-{
-    const long long gi = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (gi >= f.nvox) return;
-    const double W = f.acc.W[gi];
-    if (W == 0.0) return;
-    const unsigned fl = f.acc.flags;
-    const int vz = (int)(gi % f.g.n[2]), vy = (int)((gi / f.g.n[2]) % f.g.n[1]), vx = (int)(gi / ((long long)f.g.n[1] * f.g.n[2]));
-    const int vox[3] = {vx, vy, vz};
-    double mx[3], mv[3];
-    for (int i = 0; i < 3; ++i) {
-        mx[i] = (fl & F_X) ? f.g.w0[i] + f.g.d[i] * (vox[i] + 0.5) + f.acc.SX[3 * gi + i] / W : 0.0;
-        mv[i] = (fl & F_V) ? f.acc.SV[3 * gi + i] / W : 0.0;
-    }
-    const double M0 = f.M[gi];
-    if (M0 == 0.0) {
-        f.M[gi] = W;
-        for (int i = 0; i < 3; ++i) {
-            if (fl & F_X) f.X[3 * gi + i] = mx[i];
-            if (fl & F_V) f.V[3 * gi + i] = mv[i];
+    const double* cq = rec + 1;
+    // second moments are only recorded (and only read) when a second-order field is asked for
+    const bool two = xx || xv || vv;
+    const double C[3][3] = {{two ? rec[4] : 0.0, two ? rec[5] : 0.0, two ? rec[6] : 0.0},
+                            {two ? rec[5] : 0.0, two ? rec[7] : 0.0, two ? rec[8] : 0.0},
+                            {two ? rec[6] : 0.0, two ? rec[8] : 0.0, two ? rec[9] : 0.0}};
+    if (x || xx || xv)
+        for (int i = 0; i < 3; ++i) cm[i] = p0[i] + DX[i][0] * cq[0] + DX[i][1] * cq[1] + DX[i][2] * cq[2];
+    if (v || xv || vv)
+        for (int i = 0; i < 3; ++i) cv[i] = v0[i] + DV[i][0] * cq[0] + DV[i][1] * cq[1] + DV[i][2] * cq[2];
+    double TX[3][3], TV[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int q = 0; q < 3; ++q) {
+            TX[i][q] = (xx || xv) ? DX[i][0] * C[0][q] + DX[i][1] * C[1][q] + DX[i][2] * C[2][q] : 0.0;
+            TV[i][q] = vv ? DV[i][0] * C[0][q] + DV[i][1] * C[1][q] + DV[i][2] * C[2][q] : 0.0;
         }
-        for (int k = 0; k < 9; ++k) {
-            if (fl & F_XX) f.XX[9 * gi + k] = f.acc.XX[9 * gi + k] / W;
-            if (fl & F_XV) f.XV[9 * gi + k] = f.acc.XV[9 * gi + k] / W;
-            if (fl & F_VV) f.VV[9 * gi + k] = f.acc.VV[9 * gi + k] / W;
-        }
-        return;
-    }
-    const double Mt = M0 + W;
-    const double b = W / Mt, a = M0 / Mt;
-    double dx[3] = {0, 0, 0}, dv[3] = {0, 0, 0};
-    for (int i = 0; i < 3; ++i) {
-        if (fl & F_X) dx[i] = mx[i] - f.X[3 * gi + i];
-        if (fl & F_V) dv[i] = mv[i] - f.V[3 * gi + i];
-    }
     for (int i = 0; i < 3; ++i)
         for (int j = 0; j < 3; ++j) {
-            const int k = 3 * i + j;
-            if (fl & F_XX) f.XX[9 * gi + k] = a * f.XX[9 * gi + k] + b * (f.acc.XX[9 * gi + k] / W) + a * b * dx[i] * dx[j];
-            if (fl & F_XV) f.XV[9 * gi + k] = a * f.XV[9 * gi + k] + b * (f.acc.XV[9 * gi + k] / W) + a * b * dx[i] * dv[j];
-            if (fl & F_VV) f.VV[9 * gi + k] = a * f.VV[9 * gi + k] + b * (f.acc.VV[9 * gi + k] / W) + a * b * dv[i] * dv[j];
-        }
-    for (int i = 0; i < 3; ++i) {
-        if (fl & F_X) f.X[3 * gi + i] += b * dx[i];
-        if (fl & F_V) f.V[3 * gi + i] += b * dv[i];
-    }
-    f.M[gi] = Mt;
-}
-
-cudaError_t launch_finalize_means(const FinalArgs& f, cudaStream_t s)
-{
-    if (f.nvox == 0) return cudaSuccess;
-    k_finalize_means<<<(unsigned)((f.nvox + 255) / 256), 256, 0, s>>>(f);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_finalize_merge(const FinalArgs& f, cudaStream_t s)
-{
-    if (f.nvox == 0) return cudaSuccess;
-    k_finalize_merge<<<(unsigned)((f.nvox + 255) / 256), 256, 0, s>>>(f);
-    return cudaGetLastError();
-}
-
-// ---- deterministic mode: the reference's online update, voxel by voxel ----
-
-// One thread per run of equal voxel keys walks the run in item order and
-// applies src/geometry.c:106-186 exactly as the reference does.
-__global__ void k_apply_records(ApplyArgs a)
-{
-    const long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (r >= a.nrec) return;
-    const unsigned long long vox = a.key[r] >> 32;
-    if (r > 0 && (a.key[r - 1] >> 32) == vox) return;
-    const long long gi = (long long)vox;
-    const long long cap = a.it.cap;
-    for (long long j = r; j < a.nrec && (a.key[j] >> 32) == vox; ++j) {
-        const long long t = a.item_base + (long long)(a.key[j] & 0xFFFFFFFFull);
-        const double* mom = a.mom + (long long)a.perm[j] * a.nmom;
-        double p0[3], v0[3], DX[3][3], DV[3][3];
-        for (int i = 0; i < 3; ++i) {
-            p0[i] = a.it.p[(i)*cap + t];
-            v0[i] = a.it.u[(i)*cap + t];
-            for (int k = 0; k < 3; ++k) {
-                DX[i][k] = a.it.p[(3 * (k + 1) + i) * cap + t] - p0[i];
-                DV[i][k] = a.it.u[(3 * (k + 1) + i) * cap + t] - v0[i];
+            if (xx) sxx[i][j] = TX[i][0] * DX[j][0] + TX[i][1] * DX[j][1] + TX[i][2] * DX[j][2];
+            if (vv) svv[i][j] = TV[i][0] * DV[j][0] + TV[i][1] * DV[j][1] + TV[i][2] * DV[j][2];
+            if (xv) {
+                const double ai = p0[i] - cm[i], aj = p0[j] - cm[j], bi = v0[i] - cv[i], bj = v0[j] - cv[j];
+                sxv[i][j] = TX[i][0] * DV[j][0] + TX[i][1] * DV[j][1] + TX[i][2] * DV[j][2] + 2.0 * ai * bj - ai * aj -
+                            bi * bj;
             }
         }
-        const double mass = a.it.mass[t];
+}
+
+// Sorted records into contiguous arrays: voxel, item, moments.
+__global__ void k_gather_records(GatherArgs a)
+{
+    const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (j >= a.nrec) return;
+    const unsigned long long k = a.key[j];
+    a.vox[j] = (unsigned)(k >> a.ibits);
+    a.item[j] = (unsigned)(k & ((1ull << a.ibits) - 1ull));
+    const double* src = a.mom + (long long)a.perm[j] * a.nmom;
+    double* dst = a.mom_sorted + j * a.nmom;
+    for (int m = 0; m < a.nmom; ++m) dst[m] = src[m];
+}
+
+cudaError_t launch_gather_records(const GatherArgs& a, cudaStream_t s)
+{
+    if (a.nrec == 0) return cudaSuccess;
+    k_gather_records<<<(unsigned)((a.nrec + 255) / 256), 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+// One thread per voxel run walks the run in item order and applies
+// src/geometry.c:106-186 exactly as the reference does.  For raw FP64 records
+// this reproduces the reference's fields bit for bit.  The voxel's fields are
+// held in registers for the whole run and stored once.
+__global__ void __launch_bounds__(128) k_apply_runs(ApplyArgs a)
+{
+    const long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (r >= a.nruns) return;
+    const long long gi = (long long)a.run_vox[r];
+    const long long beg = a.run_off[r], end = beg + a.run_cnt[r];
+    const bool hx = a.X, hv = a.V, hxx = a.XX, hxv = a.XV, hvv = a.VV;
+    double M = a.M[gi], X[3] = {0, 0, 0}, V[3] = {0, 0, 0}, XX[9], XV[9], VV[9];
+    for (int i = 0; i < 3; ++i) {
+        if (hx) X[i] = a.X[3 * gi + i];
+        if (hv) V[i] = a.V[3 * gi + i];
+    }
+    for (int k = 0; k < 9; ++k) {
+        XX[k] = hxx ? a.XX[9 * gi + k] : 0.0;
+        XV[k] = hxv ? a.XV[9 * gi + k] : 0.0;
+        VV[k] = hvv ? a.VV[9 * gi + k] : 0.0;
+    }
+    for (long long j = beg; j < end; ++j) {
+        const long long t = a.item_base + (long long)a.item[j];
+        const double* mom = a.mom + j * a.nmom;
+        const double* fr = a.it.frame + t * FRAME;
+        double p0[3], v0[3], DX[3][3], DV[3][3];
+        for (int i = 0; i < 3; ++i) {
+            p0[i] = fr[i];
+            v0[i] = fr[FR_U + i];
+            for (int k = 0; k < 3; ++k) {
+                DX[i][k] = fr[3 * (k + 1) + i] - p0[i];
+                DV[i][k] = fr[FR_U + 3 * (k + 1) + i] - v0[i];
+            }
+        }
+        double mass = fr[FR_MASS];
         double cm[3], cv[3], sxx[3][3], sxv[3][3], svv[3][3];
-        if (a.X) centroid(mom, p0, DX, cm);
-        if (a.V) centroid(mom, v0, DV, cv);
-        if (a.XX) second_moment(mom, p0, cm, DX, p0, cm, DX, p0, cm, p0, cm, sxx);
-        if (a.XV) second_moment(mom, p0, cm, DX, v0, cv, DV, p0, cm, v0, cv, sxv);
-        if (a.VV) second_moment(mom, v0, cv, DV, v0, cv, DV, v0, cv, v0, cv, svv);
-        double* M = a.M;
-        const double cw = mass * mom[0] / (M[gi] + mass * mom[0]);
-        const double dw = M[gi] / (M[gi] + mass * mom[0]);
-        if (a.XX)
+        if (a.central) {
+            mass *= a.scale[t];
+            if (a.nmom > 1) mixed_fragment(mom, p0, DX, v0, DV, hx, hv, hxx, hxv, hvv, cm, cv, sxx, sxv, svv);
+        } else {
+            if (hx) centroid(mom, p0, DX, cm);
+            if (hv) centroid(mom, v0, DV, cv);
+            if (hxx) second_moment(mom, p0, cm, DX, p0, cm, DX, p0, cm, p0, cm, sxx);
+            if (hxv) second_moment(mom, p0, cm, DX, v0, cv, DV, p0, cm, v0, cv, sxv);
+            if (hvv) second_moment(mom, v0, cv, DV, v0, cv, DV, v0, cv, v0, cv, svv);
+        }
+        const double cw = mass * mom[0] / (M + mass * mom[0]);
+        const double dw = M / (M + mass * mom[0]);
+        if (hxx)
             for (int i = 0; i < 3; ++i)
-                for (int j2 = 0; j2 < 3; ++j2) {
-                    double* o = &a.XX[9 * gi + 3 * i + j2];
-                    *o = dw * *o + cw * sxx[i][j2] + cw * dw * (cm[i] - a.X[3 * gi + i]) * (cm[j2] - a.X[3 * gi + j2]);
-                }
-        if (a.XV)
+                for (int j2 = 0; j2 < 3; ++j2)
+                    XX[3 * i + j2] = dw * XX[3 * i + j2] + cw * sxx[i][j2] + cw * dw * (cm[i] - X[i]) * (cm[j2] - X[j2]);
+        if (hxv)
             for (int i = 0; i < 3; ++i)
-                for (int j2 = 0; j2 < 3; ++j2) {
-                    double* o = &a.XV[9 * gi + 3 * i + j2];
-                    *o = dw * *o + cw * sxv[i][j2] + cw * dw * (cm[i] - a.X[3 * gi + i]) * (cv[j2] - a.V[3 * gi + j2]);
-                }
-        if (a.VV)
+                for (int j2 = 0; j2 < 3; ++j2)
+                    XV[3 * i + j2] = dw * XV[3 * i + j2] + cw * sxv[i][j2] + cw * dw * (cm[i] - X[i]) * (cv[j2] - V[j2]);
+        if (hvv)
             for (int i = 0; i < 3; ++i)
-                for (int j2 = 0; j2 < 3; ++j2) {
-                    double* o = &a.VV[9 * gi + 3 * i + j2];
-                    *o = dw * *o + cw * svv[i][j2] + cw * dw * (cv[i] - a.V[3 * gi + i]) * (cv[j2] - a.V[3 * gi + j2]);
-                }
-        if (a.X)
-            for (int i = 0; i < 3; ++i) a.X[3 * gi + i] += cw * (cm[i] - a.X[3 * gi + i]);
-        if (a.V)
-            for (int i = 0; i < 3; ++i) a.V[3 * gi + i] += cw * (cv[i] - a.V[3 * gi + i]);
-        M[gi] += mass * mom[0];
+                for (int j2 = 0; j2 < 3; ++j2)
+                    VV[3 * i + j2] = dw * VV[3 * i + j2] + cw * svv[i][j2] + cw * dw * (cv[i] - V[i]) * (cv[j2] - V[j2]);
+        if (hx)
+            for (int i = 0; i < 3; ++i) X[i] += cw * (cm[i] - X[i]);
+        if (hv)
+            for (int i = 0; i < 3; ++i) V[i] += cw * (cv[i] - V[i]);
+        M += mass * mom[0];
+    }
+    a.M[gi] = M;
+    for (int i = 0; i < 3; ++i) {
+        if (hx) a.X[3 * gi + i] = X[i];
+        if (hv) a.V[3 * gi + i] = V[i];
+    }
+    for (int k = 0; k < 9; ++k) {
+        if (hxx) a.XX[9 * gi + k] = XX[k];
+        if (hxv) a.XV[9 * gi + k] = XV[k];
+        if (hvv) a.VV[9 * gi + k] = VV[k];
     }
 }
 
 cudaError_t launch_apply_records(const ApplyArgs& a, cudaStream_t s)
 {
-    if (a.nrec == 0) return cudaSuccess;
-    k_apply_records<<<(unsigned)((a.nrec + 255) / 256), 256, 0, s>>>(a);
+    if (a.nruns == 0) return cudaSuccess;
+    k_apply_runs<<<(unsigned)((a.nruns + 127) / 128), 128, 0, s>>>(a);
     return cudaGetLastError();
 }
 

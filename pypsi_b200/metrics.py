@@ -9,9 +9,11 @@ Two measures per field, over voxels whose reference mass is positive:
 * ``norm`` -- the error normalised by the voxel's own scale of that field:
   ``m``: m_ref; ``x``: max|x_ref|; ``v``: max(|v_ref|, sqrt(max diag vv_ref));
   ``xx``/``vv``: the largest diagonal entry of that voxel's tensor (which
-  bounds every entry of a covariance); ``xv``: sqrt(max diag xx * max diag vv),
-  or max|xv_ref| when those are absent.  Each scale is floored at 1e-12 of its
-  mean over the grid.  This is the bound the parity tests enforce.
+  bounds every entry of a covariance); ``xv``: the larger of sqrt(max diag xx *
+  max diag vv) and max|xv_ref| -- the reference's xv pairs its cross terms with
+  the other variable (src/geometry.c:139-140), so it is not a covariance and the
+  Cauchy-Schwarz scale alone does not bound it.  Each scale is floored at
+  1e-12 of its mean over the grid.  This is the bound the parity tests enforce.
 """
 from __future__ import annotations
 
@@ -39,10 +41,10 @@ def field_errors(test: dict, ref: dict) -> dict:
         if f in ref:
             scales[f] = _diagmax(ref[f])
     if "xv" in ref:
+        s = np.max(np.abs(ref["xv"]).reshape(m.shape + (9,)), axis=-1)
         if "xx" in ref and "vv" in ref:
-            scales["xv"] = np.sqrt(_diagmax(ref["xx"]) * _diagmax(ref["vv"]))
-        else:
-            scales["xv"] = np.max(np.abs(ref["xv"]).reshape(m.shape + (9,)), axis=-1)
+            s = np.maximum(s, np.sqrt(_diagmax(ref["xx"]) * _diagmax(ref["vv"])))
+        scales["xv"] = s
     for f, r in ref.items():
         t = test[f]
         d = np.abs(t - r)
