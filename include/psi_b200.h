@@ -136,6 +136,29 @@ void psib_host_free(void *p);
 /* Release the library's cached device buffers on the current device. */
 int psib_release_device_memory(void);
 
+/* Density deposit for callers that must not have the library allocate device
+ * memory -- e.g. an application whose own pool allocator owns all of the GPU's
+ * memory, or a time-critical loop that cannot afford an allocation.  It has no
+ * counterpart in the reference.
+ *
+ * Adds the mass of ntets tets to grid->fields[PSIB_M] (a device pointer; the
+ * other fields must be NULL).  tet_pos is a device array of ntets x 4 x 3
+ * doubles (vertex-major, positions already periodic-unwrapped by the caller),
+ * tet_mass a device array of ntets doubles (NULL: 1).  The tets are clipped
+ * against the grid window and deposited as psib_voxels would deposit simplex
+ * elements (same fragments; the sum per voxel may round differently because it
+ * is accumulated with atomics).  Runs on `stream` and returns when it is done.
+ *
+ * It calls no cudaMalloc or cudaFree: its scratch is a fixed array of about
+ * 7.9 MiB in device memory, held by every GPU that loads the library until
+ * the process exits.  Limits: a tet whose voxel index box needs a bisection
+ * deeper than 12 levels (roughly more than 16 voxels on every axis) is
+ * rejected with PSIB_ERR_ARG.  All calls on a device share that array: calls
+ * that overlap on the GPU race.  The first call on a device looks up the
+ * array's address and should come before any stream capture. */
+int psib_voxels_density_noalloc(const psib_grid *grid, const double *tet_pos, const double *tet_mass,
+                                long long ntets, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

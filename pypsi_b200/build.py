@@ -29,6 +29,7 @@ CUDA_UNITS = {  # unit -> extra flags
     "clip_mixed.cu": [],
     "tess.cu": ["--fmad=false"],
     "pipeline.cu": ["--fmad=false"],
+    "noalloc.cu": ["--fmad=false"],
 }
 HEADERS = ["psib_device.cuh", "psib_clip.cuh", "psib_kernels.h"]
 

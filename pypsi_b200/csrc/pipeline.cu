@@ -570,6 +570,8 @@ int validate(const psib_grid* g, const psib_mesh* m, int mode, const psib_option
 
 } // namespace
 
+int psib::report_error(int code, const char* msg) { return fail(code, "%s", msg); }
+
 extern "C" {
 
 const char* psib_last_error(void) { return g_err.c_str(); }

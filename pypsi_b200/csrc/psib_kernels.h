@@ -124,4 +124,7 @@ struct ApplyArgs {
 };
 cudaError_t launch_apply_records(const ApplyArgs &a, cudaStream_t s);
 
+// Record `msg` as this thread's last error (psib_last_error) and return `code`.
+int report_error(int code, const char *msg);
+
 } // namespace psib
