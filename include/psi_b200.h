@@ -49,7 +49,10 @@ extern "C" {
 
 /* arithmetic of the clip kernel */
 #define PSIB_FP64 0  /* the reference's double-precision operation order, no FMA */
-#define PSIB_MIXED 1 /* FP32 clipping on tile-recentred tets, FP64 moments and sums */
+#define PSIB_MIXED 1 /* FP32 bisection walk; fragment vertices recomputed in FP64 from their planes,
+                        FP64 moments and sums */
+#define PSIB_FP64_CENTRAL 2 /* FP64 walk with moments taken about each fragment: more accurate than the
+                               reference for tiny fragments, not bit-identical to it */
 
 /* where the pointers of psib_grid / psib_mesh live */
 #define PSIB_HOST 0   /* host memory; the library copies in and out */
@@ -104,7 +107,7 @@ typedef struct {
 } psib_stats;
 
 typedef struct {
-    int precision;     /* PSIB_FP64 or PSIB_MIXED */
+    int precision;     /* PSIB_FP64, PSIB_MIXED or PSIB_FP64_CENTRAL */
     int deterministic; /* accepted for compatibility: every call is deterministic (fragments are sorted
                           by voxel and applied in the reference's order; FP64 equals the reference bit for bit) */
     int memory;        /* PSIB_HOST or PSIB_DEVICE */
@@ -118,6 +121,24 @@ typedef struct {
  * refine_max_lvl is capped at 6 like src/refine.c:89-92. */
 int psib_voxels(const psib_grid *grid, const psib_mesh *mesh, int mode, double refine_tolerance,
                 int refine_max_lvl, const psib_options *opt);
+
+/* Adjoint of the density deposit.  The reference has no adjoint; this is
+ * the backward pass of psib_voxels's m field for differentiable use.
+ *
+ * grad->fields[PSIB_M] holds dL/dm per voxel (same grid as the forward call;
+ * every other field must be NULL).  The gradient of L with respect to the
+ * particle positions is ADDED to grad_pos (npart x 3 doubles) and, when
+ * grad_mass is not NULL, the gradient with respect to the element masses to
+ * grad_mass (nelem doubles).  grad_vel is accepted for ABI stability and left
+ * unchanged: the m field does not depend on the velocities.  The clip is
+ * recomputed in FP64 (options->precision is ignored); each fragment's mass
+ * fraction is differentiated through the faces it shares with its tet.
+ * Gradients are summed with atomics, so the last bits may vary between runs.
+ * Supported: refine_max_lvl = 0 for trilinear elements, and simplex elements.
+ * Memory and stream follow options as in psib_voxels. */
+int psib_voxels_adjoint(const psib_grid *grad, const psib_mesh *mesh, double refine_tolerance,
+                        int refine_max_lvl, double *grad_pos, double *grad_vel, double *grad_mass,
+                        const psib_options *opt);
 
 /* Message for the last failure on this thread ("" if none). */
 const char *psib_last_error(void);

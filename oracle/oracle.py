@@ -8,6 +8,9 @@ Two back ends with one interface:
 
 * ``restatement`` -- ``_build/liboracle.so`` from ``psi_oracle.c``, a step by
   step C restatement of the reference density path with work counters;
+* ``exact``       -- ``_build/liboracle_exact.so``, the same restatement with
+  quad-precision (__float128) arithmetic: the result the reference's algorithm
+  computes without rounding, to measure the reference's own rounding error;
 * ``reference``   -- ``_ref/libpsiref.so``, the reference's own sources
   (src/cpsi.c, src/geometry.c, src/refine.c, ...) compiled unchanged; its entry
   ``psi_voxels`` is declared at src/PSI.c:39 and defined at src/cpsi.c:41.
@@ -28,6 +31,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_ORACLE = os.path.join(HERE, "_build", "liboracle.so")
 LIB_REF = os.path.join(HERE, "_ref", "libpsiref.so")
+LIB_EXACT = os.path.join(HERE, "_build", "liboracle_exact.so")
+_PATHS = {"restatement": LIB_ORACLE, "exact": LIB_EXACT, "reference": LIB_REF}
 FIELD_NAMES = ("m", "x", "v", "xx", "xv", "vv")
 
 
@@ -83,11 +88,11 @@ _libs: dict[str, C.CDLL] = {}
 
 def _lib(kind: str) -> C.CDLL:
     if kind not in _libs:
-        path = LIB_ORACLE if kind == "restatement" else LIB_REF
+        path = _PATHS[kind]
         if not os.path.exists(path):
             raise FileNotFoundError(f"{path} not built (run oracle.build())")
         lib = C.CDLL(path)
-        if kind == "restatement":
+        if kind != "reference":
             lib.oracle_voxels.argtypes = [C.POINTER(_OgGrid), C.POINTER(_OgMesh), C.c_double,
                                           C.c_int, C.POINTER(Counters)]
             lib.oracle_voxels.restype = C.c_int
@@ -100,7 +105,7 @@ def _lib(kind: str) -> C.CDLL:
 
 
 def available(kind: str) -> bool:
-    return os.path.exists(LIB_ORACLE if kind == "restatement" else LIB_REF)
+    return os.path.exists(_PATHS[kind])
 
 
 @contextlib.contextmanager
@@ -160,7 +165,7 @@ def voxelize(kind, n, bounds, pos, conn, vel=None, mass=None, periodic_box=None,
     for f, a in out.items():
         assert a.dtype == np.float64 and a.flags.c_contiguous, f
     ptrs = [_dp(out.get(f)) for f in FIELD_NAMES]
-    if kind == "restatement":
+    if kind != "reference":
         g = _OgGrid()
         g.n[:] = n
         g.win[0][:] = lo

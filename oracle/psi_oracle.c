@@ -20,6 +20,16 @@
 #include <stdlib.h>
 #include <string.h>
 
+/* Arithmetic type of the clip, moments and projection.  double (default)
+ * repeats the reference bit for bit; building with -DOV_REAL=__float128 gives
+ * an "exact" oracle (113-bit mantissa) that measures the reference's own
+ * rounding error, which is large for tiny fragments: their raw q-moments about
+ * the tet's vertex 0 cancel. */
+#ifndef OV_REAL
+#define OV_REAL double
+#endif
+typedef OV_REAL ov_real;
+
 #define OV_MAXV 64        /* vertex buffer of one polyhedron (include/geometry.h:23) */
 #define OV_STACK 64       /* bisection stack depth (src/geometry.c:41-46) */
 #define OV_WALK_CAP 4096  /* bound on a face walk; the reference has none */
@@ -57,8 +67,8 @@ typedef struct {
 /* ---- polyhedron: r3d vertex graph with barycentric mass coordinates q ---- */
 
 typedef struct {
-    double pos[3];
-    double q[3];
+    ov_real pos[3];
+    ov_real q[3];
     int nbr[3];
 } ov_vert;
 
@@ -100,9 +110,9 @@ static void ov_clip(ov_poly *P, const double (*pn)[3], const double *pd, int npl
     if (P->nv <= 0) return;
     for (int p = 0; p < nplanes; ++p) {
         int onv = P->nv;
-        double s[OV_MAXV];
+        ov_real s[OV_MAXV];
         int map[OV_MAXV];
-        double smin = 1.0e30, smax = -1.0e30;
+        ov_real smin = 1.0e30, smax = -1.0e30;
         memset(map, 0, sizeof(map));
         for (int v = 0; v < onv; ++v) {
             s[v] = pd[p];
@@ -123,7 +133,7 @@ static void ov_clip(ov_poly *P, const double (*pn)[3], const double *pd, int npl
                 int vn = P->v[vc].nbr[k];
                 if (!map[vn]) continue;
                 if (nv >= OV_MAXV) { g_cnt->errors++; P->nv = 0; return; }
-                double w = 1.0 / (s[vc] - s[vn]);
+                ov_real w = 1.0 / (s[vc] - s[vn]);
                 ov_vert *a = &P->v[vc], *b = &P->v[vn], *c = &P->v[nv];
                 for (int i = 0; i < 3; ++i) c->pos[i] = w * (b->pos[i] * s[vc] - a->pos[i] * s[vn]);
                 for (int i = 0; i < 3; ++i) c->q[i] = w * (b->q[i] * s[vc] - a->q[i] * s[vn]);
@@ -151,7 +161,7 @@ static void ov_clip(ov_poly *P, const double (*pn)[3], const double *pd, int npl
  * (src/geometry.c:560-690).  `in` is used as scratch. */
 static void ov_split(ov_poly *in, ov_poly *out, double coord, int ax)
 {
-    double s[OV_MAXV];
+    ov_real s[OV_MAXV];
     int side[OV_MAXV];
     int nright = 0, onv = in->nv;
     memset(side, 0, sizeof(side));
@@ -180,9 +190,9 @@ static void ov_split(ov_poly *in, ov_poly *out, double coord, int ax)
             int vn = in->v[vc].nbr[k];
             if (!side[vn]) continue;
             if (nv + 2 > OV_MAXV) { g_cnt->errors++; out[0].nv = out[1].nv = 0; return; }
-            double w = 1.0 / (s[vc] - s[vn]);
+            ov_real w = 1.0 / (s[vc] - s[vn]);
             ov_vert *a = &in->v[vc], *b = &in->v[vn];
-            double np_[3], nq[3];
+            ov_real np_[3], nq[3];
             for (int i = 0; i < 3; ++i) {
                 np_[i] = w * (b->pos[i] * s[vc] - a->pos[i] * s[vn]);
                 nq[i] = w * (b->q[i] * s[vc] - a->q[i] * s[vn]);
@@ -220,11 +230,11 @@ static void ov_split(ov_poly *in, ov_poly *out, double coord, int ax)
 
 /* Moments of the polyhedron in q-space, orders 0..2 (1, 4 or 10 values), by
  * fan-triangulating every face (src/geometry.c:692-767). */
-static void ov_reduce(const ov_poly *P, double *mom, int order)
+static void ov_reduce(const ov_poly *P, ov_real *mom, int order)
 {
     static const int nmom[3] = {1, 4, 10};
     unsigned char done[OV_MAXV][3];
-    memset(mom, 0, nmom[order] * sizeof(double));
+    for (int i = 0; i < nmom[order]; ++i) mom[i] = 0;
     memset(done, 0, sizeof(done));
     for (int vs = 0; vs < P->nv; ++vs)
         for (int ks = 0; ks < 3; ++ks) {
@@ -232,7 +242,7 @@ static void ov_reduce(const ov_poly *P, double *mom, int order)
             int vc = vs, kn = ks, k;
             done[vc][kn] = 1;
             int vn = P->v[vc].nbr[kn];
-            const double *q0 = P->v[vc].q;
+            const ov_real *q0 = P->v[vc].q;
             for (k = 0; k < 3; ++k)
                 if (P->v[vn].nbr[k] == vc) break;
             vc = vn;
@@ -242,10 +252,10 @@ static void ov_reduce(const ov_poly *P, double *mom, int order)
             int steps = 0;
             while (vn != vs) {
                 if (++steps > OV_WALK_CAP) { g_cnt->errors++; return; }
-                const double *q1 = P->v[vn].q;
-                const double *q2 = P->v[vc].q;
+                const ov_real *q1 = P->v[vn].q;
+                const ov_real *q2 = P->v[vc].q;
                 /* 6 x signed volume of the cone (0, q0, q1, q2) */
-                double m = (-q2[0] * q1[1] * q0[2] + q1[0] * q2[1] * q0[2] + q2[0] * q0[1] * q1[2]
+                ov_real m = (-q2[0] * q1[1] * q0[2] + q1[0] * q2[1] * q0[2] + q2[0] * q0[1] * q1[2]
                             - q0[0] * q2[1] * q1[2] - q1[0] * q0[1] * q2[2] + q0[0] * q1[1] * q2[2]);
                 mom[0] += m;
                 if (order > 0) {
@@ -254,12 +264,12 @@ static void ov_reduce(const ov_poly *P, double *mom, int order)
                     mom[3] += 0.25 * m * (q0[2] + q1[2] + q2[2]);
                 }
                 if (order > 1) {
-                    mom[4] += 0.1 * m * (q0[0] * q0[0] + q1[0] * q1[0] + q2[0] * q2[0] + q1[0] * q2[0] + q0[0] * (q1[0] + q2[0]));
-                    mom[5] += 0.05 * m * (q2[0] * q0[1] + q2[0] * q1[1] + 2 * q2[0] * q2[1] + q0[0] * (2 * q0[1] + q1[1] + q2[1]) + q1[0] * (q0[1] + 2 * q1[1] + q2[1]));
-                    mom[6] += 0.05 * m * (q2[0] * q0[2] + q2[0] * q1[2] + 2 * q2[0] * q2[2] + q0[0] * (2 * q0[2] + q1[2] + q2[2]) + q1[0] * (q0[2] + 2 * q1[2] + q2[2]));
-                    mom[7] += 0.1 * m * (q0[1] * q0[1] + q1[1] * q1[1] + q2[1] * q2[1] + q1[1] * q2[1] + q0[1] * (q1[1] + q2[1]));
-                    mom[8] += 0.05 * m * (q2[1] * q0[2] + q2[1] * q1[2] + 2 * q2[1] * q2[2] + q0[1] * (2 * q0[2] + q1[2] + q2[2]) + q1[1] * (q0[2] + 2 * q1[2] + q2[2]));
-                    mom[9] += 0.1 * m * (q0[2] * q0[2] + q1[2] * q1[2] + q2[2] * q2[2] + q1[2] * q2[2] + q0[2] * (q1[2] + q2[2]));
+                    mom[4] += ((ov_real)1 / 10) * m * (q0[0] * q0[0] + q1[0] * q1[0] + q2[0] * q2[0] + q1[0] * q2[0] + q0[0] * (q1[0] + q2[0]));
+                    mom[5] += ((ov_real)1 / 20) * m * (q2[0] * q0[1] + q2[0] * q1[1] + 2 * q2[0] * q2[1] + q0[0] * (2 * q0[1] + q1[1] + q2[1]) + q1[0] * (q0[1] + 2 * q1[1] + q2[1]));
+                    mom[6] += ((ov_real)1 / 20) * m * (q2[0] * q0[2] + q2[0] * q1[2] + 2 * q2[0] * q2[2] + q0[0] * (2 * q0[2] + q1[2] + q2[2]) + q1[0] * (q0[2] + 2 * q1[2] + q2[2]));
+                    mom[7] += ((ov_real)1 / 10) * m * (q0[1] * q0[1] + q1[1] * q1[1] + q2[1] * q2[1] + q1[1] * q2[1] + q0[1] * (q1[1] + q2[1]));
+                    mom[8] += ((ov_real)1 / 20) * m * (q2[1] * q0[2] + q2[1] * q1[2] + 2 * q2[1] * q2[2] + q0[1] * (2 * q0[2] + q1[2] + q2[2]) + q1[1] * (q0[2] + 2 * q1[2] + q2[2]));
+                    mom[9] += ((ov_real)1 / 10) * m * (q0[2] * q0[2] + q1[2] * q1[2] + q2[2] * q2[2] + q1[2] * q2[2] + q0[2] * (q1[2] + q2[2]));
                 }
                 for (k = 0; k < 3; ++k)
                     if (P->v[vn].nbr[k] == vc) break;
@@ -293,7 +303,7 @@ static void ov_voxelize_tet(const double (*pos)[3], const double (*vel)[3], doub
                             const double (*rbox)[3], const og_grid *g, ov_poly *stack)
 {
     static const int qi[3][3] = {{4, 5, 6}, {5, 7, 8}, {6, 8, 9}};
-    double DX[3][3], DV[3][3];
+    ov_real DX[3][3], DV[3][3];
     for (int i = 0; i < 3; ++i)
         for (int j = 0; j < 3; ++j) {
             DX[i][j] = pos[j + 1][i] - pos[0][i];
@@ -328,7 +338,7 @@ static void ov_voxelize_tet(const double (*pos)[3], const double (*vel)[3], doub
 
     int top = 1;
     ov_poly cur;
-    double mom[10];
+    ov_real mom[10];
     while (top > 0) {
         cur = stack[--top];
         if (cur.nv <= 0) continue;
@@ -350,7 +360,7 @@ static void ov_voxelize_tet(const double (*pos)[3], const double (*vel)[3], doub
             g_cnt->fragments++;
             g_cnt->frag_verts += cur.nv;
 
-            double cm[3], cv[3], sxx[3][3], sxv[3][3], svv[3][3];
+            ov_real cm[3], cv[3], sxx[3][3], sxv[3][3], svv[3][3];
             if (g->f[1])
                 for (int i = 0; i < 3; ++i) {
                     cm[i] = mom[0] * pos[0][i];
@@ -404,8 +414,8 @@ static void ov_voxelize_tet(const double (*pos)[3], const double (*vel)[3], doub
 
             /* online weighted update (src/geometry.c:164-186) */
             double *M = g->f[0], *X = g->f[1], *V = g->f[2];
-            double cw = mass * mom[0] / (M[gi] + mass * mom[0]);
-            double dw = M[gi] / (M[gi] + mass * mom[0]);
+            ov_real cw = mass * mom[0] / (M[gi] + mass * mom[0]);
+            ov_real dw = M[gi] / (M[gi] + mass * mom[0]);
             if (g->f[3])
                 for (int i = 0; i < 3; ++i)
                     for (int j = 0; j < 3; ++j) {

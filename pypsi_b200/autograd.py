@@ -1,0 +1,78 @@
+"""Differentiable density deposit: ``torch.autograd.Function`` over the C ABI.
+
+``deposit_density(pos, mass, n=..., bounds=..., ...)`` returns the m field of
+``PSI.voxels`` (mass per voxel, float64, shape n) for particle positions held
+in a CUDA tensor.  Its backward pass is ``psib_voxels_adjoint``: the clip is
+recomputed in FP64 and each fragment's mass fraction is differentiated through
+the fragment faces that lie on the faces of its tet.  Gradients flow to the
+positions and, when it requires them, to the element masses.  The m field does
+not depend on velocities, so none are taken.
+
+PyPSI itself is not differentiable; the forward pass is its density branch
+(src/cpsi.c:41-112, src/geometry.c:60-188), computed by ``psib_voxels``.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import torch
+
+from . import capi
+
+
+@dataclass(frozen=True)
+class DepositSpec:
+    """The grid and the mesh topology of a deposit (everything but the tensors)."""
+
+    n: tuple
+    bounds: tuple
+    block_dims: tuple | None = None
+    periodic_box: tuple | None = None
+    precision: str = "fp64"
+
+
+class _DensityDeposit(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, pos, mass, connectivity, spec: DepositSpec):
+        m = torch.zeros(spec.n, dtype=torch.float64, device=pos.device)
+        capi.voxels_device({"m": m}, spec.n, spec.bounds, pos, None, mass, connectivity=connectivity,
+                           block_dims=spec.block_dims, periodic_box=spec.periodic_box, precision=spec.precision)
+        ctx.save_for_backward(pos, mass, connectivity)
+        ctx.spec = spec
+        return m
+
+    @staticmethod
+    def backward(ctx, grad_m):
+        pos, mass, connectivity = ctx.saved_tensors
+        spec = ctx.spec
+        grad_pos = torch.zeros_like(pos)
+        grad_mass = torch.zeros_like(mass) if (mass is not None and ctx.needs_input_grad[1]) else None
+        capi.adjoint_device(grad_m.contiguous(), spec.n, spec.bounds, pos, grad_pos, mass=mass,
+                            connectivity=connectivity, block_dims=spec.block_dims,
+                            periodic_box=spec.periodic_box, grad_mass=grad_mass)
+        return (grad_pos if ctx.needs_input_grad[0] else None), grad_mass, None, None
+
+
+def deposit_density(pos: torch.Tensor, mass: torch.Tensor | None = None, *, n, bounds, block_dims=None,
+                    connectivity: torch.Tensor | None = None, periodic_box=None,
+                    precision: str = "fp64") -> torch.Tensor:
+    """m field of PSI.voxels(grid, mesh) for particles at `pos`, differentiable.
+
+    pos: (npart, 3) float64 CUDA tensor (C-contiguous).  mass: (nelem,) float64
+    or None (1 per element).  The mesh is a block lattice (`block_dims`, as
+    Mesh(loader='block')) or explicit `connectivity` ((nelem, 4|8) int32), in a
+    periodic box when `periodic_box` is given.  `precision` selects the forward
+    kernel ('fp64' or 'mixed'); the backward pass is always FP64."""
+    if not pos.is_cuda:
+        raise ValueError("deposit_density runs on the GPU: pos must be a CUDA tensor")
+    if pos.dtype != torch.float64 or not pos.is_contiguous():
+        raise ValueError("pos must be a C-contiguous float64 tensor")
+    if mass is not None and (mass.dtype != torch.float64 or not mass.is_contiguous()):
+        raise ValueError("mass must be a C-contiguous float64 tensor")
+    if connectivity is None and block_dims is None:
+        raise ValueError("give block_dims or connectivity")
+    spec = DepositSpec(tuple(int(v) for v in n), tuple(tuple(float(x) for x in b) for b in bounds),
+                       tuple(int(v) for v in block_dims) if block_dims is not None else None,
+                       tuple(tuple(float(x) for x in b) for b in periodic_box) if periodic_box is not None else None,
+                       precision)
+    return _DensityDeposit.apply(pos, mass, connectivity, spec)

@@ -12,7 +12,8 @@ import ctypes as C
 
 from . import lib
 
-PSIB_FP64, PSIB_MIXED = 0, 1
+PSIB_FP64, PSIB_MIXED, PSIB_FP64_CENTRAL = 0, 1, 2
+PRECISIONS = {"fp64": PSIB_FP64, "mixed": PSIB_MIXED, "fp64-central": PSIB_FP64_CENTRAL}
 PSIB_HOST, PSIB_DEVICE = 0, 1
 FIELDS = ("m", "x", "v", "xx", "xv", "vv")
 COMPONENTS = {"m": 1, "x": 3, "v": 3, "xx": 9, "xv": 9, "vv": 9}
@@ -47,6 +48,9 @@ class Options(C.Structure):
 
 lib.psib_voxels.argtypes = [C.POINTER(Grid), C.POINTER(Mesh), C.c_int, C.c_double, C.c_int, C.POINTER(Options)]
 lib.psib_voxels.restype = C.c_int
+lib.psib_voxels_adjoint.argtypes = [C.POINTER(Grid), C.POINTER(Mesh), C.c_double, C.c_int, C.c_void_p, C.c_void_p,
+                                    C.c_void_p, C.POINTER(Options)]
+lib.psib_voxels_adjoint.restype = C.c_int
 lib.psib_last_error.restype = C.c_char_p
 lib.psib_release_device_memory.restype = C.c_int
 
@@ -109,6 +113,14 @@ def voxels_device(fields: dict, n, bounds, pos, vel=None, mass=None, connectivit
         assert t.is_cuda and t.dtype == torch.float64 and t.is_contiguous(), f
     ptr = {f: t.data_ptr() for f, t in fields.items()}
     g = make_grid(n, bounds, ptr)
+    m = mesh_from_tensors(pos, vel, mass, connectivity, block_dims, periodic_box)
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return voxels(g, m, PRECISIONS[precision], deterministic, PSIB_DEVICE,
+                  C.c_void_p(s.cuda_stream), refine_tolerance, refine_max_lvl)
+
+
+def mesh_from_tensors(pos, vel=None, mass=None, connectivity=None, block_dims=None, periodic_box=None) -> Mesh:
+    """A psib_mesh over contiguous tensors (or arrays with data_ptr())."""
     npart = pos.numel() // 3
     if connectivity is not None:
         elemtype, nelem = connectivity.shape[-1], connectivity.numel() // connectivity.shape[-1]
@@ -117,9 +129,29 @@ def voxels_device(fields: dict, n, bounds, pos, vel=None, mass=None, connectivit
         nelem = 1
         for b in block_dims:
             nelem *= b if periodic_box is not None else b - 1
-    m = make_mesh(npart, nelem, pos.data_ptr(), vel.data_ptr() if vel is not None else None,
-                  mass.data_ptr() if mass is not None else None,
-                  connectivity.data_ptr() if connectivity is not None else None, elemtype, block_dims, periodic_box)
+    return make_mesh(npart, nelem, pos.data_ptr(), vel.data_ptr() if vel is not None else None,
+                     mass.data_ptr() if mass is not None else None,
+                     connectivity.data_ptr() if connectivity is not None else None, elemtype, block_dims, periodic_box)
+
+
+def adjoint_device(grad_m, n, bounds, pos, grad_pos, mass=None, connectivity=None, block_dims=None,
+                   periodic_box=None, grad_mass=None, stream=None) -> dict:
+    """Backward pass of the m field on device-resident torch tensors.
+
+    grad_m: (nx,ny,nz) float64 CUDA tensor, dL/dm.  Adds dL/dpos to grad_pos
+    ((npart,3) float64) and, if given, dL/dmass to grad_mass ((nelem,))."""
+    import torch
+
+    for t in (grad_m, pos, grad_pos) + ((grad_mass,) if grad_mass is not None else ()):
+        assert t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()
+    g = make_grid(n, bounds, {"m": grad_m.data_ptr()})
+    m = mesh_from_tensors(pos, None, mass, connectivity, block_dims, periodic_box)
     s = stream if stream is not None else torch.cuda.current_stream()
-    return voxels(g, m, PSIB_MIXED if precision == "mixed" else PSIB_FP64, deterministic, PSIB_DEVICE,
-                  C.c_void_p(s.cuda_stream), refine_tolerance, refine_max_lvl)
+    st = Stats()
+    o = Options(precision=PSIB_FP64, deterministic=0, memory=PSIB_DEVICE, device=-1,
+                stream=C.c_void_p(s.cuda_stream), stats=C.pointer(st))
+    rc = lib.psib_voxels_adjoint(C.byref(g), C.byref(m), 1.0, 0, grad_pos.data_ptr(), None,
+                                 grad_mass.data_ptr() if grad_mass is not None else None, C.byref(o))
+    if rc != 0:
+        raise PsibError(rc)
+    return st.as_dict()

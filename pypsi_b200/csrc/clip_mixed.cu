@@ -8,40 +8,60 @@
 
 namespace psib {
 
-// The register-capped main kernel (8 resident blocks) is the default: its
-// extra warps hide more scratch latency (measured ~7% faster at 128^3 -> 256^3).
-// PSIB_CLIP_OCC=0 selects the 96-register build.
-static bool high_occupancy()
-{
-    const char* v = getenv("PSIB_CLIP_OCC");
-    return !(v && v[0] == '0');
-}
+constexpr int DEFAULT_MINB_MIXED = 0;
 
+// Main kernel variants by the minimum number of resident 128-thread blocks
+// per SM the register allocation must allow (0: no cap).  More blocks hide more
+// scratch latency but force spills; PSIB_CLIP_MINB picks one (default below,
+// from measurements at 128^3 -> 256^3).
+template <int MINB>
+__global__ void __launch_bounds__(128, MINB) k_clip_mixed_b(ClipArgs a) { clip_loop<float, NS_MAIN, true>(a); }
 __global__ void __launch_bounds__(128) k_clip_mixed(ClipArgs a) { clip_loop<float, NS_MAIN, true>(a); }
 
-// the same with registers capped for 8 resident blocks (more warps to hide scratch latency)
-__global__ void __launch_bounds__(128, 8) k_clip_mixed_occ(ClipArgs a) { clip_loop<float, NS_MAIN, true>(a); }
+static int min_blocks()
+{
+    const char* v = getenv("PSIB_CLIP_MINB");
+    return v && *v ? atoi(v) : DEFAULT_MINB_MIXED;
+}
+
+template <class F>
+static auto with_variant(F&& f)
+{
+    switch (min_blocks()) {
+    case 4: return f(k_clip_mixed_b<4>);
+    case 5: return f(k_clip_mixed_b<5>);
+    case 6: return f(k_clip_mixed_b<6>);
+    case 8: return f(k_clip_mixed_b<8>);
+    default: return f(k_clip_mixed);
+    }
+}
+
+// PSIB_FP64_CENTRAL: the FP64 walk writing centroid-form records
+__global__ void __launch_bounds__(128, 5) k_clip_fp64c(ClipArgs a) { clip_loop<double, NS_MAIN, true>(a); }
 
 // Images with deep trees or long index boxes: FP64 clipping (FP32 would lose
 // precision inside a voxel of a long tet), centroid-form records.
 __global__ void __launch_bounds__(64) k_clip_mixed_big(ClipArgs a) { clip_loop<double, NS_BIG, true>(a); }
 
-size_t scratch_bytes_mixed(bool big) { return big ? region_bytes<double, NS_BIG>() : region_bytes<float, NS_MAIN>(); }
+size_t scratch_bytes_mixed(bool big, bool fp64_walk)
+{
+    return big ? region_bytes<double, NS_BIG>() : fp64_walk ? region_bytes<double, NS_MAIN>() : region_bytes<float, NS_MAIN>();
+}
 
-cudaError_t launch_clip_mixed(const ClipArgs& a, bool big, int grid, int block, cudaStream_t s)
+cudaError_t launch_clip_mixed(const ClipArgs& a, bool big, bool fp64_walk, int grid, int block, cudaStream_t s)
 {
     if (big) k_clip_mixed_big<<<grid, block, 0, s>>>(a);
-    else if (high_occupancy()) k_clip_mixed_occ<<<grid, block, 0, s>>>(a);
-    else k_clip_mixed<<<grid, block, 0, s>>>(a);
+    else if (fp64_walk) k_clip_fp64c<<<grid, block, 0, s>>>(a);
+    else with_variant([&](auto k) { k<<<grid, block, 0, s>>>(a); return 0; });
     return cudaGetLastError();
 }
 
-int clip_blocks_per_sm_mixed(bool big, int block)
+int clip_blocks_per_sm_mixed(bool big, bool fp64_walk, int block)
 {
     int n = 0;
     cudaError_t e = big ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_clip_mixed_big, block, 0)
-                        : high_occupancy() ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_clip_mixed_occ, block, 0)
-                                           : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_clip_mixed, block, 0);
+                    : fp64_walk ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_clip_fp64c, block, 0)
+                        : with_variant([&](auto k) { return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, block, 0); });
     if (e != cudaSuccess) { cudaGetLastError(); return 1; }
     return n > 0 ? n : 1;
 }

@@ -129,7 +129,7 @@ __device__ void deposit_tet(const NaArgs& a, long long t, Poly<double>* S, unsig
         if (smax <= 0.0) { P.nv = 0; break; }
         int o;
         if (!alloc(o)) { st |= ST_OVERFLOW; return; }
-        const unsigned e = cut_poly<double, false>(P, s, um, S[o], S[o]);
+        const unsigned e = cut_poly<double, false>(P, s, um, S[o], S[o], axis_tag(ax));
         freem |= 1u << c;
         c = o;
         if (e) { st |= e; return; }
@@ -173,7 +173,7 @@ __device__ void deposit_tet(const NaArgs& a, long long t, Poly<double>* S, unsig
                 } else {
                     int l, r;
                     if (!alloc(l) || !alloc(r)) { st |= ST_OVERFLOW; return; }
-                    const unsigned e = cut_poly<double, true>(P, s, um, S[l], S[r]);
+                    const unsigned e = cut_poly<double, true>(P, s, um, S[l], S[r], axis_tag(ax));
                     if (e) { st |= e; return; }
                     for (int i = 0; i < 3; ++i) {
                         S[l].lo[i] = P.lo[i]; S[l].hi[i] = P.hi[i];

@@ -88,7 +88,7 @@ struct Ctx {
     cudaStream_t own = nullptr; // stream of host-memory calls
     cudaEvent_t ev[8] = {};
     // host-mode copies
-    DevBuf hpos, hvel, hmass, hconn, hfield[6];
+    DevBuf hpos, hvel, hmass, hconn, hfield[6], hgpos, hgmass;
     // items
     DevBuf iframe, ielem, ipid, ikey;
     DevBuf key_sorted, order_in, order;
@@ -99,7 +99,7 @@ struct Ctx {
     DevBuf rkey, rmom, rkey_sorted, rperm_in, rperm, rvox, ritem, rmom_sorted, run_vox, run_cnt, run_off;
     std::vector<DevBuf*> all()
     {
-        return {&hpos, &hpos, &hvel, &hmass, &hconn, &hfield[0], &hfield[1], &hfield[2], &hfield[3], &hfield[4],
+        return {&hpos, &hgpos, &hgmass, &hvel, &hmass, &hconn, &hfield[0], &hfield[1], &hfield[2], &hfield[3], &hfield[4],
                 &hfield[5], &iframe, &ielem, &ipid, &ikey,
                 &key_sorted, &order_in, &order, &counts, &offsets, &cub_tmp, &scratch, &scratch_big, &iscale, &small, &rkey, &rmom,
                 &rkey_sorted, &rperm_in, &rperm, &rvox, &ritem, &rmom_sorted, &run_vox, &run_cnt, &run_off};
@@ -171,6 +171,9 @@ struct Call {
     double* F[6];
     const double *pos, *vel, *mass;
     const int* conn;
+    // adjoint call: F[0] holds dL/dm; gradients accumulate into these
+    bool adjoint;
+    double *gpos, *gmass;
 };
 
 int check_status(Call& c, unsigned long long* small_host)
@@ -199,7 +202,9 @@ int run_device(Call& c)
     if (c.F[4]) flags |= F_XV;
     if (c.F[5]) flags |= F_VV;
     const int order = (flags & (F_XX | F_XV | F_VV)) ? 2 : (flags & (F_X | F_V)) ? 1 : 0;
-    const bool mixed = c.precision == PSIB_MIXED;
+    const bool mixed = c.precision == PSIB_MIXED && !c.adjoint;
+    // central-form records: the mixed kernel, or the FP64 walk in PSIB_FP64_CENTRAL
+    const bool central = (mixed || c.precision == PSIB_FP64_CENTRAL) && !c.adjoint;
     // 1, 4 or 10 moments per record (FP32 kernel: m0, q-centroid, central second moment)
     const int nmom = order == 2 ? 10 : order == 1 ? 4 : 1;
 
@@ -305,7 +310,7 @@ int run_device(Call& c)
     RET(ensure(C.key_sorted, (size_t)cap * sizeof(uint16_t)));
     RET(ensure(C.order_in, (size_t)cap * sizeof(int)));
     RET(ensure(C.order, (size_t)cap * sizeof(int)));
-    if (mixed) RET(ensure(C.iscale, (size_t)cap * sizeof(double)));
+    if (central) RET(ensure(C.iscale, (size_t)cap * sizeof(double)));
     ItemArrays it;
     it.frame = C.iframe.as<double>();
     it.elem = C.ielem.as<int>();
@@ -317,9 +322,11 @@ int run_device(Call& c)
     // persistent clip kernels: one resident wave, each thread with its own scratch region
     const int clip_block = 128, big_block = 64;
     const int clip_grid =
-        C.num_sms * (mixed ? clip_blocks_per_sm_mixed(false, clip_block) : clip_blocks_per_sm_fp64(false, clip_block));
-    const size_t main_bytes = mixed ? scratch_bytes_mixed(false) : scratch_bytes_fp64(false);
-    const size_t big_bytes = mixed ? scratch_bytes_mixed(true) : scratch_bytes_fp64(true);
+        C.num_sms * (c.adjoint ? adjoint_blocks_per_sm(false, clip_block)
+                     : central ? clip_blocks_per_sm_mixed(false, !mixed, clip_block)
+                               : clip_blocks_per_sm_fp64(false, clip_block));
+    const size_t main_bytes = central ? scratch_bytes_mixed(false, !mixed) : scratch_bytes_fp64(false);
+    const size_t big_bytes = central ? scratch_bytes_mixed(true, !mixed) : scratch_bytes_fp64(true);
     RET(ensure(C.scratch, main_bytes * (size_t)clip_grid * clip_block));
 
     ClipArgs ca = {};
@@ -332,7 +339,14 @@ int run_device(Call& c)
     ca.rec_nmom = nmom;
     ca.rec_n = &sm[S_RECN];
     ca.rec_item_base = 0;
-    ca.scale = mixed ? C.iscale.as<double>() : nullptr;
+    ca.scale = central ? C.iscale.as<double>() : nullptr;
+    if (c.adjoint) {
+        ca.adj_gm = c.F[0];
+        ca.adj_gpos = c.gpos;
+        ca.adj_npart = m.npart;
+        ca.adj_gmass = c.gmass;
+        ca.adj_mass_factor = m.elemtype == 8 ? 1.0 / 6.0 : 1.0;
+    }
 
     float ms_clip = 0.f, ms_tess = 0.f, ms_final = 0.f;
     unsigned long long clip_counts[3] = {0, 0, 0}; // fragments, fragment vertices, splits
@@ -373,6 +387,41 @@ int run_device(Call& c)
             ms_tess += t;
         }
 
+        if (c.adjoint) {
+            // ---- adjoint: walk the fragments again and pull dL/dm back to the particles ----
+            CK(cudaMemsetAsync(&sm[S_CNT], 0, 24, st));
+            CK(cudaMemsetAsync(&sm[S_HEAD], 0, 16, st));
+            CK(cudaEventRecord(C.ev[4], st));
+            if (nmain > 0) {
+                ca.scratch = C.scratch.p;
+                ca.order_base = 0;
+                ca.n = nmain;
+                ca.head = &sm[S_HEAD];
+                CK(launch_adjoint(ca, false, clip_grid, clip_block, st));
+                launches++;
+            }
+            if (ndeep > 0) {
+                const int big_grid = (int)std::min<long long>(
+                    (long long)C.num_sms * adjoint_blocks_per_sm(true, big_block), (ndeep + big_block - 1) / big_block);
+                RET(ensure(C.scratch_big, big_bytes * (size_t)big_grid * big_block));
+                ca.scratch = C.scratch_big.p;
+                ca.order_base = nmain;
+                ca.n = ndeep;
+                ca.head = &sm[S_HEAD + 1];
+                CK(launch_adjoint(ca, true, big_grid, big_block, st));
+                launches++;
+            }
+            CK(cudaEventRecord(C.ev[5], st));
+            unsigned long long h[S_WORDS];
+            CK(cudaMemcpyAsync(h, sm, sizeof(h), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            float t = 0.f;
+            CK(cudaEventElapsedTime(&t, C.ev[4], C.ev[5]));
+            ms_clip += t;
+            RET(check_status(c, h));
+            for (int w = 0; w < 3; ++w) clip_counts[w] += h[S_CNT + w];
+            continue;
+        }
         // ---- clip to fragment records; grow the record buffer and redo if it overflowed ----
         int ibits = 1, vbits = 1;
         while ((1ll << ibits) < nitems) ++ibits;
@@ -396,7 +445,7 @@ int run_device(Call& c)
                 ca.order_base = 0;
                 ca.n = nmain;
                 ca.head = &sm[S_HEAD];
-                if (mixed) CK(launch_clip_mixed(ca, false, clip_grid, clip_block, st));
+                if (central) CK(launch_clip_mixed(ca, false, !mixed, clip_grid, clip_block, st));
                 else CK(launch_clip_fp64(ca, false, clip_grid, clip_block, st));
                 launches++;
             }
@@ -407,7 +456,7 @@ int run_device(Call& c)
                 ca.order_base = nmain;
                 ca.n = ndeep;
                 ca.head = &sm[S_HEAD + 1];
-                if (mixed) CK(launch_clip_mixed(ca, true, big_grid, big_block, st));
+                if (central) CK(launch_clip_mixed(ca, true, !mixed, big_grid, big_block, st));
                 else CK(launch_clip_fp64(ca, true, big_grid, big_block, st));
                 launches++;
             }
@@ -491,7 +540,7 @@ int run_device(Call& c)
             aa.item = C.ritem.as<unsigned>();
             aa.mom = C.rmom_sorted.as<double>();
             aa.nmom = nmom;
-            aa.central = mixed;
+            aa.central = central;
             aa.scale = ca.scale;
             aa.it = it;
             aa.item_base = 0;
@@ -530,6 +579,32 @@ int run_device(Call& c)
     return PSIB_OK;
 }
 
+// Host-memory calls: copy the mesh to the context's device buffers.
+int copy_mesh_in(Call& c, Ctx& C, const psib_mesh& mesh, cudaStream_t st)
+{
+    const size_t np3 = (size_t)mesh.npart * 3 * sizeof(double);
+    RET(ensure(C.hpos, np3));
+    CK(cudaMemcpyAsync(C.hpos.p, mesh.pos, np3, cudaMemcpyHostToDevice, st));
+    c.pos = C.hpos.as<double>();
+    if (mesh.vel) {
+        RET(ensure(C.hvel, np3));
+        CK(cudaMemcpyAsync(C.hvel.p, mesh.vel, np3, cudaMemcpyHostToDevice, st));
+        c.vel = C.hvel.as<double>();
+    }
+    if (mesh.mass) {
+        RET(ensure(C.hmass, (size_t)mesh.nelem * sizeof(double)));
+        CK(cudaMemcpyAsync(C.hmass.p, mesh.mass, (size_t)mesh.nelem * sizeof(double), cudaMemcpyHostToDevice, st));
+        c.mass = C.hmass.as<double>();
+    }
+    if (mesh.connectivity) {
+        const size_t cb = (size_t)mesh.nelem * mesh.elemtype * sizeof(int);
+        RET(ensure(C.hconn, cb));
+        CK(cudaMemcpyAsync(C.hconn.p, mesh.connectivity, cb, cudaMemcpyHostToDevice, st));
+        c.conn = C.hconn.as<int>();
+    }
+    return PSIB_OK;
+}
+
 int validate(const psib_grid* g, const psib_mesh* m, int mode, const psib_options* o)
 {
     if (!g || !m) return fail(PSIB_ERR_ARG, "grid and mesh are required");
@@ -563,7 +638,7 @@ int validate(const psib_grid* g, const psib_mesh* m, int mode, const psib_option
         }
         if (np != m->npart || nel != m->nelem) return fail(PSIB_ERR_ARG, "block_dims disagree with npart/nelem");
     }
-    if (o && o->precision != PSIB_FP64 && o->precision != PSIB_MIXED)
+    if (o && o->precision != PSIB_FP64 && o->precision != PSIB_MIXED && o->precision != PSIB_FP64_CENTRAL)
         return fail(PSIB_ERR_ARG, "invalid precision %d", o->precision);
     return PSIB_OK;
 }
@@ -670,28 +745,7 @@ int psib_voxels(const psib_grid* grid, const psib_mesh* mesh, int mode, double r
     cudaStream_t st = C->own;
     c.st = st;
     CK(cudaEventRecord(C->ev[0], st));
-    const size_t np3 = (size_t)mesh->npart * 3 * sizeof(double);
-    if (mesh->nelem > 0) {
-        RET(ensure(C->hpos, np3));
-        CK(cudaMemcpyAsync(C->hpos.p, mesh->pos, np3, cudaMemcpyHostToDevice, st));
-        c.pos = C->hpos.as<double>();
-        if (mesh->vel) {
-            RET(ensure(C->hvel, np3));
-            CK(cudaMemcpyAsync(C->hvel.p, mesh->vel, np3, cudaMemcpyHostToDevice, st));
-            c.vel = C->hvel.as<double>();
-        }
-        if (mesh->mass) {
-            RET(ensure(C->hmass, (size_t)mesh->nelem * sizeof(double)));
-            CK(cudaMemcpyAsync(C->hmass.p, mesh->mass, (size_t)mesh->nelem * sizeof(double), cudaMemcpyHostToDevice, st));
-            c.mass = C->hmass.as<double>();
-        }
-        if (mesh->connectivity) {
-            const size_t cb = (size_t)mesh->nelem * mesh->elemtype * sizeof(int);
-            RET(ensure(C->hconn, cb));
-            CK(cudaMemcpyAsync(C->hconn.p, mesh->connectivity, cb, cudaMemcpyHostToDevice, st));
-            c.conn = C->hconn.as<int>();
-        }
-    }
+    if (mesh->nelem > 0) RET(copy_mesh_in(c, *C, *mesh, st));
     for (int f = 0; f < 6; ++f) {
         if (!grid->fields[f]) continue;
         const size_t b = (size_t)nvox * comps[f] * sizeof(double);
@@ -705,6 +759,87 @@ int psib_voxels(const psib_grid* grid, const psib_mesh* mesh, int mode, double r
         const size_t b = (size_t)nvox * comps[f] * sizeof(double);
         CK(cudaMemcpyAsync(grid->fields[f], c.F[f], b, cudaMemcpyDeviceToHost, st));
     }
+    CK(cudaEventRecord(C->ev[7], st));
+    CK(cudaEventSynchronize(C->ev[7]));
+    if (o.stats) CK(cudaEventElapsedTime(&o.stats->ms_total, C->ev[0], C->ev[7]));
+    return PSIB_OK;
+}
+
+int psib_voxels_adjoint(const psib_grid* grad, const psib_mesh* mesh, double refine_tolerance, int refine_max_lvl,
+                        double* grad_pos, double* grad_vel, double* grad_mass, const psib_options* opt)
+{
+    g_err.clear();
+    psib_options o = {};
+    o.precision = PSIB_FP64;
+    o.memory = PSIB_HOST;
+    o.device = -1;
+    if (opt) o = *opt;
+    RET(validate(grad, mesh, PSIB_MODE_DENSITY, &o));
+    for (int f = 1; f < 6; ++f)
+        if (grad->fields[f])
+            return fail(PSIB_ERR_UNSUPPORTED, "the adjoint takes the gradient of field m only");
+    if (refine_max_lvl > 0 && mesh->elemtype == 8)
+        return fail(PSIB_ERR_UNSUPPORTED, "the adjoint supports refine_max_lvl = 0 only");
+    if (!grad_pos && mesh->nelem > 0) return fail(PSIB_ERR_ARG, "grad_pos is required");
+    (void)grad_vel; // the density does not depend on the velocities
+    if (psib_device_count() <= 0) return fail(PSIB_ERR_NODEVICE, "no CUDA device is visible");
+    int dev = o.device;
+    if (o.memory == PSIB_DEVICE || dev < 0) CK(cudaGetDevice(&dev));
+    CK(cudaSetDevice(dev));
+    Ctx* C = nullptr;
+    RET(get_ctx(dev, &C));
+
+    Call c = {};
+    c.grid = grad;
+    c.mesh = mesh;
+    c.reftol = refine_tolerance;
+    c.maxlvl = 0;
+    c.precision = PSIB_FP64;
+    c.C = C;
+    c.stats = o.stats;
+    c.adjoint = true;
+    if (o.stats) *o.stats = psib_stats{};
+    if (mesh->nelem == 0) return PSIB_OK;
+
+    const long long nvox = (long long)grad->n[0] * grad->n[1] * grad->n[2];
+    if (o.memory == PSIB_DEVICE) {
+        c.st = (cudaStream_t)o.stream;
+        c.F[0] = grad->fields[0];
+        c.pos = mesh->pos;
+        c.vel = mesh->vel;
+        c.mass = mesh->mass;
+        c.conn = mesh->connectivity;
+        c.gpos = grad_pos;
+        c.gmass = grad_mass;
+        CK(cudaEventRecord(C->ev[0], c.st));
+        RET(run_device(c));
+        if (o.stats) {
+            CK(cudaEventRecord(C->ev[7], c.st));
+            CK(cudaEventSynchronize(C->ev[7]));
+            CK(cudaEventElapsedTime(&o.stats->ms_total, C->ev[0], C->ev[7]));
+        }
+        return PSIB_OK;
+    }
+    cudaStream_t st = C->own;
+    c.st = st;
+    CK(cudaEventRecord(C->ev[0], st));
+    RET(copy_mesh_in(c, *C, *mesh, st));
+    RET(ensure(C->hfield[0], (size_t)nvox * sizeof(double)));
+    CK(cudaMemcpyAsync(C->hfield[0].p, grad->fields[0], (size_t)nvox * sizeof(double), cudaMemcpyHostToDevice, st));
+    c.F[0] = C->hfield[0].as<double>();
+    const size_t gpb = (size_t)mesh->npart * 3 * sizeof(double);
+    RET(ensure(C->hgpos, gpb));
+    CK(cudaMemcpyAsync(C->hgpos.p, grad_pos, gpb, cudaMemcpyHostToDevice, st));
+    c.gpos = C->hgpos.as<double>();
+    if (grad_mass) {
+        RET(ensure(C->hgmass, (size_t)mesh->nelem * sizeof(double)));
+        CK(cudaMemcpyAsync(C->hgmass.p, grad_mass, (size_t)mesh->nelem * sizeof(double), cudaMemcpyHostToDevice, st));
+        c.gmass = C->hgmass.as<double>();
+    }
+    RET(run_device(c));
+    CK(cudaMemcpyAsync(grad_pos, c.gpos, gpb, cudaMemcpyDeviceToHost, st));
+    if (grad_mass)
+        CK(cudaMemcpyAsync(grad_mass, c.gmass, (size_t)mesh->nelem * sizeof(double), cudaMemcpyDeviceToHost, st));
     CK(cudaEventRecord(C->ev[7], st));
     CK(cudaEventSynchronize(C->ev[7]));
     if (o.stats) CK(cudaEventElapsedTime(&o.stats->ms_total, C->ev[0], C->ev[7]));

@@ -572,6 +572,7 @@ static PyObject *PSI_voxels(PyObject *self, PyObject *args, PyObject *kwds)
     int prec;
     if (strcmp(precstr, "fp64") == 0) prec = PSIB_FP64;
     else if (strcmp(precstr, "mixed") == 0) prec = PSIB_MIXED;
+    else if (strcmp(precstr, "fp64-central") == 0) prec = PSIB_FP64_CENTRAL;
     else {
         PyErr_Format(PyExc_ValueError, "Invalid precision for PSI.voxels(): %s", precstr);
         return NULL;

@@ -29,17 +29,21 @@
 
 namespace psib {
 
-// Per-thread scratch region: NS polyhedron slots, then (FP32 kernels) two
-// FP64 polyhedra for the window clip.  Both parts start on 16-byte boundaries.
+// Per-thread scratch region: NS polyhedron slots, then (FP32 kernels) the
+// FP64 leaf fragment and two FP64 polyhedra for the window clip.  Every part
+// starts on a 16-byte boundary.
 __host__ __device__ constexpr size_t round16(size_t b) { return (b + 15) & ~(size_t)15; }
 
 template <class R, int NS>
-__host__ __device__ constexpr size_t wclip_offset() { return round16(sizeof(Poly<R>) * NS); }
+__host__ __device__ constexpr size_t leaf_offset() { return round16(sizeof(Poly<R>) * NS); }
+
+template <class R, int NS>
+__host__ __device__ constexpr size_t wclip_offset() { return leaf_offset<R, NS>() + round16(sizeof(QPoly)); }
 
 template <class R, int NS>
 __host__ __device__ constexpr size_t region_bytes()
 {
-    return wclip_offset<R, NS>() + (sizeof(R) == 4 ? round16(2 * sizeof(Poly<double>)) : 0);
+    return sizeof(R) == 4 ? wclip_offset<R, NS>() + round16(2 * sizeof(Poly<double>)) : leaf_offset<R, NS>();
 }
 
 __device__ __forceinline__ void aabb4(const double (*p)[3], double (*rb)[3])
@@ -73,13 +77,17 @@ __device__ __forceinline__ void write_record(const ClipArgs& a, long long gi, lo
     }
 }
 
-// Voxelize item t.  S points to NS polyhedron slots owned by this thread,
-// WC to two FP64 polyhedra (FP32 kernel only).  CENTRAL: write centroid-form
+// Voxelize item t.  S points to NS polyhedron slots owned by this thread;
+// FP32 kernel only: QL to the FP64 leaf fragment, WC to two FP64 polyhedra.  CENTRAL: write centroid-form
 // records (always so in the FP32 kernel; the FP64 kernel does it when it
-// serves the mixed-precision mode).
-template <class R, int NS, bool CENTRAL>
-__device__ void clip_item(const ClipArgs& a, long long t, Poly<R>* S, Poly<double>* WC, unsigned& st, Tally& tally)
+// serves the mixed-precision mode).  ADJ (FP64 only): instead of writing
+// records, pull the upstream gradient of the m field back to the positions of
+// the image's four particles (and to its element's mass).
+template <class R, int NS, bool CENTRAL, bool ADJ = false>
+__device__ void clip_item(const ClipArgs& a, long long t, Poly<R>* S, QPoly* QL, Poly<double>* WC, unsigned& st,
+                          Tally& tally)
 {
+    static_assert(!ADJ || (sizeof(R) == 8 && !CENTRAL), "the adjoint walks the FP64 fragments");
     const double* fr = a.it.frame + t * FRAME;
     double p[4][3];
     for (int v = 0; v < 4; ++v)
@@ -149,7 +157,7 @@ __device__ void clip_item(const ClipArgs& a, long long t, Poly<R>* S, Poly<doubl
                 }
                 if (smin >= 0.0) continue;
                 if (smax <= 0.0) { W[cw]->nv = 0; break; }
-                const unsigned e = cut_poly<double, false>(*W[cw], sd, um, *W[1 - cw], *W[1 - cw]);
+                const unsigned e = cut_poly<double, false>(*W[cw], sd, um, *W[1 - cw], *W[1 - cw], axis_tag(ax));
                 if (e) { st |= e; return; }
                 cw = 1 - cw;
             }
@@ -163,10 +171,7 @@ __device__ void clip_item(const ClipArgs& a, long long t, Poly<R>* S, Poly<doubl
             P.nv = Q.nv;
             for (int v = 0; v < P.nv; ++v) {
                 P.nb[v] = Q.nb[v];
-                for (int i = 0; i < 3; ++i) {
-                    P.x[v][i] = (R)(Q.x[v][i] - org[i]);
-                    P.q[v][i] = (R)Q.q[v][i];
-                }
+                for (int i = 0; i < 3; ++i) P.x[v][i] = (R)(Q.x[v][i] - org[i]);
             }
         }
     }
@@ -198,7 +203,7 @@ __device__ void clip_item(const ClipArgs& a, long long t, Poly<R>* S, Poly<doubl
         if (smax <= (R)0) { P.nv = 0; break; }
         int o;
         PSIB_ALLOC(o);
-        const unsigned e = cut_poly<R, false>(P, s, um, S[o], S[o]);
+        const unsigned e = cut_poly<R, false>(P, s, um, S[o], S[o], axis_tag(ax));
         PSIB_FREE(c);
         c = o;
         if (e) { st |= e; return; }
@@ -207,6 +212,9 @@ __device__ void clip_item(const ClipArgs& a, long long t, Poly<R>* S, Poly<doubl
 
     double mom[10];
     const int order = a.mom_order;
+    // adjoint accumulators: sum over fragments of g dS(P)/dx_i, and of g m0
+    double A[4][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+    double B = 0.0;
     for (;;) {
         Poly<R>& P = S[c];
         bool done_node = true;
@@ -219,18 +227,44 @@ __device__ void clip_item(const ClipArgs& a, long long t, Poly<R>* S, Poly<doubl
             if (dmax <= 1) {
                 // a single voxel (src/geometry.c:873-884)
                 double o[3] = {0.0, 0.0, 0.0};
-                if constexpr (CENTRAL)
+                if constexpr (CENTRAL && sizeof(R) == 8)
                     for (int i = 0; i < 3; ++i) o[i] = (double)P.q[0][i];
-                const unsigned e = CENTRAL ? reduce_about(P, o, mom, order) : reduce_poly(P, mom, order);
+                if constexpr (sizeof(R) == 4) {
+                    // the FP32 walk fixed the fragment's graph; its vertices are
+                    // recomputed in FP64 from their planes before the moments
+                    double plo[3], phi[3], tol[3];
+                    for (int i = 0; i < 3; ++i) {
+                        plo[i] = a.g.d[i] * P.lo[i] + a.g.w0[i];
+                        phi[i] = a.g.d[i] * (P.lo[i] + 1) + a.g.w0[i];
+                        tol[i] = 1.0e-3 * a.g.d[i];
+                    }
+                    exact_vertices(P, p, org, plo, phi, tol, *QL);
+                    for (int i = 0; i < 3; ++i) o[i] = QL->q[0][i];
+                }
+                double gv = 0.0;
+                if constexpr (ADJ) {
+                    if (P.lo[0] < a.g.n[0] && P.lo[1] < a.g.n[1] && P.lo[2] < a.g.n[2])
+                        gv = a.adj_gm[((long long)a.g.n[1] * P.lo[0] + P.lo[1]) * a.g.n[2] + P.lo[2]];
+                }
+                unsigned e;
+                if constexpr (ADJ) e = gv != 0.0 ? reduce_poly(P, mom, 0) : 0u;
+                else if constexpr (sizeof(R) == 4) e = reduce_about(*QL, o, mom, order);
+                else e = CENTRAL ? reduce_about(P, o, mom, order) : reduce_poly(P, mom, order);
                 if (e) { st |= e; return; }
-                if (mom[0] > 0.0) {
+                if (ADJ && gv == 0.0) {
+                    // no upstream gradient in this voxel: nothing to pull back
+                } else if (mom[0] > 0.0) {
                     if (P.lo[0] >= a.g.n[0] || P.lo[1] >= a.g.n[1] || P.lo[2] >= a.g.n[2]) {
                         st |= ST_INDEX;
                     } else {
                         const long long gi = ((long long)a.g.n[1] * P.lo[0] + P.lo[1]) * a.g.n[2] + P.lo[2];
                         tally.frags++;
                         tally.verts += P.nv;
-                        if constexpr (CENTRAL) {
+                        if constexpr (ADJ) {
+                            const unsigned e2 = adjoint_poly(P, gv, A);
+                            if (e2) { st |= e2; return; }
+                            B += gv * mom[0];
+                        } else if constexpr (CENTRAL) {
                             // m0, q-centroid, central q second moment (xx xy xz yy yz zz)
                             vsum += mom[0];
                             double rec[10];
@@ -272,7 +306,7 @@ __device__ void clip_item(const ClipArgs& a, long long t, Poly<R>* S, Poly<doubl
                     int l, r;
                     PSIB_ALLOC(l);
                     PSIB_ALLOC(r);
-                    const unsigned e = cut_poly<R, true>(P, s, um, S[l], S[r]);
+                    const unsigned e = cut_poly<R, true>(P, s, um, S[l], S[r], axis_tag(ax));
                     if (e) { st |= e; return; }
                     for (int i = 0; i < 3; ++i) {
                         S[l].lo[i] = P.lo[i]; S[l].hi[i] = P.hi[i];
@@ -293,6 +327,36 @@ __device__ void clip_item(const ClipArgs& a, long long t, Poly<R>* S, Poly<doubl
         if (top == 0) break;
         c = stk[--top];
     }
+    if constexpr (ADJ) {
+        // d m0 / dx_i = (dS(P)/dx_i - m0 dS(T)/dx_i) / S(T), times the image's mass
+        if (B != 0.0 || A[0][0] != 0.0 || A[0][1] != 0.0 || A[0][2] != 0.0 || A[1][0] != 0.0 || A[1][1] != 0.0 ||
+            A[1][2] != 0.0 || A[2][0] != 0.0 || A[2][1] != 0.0 || A[2][2] != 0.0 || A[3][0] != 0.0 ||
+            A[3][1] != 0.0 || A[3][2] != 0.0) {
+            double e[3][3];
+            for (int v = 0; v < 3; ++v)
+                for (int i = 0; i < 3; ++i) e[v][i] = p[v + 1][i] - p[0][i];
+            double dS[4][3];
+            for (int v = 0; v < 3; ++v) {
+                const double* u = e[(v + 1) % 3];
+                const double* w = e[(v + 2) % 3];
+                dS[v + 1][0] = (u[1] * w[2] - u[2] * w[1]) * (1.0 / 6.0);
+                dS[v + 1][1] = (u[2] * w[0] - u[0] * w[2]) * (1.0 / 6.0);
+                dS[v + 1][2] = (u[0] * w[1] - u[1] * w[0]) * (1.0 / 6.0);
+            }
+            for (int i = 0; i < 3; ++i) dS[0][i] = -(dS[1][i] + dS[2][i] + dS[3][i]);
+            const double sT = e[0][0] * dS[1][0] + e[0][1] * dS[1][1] + e[0][2] * dS[1][2];
+            const double mass = fr[FR_MASS];
+            if (sT != 0.0) {
+                const double f = mass / sT;
+                for (int v = 0; v < 4; ++v) {
+                    const int pid = a.it.pid[v * a.it.cap + t];
+                    if (pid < 0 || pid >= a.adj_npart) { st |= ST_INDEX; continue; }
+                    for (int i = 0; i < 3; ++i) atomicAdd(&a.adj_gpos[3 * (long long)pid + i], f * (A[v][i] - B * dS[v][i]));
+                }
+            }
+            if (a.adj_gmass) atomicAdd(&a.adj_gmass[a.it.elem[t]], B * a.adj_mass_factor);
+        }
+    }
     if constexpr (sizeof(R) == 4) {
         // FP32 fragments miss the exact q-volume by O(1e-7): the apply kernel
         // scales this image's fragment masses by target / vsum.
@@ -305,13 +369,14 @@ __device__ void clip_item(const ClipArgs& a, long long t, Poly<R>* S, Poly<doubl
 }
 
 // Persistent kernel body: warps take 32 consecutive queue entries at a time.
-template <class R, int NS, bool CENTRAL>
+template <class R, int NS, bool CENTRAL, bool ADJ = false>
 __device__ __forceinline__ void clip_loop(const ClipArgs& a)
 {
     const int lane = threadIdx.x & 31;
     const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     char* region = (char*)a.scratch + tid * region_bytes<R, NS>();
     Poly<R>* S = (Poly<R>*)region;
+    QPoly* QL = (QPoly*)(region + leaf_offset<R, NS>());
     Poly<double>* WC = (Poly<double>*)(region + wclip_offset<R, NS>());
     unsigned st = 0;
     Tally tally;
@@ -323,7 +388,7 @@ __device__ __forceinline__ void clip_loop(const ClipArgs& a)
         const long long i = (long long)base + lane;
         if (i < a.n) {
             const long long t = a.order ? (long long)a.order[a.order_base + i] : a.order_base + i;
-            clip_item<R, NS, CENTRAL>(a, t, S, WC, st, tally);
+            clip_item<R, NS, CENTRAL, ADJ>(a, t, S, QL, WC, st, tally);
         }
     }
     if (st) atomicOr(a.status, st);

@@ -16,8 +16,10 @@
 // vertices in order, then cut vertices in creation order), and the moment sums
 // run over the same fan triangles in the same order.  Compiled without FMA
 // contraction (--fmad=false) and with R = double this reproduces the
-// reference's fragment moments bit for bit; R = float gives the mixed-precision
-// kernel (FP32 plane distances and interpolation, FP64 moments).
+// reference's fragment moments bit for bit.  R = float gives the walk of the
+// mixed-precision kernel: FP32 positions, plane distances and cuts and no q
+// at all; at each leaf the fragment's vertices are recomputed in FP64 from the
+// planes they lie on (exact_vertices) and its moments taken in FP64.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -43,11 +45,29 @@ enum : unsigned {
 
 template <class R>
 struct Poly {
+    static constexpr bool has_q = true;
     R x[MAXV][3];      // position
     R q[MAXV][3];      // barycentric mass coordinate
-    uint32_t nb[MAXV]; // neighbour links: bits 0-7, 8-15, 16-23
+    uint32_t nb[MAXV]; // neighbour links: bits 0-7, 8-15, 16-23; bits 24-30: plane tags
     int nv;
     int lo[3], hi[3];  // voxel index box
+};
+
+// The FP32 walk carries positions and links only (q is rebuilt at the leaf).
+template <>
+struct Poly<float> {
+    static constexpr bool has_q = false;
+    float x[MAXV][3];
+    uint32_t nb[MAXV];
+    int nv;
+    int lo[3], hi[3];
+};
+
+// A fragment for the moment sums: FP64 q and links.
+struct QPoly {
+    double q[MAXV][3];
+    uint32_t nb[MAXV];
+    int nv;
 };
 
 __device__ __forceinline__ int nbget(uint32_t w, int k) { return (w >> (8 * k)) & 0xFFu; }
@@ -56,6 +76,20 @@ __device__ __forceinline__ uint32_t nbset(uint32_t w, int k, int v)
     return (w & ~(0xFFu << (8 * k))) | ((uint32_t)v << (8 * k));
 }
 __device__ __forceinline__ int rank_in(uint32_t mask, int v) { return __popc(mask & ((1u << v) - 1u)); }
+
+// Plane tags of a vertex, in the top byte of its link word.  Bit 24 + j: the
+// vertex lies on the face of the original tet opposite its vertex j.  Bit
+// 28 + a: it lies on a grid (or window) plane normal to axis a.  A cut vertex
+// lies on the planes both ends of its edge lie on, plus the cutting plane, so
+// a cut ANDs the two tags and adds the cut's axis.  Generic vertices carry
+// exactly three tags.  The tags change no arithmetic: the adjoint uses them to
+// find the fragment faces that move with the tet's vertices, and the mixed
+// kernel to recompute each fragment vertex in FP64 from its three planes.
+constexpr uint32_t TAG_MASK = 0x0F000000u;   // tet faces
+constexpr uint32_t PLANE_MASK = 0x70000000u; // grid planes by axis
+constexpr uint32_t ALL_TAGS = TAG_MASK | PLANE_MASK;
+__device__ __forceinline__ uint32_t tags(uint32_t w) { return (w & TAG_MASK) >> 24; }
+__device__ __forceinline__ uint32_t axis_tag(int ax) { return 0x10000000u << ax; }
 
 // Close the cut face: each vertex created by a cut (index >= base) gets its
 // two remaining links by walking around the face it opened
@@ -86,7 +120,8 @@ __device__ __forceinline__ bool link_cut_vertices(Poly<R>& P, int base)
 // (a lower, b upper) is (b*s_a - a*s_b) / (s_a - s_b) in the reference's
 // operation order (src/geometry.c:441-445, :601-605).
 template <class R, bool BOTH>
-__device__ __forceinline__ unsigned cut_poly(const Poly<R>& in, const R* s, uint32_t umask, Poly<R>& lo, Poly<R>& up)
+__device__ __forceinline__ unsigned cut_poly(const Poly<R>& in, const R* s, uint32_t umask, Poly<R>& lo, Poly<R>& up,
+                                             uint32_t cut_tag)
 {
     const int n = in.nv;
     const uint32_t all = (1u << n) - 1u;
@@ -99,9 +134,11 @@ __device__ __forceinline__ unsigned cut_poly(const Poly<R>& in, const R* s, uint
         const uint32_t sm = u ? umask : lmask;
         const int j = rank_in(sm, v);
         o.x[j][0] = in.x[v][0]; o.x[j][1] = in.x[v][1]; o.x[j][2] = in.x[v][2];
-        o.q[j][0] = in.q[v][0]; o.q[j][1] = in.q[v][1]; o.q[j][2] = in.q[v][2];
+        if constexpr (Poly<R>::has_q) {
+            o.q[j][0] = in.q[v][0]; o.q[j][1] = in.q[v][1]; o.q[j][2] = in.q[v][2];
+        }
         const uint32_t w = in.nb[v];
-        uint32_t ow = 0xFFFFFFu;
+        uint32_t ow = 0xFFFFFFu | (w & ALL_TAGS);
         for (int k = 0; k < 3; ++k) {
             const int t = nbget(w, k);
             if (t >= n) return ST_GRAPH;
@@ -124,17 +161,24 @@ __device__ __forceinline__ unsigned cut_poly(const Poly<R>& in, const R* s, uint
             R px[3], pq[3];
             for (int i = 0; i < 3; ++i) {
                 px[i] = iw * (in.x[vn][i] * sc - in.x[vc][i] * sn);
-                pq[i] = iw * (in.q[vn][i] * sc - in.q[vc][i] * sn);
+                if constexpr (Poly<R>::has_q) pq[i] = iw * (in.q[vn][i] * sc - in.q[vc][i] * sn);
             }
             const int il = nl + k;
-            for (int i = 0; i < 3; ++i) { lo.x[il][i] = px[i]; lo.q[il][i] = pq[i]; }
-            lo.nb[il] = 0xFFFF00u | (uint32_t)jc;
+            const uint32_t tg = (w & in.nb[vn] & ALL_TAGS) | cut_tag;
+            for (int i = 0; i < 3; ++i) {
+                lo.x[il][i] = px[i];
+                if constexpr (Poly<R>::has_q) lo.q[il][i] = pq[i];
+            }
+            lo.nb[il] = 0xFFFF00u | (uint32_t)jc | tg;
             lo.nb[jc] = nbset(lo.nb[jc], np, il);
             if (BOTH) {
                 const int iu = nu + k;
                 const int jn = rank_in(umask, vn);
-                for (int i = 0; i < 3; ++i) { up.x[iu][i] = px[i]; up.q[iu][i] = pq[i]; }
-                up.nb[iu] = 0xFFFF00u | (uint32_t)jn;
+                for (int i = 0; i < 3; ++i) {
+                    up.x[iu][i] = px[i];
+                    if constexpr (Poly<R>::has_q) up.q[iu][i] = pq[i];
+                }
+                up.nb[iu] = 0xFFFF00u | (uint32_t)jn | tg;
                 const uint32_t wn = in.nb[vn];
                 const int kb = (nbget(wn, 0) == vc) ? 0 : (nbget(wn, 1) == vc) ? 1 : (nbget(wn, 2) == vc) ? 2 : 3;
                 if (kb == 3) return ST_GRAPH;
@@ -160,10 +204,11 @@ __device__ __forceinline__ void init_tet(PT& P, const T (*x)[3])
     P.nb[1] = 2u | (3u << 8) | (0u << 16);
     P.nb[2] = 0u | (3u << 8) | (1u << 16);
     P.nb[3] = 1u | (2u << 8) | (0u << 16);
+    for (int v = 0; v < 4; ++v) P.nb[v] |= (0xFu & ~(1u << v)) << 24;
     for (int v = 0; v < 4; ++v)
         for (int i = 0; i < 3; ++i) {
             P.x[v][i] = x[v][i];
-            P.q[v][i] = (v == i + 1) ? 1 : 0;
+            if constexpr (PT::has_q) P.q[v][i] = (v == i + 1) ? 1 : 0;
         }
     P.nv = 4;
 }
@@ -226,6 +271,77 @@ __device__ __forceinline__ unsigned reduce_poly(const PT& P, double* mom, int or
     return 0;
 }
 
+// Adjoint of a fragment's mass fraction with respect to the tet's vertex
+// positions.  The fraction is m0 = S(P) / S(T): the signed x-space volumes of
+// the fragment and of the tet, both in the orientation of the q-space fan
+// triangles.  When the tet's vertices move, only the fragment faces lying on
+// the tet's own faces move (voxel and window planes stay put), a point p of
+// such a face with velocity sum_i lambda_i(p) dx_i, so
+//   dS(P)/dx_i = sum over those faces of the integral of lambda_i dN
+//              = sum over their fan triangles of N lambda_i(centroid),
+// with N = (p1 - p0) x (p2 - p0) / 2 and lambda = (1 - qx - qy - qz, qx, qy, qz).
+// Adds g * dS(P)/dx_i to A[i].  A face lies on a tet face when all its vertices
+// carry that face's tag.
+template <class PT>
+__device__ __forceinline__ unsigned adjoint_poly(const PT& P, double g, double (*A)[3])
+{
+    uint64_t done[2] = {0ull, 0ull};
+    for (int vs = 0; vs < P.nv; ++vs)
+        for (int ks = 0; ks < 3; ++ks) {
+            const int b0 = 3 * vs + ks;
+            if ((done[b0 >> 6] >> (b0 & 63)) & 1ull) continue;
+            done[b0 >> 6] |= 1ull << (b0 & 63);
+            int vc = vs;
+            int vn = nbget(P.nb[vc], ks);
+            if (vn >= P.nv) return ST_GRAPH;
+            uint32_t ft = tags(P.nb[vs]);
+            uint32_t w = P.nb[vn];
+            int k = (nbget(w, 0) == vc) ? 0 : (nbget(w, 1) == vc) ? 1 : (nbget(w, 2) == vc) ? 2 : 3;
+            if (k == 3) return ST_GRAPH;
+            vc = vn;
+            int kn = (k + 1) % 3;
+            int b = 3 * vc + kn;
+            done[b >> 6] |= 1ull << (b & 63);
+            ft &= tags(w);
+            vn = nbget(P.nb[vc], kn);
+            double ns[3] = {0.0, 0.0, 0.0}, nq[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+            int steps = 0;
+            while (vn != vs) {
+                if (++steps > WALK_CAP || vn >= P.nv) return ST_GRAPH;
+                if (ft) {
+                    double e1[3], e2[3], qc[3];
+                    for (int i = 0; i < 3; ++i) {
+                        e1[i] = (double)P.x[vn][i] - (double)P.x[vs][i];
+                        e2[i] = (double)P.x[vc][i] - (double)P.x[vs][i];
+                        qc[i] = ((double)P.q[vs][i] + (double)P.q[vn][i] + (double)P.q[vc][i]) * (1.0 / 3.0);
+                    }
+                    const double n[3] = {0.5 * (e1[1] * e2[2] - e1[2] * e2[1]), 0.5 * (e1[2] * e2[0] - e1[0] * e2[2]),
+                                         0.5 * (e1[0] * e2[1] - e1[1] * e2[0])};
+                    for (int i = 0; i < 3; ++i) {
+                        ns[i] += n[i];
+                        for (int j = 0; j < 3; ++j) nq[i][j] += n[i] * qc[j];
+                    }
+                }
+                w = P.nb[vn];
+                ft &= tags(w);
+                k = (nbget(w, 0) == vc) ? 0 : (nbget(w, 1) == vc) ? 1 : (nbget(w, 2) == vc) ? 2 : 3;
+                if (k == 3) return ST_GRAPH;
+                vc = vn;
+                kn = (k + 1) % 3;
+                b = 3 * vc + kn;
+                done[b >> 6] |= 1ull << (b & 63);
+                vn = nbget(P.nb[vc], kn);
+            }
+            if (ft) {
+                for (int i = 0; i < 3; ++i) {
+                    A[0][i] += g * (ns[i] - nq[i][0] - nq[i][1] - nq[i][2]);
+                    for (int j = 0; j < 3; ++j) A[1 + j][i] += g * nq[i][j];
+                }
+            }
+        }
+    return 0;
+}
+
 // ---- per-fragment projection to physical moments (src/geometry.c:81-161) ----
 
 struct TetFrame {
@@ -268,101 +384,6 @@ __device__ __forceinline__ void second_moment(const double* mom, const double* o
 } // namespace psib
 
 namespace psib {
-
-// ---- one-sided cuts for the per-voxel path kernels ----
-//
-// A lane follows the bisection path from the tet's index box down to its own
-// voxel and keeps only the side of each split that contains that voxel.  The
-// kept half of a split is the same polyhedron, vertex for vertex, that the
-// reference's two-sided split produces for that child, so the fragment at the
-// end of the path equals the reference's bit for bit.
-
-constexpr int CAPV = 32; // vertex buffer of an in-place cut: kept vertices + cut vertices
-
-template <class R>
-struct Buf {
-    R x[CAPV][3];
-    R q[CAPV][3];
-    uint32_t nb[CAPV];
-    int nv;
-};
-
-__device__ __forceinline__ uint32_t low_mask(int n) { return n >= 32 ? 0xFFFFFFFFu : ((1u << n) - 1u); }
-
-// Keep the lower side (s >= 0, keep_upper == false) or the upper side (s < 0)
-// of a cut, in place.  The result lists the kept old vertices in order, then
-// the cut vertices in the reference's creation order (lower vertex ascending,
-// link ascending), exactly like the corresponding output of the two-sided
-// split (src/geometry.c:593-690) or of the window clip (:436-500).
-template <class R>
-__device__ __forceinline__ unsigned half_cut(Buf<R>& P, const R* s, uint32_t umask, bool keep_upper)
-{
-    const int n = P.nv;
-    const uint32_t lmask = low_mask(n) & ~umask;
-    const uint32_t kmask = keep_upper ? umask : lmask;
-    int nv = n;
-    for (int vc = 0; vc < n; ++vc) {
-        if (!((lmask >> vc) & 1u)) continue;
-        for (int np = 0; np < 3; ++np) {
-            const int vn = nbget(P.nb[vc], np);
-            if (vn >= n) return ST_GRAPH; // lower-vertex links are only rewritten after they are read
-            if (!((umask >> vn) & 1u)) continue;
-            if (nv >= CAPV) return ST_OVERFLOW;
-            const R sc = s[vc], sn = s[vn];
-            const R iw = R(1) / (sc - sn);
-            for (int i = 0; i < 3; ++i) {
-                P.x[nv][i] = iw * (P.x[vn][i] * sc - P.x[vc][i] * sn);
-                P.q[nv][i] = iw * (P.q[vn][i] * sc - P.q[vc][i] * sn);
-            }
-            if (!keep_upper) {
-                P.nb[nv] = 0xFFFF00u | (uint32_t)vc;
-                P.nb[vc] = nbset(P.nb[vc], np, nv);
-            } else {
-                P.nb[nv] = 0xFFFF00u | (uint32_t)vn;
-                const uint32_t wn = P.nb[vn];
-                const int kb = (nbget(wn, 0) == vc) ? 0 : (nbget(wn, 1) == vc) ? 1 : (nbget(wn, 2) == vc) ? 2 : 3;
-                if (kb == 3) return ST_GRAPH;
-                P.nb[vn] = nbset(wn, kb, nv);
-            }
-            ++nv;
-        }
-    }
-    // close the cut face, walking the kept side (src/geometry.c:459-482)
-    for (int vs = n; vs < nv; ++vs) {
-        int vc = vs, vn = nbget(P.nb[vs], 0);
-        int steps = 0;
-        do {
-            if (vn >= nv) return ST_GRAPH;
-            const uint32_t w = P.nb[vn];
-            const int k = (nbget(w, 0) == vc) ? 0 : (nbget(w, 1) == vc) ? 1 : (nbget(w, 2) == vc) ? 2 : 3;
-            if (k == 3 || ++steps > WALK_CAP) return ST_GRAPH;
-            vc = vn;
-            vn = nbget(P.nb[vc], (k + 1) % 3);
-        } while (vc < n);
-        P.nb[vs] = nbset(P.nb[vs], 2, vc);
-        P.nb[vc] = nbset(P.nb[vc], 1, vs);
-    }
-    // compact: kept old vertices, then the cut vertices, with links renumbered
-    const int nk = __popc(kmask);
-    for (int v = 0; v < nv; ++v) {
-        const bool keep = v >= n || ((kmask >> v) & 1u);
-        if (!keep) continue;
-        const int dst = v < n ? rank_in(kmask, v) : nk + (v - n);
-        uint32_t w = P.nb[v], ow = 0;
-        for (int k = 0; k < 3; ++k) {
-            const int t = nbget(w, k);
-            const int tt = t < n ? rank_in(kmask, t) : nk + (t - n);
-            ow |= (uint32_t)tt << (8 * k);
-        }
-        for (int i = 0; i < 3; ++i) {
-            P.x[dst][i] = P.x[v][i];
-            P.q[dst][i] = P.q[v][i];
-        }
-        P.nb[dst] = ow;
-    }
-    P.nv = nk + (nv - n);
-    return 0;
-}
 
 // Moments of a polyhedron about the q-space point o (order 0, 1 or 2): the
 // same fan triangles as reduce_poly, with every vertex taken relative to o.
@@ -422,6 +443,92 @@ __device__ __forceinline__ unsigned reduce_about(const PT& P, const double* o, d
             }
         }
     return 0;
+}
+
+// Recompute the vertices of an FP32 fragment in FP64 (mixed-precision kernel).
+// Each vertex is the intersection of the three planes its tags name, solved in
+// q-space: tet faces are q_j = 0 (j = 1..3) and qx + qy + qz = 1; the grid
+// plane x_a = c is (DX q)_a = c - x0_a with DX[a][j] = x_{j+1,a} - x_{0,a}.  Of
+// the two grid planes normal to axis a that bound the fragment's voxel
+// ([plo_a, phi_a]), the vertex lies on the nearer.  An axis tag only says "on
+// some plane normal to a": an edge from one such plane to another keeps the
+// tag after the AND, so a tag is kept only when the vertex lies within tol_a of
+// a bounding plane (FP32 positions are good to ~1e-5 of a voxel there).  The
+// tags always include the vertex's true planes; of four, the grid plane
+// farthest from the vertex is dropped.  A vertex whose tags do not name
+// three planes, or whose planes are singular, gets q = DX^-1 (x - x0) from its
+// FP32 position.  The links and tags are copied.
+// Solve n_i . q = b_i (i = 0..2) by Cramer's rule; false when singular.
+__device__ __forceinline__ bool solve3(const double (*n)[3], const double* b, double* q)
+{
+    const double c12[3] = {n[1][1] * n[2][2] - n[1][2] * n[2][1], n[1][2] * n[2][0] - n[1][0] * n[2][2],
+                           n[1][0] * n[2][1] - n[1][1] * n[2][0]};
+    const double c20[3] = {n[2][1] * n[0][2] - n[2][2] * n[0][1], n[2][2] * n[0][0] - n[2][0] * n[0][2],
+                           n[2][0] * n[0][1] - n[2][1] * n[0][0]};
+    const double c01[3] = {n[0][1] * n[1][2] - n[0][2] * n[1][1], n[0][2] * n[1][0] - n[0][0] * n[1][2],
+                           n[0][0] * n[1][1] - n[0][1] * n[1][0]};
+    const double det = n[0][0] * c12[0] + n[0][1] * c12[1] + n[0][2] * c12[2];
+    if (!(det != 0.0) || !isfinite(det)) return false;
+    const double id = 1.0 / det;
+    for (int i = 0; i < 3; ++i) q[i] = (b[0] * c12[i] + b[1] * c20[i] + b[2] * c01[i]) * id;
+    return true;
+}
+
+__device__ __forceinline__ void exact_vertices(const Poly<float>& P, const double (*p)[3], const double* org,
+                                               const double* plo, const double* phi, const double* tol,
+                                               QPoly& Q)
+{
+    double DX[3][3];
+    for (int a = 0; a < 3; ++a)
+        for (int j = 0; j < 3; ++j) DX[a][j] = p[j + 1][a] - p[0][a];
+    Q.nv = P.nv;
+    for (int v = 0; v < P.nv; ++v) {
+        const uint32_t w = P.nb[v];
+        Q.nb[v] = w;
+        const uint32_t tf = (w >> 24) & 0xFu;
+        uint32_t ap = 0;
+        double pc[3], dist[3];
+        for (int a = 0; a < 3; ++a)
+            if ((w >> (28 + a)) & 1u) {
+                const double xv = (double)P.x[v][a] + org[a];
+                const double dl = fabs(xv - plo[a]), dh = fabs(xv - phi[a]);
+                pc[a] = dl <= dh ? plo[a] : phi[a];
+                dist[a] = (dl <= dh ? dl : dh) / tol[a];
+                if (dist[a] <= 1.0) ap |= 1u << a;
+            }
+        // a vertex near the edge or corner of its voxel can keep a fourth tag:
+        // the tet-face tags are exact, so drop the farthest grid plane
+        while (__popc(tf) + __popc(ap) > 3 && ap) {
+            int far = -1;
+            for (int a = 0; a < 3; ++a)
+                if (((ap >> a) & 1u) && (far < 0 || dist[a] > dist[far])) far = a;
+            ap &= ~(1u << far);
+        }
+        double n[3][3], b[3], q[3];
+        bool ok = __popc(tf) + __popc(ap) == 3;
+        if (ok) {
+            int r = 0;
+            if (tf & 1u) { n[r][0] = 1.0; n[r][1] = 1.0; n[r][2] = 1.0; b[r] = 1.0; ++r; }
+            for (int j = 0; j < 3; ++j)
+                if ((tf >> (j + 1)) & 1u) {
+                    n[r][0] = j == 0; n[r][1] = j == 1; n[r][2] = j == 2; b[r] = 0.0; ++r;
+                }
+            for (int a = 0; a < 3; ++a)
+                if ((ap >> a) & 1u) {
+                    n[r][0] = DX[a][0]; n[r][1] = DX[a][1]; n[r][2] = DX[a][2]; b[r] = pc[a] - p[0][a]; ++r;
+                }
+            ok = solve3(n, b, q);
+        }
+        if (!ok) {
+            // position -> q through the tet's own map: rows DX[a], right side x_a - x0_a
+            for (int a = 0; a < 3; ++a) {
+                n[a][0] = DX[a][0]; n[a][1] = DX[a][1]; n[a][2] = DX[a][2];
+                b[a] = ((double)P.x[v][a] + org[a]) - p[0][a];
+            }
+            if (!solve3(n, b, q)) q[0] = q[1] = q[2] = 0.0; // a flat tet: its fragments have no volume
+        }
+        for (int i = 0; i < 3; ++i) Q.q[v][i] = q[i];
+    }
 }
 
 } // namespace psib

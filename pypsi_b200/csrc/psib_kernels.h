@@ -52,6 +52,12 @@ struct ClipArgs {
     int rec_ibits;           // bits of the item field of a record key
     double *scale;           // FP32 kernel: per item, exact / FP32 q-volume
     void *scratch;           // per-thread scratch regions (grid x block of them)
+    // adjoint kernels
+    const double *adj_gm;    // dL/dm per voxel
+    double *adj_gpos;        // dL/dpos per particle (accumulated)
+    long long adj_npart;
+    double *adj_gmass;       // dL/dmass per element (accumulated), may be null
+    double adj_mass_factor;  // element mass / tet mass
 };
 
 struct MeshDev {
@@ -82,14 +88,18 @@ struct TessArgs {
 // ---- launchers (return cudaError_t of the launch) ----
 // big: the kernel for images whose bisection tree is deeper than DMAX_MAIN
 cudaError_t launch_clip_fp64(const ClipArgs &a, bool big, int grid, int block, cudaStream_t s);
-// mixed precision: FP32 main kernel; big -> the FP64 deep-tree kernel writing centroid-form records
-cudaError_t launch_clip_mixed(const ClipArgs &a, bool big, int grid, int block, cudaStream_t s);
+// centroid-form records: the FP32 main kernel (fp64_walk: the FP64 one); big -> the FP64
+// deep-tree kernel
+cudaError_t launch_clip_mixed(const ClipArgs &a, bool big, bool fp64_walk, int grid, int block, cudaStream_t s);
 // bytes of one thread's scratch region
 size_t scratch_bytes_fp64(bool big);
-size_t scratch_bytes_mixed(bool big);
+size_t scratch_bytes_mixed(bool big, bool fp64_walk);
 // resident blocks per SM of a clip kernel at this block size
 int clip_blocks_per_sm_fp64(bool big, int block);
-int clip_blocks_per_sm_mixed(bool big, int block);
+int clip_blocks_per_sm_mixed(bool big, bool fp64_walk, int block);
+// adjoint of the density deposit (FP64 walk, no records)
+cudaError_t launch_adjoint(const ClipArgs &a, bool big, int grid, int block, cudaStream_t s);
+int adjoint_blocks_per_sm(bool big, int block);
 
 cudaError_t launch_tess_count(const TessArgs &a, cudaStream_t s);
 cudaError_t launch_tess_emit(const TessArgs &a, cudaStream_t s);

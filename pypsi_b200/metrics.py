@@ -24,11 +24,8 @@ def _diagmax(t):
     return np.max(np.abs(np.diagonal(t, axis1=-2, axis2=-1)), axis=-1)
 
 
-def field_errors(test: dict, ref: dict) -> dict:
-    out = {}
+def _scales(ref: dict) -> dict:
     m = ref["m"]
-    live = m > 0
-    nv = int(live.sum())
     scales = {"m": np.abs(m)}
     if "x" in ref:
         scales["x"] = np.max(np.abs(ref["x"]), axis=-1)
@@ -45,6 +42,36 @@ def field_errors(test: dict, ref: dict) -> dict:
         if "xx" in ref and "vv" in ref:
             s = np.maximum(s, np.sqrt(_diagmax(ref["xx"]) * _diagmax(ref["vv"])))
         scales["xv"] = s
+    return scales
+
+
+def error_maps(test: dict, ref: dict, scale_from: dict | None = None) -> dict:
+    """Per-voxel normalised error of every field (the ``norm`` measure), as an
+    array over the voxels where the scale source has positive mass.  The scales
+    come from ``scale_from`` (default ``ref``), so maps of several pairs of
+    results can be compared voxel by voxel."""
+    sref = ref if scale_from is None else scale_from
+    live = sref["m"] > 0
+    nv = int(live.sum())
+    scales = _scales(sref)
+    out = {}
+    for f, r in ref.items():
+        if f not in test:
+            continue
+        dl = np.abs(test[f] - r)[live].reshape(nv, -1)
+        sc = scales[f][live]
+        floor = 1e-12 * float(np.mean(sc)) if sc.size else 0.0
+        sc = np.maximum(sc, floor)
+        out[f] = dl.max(axis=1) / np.where(sc > 0, sc, 1.0) if nv else np.zeros(0)
+    return out
+
+
+def field_errors(test: dict, ref: dict) -> dict:
+    out = {}
+    m = ref["m"]
+    live = m > 0
+    nv = int(live.sum())
+    norms = error_maps(test, ref)
     for f, r in ref.items():
         t = test[f]
         d = np.abs(t - r)
@@ -55,11 +82,7 @@ def field_errors(test: dict, ref: dict) -> dict:
         rl = np.abs(r[live]).reshape(nv, -1)
         with np.errstate(divide="ignore", invalid="ignore"):
             rel = np.where(rl > 0, dl / rl, dl)
-        sc = scales[f][live]
-        floor = 1e-12 * float(np.mean(sc)) if sc.size else 0.0
-        sc = np.maximum(sc, floor)
-        norm = dl.max(axis=1) / np.where(sc > 0, sc, 1.0)
-        out[f] = {"rel": float(rel.max()), "norm": float(norm.max()), "abs": float(d.max())}
+        out[f] = {"rel": float(rel.max()), "norm": float(norms[f].max()), "abs": float(d.max())}
     # voxels without reference mass must stay untouched up to rounding
     dead = ~live
     out["dead_m"] = float(np.abs(test["m"][dead]).max()) if dead.any() else 0.0

@@ -81,3 +81,24 @@ def test_counters(oracle):
     assert cnt["tets"] == 6 * 16 ** 3
     assert cnt["max_verts"] <= 32
     assert 10 < cnt["fragments"] / cnt["tets"] < 25
+
+
+def test_exact_oracle_agrees_where_the_reference_is_well_conditioned(oracle):
+    """The quad-precision oracle runs the same algorithm: on a case without tiny
+    fragments it agrees with the FP64 restatement to FP64 rounding, and on
+    random simplex tets it exposes the reference's own rounding in the second
+    moments of sliver voxels (which the mixed-precision tests allow for)."""
+    from pypsi_b200.metrics import field_errors
+
+    c = make("c2_order1")
+    r = run_oracle(oracle, c, "restatement")
+    e = run_oracle(oracle, c, "exact")
+    errs = field_errors(r, e)
+    assert max(v["norm"] for k, v in errs.items() if k != "dead_m") <= 1e-12, errs
+    c = make("tets")
+    r = run_oracle(oracle, c, "restatement")
+    e = run_oracle(oracle, c, "exact")
+    errs = field_errors(r, e)
+    assert errs["m"]["rel"] <= 1e-9, errs["m"]
+    assert errs["xx"]["norm"] > 1e-6, errs["xx"]  # the reference's own error in sliver voxels
+    assert abs(e["m"].sum() - c["mass"].sum()) <= 1e-12 * c["mass"].sum()
