@@ -30,6 +30,7 @@ CUDA_UNITS = {  # unit -> extra flags
     "tess.cu": ["--fmad=false"],
     "pipeline.cu": ["--fmad=false"],
     "noalloc.cu": ["--fmad=false"],
+    "bfs.cu": [],
 }
 HEADERS = ["psib_device.cuh", "psib_clip.cuh", "psib_kernels.h"]
 

@@ -1,0 +1,577 @@
+// bfs.cu -- the mixed-precision clip of the main tet images as a breadth-first
+// walk of their bisection trees.
+//
+// The depth-first walk of one tet per thread (psib_clip.cuh) leaves most lanes
+// of a warp idle, because every lane walks a tree of its own shape, and its
+// per-thread stack of polyhedra does not fit in the caches.  Here each level
+// of the trees is one launch in which every thread makes exactly one cut of
+// one polyhedron:
+//
+//   init   tet image -> its first polyhedron (4 vertices, FP32 positions
+//          relative to the image's vertex 0), to the level queue, or to the
+//          leaf queue when its index box is one voxel; images that need the
+//          window clip go to a list for the depth-first kernel
+//   level  polyhedron -> shrink its box while the middle plane misses it, then
+//          one cut into two children; each child goes to the next level queue
+//          or, when its box is one voxel, to the leaf queue
+//   leaf   fragment -> FP64 vertices from their planes, central moments, a
+//          record (key voxel|image), as the depth-first mixed kernel does
+//
+// The split plane of a node depends only on its index box, so every fragment
+// sees the same cuts in the same order as in the depth-first walk; only the
+// order in which fragments are produced differs, and records are sorted by
+// (voxel, image) afterwards.
+//
+// Queues hold polyhedra in 32-wide tiles: element e's vertex v, coordinate c
+// sits at ((e/32 * MAXV + v) * 3 + c) * 32 + e%32, so the lanes of a warp,
+// which hold consecutive elements, touch consecutive words.  A warp reserves
+// its outputs with one atomic per queue after a warp-wide prefix sum, and
+// writes them to consecutive elements.  The links of the polyhedron being cut
+// and of its two children, and the positions of the one being cut, live in
+// shared memory as [vertex][thread] (no bank conflicts whatever vertex each
+// lane touches); the leaf kernel keeps its fragment's FP64 q there.
+//
+// A level queue never holds more polyhedra than the leaves its images will
+// produce, which is at most the sum of their index-box volumes; the host sizes
+// each pass of images by that bound.
+#include "psib_device.cuh"
+#include "psib_kernels.h"
+
+namespace psib {
+
+constexpr int BB = 128; // threads per block of every kernel here
+constexpr unsigned FULL = 0xFFFFFFFFu;
+
+__device__ __forceinline__ size_t qx(unsigned long long e, int v, int c)
+{
+    return ((size_t)(e >> 5) * (MAXV * 3) + (size_t)(v * 3 + c)) * 32 + (size_t)(e & 31);
+}
+__device__ __forceinline__ size_t qn(unsigned long long e, int v)
+{
+    return ((size_t)(e >> 5) * MAXV + (size_t)v) * 32 + (size_t)(e & 31);
+}
+
+// per-thread shared-memory arrays laid out [vertex][thread]
+#define AT(arr, v) (arr)[(v) * BB + threadIdx.x]
+
+// Warp-wide exclusive prefix sum of n (every lane calls it); one atomic on
+// *count reserves the warp's total.  Returns the warp's first element.
+__device__ __forceinline__ unsigned long long warp_reserve(unsigned long long* count, unsigned n, unsigned& off)
+{
+    const int lane = threadIdx.x & 31;
+    unsigned x = n;
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned y = __shfl_up_sync(FULL, x, o);
+        if (lane >= o) x += y;
+    }
+    const unsigned total = __shfl_sync(FULL, x, 31);
+    off = x - n;
+    unsigned long long base = 0;
+    if (lane == 0 && total) base = atomicAdd(count, (unsigned long long)total);
+    return __shfl_sync(FULL, base, 0);
+}
+
+__device__ __forceinline__ void get_box(const PolyQueue& Q, unsigned long long e, int* lo, int* hi)
+{
+    for (int a = 0; a < 3; ++a) {
+        const uint32_t w = Q.box[3 * e + a];
+        lo[a] = (int)(w & 0xFFFFu);
+        hi[a] = (int)(w >> 16);
+    }
+}
+__device__ __forceinline__ void put_box(const PolyQueue& Q, unsigned long long e, const int* lo, const int* hi)
+{
+    for (int a = 0; a < 3; ++a) Q.box[3 * e + a] = (uint32_t)lo[a] | ((uint32_t)hi[a] << 16);
+}
+__device__ __forceinline__ bool one_voxel(const int* lo, const int* hi)
+{
+    return hi[0] - lo[0] <= 1 && hi[1] - lo[1] <= 1 && hi[2] - lo[2] <= 1;
+}
+
+// ---- init: tet images -> first polyhedra ----
+
+__global__ void __launch_bounds__(BB) k_bfs_init(BfsArgs a)
+{
+    const int lane = threadIdx.x & 31;
+    const long long warp = (long long)blockIdx.x * (BB / 32) + (threadIdx.x >> 5);
+    const long long nwarp = (long long)gridDim.x * (BB / 32);
+    unsigned st = 0;
+    for (long long base = a.q0 + warp * 32; base < a.q1; base += nwarp * 32) {
+        const long long i = base + lane;
+        const bool act = i < a.q1;
+        int t = 0;
+        double p[4][3];
+        int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+        bool window = false;
+        if (act) {
+            t = a.c.order[i];
+            const double* fr = a.c.it.frame + (size_t)t * FRAME;
+            for (int v = 0; v < 4; ++v)
+                for (int c = 0; c < 3; ++c) p[v][c] = fr[3 * v + c];
+            // window planes and index box as the depth-first walk computes them (src/geometry.c:816-842)
+            for (int c = 0; c < 3; ++c) {
+                double cmin = p[0][c], cmax = p[0][c];
+                for (int v = 1; v < 4; ++v) {
+                    if (p[v][c] < cmin) cmin = p[v][c];
+                    if (p[v][c] > cmax) cmax = p[v][c];
+                }
+                const bool clo = a.c.g.w0[c] > cmin, chi = a.c.g.w1[c] < cmax;
+                window = window || clo || chi;
+                if (clo) cmin = a.c.g.w0[c];
+                if (chi) cmax = a.c.g.w1[c];
+                lo[c] = (int)floor((cmin - a.c.g.w0[c]) / a.c.g.d[c]);
+                hi[c] = (int)ceil((cmax - a.c.g.w0[c]) / a.c.g.d[c]);
+                if (lo[c] < 0) lo[c] = 0;
+                if (hi[c] > a.c.g.n[c]) hi[c] = a.c.g.n[c];
+                if (hi[c] < lo[c]) hi[c] = lo[c];
+            }
+        }
+        const bool use = act && !window;
+        const bool leaf = use && one_voxel(lo, hi);
+        unsigned od, oq, ol;
+        const unsigned long long bd = warp_reserve(a.dfs_count, act && window ? 1u : 0u, od);
+        const unsigned long long bq = warp_reserve(a.out.count, use && !leaf ? 1u : 0u, oq);
+        const unsigned long long bl = warp_reserve(a.leaf.count, leaf ? 1u : 0u, ol);
+        if (act && window) a.dfs_list[bd + od] = t;
+        if (use) {
+            a.c.scale[t] = -1.0; // marks a breadth-first image: bfs_finalize sets its mass correction
+            a.vsum[t] = 0.0;
+            const PolyQueue& Q = leaf ? a.leaf : a.out;
+            const unsigned long long e = leaf ? bl + ol : bq + oq;
+            if (e >= Q.cap) {
+                st |= ST_OVERFLOW;
+            } else {
+                // the tet's vertex graph (src/geometry.c:776-787) with its plane tags
+                const uint32_t links[4] = {1u | (3u << 8) | (2u << 16), 2u | (3u << 8) | (0u << 16),
+                                           0u | (3u << 8) | (1u << 16), 1u | (2u << 8) | (0u << 16)};
+                for (int v = 0; v < 4; ++v) {
+                    for (int c = 0; c < 3; ++c) Q.x[qx(e, v, c)] = (float)(p[v][c] - p[0][c]);
+                    Q.nb[qn(e, v)] = links[v] | ((0xFu & ~(1u << v)) << 24);
+                }
+                Q.nv[e] = 4;
+                put_box(Q, e, lo, hi);
+                Q.item[e] = (uint32_t)t;
+            }
+        }
+    }
+    if (st) atomicOr(a.c.status, st);
+}
+
+// ---- level: one cut per polyhedron ----
+
+// Close the cut face of a child whose links are in shared memory (as
+// link_cut_vertices does for a polyhedron in memory).
+__device__ __forceinline__ bool link_cut_shared(uint32_t* nbs, int base, int nv)
+{
+    for (int vs = base; vs < nv; ++vs) {
+        int vc = vs, vn = nbget(AT(nbs, vs), 0);
+        int steps = 0;
+        do {
+            if (vn >= nv) return false;
+            const uint32_t w = AT(nbs, vn);
+            const int k = (nbget(w, 0) == vc) ? 0 : (nbget(w, 1) == vc) ? 1 : (nbget(w, 2) == vc) ? 2 : 3;
+            if (k == 3 || ++steps > WALK_CAP) return false;
+            vc = vn;
+            vn = nbget(AT(nbs, vc), (k + 1) % 3);
+        } while (vc < base);
+        AT(nbs, vs) = nbset(AT(nbs, vs), 2, vc);
+        AT(nbs, vc) = nbset(AT(nbs, vc), 1, vs);
+    }
+    return true;
+}
+
+// Cut the staged polyhedron (positions in xI as [v*3+c][thread], links in
+// nbI; upper side = bits of um, s = cr - x[ax]) into element el of QL (lower
+// side) and eu of QU (upper side), with the vertex order and arithmetic of
+// cut_poly.
+__device__ __forceinline__ unsigned bfs_cut(int nv, uint32_t um, float cr, int ax, const float* xI,
+                                            const uint32_t* nbI, uint32_t* nbL, uint32_t* nbU, const PolyQueue& QL,
+                                            unsigned long long el, const PolyQueue& QU, unsigned long long eu,
+                                            uint32_t cut_tag)
+{
+    const uint32_t lmask = ((1u << nv) - 1u) & ~um;
+    const int nl = __popc(lmask), nu = __popc(um);
+    for (int v = 0; v < nv; ++v) {
+        const bool u = (um >> v) & 1u;
+        const uint32_t sm = u ? um : lmask;
+        const int j = rank_in(sm, v);
+        const PolyQueue& Q = u ? QU : QL;
+        const unsigned long long d = u ? eu : el;
+        for (int c = 0; c < 3; ++c) Q.x[qx(d, j, c)] = AT(xI, 3 * v + c);
+        const uint32_t w = AT(nbI, v);
+        uint32_t ow = 0xFFFFFFu | (w & ALL_TAGS);
+        for (int k = 0; k < 3; ++k) {
+            const int t = nbget(w, k);
+            if (t >= nv) return ST_GRAPH;
+            if ((((um >> t) & 1u) != 0) == u) ow = nbset(ow, k, rank_in(sm, t));
+        }
+        if (u) AT(nbU, j) = ow;
+        else AT(nbL, j) = ow;
+    }
+    // the cut edges (lower vertex, link) as bits 3 vc + np: taking the lowest
+    // bit first creates the cut vertices in cut_poly's order, and every lane
+    // runs the loop body on every trip
+    uint64_t cm = 0ull;
+    for (int vc = 0; vc < nv; ++vc) {
+        const uint32_t w = AT(nbI, vc);
+        const bool low = !((um >> vc) & 1u);
+#pragma unroll
+        for (int np = 0; np < 3; ++np)
+            if (low && ((um >> nbget(w, np)) & 1u)) cm |= 1ull << (3 * vc + np);
+    }
+    int k = 0;
+    while (cm) {
+        const int bit = __ffsll((long long)cm) - 1;
+        cm &= cm - 1ull;
+        const int vc = bit / 3, np = bit - 3 * vc;
+        const uint32_t w = AT(nbI, vc);
+        const int jc = rank_in(lmask, vc);
+        {
+            const int vn = nbget(w, np);
+            if (nl + k >= MAXV || nu + k >= MAXV) return ST_OVERFLOW;
+            const float sc = cr - AT(xI, 3 * vc + ax), sn = cr - AT(xI, 3 * vn + ax);
+            const float iw = 1.0f / (sc - sn);
+            for (int c = 0; c < 3; ++c) {
+                const float px = iw * (AT(xI, 3 * vn + c) * sc - AT(xI, 3 * vc + c) * sn);
+                QL.x[qx(el, nl + k, c)] = px;
+                QU.x[qx(eu, nu + k, c)] = px;
+            }
+            const uint32_t wn = AT(nbI, vn);
+            const uint32_t tg = (w & wn & ALL_TAGS) | cut_tag;
+            AT(nbL, nl + k) = 0xFFFF00u | (uint32_t)jc | tg;
+            AT(nbL, jc) = nbset(AT(nbL, jc), np, nl + k);
+            const int jn = rank_in(um, vn);
+            AT(nbU, nu + k) = 0xFFFF00u | (uint32_t)jn | tg;
+            const int kb = (nbget(wn, 0) == vc) ? 0 : (nbget(wn, 1) == vc) ? 1 : (nbget(wn, 2) == vc) ? 2 : 3;
+            if (kb == 3) return ST_GRAPH;
+            AT(nbU, jn) = nbset(AT(nbU, jn), kb, nu + k);
+            ++k;
+        }
+    }
+    if (!link_cut_shared(nbL, nl, nl + k) || !link_cut_shared(nbU, nu, nu + k)) return ST_GRAPH;
+    for (int v = 0; v < nl + k; ++v) QL.nb[qn(el, v)] = AT(nbL, v);
+    for (int v = 0; v < nu + k; ++v) QU.nb[qn(eu, v)] = AT(nbU, v);
+    QL.nv[el] = (uint8_t)(nl + k);
+    QU.nv[eu] = (uint8_t)(nu + k);
+    return 0;
+}
+
+__global__ void __launch_bounds__(BB) k_bfs_level(BfsArgs a)
+{
+    extern __shared__ uint32_t smem[];
+    uint32_t* nbI = smem;
+    uint32_t* nbL = smem + MAXV * BB;
+    uint32_t* nbU = smem + 2 * MAXV * BB;
+    float* xI = (float*)(smem + 3 * MAXV * BB); // [v * 3 + c][thread]
+    const int lane = threadIdx.x & 31;
+    const long long warp = (long long)blockIdx.x * (BB / 32) + (threadIdx.x >> 5);
+    const long long nwarp = (long long)gridDim.x * (BB / 32);
+    // a producer reserves before it checks capacity (and flags the overflow), so clamp
+    const unsigned long long n = min(*a.in.count, a.in.cap);
+    unsigned st = 0;
+    unsigned long long splits = 0;
+    for (unsigned long long base = (unsigned long long)warp * 32; base < n; base += (unsigned long long)nwarp * 32) {
+        const unsigned long long e = base + lane;
+        bool act = e < n;
+        int nv = 0, lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0}, ax = 0, nlo = 0, nup = 0;
+        uint32_t um = 0, t = 0;
+        float cr = 0.0f;
+        bool cut = false, toleaf = false;
+        if (act) {
+            nv = a.in.nv[e];
+            if (nv < 4 || nv > MAXV) act = false; // a failed cut upstream (status already set)
+        }
+        if (act) {
+            get_box(a.in, e, lo, hi);
+            t = a.in.item[e];
+            const double* fr = a.c.it.frame + (size_t)t * FRAME; // vertex 0: the origin of the FP32 positions
+            for (int v = 0; v < nv; ++v) {
+                AT(nbI, v) = a.in.nb[qn(e, v)];
+                for (int c = 0; c < 3; ++c) AT(xI, 3 * v + c) = a.in.x[qx(e, v, c)];
+            }
+            for (int guard = 0; guard < 64; ++guard) {
+                int dmax = 0;
+                ax = 0;
+                for (int c = 0; c < 3; ++c) {
+                    const int sz = hi[c] - lo[c];
+                    if (sz > dmax) { dmax = sz; ax = c; }
+                }
+                if (dmax <= 1) { toleaf = true; break; }
+                ++splits;
+                // the middle grid plane of the longest axis (src/geometry.c:886-893)
+                const double coord = a.c.g.d[ax] * (lo[ax] + dmax / 2) + a.c.g.w0[ax];
+                cr = (float)(coord - fr[ax]);
+                um = 0;
+                for (int v = 0; v < nv; ++v)
+                    if (cr - AT(xI, 3 * v + ax) < 0.0f) um |= 1u << v;
+                nlo = dmax / 2;
+                nup = dmax - nlo;
+                if (um == 0) { hi[ax] -= nup; continue; }
+                if (um == (1u << nv) - 1u) { lo[ax] += nlo; continue; }
+                cut = true;
+                break;
+            }
+            if (!cut && !toleaf) { st |= ST_DEPTH; act = false; }
+        }
+        int llo[3], lhi[3], ulo[3], uhi[3];
+        for (int c = 0; c < 3; ++c) { llo[c] = ulo[c] = lo[c]; lhi[c] = uhi[c] = hi[c]; }
+        if (cut) { lhi[ax] -= nup; ulo[ax] += nlo; }
+        const bool leafL = cut && one_voxel(llo, lhi), leafU = cut && one_voxel(ulo, uhi);
+        const unsigned nq = cut ? (unsigned)(!leafL) + (unsigned)(!leafU) : 0u;
+        const unsigned nlf = toleaf ? 1u : cut ? (unsigned)leafL + (unsigned)leafU : 0u;
+        if (a.last && nq) st |= ST_DEPTH;
+        unsigned oq, ol;
+        const unsigned long long bq = warp_reserve(a.out.count, nq, oq);
+        const unsigned long long bl = warp_reserve(a.leaf.count, nlf, ol);
+        if (toleaf) {
+            const unsigned long long d = bl + ol;
+            if (d >= a.leaf.cap) {
+                st |= ST_OVERFLOW;
+            } else {
+                for (int v = 0; v < nv; ++v) {
+                    for (int c = 0; c < 3; ++c) a.leaf.x[qx(d, v, c)] = AT(xI, 3 * v + c);
+                    a.leaf.nb[qn(d, v)] = AT(nbI, v);
+                }
+                a.leaf.nv[d] = (uint8_t)nv;
+                put_box(a.leaf, d, lo, hi);
+                a.leaf.item[d] = t;
+            }
+        }
+        if (cut) {
+            unsigned qi = 0, li = 0;
+            const PolyQueue& QL = leafL ? a.leaf : a.out;
+            const unsigned long long el = leafL ? bl + ol + li++ : bq + oq + qi++;
+            const PolyQueue& QU = leafU ? a.leaf : a.out;
+            const unsigned long long eu = leafU ? bl + ol + li++ : bq + oq + qi++;
+            if (el >= QL.cap || eu >= QU.cap) {
+                st |= ST_OVERFLOW;
+            } else {
+                const unsigned e2 = bfs_cut(nv, um, cr, ax, xI, nbI, nbL, nbU, QL, el, QU, eu, axis_tag(ax));
+                if (e2) {
+                    st |= e2;
+                    QL.nv[el] = 0; // downstream kernels skip these
+                    QU.nv[eu] = 0;
+                }
+                put_box(QL, el, llo, lhi);
+                put_box(QU, eu, ulo, uhi);
+                QL.item[el] = t;
+                QU.item[eu] = t;
+            }
+        }
+    }
+    if (st) atomicOr(a.c.status, st);
+    if (a.c.counters && splits) atomicAdd(&a.c.counters[2], splits);
+}
+
+// ---- leaf: fragment moments and records ----
+
+// Moments (order 0..2) of the fragment about q-point o (the q of vertex 0),
+// by the fan triangles of reduce_about; the vertices' FP64 q are in qs as
+// [v * 3 + c][thread].
+__device__ __forceinline__ unsigned leaf_moments(int nv, const uint32_t* nbs, const double* qs, int order, double* o,
+                                                 double* mom)
+{
+    for (int i = 0; i < 3; ++i) o[i] = AT(qs, i);
+    for (int i = 0; i < 10; ++i) mom[i] = 0.0;
+    // directed edges not yet walked (3 * MAXV = 60 bits); the lowest first is
+    // the face order of reduce_about
+    uint64_t todo = (3 * nv >= 64) ? ~0ull : ((1ull << (3 * nv)) - 1ull);
+    while (todo) {
+        {
+            const int b0 = __ffsll((long long)todo) - 1;
+            todo &= todo - 1ull;
+            const int vs = b0 / 3, ks = b0 - 3 * vs;
+            int vc = vs;
+            int vn = nbget(AT(nbs, vc), ks);
+            if (vn >= nv) return ST_GRAPH;
+            const double q0x = AT(qs, 3 * vs) - o[0], q0y = AT(qs, 3 * vs + 1) - o[1], q0z = AT(qs, 3 * vs + 2) - o[2];
+            uint32_t w = AT(nbs, vn);
+            int k = (nbget(w, 0) == vc) ? 0 : (nbget(w, 1) == vc) ? 1 : (nbget(w, 2) == vc) ? 2 : 3;
+            if (k == 3) return ST_GRAPH;
+            vc = vn;
+            int kn = (k + 1) % 3;
+            todo &= ~(1ull << (3 * vc + kn));
+            vn = nbget(AT(nbs, vc), kn);
+            int steps = 0;
+            while (vn != vs) {
+                if (++steps > WALK_CAP || vn >= nv) return ST_GRAPH;
+                const double q1x = AT(qs, 3 * vn) - o[0], q1y = AT(qs, 3 * vn + 1) - o[1], q1z = AT(qs, 3 * vn + 2) - o[2];
+                const double q2x = AT(qs, 3 * vc) - o[0], q2y = AT(qs, 3 * vc + 1) - o[1], q2z = AT(qs, 3 * vc + 2) - o[2];
+                const double m = (-q2x * q1y * q0z + q1x * q2y * q0z + q2x * q0y * q1z
+                                  - q0x * q2y * q1z - q1x * q0y * q2z + q0x * q1y * q2z);
+                mom[0] += m;
+                if (order > 0) {
+                    mom[1] += 0.25 * m * (q0x + q1x + q2x);
+                    mom[2] += 0.25 * m * (q0y + q1y + q2y);
+                    mom[3] += 0.25 * m * (q0z + q1z + q2z);
+                }
+                if (order > 1) {
+                    mom[4] += 0.1 * m * (q0x * q0x + q1x * q1x + q2x * q2x + q1x * q2x + q0x * (q1x + q2x));
+                    mom[5] += 0.05 * m * (q2x * q0y + q2x * q1y + 2 * q2x * q2y + q0x * (2 * q0y + q1y + q2y) + q1x * (q0y + 2 * q1y + q2y));
+                    mom[6] += 0.05 * m * (q2x * q0z + q2x * q1z + 2 * q2x * q2z + q0x * (2 * q0z + q1z + q2z) + q1x * (q0z + 2 * q1z + q2z));
+                    mom[7] += 0.1 * m * (q0y * q0y + q1y * q1y + q2y * q2y + q1y * q2y + q0y * (q1y + q2y));
+                    mom[8] += 0.05 * m * (q2y * q0z + q2y * q1z + 2 * q2y * q2z + q0y * (2 * q0z + q1z + q2z) + q1y * (q0z + 2 * q1z + q2z));
+                    mom[9] += 0.1 * m * (q0z * q0z + q1z * q1z + q2z * q2z + q1z * q2z + q0z * (q1z + q2z));
+                }
+                w = AT(nbs, vn);
+                k = (nbget(w, 0) == vc) ? 0 : (nbget(w, 1) == vc) ? 1 : (nbget(w, 2) == vc) ? 2 : 3;
+                if (k == 3) return ST_GRAPH;
+                vc = vn;
+                kn = (k + 1) % 3;
+                todo &= ~(1ull << (3 * vc + kn));
+                vn = nbget(AT(nbs, vc), kn);
+            }
+        }
+    }
+    return 0;
+}
+
+__global__ void __launch_bounds__(BB) k_bfs_leaf(BfsArgs a)
+{
+    extern __shared__ uint32_t smem[];
+    uint32_t* nbs = smem;
+    double* qs = (double*)(smem + MAXV * BB); // [v * 3 + c][thread]
+    const int lane = threadIdx.x & 31;
+    const long long warp = (long long)blockIdx.x * (BB / 32) + (threadIdx.x >> 5);
+    const long long nwarp = (long long)gridDim.x * (BB / 32);
+    const unsigned long long n = min(*a.leaf.count, a.leaf.cap);
+    const ClipArgs& c = a.c;
+    unsigned st = 0;
+    unsigned long long frags = 0, verts = 0;
+    for (unsigned long long base = (unsigned long long)warp * 32; base < n; base += (unsigned long long)nwarp * 32) {
+        const unsigned long long e = base + lane;
+        bool has = false;
+        double rec[10];
+        unsigned long long key = 0;
+        if (e < n) {
+            const int nv = a.leaf.nv[e];
+            if (nv >= 4 && nv <= MAXV) {
+                int lo[3], hi[3];
+                get_box(a.leaf, e, lo, hi);
+                const uint32_t t = a.leaf.item[e];
+                const double* fr = c.it.frame + (size_t)t * FRAME;
+                double p0[3], DX[3][3], plo[3], phi[3], tol[3];
+                for (int i = 0; i < 3; ++i) p0[i] = fr[i];
+                for (int i = 0; i < 3; ++i)
+                    for (int j = 0; j < 3; ++j) DX[i][j] = fr[3 * (j + 1) + i] - p0[i];
+                for (int i = 0; i < 3; ++i) {
+                    plo[i] = c.g.d[i] * lo[i] + c.g.w0[i];
+                    phi[i] = c.g.d[i] * (lo[i] + 1) + c.g.w0[i];
+                    tol[i] = 1.0e-3 * c.g.d[i];
+                }
+                for (int v = 0; v < nv; ++v) {
+                    const uint32_t w = a.leaf.nb[qn(e, v)];
+                    AT(nbs, v) = w;
+                    const float x[3] = {a.leaf.x[qx(e, v, 0)], a.leaf.x[qx(e, v, 1)], a.leaf.x[qx(e, v, 2)]};
+                    double q[3];
+                    exact_q(x, w, p0, DX, p0, plo, phi, tol, q);
+                    for (int i = 0; i < 3; ++i) AT(qs, 3 * v + i) = q[i];
+                }
+                double o[3], mom[10];
+                const unsigned e2 = leaf_moments(nv, nbs, qs, c.mom_order, o, mom);
+                if (e2) {
+                    st |= e2;
+                } else if (mom[0] > 0.0) {
+                    if (lo[0] >= c.g.n[0] || lo[1] >= c.g.n[1] || lo[2] >= c.g.n[2]) {
+                        st |= ST_INDEX;
+                    } else {
+                        const long long gi = ((long long)c.g.n[1] * lo[0] + lo[1]) * c.g.n[2] + lo[2];
+                        key = ((unsigned long long)gi << c.rec_ibits) | (unsigned long long)(t - c.rec_item_base);
+                        const double m0 = mom[0];
+                        double u[3];
+                        for (int i = 0; i < 3; ++i) u[i] = mom[1 + i] / m0;
+                        rec[0] = m0;
+                        for (int i = 0; i < 3; ++i) rec[1 + i] = o[i] + u[i];
+                        rec[4] = mom[4] / m0 - u[0] * u[0];
+                        rec[5] = mom[5] / m0 - u[0] * u[1];
+                        rec[6] = mom[6] / m0 - u[0] * u[2];
+                        rec[7] = mom[7] / m0 - u[1] * u[1];
+                        rec[8] = mom[8] / m0 - u[1] * u[2];
+                        rec[9] = mom[9] / m0 - u[2] * u[2];
+                        has = true;
+                        ++frags;
+                        verts += nv;
+                        atomicAdd(&a.vsum[t], m0);
+                    }
+                }
+            }
+        }
+        unsigned off;
+        const unsigned long long r0 = warp_reserve(c.rec_n, has ? 1u : 0u, off);
+        if (has) {
+            const unsigned long long r = r0 + off;
+            if (r < c.rec_cap) {
+                c.rec_key[r] = key;
+                double* dst = c.rec_mom + r * c.rec_nmom;
+#pragma unroll
+                for (int k = 0; k < 10; ++k)
+                    if (k < c.rec_nmom) dst[k] = rec[k];
+            } else {
+                st |= ST_RECORDS;
+            }
+        }
+    }
+    if (st) atomicOr(c.status, st);
+    if (c.counters && frags) {
+        atomicAdd(&c.counters[0], frags);
+        atomicAdd(&c.counters[1], verts);
+    }
+}
+
+// FP32 walks can misplace a vertex that falls back to its FP32 position by
+// ~1e-7 of the tet: each breadth-first image's fragment masses are scaled by
+// 1 / (sum of its fragment q-volumes), so that it deposits exactly its mass.
+__global__ void k_bfs_finalize(BfsArgs a, long long nitems)
+{
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nitems; t += (long long)gridDim.x * blockDim.x)
+        if (a.c.scale[t] == -1.0) a.c.scale[t] = a.vsum[t] > 0.0 ? 1.0 / a.vsum[t] : 1.0;
+}
+
+cudaError_t launch_bfs_finalize(const BfsArgs& a, long long nitems, int num_sms, cudaStream_t s)
+{
+    k_bfs_finalize<<<num_sms * 8, 256, 0, s>>>(a, nitems);
+    return cudaGetLastError();
+}
+
+// ---- launchers ----
+
+static constexpr size_t LEVEL_SMEM = 6 * MAXV * BB * sizeof(uint32_t);
+static constexpr size_t LEAF_SMEM = MAXV * BB * (sizeof(uint32_t) + 3 * sizeof(double));
+
+// resident blocks per SM of each kernel (one full wave of grid-stride blocks)
+static int g_blocks[3] = {0, 0, 0};
+static void occupancy()
+{
+    if (g_blocks[0]) return;
+    cudaFuncSetAttribute(k_bfs_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LEVEL_SMEM);
+    cudaFuncSetAttribute(k_bfs_leaf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LEAF_SMEM);
+    int b[3] = {1, 1, 1};
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b[0], k_bfs_init, BB, 0) != cudaSuccess) b[0] = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b[1], k_bfs_level, BB, LEVEL_SMEM) != cudaSuccess) b[1] = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b[2], k_bfs_leaf, BB, LEAF_SMEM) != cudaSuccess) b[2] = 1;
+    cudaGetLastError();
+    for (int i = 0; i < 3; ++i) g_blocks[i] = b[i] > 0 ? b[i] : 1;
+}
+
+cudaError_t launch_bfs_init(const BfsArgs& a, int num_sms, cudaStream_t s)
+{
+    occupancy();
+    k_bfs_init<<<num_sms * g_blocks[0], BB, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bfs_level(const BfsArgs& a, int num_sms, cudaStream_t s)
+{
+    occupancy();
+    k_bfs_level<<<num_sms * g_blocks[1], BB, LEVEL_SMEM, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bfs_leaf(const BfsArgs& a, int num_sms, cudaStream_t s)
+{
+    occupancy();
+    k_bfs_leaf<<<num_sms * g_blocks[2], BB, LEAF_SMEM, s>>>(a);
+    return cudaGetLastError();
+}
+
+} // namespace psib

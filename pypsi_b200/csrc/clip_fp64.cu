@@ -7,7 +7,7 @@
 
 namespace psib {
 
-constexpr int DEFAULT_MINB_FP64 = 8;
+constexpr int DEFAULT_MINB_FP64 = 6;
 
 // Main kernel variants by the minimum number of resident 128-thread blocks
 // per SM the register allocation must allow (0: no cap); PSIB_CLIP_MINB picks

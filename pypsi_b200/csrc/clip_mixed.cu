@@ -8,7 +8,7 @@
 
 namespace psib {
 
-constexpr int DEFAULT_MINB_MIXED = 0;
+constexpr int DEFAULT_MINB_MIXED = 6;
 
 // Main kernel variants by the minimum number of resident 128-thread blocks
 // per SM the register allocation must allow (0: no cap).  More blocks hide more

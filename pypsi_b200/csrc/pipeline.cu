@@ -97,12 +97,16 @@ struct Ctx {
     DevBuf small; // status, counters, queue heads
     // records
     DevBuf rkey, rmom, rkey_sorted, rperm_in, rperm, rvox, ritem, rmom_sorted, run_vox, run_cnt, run_off;
+    // breadth-first clip: three polyhedron queues, the volume histogram, per-level counters, window list
+    DevBuf qx[3], qnb[3], qnv[3], qbox[3], qitem[3], hist, bfs_cnt, dfs_list, vsum;
     std::vector<DevBuf*> all()
     {
         return {&hpos, &hgpos, &hgmass, &hvel, &hmass, &hconn, &hfield[0], &hfield[1], &hfield[2], &hfield[3], &hfield[4],
                 &hfield[5], &iframe, &ielem, &ipid, &ikey,
                 &key_sorted, &order_in, &order, &counts, &offsets, &cub_tmp, &scratch, &scratch_big, &iscale, &small, &rkey, &rmom,
-                &rkey_sorted, &rperm_in, &rperm, &rvox, &ritem, &rmom_sorted, &run_vox, &run_cnt, &run_off};
+                &rkey_sorted, &rperm_in, &rperm, &rvox, &ritem, &rmom_sorted, &run_vox, &run_cnt, &run_off,
+                &qx[0], &qx[1], &qx[2], &qnb[0], &qnb[1], &qnb[2], &qnv[0], &qnv[1], &qnv[2], &qbox[0], &qbox[1],
+                &qbox[2], &qitem[0], &qitem[1], &qitem[2], &hist, &bfs_cnt, &dfs_list, &vsum};
     }
 };
 
@@ -127,7 +131,13 @@ int get_ctx(int dev, Ctx** out)
 
 // small device block layout (unsigned long long words)
 enum { S_STATUS = 0, S_CNT = 1 /* 3 words */, S_TESS = 4 /* 2 */, S_HEAD = 8 /* 4 */, S_RECN = 12, S_NDEEP = 13,
-       S_WORDS = 16 };
+       S_DFS = 14, S_WORDS = 16 };
+
+__global__ void k_key_hist(const uint16_t* key, long long n, unsigned* hist)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        atomicAdd(&hist[key[i]], 1u);
+}
 
 __global__ void k_count_deep(const uint16_t* key, long long n, unsigned long long* out)
 {
@@ -187,6 +197,112 @@ int check_status(Call& c, unsigned long long* small_host)
     return fail(PSIB_ERR_CUDA, "kernel status 0x%x", st);
 }
 
+// Mixed-precision clip of queue positions [0, nmain) by the breadth-first
+// walk (bfs.cu); images that need the window clip come back in a list and go to
+// the depth-first kernel.  Images are sorted by index-box volume, largest
+// first; a pass takes images while the sum of their box volumes -- a bound on
+// every queue of the pass -- stays within the queue capacity.
+int bfs_clip(Ctx& C, ClipArgs& ca, long long nmain, long long nitems, unsigned long long* sm, int clip_grid,
+             int clip_block, cudaStream_t st, long long& launches, long long& klaunch)
+{
+    RET(ensure(C.hist, 65536 * sizeof(unsigned)));
+    CK(cudaMemsetAsync(C.hist.p, 0, 65536 * sizeof(unsigned), st));
+    k_key_hist<<<C.num_sms * 4, 256, 0, st>>>(C.key_sorted.as<uint16_t>(), nmain, C.hist.as<unsigned>());
+    CK(cudaGetLastError());
+    klaunch++;
+    std::vector<unsigned> hist(65536);
+    CK(cudaMemcpyAsync(hist.data(), C.hist.p, 65536 * sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    const long long cap = std::max<long long>(env_ll("PSIB_BFS_CAP", 16ll << 20), 1024);
+    std::vector<long long> qb{0};
+    long long cur = 0, pos = 0;
+    for (int k = 0; k < 0xFFFF; ++k) {
+        long long cnt = hist[k];
+        const long long vol = std::max(1, 0xFFFE - k);
+        while (cnt > 0) {
+            const long long take = std::min(cnt, (cap - cur) / vol);
+            if (take == 0) {
+                qb.push_back(pos);
+                cur = 0;
+                continue;
+            }
+            cur += take * vol;
+            pos += take;
+            cnt -= take;
+        }
+    }
+    if (qb.back() != pos) qb.push_back(pos);
+    if (pos != nmain) return fail(PSIB_ERR_CUDA, "footprint histogram covers %lld of %lld images", pos, nmain);
+
+    const size_t tiles = (size_t)(cap + 31) / 32;
+    PolyQueue Q[3];
+    for (int i = 0; i < 3; ++i) {
+        RET(ensure(C.qx[i], tiles * 32 * MAXV * 3 * sizeof(float)));
+        RET(ensure(C.qnb[i], tiles * 32 * MAXV * sizeof(uint32_t)));
+        RET(ensure(C.qnv[i], tiles * 32));
+        RET(ensure(C.qbox[i], tiles * 32 * 3 * sizeof(uint32_t)));
+        RET(ensure(C.qitem[i], tiles * 32 * sizeof(uint32_t)));
+        Q[i] = PolyQueue{C.qx[i].as<float>(), C.qnb[i].as<uint32_t>(), C.qnv[i].as<uint8_t>(),
+                         C.qbox[i].as<uint32_t>(), C.qitem[i].as<uint32_t>(), nullptr,
+                         (unsigned long long)tiles * 32};
+    }
+    RET(ensure(C.dfs_list, (size_t)std::max<long long>(nmain, 1) * sizeof(int)));
+    // per pass: level-queue counts [0, DMAX_MAIN] and leaf-queue counts [DMAX_MAIN + 1, 2 DMAX_MAIN + 1]
+    constexpr int NCNT = 2 * DMAX_MAIN + 2;
+    RET(ensure(C.bfs_cnt, NCNT * sizeof(unsigned long long)));
+    unsigned long long* cq = C.bfs_cnt.as<unsigned long long>();
+    unsigned long long* cl = cq + DMAX_MAIN + 1;
+    CK(cudaMemsetAsync(&sm[S_DFS], 0, 8, st));
+
+    BfsArgs ba = {};
+    ba.c = ca;
+    ba.dfs_list = C.dfs_list.as<int>();
+    ba.dfs_count = &sm[S_DFS];
+    RET(ensure(C.vsum, (size_t)std::max<long long>(nitems, 1) * sizeof(double)));
+    ba.vsum = C.vsum.as<double>();
+    const int grid = C.num_sms;
+    for (size_t p = 0; p + 1 < qb.size(); ++p) {
+        CK(cudaMemsetAsync(cq, 0, NCNT * sizeof(unsigned long long), st));
+        ba.q0 = qb[p];
+        ba.q1 = qb[p + 1];
+        ba.out = Q[0];
+        ba.out.count = &cq[0];
+        ba.leaf = Q[2];
+        ba.leaf.count = &cl[0];
+        CK(launch_bfs_init(ba, grid, st));
+        CK(launch_bfs_leaf(ba, grid, st));
+        int ia = 0;
+        for (int lvl = 0; lvl < DMAX_MAIN; ++lvl) {
+            ba.in = Q[ia];
+            ba.in.count = &cq[lvl];
+            ba.out = Q[1 - ia];
+            ba.out.count = &cq[lvl + 1];
+            ba.leaf.count = &cl[lvl + 1];
+            ba.last = lvl == DMAX_MAIN - 1;
+            CK(launch_bfs_level(ba, grid, st));
+            CK(launch_bfs_leaf(ba, grid, st));
+            ia = 1 - ia;
+        }
+        klaunch += 2 + 2 * DMAX_MAIN;
+        launches += 2 + 2 * DMAX_MAIN;
+    }
+    CK(launch_bfs_finalize(ba, nitems, C.num_sms, st));
+    klaunch++;
+    unsigned long long ndfs = 0;
+    CK(cudaMemcpyAsync(&ndfs, &sm[S_DFS], 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (ndfs > 0) {
+        ClipArgs cw = ca;
+        cw.order = C.dfs_list.as<int>();
+        cw.order_base = 0;
+        cw.n = (long long)ndfs;
+        cw.head = &sm[S_HEAD];
+        CK(launch_clip_mixed(cw, false, false, clip_grid, clip_block, st));
+        launches++;
+    }
+    return PSIB_OK;
+}
+
 int run_device(Call& c)
 {
     Ctx& C = *c.C;
@@ -205,6 +321,10 @@ int run_device(Call& c)
     const bool mixed = c.precision == PSIB_MIXED && !c.adjoint;
     // central-form records: the mixed kernel, or the FP64 walk in PSIB_FP64_CENTRAL
     const bool central = (mixed || c.precision == PSIB_FP64_CENTRAL) && !c.adjoint;
+    // the mixed kernel walks the main images breadth first (PSIB_BFS=0: depth first)
+    bool use_bfs = mixed && env_ll("PSIB_BFS", 1) != 0;
+    for (int i = 0; i < 3; ++i)
+        if (g.n[i] >= 0xFFFF) use_bfs = false; // box bounds are packed in 16 bits
     // 1, 4 or 10 moments per record (FP32 kernel: m0, q-centroid, central second moment)
     const int nmom = order == 2 ? 10 : order == 1 ? 4 : 1;
 
@@ -440,7 +560,10 @@ int run_device(Call& c)
             CK(cudaMemsetAsync(&sm[S_CNT], 0, 24, st)); // this attempt's counters
             CK(cudaMemsetAsync(&sm[S_HEAD], 0, 16, st));
             CK(cudaEventRecord(C.ev[4], st));
-            if (nmain > 0) {
+            if (nmain > 0 && use_bfs) {
+                ca.scratch = C.scratch.p;
+                RET(bfs_clip(C, ca, nmain, nitems, sm, clip_grid, clip_block, st, launches, klaunch));
+            } else if (nmain > 0) {
                 ca.scratch = C.scratch.p;
                 ca.order_base = 0;
                 ca.n = nmain;

@@ -67,7 +67,15 @@ struct Tally {
 __device__ __forceinline__ void write_record(const ClipArgs& a, long long gi, long long t, const double* mom,
                                              unsigned& st)
 {
-    const unsigned long long r = atomicAdd(a.rec_n, 1ull);
+    // one atomic per group of lanes that reach this point together: the record
+    // counter is a single address that every fragment of the launch hits
+    const unsigned act = __activemask();
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(act) - 1;
+    unsigned long long base = 0;
+    if (lane == leader) base = atomicAdd(a.rec_n, (unsigned long long)__popc(act));
+    base = __shfl_sync(act, base, leader);
+    const unsigned long long r = base + __popc(act & ((1u << lane) - 1u));
     if (r < a.rec_cap) {
         a.rec_key[r] = ((unsigned long long)gi << a.rec_ibits) | (unsigned long long)(t - a.rec_item_base);
         double* dst = a.rec_mom + r * a.rec_nmom;

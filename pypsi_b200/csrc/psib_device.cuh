@@ -474,6 +474,77 @@ __device__ __forceinline__ bool solve3(const double (*n)[3], const double* b, do
     return true;
 }
 
+// Plane idx of a vertex's tags as a row n . q = b: idx 0..3 is the tet face
+// opposite vertex idx (qx + qy + qz = 1, or q_{idx-1} = 0), idx 4..6 the grid
+// plane x_a = pc_a (a = idx - 4), i.e. DX[a] . q = pc_a - p0_a.  Selects by
+// value so that everything stays in registers.
+__device__ __forceinline__ void plane_row(int idx, const double (*DX)[3], const double* pc, const double* p0,
+                                          double* n, double& b)
+{
+    if (idx < 4) {
+        n[0] = (idx == 0 || idx == 1) ? 1.0 : 0.0;
+        n[1] = (idx == 0 || idx == 2) ? 1.0 : 0.0;
+        n[2] = (idx == 0 || idx == 3) ? 1.0 : 0.0;
+        b = idx == 0 ? 1.0 : 0.0;
+    } else {
+        const int a = idx - 4;
+        for (int c = 0; c < 3; ++c) n[c] = a == 0 ? DX[0][c] : a == 1 ? DX[1][c] : DX[2][c];
+        b = a == 0 ? pc[0] - p0[0] : a == 1 ? pc[1] - p0[1] : pc[2] - p0[2];
+    }
+}
+
+// q of one vertex of an FP32 fragment: x is its FP32 position relative to org,
+// w its link word (tags), DX the tet's edge matrix, p0 its vertex 0.
+__device__ __forceinline__ void exact_q(const float* x, uint32_t w, const double* p0, const double (*DX)[3],
+                                        const double* org, const double* plo, const double* phi, const double* tol,
+                                        double* q)
+{
+    const uint32_t tf = (w >> 24) & 0xFu;
+    uint32_t ap = 0;
+    double pc[3], dist[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const double xv = (double)x[a] + org[a];
+        const double dl = fabs(xv - plo[a]), dh = fabs(xv - phi[a]);
+        pc[a] = dl <= dh ? plo[a] : phi[a];
+        dist[a] = (dl <= dh ? dl : dh) / tol[a];
+        if (((w >> (28 + a)) & 1u) && dist[a] <= 1.0) ap |= 1u << a;
+    }
+    // a vertex near the edge or corner of its voxel can keep a fourth tag:
+    // the tet-face tags are exact, so drop the farthest grid plane
+    while (__popc(tf) + __popc(ap) > 3) {
+        int far = -1;
+        double df = -1.0;
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+            if (((ap >> a) & 1u) && dist[a] > df) { far = a; df = dist[a]; }
+        if (far < 0) break;
+        ap &= ~(1u << far);
+    }
+    double n0[3], n1[3], n2[3], b0, b1, b2;
+    bool ok = __popc(tf) + __popc(ap) == 3;
+    if (ok) {
+        uint32_t m = tf | (ap << 4);
+        const int i0 = __ffs(m) - 1;
+        m &= m - 1;
+        const int i1 = __ffs(m) - 1;
+        m &= m - 1;
+        const int i2 = __ffs(m) - 1;
+        plane_row(i0, DX, pc, p0, n0, b0);
+        plane_row(i1, DX, pc, p0, n1, b1);
+        plane_row(i2, DX, pc, p0, n2, b2);
+        const double nn[3][3] = {{n0[0], n0[1], n0[2]}, {n1[0], n1[1], n1[2]}, {n2[0], n2[1], n2[2]}};
+        const double bb[3] = {b0, b1, b2};
+        ok = solve3(nn, bb, q);
+    }
+    if (!ok) {
+        // position -> q through the tet's own map: rows DX[a], right side x_a - x0_a
+        const double bb[3] = {((double)x[0] + org[0]) - p0[0], ((double)x[1] + org[1]) - p0[1],
+                              ((double)x[2] + org[2]) - p0[2]};
+        if (!solve3(DX, bb, q)) q[0] = q[1] = q[2] = 0.0; // a flat tet: its fragments have no volume
+    }
+}
+
 __device__ __forceinline__ void exact_vertices(const Poly<float>& P, const double (*p)[3], const double* org,
                                                const double* plo, const double* phi, const double* tol,
                                                QPoly& Q)
@@ -483,51 +554,8 @@ __device__ __forceinline__ void exact_vertices(const Poly<float>& P, const doubl
         for (int j = 0; j < 3; ++j) DX[a][j] = p[j + 1][a] - p[0][a];
     Q.nv = P.nv;
     for (int v = 0; v < P.nv; ++v) {
-        const uint32_t w = P.nb[v];
-        Q.nb[v] = w;
-        const uint32_t tf = (w >> 24) & 0xFu;
-        uint32_t ap = 0;
-        double pc[3], dist[3];
-        for (int a = 0; a < 3; ++a)
-            if ((w >> (28 + a)) & 1u) {
-                const double xv = (double)P.x[v][a] + org[a];
-                const double dl = fabs(xv - plo[a]), dh = fabs(xv - phi[a]);
-                pc[a] = dl <= dh ? plo[a] : phi[a];
-                dist[a] = (dl <= dh ? dl : dh) / tol[a];
-                if (dist[a] <= 1.0) ap |= 1u << a;
-            }
-        // a vertex near the edge or corner of its voxel can keep a fourth tag:
-        // the tet-face tags are exact, so drop the farthest grid plane
-        while (__popc(tf) + __popc(ap) > 3 && ap) {
-            int far = -1;
-            for (int a = 0; a < 3; ++a)
-                if (((ap >> a) & 1u) && (far < 0 || dist[a] > dist[far])) far = a;
-            ap &= ~(1u << far);
-        }
-        double n[3][3], b[3], q[3];
-        bool ok = __popc(tf) + __popc(ap) == 3;
-        if (ok) {
-            int r = 0;
-            if (tf & 1u) { n[r][0] = 1.0; n[r][1] = 1.0; n[r][2] = 1.0; b[r] = 1.0; ++r; }
-            for (int j = 0; j < 3; ++j)
-                if ((tf >> (j + 1)) & 1u) {
-                    n[r][0] = j == 0; n[r][1] = j == 1; n[r][2] = j == 2; b[r] = 0.0; ++r;
-                }
-            for (int a = 0; a < 3; ++a)
-                if ((ap >> a) & 1u) {
-                    n[r][0] = DX[a][0]; n[r][1] = DX[a][1]; n[r][2] = DX[a][2]; b[r] = pc[a] - p[0][a]; ++r;
-                }
-            ok = solve3(n, b, q);
-        }
-        if (!ok) {
-            // position -> q through the tet's own map: rows DX[a], right side x_a - x0_a
-            for (int a = 0; a < 3; ++a) {
-                n[a][0] = DX[a][0]; n[a][1] = DX[a][1]; n[a][2] = DX[a][2];
-                b[a] = ((double)P.x[v][a] + org[a]) - p[0][a];
-            }
-            if (!solve3(n, b, q)) q[0] = q[1] = q[2] = 0.0; // a flat tet: its fragments have no volume
-        }
-        for (int i = 0; i < 3; ++i) Q.q[v][i] = q[i];
+        Q.nb[v] = P.nb[v];
+        exact_q(P.x[v], P.nb[v], p[0], DX, org, plo, phi, tol, Q.q[v]);
     }
 }
 

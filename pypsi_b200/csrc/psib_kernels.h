@@ -101,6 +101,34 @@ int clip_blocks_per_sm_mixed(bool big, bool fp64_walk, int block);
 cudaError_t launch_adjoint(const ClipArgs &a, bool big, int grid, int block, cudaStream_t s);
 int adjoint_blocks_per_sm(bool big, int block);
 
+// Breadth-first clip of the main tet images (mixed precision, bfs.cu).
+// Polyhedra in flight between levels, in 32-wide tiles: element e's vertex v,
+// coordinate c at x[((e/32 * MAXV + v) * 3 + c) * 32 + e%32], its links at
+// nb[(e/32 * MAXV + v) * 32 + e%32]; nv == 0 marks an element to skip.
+struct PolyQueue {
+    float *x;
+    uint32_t *nb;
+    uint8_t *nv;
+    uint32_t *box;            // 3 per element: lo | hi << 16
+    uint32_t *item;
+    unsigned long long *count;
+    unsigned long long cap;
+};
+struct BfsArgs {
+    ClipArgs c;               // frames, queue order, grid, records, status, counters, scale
+    PolyQueue in, out, leaf;  // level: in -> out and leaf; init: -> out and leaf; leaf kernel: leaf
+    long long q0, q1;         // init: queue positions of this pass
+    int *dfs_list;            // init: images that need the window clip (depth-first kernel)
+    unsigned long long *dfs_count;
+    int last;                 // level: the last level, which must leave no polyhedron unfinished
+    double *vsum;             // per image: sum of its fragment q-volumes (leaf), for the mass correction
+};
+// each launches one resident wave of grid-stride blocks on num_sms SMs
+cudaError_t launch_bfs_init(const BfsArgs &a, int num_sms, cudaStream_t s);
+cudaError_t launch_bfs_level(const BfsArgs &a, int num_sms, cudaStream_t s);
+cudaError_t launch_bfs_leaf(const BfsArgs &a, int num_sms, cudaStream_t s);
+cudaError_t launch_bfs_finalize(const BfsArgs &a, long long nitems, int num_sms, cudaStream_t s);
+
 cudaError_t launch_tess_count(const TessArgs &a, cudaStream_t s);
 cudaError_t launch_tess_emit(const TessArgs &a, cudaStream_t s);
 
