@@ -90,6 +90,37 @@ __device__ __forceinline__ bool one_voxel(const int* lo, const int* hi)
 
 // ---- init: tet images -> first polyhedra ----
 
+// q-volume (fraction of the tet) inside the window planes of wmask, clipped in
+// FP64 as the depth-first kernel's window clip does.
+__device__ double window_volume(const double (*p)[3], uint32_t wmask, const GridDev& g)
+{
+    Poly<double> W[2];
+    init_tet(W[0], p);
+    int cw = 0;
+    double sd[MAXV];
+    for (int pl = 0; pl < 6 && W[cw].nv > 0; ++pl) {
+        if (!((wmask >> pl) & 1u)) continue;
+        const int ax = pl >> 1;
+        const bool lo_side = !(pl & 1);
+        double smin = 1.0e30, smax = -1.0e30;
+        uint32_t um = 0;
+        for (int v = 0; v < W[cw].nv; ++v) {
+            const double t0 = lo_side ? W[cw].x[v][ax] - g.w0[ax] : g.w1[ax] - W[cw].x[v][ax];
+            sd[v] = t0;
+            if (t0 < smin) smin = t0;
+            if (t0 > smax) smax = t0;
+            if (t0 < 0.0) um |= 1u << v;
+        }
+        if (smin >= 0.0) continue;
+        if (smax <= 0.0) return 0.0;
+        if (cut_poly<double, false>(W[cw], sd, um, W[1 - cw], W[1 - cw], axis_tag(ax))) return 0.0;
+        cw = 1 - cw;
+    }
+    double m[10];
+    if (reduce_poly(W[cw], m, 0)) return 0.0;
+    return m[0];
+}
+
 __global__ void __launch_bounds__(BB) k_bfs_init(BfsArgs a)
 {
     const int lane = threadIdx.x & 31;
@@ -103,6 +134,7 @@ __global__ void __launch_bounds__(BB) k_bfs_init(BfsArgs a)
         double p[4][3];
         int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
         bool window = false;
+        uint32_t wmask = 0; // window planes: bit 2a keeps x_a >= w0_a, bit 2a+1 keeps x_a <= w1_a
         if (act) {
             t = a.c.order[i];
             const double* fr = a.c.it.frame + (size_t)t * FRAME;
@@ -117,6 +149,7 @@ __global__ void __launch_bounds__(BB) k_bfs_init(BfsArgs a)
                 }
                 const bool clo = a.c.g.w0[c] > cmin, chi = a.c.g.w1[c] < cmax;
                 window = window || clo || chi;
+                wmask |= (clo ? 1u : 0u) << (2 * c) | (chi ? 1u : 0u) << (2 * c + 1);
                 if (clo) cmin = a.c.g.w0[c];
                 if (chi) cmax = a.c.g.w1[c];
                 lo[c] = (int)floor((cmin - a.c.g.w0[c]) / a.c.g.d[c]);
@@ -126,15 +159,21 @@ __global__ void __launch_bounds__(BB) k_bfs_init(BfsArgs a)
                 if (hi[c] < lo[c]) hi[c] = lo[c];
             }
         }
-        const bool use = act && !window;
-        const bool leaf = use && one_voxel(lo, hi);
+        // the exact FP64 q-volume of a window-clipped image: its mass correction target
+        double target = 1.0;
+        const bool wbfs = act && window && a.window_bfs;
+        if (wbfs) target = window_volume(p, wmask, a.c.g);
+        const bool to_dfs = act && window && !a.window_bfs;
+        const bool use = act && (!window || (wbfs && target > 0.0));
+        const bool leaf = use && !wbfs && one_voxel(lo, hi);
         unsigned od, oq, ol;
-        const unsigned long long bd = warp_reserve(a.dfs_count, act && window ? 1u : 0u, od);
+        const unsigned long long bd = warp_reserve(a.dfs_count, to_dfs ? 1u : 0u, od);
         const unsigned long long bq = warp_reserve(a.out.count, use && !leaf ? 1u : 0u, oq);
         const unsigned long long bl = warp_reserve(a.leaf.count, leaf ? 1u : 0u, ol);
-        if (act && window) a.dfs_list[bd + od] = t;
+        if (to_dfs) a.dfs_list[bd + od] = t;
+        if (wbfs && !use) a.c.scale[t] = 1.0; // wholly outside the window: deposits nothing
         if (use) {
-            a.c.scale[t] = -1.0; // marks a breadth-first image: bfs_finalize sets its mass correction
+            a.c.scale[t] = -target; // marks a breadth-first image: bfs_finalize sets its mass correction
             a.vsum[t] = 0.0;
             const PolyQueue& Q = leaf ? a.leaf : a.out;
             const unsigned long long e = leaf ? bl + ol : bq + oq;
@@ -149,6 +188,7 @@ __global__ void __launch_bounds__(BB) k_bfs_init(BfsArgs a)
                     Q.nb[qn(e, v)] = links[v] | ((0xFu & ~(1u << v)) << 24);
                 }
                 Q.nv[e] = 4;
+                Q.win[e] = (uint8_t)(wbfs ? wmask : 0u);
                 put_box(Q, e, lo, hi);
                 Q.item[e] = (uint32_t)t;
             }
@@ -184,10 +224,10 @@ __device__ __forceinline__ bool link_cut_shared(uint32_t* nbs, int base, int nv)
 // nbI; upper side = bits of um, s = cr - x[ax]) into element el of QL (lower
 // side) and eu of QU (upper side), with the vertex order and arithmetic of
 // cut_poly.
-__device__ __forceinline__ unsigned bfs_cut(int nv, uint32_t um, float cr, int ax, const float* xI,
+__device__ __forceinline__ unsigned bfs_cut(int nv, uint32_t um, float cr, float sg, int ax, const float* xI,
                                             const uint32_t* nbI, uint32_t* nbL, uint32_t* nbU, const PolyQueue& QL,
                                             unsigned long long el, const PolyQueue& QU, unsigned long long eu,
-                                            uint32_t cut_tag)
+                                            bool keep_up, uint32_t cut_tag)
 {
     const uint32_t lmask = ((1u << nv) - 1u) & ~um;
     const int nl = __popc(lmask), nu = __popc(um);
@@ -197,7 +237,8 @@ __device__ __forceinline__ unsigned bfs_cut(int nv, uint32_t um, float cr, int a
         const int j = rank_in(sm, v);
         const PolyQueue& Q = u ? QU : QL;
         const unsigned long long d = u ? eu : el;
-        for (int c = 0; c < 3; ++c) Q.x[qx(d, j, c)] = AT(xI, 3 * v + c);
+        if (!u || keep_up)
+            for (int c = 0; c < 3; ++c) Q.x[qx(d, j, c)] = AT(xI, 3 * v + c);
         const uint32_t w = AT(nbI, v);
         uint32_t ow = 0xFFFFFFu | (w & ALL_TAGS);
         for (int k = 0; k < 3; ++k) {
@@ -229,12 +270,12 @@ __device__ __forceinline__ unsigned bfs_cut(int nv, uint32_t um, float cr, int a
         {
             const int vn = nbget(w, np);
             if (nl + k >= MAXV || nu + k >= MAXV) return ST_OVERFLOW;
-            const float sc = cr - AT(xI, 3 * vc + ax), sn = cr - AT(xI, 3 * vn + ax);
+            const float sc = sg * (cr - AT(xI, 3 * vc + ax)), sn = sg * (cr - AT(xI, 3 * vn + ax));
             const float iw = 1.0f / (sc - sn);
             for (int c = 0; c < 3; ++c) {
                 const float px = iw * (AT(xI, 3 * vn + c) * sc - AT(xI, 3 * vc + c) * sn);
                 QL.x[qx(el, nl + k, c)] = px;
-                QU.x[qx(eu, nu + k, c)] = px;
+                if (keep_up) QU.x[qx(eu, nu + k, c)] = px;
             }
             const uint32_t wn = AT(nbI, vn);
             const uint32_t tg = (w & wn & ALL_TAGS) | cut_tag;
@@ -248,11 +289,13 @@ __device__ __forceinline__ unsigned bfs_cut(int nv, uint32_t um, float cr, int a
             ++k;
         }
     }
-    if (!link_cut_shared(nbL, nl, nl + k) || !link_cut_shared(nbU, nu, nu + k)) return ST_GRAPH;
+    if (!link_cut_shared(nbL, nl, nl + k) || (keep_up && !link_cut_shared(nbU, nu, nu + k))) return ST_GRAPH;
     for (int v = 0; v < nl + k; ++v) QL.nb[qn(el, v)] = AT(nbL, v);
-    for (int v = 0; v < nu + k; ++v) QU.nb[qn(eu, v)] = AT(nbU, v);
     QL.nv[el] = (uint8_t)(nl + k);
-    QU.nv[eu] = (uint8_t)(nu + k);
+    if (keep_up) {
+        for (int v = 0; v < nu + k; ++v) QU.nb[qn(eu, v)] = AT(nbU, v);
+        QU.nv[eu] = (uint8_t)(nu + k);
+    }
     return 0;
 }
 
@@ -274,9 +317,9 @@ __global__ void __launch_bounds__(BB) k_bfs_level(BfsArgs a)
         const unsigned long long e = base + lane;
         bool act = e < n;
         int nv = 0, lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0}, ax = 0, nlo = 0, nup = 0;
-        uint32_t um = 0, t = 0;
-        float cr = 0.0f;
-        bool cut = false, toleaf = false;
+        uint32_t um = 0, t = 0, win = 0;
+        float cr = 0.0f, sg = 1.0f;
+        bool cut = false, toleaf = false, wcut = false;
         if (act) {
             nv = a.in.nv[e];
             if (nv < 4 || nv > MAXV) act = false; // a failed cut upstream (status already set)
@@ -289,7 +332,26 @@ __global__ void __launch_bounds__(BB) k_bfs_level(BfsArgs a)
                 AT(nbI, v) = a.in.nb[qn(e, v)];
                 for (int c = 0; c < 3; ++c) AT(xI, 3 * v + c) = a.in.x[qx(e, v, c)];
             }
+            win = a.in.win[e];
             for (int guard = 0; guard < 64; ++guard) {
+                if (win) {
+                    // a pending window plane, kept side s >= 0 as in the window clip
+                    // (src/geometry.c:391-501): s = x - w0 or w1 - x
+                    const int pl = __ffs(win) - 1;
+                    win &= ~(1u << pl);
+                    ax = pl >> 1;
+                    const bool lo_side = !(pl & 1);
+                    cr = (float)((lo_side ? a.c.g.w0[ax] : a.c.g.w1[ax]) - fr[ax]);
+                    sg = lo_side ? -1.0f : 1.0f;
+                    um = 0;
+                    for (int v = 0; v < nv; ++v)
+                        if (sg * (cr - AT(xI, 3 * v + ax)) < 0.0f) um |= 1u << v;
+                    if (um == 0) continue;                   // wholly inside this plane
+                    if (um == (1u << nv) - 1u) { act = false; break; } // wholly outside
+                    wcut = true;
+                    break;
+                }
+                sg = 1.0f;
                 int dmax = 0;
                 ax = 0;
                 for (int c = 0; c < 3; ++c) {
@@ -311,14 +373,16 @@ __global__ void __launch_bounds__(BB) k_bfs_level(BfsArgs a)
                 cut = true;
                 break;
             }
-            if (!cut && !toleaf) { st |= ST_DEPTH; act = false; }
+            if (act && !cut && !toleaf && !wcut) { st |= ST_DEPTH; act = false; }
         }
+        if (!act) { cut = toleaf = wcut = false; }
         int llo[3], lhi[3], ulo[3], uhi[3];
         for (int c = 0; c < 3; ++c) { llo[c] = ulo[c] = lo[c]; lhi[c] = uhi[c] = hi[c]; }
         if (cut) { lhi[ax] -= nup; ulo[ax] += nlo; }
-        const bool leafL = cut && one_voxel(llo, lhi), leafU = cut && one_voxel(ulo, uhi);
-        const unsigned nq = cut ? (unsigned)(!leafL) + (unsigned)(!leafU) : 0u;
-        const unsigned nlf = toleaf ? 1u : cut ? (unsigned)leafL + (unsigned)leafU : 0u;
+        const bool leafL = (cut && one_voxel(llo, lhi)) || (wcut && !win && one_voxel(lo, hi));
+        const bool leafU = cut && one_voxel(ulo, uhi);
+        const unsigned nq = cut ? (unsigned)(!leafL) + (unsigned)(!leafU) : wcut ? (unsigned)(!leafL) : 0u;
+        const unsigned nlf = toleaf ? 1u : cut ? (unsigned)leafL + (unsigned)leafU : wcut ? (unsigned)leafL : 0u;
         if (a.last && nq) st |= ST_DEPTH;
         unsigned oq, ol;
         const unsigned long long bq = warp_reserve(a.out.count, nq, oq);
@@ -346,7 +410,8 @@ __global__ void __launch_bounds__(BB) k_bfs_level(BfsArgs a)
             if (el >= QL.cap || eu >= QU.cap) {
                 st |= ST_OVERFLOW;
             } else {
-                const unsigned e2 = bfs_cut(nv, um, cr, ax, xI, nbI, nbL, nbU, QL, el, QU, eu, axis_tag(ax));
+                const unsigned e2 =
+                    bfs_cut(nv, um, cr, 1.0f, ax, xI, nbI, nbL, nbU, QL, el, QU, eu, true, axis_tag(ax));
                 if (e2) {
                     st |= e2;
                     QL.nv[el] = 0; // downstream kernels skip these
@@ -356,6 +421,25 @@ __global__ void __launch_bounds__(BB) k_bfs_level(BfsArgs a)
                 put_box(QU, eu, ulo, uhi);
                 QL.item[el] = t;
                 QU.item[eu] = t;
+                QL.win[el] = 0;
+                QU.win[eu] = 0;
+            }
+        }
+        if (wcut) {
+            // the window cut keeps one child: the side with s >= 0
+            const PolyQueue& QL = leafL ? a.leaf : a.out;
+            const unsigned long long el = leafL ? bl + ol : bq + oq;
+            if (el >= QL.cap) {
+                st |= ST_OVERFLOW;
+            } else {
+                const unsigned e2 = bfs_cut(nv, um, cr, sg, ax, xI, nbI, nbL, nbU, QL, el, QL, el, false, axis_tag(ax));
+                if (e2) {
+                    st |= e2;
+                    QL.nv[el] = 0;
+                }
+                put_box(QL, el, lo, hi);
+                QL.item[el] = t;
+                QL.win[el] = (uint8_t)win;
             }
         }
     }
@@ -520,11 +604,13 @@ __global__ void __launch_bounds__(BB) k_bfs_leaf(BfsArgs a)
 
 // FP32 walks can misplace a vertex that falls back to its FP32 position by
 // ~1e-7 of the tet: each breadth-first image's fragment masses are scaled by
-// 1 / (sum of its fragment q-volumes), so that it deposits exactly its mass.
+// target / (sum of its fragment q-volumes), so that it deposits exactly its
+// mass inside the window.  init stores -target in scale (1, or the image's
+// exact FP64 q-volume inside the window).
 __global__ void k_bfs_finalize(BfsArgs a, long long nitems)
 {
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nitems; t += (long long)gridDim.x * blockDim.x)
-        if (a.c.scale[t] == -1.0) a.c.scale[t] = a.vsum[t] > 0.0 ? 1.0 / a.vsum[t] : 1.0;
+        if (a.c.scale[t] < 0.0) a.c.scale[t] = a.vsum[t] > 0.0 ? -a.c.scale[t] / a.vsum[t] : 1.0;
 }
 
 cudaError_t launch_bfs_finalize(const BfsArgs& a, long long nitems, int num_sms, cudaStream_t s)

@@ -98,7 +98,7 @@ struct Ctx {
     // records
     DevBuf rkey, rmom, rkey_sorted, rperm_in, rperm, rvox, ritem, rmom_sorted, run_vox, run_cnt, run_off;
     // breadth-first clip: three polyhedron queues, the volume histogram, per-level counters, window list
-    DevBuf qx[3], qnb[3], qnv[3], qbox[3], qitem[3], hist, bfs_cnt, dfs_list, vsum;
+    DevBuf qx[3], qnb[3], qnv[3], qwin[3], qbox[3], qitem[3], hist, bfs_cnt, dfs_list, vsum;
     std::vector<DevBuf*> all()
     {
         return {&hpos, &hgpos, &hgmass, &hvel, &hmass, &hconn, &hfield[0], &hfield[1], &hfield[2], &hfield[3], &hfield[4],
@@ -106,7 +106,8 @@ struct Ctx {
                 &key_sorted, &order_in, &order, &counts, &offsets, &cub_tmp, &scratch, &scratch_big, &iscale, &small, &rkey, &rmom,
                 &rkey_sorted, &rperm_in, &rperm, &rvox, &ritem, &rmom_sorted, &run_vox, &run_cnt, &run_off,
                 &qx[0], &qx[1], &qx[2], &qnb[0], &qnb[1], &qnb[2], &qnv[0], &qnv[1], &qnv[2], &qbox[0], &qbox[1],
-                &qbox[2], &qitem[0], &qitem[1], &qitem[2], &hist, &bfs_cnt, &dfs_list, &vsum};
+                &qbox[2], &qitem[0], &qitem[1], &qitem[2], &hist, &bfs_cnt, &dfs_list, &vsum, &qwin[0], &qwin[1],
+                &qwin[2]};
     }
 };
 
@@ -133,10 +134,18 @@ int get_ctx(int dev, Ctx** out)
 enum { S_STATUS = 0, S_CNT = 1 /* 3 words */, S_TESS = 4 /* 2 */, S_HEAD = 8 /* 4 */, S_RECN = 12, S_NDEEP = 13,
        S_DFS = 14, S_WORDS = 16 };
 
+// Histogram of the sorted footprint keys: lanes holding equal keys (most of a
+// warp, as the keys are sorted) add with one atomic.
 __global__ void k_key_hist(const uint16_t* key, long long n, unsigned* hist)
 {
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        atomicAdd(&hist[key[i]], 1u);
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long n32 = (n + 31) / 32 * 32;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n32; i += stride) {
+        const bool act = i < n;
+        const unsigned k = act ? key[i] : 0x10000u;
+        const unsigned peers = __match_any_sync(0xFFFFFFFFu, k);
+        if (act && (threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&hist[k], (unsigned)__popc(peers));
+    }
 }
 
 __global__ void k_count_deep(const uint16_t* key, long long n, unsigned long long* out)
@@ -233,31 +242,54 @@ int bfs_clip(Ctx& C, ClipArgs& ca, long long nmain, long long nitems, unsigned l
     }
     if (qb.back() != pos) qb.push_back(pos);
     if (pos != nmain) return fail(PSIB_ERR_CUDA, "footprint histogram covers %lld of %lld images", pos, nmain);
-
-    const size_t tiles = (size_t)(cap + 31) / 32;
+    // the largest pass bounds every queue
+    long long need = 0;
+    {
+        size_t p = 0;
+        long long acc = 0, at = 0;
+        for (int k = 0; k < 0xFFFF && p + 1 < qb.size(); ++k) {
+            const long long vol = std::max(1, 0xFFFE - k);
+            for (long long cnt = hist[k]; cnt > 0;) {
+                const long long take = std::min(cnt, qb[p + 1] - at);
+                acc += take * vol;
+                at += take;
+                cnt -= take;
+                if (at == qb[p + 1]) {
+                    need = std::max(need, acc);
+                    acc = 0;
+                    if (++p + 1 >= qb.size()) break;
+                }
+            }
+        }
+    }
+    const size_t tiles = (size_t)(std::max<long long>(std::min(need, cap), 32) + 31) / 32;
     PolyQueue Q[3];
     for (int i = 0; i < 3; ++i) {
         RET(ensure(C.qx[i], tiles * 32 * MAXV * 3 * sizeof(float)));
         RET(ensure(C.qnb[i], tiles * 32 * MAXV * sizeof(uint32_t)));
         RET(ensure(C.qnv[i], tiles * 32));
+        RET(ensure(C.qwin[i], tiles * 32));
         RET(ensure(C.qbox[i], tiles * 32 * 3 * sizeof(uint32_t)));
         RET(ensure(C.qitem[i], tiles * 32 * sizeof(uint32_t)));
         Q[i] = PolyQueue{C.qx[i].as<float>(), C.qnb[i].as<uint32_t>(), C.qnv[i].as<uint8_t>(),
-                         C.qbox[i].as<uint32_t>(), C.qitem[i].as<uint32_t>(), nullptr,
+                         C.qwin[i].as<uint8_t>(), C.qbox[i].as<uint32_t>(), C.qitem[i].as<uint32_t>(), nullptr,
                          (unsigned long long)tiles * 32};
     }
     RET(ensure(C.dfs_list, (size_t)std::max<long long>(nmain, 1) * sizeof(int)));
-    // per pass: level-queue counts [0, DMAX_MAIN] and leaf-queue counts [DMAX_MAIN + 1, 2 DMAX_MAIN + 1]
-    constexpr int NCNT = 2 * DMAX_MAIN + 2;
+    // levels: the bisection (at most DMAX_MAIN cuts) and up to 6 window planes
+    constexpr int NLEV = DMAX_MAIN + 6;
+    // per pass: level-queue counts [0, NLEV] and leaf-queue counts [NLEV + 1, 2 NLEV + 1]
+    constexpr int NCNT = 2 * NLEV + 2;
     RET(ensure(C.bfs_cnt, NCNT * sizeof(unsigned long long)));
     unsigned long long* cq = C.bfs_cnt.as<unsigned long long>();
-    unsigned long long* cl = cq + DMAX_MAIN + 1;
+    unsigned long long* cl = cq + NLEV + 1;
     CK(cudaMemsetAsync(&sm[S_DFS], 0, 8, st));
 
     BfsArgs ba = {};
     ba.c = ca;
     ba.dfs_list = C.dfs_list.as<int>();
     ba.dfs_count = &sm[S_DFS];
+    ba.window_bfs = env_ll("PSIB_BFS_WINDOW", 1) != 0;
     RET(ensure(C.vsum, (size_t)std::max<long long>(nitems, 1) * sizeof(double)));
     ba.vsum = C.vsum.as<double>();
     const int grid = C.num_sms;
@@ -272,19 +304,19 @@ int bfs_clip(Ctx& C, ClipArgs& ca, long long nmain, long long nitems, unsigned l
         CK(launch_bfs_init(ba, grid, st));
         CK(launch_bfs_leaf(ba, grid, st));
         int ia = 0;
-        for (int lvl = 0; lvl < DMAX_MAIN; ++lvl) {
+        for (int lvl = 0; lvl < NLEV; ++lvl) {
             ba.in = Q[ia];
             ba.in.count = &cq[lvl];
             ba.out = Q[1 - ia];
             ba.out.count = &cq[lvl + 1];
             ba.leaf.count = &cl[lvl + 1];
-            ba.last = lvl == DMAX_MAIN - 1;
+            ba.last = lvl == NLEV - 1;
             CK(launch_bfs_level(ba, grid, st));
             CK(launch_bfs_leaf(ba, grid, st));
             ia = 1 - ia;
         }
-        klaunch += 2 + 2 * DMAX_MAIN;
-        launches += 2 + 2 * DMAX_MAIN;
+        klaunch += 2 + 2 * NLEV;
+        launches += 2 + 2 * NLEV;
     }
     CK(launch_bfs_finalize(ba, nitems, C.num_sms, st));
     klaunch++;

@@ -507,17 +507,17 @@ __device__ __forceinline__ void exact_q(const float* x, uint32_t w, const double
         const double xv = (double)x[a] + org[a];
         const double dl = fabs(xv - plo[a]), dh = fabs(xv - phi[a]);
         pc[a] = dl <= dh ? plo[a] : phi[a];
-        dist[a] = (dl <= dh ? dl : dh) / tol[a];
-        if (((w >> (28 + a)) & 1u) && dist[a] <= 1.0) ap |= 1u << a;
+        dist[a] = dl <= dh ? dl : dh;
+        if (((w >> (28 + a)) & 1u) && dist[a] <= tol[a]) ap |= 1u << a;
     }
     // a vertex near the edge or corner of its voxel can keep a fourth tag:
-    // the tet-face tags are exact, so drop the farthest grid plane
+    // the tet-face tags are exact, so drop the grid plane farthest in units of tol
     while (__popc(tf) + __popc(ap) > 3) {
         int far = -1;
         double df = -1.0;
 #pragma unroll
         for (int a = 0; a < 3; ++a)
-            if (((ap >> a) & 1u) && dist[a] > df) { far = a; df = dist[a]; }
+            if (((ap >> a) & 1u) && dist[a] / tol[a] > df) { far = a; df = dist[a] / tol[a]; }
         if (far < 0) break;
         ap &= ~(1u << far);
     }

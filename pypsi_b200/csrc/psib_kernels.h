@@ -109,6 +109,7 @@ struct PolyQueue {
     float *x;
     uint32_t *nb;
     uint8_t *nv;
+    uint8_t *win;             // window planes still to cut: bit 2a keeps x_a >= w0_a, 2a+1 keeps x_a <= w1_a
     uint32_t *box;            // 3 per element: lo | hi << 16
     uint32_t *item;
     unsigned long long *count;
@@ -122,6 +123,8 @@ struct BfsArgs {
     unsigned long long *dfs_count;
     int last;                 // level: the last level, which must leave no polyhedron unfinished
     double *vsum;             // per image: sum of its fragment q-volumes (leaf), for the mass correction
+    int window_bfs;           // init: window-clipped images are walked here too (else listed for the
+                              // depth-first kernel)
 };
 // each launches one resident wave of grid-stride blocks on num_sms SMs
 cudaError_t launch_bfs_init(const BfsArgs &a, int num_sms, cudaStream_t s);
