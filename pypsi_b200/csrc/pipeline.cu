@@ -644,7 +644,7 @@ int run_device(Call& c)
             RET(ensure(C.rperm, nrec * 4));
             RET(ensure(C.rvox, nrec * 4));
             RET(ensure(C.ritem, nrec * 4));
-            RET(ensure(C.rmom_sorted, nrec * 8 * nmom));
+            if (!central) RET(ensure(C.rmom_sorted, nrec * 8 * nmom));
             const long long maxruns = std::min<long long>((long long)nrec, nvox);
             RET(ensure(C.run_vox, (size_t)maxruns * 4));
             RET(ensure(C.run_cnt, (size_t)maxruns * 4 + 8));
@@ -668,7 +668,7 @@ int run_device(Call& c)
             ga.ibits = ibits;
             ga.vox = C.rvox.as<unsigned>();
             ga.item = C.ritem.as<unsigned>();
-            ga.mom_sorted = C.rmom_sorted.as<double>();
+            ga.mom_sorted = central ? nullptr : C.rmom_sorted.as<double>();
             CK(launch_gather_records(ga, st));
             // voxel runs: (voxel, count) pairs, then their offsets
             int* d_nruns = (int*)(C.run_cnt.as<char>() + (size_t)maxruns * 4);
@@ -693,7 +693,8 @@ int run_device(Call& c)
             aa.run_off = C.run_off.as<long long>();
             aa.nruns = nruns;
             aa.item = C.ritem.as<unsigned>();
-            aa.mom = C.rmom_sorted.as<double>();
+            aa.mom = central ? C.rmom.as<double>() : C.rmom_sorted.as<double>();
+            aa.perm = C.rperm.as<unsigned>();
             aa.nmom = nmom;
             aa.central = central;
             aa.scale = ca.scale;

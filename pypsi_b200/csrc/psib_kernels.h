@@ -144,7 +144,7 @@ struct GatherArgs {
     int nmom, ibits;
     unsigned *vox;                 // out: voxel of each sorted record
     unsigned *item;                // out: item of each sorted record
-    double *mom_sorted;            // out: moments in key order
+    double *mom_sorted;            // out: moments in key order (null: not gathered)
 };
 cudaError_t launch_gather_records(const GatherArgs &a, cudaStream_t s);
 
@@ -155,7 +155,8 @@ struct ApplyArgs {
     const long long *run_off;      // first sorted record of each run
     long long nruns;
     const unsigned *item;          // item of each sorted record
-    const double *mom;             // moments of each sorted record
+    const double *mom;             // moments: of each sorted record, or (central) in record order
+    const unsigned *perm;          // central: sorted position -> record
     int nmom;
     int central;                   // records hold m0, q-centroid, central second moment
     const double *scale;           // per item mass correction (central records)

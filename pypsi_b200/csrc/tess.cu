@@ -401,6 +401,7 @@ __global__ void k_gather_records(GatherArgs a)
     const unsigned long long k = a.key[j];
     a.vox[j] = (unsigned)(k >> a.ibits);
     a.item[j] = (unsigned)(k & ((1ull << a.ibits) - 1ull));
+    if (!a.mom_sorted) return; // central records are read through the permutation
     const double* src = a.mom + (long long)a.perm[j] * a.nmom;
     double* dst = a.mom_sorted + j * a.nmom;
     for (int m = 0; m < a.nmom; ++m) dst[m] = src[m];
@@ -491,10 +492,169 @@ __global__ void __launch_bounds__(128) k_apply_runs(ApplyArgs a)
     }
 }
 
+// Central-form records (mixed precision and FP64-central): the update order
+// within a voxel is free, because the merge of src/geometry.c:164-186 is
+// associative in exact arithmetic -- the result is
+//   M = sum m_f,  X = sum m_f x_f / M,
+//   XX = (sum m_f S_f + sum m_f (x_f - X)(x_f - X)^T) / M   (XV, VV alike).
+// A group of AG lanes takes one voxel run: each lane projects every AG-th
+// record (read through the sort permutation) and sums m, m dx, m dv and
+// m (S + dx dy^T) about the centroid of the run's first record (no
+// cancellation in FP64); the group adds its lanes' sums with shuffles, and its
+// first lane merges them once into the voxel's fields.
+constexpr int AG = 8;
+
+__device__ __forceinline__ double group_sum(double v)
+{
+#pragma unroll
+    for (int o = AG / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+    return v;
+}
+
+__global__ void __launch_bounds__(128) k_apply_central(ApplyArgs a)
+{
+    const long long gid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long r = gid / AG;
+    const int l = (int)(gid % AG);
+    // whole groups run the shuffles; a group past the last run does nothing else
+    const bool run_ok = r < a.nruns;
+    const bool hx = a.X, hv = a.V, hxx = a.XX, hxv = a.XV, hvv = a.VV;
+    const long long beg = run_ok ? a.run_off[r] : 0, cnt = run_ok ? a.run_cnt[r] : 0;
+    double rx[3] = {0, 0, 0}, rv[3] = {0, 0, 0}; // reference point: the first record's centroids
+    double sm = 0.0, sx[3] = {0, 0, 0}, sv[3] = {0, 0, 0}, sxx[6] = {0, 0, 0, 0, 0, 0}, svv[6] = {0, 0, 0, 0, 0, 0};
+    double sxv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    auto project = [&](long long j, double& m, double* cm, double* cv, double (*Sxx)[3], double (*Sxv)[3],
+                       double (*Svv)[3]) {
+        const long long jj = beg + j;
+        const long long t = a.item_base + (long long)a.item[jj];
+        const double* mom = a.mom + (long long)a.perm[jj] * a.nmom;
+        const double* fr = a.it.frame + t * FRAME;
+        double p0[3], v0[3], DX[3][3], DV[3][3];
+        for (int i = 0; i < 3; ++i) {
+            p0[i] = fr[i];
+            v0[i] = fr[FR_U + i];
+            for (int k = 0; k < 3; ++k) {
+                DX[i][k] = fr[3 * (k + 1) + i] - p0[i];
+                DV[i][k] = fr[FR_U + 3 * (k + 1) + i] - v0[i];
+            }
+        }
+        m = fr[FR_MASS] * a.scale[t] * mom[0];
+        if (a.nmom > 1) mixed_fragment(mom, p0, DX, v0, DV, hx, hv, hxx, hxv, hvv, cm, cv, Sxx, Sxv, Svv);
+    };
+    auto accumulate = [&](double m, const double* cm, const double* cv, const double (*Sxx)[3],
+                          const double (*Sxv)[3], const double (*Svv)[3]) {
+        double dx[3], dv[3];
+        for (int i = 0; i < 3; ++i) {
+            dx[i] = cm[i] - rx[i];
+            dv[i] = cv[i] - rv[i];
+        }
+        sm += m;
+        for (int i = 0; i < 3; ++i) {
+            sx[i] += m * dx[i];
+            sv[i] += m * dv[i];
+        }
+        int k = 0;
+        for (int i = 0; i < 3; ++i)
+            for (int j2 = i; j2 < 3; ++j2, ++k) {
+                if (hxx) sxx[k] += m * (Sxx[i][j2] + dx[i] * dx[j2]);
+                if (hvv) svv[k] += m * (Svv[i][j2] + dv[i] * dv[j2]);
+            }
+        if (hxv)
+            for (int i = 0; i < 3; ++i)
+                for (int j2 = 0; j2 < 3; ++j2) sxv[3 * i + j2] += m * (Sxv[i][j2] + dx[i] * dv[j2]);
+    };
+    {
+        // the first record of each lane; lane 0's (always present in a run) is the reference point,
+        // broadcast by every lane of the warp outside any divergent loop
+        double m = 0.0, cm[3] = {0, 0, 0}, cv[3] = {0, 0, 0}, Sxx[3][3], Sxv[3][3], Svv[3][3];
+        const bool has = l < cnt;
+        if (has) project(l, m, cm, cv, Sxx, Sxv, Svv);
+        const int src = (threadIdx.x & 31) & ~(AG - 1);
+        for (int i = 0; i < 3; ++i) {
+            rx[i] = __shfl_sync(0xFFFFFFFFu, cm[i], src);
+            rv[i] = __shfl_sync(0xFFFFFFFFu, cv[i], src);
+        }
+        if (has) accumulate(m, cm, cv, Sxx, Sxv, Svv);
+    }
+    for (long long j = AG + l; j < cnt; j += AG) {
+        double m = 0.0, cm[3] = {0, 0, 0}, cv[3] = {0, 0, 0}, Sxx[3][3], Sxv[3][3], Svv[3][3];
+        project(j, m, cm, cv, Sxx, Sxv, Svv);
+        accumulate(m, cm, cv, Sxx, Sxv, Svv);
+    }
+    sm = group_sum(sm);
+    for (int i = 0; i < 3; ++i) {
+        if (hx || hxx || hxv) sx[i] = group_sum(sx[i]);
+        if (hv || hvv || hxv) sv[i] = group_sum(sv[i]);
+    }
+    for (int k = 0; k < 6; ++k) {
+        if (hxx) sxx[k] = group_sum(sxx[k]);
+        if (hvv) svv[k] = group_sum(svv[k]);
+    }
+    if (hxv)
+        for (int k = 0; k < 9; ++k) sxv[k] = group_sum(sxv[k]);
+    if (!run_ok || l != 0 || !(sm > 0.0)) return;
+    // this voxel's new fragments as one: mass, means, central (co)variances
+    const long long gi = (long long)a.run_vox[r];
+    double xr[3], vr[3], dxr[3], dvr[3];
+    for (int i = 0; i < 3; ++i) {
+        dxr[i] = sx[i] / sm;
+        dvr[i] = sv[i] / sm;
+        xr[i] = rx[i] + dxr[i];
+        vr[i] = rv[i] + dvr[i];
+    }
+    const double M0 = a.M[gi], Mf = M0 + sm;
+    const double cw = sm / Mf, dw = M0 / Mf;
+    // merged with what the voxel holds (src/geometry.c:164-186 for one combined fragment)
+    double X0[3] = {0, 0, 0}, V0[3] = {0, 0, 0};
+    for (int i = 0; i < 3; ++i) {
+        if (hx) X0[i] = a.X[3 * gi + i];
+        if (hv) V0[i] = a.V[3 * gi + i];
+    }
+    if (hxx) {
+        int k = 0;
+        double C[3][3];
+        for (int i = 0; i < 3; ++i)
+            for (int j2 = i; j2 < 3; ++j2, ++k) C[i][j2] = C[j2][i] = sxx[k] / sm - dxr[i] * dxr[j2];
+        for (int i = 0; i < 3; ++i)
+            for (int j2 = 0; j2 < 3; ++j2) {
+                double* t = &a.XX[9 * gi + 3 * i + j2];
+                *t = dw * *t + cw * C[i][j2] + cw * dw * (xr[i] - X0[i]) * (xr[j2] - X0[j2]);
+            }
+    }
+    if (hvv) {
+        int k = 0;
+        double C[3][3];
+        for (int i = 0; i < 3; ++i)
+            for (int j2 = i; j2 < 3; ++j2, ++k) C[i][j2] = C[j2][i] = svv[k] / sm - dvr[i] * dvr[j2];
+        for (int i = 0; i < 3; ++i)
+            for (int j2 = 0; j2 < 3; ++j2) {
+                double* t = &a.VV[9 * gi + 3 * i + j2];
+                *t = dw * *t + cw * C[i][j2] + cw * dw * (vr[i] - V0[i]) * (vr[j2] - V0[j2]);
+            }
+    }
+    if (hxv)
+        for (int i = 0; i < 3; ++i)
+            for (int j2 = 0; j2 < 3; ++j2) {
+                const double C = sxv[3 * i + j2] / sm - dxr[i] * dvr[j2];
+                double* t = &a.XV[9 * gi + 3 * i + j2];
+                *t = dw * *t + cw * C + cw * dw * (xr[i] - X0[i]) * (vr[j2] - V0[j2]);
+            }
+    if (hx)
+        for (int i = 0; i < 3; ++i) a.X[3 * gi + i] = X0[i] + cw * (xr[i] - X0[i]);
+    if (hv)
+        for (int i = 0; i < 3; ++i) a.V[3 * gi + i] = V0[i] + cw * (vr[i] - V0[i]);
+    a.M[gi] = Mf;
+}
+
 cudaError_t launch_apply_records(const ApplyArgs& a, cudaStream_t s)
 {
     if (a.nruns == 0) return cudaSuccess;
-    k_apply_runs<<<(unsigned)((a.nruns + 127) / 128), 128, 0, s>>>(a);
+    if (a.central) {
+        const long long threads = a.nruns * AG;
+        k_apply_central<<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(a);
+    } else {
+        k_apply_runs<<<(unsigned)((a.nruns + 127) / 128), 128, 0, s>>>(a);
+    }
     return cudaGetLastError();
 }
 

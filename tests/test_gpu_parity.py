@@ -154,6 +154,21 @@ def test_accumulates_into_existing_grid(gpu, oracle, det):
         check(field_errors(out, ref), FP64_TOL, "accumulate")
 
 
+def test_mixed_accumulates_into_existing_grid(gpu, oracle):
+    """The mixed path merges each voxel's new fragments into the fields already
+    on the grid in one step; the result is the reference's sequential update
+    within the mixed bound."""
+    a, b = make("c2_small"), make("c2_order1")
+    b["fields"] = a["fields"]
+    ref = run_oracle(oracle, a)
+    ref = oracle.voxelize("restatement", n=b["n"], bounds=b["bounds"], pos=b["pos"].reshape(-1, 3),
+                          vel=b["vel"].reshape(-1, 3), conn=oracle.block_connectivity((16, 16, 16), True),
+                          periodic_box=b["periodic_box"], fields=b["fields"], out=ref)
+    _, grid, _ = run_psi(gpu, a, precision="mixed")
+    out, _, _ = run_psi(gpu, b, grid=grid, precision="mixed")
+    check(field_errors(out, ref), MIXED_TOL, "accumulate mixed")
+
+
 def test_chunked_streaming_matches(gpu, oracle, monkeypatch):
     """Tets streamed in element chunks (a tiny item budget) give the same result."""
     ref, _ = reference(oracle, "c2_small")
