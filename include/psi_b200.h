@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define PSIB_ABI_VERSION 1
+#define PSIB_ABI_VERSION 2
 
 /* status codes */
 #define PSIB_OK 0
@@ -53,6 +53,14 @@ extern "C" {
                         FP64 moments and sums */
 #define PSIB_FP64_CENTRAL 2 /* FP64 walk with moments taken about each fragment: more accurate than the
                                reference for tiny fragments, not bit-identical to it */
+
+/* refinement criterion of trilinear elements (psib_options.refine_mode) */
+#define PSIB_REFINE_MIDPOINT 0 /* the reference's: an edge midpoint of the trilinear map deviates from the
+                                  straight edge by more than refine_tolerance x the smallest cell
+                                  (src/refine.c:223-289, src/cpsi.c:63-66) */
+#define PSIB_REFINE_STRETCH 1  /* not in the reference: a (sub)cube of level l is refined when an edge along
+                                  axis a exceeds refine_tolerance x refine_cell[a] / 2^l, or its volume exceeds
+                                  refine_tolerance x the cell volume / 8^l */
 
 /* where the pointers of psib_grid / psib_mesh live */
 #define PSIB_HOST 0   /* host memory; the library copies in and out */
@@ -114,6 +122,8 @@ typedef struct {
     int device;        /* CUDA device ordinal for PSIB_HOST calls (-1: current) */
     void *stream;      /* cudaStream_t for PSIB_DEVICE calls; NULL: legacy default stream */
     psib_stats *stats; /* optional */
+    int refine_mode;   /* PSIB_REFINE_MIDPOINT (0) or PSIB_REFINE_STRETCH */
+    double refine_cell[3]; /* stretch: the Lagrangian cell; all <= 0: box / block_dims of a periodic block mesh */
 } psib_options;
 
 /* Deposit the mesh's tets on the grid: the density branch of psi_voxels

@@ -96,6 +96,9 @@ def _lib(kind: str) -> C.CDLL:
             lib.oracle_voxels.argtypes = [C.POINTER(_OgGrid), C.POINTER(_OgMesh), C.c_double,
                                           C.c_int, C.POINTER(Counters)]
             lib.oracle_voxels.restype = C.c_int
+            lib.oracle_voxels_ex.argtypes = [C.POINTER(_OgGrid), C.POINTER(_OgMesh), C.c_double, C.c_int, C.c_int,
+                                             C.POINTER(C.c_double), C.POINTER(Counters)]
+            lib.oracle_voxels_ex.restype = C.c_int
         else:
             lib.psi_voxels.argtypes = [C.POINTER(_PsiGrid), C.POINTER(_PsiMesh), C.c_void_p,
                                        C.c_int, C.c_double, C.c_int]
@@ -141,13 +144,15 @@ def new_fields(n, fields):
 
 
 def voxelize(kind, n, bounds, pos, conn, vel=None, mass=None, periodic_box=None, fields=(),
-             reftol=1.0, maxlvl=0, out=None, counters=False):
+             reftol=1.0, maxlvl=0, out=None, counters=False, refine_mode=0, refine_cell=None):
     """Run the density path of the chosen back end.
 
     pos (npart,3) f64, conn (nelem, 4|8) i32, vel like pos (zeros if None),
     mass (nelem,) (ones if None).  ``out`` (a dict of field arrays) is
     accumulated into, as the reference accumulates into grid.fields.
     """
+    if refine_mode and kind == "reference":
+        raise ValueError("the reference has only the midpoint refinement criterion")
     lib = _lib(kind)
     pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
     conn = np.ascontiguousarray(conn, dtype=np.int32)
@@ -178,7 +183,12 @@ def voxelize(kind, n, bounds, pos, conn, vel=None, mass=None, periodic_box=None,
         m.box[0][:] = [float(v) for v in box[0]]
         m.box[1][:] = [float(v) for v in box[1]]
         cnt = Counters()
-        rc = lib.oracle_voxels(C.byref(g), C.byref(m), float(reftol), int(maxlvl), C.byref(cnt))
+        if refine_mode:
+            lag = (C.c_double * 3)(*[float(v) for v in refine_cell])
+            rc = lib.oracle_voxels_ex(C.byref(g), C.byref(m), float(reftol), int(maxlvl), int(refine_mode), lag,
+                                      C.byref(cnt))
+        else:
+            rc = lib.oracle_voxels(C.byref(g), C.byref(m), float(reftol), int(maxlvl), C.byref(cnt))
         if rc != 0:
             raise RuntimeError("oracle_voxels failed")
         return (out, cnt.as_dict()) if counters else out

@@ -463,6 +463,8 @@ typedef struct {
     int num, cap;
     int max_lvl;
     double ptol2;
+    int mode;          /* 0: the reference's midpoint test; 1: the stretch test (not in the reference) */
+    double stretch, lag[3];
 } ov_tetbuf;
 
 static const int TET_CORNERS[6][4] = {{2, 0, 6, 18}, {8, 2, 6, 18}, {8, 20, 2, 18},
@@ -524,19 +526,57 @@ static void interp_trilinear(const double (*in)[3], double (*out)[3])
 }
 
 /* Adaptive octree refinement of a trilinear element (src/refine.c:223-289). */
+/* EXTENSION, not in the reference: refine a (sub)cube of level lvl whose edge
+ * along axis a is longer than T lag_a / 2^lvl, or whose volume (sum of the
+ * |volume| of its six tets) exceeds T lag_x lag_y lag_z / 8^lvl.  The GPU
+ * tessellation (stretch_refine) states the same test in the same order. */
+static int stretch_refine(const double (*p)[3], int lvl, double T, const double *lag)
+{
+    const double s = 1.0 / (double)(1 << lvl);
+    for (int a = 0; a < 3; ++a) {
+        const double lim = T * lag[a] * s;
+        for (int u = 0; u < 3; u += 2)
+            for (int w = 0; w < 3; w += 2) {
+                const int i0 = a == 0 ? I3(0, u, w) : a == 1 ? I3(u, 0, w) : I3(u, w, 0);
+                const int i1 = a == 0 ? I3(2, u, w) : a == 1 ? I3(u, 2, w) : I3(u, w, 2);
+                double d2 = 0.0;
+                for (int c = 0; c < 3; ++c) d2 += (p[i1][c] - p[i0][c]) * (p[i1][c] - p[i0][c]);
+                if (d2 > lim * lim) return 1;
+            }
+    }
+    double vol = 0.0;
+    for (int t = 0; t < 6; ++t) {
+        const double *q0 = p[TET_CORNERS[t][0]];
+        double e[3][3];
+        for (int v = 0; v < 3; ++v)
+            for (int c = 0; c < 3; ++c) e[v][c] = p[TET_CORNERS[t][v + 1]][c] - q0[c];
+        const double det = e[0][0] * (e[1][1] * e[2][2] - e[1][2] * e[2][1]) -
+                           e[0][1] * (e[1][0] * e[2][2] - e[1][2] * e[2][0]) +
+                           e[0][2] * (e[1][0] * e[2][1] - e[1][1] * e[2][0]);
+        vol += fabs(det);
+    }
+    return vol / 6.0 > T * lag[0] * lag[1] * lag[2] * (s * s * s);
+}
+
 static int refine_trilinear(ov_tetbuf *tb, const double (*p)[3], const double (*u)[3], double mass, int lvl)
 {
     static const int edges[7][3] = {{2, 4, 6}, {2, 10, 18}, {6, 12, 18}, {8, 13, 18},
                                     {8, 14, 20}, {8, 16, 24}, {20, 22, 24}};
     if (lvl < tb->max_lvl)
         for (int e = 0; e < 7; ++e) {
-            double err2 = 0.0;
-            for (int i = 0; i < 3; ++i) {
-                double mt = 0.5 * (p[edges[e][0]][i] + p[edges[e][2]][i]);
-                double ml = p[edges[e][1]][i];
-                err2 += (mt - ml) * (mt - ml);
+            int refine;
+            if (tb->mode == 1) {
+                refine = e == 0 && stretch_refine(p, lvl, tb->stretch, tb->lag);
+            } else {
+                double err2 = 0.0;
+                for (int i = 0; i < 3; ++i) {
+                    double mt = 0.5 * (p[edges[e][0]][i] + p[edges[e][2]][i]);
+                    double ml = p[edges[e][1]][i];
+                    err2 += (mt - ml) * (mt - ml);
+                }
+                refine = err2 > tb->ptol2;
             }
-            if (err2 > tb->ptol2) {
+            if (refine) {
                 double cp[8][3], cu[8][3], np_[27][3], nu[27][3];
                 for (int i = 0; i < 2; ++i)
                     for (int j = 0; j < 2; ++j)
@@ -630,7 +670,24 @@ static int make_images(double (*p)[3], double (*rb)[3], const og_grid *g, const 
 
 /* The density branch of psi_voxels (src/cpsi.c:41-112).  Returns 0, or -1 on
  * an unsupported element type / allocation failure. */
+static int voxels_impl(og_grid *g, const og_mesh *m, double reftol, int max_lvl, int mode, const double *lag,
+                       og_counters *cnt);
+
 int oracle_voxels(og_grid *g, const og_mesh *m, double reftol, int max_lvl, og_counters *cnt)
+{
+    return voxels_impl(g, m, reftol, max_lvl, 0, NULL, cnt);
+}
+
+/* With the refinement criterion of the GPU library's PSIB_REFINE_STRETCH
+ * (mode 1, threshold reftol, Lagrangian cell lag). */
+int oracle_voxels_ex(og_grid *g, const og_mesh *m, double reftol, int max_lvl, int mode, const double *lag,
+                     og_counters *cnt)
+{
+    return voxels_impl(g, m, reftol, max_lvl, mode, lag, cnt);
+}
+
+static int voxels_impl(og_grid *g, const og_mesh *m, double reftol, int max_lvl, int mode, const double *lag,
+                       og_counters *cnt)
 {
     og_counters dummy;
     memset(&dummy, 0, sizeof(dummy));
@@ -644,6 +701,9 @@ int oracle_voxels(og_grid *g, const og_mesh *m, double reftol, int max_lvl, og_c
     if (max_lvl > 6) max_lvl = 6; /* src/refine.c:89-92 */
     tb.max_lvl = max_lvl;
     tb.ptol2 = (reftol * dxmin) * (reftol * dxmin);
+    tb.mode = mode;
+    tb.stretch = reftol;
+    for (int i = 0; i < 3; ++i) tb.lag[i] = lag ? lag[i] : 0.0;
     ov_poly *stack = malloc(OV_STACK * sizeof(ov_poly));
     if (!stack) return -1;
     int vpe = m->elemtype;

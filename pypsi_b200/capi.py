@@ -43,7 +43,8 @@ class Stats(C.Structure):
 
 class Options(C.Structure):
     _fields_ = [("precision", C.c_int), ("deterministic", C.c_int), ("memory", C.c_int), ("device", C.c_int),
-                ("stream", C.c_void_p), ("stats", C.POINTER(Stats))]
+                ("stream", C.c_void_p), ("stats", C.POINTER(Stats)), ("refine_mode", C.c_int),
+                ("refine_cell", C.c_double * 3)]
 
 
 lib.psib_voxels.argtypes = [C.POINTER(Grid), C.POINTER(Mesh), C.c_int, C.c_double, C.c_int, C.POINTER(Options)]
@@ -87,11 +88,16 @@ def make_mesh(npart, nelem, pos_ptr, vel_ptr=None, mass_ptr=None, conn_ptr=None,
     return m
 
 
+REFINE = {"midpoint": 0, "stretch": 1}
+
+
 def voxels(grid: Grid, mesh: Mesh, precision=PSIB_FP64, deterministic=False, memory=PSIB_DEVICE, stream=None,
-           refine_tolerance=1.0, refine_max_lvl=0) -> dict:
+           refine_tolerance=1.0, refine_max_lvl=0, refine_criterion="midpoint", refine_cell=None) -> dict:
     st = Stats()
     o = Options(precision=precision, deterministic=int(bool(deterministic)), memory=memory, device=-1,
-                stream=stream, stats=C.pointer(st))
+                stream=stream, stats=C.pointer(st), refine_mode=REFINE[refine_criterion])
+    if refine_cell is not None:
+        o.refine_cell[:] = [float(v) for v in refine_cell]
     rc = lib.psib_voxels(C.byref(grid), C.byref(mesh), 0, float(refine_tolerance), int(refine_max_lvl), C.byref(o))
     if rc != 0:
         raise PsibError(rc)
@@ -100,7 +106,7 @@ def voxels(grid: Grid, mesh: Mesh, precision=PSIB_FP64, deterministic=False, mem
 
 def voxels_device(fields: dict, n, bounds, pos, vel=None, mass=None, connectivity=None, block_dims=None,
                   periodic_box=None, precision="fp64", deterministic=False, refine_tolerance=1.0, refine_max_lvl=0,
-                  stream=None) -> dict:
+                  stream=None, refine_criterion="midpoint", refine_cell=None) -> dict:
     """Deposit on device-resident torch tensors.
 
     fields: {"m": (nx,ny,nz) float64 CUDA tensor, "x": (...,3), ...}; pos/vel:
@@ -116,7 +122,7 @@ def voxels_device(fields: dict, n, bounds, pos, vel=None, mass=None, connectivit
     m = mesh_from_tensors(pos, vel, mass, connectivity, block_dims, periodic_box)
     s = stream if stream is not None else torch.cuda.current_stream()
     return voxels(g, m, PRECISIONS[precision], deterministic, PSIB_DEVICE,
-                  C.c_void_p(s.cuda_stream), refine_tolerance, refine_max_lvl)
+                  C.c_void_p(s.cuda_stream), refine_tolerance, refine_max_lvl, refine_criterion, refine_cell)
 
 
 def mesh_from_tensors(pos, vel=None, mass=None, connectivity=None, block_dims=None, periodic_box=None) -> Mesh:

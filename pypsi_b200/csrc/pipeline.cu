@@ -190,6 +190,8 @@ struct Call {
     double* F[6];
     const double *pos, *vel, *mass;
     const int* conn;
+    int refine_mode;
+    double refine_cell[3];
     // adjoint call: F[0] holds dL/dm; gradients accumulate into these
     bool adjoint;
     double *gpos, *gmass;
@@ -402,6 +404,9 @@ int run_device(Call& c)
     ta.g = gd;
     ta.max_lvl = c.maxlvl;
     ta.ptol2 = tol * tol;
+    ta.refine_mode = c.refine_mode;
+    ta.stretch = c.reftol;
+    for (int i = 0; i < 3; ++i) ta.lag[i] = c.refine_cell[i];
     ta.status = (unsigned*)&sm[S_STATUS];
     ta.counters = &sm[S_TESS];
     std::vector<long long> offs_host;
@@ -794,6 +799,8 @@ int validate(const psib_grid* g, const psib_mesh* m, int mode, const psib_option
         }
         if (np != m->npart || nel != m->nelem) return fail(PSIB_ERR_ARG, "block_dims disagree with npart/nelem");
     }
+    if (o && o->refine_mode != PSIB_REFINE_MIDPOINT && o->refine_mode != PSIB_REFINE_STRETCH)
+        return fail(PSIB_ERR_ARG, "invalid refine_mode %d", o->refine_mode);
     if (o && o->precision != PSIB_FP64 && o->precision != PSIB_MIXED && o->precision != PSIB_FP64_CENTRAL)
         return fail(PSIB_ERR_ARG, "invalid precision %d", o->precision);
     return PSIB_OK;
@@ -875,6 +882,17 @@ int psib_voxels(const psib_grid* grid, const psib_mesh* mesh, int mode, double r
     c.maxlvl = refine_max_lvl > 6 ? 6 : (refine_max_lvl < 0 ? 0 : refine_max_lvl);
     c.precision = o.precision;
     c.deterministic = o.deterministic;
+    c.refine_mode = o.refine_mode;
+    if (o.refine_mode == PSIB_REFINE_STRETCH) {
+        const bool given = o.refine_cell[0] > 0.0 && o.refine_cell[1] > 0.0 && o.refine_cell[2] > 0.0;
+        for (int i = 0; i < 3; ++i) {
+            if (given) c.refine_cell[i] = o.refine_cell[i];
+            else if (mesh->periodic && mesh->block_dims[i] > 0)
+                c.refine_cell[i] = (mesh->box[1][i] - mesh->box[0][i]) / mesh->block_dims[i];
+            else return fail(PSIB_ERR_ARG, "the stretch criterion needs refine_cell or a periodic block mesh");
+        }
+        if (!(refine_tolerance > 0.0)) return fail(PSIB_ERR_ARG, "the stretch threshold must be positive");
+    }
     c.C = C;
     c.stats = o.stats;
     if (o.stats) *o.stats = psib_stats{};

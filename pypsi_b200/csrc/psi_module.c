@@ -546,14 +546,21 @@ static PyObject *PSI_voxels(PyObject *self, PyObject *args, PyObject *kwds)
     (void)self;
     Grid *grid;
     Mesh *mesh;
-    char *modestr = "density", *precstr = "fp64";
+    char *modestr = "density", *precstr = "fp64", *critstr = "midpoint";
     double reftol = 1.0;
     int maxlvl = 0, det = 0;
     static char *kwlist[] = {"grid", "mesh", "mode", "refine_tolerance", "refine_max_lvl", "precision",
-                             "deterministic", NULL};
-    if (!PyArg_ParseTupleAndKeywords(args, kwds, "O!O!|sdisp", kwlist, &GridType, &grid, &MeshType, &mesh, &modestr,
-                                     &reftol, &maxlvl, &precstr, &det))
+                             "deterministic", "refine_criterion", NULL};
+    if (!PyArg_ParseTupleAndKeywords(args, kwds, "O!O!|sdispz", kwlist, &GridType, &grid, &MeshType, &mesh, &modestr,
+                                     &reftol, &maxlvl, &precstr, &det, &critstr))
         return NULL;
+    int crit;
+    if (!critstr || strcmp(critstr, "midpoint") == 0) crit = PSIB_REFINE_MIDPOINT;
+    else if (strcmp(critstr, "stretch") == 0) crit = PSIB_REFINE_STRETCH;
+    else {
+        PyErr_Format(PyExc_ValueError, "Invalid refine_criterion for PSI.voxels(): %s", critstr);
+        return NULL;
+    }
     if (grid->ctype != GRID_CART) {
         PyErr_SetString(PyExc_ValueError, "Only cartesian grids are supported by PSI.voxels()");
         return NULL;
@@ -624,6 +631,7 @@ static PyObject *PSI_voxels(PyObject *self, PyObject *args, PyObject *kwds)
     psib_options o;
     memset(&o, 0, sizeof(o));
     o.precision = prec;
+    o.refine_mode = crit;
     o.deterministic = det;
     o.memory = PSIB_HOST;
     o.device = -1;

@@ -77,6 +77,8 @@ struct TessArgs {
     long long e0, e1;          // element range
     int max_lvl;
     double ptol2;
+    int refine_mode;           // 0: the reference's midpoint test (ptol2); 1: stretch beyond `stretch` x lag
+    double stretch, lag[3];
     const long long *offset;   // per element, exclusive (emit)
     long long offset_base;
     int *count;                // per element (count)

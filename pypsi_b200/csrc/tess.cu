@@ -210,10 +210,43 @@ struct RefNode {
     int child;
 };
 
+// The stretch criterion (PSIB_REFINE_STRETCH; the reference has only the
+// midpoint test): refine a (sub)cube of level lvl whose edge along axis a is
+// longer than T lag_a / 2^lvl, or whose volume (the sum of |volume| of its six
+// tets) exceeds T lag_x lag_y lag_z / 8^lvl, lag being the Lagrangian cell.
+// The oracle states the same test in the same operation order.
+__device__ bool stretch_refine(const double (*p)[3], int lvl, double T, const double* lag)
+{
+    const double s = 1.0 / (double)(1 << lvl);
+    for (int a = 0; a < 3; ++a) {
+        const double lim = T * lag[a] * s;
+        for (int u = 0; u < 3; u += 2)
+            for (int w = 0; w < 3; w += 2) {
+                const int i0 = a == 0 ? I3(0, u, w) : a == 1 ? I3(u, 0, w) : I3(u, w, 0);
+                const int i1 = a == 0 ? I3(2, u, w) : a == 1 ? I3(u, 2, w) : I3(u, w, 2);
+                double d2 = 0.0;
+                for (int c = 0; c < 3; ++c) d2 += (p[i1][c] - p[i0][c]) * (p[i1][c] - p[i0][c]);
+                if (d2 > lim * lim) return true;
+            }
+    }
+    double vol = 0.0;
+    for (int t = 0; t < 6; ++t) {
+        const double* q0 = p[c_tet_nodes[t][0]];
+        double e[3][3];
+        for (int v = 0; v < 3; ++v)
+            for (int c = 0; c < 3; ++c) e[v][c] = p[c_tet_nodes[t][v + 1]][c] - q0[c];
+        const double det = e[0][0] * (e[1][1] * e[2][2] - e[1][2] * e[2][1]) -
+                           e[0][1] * (e[1][0] * e[2][2] - e[1][2] * e[2][0]) +
+                           e[0][2] * (e[1][0] * e[2][1] - e[1][1] * e[2][0]);
+        vol += fabs(det);
+    }
+    return vol / 6.0 > T * lag[0] * lag[1] * lag[2] * (s * s * s);
+}
+
 // Adaptive refinement of a trilinear element, depth first in the reference's
 // child order (src/refine.c:223-289).
 __device__ void refine_element(Emitter& em, const double (*cp)[3], const double (*cu)[3], double mass, long long e,
-                               int max_lvl, double ptol2, RefNode* L)
+                               int max_lvl, double ptol2, int mode, double T, const double* lag, RefNode* L)
 {
     interp_trilinear(cp, L[0].p);
     interp_trilinear(cu, L[0].u);
@@ -224,7 +257,8 @@ __device__ void refine_element(Emitter& em, const double (*cp)[3], const double 
         RefNode& N = L[d];
         if (N.child < 0) {
             bool refine = false;
-            if (d < max_lvl)
+            if (d < max_lvl && mode == 1) refine = stretch_refine(N.p, d, T, lag);
+            else if (d < max_lvl)
                 for (int k = 0; k < 7 && !refine; ++k) {
                     double err2 = 0.0;
                     for (int i = 0; i < 3; ++i) {
@@ -302,7 +336,8 @@ __device__ int element_items(const TessArgs& a, bool write, long long e, long lo
             em.tet(tp, tu, me * (1.0 / 6), e, pid);
         }
     } else {
-        if constexpr (REFINE) refine_element(em, p, u, me, e, a.max_lvl, a.ptol2, L);
+        if constexpr (REFINE)
+            refine_element(em, p, u, me, e, a.max_lvl, a.ptol2, a.refine_mode, a.stretch, a.lag, L);
     }
     tets += em.tets;
     return em.n;

@@ -62,6 +62,11 @@ def make(name: str) -> dict:
         return dict(kind="array", pos=pos, vel=rng.normal(size=(4, 3)), mass=None,
                     conn=np.arange(4, dtype=np.int32).reshape(1, 4), periodic_box=None, n=(64, 64, 64),
                     bounds=((0.0, 0.0, 0.0), (1.0, 1.0, 1.0)), fields=["x", "v"], reftol=1.0, maxlvl=0)
+    if name == "stretch":  # the stretch refinement criterion (not in the reference), 2 levels, threshold 2
+        pos, vel = zeldovich(12, 3.0, 110)
+        c = _block(pos, vel, 24, ["v"], reftol=2.0, maxlvl=2)
+        c.update(refine_mode=1, refine_cell=(100.0 / 12,) * 3)
+        return c
     raise KeyError(name)
 
 
@@ -81,7 +86,8 @@ def run_oracle(O, c, kind="restatement", counters=False):
     mass = None if c["mass"] is None else np.asarray(c["mass"]).reshape(-1)
     return O.voxelize(kind, n=c["n"], bounds=c["bounds"], pos=c["pos"].reshape(-1, 3), vel=c["vel"].reshape(-1, 3),
                       conn=conn_of(c), mass=mass, periodic_box=c["periodic_box"], fields=c["fields"],
-                      reftol=c["reftol"], maxlvl=c["maxlvl"], counters=counters)
+                      reftol=c["reftol"], maxlvl=c["maxlvl"], counters=counters,
+                      refine_mode=c.get("refine_mode", 0), refine_cell=c.get("refine_cell"))
 
 
 def run_psi(PSI, c, grid=None, **kw):
@@ -96,6 +102,8 @@ def run_psi(PSI, c, grid=None, **kw):
     if c["periodic_box"] is not None:
         mk["periodic_box"] = c["periodic_box"]
     mesh = PSI.Mesh(**mk)
+    if c.get("refine_mode"):
+        kw.setdefault("refine_criterion", "stretch")
     PSI.voxels(grid=grid, mesh=mesh, refine_tolerance=c["reftol"], refine_max_lvl=c["maxlvl"], **kw)
     return {k: np.array(v) for k, v in grid.fields.items()}, grid, mesh
 

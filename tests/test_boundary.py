@@ -31,7 +31,7 @@ def test_abi_version_and_no_device_error(psi):
     import pypsi_b200
 
     lib = pypsi_b200.lib
-    assert lib.psib_abi_version() == 1
+    assert lib.psib_abi_version() == 2
     lib.psib_voxels.restype = ctypes.c_int
     # argument validation runs before any device work
     assert lib.psib_voxels(None, None, 0, ctypes.c_double(1.0), 0, None) == 1  # PSIB_ERR_ARG

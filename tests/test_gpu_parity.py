@@ -154,6 +154,22 @@ def test_accumulates_into_existing_grid(gpu, oracle, det):
         check(field_errors(out, ref), FP64_TOL, "accumulate")
 
 
+def test_stretch_refinement_fp64_bitwise_and_mixed(gpu, oracle):
+    """The stretch refinement criterion: the same tets as the oracle's
+    statement of it, FP64 fields bit for bit, mixed within 1e-5 of exact."""
+    c = make("stretch")
+    ref, cnt = run_oracle(oracle, c, counters=True)
+    assert cnt["tets"] > 6 * 12 ** 3  # the criterion refined something
+    out, _, _ = run_psi(gpu, c, precision="fp64")
+    assert gpu.last_stats()["tets"] == cnt["tets"]
+    for f in ref:
+        assert np.array_equal(out[f], ref[f]), f
+    out, _, _ = run_psi(gpu, c, precision="mixed")
+    ex = run_oracle(oracle, c, kind="exact")
+    check_vs_exact_and_reference(out, ref, ex, MIXED_TOL, "stretch")
+    assert mass_error(out["m"], total_mass(c)) <= MASS_TOL
+
+
 def test_mixed_accumulates_into_existing_grid(gpu, oracle):
     """The mixed path merges each voxel's new fragments into the fields already
     on the grid in one step; the result is the reference's sequential update

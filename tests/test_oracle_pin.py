@@ -102,3 +102,19 @@ def test_exact_oracle_agrees_where_the_reference_is_well_conditioned(oracle):
     assert errs["m"]["rel"] <= 1e-9, errs["m"]
     assert errs["xx"]["norm"] > 1e-6, errs["xx"]  # the reference's own error in sliver voxels
     assert abs(e["m"].sum() - c["mass"].sum()) <= 1e-12 * c["mass"].sum()
+
+
+def test_stretch_criterion_limits_in_the_oracle(oracle):
+    """The stretch refinement criterion (an extension the GPU library shares):
+    a huge threshold refines nothing, a tiny one refines every element to the
+    maximum level, and mass is conserved either way."""
+    c = make("stretch")
+    n = c["pos"].shape[0]
+    for T, want in [(1.0e9, 6 * n ** 3), (1.0e-9, 6 * n ** 3 * 64)]:
+        c["reftol"] = T
+        out, cnt = run_oracle(oracle, c, counters=True)
+        assert cnt["tets"] == want, (T, cnt["tets"])
+        assert abs(out["m"].sum() / n ** 3 - 1.0) < 1e-13
+    c["reftol"] = 2.0
+    _, cnt = run_oracle(oracle, c, counters=True)
+    assert 6 * n ** 3 < cnt["tets"] < 6 * n ** 3 * 64, cnt["tets"]
