@@ -54,8 +54,9 @@ def parse():
     ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c5"],
-                    help="c2: the headline (128^3 -> 256^3, order 2); c5: 256^3 -> 512^3 with stretch refinement")
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c5"],
+                    help="c2: the headline (128^3 -> 256^3, order 2); c3: 512 uneven cutouts in one batch; "
+                         "c5: 256^3 -> 512^3 with stretch refinement")
     args = ap.parse_args()
     if (args.n_part, args.n_grid) != (N_PART, N_GRID) or args.precision != "both":
         args.no_cpu_baseline = True
@@ -262,6 +263,68 @@ def time_fwd_bwd(x0, n_part, n_grid, steps, warmup, barrier):
     out["ratio"] = out["fwd_bwd_ms"] / out["fwd_ms"]
     out["tets_per_s_fwd_bwd"] = 6 * n_part ** 3 / (out["fwd_bwd_ms"] * 1e-3)
     return out
+
+
+def run_c3(args):
+    """512 independent cutouts, edge n log-uniform in [8, 64], Zel'dovich rms 1.5
+    cells in their own periodic box of side 100, density on their own (2n)^3 grid:
+    one psib_voxels_batch call against 512 separate psib_voxels calls."""
+    import math
+
+    import numpy as np
+    import torch
+
+    from pypsi_b200 import capi
+    from pypsi_b200.synth import zeldovich
+
+    rank, world, local = env_rank()
+    torch.cuda.set_device(local)
+    rng = np.random.default_rng(333 + rank)
+    ns = [int(round(math.exp(rng.uniform(math.log(8), math.log(64))))) for _ in range(512)]
+    cut = []
+    for b, n in enumerate(ns):
+        pos, _ = zeldovich(n, 1.5, 10000 + 512 * rank + b)
+        cut.append(dict(n=(2 * n,) * 3, bounds=BOX, pos=torch.from_numpy(pos.reshape(-1, 3)).cuda(),
+                        block_dims=(n,) * 3, periodic_box=BOX,
+                        fields={"m": torch.zeros((2 * n,) * 3, dtype=torch.float64, device="cuda")}))
+    tets = sum(6 * n ** 3 for n in ns)
+    stream = torch.cuda.current_stream()
+
+    def batch():
+        return capi.voxels_batch_device(cut, precision="mixed", stream=stream)
+
+    def separate():
+        return [capi.voxels_device(c["fields"], c["n"], c["bounds"], c["pos"], block_dims=c["block_dims"],
+                                   periodic_box=c["periodic_box"], precision="mixed", stream=stream) for c in cut]
+
+    def timed(fn, steps):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = [fn() for _ in range(steps)]
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps, out
+
+    ck = Clocks(local)
+    ck.__enter__()
+    ms_b, st_b = timed(batch, args.steps)
+    ck.__exit__()
+    ms_s, _ = timed(separate, max(1, args.steps // 2))
+    line = {"metric": "tets/s, 512 uneven cutouts (n in [8,64], (2n)^3 grids, density), one batch call", "value":
+            tets / (ms_b * 1e-3), "unit": "tets/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_b, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+            "data": "synthetic: 512 seeded Zel'dovich lattices, rms 1.5 cells, element mass 1",
+            "config": {"workload": "512 cutouts, edge log-uniform in [8,64], own box of side 100, (2n)^3 grids, m only",
+                       "precision": "mixed"},
+            "separate_calls": {"value": tets / (ms_s * 1e-3), "ms_per_step": ms_s, "calls": 512},
+            "batch_over_separate": ms_s / ms_b, "work": {"tets": tets, "cutouts": 512, "edge_min": min(ns),
+                                                         "edge_max": max(ns)},
+            "gpu_launches": int(st_b[-1]["kernel_launches"]), "clocks": ck.summary()}
+    capi.lib.psib_release_device_memory()
+    print(json.dumps(line), flush=True)
 
 
 def run_c5(args):
@@ -529,6 +592,8 @@ def main():
         run_reference(args)
     elif args.workload == "c5":
         run_c5(args)
+    elif args.workload == "c3":
+        run_c3(args)
     else:
         run_ours(args)
 

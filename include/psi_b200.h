@@ -132,6 +132,20 @@ typedef struct {
 int psib_voxels(const psib_grid *grid, const psib_mesh *mesh, int mode, double refine_tolerance,
                 int refine_max_lvl, const psib_options *opt);
 
+/* A batch of independent deposits -- many cutouts of uneven size, each a
+ * psib_voxels call of its own (grids[b], meshes[b]) -- run as one pass: every
+ * stage (tessellation, ordering by footprint, the clip walk, the record sort,
+ * the field update) is one set of launches over the tets of all cutouts, whose
+ * work queues mix them.  Each cutout's fields equal those of its own
+ * psib_voxels call (FP64: bit for bit).  The reference has no batch call; it
+ * replaces a loop of psi_voxels calls (src/cpsi.c:41).
+ * All pointers are device memory (options->memory must be PSIB_DEVICE), every
+ * grid has the same set of fields, 1 <= nbatch <= 65535, fewer than 2^32
+ * voxels and 2^31 elements in all.  The refinement arguments apply to every
+ * cutout. */
+int psib_voxels_batch(const psib_grid *grids, const psib_mesh *meshes, int nbatch, int mode,
+                      double refine_tolerance, int refine_max_lvl, const psib_options *opt);
+
 /* Adjoint of the density deposit.  The reference has no adjoint; this is
  * the backward pass of psib_voxels's m field for differentiable use.
  *

@@ -52,6 +52,9 @@ lib.psib_voxels.restype = C.c_int
 lib.psib_voxels_adjoint.argtypes = [C.POINTER(Grid), C.POINTER(Mesh), C.c_double, C.c_int, C.c_void_p, C.c_void_p,
                                     C.c_void_p, C.POINTER(Options)]
 lib.psib_voxels_adjoint.restype = C.c_int
+lib.psib_voxels_batch.argtypes = [C.POINTER(Grid), C.POINTER(Mesh), C.c_int, C.c_int, C.c_double, C.c_int,
+                                  C.POINTER(Options)]
+lib.psib_voxels_batch.restype = C.c_int
 lib.psib_last_error.restype = C.c_char_p
 lib.psib_release_device_memory.restype = C.c_int
 
@@ -158,6 +161,36 @@ def adjoint_device(grad_m, n, bounds, pos, grad_pos, mass=None, connectivity=Non
                 stream=C.c_void_p(s.cuda_stream), stats=C.pointer(st))
     rc = lib.psib_voxels_adjoint(C.byref(g), C.byref(m), 1.0, 0, grad_pos.data_ptr(), None,
                                  grad_mass.data_ptr() if grad_mass is not None else None, C.byref(o))
+    if rc != 0:
+        raise PsibError(rc)
+    return st.as_dict()
+
+
+def voxels_batch_device(cutouts: list, precision="fp64", refine_tolerance=1.0, refine_max_lvl=0,
+                        refine_criterion="midpoint", refine_cell=None, stream=None) -> dict:
+    """Many independent deposits in one pass (psib_voxels_batch).
+
+    cutouts: dicts with the arguments of voxels_device -- fields, n, bounds,
+    pos and optionally vel, mass, connectivity, block_dims, periodic_box --
+    all on the GPU; every cutout must ask for the same fields."""
+    import torch
+
+    nb = len(cutouts)
+    grids = (Grid * nb)()
+    meshes = (Mesh * nb)()
+    for b, c in enumerate(cutouts):
+        for f, t in c["fields"].items():
+            assert t.is_cuda and t.dtype == torch.float64 and t.is_contiguous(), f
+        grids[b] = make_grid(c["n"], c["bounds"], {f: t.data_ptr() for f, t in c["fields"].items()})
+        meshes[b] = mesh_from_tensors(c["pos"], c.get("vel"), c.get("mass"), c.get("connectivity"),
+                                      c.get("block_dims"), c.get("periodic_box"))
+    s = stream if stream is not None else torch.cuda.current_stream()
+    st = Stats()
+    o = Options(precision=PRECISIONS[precision], deterministic=0, memory=PSIB_DEVICE, device=-1,
+                stream=C.c_void_p(s.cuda_stream), stats=C.pointer(st), refine_mode=REFINE[refine_criterion])
+    if refine_cell is not None:
+        o.refine_cell[:] = [float(v) for v in refine_cell]
+    rc = lib.psib_voxels_batch(grids, meshes, nb, 0, float(refine_tolerance), int(refine_max_lvl), C.byref(o))
     if rc != 0:
         raise PsibError(rc)
     return st.as_dict()

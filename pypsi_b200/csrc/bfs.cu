@@ -88,6 +88,12 @@ __device__ __forceinline__ bool one_voxel(const int* lo, const int* hi)
     return hi[0] - lo[0] <= 1 && hi[1] - lo[1] <= 1 && hi[2] - lo[2] <= 1;
 }
 
+// The grid of image t: its cutout's in a batch.
+__device__ __forceinline__ const GridDev& grid_of(const ClipArgs& c, long long t)
+{
+    return c.grids ? c.grids[c.it.grid[t]] : c.g;
+}
+
 // ---- init: tet images -> first polyhedra ----
 
 // q-volume (fraction of the tet) inside the window planes of wmask, clipped in
@@ -134,9 +140,11 @@ __global__ void __launch_bounds__(BB) k_bfs_init(BfsArgs a)
         double p[4][3];
         int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
         bool window = false;
+        const GridDev* gp = &a.c.g;
         uint32_t wmask = 0; // window planes: bit 2a keeps x_a >= w0_a, bit 2a+1 keeps x_a <= w1_a
         if (act) {
             t = a.c.order[i];
+            gp = &grid_of(a.c, t);
             const double* fr = a.c.it.frame + (size_t)t * FRAME;
             for (int v = 0; v < 4; ++v)
                 for (int c = 0; c < 3; ++c) p[v][c] = fr[3 * v + c];
@@ -147,22 +155,22 @@ __global__ void __launch_bounds__(BB) k_bfs_init(BfsArgs a)
                     if (p[v][c] < cmin) cmin = p[v][c];
                     if (p[v][c] > cmax) cmax = p[v][c];
                 }
-                const bool clo = a.c.g.w0[c] > cmin, chi = a.c.g.w1[c] < cmax;
+                const bool clo = gp->w0[c] > cmin, chi = gp->w1[c] < cmax;
                 window = window || clo || chi;
                 wmask |= (clo ? 1u : 0u) << (2 * c) | (chi ? 1u : 0u) << (2 * c + 1);
-                if (clo) cmin = a.c.g.w0[c];
-                if (chi) cmax = a.c.g.w1[c];
-                lo[c] = (int)floor((cmin - a.c.g.w0[c]) / a.c.g.d[c]);
-                hi[c] = (int)ceil((cmax - a.c.g.w0[c]) / a.c.g.d[c]);
+                if (clo) cmin = gp->w0[c];
+                if (chi) cmax = gp->w1[c];
+                lo[c] = (int)floor((cmin - gp->w0[c]) / gp->d[c]);
+                hi[c] = (int)ceil((cmax - gp->w0[c]) / gp->d[c]);
                 if (lo[c] < 0) lo[c] = 0;
-                if (hi[c] > a.c.g.n[c]) hi[c] = a.c.g.n[c];
+                if (hi[c] > gp->n[c]) hi[c] = gp->n[c];
                 if (hi[c] < lo[c]) hi[c] = lo[c];
             }
         }
         // the exact FP64 q-volume of a window-clipped image: its mass correction target
         double target = 1.0;
         const bool wbfs = act && window && a.window_bfs;
-        if (wbfs) target = window_volume(p, wmask, a.c.g);
+        if (wbfs) target = window_volume(p, wmask, *gp);
         const bool to_dfs = act && window && !a.window_bfs;
         const bool use = act && (!window || (wbfs && target > 0.0));
         const bool leaf = use && !wbfs && one_voxel(lo, hi);
@@ -327,6 +335,7 @@ __global__ void __launch_bounds__(BB) k_bfs_level(BfsArgs a)
         if (act) {
             get_box(a.in, e, lo, hi);
             t = a.in.item[e];
+            const GridDev& g = grid_of(a.c, t);
             const double* fr = a.c.it.frame + (size_t)t * FRAME; // vertex 0: the origin of the FP32 positions
             for (int v = 0; v < nv; ++v) {
                 AT(nbI, v) = a.in.nb[qn(e, v)];
@@ -341,7 +350,7 @@ __global__ void __launch_bounds__(BB) k_bfs_level(BfsArgs a)
                     win &= ~(1u << pl);
                     ax = pl >> 1;
                     const bool lo_side = !(pl & 1);
-                    cr = (float)((lo_side ? a.c.g.w0[ax] : a.c.g.w1[ax]) - fr[ax]);
+                    cr = (float)((lo_side ? g.w0[ax] : g.w1[ax]) - fr[ax]);
                     sg = lo_side ? -1.0f : 1.0f;
                     um = 0;
                     for (int v = 0; v < nv; ++v)
@@ -361,7 +370,7 @@ __global__ void __launch_bounds__(BB) k_bfs_level(BfsArgs a)
                 if (dmax <= 1) { toleaf = true; break; }
                 ++splits;
                 // the middle grid plane of the longest axis (src/geometry.c:886-893)
-                const double coord = a.c.g.d[ax] * (lo[ax] + dmax / 2) + a.c.g.w0[ax];
+                const double coord = g.d[ax] * (lo[ax] + dmax / 2) + g.w0[ax];
                 cr = (float)(coord - fr[ax]);
                 um = 0;
                 for (int v = 0; v < nv; ++v)
@@ -533,15 +542,17 @@ __global__ void __launch_bounds__(BB) k_bfs_leaf(BfsArgs a)
                 int lo[3], hi[3];
                 get_box(a.leaf, e, lo, hi);
                 const uint32_t t = a.leaf.item[e];
+                const GridDev& g = grid_of(c, t);
+                const unsigned long long vbase = c.voff ? c.voff[c.it.grid[t]] : 0ull;
                 const double* fr = c.it.frame + (size_t)t * FRAME;
                 double p0[3], DX[3][3], plo[3], phi[3], tol[3];
                 for (int i = 0; i < 3; ++i) p0[i] = fr[i];
                 for (int i = 0; i < 3; ++i)
                     for (int j = 0; j < 3; ++j) DX[i][j] = fr[3 * (j + 1) + i] - p0[i];
                 for (int i = 0; i < 3; ++i) {
-                    plo[i] = c.g.d[i] * lo[i] + c.g.w0[i];
-                    phi[i] = c.g.d[i] * (lo[i] + 1) + c.g.w0[i];
-                    tol[i] = 1.0e-3 * c.g.d[i];
+                    plo[i] = g.d[i] * lo[i] + g.w0[i];
+                    phi[i] = g.d[i] * (lo[i] + 1) + g.w0[i];
+                    tol[i] = 1.0e-3 * g.d[i];
                 }
                 for (int v = 0; v < nv; ++v) {
                     const uint32_t w = a.leaf.nb[qn(e, v)];
@@ -556,10 +567,11 @@ __global__ void __launch_bounds__(BB) k_bfs_leaf(BfsArgs a)
                 if (e2) {
                     st |= e2;
                 } else if (mom[0] > 0.0) {
-                    if (lo[0] >= c.g.n[0] || lo[1] >= c.g.n[1] || lo[2] >= c.g.n[2]) {
+                    if (lo[0] >= g.n[0] || lo[1] >= g.n[1] || lo[2] >= g.n[2]) {
                         st |= ST_INDEX;
                     } else {
-                        const long long gi = ((long long)c.g.n[1] * lo[0] + lo[1]) * c.g.n[2] + lo[2];
+                        const long long gi =
+                            (long long)vbase + ((long long)g.n[1] * lo[0] + lo[1]) * g.n[2] + lo[2];
                         key = ((unsigned long long)gi << c.rec_ibits) | (unsigned long long)(t - c.rec_item_base);
                         const double m0 = mom[0];
                         double u[3];

@@ -99,6 +99,7 @@ struct Ctx {
     DevBuf rkey, rmom, rkey_sorted, rperm_in, rperm, rvox, ritem, rmom_sorted, run_vox, run_cnt, run_off;
     // breadth-first clip: three polyhedron queues, the volume histogram, per-level counters, window list
     DevBuf qx[3], qnb[3], qnv[3], qwin[3], qbox[3], qitem[3], hist, bfs_cnt, dfs_list, vsum;
+    DevBuf btab, igrid; // batch tables, image -> cutout
     std::vector<DevBuf*> all()
     {
         return {&hpos, &hgpos, &hgmass, &hvel, &hmass, &hconn, &hfield[0], &hfield[1], &hfield[2], &hfield[3], &hfield[4],
@@ -107,7 +108,7 @@ struct Ctx {
                 &rkey_sorted, &rperm_in, &rperm, &rvox, &ritem, &rmom_sorted, &run_vox, &run_cnt, &run_off,
                 &qx[0], &qx[1], &qx[2], &qnb[0], &qnb[1], &qnb[2], &qnv[0], &qnv[1], &qnv[2], &qbox[0], &qbox[1],
                 &qbox[2], &qitem[0], &qitem[1], &qitem[2], &hist, &bfs_cnt, &dfs_list, &vsum, &qwin[0], &qwin[1],
-                &qwin[2]};
+                &qwin[2], &btab, &igrid};
     }
 };
 
@@ -169,6 +170,8 @@ __global__ void k_iota_u(unsigned* o, long long n)
         o[i] = (unsigned)i;
 }
 
+size_t round_up(size_t b) { return (b + 15) & ~(size_t)15; }
+
 long long env_ll(const char* name, long long dflt)
 {
     const char* s = getenv(name);
@@ -192,6 +195,11 @@ struct Call {
     const int* conn;
     int refine_mode;
     double refine_cell[3];
+    // a batch of cutouts (nbatch > 0): host arrays of grids and meshes (device pointers)
+    int nbatch;
+    const psib_grid* grids;
+    const psib_mesh* meshes;
+    const double* refine_cell_given;
     // adjoint call: F[0] holds dL/dm; gradients accumulate into these
     bool adjoint;
     double *gpos, *gmass;
@@ -337,13 +345,80 @@ int bfs_clip(Ctx& C, ClipArgs& ca, long long nmain, long long nitems, unsigned l
     return PSIB_OK;
 }
 
+GridDev grid_dev(const psib_grid& g)
+{
+    GridDev gd;
+    for (int i = 0; i < 3; ++i) {
+        gd.n[i] = g.n[i];
+        gd.w0[i] = g.window[0][i];
+        gd.w1[i] = g.window[1][i];
+        gd.d[i] = g.d[i];
+    }
+    return gd;
+}
+
+// The device view of a mesh on a grid: arrays, lattice, box, and the
+// refinement parameters that depend on the grid (midpoint tolerance) or the
+// mesh (Lagrangian cell of the stretch criterion).
+MeshDev mesh_dev(const psib_mesh& m, const psib_grid& g, const double* pos, const double* vel, const double* mass,
+                 const int* conn, double reftol, const double* lag)
+{
+    MeshDev md;
+    md.elemtype = m.elemtype;
+    md.npart = m.npart;
+    md.nelem = m.nelem;
+    md.pos = pos;
+    md.vel = vel;
+    md.mass = mass;
+    md.conn = conn;
+    md.periodic = m.periodic ? 1 : 0;
+    for (int i = 0; i < 3; ++i) {
+        md.bdim[i] = m.block_dims[i];
+        md.edim[i] = m.periodic ? m.block_dims[i] : m.block_dims[i] - 1;
+        md.box0[i] = m.box[0][i];
+        md.box1[i] = m.box[1][i];
+        md.lag[i] = lag ? lag[i] : 0.0;
+    }
+    double dxmin = 1.0e30;
+    for (int i = 0; i < 3; ++i)
+        if (g.d[i] < dxmin) dxmin = g.d[i];
+    const double tol = reftol * dxmin;
+    md.ptol2 = tol * tol;
+    return md;
+}
+
+// the Lagrangian cell of the stretch criterion: given, or box / block_dims of a periodic block mesh
+int stretch_cell(const psib_mesh& m, const double* given, double* lag)
+{
+    const bool ok = given && given[0] > 0.0 && given[1] > 0.0 && given[2] > 0.0;
+    for (int i = 0; i < 3; ++i) {
+        if (ok) lag[i] = given[i];
+        else if (m.periodic && m.block_dims[i] > 0) lag[i] = (m.box[1][i] - m.box[0][i]) / m.block_dims[i];
+        else return fail(PSIB_ERR_ARG, "the stretch criterion needs refine_cell or a periodic block mesh");
+    }
+    return PSIB_OK;
+}
+
 int run_device(Call& c)
 {
     Ctx& C = *c.C;
     const psib_grid& g = *c.grid;
     const psib_mesh& m = *c.mesh;
     cudaStream_t st = c.st;
-    const long long nvox = (long long)g.n[0] * g.n[1] * g.n[2];
+    const bool batch = c.nbatch > 0;
+    long long nvox = (long long)g.n[0] * g.n[1] * g.n[2];
+    long long ne = m.nelem;
+    std::vector<long long> eoff{0};
+    std::vector<unsigned long long> voff{0};
+    if (batch) {
+        for (int b = 0; b < c.nbatch; ++b) {
+            const psib_grid& gb = c.grids[b];
+            eoff.push_back(eoff.back() + c.meshes[b].nelem);
+            voff.push_back(voff.back() + (unsigned long long)gb.n[0] * gb.n[1] * gb.n[2]);
+        }
+        nvox = (long long)voff.back();
+        ne = eoff.back();
+    }
 
     unsigned flags = 0;
     if (c.F[1]) flags |= F_X;
@@ -357,38 +432,46 @@ int run_device(Call& c)
     const bool central = (mixed || c.precision == PSIB_FP64_CENTRAL) && !c.adjoint;
     // the mixed kernel walks the main images breadth first (PSIB_BFS=0: depth first)
     bool use_bfs = mixed && env_ll("PSIB_BFS", 1) != 0;
-    for (int i = 0; i < 3; ++i)
-        if (g.n[i] >= 0xFFFF) use_bfs = false; // box bounds are packed in 16 bits
+    for (int b = 0; b < (batch ? c.nbatch : 1); ++b)
+        for (int i = 0; i < 3; ++i)
+            if ((batch ? c.grids[b] : g).n[i] >= 0xFFFF) use_bfs = false; // box bounds are packed in 16 bits
     // 1, 4 or 10 moments per record (FP32 kernel: m0, q-centroid, central second moment)
     const int nmom = order == 2 ? 10 : order == 1 ? 4 : 1;
 
-    GridDev gd;
-    for (int i = 0; i < 3; ++i) {
-        gd.n[i] = g.n[i];
-        gd.w0[i] = g.window[0][i];
-        gd.w1[i] = g.window[1][i];
-        gd.d[i] = g.d[i];
+    const GridDev gd = grid_dev(g);
+    const MeshDev md = mesh_dev(m, g, c.pos, c.vel, c.mass, c.conn, c.reftol, c.refine_cell);
+    // a batch: per-cutout meshes and grids, element and voxel offsets, field pointers
+    const MeshDev* d_meshes = nullptr;
+    const GridDev* d_grids = nullptr;
+    const long long* d_eoff = nullptr;
+    const unsigned long long* d_voff = nullptr;
+    double* const* d_fptr = nullptr;
+    if (batch) {
+        const int nb = c.nbatch;
+        const size_t o_mesh = 0, o_grid = round_up(o_mesh + nb * sizeof(MeshDev)),
+                     o_eoff = round_up(o_grid + nb * sizeof(GridDev)), o_voff = round_up(o_eoff + (nb + 1) * 8),
+                     o_fptr = round_up(o_voff + (nb + 1) * 8), total = round_up(o_fptr + 6 * nb * sizeof(double*));
+        std::vector<char> h(total, 0);
+        for (int b = 0; b < nb; ++b) {
+            const psib_mesh& mb = c.meshes[b];
+            double lag[3] = {0.0, 0.0, 0.0};
+            if (c.refine_mode == PSIB_REFINE_STRETCH) RET(stretch_cell(mb, c.refine_cell_given, lag));
+            ((MeshDev*)(h.data() + o_mesh))[b] =
+                mesh_dev(mb, c.grids[b], mb.pos, mb.vel, mb.mass, mb.connectivity, c.reftol, lag);
+            ((GridDev*)(h.data() + o_grid))[b] = grid_dev(c.grids[b]);
+            for (int f = 0; f < 6; ++f) ((double**)(h.data() + o_fptr))[6 * b + f] = c.grids[b].fields[f];
+        }
+        memcpy(h.data() + o_eoff, eoff.data(), (nb + 1) * 8);
+        memcpy(h.data() + o_voff, voff.data(), (nb + 1) * 8);
+        RET(ensure(C.btab, total));
+        CK(cudaMemcpyAsync(C.btab.p, h.data(), total, cudaMemcpyHostToDevice, st));
+        CK(cudaStreamSynchronize(st)); // the host copy goes out of scope
+        d_meshes = (const MeshDev*)(C.btab.as<char>() + o_mesh);
+        d_grids = (const GridDev*)(C.btab.as<char>() + o_grid);
+        d_eoff = (const long long*)(C.btab.as<char>() + o_eoff);
+        d_voff = (const unsigned long long*)(C.btab.as<char>() + o_voff);
+        d_fptr = (double* const*)(C.btab.as<char>() + o_fptr);
     }
-
-    MeshDev md;
-    md.elemtype = m.elemtype;
-    md.npart = m.npart;
-    md.nelem = m.nelem;
-    md.pos = c.pos;
-    md.vel = c.vel;
-    md.mass = c.mass;
-    md.conn = c.conn;
-    md.periodic = m.periodic ? 1 : 0;
-    for (int i = 0; i < 3; ++i) {
-        md.bdim[i] = m.block_dims[i];
-        md.edim[i] = m.periodic ? m.block_dims[i] : m.block_dims[i] - 1;
-        md.box0[i] = m.box[0][i];
-        md.box1[i] = m.box[1][i];
-    }
-    double dxmin = 1.0e30;
-    for (int i = 0; i < 3; ++i)
-        if (g.d[i] < dxmin) dxmin = g.d[i];
-    const double tol = c.reftol * dxmin;
 
     RET(ensure(C.small, S_WORDS * 8));
     unsigned long long* sm = C.small.as<unsigned long long>();
@@ -396,17 +479,18 @@ int run_device(Call& c)
 
     CK(cudaEventRecord(C.ev[1], st));
     // ---- count tet images per element ----
-    const long long ne = m.nelem;
     RET(ensure(C.counts, (size_t)(ne + 1) * sizeof(long long)));
     RET(ensure(C.offsets, (size_t)(ne + 1) * sizeof(long long)));
     TessArgs ta = {};
     ta.m = md;
+    ta.nbatch = batch ? c.nbatch : 0;
+    ta.meshes = d_meshes;
+    ta.grids = d_grids;
+    ta.eoff = d_eoff;
     ta.g = gd;
     ta.max_lvl = c.maxlvl;
-    ta.ptol2 = tol * tol;
     ta.refine_mode = c.refine_mode;
     ta.stretch = c.reftol;
-    for (int i = 0; i < 3; ++i) ta.lag[i] = c.refine_cell[i];
     ta.status = (unsigned*)&sm[S_STATUS];
     ta.counters = &sm[S_TESS];
     std::vector<long long> offs_host;
@@ -473,6 +557,11 @@ int run_device(Call& c)
     it.elem = C.ielem.as<int>();
     it.pid = C.ipid.as<int>();
     it.key = C.ikey.as<uint16_t>();
+    it.grid = nullptr;
+    if (batch) {
+        RET(ensure(C.igrid, (size_t)cap * sizeof(uint16_t)));
+        it.grid = C.igrid.as<uint16_t>();
+    }
     it.cap = cap;
     ta.it = it;
 
@@ -490,6 +579,8 @@ int run_device(Call& c)
     ca.it = it;
     ca.order = C.order.as<int>();
     ca.g = gd;
+    ca.grids = d_grids;
+    ca.voff = d_voff;
     ca.mom_order = order;
     ca.status = (unsigned*)&sm[S_STATUS];
     ca.counters = &sm[S_CNT];
@@ -706,6 +797,9 @@ int run_device(Call& c)
             aa.it = it;
             aa.item_base = 0;
             aa.M = c.F[0]; aa.X = c.F[1]; aa.V = c.F[2]; aa.XX = c.F[3]; aa.XV = c.F[4]; aa.VV = c.F[5];
+            aa.nbatch = batch ? c.nbatch : 0;
+            aa.voff = d_voff;
+            aa.fptr = d_fptr;
             CK(launch_apply_records(aa, st));
             klaunch += 3; // iota, gather, apply
             CK(cudaEventRecord(C.ev[7], st));
@@ -936,6 +1030,72 @@ int psib_voxels(const psib_grid* grid, const psib_mesh* mesh, int mode, double r
     CK(cudaEventRecord(C->ev[7], st));
     CK(cudaEventSynchronize(C->ev[7]));
     if (o.stats) CK(cudaEventElapsedTime(&o.stats->ms_total, C->ev[0], C->ev[7]));
+    return PSIB_OK;
+}
+
+int psib_voxels_batch(const psib_grid* grids, const psib_mesh* meshes, int nbatch, int mode, double refine_tolerance,
+                      int refine_max_lvl, const psib_options* opt)
+{
+    g_err.clear();
+    psib_options o = {};
+    o.precision = PSIB_FP64;
+    o.memory = PSIB_DEVICE;
+    o.device = -1;
+    if (opt) o = *opt;
+    if (!grids || !meshes || nbatch <= 0) return fail(PSIB_ERR_ARG, "grids, meshes and nbatch > 0 are required");
+    if (nbatch > 65535) return fail(PSIB_ERR_ARG, "at most 65535 cutouts per batch");
+    if (o.memory != PSIB_DEVICE) return fail(PSIB_ERR_UNSUPPORTED, "a batch takes device memory (PSIB_DEVICE)");
+    unsigned long long nvox = 0;
+    long long nelem = 0;
+    for (int b = 0; b < nbatch; ++b) {
+        if (int r = validate(&grids[b], &meshes[b], mode, &o)) {
+            g_err = "cutout " + std::to_string(b) + ": " + g_err;
+            return r;
+        }
+        for (int f = 0; f < 6; ++f)
+            if ((grids[b].fields[f] == nullptr) != (grids[0].fields[f] == nullptr))
+                return fail(PSIB_ERR_ARG, "cutout %d: every grid of a batch must have the same fields", b);
+        nvox += (unsigned long long)grids[b].n[0] * grids[b].n[1] * grids[b].n[2];
+        nelem += meshes[b].nelem;
+    }
+    if (nvox >= (1ull << 32)) return fail(PSIB_ERR_ARG, "a batch of 2^32 voxels or more is not supported");
+    if (nelem >= (1ll << 31)) return fail(PSIB_ERR_ARG, "a batch of 2^31 elements or more is not supported");
+    if (o.refine_mode == PSIB_REFINE_STRETCH && !(refine_tolerance > 0.0))
+        return fail(PSIB_ERR_ARG, "the stretch threshold must be positive");
+    if (psib_device_count() <= 0) return fail(PSIB_ERR_NODEVICE, "no CUDA device is visible");
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    Ctx* C = nullptr;
+    RET(get_ctx(dev, &C));
+    Call c = {};
+    c.grid = &grids[0];
+    c.mesh = &meshes[0];
+    c.nbatch = nbatch;
+    c.grids = grids;
+    c.meshes = meshes;
+    c.refine_cell_given = o.refine_cell;
+    c.reftol = refine_tolerance;
+    c.maxlvl = refine_max_lvl > 6 ? 6 : (refine_max_lvl < 0 ? 0 : refine_max_lvl);
+    c.precision = o.precision;
+    c.deterministic = o.deterministic;
+    c.refine_mode = o.refine_mode;
+    c.C = C;
+    c.stats = o.stats;
+    if (o.stats) *o.stats = psib_stats{};
+    c.st = (cudaStream_t)o.stream;
+    for (int f = 0; f < 6; ++f) c.F[f] = grids[0].fields[f];
+    c.pos = meshes[0].pos;
+    c.vel = meshes[0].vel;
+    c.mass = meshes[0].mass;
+    c.conn = meshes[0].connectivity;
+    if (nelem == 0) return PSIB_OK;
+    CK(cudaEventRecord(C->ev[0], c.st));
+    RET(run_device(c));
+    if (o.stats) {
+        CK(cudaEventRecord(C->ev[7], c.st));
+        CK(cudaEventSynchronize(C->ev[7]));
+        CK(cudaEventElapsedTime(&o.stats->ms_total, C->ev[0], C->ev[7]));
+    }
     return PSIB_OK;
 }
 

@@ -96,6 +96,9 @@ __device__ void clip_item(const ClipArgs& a, long long t, Poly<R>* S, QPoly* QL,
                           Tally& tally)
 {
     static_assert(!ADJ || (sizeof(R) == 8 && !CENTRAL), "the adjoint walks the FP64 fragments");
+    // the image's grid: its cutout's in a batch, whose voxels start at vbase
+    const GridDev& g = a.grids ? a.grids[a.it.grid[t]] : a.g;
+    const unsigned long long vbase = a.voff ? a.voff[a.it.grid[t]] : 0ull;
     const double* fr = a.it.frame + t * FRAME;
     double p[4][3];
     for (int v = 0; v < 4; ++v)
@@ -109,15 +112,15 @@ __device__ void clip_item(const ClipArgs& a, long long t, Poly<R>* S, QPoly* QL,
     int lo[3], hi[3];
     for (int i = 0; i < 3; ++i) {
         double cmin = rb[0][i], cmax = rb[1][i];
-        const bool clo = a.g.w0[i] > cmin, chi = a.g.w1[i] < cmax;
-        if (clo) cmin = a.g.w0[i];
-        if (chi) cmax = a.g.w1[i];
+        const bool clo = g.w0[i] > cmin, chi = g.w1[i] < cmax;
+        if (clo) cmin = g.w0[i];
+        if (chi) cmax = g.w1[i];
         if (clo) { pax[npl] = i; psg[npl] = 1; pdd[npl] = -cmin; npl++; }
         if (chi) { pax[npl] = i; psg[npl] = -1; pdd[npl] = cmax; npl++; }
-        lo[i] = (int)floor((cmin - a.g.w0[i]) / a.g.d[i]);
-        hi[i] = (int)ceil((cmax - a.g.w0[i]) / a.g.d[i]);
+        lo[i] = (int)floor((cmin - g.w0[i]) / g.d[i]);
+        hi[i] = (int)ceil((cmax - g.w0[i]) / g.d[i]);
         if (lo[i] < 0) lo[i] = 0;
-        if (hi[i] > a.g.n[i]) hi[i] = a.g.n[i];
+        if (hi[i] > g.n[i]) hi[i] = g.n[i];
     }
 
     // slot pool
@@ -242,17 +245,17 @@ __device__ void clip_item(const ClipArgs& a, long long t, Poly<R>* S, QPoly* QL,
                     // recomputed in FP64 from their planes before the moments
                     double plo[3], phi[3], tol[3];
                     for (int i = 0; i < 3; ++i) {
-                        plo[i] = a.g.d[i] * P.lo[i] + a.g.w0[i];
-                        phi[i] = a.g.d[i] * (P.lo[i] + 1) + a.g.w0[i];
-                        tol[i] = 1.0e-3 * a.g.d[i];
+                        plo[i] = g.d[i] * P.lo[i] + g.w0[i];
+                        phi[i] = g.d[i] * (P.lo[i] + 1) + g.w0[i];
+                        tol[i] = 1.0e-3 * g.d[i];
                     }
                     exact_vertices(P, p, org, plo, phi, tol, *QL);
                     for (int i = 0; i < 3; ++i) o[i] = QL->q[0][i];
                 }
                 double gv = 0.0;
                 if constexpr (ADJ) {
-                    if (P.lo[0] < a.g.n[0] && P.lo[1] < a.g.n[1] && P.lo[2] < a.g.n[2])
-                        gv = a.adj_gm[((long long)a.g.n[1] * P.lo[0] + P.lo[1]) * a.g.n[2] + P.lo[2]];
+                    if (P.lo[0] < g.n[0] && P.lo[1] < g.n[1] && P.lo[2] < g.n[2])
+                        gv = a.adj_gm[((long long)g.n[1] * P.lo[0] + P.lo[1]) * g.n[2] + P.lo[2]];
                 }
                 unsigned e;
                 if constexpr (ADJ) e = gv != 0.0 ? reduce_poly(P, mom, 0) : 0u;
@@ -262,10 +265,11 @@ __device__ void clip_item(const ClipArgs& a, long long t, Poly<R>* S, QPoly* QL,
                 if (ADJ && gv == 0.0) {
                     // no upstream gradient in this voxel: nothing to pull back
                 } else if (mom[0] > 0.0) {
-                    if (P.lo[0] >= a.g.n[0] || P.lo[1] >= a.g.n[1] || P.lo[2] >= a.g.n[2]) {
+                    if (P.lo[0] >= g.n[0] || P.lo[1] >= g.n[1] || P.lo[2] >= g.n[2]) {
                         st |= ST_INDEX;
                     } else {
-                        const long long gi = ((long long)a.g.n[1] * P.lo[0] + P.lo[1]) * a.g.n[2] + P.lo[2];
+                        const long long gi =
+                            (long long)vbase + ((long long)g.n[1] * P.lo[0] + P.lo[1]) * g.n[2] + P.lo[2];
                         tally.frags++;
                         tally.verts += P.nv;
                         if constexpr (ADJ) {
@@ -296,7 +300,7 @@ __device__ void clip_item(const ClipArgs& a, long long t, Poly<R>* S, QPoly* QL,
             } else {
                 // split at the middle grid plane of the longest axis (src/geometry.c:886-893)
                 tally.splits++;
-                const double coord = a.g.d[ax] * (P.lo[ax] + dmax / 2) + a.g.w0[ax];
+                const double coord = g.d[ax] * (P.lo[ax] + dmax / 2) + g.w0[ax];
                 const R cr = (sizeof(R) == 8) ? (R)coord : (R)(coord - org[ax]);
                 uint32_t um = 0;
                 for (int v = 0; v < P.nv; ++v) {

@@ -24,6 +24,7 @@ struct ItemArrays {
     int *elem;       // cap: element index
     int *pid;        // 4 x cap: particle ids of the 4 vertices (unrefined meshes), else -1
     uint16_t *key;   // cap: 0xFFFF for images the deep-tree kernel takes, else larger boxes first
+    uint16_t *grid;  // cap: the image's cutout in a batch (null for a single grid)
     long long cap;
 };
 
@@ -42,6 +43,10 @@ struct ClipArgs {
     int mom_order;           // polynomial order of the moments (0, 1, 2)
     unsigned *status;
     unsigned long long *counters; // fragments, fragment vertices, splits
+    // a batch of cutouts: each image's grid is grids[it.grid[t]], its voxels are
+    // numbered from voff[it.grid[t]] (null for a single grid: g, from 0)
+    const GridDev *grids;
+    const unsigned long long *voff;
     // fragment records
     unsigned long long *rec_key; // voxel << rec_ibits | item
     double *rec_mom;             // rec_nmom doubles per record
@@ -69,6 +74,8 @@ struct MeshDev {
     int edim[3];  // element lattice of an implicit block mesh
     int periodic;
     double box0[3], box1[3];
+    double ptol2;   // midpoint refinement: squared tolerance (reftol x the grid's smallest cell)^2
+    double lag[3];  // stretch refinement: the Lagrangian cell
 };
 
 struct TessArgs {
@@ -76,9 +83,14 @@ struct TessArgs {
     GridDev g;
     long long e0, e1;          // element range
     int max_lvl;
-    double ptol2;
-    int refine_mode;           // 0: the reference's midpoint test (ptol2); 1: stretch beyond `stretch` x lag
-    double stretch, lag[3];
+    int refine_mode;           // 0: the reference's midpoint test (m.ptol2); 1: stretch beyond `stretch` x m.lag
+    double stretch;
+    // a batch of cutouts (nbatch > 0): element E belongs to cutout b with
+    // eoff[b] <= E < eoff[b + 1]; its mesh and grid are meshes[b], grids[b]
+    int nbatch;
+    const MeshDev *meshes;
+    const GridDev *grids;
+    const long long *eoff;
     const long long *offset;   // per element, exclusive (emit)
     long long offset_base;
     int *count;                // per element (count)
@@ -165,6 +177,11 @@ struct ApplyArgs {
     ItemArrays it;
     long long item_base;
     double *M, *X, *V, *XX, *XV, *VV;
+    // a batch: voxel v of the runs belongs to cutout b with voff[b] <= v < voff[b + 1],
+    // whose fields are fptr[6 b .. 6 b + 5] (m x v xx xv vv); M..VV are then cutout 0's
+    int nbatch;
+    const unsigned long long *voff;
+    double *const *fptr;
 };
 cudaError_t launch_apply_records(const ApplyArgs &a, cudaStream_t s);
 

@@ -164,6 +164,9 @@ __device__ uint16_t footprint_key(const double (*rb)[3], const GridDev& g)
 
 struct Emitter {
     const TessArgs& a;
+    const MeshDev& m; // the element's mesh and grid (its cutout's in a batch)
+    const GridDev& g;
+    int gid;          // the cutout
     bool write;      // false: count only
     long long pos;   // next item index (emit)
     int n;           // items so far
@@ -171,7 +174,7 @@ struct Emitter {
     __device__ void tet(const double (*p)[3], const double (*u)[3], double mass, long long e, const int* pid)
     {
         double rb[2][3];
-        const unsigned keep = tet_images(p, a.m, a.g, rb);
+        const unsigned keep = tet_images(p, m, g, rb);
         tets++;
         for (int s = 0; s < 8; ++s) {
             if (!((keep >> s) & 1u)) continue;
@@ -182,13 +185,13 @@ struct Emitter {
                 double* fr = a.it.frame + t * FRAME;
                 for (int v = 0; v < 4; ++v)
                     for (int i = 0; i < 3; ++i) {
-                        const double sh = (a.m.box1[i] - a.m.box0[i]) * (1 & (s >> i));
+                        const double sh = (m.box1[i] - m.box0[i]) * (1 & (s >> i));
                         q[v][i] = s ? p[v][i] + sh : p[v][i];
                         fr[3 * v + i] = q[v][i];
                         fr[FR_U + 3 * v + i] = u[v][i];
                     }
                 for (int i = 0; i < 3; ++i) {
-                    const double sh = (a.m.box1[i] - a.m.box0[i]) * (1 & (s >> i));
+                    const double sh = (m.box1[i] - m.box0[i]) * (1 & (s >> i));
                     rq[0][i] = s ? rb[0][i] + sh : rb[0][i];
                     rq[1][i] = s ? rb[1][i] + sh : rb[1][i];
                 }
@@ -196,7 +199,8 @@ struct Emitter {
                 fr[FR_MASS + 1] = 0.0;
                 a.it.elem[t] = (int)e;
                 for (int v = 0; v < 4; ++v) a.it.pid[v * cap + t] = pid ? pid[v] : -1;
-                a.it.key[t] = footprint_key(rq, a.g);
+                a.it.key[t] = footprint_key(rq, g);
+                if (a.it.grid) a.it.grid[t] = (uint16_t)gid;
             }
             n++;
         }
@@ -306,19 +310,19 @@ __device__ void refine_element(Emitter& em, const double (*cp)[3], const double 
 }
 
 template <bool REFINE>
-__device__ int element_items(const TessArgs& a, bool write, long long e, long long pos, unsigned long long& tets,
-                             RefNode* L)
+__device__ int element_items(const TessArgs& a, const MeshDev& m, const GridDev& g, int gid, bool write, long long e,
+                             long long pos, unsigned long long& tets, RefNode* L)
 {
     double p[8][3], u[8][3];
     int ids[8];
-    if (!gather(a.m, e, p, u, ids)) {
+    if (!gather(m, e, p, u, ids)) {
         atomicOr(a.status, ST_INDEX);
         return 0;
     }
-    const int et = a.m.elemtype;
-    if (!aabb_periodic(p, et, a.m, a.g)) return 0;
-    const double me = a.m.mass ? a.m.mass[e] : 1.0;
-    Emitter em{a, write, pos, 0, 0};
+    const int et = m.elemtype;
+    if (!aabb_periodic(p, et, m, g)) return 0;
+    const double me = m.mass ? m.mass[e] : 1.0;
+    Emitter em{a, m, g, gid, write, pos, 0, 0};
     if (et == 4) {
         em.tet(p, u, me, e, ids); // a simplex element is one tet (src/refine.c:60-66)
     } else if (!REFINE) {
@@ -336,8 +340,7 @@ __device__ int element_items(const TessArgs& a, bool write, long long e, long lo
             em.tet(tp, tu, me * (1.0 / 6), e, pid);
         }
     } else {
-        if constexpr (REFINE)
-            refine_element(em, p, u, me, e, a.max_lvl, a.ptol2, a.refine_mode, a.stretch, a.lag, L);
+        if constexpr (REFINE) refine_element(em, p, u, me, e, a.max_lvl, m.ptol2, a.refine_mode, a.stretch, m.lag, L);
     }
     tets += em.tets;
     return em.n;
@@ -353,7 +356,19 @@ __global__ void __launch_bounds__(128) k_tess(TessArgs a)
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long e = a.e0 + blockIdx.x * (long long)blockDim.x + threadIdx.x; e < a.e1; e += stride) {
         const long long pos = EMIT ? a.offset[e - a.e0] - a.offset_base : 0;
-        const int n = element_items<REFINE>(a, EMIT, e, pos, tets, L);
+        int n;
+        if (a.nbatch) {
+            // the element's cutout: the last b with eoff[b] <= e
+            int lo = 0, hi = a.nbatch;
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (a.eoff[mid] <= e) lo = mid;
+                else hi = mid;
+            }
+            n = element_items<REFINE>(a, a.meshes[lo], a.grids[lo], lo, EMIT, e - a.eoff[lo], pos, tets, L);
+        } else {
+            n = element_items<REFINE>(a, a.m, a.g, 0, EMIT, e, pos, tets, L);
+        }
         if (!EMIT) a.count[e - a.e0] = n;
         kept += (n > 0);
     }
@@ -372,7 +387,7 @@ static int tess_grid(long long n)
 cudaError_t launch_tess_count(const TessArgs& a, cudaStream_t s)
 {
     const int g = tess_grid(a.e1 - a.e0);
-    if (a.max_lvl > 0 && a.m.elemtype == 8)
+    if (a.max_lvl > 0 && (a.nbatch || a.m.elemtype == 8))
         k_tess<true, false><<<g, 128, 0, s>>>(a);
     else
         k_tess<false, false><<<g, 128, 0, s>>>(a);
@@ -382,7 +397,7 @@ cudaError_t launch_tess_count(const TessArgs& a, cudaStream_t s)
 cudaError_t launch_tess_emit(const TessArgs& a, cudaStream_t s)
 {
     const int g = tess_grid(a.e1 - a.e0);
-    if (a.max_lvl > 0 && a.m.elemtype == 8)
+    if (a.max_lvl > 0 && (a.nbatch || a.m.elemtype == 8))
         k_tess<true, true><<<g, 128, 0, s>>>(a);
     else
         k_tess<false, true><<<g, 128, 0, s>>>(a);
@@ -449,6 +464,25 @@ cudaError_t launch_gather_records(const GatherArgs& a, cudaStream_t s)
     return cudaGetLastError();
 }
 
+// The fields of the run's voxel gv: its cutout's in a batch, with the voxel's
+// index within that cutout.
+struct Fields {
+    double *M, *X, *V, *XX, *XV, *VV;
+    long long gi;
+};
+__device__ __forceinline__ Fields fields_of(const ApplyArgs& a, long long gv)
+{
+    if (!a.nbatch) return Fields{a.M, a.X, a.V, a.XX, a.XV, a.VV, gv};
+    int lo = 0, hi = a.nbatch;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (a.voff[mid] <= (unsigned long long)gv) lo = mid;
+        else hi = mid;
+    }
+    double* const* f = a.fptr + 6 * lo;
+    return Fields{f[0], f[1], f[2], f[3], f[4], f[5], gv - (long long)a.voff[lo]};
+}
+
 // One thread per voxel run walks the run in item order and applies
 // src/geometry.c:106-186 exactly as the reference does.  For raw FP64 records
 // this reproduces the reference's fields bit for bit.  The voxel's fields are
@@ -457,18 +491,19 @@ __global__ void __launch_bounds__(128) k_apply_runs(ApplyArgs a)
 {
     const long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (r >= a.nruns) return;
-    const long long gi = (long long)a.run_vox[r];
+    const Fields F = fields_of(a, (long long)a.run_vox[r]);
+    const long long gi = F.gi;
     const long long beg = a.run_off[r], end = beg + a.run_cnt[r];
     const bool hx = a.X, hv = a.V, hxx = a.XX, hxv = a.XV, hvv = a.VV;
-    double M = a.M[gi], X[3] = {0, 0, 0}, V[3] = {0, 0, 0}, XX[9], XV[9], VV[9];
+    double M = F.M[gi], X[3] = {0, 0, 0}, V[3] = {0, 0, 0}, XX[9], XV[9], VV[9];
     for (int i = 0; i < 3; ++i) {
-        if (hx) X[i] = a.X[3 * gi + i];
-        if (hv) V[i] = a.V[3 * gi + i];
+        if (hx) X[i] = F.X[3 * gi + i];
+        if (hv) V[i] = F.V[3 * gi + i];
     }
     for (int k = 0; k < 9; ++k) {
-        XX[k] = hxx ? a.XX[9 * gi + k] : 0.0;
-        XV[k] = hxv ? a.XV[9 * gi + k] : 0.0;
-        VV[k] = hvv ? a.VV[9 * gi + k] : 0.0;
+        XX[k] = hxx ? F.XX[9 * gi + k] : 0.0;
+        XV[k] = hxv ? F.XV[9 * gi + k] : 0.0;
+        VV[k] = hvv ? F.VV[9 * gi + k] : 0.0;
     }
     for (long long j = beg; j < end; ++j) {
         const long long t = a.item_base + (long long)a.item[j];
@@ -515,15 +550,15 @@ __global__ void __launch_bounds__(128) k_apply_runs(ApplyArgs a)
             for (int i = 0; i < 3; ++i) V[i] += cw * (cv[i] - V[i]);
         M += mass * mom[0];
     }
-    a.M[gi] = M;
+    F.M[gi] = M;
     for (int i = 0; i < 3; ++i) {
-        if (hx) a.X[3 * gi + i] = X[i];
-        if (hv) a.V[3 * gi + i] = V[i];
+        if (hx) F.X[3 * gi + i] = X[i];
+        if (hv) F.V[3 * gi + i] = V[i];
     }
     for (int k = 0; k < 9; ++k) {
-        if (hxx) a.XX[9 * gi + k] = XX[k];
-        if (hxv) a.XV[9 * gi + k] = XV[k];
-        if (hvv) a.VV[9 * gi + k] = VV[k];
+        if (hxx) F.XX[9 * gi + k] = XX[k];
+        if (hxv) F.XV[9 * gi + k] = XV[k];
+        if (hvv) F.VV[9 * gi + k] = VV[k];
     }
 }
 
@@ -629,7 +664,8 @@ __global__ void __launch_bounds__(128) k_apply_central(ApplyArgs a)
         for (int k = 0; k < 9; ++k) sxv[k] = group_sum(sxv[k]);
     if (!run_ok || l != 0 || !(sm > 0.0)) return;
     // this voxel's new fragments as one: mass, means, central (co)variances
-    const long long gi = (long long)a.run_vox[r];
+    const Fields F = fields_of(a, (long long)a.run_vox[r]);
+    const long long gi = F.gi;
     double xr[3], vr[3], dxr[3], dvr[3];
     for (int i = 0; i < 3; ++i) {
         dxr[i] = sx[i] / sm;
@@ -637,13 +673,13 @@ __global__ void __launch_bounds__(128) k_apply_central(ApplyArgs a)
         xr[i] = rx[i] + dxr[i];
         vr[i] = rv[i] + dvr[i];
     }
-    const double M0 = a.M[gi], Mf = M0 + sm;
+    const double M0 = F.M[gi], Mf = M0 + sm;
     const double cw = sm / Mf, dw = M0 / Mf;
     // merged with what the voxel holds (src/geometry.c:164-186 for one combined fragment)
     double X0[3] = {0, 0, 0}, V0[3] = {0, 0, 0};
     for (int i = 0; i < 3; ++i) {
-        if (hx) X0[i] = a.X[3 * gi + i];
-        if (hv) V0[i] = a.V[3 * gi + i];
+        if (hx) X0[i] = F.X[3 * gi + i];
+        if (hv) V0[i] = F.V[3 * gi + i];
     }
     if (hxx) {
         int k = 0;
@@ -652,7 +688,7 @@ __global__ void __launch_bounds__(128) k_apply_central(ApplyArgs a)
             for (int j2 = i; j2 < 3; ++j2, ++k) C[i][j2] = C[j2][i] = sxx[k] / sm - dxr[i] * dxr[j2];
         for (int i = 0; i < 3; ++i)
             for (int j2 = 0; j2 < 3; ++j2) {
-                double* t = &a.XX[9 * gi + 3 * i + j2];
+                double* t = &F.XX[9 * gi + 3 * i + j2];
                 *t = dw * *t + cw * C[i][j2] + cw * dw * (xr[i] - X0[i]) * (xr[j2] - X0[j2]);
             }
     }
@@ -663,7 +699,7 @@ __global__ void __launch_bounds__(128) k_apply_central(ApplyArgs a)
             for (int j2 = i; j2 < 3; ++j2, ++k) C[i][j2] = C[j2][i] = svv[k] / sm - dvr[i] * dvr[j2];
         for (int i = 0; i < 3; ++i)
             for (int j2 = 0; j2 < 3; ++j2) {
-                double* t = &a.VV[9 * gi + 3 * i + j2];
+                double* t = &F.VV[9 * gi + 3 * i + j2];
                 *t = dw * *t + cw * C[i][j2] + cw * dw * (vr[i] - V0[i]) * (vr[j2] - V0[j2]);
             }
     }
@@ -671,14 +707,14 @@ __global__ void __launch_bounds__(128) k_apply_central(ApplyArgs a)
         for (int i = 0; i < 3; ++i)
             for (int j2 = 0; j2 < 3; ++j2) {
                 const double C = sxv[3 * i + j2] / sm - dxr[i] * dvr[j2];
-                double* t = &a.XV[9 * gi + 3 * i + j2];
+                double* t = &F.XV[9 * gi + 3 * i + j2];
                 *t = dw * *t + cw * C + cw * dw * (xr[i] - X0[i]) * (vr[j2] - V0[j2]);
             }
     if (hx)
-        for (int i = 0; i < 3; ++i) a.X[3 * gi + i] = X0[i] + cw * (xr[i] - X0[i]);
+        for (int i = 0; i < 3; ++i) F.X[3 * gi + i] = X0[i] + cw * (xr[i] - X0[i]);
     if (hv)
-        for (int i = 0; i < 3; ++i) a.V[3 * gi + i] = V0[i] + cw * (vr[i] - V0[i]);
-    a.M[gi] = Mf;
+        for (int i = 0; i < 3; ++i) F.V[3 * gi + i] = V0[i] + cw * (vr[i] - V0[i]);
+    F.M[gi] = Mf;
 }
 
 cudaError_t launch_apply_records(const ApplyArgs& a, cudaStream_t s)
