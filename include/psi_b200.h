@@ -124,6 +124,9 @@ typedef struct {
     psib_stats *stats; /* optional */
     int refine_mode;   /* PSIB_REFINE_MIDPOINT (0) or PSIB_REFINE_STRETCH */
     double refine_cell[3]; /* stretch: the Lagrangian cell; all <= 0: box / block_dims of a periodic block mesh */
+    long long queue_voxels; /* mixed precision: tets walked per pass, bounded by the sum of their index-box
+                               volumes (the size of every polyhedron queue); 0: automatic (up to 64M, within
+                               35% of the free device memory) */
 } psib_options;
 
 /* Deposit the mesh's tets on the grid: the density branch of psi_voxels

@@ -44,7 +44,7 @@ class Stats(C.Structure):
 class Options(C.Structure):
     _fields_ = [("precision", C.c_int), ("deterministic", C.c_int), ("memory", C.c_int), ("device", C.c_int),
                 ("stream", C.c_void_p), ("stats", C.POINTER(Stats)), ("refine_mode", C.c_int),
-                ("refine_cell", C.c_double * 3)]
+                ("refine_cell", C.c_double * 3), ("queue_voxels", C.c_longlong)]
 
 
 lib.psib_voxels.argtypes = [C.POINTER(Grid), C.POINTER(Mesh), C.c_int, C.c_double, C.c_int, C.POINTER(Options)]
@@ -167,7 +167,7 @@ def adjoint_device(grad_m, n, bounds, pos, grad_pos, mass=None, connectivity=Non
 
 
 def voxels_batch_device(cutouts: list, precision="fp64", refine_tolerance=1.0, refine_max_lvl=0,
-                        refine_criterion="midpoint", refine_cell=None, stream=None) -> dict:
+                        refine_criterion="midpoint", refine_cell=None, stream=None, queue_voxels=0) -> dict:
     """Many independent deposits in one pass (psib_voxels_batch).
 
     cutouts: dicts with the arguments of voxels_device -- fields, n, bounds,
@@ -187,10 +187,43 @@ def voxels_batch_device(cutouts: list, precision="fp64", refine_tolerance=1.0, r
     s = stream if stream is not None else torch.cuda.current_stream()
     st = Stats()
     o = Options(precision=PRECISIONS[precision], deterministic=0, memory=PSIB_DEVICE, device=-1,
-                stream=C.c_void_p(s.cuda_stream), stats=C.pointer(st), refine_mode=REFINE[refine_criterion])
+                stream=C.c_void_p(s.cuda_stream), stats=C.pointer(st), refine_mode=REFINE[refine_criterion],
+                queue_voxels=int(queue_voxels))
     if refine_cell is not None:
         o.refine_cell[:] = [float(v) for v in refine_cell]
     rc = lib.psib_voxels_batch(grids, meshes, nb, 0, float(refine_tolerance), int(refine_max_lvl), C.byref(o))
     if rc != 0:
         raise PsibError(rc)
     return st.as_dict()
+
+
+def autotune_batch(cutouts: list, candidates=(8 << 20, 16 << 20, 32 << 20, 64 << 20), precision="mixed",
+                   repeats=2, **kw) -> int:
+    """Pick the queue capacity (psib_options.queue_voxels) for a batch that will
+    be deposited many times (the same cutouts with new positions, say).
+
+    Each candidate is timed with CUDA events over `repeats` batch calls after
+    one warm-up call; the fields of the cutouts are zeroed afterwards.  Returns
+    the fastest capacity, to pass as voxels_batch_device(queue_voxels=...)."""
+    import torch
+
+    best, best_ms = 0, float("inf")
+    stream = torch.cuda.current_stream()
+    for cap in candidates:
+        try:
+            voxels_batch_device(cutouts, precision=precision, queue_voxels=cap, **kw)
+        except PsibError:
+            continue  # e.g. not enough memory for this capacity
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(repeats):
+            voxels_batch_device(cutouts, precision=precision, queue_voxels=cap, **kw)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / repeats
+        if ms < best_ms:
+            best, best_ms = cap, ms
+    for c in cutouts:
+        for t in c["fields"].values():
+            t.zero_()
+    return best

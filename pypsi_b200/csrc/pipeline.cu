@@ -195,6 +195,7 @@ struct Call {
     const int* conn;
     int refine_mode;
     double refine_cell[3];
+    long long queue_voxels;
     // a batch of cutouts (nbatch > 0): host arrays of grids and meshes (device pointers)
     int nbatch;
     const psib_grid* grids;
@@ -222,7 +223,7 @@ int check_status(Call& c, unsigned long long* small_host)
 // first; a pass takes images while the sum of their box volumes -- a bound on
 // every queue of the pass -- stays within the queue capacity.
 int bfs_clip(Ctx& C, ClipArgs& ca, long long nmain, long long nitems, unsigned long long* sm, int clip_grid,
-             int clip_block, cudaStream_t st, long long& launches, long long& klaunch)
+             int clip_block, long long queue_voxels, cudaStream_t st, long long& launches, long long& klaunch)
 {
     RET(ensure(C.hist, 65536 * sizeof(unsigned)));
     CK(cudaMemsetAsync(C.hist.p, 0, 65536 * sizeof(unsigned), st));
@@ -232,7 +233,21 @@ int bfs_clip(Ctx& C, ClipArgs& ca, long long nmain, long long nitems, unsigned l
     std::vector<unsigned> hist(65536);
     CK(cudaMemcpyAsync(hist.data(), C.hist.p, 65536 * sizeof(unsigned), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
-    const long long cap = std::max<long long>(env_ll("PSIB_BFS_CAP", 16ll << 20), 1024);
+    // queue capacity in box voxels: asked for, or up to 64M within 35% of the free memory
+    // (three queues of bytes_per_elem each)
+    long long cap = queue_voxels;
+    if (cap <= 0) {
+        const long long bytes_per_elem = MAXV * 3 * 4 + MAXV * 4 + 1 + 1 + 12 + 4;
+        size_t freeb = 0, totalb = 0;
+        if (cudaMemGetInfo(&freeb, &totalb) != cudaSuccess) {
+            cudaGetLastError();
+            freeb = 0;
+        }
+        long long have = (long long)(C.qx[0].n / (MAXV * 3 * 4)); // queues already allocated count as free
+        cap = std::max<long long>(have, (long long)(0.35 * (double)freeb) / (3 * bytes_per_elem));
+        cap = std::min<long long>(cap, 64ll << 20);
+    }
+    cap = std::max<long long>(env_ll("PSIB_BFS_CAP", cap), 1024);
     std::vector<long long> qb{0};
     long long cur = 0, pos = 0;
     for (int k = 0; k < 0xFFFF; ++k) {
@@ -690,7 +705,8 @@ int run_device(Call& c)
             CK(cudaEventRecord(C.ev[4], st));
             if (nmain > 0 && use_bfs) {
                 ca.scratch = C.scratch.p;
-                RET(bfs_clip(C, ca, nmain, nitems, sm, clip_grid, clip_block, st, launches, klaunch));
+                RET(bfs_clip(C, ca, nmain, nitems, sm, clip_grid, clip_block, c.queue_voxels, st, launches,
+                             klaunch));
             } else if (nmain > 0) {
                 ca.scratch = C.scratch.p;
                 ca.order_base = 0;
@@ -977,6 +993,7 @@ int psib_voxels(const psib_grid* grid, const psib_mesh* mesh, int mode, double r
     c.precision = o.precision;
     c.deterministic = o.deterministic;
     c.refine_mode = o.refine_mode;
+    c.queue_voxels = o.queue_voxels;
     if (o.refine_mode == PSIB_REFINE_STRETCH) {
         const bool given = o.refine_cell[0] > 0.0 && o.refine_cell[1] > 0.0 && o.refine_cell[2] > 0.0;
         for (int i = 0; i < 3; ++i) {
@@ -1079,6 +1096,7 @@ int psib_voxels_batch(const psib_grid* grids, const psib_mesh* meshes, int nbatc
     c.precision = o.precision;
     c.deterministic = o.deterministic;
     c.refine_mode = o.refine_mode;
+    c.queue_voxels = o.queue_voxels;
     c.C = C;
     c.stats = o.stats;
     if (o.stats) *o.stats = psib_stats{};

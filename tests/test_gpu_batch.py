@@ -98,3 +98,22 @@ def test_batch_rejects_mismatched_fields_and_host_memory(gpu):
     m = (capi.Mesh * 1)()
     assert lib.psib_voxels_batch(g, m, 1, 0, 1.0, 0, C.byref(o)) == 6  # PSIB_ERR_UNSUPPORTED
     assert b"device memory" in lib.psib_last_error()
+
+
+def test_autotune_batch_picks_a_candidate_and_clears(gpu):
+    from pypsi_b200 import capi
+
+    cutouts = _cutouts(6, 5)
+    import torch
+
+    for c in cutouts:
+        c["fields"] = {f: torch.zeros(sh, dtype=torch.float64, device="cuda") for f, sh in c["shapes"].items()}
+    args = [{k: v for k, v in c.items() if k != "shapes"} for c in cutouts]
+    cap = capi.autotune_batch(args, candidates=(4096, 1 << 16), repeats=1)
+    assert cap in (4096, 1 << 16)
+    assert all(float(t.abs().max()) == 0.0 for c in cutouts for t in c["fields"].values())
+    # a tiny capacity forces many passes and must give the same fields
+    ref, _ = _run(cutouts, "mixed", True)
+    small, _ = _run(cutouts, "mixed", True, queue_voxels=4096)
+    for s, t in zip(ref, small):
+        assert np.abs(s["m"] - t["m"]).max() <= 1e-12 * s["m"].max()
