@@ -531,21 +531,27 @@ def run_ours(args):
     if rank != 0:
         return
 
-    # roofline of the clip kernels: algorithmic FP64 flops per fragment
-    # F_2 = 20 V + 132 (2V - 4) + 520 (V = mean vertices per fragment; clip,
-    # order-2 reduce, projection and update)
+    # roofline of the clip walk (k_bfs_init/level/leaf plus the small deep-tree
+    # kernel): the algorithmic bytes it moves -- polyhedra read and written
+    # between levels, tet vertices, fragment records -- counted by the kernels
+    # (walk_bytes), over the walk's event time, against the measured HBM copy
+    # bandwidth; beside it the FP64 arithmetic per fragment,
+    # F_2 = 20 V + 132 (2V - 4) + 520 (V = mean vertices per fragment), against
+    # the FP64 issue rate
     s = st_mixed[-1]
     frags = s["fragments"] / s["passes"]
     vbar = s["frag_verts"] / max(1, s["fragments"])
     flops = frags * (20 * vbar + 132 * (2 * vbar - 4) + 520)
     clip_ms = statistics.mean(x["ms_clip"] for x in st_mixed)
     launches = s["clip_launches"]
-    achieved = flops / (clip_ms * 1e-3) / 1e12
-    peak = 148 * FP64_FMA_PER_CLK_PER_SM * 2 * 1965e6 / 1e12
+    fp64_tflops = flops / (clip_ms * 1e-3) / 1e12
+    fp64_peak = 148 * FP64_FMA_PER_CLK_PER_SM * 2 * 1965e6 / 1e12
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except OSError:
         peaks = {}
+    hbm_peak = peaks.get("hbm_gbs") or 6650.0
+    walk_gbs = s["walk_bytes"] / (clip_ms * 1e-3) / 1e9
     value = world * tets_per_step / (ms_mixed * 1e-3)
     line = {
         "metric": METRIC, "value": value, "unit": "tets/s", "n_gpus": world, "steps": args.steps,
@@ -573,13 +579,19 @@ def run_ours(args):
                      "sort_and_apply": statistics.mean(x["ms_final"] for x in st_mixed)},
         "work": {"tets": tets_per_step, "tet_images": s["tet_images"], "fragments_per_pass": frags,
                  "verts_per_fragment": vbar, "passes": s["passes"], "splits_per_pass": s["splits"] / s["passes"]},
-        "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                     "traffic": None, "kernel": "clip (records)",
-                     "achieved_def": "sum over fragments of F_2 algorithmic FP64 flops / clip-kernel event time",
-                     "peak_source": "FP64 FMA issue rate 64/clk/SM x 148 SMs x 2 flop at 1965 MHz; "
-                                    "MEASURED_PEAKS.json has no FP64 figure",
-                     "clip_ms_per_step": clip_ms, "clip_launches_per_step": launches,
-                     "hbm_peak_gbs_measured": peaks.get("hbm_gbs")},
+        "roofline": {"bound": "hbm", "achieved": walk_gbs, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": walk_gbs / hbm_peak, "traffic": None,
+                     "kernel": "clip walk (k_bfs_init, k_bfs_level, k_bfs_leaf, k_clip_mixed_big)",
+                     "achieved_def": "walk_bytes (algorithmic bytes counted by the kernels: polyhedra read and "
+                                     "written, tet vertices, records) / clip event time",
+                     "units": {"walk_bytes_per_step": s["walk_bytes"], "fragments_per_step": frags},
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks.get("hbm_gbs")
+                     else "fallback 6650 GB/s",
+                     "fp64": {"achieved": fp64_tflops, "peak": fp64_peak, "unit": "TFLOP/s",
+                              "frac": fp64_tflops / fp64_peak,
+                              "def": "F_2 algorithmic FP64 flops per fragment / clip event time; peak = FP64 FMA "
+                                     "issue rate 64/clk/SM x 148 SMs x 2 flop at 1965 MHz"},
+                     "clip_ms_per_step": clip_ms, "clip_launches_per_step": launches},
         "e2e": e2e,
         "gpu_launches": int(sum(x["kernel_launches"] for x in st_mixed)),
         "clocks": clocks,

@@ -112,6 +112,8 @@ typedef struct {
     float ms_final;          /* device time of the record sort and the field update */
     long long clip_launches; /* launches of the clip kernels */
     long long kernel_launches; /* launches of this library's own kernels (library scans/sorts excluded) */
+    long long walk_bytes;    /* mixed precision: bytes the breadth-first walk reads and writes by its
+                                algorithm (polyhedra, tet vertices, fragment records) */
 } psib_stats;
 
 typedef struct {

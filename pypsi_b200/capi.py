@@ -35,7 +35,7 @@ class Stats(C.Structure):
                 ("fragments", C.c_longlong), ("frag_verts", C.c_longlong), ("splits", C.c_longlong),
                 ("passes", C.c_int), ("chunks", C.c_int), ("ms_total", C.c_float), ("ms_clip", C.c_float),
                 ("ms_tess", C.c_float), ("ms_final", C.c_float), ("clip_launches", C.c_longlong),
-                ("kernel_launches", C.c_longlong)]
+                ("kernel_launches", C.c_longlong), ("walk_bytes", C.c_longlong)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

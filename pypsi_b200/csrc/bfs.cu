@@ -83,6 +83,9 @@ __device__ __forceinline__ void put_box(const PolyQueue& Q, unsigned long long e
 {
     for (int a = 0; a < 3; ++a) Q.box[3 * e + a] = (uint32_t)lo[a] | ((uint32_t)hi[a] << 16);
 }
+// queue element bytes: positions and links of nv vertices, nv, window mask, box, image
+__device__ __forceinline__ unsigned long long elem_bytes(int nv) { return 16ull * nv + 18ull; }
+
 __device__ __forceinline__ bool one_voxel(const int* lo, const int* hi)
 {
     return hi[0] - lo[0] <= 1 && hi[1] - lo[1] <= 1 && hi[2] - lo[2] <= 1;
@@ -133,6 +136,7 @@ __global__ void __launch_bounds__(BB) k_bfs_init(BfsArgs a)
     const long long warp = (long long)blockIdx.x * (BB / 32) + (threadIdx.x >> 5);
     const long long nwarp = (long long)gridDim.x * (BB / 32);
     unsigned st = 0;
+    unsigned long long moved = 0;
     for (long long base = a.q0 + warp * 32; base < a.q1; base += nwarp * 32) {
         const long long i = base + lane;
         const bool act = i < a.q1;
@@ -196,6 +200,7 @@ __global__ void __launch_bounds__(BB) k_bfs_init(BfsArgs a)
                     Q.nb[qn(e, v)] = links[v] | ((0xFu & ~(1u << v)) << 24);
                 }
                 Q.nv[e] = 4;
+                moved += 96 + elem_bytes(4);
                 Q.win[e] = (uint8_t)(wbfs ? wmask : 0u);
                 put_box(Q, e, lo, hi);
                 Q.item[e] = (uint32_t)t;
@@ -203,6 +208,7 @@ __global__ void __launch_bounds__(BB) k_bfs_init(BfsArgs a)
         }
     }
     if (st) atomicOr(a.c.status, st);
+    if (a.bytes && moved) atomicAdd(a.bytes, moved);
 }
 
 // ---- level: one cut per polyhedron ----
@@ -320,7 +326,7 @@ __global__ void __launch_bounds__(BB) k_bfs_level(BfsArgs a)
     // a producer reserves before it checks capacity (and flags the overflow), so clamp
     const unsigned long long n = min(*a.in.count, a.in.cap);
     unsigned st = 0;
-    unsigned long long splits = 0;
+    unsigned long long splits = 0, moved = 0;
     for (unsigned long long base = (unsigned long long)warp * 32; base < n; base += (unsigned long long)nwarp * 32) {
         const unsigned long long e = base + lane;
         bool act = e < n;
@@ -334,6 +340,7 @@ __global__ void __launch_bounds__(BB) k_bfs_level(BfsArgs a)
         }
         if (act) {
             get_box(a.in, e, lo, hi);
+            moved += elem_bytes(nv);
             t = a.in.item[e];
             const GridDev& g = grid_of(a.c, t);
             const double* fr = a.c.it.frame + (size_t)t * FRAME; // vertex 0: the origin of the FP32 positions
@@ -406,6 +413,7 @@ __global__ void __launch_bounds__(BB) k_bfs_level(BfsArgs a)
                     a.leaf.nb[qn(d, v)] = AT(nbI, v);
                 }
                 a.leaf.nv[d] = (uint8_t)nv;
+                moved += elem_bytes(nv);
                 put_box(a.leaf, d, lo, hi);
                 a.leaf.item[d] = t;
             }
@@ -425,6 +433,8 @@ __global__ void __launch_bounds__(BB) k_bfs_level(BfsArgs a)
                     st |= e2;
                     QL.nv[el] = 0; // downstream kernels skip these
                     QU.nv[eu] = 0;
+                } else {
+                    moved += elem_bytes(QL.nv[el]) + elem_bytes(QU.nv[eu]);
                 }
                 put_box(QL, el, llo, lhi);
                 put_box(QU, eu, ulo, uhi);
@@ -445,6 +455,8 @@ __global__ void __launch_bounds__(BB) k_bfs_level(BfsArgs a)
                 if (e2) {
                     st |= e2;
                     QL.nv[el] = 0;
+                } else {
+                    moved += elem_bytes(QL.nv[el]);
                 }
                 put_box(QL, el, lo, hi);
                 QL.item[el] = t;
@@ -454,6 +466,7 @@ __global__ void __launch_bounds__(BB) k_bfs_level(BfsArgs a)
     }
     if (st) atomicOr(a.c.status, st);
     if (a.c.counters && splits) atomicAdd(&a.c.counters[2], splits);
+    if (a.bytes && moved) atomicAdd(a.bytes, moved);
 }
 
 // ---- leaf: fragment moments and records ----
@@ -530,7 +543,7 @@ __global__ void __launch_bounds__(BB) k_bfs_leaf(BfsArgs a)
     const unsigned long long n = min(*a.leaf.count, a.leaf.cap);
     const ClipArgs& c = a.c;
     unsigned st = 0;
-    unsigned long long frags = 0, verts = 0;
+    unsigned long long frags = 0, verts = 0, moved = 0;
     for (unsigned long long base = (unsigned long long)warp * 32; base < n; base += (unsigned long long)nwarp * 32) {
         const unsigned long long e = base + lane;
         bool has = false;
@@ -562,6 +575,7 @@ __global__ void __launch_bounds__(BB) k_bfs_leaf(BfsArgs a)
                     exact_q(x, w, p0, DX, p0, plo, phi, tol, q);
                     for (int i = 0; i < 3; ++i) AT(qs, 3 * v + i) = q[i];
                 }
+                moved += elem_bytes(nv) + 96; // the fragment and its image's vertices
                 double o[3], mom[10];
                 const unsigned e2 = leaf_moments(nv, nbs, qs, c.mom_order, o, mom);
                 if (e2) {
@@ -597,6 +611,7 @@ __global__ void __launch_bounds__(BB) k_bfs_leaf(BfsArgs a)
         if (has) {
             const unsigned long long r = r0 + off;
             if (r < c.rec_cap) {
+                moved += 8ull * (1 + c.rec_nmom);
                 c.rec_key[r] = key;
                 double* dst = c.rec_mom + r * c.rec_nmom;
 #pragma unroll
@@ -612,6 +627,7 @@ __global__ void __launch_bounds__(BB) k_bfs_leaf(BfsArgs a)
         atomicAdd(&c.counters[0], frags);
         atomicAdd(&c.counters[1], verts);
     }
+    if (a.bytes && moved) atomicAdd(a.bytes, moved);
 }
 
 // FP32 walks can misplace a vertex that falls back to its FP32 position by

@@ -133,7 +133,7 @@ int get_ctx(int dev, Ctx** out)
 
 // small device block layout (unsigned long long words)
 enum { S_STATUS = 0, S_CNT = 1 /* 3 words */, S_TESS = 4 /* 2 */, S_HEAD = 8 /* 4 */, S_RECN = 12, S_NDEEP = 13,
-       S_DFS = 14, S_WORDS = 16 };
+       S_DFS = 14, S_BYTES = 15, S_WORDS = 16 };
 
 // Histogram of the sorted footprint keys: lanes holding equal keys (most of a
 // warp, as the keys are sorted) add with one atomic.
@@ -314,6 +314,7 @@ int bfs_clip(Ctx& C, ClipArgs& ca, long long nmain, long long nitems, unsigned l
     ba.c = ca;
     ba.dfs_list = C.dfs_list.as<int>();
     ba.dfs_count = &sm[S_DFS];
+    ba.bytes = &sm[S_BYTES];
     ba.window_bfs = env_ll("PSIB_BFS_WINDOW", 1) != 0;
     RET(ensure(C.vsum, (size_t)std::max<long long>(nitems, 1) * sizeof(double)));
     ba.vsum = C.vsum.as<double>();
@@ -613,6 +614,7 @@ int run_device(Call& c)
 
     float ms_clip = 0.f, ms_tess = 0.f, ms_final = 0.f;
     unsigned long long clip_counts[3] = {0, 0, 0}; // fragments, fragment vertices, splits
+    unsigned long long walk_bytes = 0;
     long long launches = 0;
     for (int k = 0; k < nchunks; ++k) {
         const long long e0 = cb[k], e1 = cb[k + 1];
@@ -700,6 +702,7 @@ int run_device(Call& c)
             ca.rec_mom = C.rmom.as<double>();
             ca.rec_cap = std::min<unsigned long long>(C.rkey.n / 8, C.rmom.n / (8 * nmom));
             CK(cudaMemsetAsync(&sm[S_RECN], 0, 8, st));
+            CK(cudaMemsetAsync(&sm[S_BYTES], 0, 8, st));
             CK(cudaMemsetAsync(&sm[S_CNT], 0, 24, st)); // this attempt's counters
             CK(cudaMemsetAsync(&sm[S_HEAD], 0, 16, st));
             CK(cudaEventRecord(C.ev[4], st));
@@ -747,6 +750,7 @@ int run_device(Call& c)
             }
             RET(check_status(c, h));
             for (int w = 0; w < 3; ++w) clip_counts[w] += h[S_CNT + w];
+            walk_bytes += h[S_BYTES];
             if (nrec >= (1ull << 32)) return fail(PSIB_ERR_OVERFLOW, "too many fragments in one chunk");
             if (nrec == 0) break;
             // ---- sort records by (voxel, image), gather them in that order, apply each voxel's run ----
@@ -845,6 +849,7 @@ int run_device(Call& c)
         s.ms_final = ms_final;
         s.clip_launches = launches;
         s.kernel_launches = klaunch + launches;
+        s.walk_bytes = (long long)walk_bytes;
     }
     (void)nvox;
     return PSIB_OK;

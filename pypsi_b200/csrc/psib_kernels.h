@@ -137,6 +137,7 @@ struct BfsArgs {
     unsigned long long *dfs_count;
     int last;                 // level: the last level, which must leave no polyhedron unfinished
     double *vsum;             // per image: sum of its fragment q-volumes (leaf), for the mass correction
+    unsigned long long *bytes; // algorithmic bytes the walk reads and writes (polyhedra, frames, records)
     int window_bfs;           // init: window-clipped images are walked here too (else listed for the
                               // depth-first kernel)
 };
