@@ -85,7 +85,9 @@ int ensure(DevBuf& b, size_t bytes)
 struct Ctx {
     int device = -1;
     int num_sms = 0;
-    cudaStream_t own = nullptr; // stream of host-memory calls
+    cudaStream_t own = nullptr;  // stream of host-memory calls
+    cudaStream_t copy = nullptr; // host-memory calls: the field copies, beside the first stages
+    cudaEvent_t fields_in = nullptr;
     cudaEvent_t ev[8] = {};
     // host-mode copies
     DevBuf hpos, hvel, hmass, hconn, hfield[6], hgpos, hgmass;
@@ -124,6 +126,8 @@ int get_ctx(int dev, Ctx** out)
         c->device = dev;
         CK(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, dev));
         CK(cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&c->fields_in, cudaEventDisableTiming));
         for (auto& e : c->ev) CK(cudaEventCreate(&e));
         g_ctx[dev] = c;
     }
@@ -196,6 +200,7 @@ struct Call {
     int refine_mode;
     double refine_cell[3];
     long long queue_voxels;
+    cudaEvent_t fields_ready; // host-memory calls: recorded when the fields are on the device
     // a batch of cutouts (nbatch > 0): host arrays of grids and meshes (device pointers)
     int nbatch;
     const psib_grid* grids;
@@ -820,6 +825,8 @@ int run_device(Call& c)
             aa.nbatch = batch ? c.nbatch : 0;
             aa.voff = d_voff;
             aa.fptr = d_fptr;
+            // host-memory calls copy the fields in beside the first stages; only this one needs them
+            if (c.fields_ready) CK(cudaStreamWaitEvent(st, c.fields_ready, 0));
             CK(launch_apply_records(aa, st));
             klaunch += 3; // iota, gather, apply
             CK(cudaEventRecord(C.ev[7], st));
@@ -1036,14 +1043,20 @@ int psib_voxels(const psib_grid* grid, const psib_mesh* mesh, int mode, double r
     c.st = st;
     CK(cudaEventRecord(C->ev[0], st));
     if (mesh->nelem > 0) RET(copy_mesh_in(c, *C, *mesh, st));
+    // the grid fields travel on a second stream while the mesh is tessellated and clipped;
+    // the field update waits for them (the previous call ended with a synchronize, so the
+    // device copies are free)
     for (int f = 0; f < 6; ++f) {
         if (!grid->fields[f]) continue;
         const size_t b = (size_t)nvox * comps[f] * sizeof(double);
         RET(ensure(C->hfield[f], b));
-        CK(cudaMemcpyAsync(C->hfield[f].p, grid->fields[f], b, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(C->hfield[f].p, grid->fields[f], b, cudaMemcpyHostToDevice, C->copy));
         c.F[f] = C->hfield[f].as<double>();
     }
+    CK(cudaEventRecord(C->fields_in, C->copy));
+    c.fields_ready = C->fields_in;
     if (mesh->nelem > 0) RET(run_device(c));
+    CK(cudaStreamWaitEvent(st, C->fields_in, 0));
     for (int f = 0; f < 6; ++f) {
         if (!grid->fields[f]) continue;
         const size_t b = (size_t)nvox * comps[f] * sizeof(double);
