@@ -59,6 +59,9 @@ int fail(int code, const char* fmt, ...)
         if (_r != PSIB_OK) return _r;  \
     } while (0)
 
+// host-memory calls copy the fields out in this many voxel slabs, each beside the update of the next
+constexpr int NOUT = 4;
+
 struct DevBuf {
     void* p = nullptr;
     size_t n = 0;
@@ -88,6 +91,7 @@ struct Ctx {
     cudaStream_t own = nullptr;  // stream of host-memory calls
     cudaStream_t copy = nullptr; // host-memory calls: the field copies, beside the first stages
     cudaEvent_t fields_in = nullptr;
+    cudaEvent_t ev_out[NOUT] = {};
     cudaEvent_t ev[8] = {};
     // host-mode copies
     DevBuf hpos, hvel, hmass, hconn, hfield[6], hgpos, hgmass;
@@ -128,6 +132,7 @@ int get_ctx(int dev, Ctx** out)
         CK(cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking));
         CK(cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking));
         CK(cudaEventCreateWithFlags(&c->fields_in, cudaEventDisableTiming));
+        for (auto& e : c->ev_out) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         for (auto& e : c->ev) CK(cudaEventCreate(&e));
         g_ctx[dev] = c;
     }
@@ -201,6 +206,8 @@ struct Call {
     double refine_cell[3];
     long long queue_voxels;
     cudaEvent_t fields_ready; // host-memory calls: recorded when the fields are on the device
+    double* const* host_fields; // host-memory calls: where the fields go back (the caller's arrays)
+    bool copied_out;          // run_device copied the fields back itself
     // a batch of cutouts (nbatch > 0): host arrays of grids and meshes (device pointers)
     int nbatch;
     const psib_grid* grids;
@@ -827,7 +834,42 @@ int run_device(Call& c)
             aa.fptr = d_fptr;
             // host-memory calls copy the fields in beside the first stages; only this one needs them
             if (c.fields_ready) CK(cudaStreamWaitEvent(st, c.fields_ready, 0));
-            CK(launch_apply_records(aa, st));
+            if (c.host_fields && k == nchunks - 1 && !batch && nruns >= 4 * NOUT) {
+                // The last chunk: apply the runs in NOUT slabs of voxels (runs are sorted by
+                // voxel) and copy each slab of every field to the host on the copy stream
+                // while the next slab is applied.
+                long long rb[NOUT + 1];
+                unsigned vb[NOUT + 1];
+                for (int p = 0; p <= NOUT; ++p) rb[p] = (long long)nruns * p / NOUT;
+                vb[0] = 0;
+                vb[NOUT] = (unsigned)nvox;
+                for (int p = 1; p < NOUT; ++p)
+                    CK(cudaMemcpyAsync(&vb[p], C.run_vox.as<unsigned>() + rb[p], sizeof(unsigned),
+                                       cudaMemcpyDeviceToHost, st));
+                CK(cudaStreamSynchronize(st));
+                static const int comps[6] = {1, 3, 3, 9, 9, 9};
+                for (int p = 0; p < NOUT; ++p) {
+                    ApplyArgs ap = aa;
+                    ap.run_vox = aa.run_vox + rb[p];
+                    ap.run_cnt = aa.run_cnt + rb[p];
+                    ap.run_off = aa.run_off + rb[p];
+                    ap.nruns = rb[p + 1] - rb[p];
+                    CK(launch_apply_records(ap, st));
+                    CK(cudaEventRecord(C.ev_out[p], st));
+                    CK(cudaStreamWaitEvent(C.copy, C.ev_out[p], 0));
+                    for (int f = 0; f < 6; ++f) {
+                        if (!c.F[f]) continue;
+                        const size_t o = (size_t)vb[p] * comps[f] * sizeof(double);
+                        const size_t n = (size_t)(vb[p + 1] - vb[p]) * comps[f] * sizeof(double);
+                        CK(cudaMemcpyAsync((char*)c.host_fields[f] + o, (const char*)c.F[f] + o, n,
+                                           cudaMemcpyDeviceToHost, C.copy));
+                    }
+                }
+                c.copied_out = true;
+                klaunch += NOUT - 1;
+            } else {
+                CK(launch_apply_records(aa, st));
+            }
             klaunch += 3; // iota, gather, apply
             CK(cudaEventRecord(C.ev[7], st));
             CK(cudaEventSynchronize(C.ev[7]));
@@ -1055,12 +1097,18 @@ int psib_voxels(const psib_grid* grid, const psib_mesh* mesh, int mode, double r
     }
     CK(cudaEventRecord(C->fields_in, C->copy));
     c.fields_ready = C->fields_in;
+    c.host_fields = grid->fields;
     if (mesh->nelem > 0) RET(run_device(c));
-    CK(cudaStreamWaitEvent(st, C->fields_in, 0));
-    for (int f = 0; f < 6; ++f) {
-        if (!grid->fields[f]) continue;
-        const size_t b = (size_t)nvox * comps[f] * sizeof(double);
-        CK(cudaMemcpyAsync(grid->fields[f], c.F[f], b, cudaMemcpyDeviceToHost, st));
+    if (c.copied_out) {
+        CK(cudaEventRecord(C->fields_in, C->copy)); // the last slab is on its way back
+        CK(cudaStreamWaitEvent(st, C->fields_in, 0));
+    } else {
+        CK(cudaStreamWaitEvent(st, C->fields_in, 0));
+        for (int f = 0; f < 6; ++f) {
+            if (!grid->fields[f]) continue;
+            const size_t b = (size_t)nvox * comps[f] * sizeof(double);
+            CK(cudaMemcpyAsync(grid->fields[f], c.F[f], b, cudaMemcpyDeviceToHost, st));
+        }
     }
     CK(cudaEventRecord(C->ev[7], st));
     CK(cudaEventSynchronize(C->ev[7]));
