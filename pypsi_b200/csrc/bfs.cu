@@ -135,11 +135,13 @@ __global__ void __launch_bounds__(BB) k_bfs_init(BfsArgs a)
     const int lane = threadIdx.x & 31;
     const long long warp = (long long)blockIdx.x * (BB / 32) + (threadIdx.x >> 5);
     const long long nwarp = (long long)gridDim.x * (BB / 32);
+    const unsigned long long p = *a.pass_idx;
+    const long long q0 = a.passes[p], q1 = a.passes[p + 1];
     unsigned st = 0;
     unsigned long long moved = 0;
-    for (long long base = a.q0 + warp * 32; base < a.q1; base += nwarp * 32) {
+    for (long long base = q0 + warp * 32; base < q1; base += nwarp * 32) {
         const long long i = base + lane;
-        const bool act = i < a.q1;
+        const bool act = i < q1;
         int t = 0;
         double p[4][3];
         int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
@@ -641,6 +643,14 @@ __global__ void k_bfs_finalize(BfsArgs a, long long nitems)
         if (a.c.scale[t] < 0.0) a.c.scale[t] = a.vsum[t] > 0.0 ? -a.c.scale[t] / a.vsum[t] : 1.0;
 }
 
+__global__ void k_bfs_advance(BfsArgs a) { ++*a.pass_idx; }
+
+cudaError_t launch_bfs_advance(const BfsArgs& a, cudaStream_t s)
+{
+    k_bfs_advance<<<1, 1, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_bfs_finalize(const BfsArgs& a, long long nitems, int num_sms, cudaStream_t s)
 {
     k_bfs_finalize<<<num_sms * 8, 256, 0, s>>>(a, nitems);
@@ -654,6 +664,8 @@ static constexpr size_t LEAF_SMEM = MAXV * BB * (sizeof(uint32_t) + 3 * sizeof(d
 
 // resident blocks per SM of each kernel (one full wave of grid-stride blocks)
 static int g_blocks[3] = {0, 0, 0};
+static void occupancy();
+void bfs_prepare() { occupancy(); }
 static void occupancy()
 {
     if (g_blocks[0]) return;

@@ -85,12 +85,21 @@ int ensure(DevBuf& b, size_t bytes)
     return PSIB_OK;
 }
 
+// The arguments a recorded breadth-first pass depends on.
+struct PassKey {
+    BfsArgs ba;
+    PolyQueue q[3];
+    unsigned long long* cq;
+    int grid;
+};
+
 struct Ctx {
     int device = -1;
     int num_sms = 0;
     cudaStream_t own = nullptr;  // stream of host-memory calls
     cudaStream_t copy = nullptr; // host-memory calls: the field copies, beside the first stages
     cudaEvent_t fields_in = nullptr;
+    cudaEvent_t enter = nullptr, leave = nullptr; // device-memory calls: fences with the caller's stream
     cudaEvent_t ev_out[NOUT] = {};
     cudaEvent_t ev[8] = {};
     // host-mode copies
@@ -106,6 +115,9 @@ struct Ctx {
     // breadth-first clip: three polyhedron queues, the volume histogram, per-level counters, window list
     DevBuf qx[3], qnb[3], qnv[3], qwin[3], qbox[3], qitem[3], hist, bfs_cnt, dfs_list, vsum;
     DevBuf btab, igrid; // batch tables, image -> cutout
+    DevBuf passes;      // breadth-first pass table
+    cudaGraphExec_t pass_exec = nullptr; // one breadth-first pass as a CUDA graph
+    PassKey pass_key{};                  // the arguments it was recorded with
     std::vector<DevBuf*> all()
     {
         return {&hpos, &hgpos, &hgmass, &hvel, &hmass, &hconn, &hfield[0], &hfield[1], &hfield[2], &hfield[3], &hfield[4],
@@ -114,7 +126,7 @@ struct Ctx {
                 &rkey_sorted, &rperm_in, &rperm, &rvox, &ritem, &rmom_sorted, &run_vox, &run_cnt, &run_off,
                 &qx[0], &qx[1], &qx[2], &qnb[0], &qnb[1], &qnb[2], &qnv[0], &qnv[1], &qnv[2], &qbox[0], &qbox[1],
                 &qbox[2], &qitem[0], &qitem[1], &qitem[2], &hist, &bfs_cnt, &dfs_list, &vsum, &qwin[0], &qwin[1],
-                &qwin[2], &btab, &igrid};
+                &qwin[2], &btab, &igrid, &passes};
     }
 };
 
@@ -132,6 +144,8 @@ int get_ctx(int dev, Ctx** out)
         CK(cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking));
         CK(cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking));
         CK(cudaEventCreateWithFlags(&c->fields_in, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&c->enter, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&c->leave, cudaEventDisableTiming));
         for (auto& e : c->ev_out) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         for (auto& e : c->ev) CK(cudaEventCreate(&e));
         g_ctx[dev] = c;
@@ -142,7 +156,7 @@ int get_ctx(int dev, Ctx** out)
 
 // small device block layout (unsigned long long words)
 enum { S_STATUS = 0, S_CNT = 1 /* 3 words */, S_TESS = 4 /* 2 */, S_HEAD = 8 /* 4 */, S_RECN = 12, S_NDEEP = 13,
-       S_DFS = 14, S_BYTES = 15, S_WORDS = 16 };
+       S_DFS = 14, S_BYTES = 15, S_PASS = 6, S_WORDS = 16 };
 
 // Histogram of the sorted footprint keys: lanes holding equal keys (most of a
 // warp, as the keys are sorted) add with one atomic.
@@ -234,8 +248,25 @@ int check_status(Call& c, unsigned long long* small_host)
 // the depth-first kernel.  Images are sorted by index-box volume, largest
 // first; a pass takes images while the sum of their box volumes -- a bound on
 // every queue of the pass -- stays within the queue capacity.
+// Device-memory calls run on the library's own non-blocking stream (a CUDA graph cannot be
+// recorded on the legacy default stream), after the work already queued on the caller's stream
+// and before anything the caller queues next.
+int enter_own_stream(Ctx& C, cudaStream_t user)
+{
+    CK(cudaEventRecord(C.enter, user));
+    CK(cudaStreamWaitEvent(C.own, C.enter, 0));
+    return PSIB_OK;
+}
+int leave_own_stream(Ctx& C, cudaStream_t user)
+{
+    CK(cudaEventRecord(C.leave, C.own));
+    CK(cudaStreamWaitEvent(user, C.leave, 0));
+    return PSIB_OK;
+}
+
 int bfs_clip(Ctx& C, ClipArgs& ca, long long nmain, long long nitems, unsigned long long* sm, int clip_grid,
-             int clip_block, long long queue_voxels, cudaStream_t st, long long& launches, long long& klaunch)
+             int clip_block, long long queue_voxels, bool batch, cudaStream_t st, long long& launches,
+             long long& klaunch)
 {
     RET(ensure(C.hist, 65536 * sizeof(unsigned)));
     CK(cudaMemsetAsync(C.hist.p, 0, 65536 * sizeof(unsigned), st));
@@ -330,32 +361,82 @@ int bfs_clip(Ctx& C, ClipArgs& ca, long long nmain, long long nitems, unsigned l
     ba.window_bfs = env_ll("PSIB_BFS_WINDOW", 1) != 0;
     RET(ensure(C.vsum, (size_t)std::max<long long>(nitems, 1) * sizeof(double)));
     ba.vsum = C.vsum.as<double>();
+    // the pass table on the device; a device counter picks the pass, so every pass runs
+    // the same launches
+    const long long npass = (long long)qb.size() - 1;
+    RET(ensure(C.passes, qb.size() * sizeof(long long)));
+    CK(cudaMemcpyAsync(C.passes.p, qb.data(), qb.size() * sizeof(long long), cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(&sm[S_PASS], 0, 8, st));
+    ba.passes = C.passes.as<long long>();
+    ba.pass_idx = &sm[S_PASS];
     const int grid = C.num_sms;
-    for (size_t p = 0; p + 1 < qb.size(); ++p) {
-        CK(cudaMemsetAsync(cq, 0, NCNT * sizeof(unsigned long long), st));
-        ba.q0 = qb[p];
-        ba.q1 = qb[p + 1];
-        ba.out = Q[0];
-        ba.out.count = &cq[0];
-        ba.leaf = Q[2];
-        ba.leaf.count = &cl[0];
-        CK(launch_bfs_init(ba, grid, st));
-        CK(launch_bfs_leaf(ba, grid, st));
+    bfs_prepare();
+    // One pass: reset the per-level counts, then init, leaf, and NLEV x (level, leaf), then
+    // advance the pass counter.  Batches record it once as a CUDA graph and replay it for every
+    // pass (and in later calls whose arguments are the same); plain launches if the graph cannot
+    // be made.  Single calls launch directly: measured at 128^3 -> 256^3 the replay was 3 %
+    // slower, and for 512 cutouts no faster (PSIB_BFS_GRAPH=0/1 overrides).
+    auto pass = [&](cudaStream_t s) -> cudaError_t {
+        cudaError_t e = cudaMemsetAsync(cq, 0, NCNT * sizeof(unsigned long long), s);
+        BfsArgs b = ba;
+        b.out = Q[0];
+        b.out.count = &cq[0];
+        b.leaf = Q[2];
+        b.leaf.count = &cl[0];
+        if (e == cudaSuccess) e = launch_bfs_init(b, grid, s);
+        if (e == cudaSuccess) e = launch_bfs_leaf(b, grid, s);
         int ia = 0;
-        for (int lvl = 0; lvl < NLEV; ++lvl) {
-            ba.in = Q[ia];
-            ba.in.count = &cq[lvl];
-            ba.out = Q[1 - ia];
-            ba.out.count = &cq[lvl + 1];
-            ba.leaf.count = &cl[lvl + 1];
-            ba.last = lvl == NLEV - 1;
-            CK(launch_bfs_level(ba, grid, st));
-            CK(launch_bfs_leaf(ba, grid, st));
+        for (int lvl = 0; lvl < NLEV && e == cudaSuccess; ++lvl) {
+            b.in = Q[ia];
+            b.in.count = &cq[lvl];
+            b.out = Q[1 - ia];
+            b.out.count = &cq[lvl + 1];
+            b.leaf.count = &cl[lvl + 1];
+            b.last = lvl == NLEV - 1;
+            e = launch_bfs_level(b, grid, s);
+            if (e == cudaSuccess) e = launch_bfs_leaf(b, grid, s);
             ia = 1 - ia;
         }
-        klaunch += 2 + 2 * NLEV;
-        launches += 2 + 2 * NLEV;
+        if (e == cudaSuccess) e = launch_bfs_advance(b, s);
+        return e;
+    };
+    bool graphed = false;
+    if (env_ll("PSIB_BFS_GRAPH", batch ? 1 : 0) != 0) {
+        PassKey key{};
+        key.ba = ba;
+        key.ba.c.n = 0; // depth-first fields the walk does not read
+        key.ba.c.order_base = 0;
+        key.ba.c.head = nullptr;
+        key.ba.c.scratch = nullptr;
+        for (int i = 0; i < 3; ++i) key.q[i] = Q[i];
+        key.cq = cq;
+        key.grid = grid;
+        if (!C.pass_exec || memcmp(&key, &C.pass_key, sizeof(key)) != 0) {
+            if (C.pass_exec) cudaGraphExecDestroy(C.pass_exec);
+            C.pass_exec = nullptr;
+            cudaGraph_t gph = nullptr;
+            if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+                const cudaError_t e = pass(st);
+                const cudaError_t e2 = cudaStreamEndCapture(st, &gph);
+                if (e == cudaSuccess && e2 == cudaSuccess && gph &&
+                    cudaGraphInstantiate(&C.pass_exec, gph, 0) == cudaSuccess) {
+                    C.pass_key = key;
+                } else {
+                    C.pass_exec = nullptr;
+                }
+                if (gph) cudaGraphDestroy(gph);
+            }
+            cudaGetLastError(); // a failed capture falls back to plain launches
+        }
+        if (C.pass_exec) {
+            for (long long p = 0; p < npass; ++p) CK(cudaGraphLaunch(C.pass_exec, st));
+            graphed = true;
+        }
     }
+    if (!graphed)
+        for (long long p = 0; p < npass; ++p) CK(pass(st));
+    klaunch += (3 + 2 * NLEV) * npass;
+    launches += (2 + 2 * NLEV) * npass;
     CK(launch_bfs_finalize(ba, nitems, C.num_sms, st));
     klaunch++;
     unsigned long long ndfs = 0;
@@ -720,7 +801,7 @@ int run_device(Call& c)
             CK(cudaEventRecord(C.ev[4], st));
             if (nmain > 0 && use_bfs) {
                 ca.scratch = C.scratch.p;
-                RET(bfs_clip(C, ca, nmain, nitems, sm, clip_grid, clip_block, c.queue_voxels, st, launches,
+                RET(bfs_clip(C, ca, nmain, nitems, sm, clip_grid, clip_block, c.queue_voxels, batch, st, launches,
                              klaunch));
             } else if (nmain > 0) {
                 ca.scratch = C.scratch.p;
@@ -1013,6 +1094,8 @@ int psib_release_device_memory(void)
     std::lock_guard<std::mutex> lk(g_mu);
     if (dev >= 0 && dev < 64 && g_ctx[dev]) {
         CK(cudaDeviceSynchronize());
+        if (g_ctx[dev]->pass_exec) cudaGraphExecDestroy(g_ctx[dev]->pass_exec); // it refers to the buffers
+        g_ctx[dev]->pass_exec = nullptr;
         for (DevBuf* b : g_ctx[dev]->all()) {
             if (b->p) cudaFree(b->p);
             b->p = nullptr;
@@ -1065,14 +1148,17 @@ int psib_voxels(const psib_grid* grid, const psib_mesh* mesh, int mode, double r
     const long long nvox = (long long)grid->n[0] * grid->n[1] * grid->n[2];
     static const int comps[6] = {1, 3, 3, 9, 9, 9};
     if (o.memory == PSIB_DEVICE) {
-        c.st = (cudaStream_t)o.stream;
+        RET(enter_own_stream(*C, (cudaStream_t)o.stream));
+        c.st = C->own;
         for (int f = 0; f < 6; ++f) c.F[f] = grid->fields[f];
         c.pos = mesh->pos;
         c.vel = mesh->vel;
         c.mass = mesh->mass;
         c.conn = mesh->connectivity;
         CK(cudaEventRecord(C->ev[0], c.st));
-        RET(run_device(c));
+        const int r = run_device(c);
+        RET(leave_own_stream(*C, (cudaStream_t)o.stream));
+        RET(r);
         if (o.stats) {
             CK(cudaEventRecord(C->ev[7], c.st));
             CK(cudaEventSynchronize(C->ev[7]));
@@ -1166,15 +1252,18 @@ int psib_voxels_batch(const psib_grid* grids, const psib_mesh* meshes, int nbatc
     c.C = C;
     c.stats = o.stats;
     if (o.stats) *o.stats = psib_stats{};
-    c.st = (cudaStream_t)o.stream;
     for (int f = 0; f < 6; ++f) c.F[f] = grids[0].fields[f];
     c.pos = meshes[0].pos;
     c.vel = meshes[0].vel;
     c.mass = meshes[0].mass;
     c.conn = meshes[0].connectivity;
     if (nelem == 0) return PSIB_OK;
+    RET(enter_own_stream(*C, (cudaStream_t)o.stream));
+    c.st = C->own;
     CK(cudaEventRecord(C->ev[0], c.st));
-    RET(run_device(c));
+    const int r = run_device(c);
+    RET(leave_own_stream(*C, (cudaStream_t)o.stream));
+    RET(r);
     if (o.stats) {
         CK(cudaEventRecord(C->ev[7], c.st));
         CK(cudaEventSynchronize(C->ev[7]));

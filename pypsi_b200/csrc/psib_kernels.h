@@ -132,7 +132,8 @@ struct PolyQueue {
 struct BfsArgs {
     ClipArgs c;               // frames, queue order, grid, records, status, counters, scale
     PolyQueue in, out, leaf;  // level: in -> out and leaf; init: -> out and leaf; leaf kernel: leaf
-    long long q0, q1;         // init: queue positions of this pass
+    const long long *passes;  // init: queue positions of pass p are [passes[p], passes[p + 1])
+    unsigned long long *pass_idx; // the current pass (advanced by launch_bfs_advance)
     int *dfs_list;            // init: images that need the window clip (depth-first kernel)
     unsigned long long *dfs_count;
     int last;                 // level: the last level, which must leave no polyhedron unfinished
@@ -146,6 +147,9 @@ cudaError_t launch_bfs_init(const BfsArgs &a, int num_sms, cudaStream_t s);
 cudaError_t launch_bfs_level(const BfsArgs &a, int num_sms, cudaStream_t s);
 cudaError_t launch_bfs_leaf(const BfsArgs &a, int num_sms, cudaStream_t s);
 cudaError_t launch_bfs_finalize(const BfsArgs &a, long long nitems, int num_sms, cudaStream_t s);
+cudaError_t launch_bfs_advance(const BfsArgs &a, cudaStream_t s);
+// kernel attributes and occupancy, queried once before any launch or stream capture
+void bfs_prepare();
 
 cudaError_t launch_tess_count(const TessArgs &a, cudaStream_t s);
 cudaError_t launch_tess_emit(const TessArgs &a, cudaStream_t s);

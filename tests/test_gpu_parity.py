@@ -233,3 +233,21 @@ def test_full_size_properties(gpu):
         outs[prec] = {k: np.array(v) for k, v in grid.fields.items()}
         del grid
     check_vs_exact_and_reference(outs["mixed"], outs["fp64"], outs["fp64-central"], MIXED_TOL, "full")
+
+
+def test_config1_size_bitwise_against_compiled_reference(gpu, oracle):
+    """The reference's CPU-runnable workload at its own size: 32^3 particles
+    (rms 0.3 cells) onto a 64^3 grid, density only, against the reference's C
+    code compiled from its sources -- bit for bit in FP64, 1e-5 in mixed."""
+    from pypsi_b200.synth import zeldovich
+
+    pos, vel = zeldovich(32, 0.3, 2031)
+    c = {"kind": "block", "pos": pos, "vel": vel, "mass": None, "periodic_box": ((0.0,) * 3, (100.0,) * 3),
+         "n": (64, 64, 64), "bounds": ((0.0,) * 3, (100.0,) * 3), "fields": [], "reftol": 1.0, "maxlvl": 0}
+    kind = "reference" if oracle.available("reference") else "restatement"
+    ref = run_oracle(oracle, c, kind=kind)
+    out, _, _ = run_psi(gpu, c, precision="fp64")
+    assert np.array_equal(out["m"], ref["m"])
+    out, _, _ = run_psi(gpu, c, precision="mixed")
+    check(field_errors(out, ref), MIXED_TOL, "config 1")
+    assert mass_error(out["m"], 32 ** 3) <= MASS_TOL
