@@ -593,6 +593,8 @@ int run_device(Call& c)
     TessArgs ta = {};
     ta.m = md;
     ta.nbatch = batch ? c.nbatch : 0;
+    ta.quad = m.elemtype == 27;
+    for (int b = 0; batch && b < c.nbatch; ++b) ta.quad |= c.meshes[b].elemtype == 27;
     ta.meshes = d_meshes;
     ta.grids = d_grids;
     ta.eoff = d_eoff;
@@ -1028,8 +1030,8 @@ int validate(const psib_grid* g, const psib_mesh* m, int mode, const psib_option
     if (g->fields[PSIB_XV] && !(g->fields[PSIB_X] && g->fields[PSIB_V]))
         return fail(PSIB_ERR_ARG, "field 'xv' requires fields 'x' and 'v'");
     if (g->fields[PSIB_VV] && !g->fields[PSIB_V]) return fail(PSIB_ERR_ARG, "field 'vv' requires field 'v'");
-    if (m->elemtype == 27) return fail(PSIB_ERR_UNSUPPORTED, "triquadratic elements are not implemented");
-    if (m->elemtype != 4 && m->elemtype != 8) return fail(PSIB_ERR_ARG, "elemtype must be 4 or 8");
+    if (m->elemtype != 4 && m->elemtype != 8 && m->elemtype != 27)
+        return fail(PSIB_ERR_ARG, "elemtype must be 4, 8 or 27");
     if (m->nelem < 0 || m->npart < 0) return fail(PSIB_ERR_ARG, "negative mesh size");
     if (m->nelem >= (1ll << 31) || m->npart >= (1ll << 31))
         return fail(PSIB_ERR_ARG, "meshes of 2^31 elements or particles are not supported");
@@ -1287,6 +1289,7 @@ int psib_voxels_adjoint(const psib_grid* grad, const psib_mesh* mesh, double ref
             return fail(PSIB_ERR_UNSUPPORTED, "the adjoint takes the gradient of field m only");
     if (refine_max_lvl > 0 && mesh->elemtype == 8)
         return fail(PSIB_ERR_UNSUPPORTED, "the adjoint supports refine_max_lvl = 0 only");
+    if (mesh->elemtype == 27) return fail(PSIB_ERR_UNSUPPORTED, "the adjoint supports 4- and 8-node elements");
     if (!grad_pos && mesh->nelem > 0) return fail(PSIB_ERR_ARG, "grad_pos is required");
     (void)grad_vel; // the density does not depend on the velocities
     if (psib_device_count() <= 0) return fail(PSIB_ERR_NODEVICE, "no CUDA device is visible");

@@ -584,11 +584,6 @@ static PyObject *PSI_voxels(PyObject *self, PyObject *args, PyObject *kwds)
         PyErr_Format(PyExc_ValueError, "Invalid precision for PSI.voxels(): %s", precstr);
         return NULL;
     }
-    if (mesh->elemtype == 27) {
-        PyErr_SetString(PyExc_NotImplementedError, "triquadratic elements are not provided by this build");
-        return NULL;
-    }
-
     psib_grid g;
     memset(&g, 0, sizeof(g));
     for (int i = 0; i < 3; ++i) {

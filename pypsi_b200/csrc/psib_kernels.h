@@ -83,6 +83,7 @@ struct TessArgs {
     GridDev g;
     long long e0, e1;          // element range
     int max_lvl;
+    int quad;                  // some element is triquadratic (27 nodes): the kernel variant that holds them
     int refine_mode;           // 0: the reference's midpoint test (m.ptol2); 1: stretch beyond `stretch` x m.lag
     double stretch;
     // a batch of cutouts (nbatch > 0): element E belongs to cutout b with

@@ -18,6 +18,13 @@ __constant__ int c_tet_corners[6][4] = {{1, 0, 2, 4}, {3, 1, 2, 4}, {3, 5, 1, 4}
 __constant__ int c_ref_edges[7][3] = {{2, 4, 6}, {2, 10, 18}, {6, 12, 18}, {8, 13, 18},
                                       {8, 14, 20}, {8, 16, 24}, {20, 22, 24}};
 
+// Edges (end, midpoint, end) of the tets of a 27-node cube whose midpoint deviation
+// drives the refinement of a triquadratic element (src/refine.c:157-161).
+__constant__ int c_quad_edges[19][3] = {{0, 1, 2},    {0, 3, 6},    {0, 9, 18},   {2, 4, 6},    {2, 5, 8},
+                                        {2, 10, 18},  {2, 11, 20},  {6, 7, 8},    {6, 12, 18},  {6, 15, 24},
+                                        {8, 13, 18},  {8, 14, 20},  {8, 16, 24},  {8, 17, 26},  {18, 19, 20},
+                                        {18, 21, 24}, {20, 22, 24}, {20, 23, 26}, {24, 25, 26}};
+
 constexpr int MAX_REFINE = 6; // src/refine.c:89-92
 
 __device__ __forceinline__ int I2(int a, int b, int c) { return 4 * a + 2 * b + c; }
@@ -309,12 +316,112 @@ __device__ void refine_element(Emitter& em, const double (*cp)[3], const double 
     }
 }
 
-template <bool REFINE>
+// Triquadratic interpolation of a 27-node cube onto the 125 nodes of its
+// half-size lattice (src/refine.c:321-345), one node at a time: node (A,B,C)
+// of the 5-lattice (A,B,C in 0..4).  The reference fills the lattice in three
+// sweeps -- x on the even y,z planes, then y on the even z planes, then z --
+// each new node 0.125 (3 n_near + 6 n_mid - n_far) of the three nodes before it
+// on its line; these functions evaluate the same expressions on the same
+// operands, so every node has the reference's value bit for bit.
+__device__ __forceinline__ double quad_line(int a, double n0, double n2, double n4)
+{
+    return a == 1 ? 0.125 * (3.0 * n0 + 6.0 * n2 - n4) : 0.125 * (3.0 * n4 + 6.0 * n2 - n0);
+}
+__device__ double quad_x(const double (*in)[3], int A, int B, int C, int ax) // B, C even
+{
+    if (!(A & 1)) return in[I3(A >> 1, B >> 1, C >> 1)][ax];
+    return quad_line(A, in[I3(0, B >> 1, C >> 1)][ax], in[I3(1, B >> 1, C >> 1)][ax], in[I3(2, B >> 1, C >> 1)][ax]);
+}
+__device__ double quad_y(const double (*in)[3], int A, int B, int C, int ax) // C even
+{
+    if (!(B & 1)) return quad_x(in, A, B, C, ax);
+    return quad_line(B, quad_x(in, A, 0, C, ax), quad_x(in, A, 2, C, ax), quad_x(in, A, 4, C, ax));
+}
+__device__ double quad_node(const double (*in)[3], int A, int B, int C, int ax)
+{
+    if (!(C & 1)) return quad_y(in, A, B, C, ax);
+    return quad_line(C, quad_y(in, A, B, 0, ax), quad_y(in, A, B, 2, ax), quad_y(in, A, B, 4, ax));
+}
+
+// Adaptive refinement of a triquadratic element, depth first in the reference's
+// child order (src/refine.c:152-221): a cube is cut into 8 when the midpoint of
+// one of its 19 tet edges deviates from the straight edge by more than the
+// tolerance; child (i,j,k) takes nodes (2i..2i+2, ...) of the parent's
+// 125-node interpolation; a leaf gives the 6 tets of its corner nodes
+// (src/refine.c:299-319).
+__device__ void refine_element_quad(Emitter& em, const double (*cp)[3], const double (*cu)[3], double mass,
+                                    long long e, int max_lvl, double ptol2, int mode, double T, const double* lag,
+                                    RefNode* L)
+{
+    for (int n = 0; n < 27; ++n)
+        for (int i = 0; i < 3; ++i) {
+            L[0].p[n][i] = cp[n][i];
+            L[0].u[n][i] = cu[n][i];
+        }
+    L[0].mass = mass;
+    L[0].child = -1;
+    int d = 0;
+    while (d >= 0) {
+        RefNode& N = L[d];
+        if (N.child < 0) {
+            bool refine = false;
+            if (d < max_lvl && mode == 1) refine = stretch_refine(N.p, d, T, lag);
+            else if (d < max_lvl)
+                for (int k = 0; k < 19 && !refine; ++k) {
+                    double err2 = 0.0;
+                    for (int i = 0; i < 3; ++i) {
+                        const double mt = 0.5 * (N.p[c_quad_edges[k][0]][i] + N.p[c_quad_edges[k][2]][i]);
+                        const double mq = N.p[c_quad_edges[k][1]][i];
+                        err2 += (mt - mq) * (mt - mq);
+                    }
+                    refine = err2 > ptol2;
+                }
+            if (!refine) {
+                for (int t = 0; t < 6; ++t) {
+                    double tp[4][3], tu[4][3];
+                    for (int v = 0; v < 4; ++v)
+                        for (int i = 0; i < 3; ++i) {
+                            tp[v][i] = N.p[c_tet_nodes[t][v]][i];
+                            tu[v][i] = N.u[c_tet_nodes[t][v]][i];
+                        }
+                    em.tet(tp, tu, N.mass * (1.0 / 6), e, nullptr);
+                }
+                d--;
+                continue;
+            }
+            N.child = 0;
+        }
+        if (N.child < 8) {
+            const int c = N.child++;
+            const int ci = c >> 2, cj = (c >> 1) & 1, ck = c & 1;
+            RefNode& K = L[d + 1];
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b)
+                    for (int cc = 0; cc < 3; ++cc)
+                        for (int i = 0; i < 3; ++i) {
+                            K.p[I3(a, b, cc)][i] = quad_node(N.p, a + 2 * ci, b + 2 * cj, cc + 2 * ck, i);
+                            K.u[I3(a, b, cc)][i] = quad_node(N.u, a + 2 * ci, b + 2 * cj, cc + 2 * ck, i);
+                        }
+            K.mass = 0.125 * N.mass;
+            K.child = -1;
+            d++;
+        } else {
+            d--;
+        }
+    }
+}
+
+template <bool REFINE, bool QUAD>
 __device__ int element_items(const TessArgs& a, const MeshDev& m, const GridDev& g, int gid, bool write, long long e,
                              long long pos, unsigned long long& tets, RefNode* L)
 {
-    double p[8][3], u[8][3];
-    int ids[8];
+    constexpr int NV = QUAD ? 27 : 8; // vertices an element may have
+    double p[NV][3], u[NV][3];
+    int ids[NV];
+    if (!QUAD && m.elemtype == 27) {
+        atomicOr(a.status, ST_INDEX); // launched without the triquadratic variant
+        return 0;
+    }
     if (!gather(m, e, p, u, ids)) {
         atomicOr(a.status, ST_INDEX);
         return 0;
@@ -325,6 +432,10 @@ __device__ int element_items(const TessArgs& a, const MeshDev& m, const GridDev&
     Emitter em{a, m, g, gid, write, pos, 0, 0};
     if (et == 4) {
         em.tet(p, u, me, e, ids); // a simplex element is one tet (src/refine.c:60-66)
+    } else if (QUAD && et == 27) {
+        if constexpr (QUAD)
+            refine_element_quad(em, p, u, me, e, REFINE ? a.max_lvl : 0, m.ptol2, a.refine_mode, a.stretch, m.lag,
+                                L);
     } else if (!REFINE) {
         for (int t = 0; t < 6; ++t) {
             double tp[4][3], tu[4][3];
@@ -346,12 +457,12 @@ __device__ int element_items(const TessArgs& a, const MeshDev& m, const GridDev&
     return em.n;
 }
 
-template <bool REFINE, bool EMIT>
+template <bool REFINE, bool EMIT, bool QUAD>
 __global__ void __launch_bounds__(128) k_tess(TessArgs a)
 {
     RefNode* L = nullptr;
-    RefNode Lbuf[REFINE ? MAX_REFINE + 1 : 1];
-    if constexpr (REFINE) L = Lbuf;
+    RefNode Lbuf[(REFINE || QUAD) ? MAX_REFINE + 1 : 1];
+    if constexpr (REFINE || QUAD) L = Lbuf;
     unsigned long long kept = 0, tets = 0;
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long e = a.e0 + blockIdx.x * (long long)blockDim.x + threadIdx.x; e < a.e1; e += stride) {
@@ -365,9 +476,9 @@ __global__ void __launch_bounds__(128) k_tess(TessArgs a)
                 if (a.eoff[mid] <= e) lo = mid;
                 else hi = mid;
             }
-            n = element_items<REFINE>(a, a.meshes[lo], a.grids[lo], lo, EMIT, e - a.eoff[lo], pos, tets, L);
+            n = element_items<REFINE, QUAD>(a, a.meshes[lo], a.grids[lo], lo, EMIT, e - a.eoff[lo], pos, tets, L);
         } else {
-            n = element_items<REFINE>(a, a.m, a.g, 0, EMIT, e, pos, tets, L);
+            n = element_items<REFINE, QUAD>(a, a.m, a.g, 0, EMIT, e, pos, tets, L);
         }
         if (!EMIT) a.count[e - a.e0] = n;
         kept += (n > 0);
@@ -384,23 +495,29 @@ static int tess_grid(long long n)
     return (int)(b < 148 * 16 ? (b < 1 ? 1 : b) : 148 * 16);
 }
 
-cudaError_t launch_tess_count(const TessArgs& a, cudaStream_t s)
+template <bool EMIT>
+static void launch_tess(const TessArgs& a, cudaStream_t s)
 {
     const int g = tess_grid(a.e1 - a.e0);
-    if (a.max_lvl > 0 && (a.nbatch || a.m.elemtype == 8))
-        k_tess<true, false><<<g, 128, 0, s>>>(a);
-    else
-        k_tess<false, false><<<g, 128, 0, s>>>(a);
+    const bool refine = a.max_lvl > 0 && (a.nbatch || a.m.elemtype != 4);
+    if (a.quad) {
+        if (refine) k_tess<true, EMIT, true><<<g, 128, 0, s>>>(a);
+        else k_tess<false, EMIT, true><<<g, 128, 0, s>>>(a);
+    } else {
+        if (refine) k_tess<true, EMIT, false><<<g, 128, 0, s>>>(a);
+        else k_tess<false, EMIT, false><<<g, 128, 0, s>>>(a);
+    }
+}
+
+cudaError_t launch_tess_count(const TessArgs& a, cudaStream_t s)
+{
+    launch_tess<false>(a, s);
     return cudaGetLastError();
 }
 
 cudaError_t launch_tess_emit(const TessArgs& a, cudaStream_t s)
 {
-    const int g = tess_grid(a.e1 - a.e0);
-    if (a.max_lvl > 0 && (a.nbatch || a.m.elemtype == 8))
-        k_tess<true, true><<<g, 128, 0, s>>>(a);
-    else
-        k_tess<false, true><<<g, 128, 0, s>>>(a);
+    launch_tess<true>(a, s);
     return cudaGetLastError();
 }
 
