@@ -209,6 +209,26 @@ int psib_release_device_memory(void);
 int psib_voxels_density_noalloc(const psib_grid *grid, const double *tet_pos, const double *tet_mass,
                                 long long ntets, void *stream);
 
+/* Snapshot readers: a Gadget-2 (format 1) file as the periodic trilinear mesh
+ * of PSI.Mesh(loader='gadget2') (src/mesh.c:35-160) or, with 64-bit particle
+ * IDs and particles numbered in tiles of 4^3, loader='gevolution'
+ * (src/mesh.c:163-302); src/PSI.c:659-709 is the caller they replace.
+ *
+ * psib_peek_gadget2 reads the header: the number of type-1 particles (also
+ * the number of elements) and the box size; the box is [0, box_size]^3.
+ * psib_load_* fill pos and vel (npart x 3 doubles, particle p at row ID[p]),
+ * mass (npart doubles, each header.mass[1] / npart) and connectivity
+ * (npart x 8 ints, elements of 8 nodes); npart must equal the header's count.
+ * Host memory only; no device is needed.  A file whose IDs are not a
+ * permutation of 0..npart-1 fails with PSIB_ERR_INDEX; one whose particles do
+ * not form a cubic lattice (gevolution: of a side that is a multiple of 4),
+ * or whose block lengths disagree with npart, with PSIB_ERR_ARG. */
+int psib_peek_gadget2(const char *filename, long long *npart, double *box_size);
+int psib_load_gadget2(const char *filename, long long npart, double *pos, double *vel, double *mass,
+                      int *connectivity);
+int psib_load_gevolution(const char *filename, long long npart, double *pos, double *vel, double *mass,
+                         int *connectivity);
+
 #ifdef __cplusplus
 }
 #endif

@@ -222,3 +222,83 @@ def block_connectivity(nside, periodic):
                 conn[..., 4 * ii + 2 * jj + kk] = (ny * nz * ((i + ii) % nx) + nz * ((j + jj) % ny)
                                                    + ((k + kk) % nz))
     return conn.reshape(-1, 8)
+
+
+# ---- snapshot loaders (src/mesh.c:35-302) ----
+def _gevolution_tile_tables():
+    """The 4^3-tile numbering of src/mesh.c:166-168, rebuilt: slot s of a tile
+    holds the particle at 2*G(s // 8) + G(s % 8), G the 3-bit reflected Gray
+    code read as (i, j, k) bits, most significant first.  Returns
+    (slot -> (i,j,k), [i,j,k] -> slot)."""
+    def g3(v):
+        gv = v ^ (v >> 1)
+        return np.array([(gv >> 2) & 1, (gv >> 1) & 1, gv & 1])
+
+    to_cube = np.array([2 * g3(s // 8) + g3(s % 8) for s in range(64)], dtype=np.int64)
+    to_flat = np.full((4, 4, 4), -1, dtype=np.int64)
+    for s in range(64):
+        to_flat[tuple(to_cube[s])] = s
+    assert (to_flat >= 0).all()
+    return to_cube, to_flat
+
+
+def load_snapshot(kind, path, flavour="gadget2"):
+    """pos, vel (npart,3), mass (npart,), connectivity (npart,8) int32 and the
+    box size of a Gadget-2 format-1 snapshot, as PSI.Mesh(loader=flavour) reads
+    it.  kind 'restatement': numpy, following src/mesh.c:64-160 ('gadget2') and
+    :163-302 ('gevolution'); kind 'reference': the reference's own
+    peek_gadget2 + load_gadget2 / load_gevolution from _ref/libpsiref.so."""
+    if kind == "reference":
+        lib = _lib("reference")
+        m = _PsiMesh()
+        with _quiet_stdout():
+            ok = lib.peek_gadget2(C.byref(m), path.encode())
+        if not ok:
+            raise ValueError("peek_gadget2 failed")
+        npart = m.npart
+        pos, vel = np.zeros((npart, 3)), np.zeros((npart, 3))
+        mass, conn = np.zeros(npart), np.zeros((npart, 8), dtype=np.int32)
+        m.pos, m.vel, m.mass = _dp(pos), _dp(vel), _dp(mass)
+        m.connectivity = conn.ctypes.data_as(C.POINTER(C.c_int))
+        fn = lib.load_gadget2 if flavour == "gadget2" else lib.load_gevolution
+        with _quiet_stdout():
+            ok = fn(C.byref(m), path.encode())
+        if not ok:
+            raise ValueError(f"{fn.__name__} failed")
+        return pos, vel, mass, conn, m.box[1][0]
+    raw = open(path, "rb").read()
+    hdr = raw[4:260]
+    npart = int(np.frombuffer(hdr, np.int32, 6, 0)[1])
+    mass1 = float(np.frombuffer(hdr, np.float64, 6, 24)[1])
+    box = float(np.frombuffer(hdr, np.float64, 1, 128)[0])
+    at = 264 + 4
+    tpos = np.frombuffer(raw, np.float32, 3 * npart, at).reshape(npart, 3)
+    at += 12 * npart + 8
+    tvel = np.frombuffer(raw, np.float32, 3 * npart, at).reshape(npart, 3)
+    at += 12 * npart + 8
+    idt = np.int32 if flavour == "gadget2" else np.int64
+    tid = np.frombuffer(raw, idt, npart, at).astype(np.int64)
+    pos, vel = np.zeros((npart, 3)), np.zeros((npart, 3))
+    pos[tid] = tpos
+    vel[tid] = tvel
+    mass = np.full(npart, mass1 / npart)
+    nside = int(np.floor((npart + 0.5) ** (1.0 / 3.0)))
+    if flavour == "gadget2":
+        conn = block_connectivity((nside,) * 3, True)
+    else:
+        to_cube, to_flat = _gevolution_tile_tables()
+        tn = nside // 4
+        p = np.arange(npart)
+        t = p // 64
+        tile = np.stack([t % tn, (t // tn) % tn, t // (tn * tn)], axis=1)
+        cube = to_cube[p % 64]
+        conn = np.empty((npart, 8), dtype=np.int32)
+        for ii in range(2):
+            for jj in range(2):
+                for kk in range(2):
+                    q = cube + np.array([ii, jj, kk])
+                    dt, q = q // 4, q % 4
+                    tt = (tile + dt) % tn
+                    flat = tt[:, 0] + tn * tt[:, 1] + tn * tn * tt[:, 2]
+                    conn[:, 4 * ii + 2 * jj + kk] = 64 * flat + to_flat[q[:, 0], q[:, 1], q[:, 2]]
+    return pos, vel, mass, conn, box

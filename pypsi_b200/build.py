@@ -31,6 +31,7 @@ CUDA_UNITS = {  # unit -> extra flags
     "pipeline.cu": ["--fmad=false"],
     "noalloc.cu": ["--fmad=false"],
     "bfs.cu": [],
+    "loaders.cpp": [],  # host code only: the snapshot readers
 }
 HEADERS = ["psib_device.cuh", "psib_clip.cuh", "psib_kernels.h"]
 
@@ -58,7 +59,7 @@ def build(force: bool = False, verbose: bool = False) -> None:
     objs = []
     for unit, extra in CUDA_UNITS.items():
         src = os.path.join(CSRC, unit)
-        obj = os.path.join(BUILD, unit.replace(".cu", ".o"))
+        obj = os.path.join(BUILD, os.path.splitext(unit)[0] + ".o")
         objs.append(obj)
         if force or _newer(obj, [src, __file__] + hdrs):
             _run([NVCC, "-std=c++17", "-O3", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC", "-I", INCLUDE, "-I", CSRC,

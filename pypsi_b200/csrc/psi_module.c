@@ -11,7 +11,8 @@
  * precision='fp64'|'mixed' and deterministic=False of voxels(), and
  * PSI.last_stats() / PSI.device_count().
  *
- * Not provided here: the 'gadget2' / 'gevolution' file loaders, annihilation
+ * The 'gadget2' / 'gevolution' loaders read snapshots through
+ * psib_load_gadget2 / psib_load_gevolution.  Not provided here: annihilation
  * mode, PSI.RStarTree and PSI.VDF (other paths of the reference).
  */
 #define PY_SSIZE_T_CLEAN
@@ -471,8 +472,48 @@ static int Mesh_init(Mesh *self, PyObject *args, PyObject *kwds)
                 }
         swap_ref(&self->connectivity, c);
     } else if (strcmp(cloader, "gadget2") == 0 || strcmp(cloader, "gevolution") == 0) {
-        PyErr_Format(PyExc_NotImplementedError, "The %s loader is not provided by this build", cloader);
-        return -1;
+        /* src/PSI.c:659-709: peek at the header, allocate, then load */
+        long long np = 0;
+        double boxsize = 0.0;
+        if (!cfile || psib_peek_gadget2(cfile, &np, &boxsize) != PSIB_OK || np < 0) {
+            PyErr_Format(PyExc_ValueError, "Bad file name: %s", cfile ? cfile : "(none)");
+            return -1;
+        }
+        nd[0] = (npy_intp)np;
+        nd[1] = 3;
+        PyObject *p = PyArray_SimpleNew(2, nd, NPY_FLOAT64);
+        if (!p) return -1;
+        swap_ref(&self->pos, p);
+        PyObject *v = PyArray_SimpleNew(2, nd, NPY_FLOAT64);
+        if (!v) return -1;
+        swap_ref(&self->vel, v);
+        PyObject *m = PyArray_SimpleNew(1, nd, NPY_FLOAT64);
+        if (!m) return -1;
+        swap_ref(&self->mass, m);
+        nd[1] = 8;
+        PyObject *c = PyArray_SimpleNew(2, nd, NPY_INT32);
+        if (!c) return -1;
+        swap_ref(&self->connectivity, c);
+        int rc;
+        double *pp = (double *)PyArray_DATA((PyArrayObject *)p), *vp = (double *)PyArray_DATA((PyArrayObject *)v);
+        double *mp = (double *)PyArray_DATA((PyArrayObject *)m);
+        int *cp = (int *)PyArray_DATA((PyArrayObject *)c);
+        Py_BEGIN_ALLOW_THREADS rc = strcmp(cloader, "gadget2") == 0 ? psib_load_gadget2(cfile, np, pp, vp, mp, cp)
+                                                                   : psib_load_gevolution(cfile, np, pp, vp, mp, cp);
+        Py_END_ALLOW_THREADS if (rc != PSIB_OK) {
+            PyErr_Format(PyExc_ValueError, "Could not read %s: %s", cfile, psib_last_error());
+            return -1;
+        }
+        self->block = 0;
+        self->dim = 3;
+        self->elemtype = 8;
+        self->npart = np;
+        self->nelem = np;
+        self->periodic = 1;
+        for (int i = 0; i < 3; ++i) {
+            self->box[0][i] = 0.0;
+            self->box[1][i] = boxsize;
+        }
     } else {
         PyErr_SetString(PyExc_ValueError, "Invalid mesh loader.");
         return -1;
