@@ -45,7 +45,8 @@ extern "C" {
 
 /* deposit mode, as include/psi.h:69-70 */
 #define PSIB_MODE_DENSITY 0
-#define PSIB_MODE_ANNIHILATION 1 /* not implemented: returns PSIB_ERR_UNSUPPORTED */
+#define PSIB_MODE_ANNIHILATION 1 /* src/cpsi.c:115-158: adds to m the integral of rho_0 rho_1 over every
+                                    pair of overlapping tets (FP64; precision is ignored) */
 
 /* arithmetic of the clip kernel */
 #define PSIB_FP64 0  /* the reference's double-precision operation order, no FMA */

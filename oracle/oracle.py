@@ -99,6 +99,9 @@ def _lib(kind: str) -> C.CDLL:
             lib.oracle_voxels_ex.argtypes = [C.POINTER(_OgGrid), C.POINTER(_OgMesh), C.c_double, C.c_int, C.c_int,
                                              C.POINTER(C.c_double), C.POINTER(Counters)]
             lib.oracle_voxels_ex.restype = C.c_int
+            lib.oracle_annihilation.argtypes = [C.POINTER(_OgGrid), C.POINTER(_OgMesh), C.c_double, C.c_int,
+                                                C.POINTER(Counters)]
+            lib.oracle_annihilation.restype = C.c_int
         else:
             lib.psi_voxels.argtypes = [C.POINTER(_PsiGrid), C.POINTER(_PsiMesh), C.c_void_p,
                                        C.c_int, C.c_double, C.c_int]
@@ -144,8 +147,9 @@ def new_fields(n, fields):
 
 
 def voxelize(kind, n, bounds, pos, conn, vel=None, mass=None, periodic_box=None, fields=(),
-             reftol=1.0, maxlvl=0, out=None, counters=False, refine_mode=0, refine_cell=None):
-    """Run the density path of the chosen back end.
+             reftol=1.0, maxlvl=0, out=None, counters=False, refine_mode=0, refine_cell=None, mode="density"):
+    """Run the density (or, mode='annihilation', the annihilation) path of the
+    chosen back end.
 
     pos (npart,3) f64, conn (nelem, 4|8) i32, vel like pos (zeros if None),
     mass (nelem,) (ones if None).  ``out`` (a dict of field arrays) is
@@ -183,7 +187,11 @@ def voxelize(kind, n, bounds, pos, conn, vel=None, mass=None, periodic_box=None,
         m.box[0][:] = [float(v) for v in box[0]]
         m.box[1][:] = [float(v) for v in box[1]]
         cnt = Counters()
-        if refine_mode:
+        if mode == "annihilation":
+            if refine_mode:
+                raise ValueError("annihilation takes the midpoint refinement criterion")
+            rc = lib.oracle_annihilation(C.byref(g), C.byref(m), float(reftol), int(maxlvl), C.byref(cnt))
+        elif refine_mode:
             lag = (C.c_double * 3)(*[float(v) for v in refine_cell])
             rc = lib.oracle_voxels_ex(C.byref(g), C.byref(m), float(reftol), int(maxlvl), int(refine_mode), lag,
                                       C.byref(cnt))
@@ -205,7 +213,7 @@ def voxelize(kind, n, bounds, pos, conn, vel=None, mass=None, periodic_box=None,
     m.box[0][:] = [float(v) for v in box[0]]
     m.box[1][:] = [float(v) for v in box[1]]
     with _quiet_stdout():
-        lib.psi_voxels(C.byref(g), C.byref(m), None, 0, float(reftol), int(maxlvl))
+        lib.psi_voxels(C.byref(g), C.byref(m), None, 1 if mode == "annihilation" else 0, float(reftol), int(maxlvl))
     return (out, None) if counters else out
 
 

@@ -1,5 +1,6 @@
 /*
- * psi_oracle.c -- CPU restatement of PSI.voxels(grid, mesh) in density mode.
+ * psi_oracle.c -- CPU restatement of PSI.voxels(grid, mesh) in density and
+ * annihilation mode.
  *
  * TEST INFRASTRUCTURE ONLY.  This file is the checker for the CUDA path.  Only
  * tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg load it; the
@@ -105,7 +106,7 @@ static int link_new_vertices(ov_poly *P, int onv, int nv)
 }
 
 /* Clip by half-spaces n.x + d >= 0 (src/geometry.c:391-501). */
-static void ov_clip(ov_poly *P, const double (*pn)[3], const double *pd, int nplanes)
+static void ov_clip(ov_poly *P, const ov_real (*pn)[3], const ov_real *pd, int nplanes)
 {
     if (P->nv <= 0) return;
     for (int p = 0; p < nplanes; ++p) {
@@ -317,7 +318,7 @@ static void ov_voxelize_tet(const double (*pos)[3], const double (*vel)[3], doub
     ov_init_tet(P, pos);
 
     /* window planes and index box (src/geometry.c:806-843) */
-    double pn[6][3], pd[6];
+    ov_real pn[6][3], pd[6];
     int npl = 0;
     memset(pn, 0, sizeof(pn));
     memset(pd, 0, sizeof(pd));
@@ -334,7 +335,7 @@ static void ov_voxelize_tet(const double (*pos)[3], const double (*vel)[3], doub
         if (P->hi[i] > g->n[i]) P->hi[i] = g->n[i];
     }
     note_nv(P->nv);
-    ov_clip(P, (const double(*)[3])pn, pd, npl);
+    ov_clip(P, (const ov_real(*)[3])pn, pd, npl);
 
     int top = 1;
     ov_poly cur;
@@ -745,6 +746,250 @@ static int voxels_impl(og_grid *g, const og_mesh *m, double reftol, int max_lvl,
         }
     }
     free(stack);
+    free(tb.pos);
+    free(tb.vel);
+    free(tb.mass);
+    return rc;
+}
+
+/* ---- annihilation mode (src/cpsi.c:115-158, src/geometry.c:190-252) ----
+ *
+ * For every element e that survives the window cull (its vertices unwrapped,
+ * src/cpsi.c:309-341), every element e1 that survives it too and whose
+ * unwrapped box touches e's (closed intervals: the R*-tree query of
+ * src/rtree.c:83-125), every tet t of e (refined from the unwrapped vertices)
+ * and every tet t1 of e1 (refined from e1's vertices as stored, without the
+ * unwrap, src/cpsi.c:123-131) whose boxes overlap with positive extent
+ * (src/cpsi.c:293-306): the intersection of t and t1 deposits
+ * rho_t rho_t1 x (its volume in each voxel) into m.
+ *
+ * The reference visits e1 in the depth-first order of its R*-tree.  With at
+ * most 32 surviving elements that tree is one leaf holding them in index order,
+ * whose query returns them last first; this restatement takes that order
+ * (descending e1) for every mesh, so it equals the reference bit for bit up to
+ * 32 surviving elements and to rounding beyond. */
+
+static ov_real ov_third(void) { return (ov_real)1 / 3; }
+
+/* psi_orient_tet (src/geometry.c:190-224): six times the signed volume is the
+ * triple product of the edges from vertex 3, expanded as
+ * a.x (b x c).x + b.x (c x a).x + c.x (a x b).x; a negative tet has vertices
+ * 0 and 1 swapped.  Returns the volume. */
+static ov_real orient_tet(double (*p)[3])
+{
+    ov_real a[3], b[3], c[3];
+    for (int i = 0; i < 3; ++i) {
+        a[i] = (ov_real)p[0][i] - p[3][i];
+        b[i] = (ov_real)p[1][i] - p[3][i];
+        c[i] = (ov_real)p[2][i] - p[3][i];
+    }
+    const ov_real s = a[0] * (b[1] * c[2] - b[2] * c[1]) + b[0] * (c[1] * a[2] - c[2] * a[1]) +
+                      c[0] * (a[1] * b[2] - a[2] * b[1]);
+    ov_real vol = -((ov_real)1 / 6) * s;
+    if (vol < 0.0) {
+        for (int i = 0; i < 3; ++i) {
+            double t = p[0][i];
+            p[0][i] = p[1][i];
+            p[1][i] = t;
+        }
+        vol = -vol;
+    }
+    return vol;
+}
+
+/* One face plane n.x + d >= 0 of a tet (src/geometry.c:503-558): n = A x B of
+ * the two edge vectors A = a1 - a0, B = b1 - b0 the reference uses for that
+ * face, d = -n . (third of the sum of the face's vertices f0 + f1 + f2). */
+static void face_plane(const double *a0, const double *a1, const double *b0, const double *b1, const double *f0,
+                       const double *f1, const double *f2, ov_real *n, ov_real *d)
+{
+    ov_real A[3], B[3], c[3];
+    for (int i = 0; i < 3; ++i) {
+        A[i] = (ov_real)a1[i] - a0[i];
+        B[i] = (ov_real)b1[i] - b0[i];
+        c[i] = ov_third() * ((ov_real)f0[i] + f1[i] + f2[i]);
+    }
+    n[0] = A[1] * B[2] - A[2] * B[1];
+    n[1] = A[2] * B[0] - A[0] * B[2];
+    n[2] = A[0] * B[1] - A[1] * B[0];
+    *d = -(n[0] * c[0] + n[1] * c[1] + n[2] * c[2]);
+}
+
+static void tet_faces(const double (*v)[3], ov_real (*n)[3], ov_real *d)
+{
+    face_plane(v[1], v[3], v[1], v[2], v[1], v[2], v[3], n[0], &d[0]);
+    face_plane(v[0], v[2], v[2], v[3], v[2], v[3], v[0], n[1], &d[1]);
+    face_plane(v[3], v[1], v[3], v[0], v[3], v[0], v[1], n[2], &d[2]);
+    face_plane(v[2], v[0], v[0], v[1], v[0], v[1], v[2], n[3], &d[3]);
+}
+
+/* psi_voxelize_annihilation (src/geometry.c:226-252) of two oriented tets. */
+static void ov_annihilate(const double (*p0)[3], ov_real vol0, ov_real rho0, const double (*p1)[3], ov_real rho1,
+                          const double (*mbox)[3], const og_grid *g, ov_poly *stack)
+{
+    ov_poly *P = &stack[0];
+    ov_init_tet(P, p0);
+    ov_real fn[4][3], fd[4];
+    tet_faces(p1, fn, fd);
+    ov_clip(P, (const ov_real(*)[3])fn, fd, 4);
+
+    ov_real pn[6][3], pd[6];
+    int npl = 0;
+    memset(pn, 0, sizeof(pn));
+    memset(pd, 0, sizeof(pd));
+    for (int i = 0; i < 3; ++i) {
+        double cmin = mbox[0][i], cmax = mbox[1][i];
+        int clo = 0, chi = 0;
+        if (g->win[0][i] > cmin) { cmin = g->win[0][i]; clo = 1; }
+        if (g->win[1][i] < cmax) { cmax = g->win[1][i]; chi = 1; }
+        if (clo) { pn[npl][i] = 1.0; pd[npl] = -cmin; npl++; }
+        if (chi) { pn[npl][i] = -1.0; pd[npl] = cmax; npl++; }
+        P->lo[i] = (int)floor((cmin - g->win[0][i]) / g->d[i]);
+        P->hi[i] = (int)ceil((cmax - g->win[0][i]) / g->d[i]);
+        if (P->lo[i] < 0) P->lo[i] = 0;
+        if (P->hi[i] > g->n[i]) P->hi[i] = g->n[i];
+    }
+    note_nv(P->nv);
+    ov_clip(P, (const ov_real(*)[3])pn, pd, npl);
+
+    const ov_real w = rho0 * rho1 * vol0;
+    int top = 1;
+    ov_poly cur;
+    ov_real mom[10];
+    while (top > 0) {
+        cur = stack[--top];
+        if (cur.nv <= 0) continue;
+        int dmax = 0, ax = 0;
+        for (int i = 0; i < 3; ++i) {
+            int sz = cur.hi[i] - cur.lo[i];
+            if (sz > dmax) { dmax = sz; ax = i; }
+        }
+        if (dmax <= 1) {
+            ov_reduce(&cur, mom, 0);
+            if (mom[0] <= 0.0) continue;
+            if (cur.lo[0] >= g->n[0] || cur.lo[1] >= g->n[1] || cur.lo[2] >= g->n[2]) {
+                g_cnt->errors++;
+                continue;
+            }
+            long long gi = (long long)g->n[1] * g->n[2] * cur.lo[0] + (long long)g->n[2] * cur.lo[1] + cur.lo[2];
+            g_cnt->fragments++;
+            g_cnt->frag_verts += cur.nv;
+            g->f[0][gi] += w * mom[0];
+            continue;
+        }
+        if (top + 2 > OV_STACK) { g_cnt->errors++; continue; }
+        double coord = g->d[ax] * (cur.lo[ax] + dmax / 2) + g->win[0][ax];
+        ov_split(&cur, &stack[top], coord, ax);
+        memcpy(stack[top].lo, cur.lo, sizeof(cur.lo));
+        memcpy(stack[top].hi, cur.hi, sizeof(cur.hi));
+        stack[top].hi[ax] -= dmax - dmax / 2;
+        memcpy(stack[top + 1].lo, cur.lo, sizeof(cur.lo));
+        memcpy(stack[top + 1].hi, cur.hi, sizeof(cur.hi));
+        stack[top + 1].lo[ax] += dmax / 2;
+        top += 2;
+    }
+}
+
+/* An element's tets into tb (src/refine.c:58-150): a simplex is one tet of the
+ * element's mass, a trilinear element is refined. */
+static int element_tets(ov_tetbuf *tb, const double (*p)[3], const double (*u)[3], double mass, int vpe)
+{
+    tb->num = 0;
+    if (vpe == 4) {
+        if (tetbuf_reserve(tb, 1)) return -1;
+        memcpy(tb->pos[0], p, sizeof(double) * 12);
+        memcpy(tb->vel[0], u, sizeof(double) * 12);
+        tb->mass[0] = mass;
+        tb->num = 1;
+        return 0;
+    }
+    double np_[27][3], nu[27][3];
+    interp_trilinear(p, np_);
+    interp_trilinear(u, nu);
+    return refine_trilinear(tb, (const double(*)[3])np_, (const double(*)[3])nu, mass, 0);
+}
+
+int oracle_annihilation(og_grid *g, const og_mesh *m, double reftol, int max_lvl, og_counters *cnt)
+{
+    og_counters dummy;
+    memset(&dummy, 0, sizeof(dummy));
+    g_cnt = cnt ? cnt : &dummy;
+    if (m->elemtype != 4 && m->elemtype != 8) return -1;
+    const int vpe = m->elemtype;
+    double dxmin = 1.0e30;
+    for (int i = 0; i < 3; ++i)
+        if (g->d[i] < dxmin) dxmin = g->d[i];
+    if (max_lvl > 6) max_lvl = 6;
+    ov_tetbuf ta, tb;
+    memset(&ta, 0, sizeof(ta));
+    memset(&tb, 0, sizeof(tb));
+    ta.max_lvl = tb.max_lvl = max_lvl;
+    ta.ptol2 = tb.ptol2 = (reftol * dxmin) * (reftol * dxmin);
+    double(*box)[2][3] = malloc((size_t)(m->nelem > 0 ? m->nelem : 1) * sizeof(*box));
+    char *kept = calloc((size_t)(m->nelem > 0 ? m->nelem : 1), 1);
+    ov_poly *stack = malloc(OV_STACK * sizeof(ov_poly));
+    int rc = (box && kept && stack) ? 0 : -1;
+    /* element boxes after the unwrap, and the cull (src/rtree.c:48-73) */
+    for (int e = 0; rc == 0 && e < m->nelem; ++e) {
+        double tp[8][3];
+        for (int v = 0; v < vpe; ++v) memcpy(tp[v], &m->pos[3 * (size_t)m->conn[e * vpe + v]], sizeof(tp[v]));
+        kept[e] = (char)aabb_periodic(tp, vpe, box[e], g, m);
+    }
+    for (int e = 0; rc == 0 && e < m->nelem; ++e) {
+        if (!kept[e]) continue;
+        g_cnt->elements_kept++;
+        double tp[8][3], tu[8][3], rb[2][3];
+        for (int v = 0; v < vpe; ++v) {
+            int id = m->conn[e * vpe + v];
+            memcpy(tp[v], &m->pos[3 * (size_t)id], sizeof(tp[v]));
+            memcpy(tu[v], &m->vel[3 * (size_t)id], sizeof(tu[v]));
+        }
+        aabb_periodic(tp, vpe, rb, g, m);
+        if (element_tets(&ta, (const double(*)[3])tp, (const double(*)[3])tu, m->mass[e], vpe)) { rc = -1; break; }
+        g_cnt->tets += ta.num;
+        for (int e1 = m->nelem - 1; e1 >= 0; --e1) {
+            if (!kept[e1]) continue;
+            int touch = 1;
+            for (int i = 0; i < 3; ++i)
+                if (box[e][1][i] < box[e1][0][i] || box[e][0][i] > box[e1][1][i]) touch = 0;
+            if (!touch) continue;
+            double sp[8][3], su[8][3];
+            for (int v = 0; v < vpe; ++v) {
+                int id = m->conn[e1 * vpe + v];
+                memcpy(sp[v], &m->pos[3 * (size_t)id], sizeof(sp[v]));
+                memcpy(su[v], &m->vel[3 * (size_t)id], sizeof(su[v]));
+            }
+            if (element_tets(&tb, (const double(*)[3])sp, (const double(*)[3])su, m->mass[e1], vpe)) { rc = -1; break; }
+            for (int t = 0; t < ta.num; ++t) {
+                double b0[2][3];
+                aabb((const double(*)[3])ta.pos[4 * t], 4, b0);
+                for (int t1 = 0; t1 < tb.num; ++t1) {
+                    double b1[2][3], mb[2][3];
+                    aabb((const double(*)[3])tb.pos[4 * t1], 4, b1);
+                    int ok = 1;
+                    for (int i = 0; i < 3; ++i) {
+                        mb[0][i] = fmax(b0[0][i], b1[0][i]);
+                        mb[1][i] = fmin(b0[1][i], b1[1][i]);
+                        ok &= mb[1][i] > mb[0][i];
+                    }
+                    if (!ok) continue;
+                    g_cnt->tet_images++;
+                    /* orienting a tet in place is idempotent: each tet is oriented once */
+                    ov_real vol0 = orient_tet(ta.pos + 4 * t);
+                    ov_real vol1 = orient_tet(tb.pos + 4 * t1);
+                    ov_real rho0 = ta.mass[t] / vol0, rho1 = tb.mass[t1] / vol1;
+                    ov_annihilate((const double(*)[3])(ta.pos + 4 * t), vol0, rho0,
+                                  (const double(*)[3])(tb.pos + 4 * t1), rho1, (const double(*)[3])mb, g, stack);
+                }
+            }
+        }
+    }
+    free(box);
+    free(kept);
+    free(stack);
+    free(ta.pos);
+    free(ta.vel);
+    free(ta.mass);
     free(tb.pos);
     free(tb.vel);
     free(tb.mass);

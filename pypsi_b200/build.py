@@ -31,6 +31,7 @@ CUDA_UNITS = {  # unit -> extra flags
     "pipeline.cu": ["--fmad=false"],
     "noalloc.cu": ["--fmad=false"],
     "bfs.cu": [],
+    "annihilation.cu": ["--fmad=false"],
     "loaders.cpp": [],  # host code only: the snapshot readers
 }
 HEADERS = ["psib_device.cuh", "psib_clip.cuh", "psib_kernels.h"]

@@ -92,16 +92,19 @@ def make_mesh(npart, nelem, pos_ptr, vel_ptr=None, mass_ptr=None, conn_ptr=None,
 
 
 REFINE = {"midpoint": 0, "stretch": 1}
+MODES = {"density": 0, "annihilation": 1}
 
 
 def voxels(grid: Grid, mesh: Mesh, precision=PSIB_FP64, deterministic=False, memory=PSIB_DEVICE, stream=None,
-           refine_tolerance=1.0, refine_max_lvl=0, refine_criterion="midpoint", refine_cell=None) -> dict:
+           refine_tolerance=1.0, refine_max_lvl=0, refine_criterion="midpoint", refine_cell=None,
+           mode="density") -> dict:
     st = Stats()
     o = Options(precision=precision, deterministic=int(bool(deterministic)), memory=memory, device=-1,
                 stream=stream, stats=C.pointer(st), refine_mode=REFINE[refine_criterion])
     if refine_cell is not None:
         o.refine_cell[:] = [float(v) for v in refine_cell]
-    rc = lib.psib_voxels(C.byref(grid), C.byref(mesh), 0, float(refine_tolerance), int(refine_max_lvl), C.byref(o))
+    rc = lib.psib_voxels(C.byref(grid), C.byref(mesh), MODES[mode], float(refine_tolerance), int(refine_max_lvl),
+                         C.byref(o))
     if rc != 0:
         raise PsibError(rc)
     return st.as_dict()
@@ -109,8 +112,9 @@ def voxels(grid: Grid, mesh: Mesh, precision=PSIB_FP64, deterministic=False, mem
 
 def voxels_device(fields: dict, n, bounds, pos, vel=None, mass=None, connectivity=None, block_dims=None,
                   periodic_box=None, precision="fp64", deterministic=False, refine_tolerance=1.0, refine_max_lvl=0,
-                  stream=None, refine_criterion="midpoint", refine_cell=None) -> dict:
-    """Deposit on device-resident torch tensors.
+                  stream=None, refine_criterion="midpoint", refine_cell=None, mode="density") -> dict:
+    """Deposit on device-resident torch tensors (mode 'density', or
+    'annihilation': m gains the integral of rho_0 rho_1 over overlapping tets).
 
     fields: {"m": (nx,ny,nz) float64 CUDA tensor, "x": (...,3), ...}; pos/vel:
     (npart,3) float64; mass: (nelem,) float64; connectivity: (nelem, 4|8) int32
@@ -125,7 +129,7 @@ def voxels_device(fields: dict, n, bounds, pos, vel=None, mass=None, connectivit
     m = mesh_from_tensors(pos, vel, mass, connectivity, block_dims, periodic_box)
     s = stream if stream is not None else torch.cuda.current_stream()
     return voxels(g, m, PRECISIONS[precision], deterministic, PSIB_DEVICE,
-                  C.c_void_p(s.cuda_stream), refine_tolerance, refine_max_lvl, refine_criterion, refine_cell)
+                  C.c_void_p(s.cuda_stream), refine_tolerance, refine_max_lvl, refine_criterion, refine_cell, mode)
 
 
 def mesh_from_tensors(pos, vel=None, mass=None, connectivity=None, block_dims=None, periodic_box=None) -> Mesh:

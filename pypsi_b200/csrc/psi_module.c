@@ -12,8 +12,9 @@
  * PSI.last_stats() / PSI.device_count().
  *
  * The 'gadget2' / 'gevolution' loaders read snapshots through
- * psib_load_gadget2 / psib_load_gevolution.  Not provided here: annihilation
- * mode, PSI.RStarTree and PSI.VDF (other paths of the reference).
+ * psib_load_gadget2 / psib_load_gevolution; mode='annihilation' runs the
+ * library's annihilation deposit.  Not provided here: PSI.RStarTree and
+ * PSI.VDF (other paths of the reference).
  */
 #define PY_SSIZE_T_CLEAN
 #include <Python.h>

@@ -45,7 +45,9 @@ enum : unsigned {
 
 template <class R>
 struct Poly {
+    using real = R;
     static constexpr bool has_q = true;
+    static constexpr int CAP = MAXV;
     R x[MAXV][3];      // position
     R q[MAXV][3];      // barycentric mass coordinate
     uint32_t nb[MAXV]; // neighbour links: bits 0-7, 8-15, 16-23; bits 24-30: plane tags
@@ -56,7 +58,9 @@ struct Poly {
 // The FP32 walk carries positions and links only (q is rebuilt at the leaf).
 template <>
 struct Poly<float> {
+    using real = float;
     static constexpr bool has_q = false;
+    static constexpr int CAP = MAXV;
     float x[MAXV][3];
     uint32_t nb[MAXV];
     int nv;
@@ -94,8 +98,8 @@ __device__ __forceinline__ uint32_t axis_tag(int ax) { return 0x10000000u << ax;
 // Close the cut face: each vertex created by a cut (index >= base) gets its
 // two remaining links by walking around the face it opened
 // (src/geometry.c:459-482, :646-669).
-template <class R>
-__device__ __forceinline__ bool link_cut_vertices(Poly<R>& P, int base)
+template <class PT>
+__device__ __forceinline__ bool link_cut_vertices(PT& P, int base)
 {
     for (int vs = base; vs < P.nv; ++vs) {
         int vc = vs, vn = nbget(P.nb[vs], 0);
@@ -119,10 +123,12 @@ __device__ __forceinline__ bool link_cut_vertices(Poly<R>& P, int base)
 // to `lo` and, when BOTH, the upper side to `up`.  The cut vertex on edge
 // (a lower, b upper) is (b*s_a - a*s_b) / (s_a - s_b) in the reference's
 // operation order (src/geometry.c:441-445, :601-605).
-template <class R, bool BOTH>
-__device__ __forceinline__ unsigned cut_poly(const Poly<R>& in, const R* s, uint32_t umask, Poly<R>& lo, Poly<R>& up,
-                                             uint32_t cut_tag)
+template <class PT, bool BOTH>
+__device__ __forceinline__ unsigned cut_any(const PT& in, const typename PT::real* s, uint32_t umask, PT& lo, PT& up,
+                                            uint32_t cut_tag)
 {
+    using R = typename PT::real;
+    constexpr int CAP = PT::CAP;
     const int n = in.nv;
     const uint32_t all = (1u << n) - 1u;
     const uint32_t lmask = all & ~umask;
@@ -130,11 +136,11 @@ __device__ __forceinline__ unsigned cut_poly(const Poly<R>& in, const R* s, uint
     for (int v = 0; v < n; ++v) {
         const bool u = (umask >> v) & 1u;
         if (!BOTH && u) continue;
-        Poly<R>& o = u ? up : lo;
+        PT& o = u ? up : lo;
         const uint32_t sm = u ? umask : lmask;
         const int j = rank_in(sm, v);
         o.x[j][0] = in.x[v][0]; o.x[j][1] = in.x[v][1]; o.x[j][2] = in.x[v][2];
-        if constexpr (Poly<R>::has_q) {
+        if constexpr (PT::has_q) {
             o.q[j][0] = in.q[v][0]; o.q[j][1] = in.q[v][1]; o.q[j][2] = in.q[v][2];
         }
         const uint32_t w = in.nb[v];
@@ -155,19 +161,19 @@ __device__ __forceinline__ unsigned cut_poly(const Poly<R>& in, const R* s, uint
             const int vn = nbget(w, np);
             if (vn >= n) return ST_GRAPH;
             if (!((umask >> vn) & 1u)) continue;
-            if (nl + k >= MAXV || (BOTH && nu + k >= MAXV)) return ST_OVERFLOW;
+            if (nl + k >= CAP || (BOTH && nu + k >= CAP)) return ST_OVERFLOW;
             const R sc = s[vc], sn = s[vn];
             const R iw = R(1) / (sc - sn);
             R px[3], pq[3];
             for (int i = 0; i < 3; ++i) {
                 px[i] = iw * (in.x[vn][i] * sc - in.x[vc][i] * sn);
-                if constexpr (Poly<R>::has_q) pq[i] = iw * (in.q[vn][i] * sc - in.q[vc][i] * sn);
+                if constexpr (PT::has_q) pq[i] = iw * (in.q[vn][i] * sc - in.q[vc][i] * sn);
             }
             const int il = nl + k;
             const uint32_t tg = (w & in.nb[vn] & ALL_TAGS) | cut_tag;
             for (int i = 0; i < 3; ++i) {
                 lo.x[il][i] = px[i];
-                if constexpr (Poly<R>::has_q) lo.q[il][i] = pq[i];
+                if constexpr (PT::has_q) lo.q[il][i] = pq[i];
             }
             lo.nb[il] = 0xFFFF00u | (uint32_t)jc | tg;
             lo.nb[jc] = nbset(lo.nb[jc], np, il);
@@ -176,7 +182,7 @@ __device__ __forceinline__ unsigned cut_poly(const Poly<R>& in, const R* s, uint
                 const int jn = rank_in(umask, vn);
                 for (int i = 0; i < 3; ++i) {
                     up.x[iu][i] = px[i];
-                    if constexpr (Poly<R>::has_q) up.q[iu][i] = pq[i];
+                    if constexpr (PT::has_q) up.q[iu][i] = pq[i];
                 }
                 up.nb[iu] = 0xFFFF00u | (uint32_t)jn | tg;
                 const uint32_t wn = in.nb[vn];
@@ -194,6 +200,13 @@ __device__ __forceinline__ unsigned cut_poly(const Poly<R>& in, const R* s, uint
         if (!link_cut_vertices(up, nu)) return ST_GRAPH;
     }
     return 0;
+}
+
+template <class R, bool BOTH>
+__device__ __forceinline__ unsigned cut_poly(const Poly<R>& in, const R* s, uint32_t umask, Poly<R>& lo, Poly<R>& up,
+                                             uint32_t cut_tag)
+{
+    return cut_any<Poly<R>, BOTH>(in, s, umask, lo, up, cut_tag);
 }
 
 // The tet as a vertex graph with q = (0, e_x, e_y, e_z) (src/geometry.c:769-804).

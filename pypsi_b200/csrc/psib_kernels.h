@@ -191,6 +191,99 @@ struct ApplyArgs {
 };
 cudaError_t launch_apply_records(const ApplyArgs &a, cudaStream_t s);
 
+// ---- annihilation mode (annihilation.cu; the element stage in tess.cu) ----
+// A tet record: 4 oriented vertices (vertex-major), rho = mass / volume, the
+// volume, and the bounding box (lo, hi).
+constexpr int TREC = 20;
+constexpr int TR_RHO = 12, TR_VOL = 13, TR_BOX = 14;
+
+struct AnnTessArgs {
+    MeshDev m;
+    GridDev g;
+    int max_lvl;
+    int quad;
+    // count pass: per element the number of tets of each side (0: culled) and the
+    // unwrapped element box (6 doubles: lo, hi)
+    int *cnt_a, *cnt_b;
+    double *ebox;
+    // emit pass: exclusive offsets and the tet records; side A is refined from the
+    // unwrapped element, side B from the element's vertices as stored
+    const long long *off_a, *off_b;
+    double *tets_a, *tets_b;
+    unsigned *status;
+    unsigned long long *counters; // elements kept, side-A tets
+};
+cudaError_t launch_ann_tess(const AnnTessArgs &a, bool emit, cudaStream_t s);
+
+// Uniform cells over the element boxes: origin, cell size and cells per axis.
+struct CellGrid {
+    double o[3], h[3];
+    long long n[3];
+};
+struct AnnArgs {
+    long long nelem;
+    const double *ebox;
+    const int *cnt_a, *cnt_b;
+    const long long *off_a, *off_b;
+    const double *tets_a, *tets_b;
+    CellGrid cg;
+    // cell registrations: (cell key, element)
+    const long long *reg_off; // per element, exclusive (emit)
+    long long *reg_cnt;       // per element (count)
+    unsigned long long *reg_key;
+    int *reg_elem;
+    long long nreg;
+    const long long *run_lo, *run_hi; // per sorted registration: its cell's run [lo, hi)
+    // element pairs: key (e << 32) | (2^32 - 1 - e1), so that sorting gives e ascending, e1 descending
+    const long long *pair_off;
+    long long *pair_cnt;
+    unsigned long long *pair_key;
+    long long npair;
+    // side-A tet slots of the element pairs: slot u is tet u - aoff[p] of pair p's element e
+    const long long *aoff;
+    long long nslot, slot0, slot1; // slots [slot0, slot1) of this launch
+    const long long *tp_excl; // per slot, exclusive over all slots (emit); tp_base: that of slot0
+    long long tp_base;
+    long long *tp_cnt;        // per slot (count)
+    int2 *tpairs;             // (side-A tet, side-B tet) of every tet pair of the chunk
+    unsigned *status;
+};
+// stats of the kept element boxes: 2 x 3 ordered-int min/max, 3 extent sums, kept count
+cudaError_t launch_ann_box_stats(const AnnArgs &a, unsigned long long *out, double *ext, cudaStream_t s);
+cudaError_t launch_ann_cells(const AnnArgs &a, bool emit, cudaStream_t s);
+cudaError_t launch_ann_runs(const unsigned *run_cnt_u, const long long *run_off, long long nruns, long long *lo,
+                            long long *hi, cudaStream_t s);
+cudaError_t launch_ann_pairs(const AnnArgs &a, bool emit, cudaStream_t s);
+cudaError_t launch_ann_pair_sides(const AnnArgs &a, long long *na, cudaStream_t s);
+cudaError_t launch_ann_tpairs(const AnnArgs &a, bool emit, cudaStream_t s);
+// chunk plan: bounds[k] = the first slot whose exclusive tet-pair offset reaches k * budget
+// (bounds[0] = 0, bounds[nb] = nslot); tp_excl holds nslot + 1 offsets
+cudaError_t launch_ann_chunk_bounds(const long long *tp_excl, long long nslot, long long budget, int nb,
+                                    long long *bounds, cudaStream_t s);
+
+struct AnnClipArgs {
+    const int2 *tpairs;
+    long long n;             // tet pairs of this launch
+    const int *list;         // null: tet pairs [0, n); else their indices
+    const double *tets_a, *tets_b;
+    GridDev g;
+    unsigned long long *head;
+    int *deep;               // main kernel: tet pairs whose bisection is deeper than it serves
+    unsigned long long *ndeep;
+    unsigned long long *rec_key; // voxel << rec_ibits | tet pair
+    double *rec_val;
+    unsigned long long *rec_n, rec_cap;
+    int rec_ibits;
+    unsigned *status;
+    unsigned long long *counters; // fragments, fragment vertices, splits
+    void *scratch;
+};
+cudaError_t launch_ann_clip(const AnnClipArgs &a, bool big, int grid, int block, cudaStream_t s);
+size_t ann_scratch_bytes(bool big);
+int ann_blocks_per_sm(bool big, int block);
+// sequential sum of each voxel run of the sorted records into m
+cudaError_t launch_ann_apply(const ApplyArgs &a, cudaStream_t s);
+
 // Record `msg` as this thread's last error (psib_last_error) and return `code`.
 int report_error(int code, const char *msg);
 

@@ -256,7 +256,8 @@ __device__ bool stretch_refine(const double (*p)[3], int lvl, double T, const do
 
 // Adaptive refinement of a trilinear element, depth first in the reference's
 // child order (src/refine.c:223-289).
-__device__ void refine_element(Emitter& em, const double (*cp)[3], const double (*cu)[3], double mass, long long e,
+template <class EM>
+__device__ void refine_element(EM& em, const double (*cp)[3], const double (*cu)[3], double mass, long long e,
                                int max_lvl, double ptol2, int mode, double T, const double* lag, RefNode* L)
 {
     interp_trilinear(cp, L[0].p);
@@ -349,7 +350,8 @@ __device__ double quad_node(const double (*in)[3], int A, int B, int C, int ax)
 // tolerance; child (i,j,k) takes nodes (2i..2i+2, ...) of the parent's
 // 125-node interpolation; a leaf gives the 6 tets of its corner nodes
 // (src/refine.c:299-319).
-__device__ void refine_element_quad(Emitter& em, const double (*cp)[3], const double (*cu)[3], double mass,
+template <class EM>
+__device__ void refine_element_quad(EM& em, const double (*cp)[3], const double (*cu)[3], double mass,
                                     long long e, int max_lvl, double ptol2, int mode, double T, const double* lag,
                                     RefNode* L)
 {
@@ -518,6 +520,148 @@ cudaError_t launch_tess_count(const TessArgs& a, cudaStream_t s)
 cudaError_t launch_tess_emit(const TessArgs& a, cudaStream_t s)
 {
     launch_tess<true>(a, s);
+    return cudaGetLastError();
+}
+
+// ---- annihilation: the tets of each element, from its unwrapped and its stored vertices ----
+
+// Orientation and density of a tet as psi_orient_tet computes them
+// (src/geometry.c:190-224): six times the signed volume is the triple product
+// of the edges from vertex 3, a.x (b x c).x + b.x (c x a).x + c.x (a x b).x; a
+// negative tet has vertices 0 and 1 swapped.  Orienting is idempotent (the
+// swapped tet's volume is the exact negation), so orienting once here equals
+// the reference's orienting at every use.  Writes a TREC record.
+__device__ void ann_record(const double (*p)[3], double mass, double* r)
+{
+    double a[3], b[3], c[3];
+    for (int i = 0; i < 3; ++i) {
+        a[i] = p[0][i] - p[3][i];
+        b[i] = p[1][i] - p[3][i];
+        c[i] = p[2][i] - p[3][i];
+    }
+    const double s = a[0] * (b[1] * c[2] - b[2] * c[1]) + b[0] * (c[1] * a[2] - c[2] * a[1]) +
+                     c[0] * (a[1] * b[2] - a[2] * b[1]);
+    double vol = -(1.0 / 6.0) * s;
+    const bool swap = vol < 0.0;
+    if (swap) vol = -vol;
+    for (int v = 0; v < 4; ++v) {
+        const int src = swap && v < 2 ? 1 - v : v;
+        for (int i = 0; i < 3; ++i) r[3 * v + i] = p[src][i];
+    }
+    r[TR_RHO] = mass / vol;
+    r[TR_VOL] = vol;
+    for (int i = 0; i < 3; ++i) {
+        double lo = p[0][i], hi = p[0][i];
+        for (int v = 1; v < 4; ++v) {
+            lo = p[v][i] < lo ? p[v][i] : lo;
+            hi = p[v][i] > hi ? p[v][i] : hi;
+        }
+        r[TR_BOX + i] = lo;
+        r[TR_BOX + 3 + i] = hi;
+    }
+}
+
+struct AnnEmitter {
+    double* out; // null: count only
+    long long pos;
+    int n;
+    unsigned long long tets;
+    __device__ void tet(const double (*p)[3], const double (*)[3], double mass, long long, const int*)
+    {
+        if (out) ann_record(p, mass, out + (pos++) * TREC);
+        n++;
+        tets++;
+    }
+};
+
+template <bool REFINE, bool QUAD>
+__device__ int ann_side(const AnnTessArgs& a, const double (*p)[3], const double (*u)[3], double me, long long e,
+                        double* out, long long pos, RefNode* L)
+{
+    AnnEmitter em{out, pos, 0, 0};
+    const int et = a.m.elemtype;
+    if (et == 4) {
+        em.tet(p, u, me, e, nullptr);
+    } else if (QUAD && et == 27) {
+        if constexpr (QUAD) refine_element_quad(em, p, u, me, e, REFINE ? a.max_lvl : 0, a.m.ptol2, 0, 0.0, a.m.lag, L);
+    } else if (!REFINE) {
+        for (int t = 0; t < 6; ++t) {
+            double tp[4][3];
+            for (int v = 0; v < 4; ++v)
+                for (int i = 0; i < 3; ++i) tp[v][i] = p[c_tet_corners[t][v]][i];
+            em.tet(tp, tp, me * (1.0 / 6), e, nullptr);
+        }
+    } else {
+        if constexpr (REFINE) refine_element(em, p, u, me, e, a.max_lvl, a.m.ptol2, 0, 0.0, a.m.lag, L);
+    }
+    return em.n;
+}
+
+// One thread per element: the cull of src/cpsi.c:88-93 (which unwraps the
+// element), then its tets on side A (unwrapped vertices, the element loop of
+// src/cpsi.c:95) and side B (stored vertices, the R*-tree partner of
+// src/cpsi.c:123-131).  Count pass: tet counts and the unwrapped element box;
+// emit pass: the tet records.
+template <bool REFINE, bool QUAD, bool EMIT>
+__global__ void __launch_bounds__(128) k_ann_tess(AnnTessArgs a)
+{
+    constexpr int NV = QUAD ? 27 : 8;
+    RefNode* L = nullptr;
+    RefNode Lbuf[(REFINE || QUAD) ? MAX_REFINE + 1 : 1];
+    if constexpr (REFINE || QUAD) L = Lbuf;
+    unsigned long long kept = 0, tets = 0;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < a.m.nelem; e += stride) {
+        double p[NV][3], u[NV][3], q[NV][3];
+        int ids[NV];
+        if ((!QUAD && a.m.elemtype == 27) || !gather(a.m, e, p, u, ids)) {
+            atomicOr(a.status, ST_INDEX);
+            if (!EMIT) a.cnt_a[e] = a.cnt_b[e] = 0;
+            continue;
+        }
+        const int et = a.m.elemtype;
+        for (int v = 0; v < et; ++v)
+            for (int i = 0; i < 3; ++i) q[v][i] = p[v][i];
+        const bool keep = aabb_periodic(q, et, a.m, a.g);
+        if (!EMIT) {
+            double rb[2][3];
+            aabb_n(q, et, rb);
+            for (int i = 0; i < 3; ++i) {
+                a.ebox[6 * e + i] = rb[0][i];
+                a.ebox[6 * e + 3 + i] = rb[1][i];
+            }
+        }
+        if (!keep) {
+            if (!EMIT) a.cnt_a[e] = a.cnt_b[e] = 0;
+            continue;
+        }
+        const double me = a.m.mass ? a.m.mass[e] : 1.0;
+        const int na = ann_side<REFINE, QUAD>(a, q, u, me, e, EMIT ? a.tets_a : nullptr, EMIT ? a.off_a[e] : 0, L);
+        const int nb = ann_side<REFINE, QUAD>(a, p, u, me, e, EMIT ? a.tets_b : nullptr, EMIT ? a.off_b[e] : 0, L);
+        if (!EMIT) {
+            a.cnt_a[e] = na;
+            a.cnt_b[e] = nb;
+        }
+        kept++;
+        tets += na;
+    }
+    if (a.counters && EMIT) {
+        atomicAdd(&a.counters[0], kept);
+        atomicAdd(&a.counters[1], tets);
+    }
+}
+
+cudaError_t launch_ann_tess(const AnnTessArgs& a, bool emit, cudaStream_t s)
+{
+    const int g = tess_grid(a.m.nelem);
+    const bool refine = a.max_lvl > 0 && a.m.elemtype != 4;
+    if (a.quad) {
+        if (refine) emit ? k_ann_tess<true, true, true><<<g, 128, 0, s>>>(a) : k_ann_tess<true, true, false><<<g, 128, 0, s>>>(a);
+        else emit ? k_ann_tess<false, true, true><<<g, 128, 0, s>>>(a) : k_ann_tess<false, true, false><<<g, 128, 0, s>>>(a);
+    } else {
+        if (refine) emit ? k_ann_tess<true, false, true><<<g, 128, 0, s>>>(a) : k_ann_tess<true, false, false><<<g, 128, 0, s>>>(a);
+        else emit ? k_ann_tess<false, false, true><<<g, 128, 0, s>>>(a) : k_ann_tess<false, false, false><<<g, 128, 0, s>>>(a);
+    }
     return cudaGetLastError();
 }
 
