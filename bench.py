@@ -54,9 +54,9 @@ def parse():
     ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c5"],
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c5", "ann"],
                     help="c2: the headline (128^3 -> 256^3, order 2); c3: 512 uneven cutouts in one batch; "
-                         "c5: 256^3 -> 512^3 with stretch refinement")
+                         "c5: 256^3 -> 512^3 with stretch refinement; ann: annihilation mode, 64^3 -> 128^3")
     args = ap.parse_args()
     if (args.n_part, args.n_grid) != (N_PART, N_GRID) or args.precision != "both":
         args.no_cpu_baseline = True
@@ -217,6 +217,180 @@ def cpu_baseline_single(seconds=12.0):
     return {"value": tets / secs, "unit": "tets/s", "cores": 1, "kind": "reference" if kind == "reference" else "port",
             "sample": f"{nb} Lagrangian 16^3-element sub-blocks of the workload ({tets} tets, {secs:.1f} s), "
                       f"each on a window covering it at the 256^3 voxel size"}
+
+
+# ---------------------------------------------------------------- annihilation (--workload ann)
+ANN_N, ANN_GRID, ANN_RMS = 64, 128, 1.5
+ANN_METRIC = "tet pairs/s @64³→128³ annihilation (m += rho0 rho1 V over overlapping tets), FP64"
+ANN_WORKLOAD = ("64^3 particles, open lattice (63^3 trilinear elements), Zel'dovich rms 1.5 cells -> 128^3 grid "
+                "over the box, annihilation mode, m only")
+ANN_DATA = "synthetic: seeded Zel'dovich-displaced particle lattice (P(k)~k^-2), unwrapped, element mass 1"
+
+
+def _ann_init(seed):
+    global _A
+    sys.path[:0] = [ROOT, os.path.join(ROOT, "oracle")]
+    from pypsi_b200.synth import zeldovich
+
+    _A = zeldovich(ANN_N, ANN_RMS, seed, wrap=False)[0]
+
+
+def ann_blocks(edge=16):
+    nb = (ANN_N - 1) // edge
+    return [(i * edge, j * edge, k * edge) for i in range(nb) for j in range(nb) for k in range(nb)]
+
+
+def _ann_block(args):
+    """Annihilation of the elements of one Lagrangian sub-block (edge^3 elements)
+    on a window covering it at the workload's voxel size: the reference's
+    psi_voxels times it; the oracle's restatement (not timed) counts its tet
+    pairs.  Returns (tet pairs, seconds)."""
+    origin, edge, kind = args
+    import numpy as np
+
+    import oracle as O
+
+    i0, j0, k0 = origin
+    p = np.ascontiguousarray(_A[i0:i0 + edge + 1, j0:j0 + edge + 1, k0:k0 + edge + 1].reshape(-1, 3))
+    conn = O.block_connectivity((edge + 1,) * 3, False)
+    d = BOX[1][0] / ANN_GRID
+    lo = np.floor(p.min(axis=0) / d) - 1
+    hi = np.ceil(p.max(axis=0) / d) + 1
+    bounds = (tuple(lo * d), tuple(hi * d))
+    ng = tuple(int(v) for v in (hi - lo))
+    t0 = time.perf_counter()
+    O.voxelize(kind, n=ng, bounds=bounds, pos=p, conn=conn, mode="annihilation")
+    secs = time.perf_counter() - t0
+    _, cnt = O.voxelize("restatement", n=ng, bounds=bounds, pos=p, conn=conn, mode="annihilation", counters=True)
+    return cnt["tet_images"], secs
+
+
+def _ann_sample_line(kind, nb, pairs, secs, cores, per="per step"):
+    return {"value": pairs / secs, "unit": "tet pairs/s", "cores": cores,
+            "kind": "reference" if kind == "reference" else "port",
+            "sample": f"{nb} Lagrangian 16^3-element sub-blocks of the workload {per} ({pairs} tet pairs, "
+                      f"{secs:.1f} s of the reference's psi_voxels), each on a window covering it at the 128^3 "
+                      f"voxel size; tet pairs counted by the oracle"}
+
+
+def run_reference_ann(args):
+    rank, world, _ = env_rank()
+    if rank != 0:
+        return
+    import multiprocessing as mp
+
+    sys.path[:0] = [os.path.join(ROOT, "oracle")]
+    import oracle as O
+
+    kind = "reference" if O.available("reference") else "restatement"
+    cores = len(os.sched_getaffinity(0))
+    blocks = ann_blocks()
+    per_step = blocks[: max(1, min(len(blocks), cores))]
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores, initializer=_ann_init, initargs=(4242,)) as pool:
+        def step():
+            t0 = time.perf_counter()
+            res = pool.map(_ann_block, [(b, 16, kind) for b in per_step], chunksize=1)
+            return sum(r[0] for r in res), time.perf_counter() - t0
+
+        for _ in range(args.warmup):
+            step()
+        pairs, secs = 0, 0.0
+        for _ in range(args.steps):
+            t, s_ = step()
+            pairs += t
+            secs += s_
+    value = pairs / secs
+    line = {"impl": "reference", "metric": ANN_METRIC, "value": value, "unit": "tet pairs/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * secs / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": ANN_DATA,
+            "config": {"workload": ANN_WORKLOAD, "precision": "fp64 (reference C)"},
+            "cpu_baseline": _ann_sample_line(kind, len(per_step), pairs, secs, cores, "per step, one per process"),
+            "e2e": {"value": value, "unit": "tet pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    line["cpu_baseline"]["value"] = value
+    print(json.dumps(line), flush=True)
+
+
+def run_ann(args):
+    """Annihilation of a 64^3 open lattice on a 128^3 grid: device-resident
+    timing through the C ABI, and the drop-in module on host arrays (e2e)."""
+    import numpy as np
+    import torch
+
+    from pypsi_b200 import PSI, capi
+    from pypsi_b200.synth import zeldovich
+
+    rank, world, local = env_rank()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pos = zeldovich(ANN_N, ANN_RMS, 4242 + rank, wrap=False)[0]
+    dpos = torch.from_numpy(pos.reshape(-1, 3)).to(dev)
+    m = torch.zeros((ANN_GRID,) * 3, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream()
+
+    def step():
+        return capi.voxels_device({"m": m}, (ANN_GRID,) * 3, BOX, dpos, block_dims=(ANN_N,) * 3, mode="annihilation",
+                                  stream=stream)
+
+    for _ in range(max(1, args.warmup)):
+        m.zero_()
+        st = step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ck = Clocks(local)
+    ck.__enter__()
+    e0.record(stream)
+    stats = [step() for _ in range(args.steps)]
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ck.__exit__()
+    ms = e0.elapsed_time(e1) / args.steps
+    pairs = st["tet_images"]
+    # end to end: PSI.voxels(mode='annihilation') on host arrays (the copies in the timed region)
+    e2e = None
+    if not args.no_e2e:
+        grid = PSI.Grid(n=(ANN_GRID,) * 3, bounds=BOX)
+        mesh = PSI.Mesh(loader="block", pos=np.ascontiguousarray(pos))
+        PSI.voxels(grid=grid, mesh=mesh, mode="annihilation")
+        ts = []
+        for _ in range(max(1, args.e2e_steps)):
+            grid.fields["m"][...] = 0.0
+            t0 = time.perf_counter()
+            PSI.voxels(grid=grid, mesh=mesh, mode="annihilation")
+            ts.append(time.perf_counter() - t0)
+        t = statistics.median(ts)
+        e2e = {"value": pairs / t, "unit": "tet pairs/s", "h2d_bytes_per_step": int(pos.nbytes + grid.fields["m"].nbytes),
+               "d2h_bytes_per_step": int(grid.fields["m"].nbytes), "api": "PSI.voxels(grid, mesh, mode='annihilation')"
+               " on host numpy arrays", "ms_per_step": 1000 * t}
+    line = {"metric": ANN_METRIC, "value": pairs / (ms * 1e-3), "unit": "tet pairs/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": ANN_DATA,
+            "config": {"workload": ANN_WORKLOAD, "l2": "inputs larger than L2 (tet records and fragment records)"},
+            "work": {"elements_kept": st["elements_kept"], "tets": st["tets"], "tet_pairs": pairs,
+                     "fragments": st["fragments"], "splits": st["splits"], "chunks": st["chunks"]},
+            "stage_ms": {"elements_pairs_and_tet_pairs": st["ms_tess"], "clip": st["ms_clip"],
+                         "sort_and_apply": st["ms_final"]},
+            "gpu_launches": int(sum(x["kernel_launches"] for x in stats)), "clocks": ck.summary()}
+    if e2e:
+        line["e2e"] = e2e
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sys.path[:0] = [os.path.join(ROOT, "oracle")]
+        import oracle as O
+
+        kind = "reference" if O.available("reference") else "restatement"
+        _ann_init(4242)
+        pairs_c, secs, nb = 0, 0.0, 0
+        for b in ann_blocks():
+            pc, sc = _ann_block((b, 16, kind))
+            pairs_c += pc
+            secs += sc
+            nb += 1
+            if secs > 12.0:
+                break
+        line["cpu_baseline"] = _ann_sample_line(kind, nb, pairs_c, secs, 1, "in all")
+    capi.lib.psib_release_device_memory()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
 
 
 # ---------------------------------------------------------------- our arm
@@ -603,8 +777,12 @@ def run_ours(args):
 
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.impl == "reference" and args.workload == "ann":
+        run_reference_ann(args)
+    elif args.impl == "reference":
         run_reference(args)
+    elif args.workload == "ann":
+        run_ann(args)
     elif args.workload == "c5":
         run_c5(args)
     elif args.workload == "c3":

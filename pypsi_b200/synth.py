@@ -12,8 +12,9 @@ from __future__ import annotations
 import numpy as np
 
 
-def zeldovich(n: int, rms_cells: float, seed: int, box: float = 100.0):
-    """Return ``pos, vel`` as float64 arrays of shape (n, n, n, 3)."""
+def zeldovich(n: int, rms_cells: float, seed: int, box: float = 100.0, wrap: bool = True):
+    """Return ``pos, vel`` as float64 arrays of shape (n, n, n, 3); with
+    ``wrap=False`` the positions are left unwrapped (an open lattice)."""
     rng = np.random.default_rng(seed)
     white = rng.standard_normal((n, n, n))
     wk = np.fft.rfftn(white)
@@ -32,7 +33,7 @@ def zeldovich(n: int, rms_cells: float, seed: int, box: float = 100.0):
         psi *= rms_cells * (box / n) / rms
     idx = (np.arange(n) + 0.5) * (box / n)
     q = np.stack(np.meshgrid(idx, idx, idx, indexing="ij"), axis=-1)
-    pos = np.mod(q + psi, box)
+    pos = np.mod(q + psi, box) if wrap else q + psi
     vel = (10.0 * psi).astype(np.float32).astype(np.float64)
     return np.ascontiguousarray(pos), np.ascontiguousarray(vel)
 
