@@ -22,11 +22,14 @@
 namespace psib {
 
 // The polyhedron of a tet pair: the intersection of two tets, the window and a
-// voxel has up to 14 faces, so up to 24 vertices -- more than the density
-// path's polyhedron holds.
-constexpr int MAXV_ANN = 30; // vertex masks are 32 bits wide
+// voxel has up to 14 faces, so 24 vertices when no more than three planes meet
+// at a point, and more where the vertex graph repeats a point at which several
+// planes meet (tets that share faces, a tet against itself).  The reference's
+// buffer holds 64 (include/geometry.h:23).
+constexpr int MAXV_ANN = 62;
 struct PolyA {
     using real = double;
+    using mask_t = uint64_t;
     static constexpr bool has_q = true;
     static constexpr int CAP = MAXV_ANN;
     double x[MAXV_ANN][3];
@@ -419,7 +422,7 @@ __device__ bool ann_clip_pair(const AnnClipArgs& a, long long k, PolyA* S, unsig
             dd = pdd[w];
         }
         double smin = 1.0e30, smax = -1.0e30;
-        uint32_t um = 0;
+        uint64_t um = 0;
         for (int v = 0; v < P.nv; ++v) {
             // ((d + x0 n0) + x1 n1) + x2 n2 (src/geometry.c:418-425)
             double t0 = dd;
@@ -427,7 +430,7 @@ __device__ bool ann_clip_pair(const AnnClipArgs& a, long long k, PolyA* S, unsig
             s[v] = t0;
             if (t0 < smin) smin = t0;
             if (t0 > smax) smax = t0;
-            if (t0 < 0.0) um |= 1u << v;
+            if (t0 < 0.0) um |= 1ull << v;
         }
         if (smin >= 0.0) continue;
         if (smax <= 0.0) { P.nv = 0; break; }
@@ -468,16 +471,16 @@ __device__ bool ann_clip_pair(const AnnClipArgs& a, long long k, PolyA* S, unsig
             } else {
                 tally.splits++;
                 const double coord = g.d[ax] * (P.lo[ax] + dm / 2) + g.w0[ax];
-                uint32_t um = 0;
+                uint64_t um = 0;
                 for (int v = 0; v < P.nv; ++v) {
                     s[v] = coord - P.x[v][ax];
-                    if (s[v] < 0.0) um |= 1u << v;
+                    if (s[v] < 0.0) um |= 1ull << v;
                 }
                 const int nlo = dm / 2, nup = dm - dm / 2;
                 if (um == 0) {
                     P.hi[ax] -= nup;
                     done_node = false;
-                } else if (um == (1u << P.nv) - 1u) {
+                } else if (um == (1ull << P.nv) - 1ull) {
                     P.lo[ax] += nlo;
                     done_node = false;
                 } else {

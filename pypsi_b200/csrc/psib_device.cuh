@@ -46,6 +46,7 @@ enum : unsigned {
 template <class R>
 struct Poly {
     using real = R;
+    using mask_t = uint32_t; // one bit per vertex
     static constexpr bool has_q = true;
     static constexpr int CAP = MAXV;
     R x[MAXV][3];      // position
@@ -59,6 +60,7 @@ struct Poly {
 template <>
 struct Poly<float> {
     using real = float;
+    using mask_t = uint32_t;
     static constexpr bool has_q = false;
     static constexpr int CAP = MAXV;
     float x[MAXV][3];
@@ -69,6 +71,7 @@ struct Poly<float> {
 
 // A fragment for the moment sums: FP64 q and links.
 struct QPoly {
+    static constexpr int CAP = MAXV;
     double q[MAXV][3];
     uint32_t nb[MAXV];
     int nv;
@@ -80,6 +83,9 @@ __device__ __forceinline__ uint32_t nbset(uint32_t w, int k, int v)
     return (w & ~(0xFFu << (8 * k))) | ((uint32_t)v << (8 * k));
 }
 __device__ __forceinline__ int rank_in(uint32_t mask, int v) { return __popc(mask & ((1u << v) - 1u)); }
+__device__ __forceinline__ int rank_in(uint64_t mask, int v) { return __popcll(mask & ((1ull << v) - 1ull)); }
+__device__ __forceinline__ int popc_of(uint32_t m) { return __popc(m); }
+__device__ __forceinline__ int popc_of(uint64_t m) { return __popcll(m); }
 
 // Plane tags of a vertex, in the top byte of its link word.  Bit 24 + j: the
 // vertex lies on the face of the original tet opposite its vertex j.  Bit
@@ -124,20 +130,22 @@ __device__ __forceinline__ bool link_cut_vertices(PT& P, int base)
 // (a lower, b upper) is (b*s_a - a*s_b) / (s_a - s_b) in the reference's
 // operation order (src/geometry.c:441-445, :601-605).
 template <class PT, bool BOTH>
-__device__ __forceinline__ unsigned cut_any(const PT& in, const typename PT::real* s, uint32_t umask, PT& lo, PT& up,
-                                            uint32_t cut_tag)
+__device__ __forceinline__ unsigned cut_any(const PT& in, const typename PT::real* s, typename PT::mask_t umask, PT& lo,
+                                            PT& up, uint32_t cut_tag)
 {
     using R = typename PT::real;
+    using M = typename PT::mask_t;
     constexpr int CAP = PT::CAP;
+    static_assert(CAP < 8 * (int)sizeof(M), "a vertex mask bit for every vertex");
     const int n = in.nv;
-    const uint32_t all = (1u << n) - 1u;
-    const uint32_t lmask = all & ~umask;
-    const int nl = __popc(lmask), nu = __popc(umask);
+    const M all = ((M)1 << n) - (M)1;
+    const M lmask = all & ~umask;
+    const int nl = popc_of(lmask), nu = popc_of(umask);
     for (int v = 0; v < n; ++v) {
         const bool u = (umask >> v) & 1u;
         if (!BOTH && u) continue;
         PT& o = u ? up : lo;
-        const uint32_t sm = u ? umask : lmask;
+        const M sm = u ? umask : lmask;
         const int j = rank_in(sm, v);
         o.x[j][0] = in.x[v][0]; o.x[j][1] = in.x[v][1]; o.x[j][2] = in.x[v][2];
         if constexpr (PT::has_q) {
@@ -233,7 +241,9 @@ template <class PT>
 __device__ __forceinline__ unsigned reduce_poly(const PT& P, double* mom, int order)
 {
     for (int i = 0; i < 10; ++i) mom[i] = 0.0;
-    uint64_t done[2] = {0ull, 0ull};
+    // one bit per (vertex, link); at least two words, as the density path has always used
+    constexpr int NW = (3 * PT::CAP + 63) / 64 > 2 ? (3 * PT::CAP + 63) / 64 : 2;
+    uint64_t done[NW] = {};
     for (int vs = 0; vs < P.nv; ++vs)
         for (int ks = 0; ks < 3; ++ks) {
             const int b0 = 3 * vs + ks;
@@ -298,7 +308,9 @@ __device__ __forceinline__ unsigned reduce_poly(const PT& P, double* mom, int or
 template <class PT>
 __device__ __forceinline__ unsigned adjoint_poly(const PT& P, double g, double (*A)[3])
 {
-    uint64_t done[2] = {0ull, 0ull};
+    // one bit per (vertex, link); at least two words, as the density path has always used
+    constexpr int NW = (3 * PT::CAP + 63) / 64 > 2 ? (3 * PT::CAP + 63) / 64 : 2;
+    uint64_t done[NW] = {};
     for (int vs = 0; vs < P.nv; ++vs)
         for (int ks = 0; ks < 3; ++ks) {
             const int b0 = 3 * vs + ks;
@@ -407,7 +419,9 @@ template <class PT>
 __device__ __forceinline__ unsigned reduce_about(const PT& P, const double* o, double* mom, int order)
 {
     for (int i = 0; i < 10; ++i) mom[i] = 0.0;
-    uint64_t done[2] = {0ull, 0ull};
+    // one bit per (vertex, link); at least two words, as the density path has always used
+    constexpr int NW = (3 * PT::CAP + 63) / 64 > 2 ? (3 * PT::CAP + 63) / 64 : 2;
+    uint64_t done[NW] = {};
     for (int vs = 0; vs < P.nv; ++vs)
         for (int ks = 0; ks < 3; ++ks) {
             const int b0 = 3 * vs + ks;
