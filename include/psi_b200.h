@@ -210,6 +210,43 @@ int psib_release_device_memory(void);
 int psib_voxels_density_noalloc(const psib_grid *grid, const double *tet_pos, const double *tet_mass,
                                 long long ntets, void *stream);
 
+/* Element queries: for each of nboxes boxes (6 doubles each: lo xyz, hi xyz)
+ * the elements whose box touches it (closed intervals) -- PSI.RStarTree(mesh)
+ * .query(box) (src/PSI.c:817-862) over the tree of src/rtree.c:48-73, whose
+ * elements are those that survive the cull against `window` (after their
+ * periodic unwrap, src/cpsi.c:309-341): the periodic box of a periodic mesh,
+ * +-1e30 for an open one (src/PSI.c:877-893).  No tree is built: the boxes are
+ * tested against every element on the GPU.
+ *
+ * offsets (nboxes + 1) receives the exclusive offsets of each box's results;
+ * with elements == NULL nothing else is written (a size query), else the
+ * element indices of box b go to elements[offsets[b] .. offsets[b + 1]) in
+ * descending index -- the order of the reference's tree while it is one leaf
+ * (at most 32 elements; larger trees return the same set in another order).
+ * PSIB_ERR_OVERFLOW when capacity is below the total.  Memory follows
+ * options->memory (host by default); device-memory calls run on
+ * options->stream and return when the results are written. */
+int psib_query_elements(const psib_mesh *mesh, const double window[2][3], const double *boxes, long long nboxes,
+                        long long *offsets, int *elements, long long capacity, const psib_options *opt);
+
+/* Phase-space samples of the sheet at each of npoints points (3 doubles each)
+ * -- PSI.VDF(mesh, sample_pos, tree, refine_tolerance, refine_max_lvl)
+ * (src/PSI.c:1022-1057, src/cpsi.c:177-275) for many points at once.  Every
+ * element whose box (over the elements that survive the cull against `window`:
+ * a tree's window as psib_query_elements describes it, or, as the reference
+ * uses when PSI.VDF is given no tree, the mesh's own box -- zero for an open
+ * mesh) contains the point is refined from its vertices as stored, with the
+ * absolute tolerance refine_tolerance; each of its tets that contains the
+ * point (barycentric coordinates >= 0, nonzero volume, src/geometry.c:335-389)
+ * gives one sample: density mass / volume (rho) and the velocity interpolated
+ * at the point (vel, 3 doubles).  Samples of point p go to
+ * [offsets[p], offsets[p + 1]), in the order element (descending), tet.
+ * rho == NULL: offsets only.  PSIB_ERR_OVERFLOW when capacity (samples) is
+ * below the total.  Memory and stream as psib_query_elements. */
+int psib_sample_vdf(const psib_mesh *mesh, const double window[2][3], const double *points, long long npoints,
+                    double refine_tolerance, int refine_max_lvl, long long *offsets, double *rho, double *vel,
+                    long long capacity, const psib_options *opt);
+
 /* Snapshot readers: a Gadget-2 (format 1) file as the periodic trilinear mesh
  * of PSI.Mesh(loader='gadget2') (src/mesh.c:35-160) or, with 64-bit particle
  * IDs and particles numbered in tiles of 4^3, loader='gevolution'

@@ -310,3 +310,105 @@ def load_snapshot(kind, path, flavour="gadget2"):
                     flat = tt[:, 0] + tn * tt[:, 1] + tn * tn * tt[:, 2]
                     conn[:, 4 * ii + 2 * jj + kk] = 64 * flat + to_flat[q[:, 0], q[:, 1], q[:, 2]]
     return pos, vel, mass, conn, box
+
+
+# ---- element queries and phase-space samples (src/rtree.c, src/cpsi.c:177-275) ----
+class _PsiRtree(C.Structure):
+    _fields_ = [("root", C.c_int), ("depth", C.c_int), ("allnodes", C.c_void_p), ("nodecap", C.c_int),
+                ("nnodes", C.c_int)]
+
+
+class _Rvec(C.Structure):
+    _fields_ = [("x", C.c_double), ("y", C.c_double), ("z", C.c_double)]
+
+
+def _meshes(pos, conn, vel=None, mass=None, periodic_box=None):
+    pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
+    conn = np.ascontiguousarray(conn, dtype=np.int32)
+    conn = conn.reshape(conn.shape[0], -1)
+    vel = np.zeros_like(pos) if vel is None else np.ascontiguousarray(vel, dtype=np.float64).reshape(-1, 3)
+    mass = np.ones(conn.shape[0]) if mass is None else np.ascontiguousarray(mass, dtype=np.float64).reshape(-1)
+    box = periodic_box if periodic_box is not None else ((0.0,) * 3, (0.0,) * 3)
+    keep = (pos, conn, vel, mass)
+    og = _OgMesh(elemtype=conn.shape[1], npart=pos.shape[0], nelem=conn.shape[0], pos=_dp(pos), vel=_dp(vel),
+                 mass=_dp(mass), conn=conn.ctypes.data_as(C.POINTER(C.c_int)), periodic=int(periodic_box is not None))
+    ps = _PsiMesh(elemtype=conn.shape[1], dim=3, pos=_dp(pos), vel=_dp(vel), mass=_dp(mass), npart=pos.shape[0],
+                  nelem=conn.shape[0], connectivity=conn.ctypes.data_as(C.POINTER(C.c_int)),
+                  periodic=int(periodic_box is not None))
+    for m in (og, ps):
+        m.box[0][:] = [float(v) for v in box[0]]
+        m.box[1][:] = [float(v) for v in box[1]]
+    return og, ps, keep, box
+
+
+def tree_window(periodic_box):
+    """The cull window of PSI.RStarTree(mesh) (src/PSI.c:865-896)."""
+    if periodic_box is not None:
+        return tuple(tuple(float(v) for v in b) for b in periodic_box)
+    return ((-1.0e30,) * 3, (1.0e30,) * 3)
+
+
+def query_elements(kind, pos, conn, window, box, periodic_box=None):
+    """Element indices whose unwrapped box touches `box`, over the elements that
+    survive the cull against `window`: PSI.RStarTree(...).query (src/PSI.c:817-862)."""
+    og, ps, keep, _ = _meshes(pos, conn, periodic_box=periodic_box)
+    lib = _lib(kind)
+    win = np.ascontiguousarray(window, dtype=np.float64).reshape(2, 3)
+    q = np.ascontiguousarray(box, dtype=np.float64).reshape(2, 3)
+    if kind != "reference":
+        lib.oracle_query.restype = C.c_longlong
+        n = lib.oracle_query(C.byref(og), _dp(win), _dp(q), None, C.c_longlong(0))
+        out = np.zeros(max(n, 1), dtype=np.int32)
+        lib.oracle_query(C.byref(og), _dp(win), _dp(q), out.ctypes.data_as(C.POINTER(C.c_int)), C.c_longlong(n))
+        return out[:n]
+    tree = _PsiRtree()
+    qry = C.create_string_buffer(1 << 15)
+    res = []
+    with _quiet_stdout():
+        lib.psi_rtree_from_mesh(C.byref(tree), C.byref(ps), _dp(win))
+        lib.psi_rtree_query_init(qry, C.byref(tree), _dp(q))
+        e = C.c_int()
+        while lib.psi_rtree_query_next(qry, C.byref(e)):
+            res.append(e.value)
+        lib.psi_rtree_destroy(C.byref(tree))
+    return np.array(res, dtype=np.int32)
+
+
+def sample_vdf(kind, pos, conn, point, vel=None, mass=None, periodic_box=None, window=None, reftol=1.0, maxlvl=0):
+    """PSI.VDF(mesh, sample_pos, tree, ...) (src/PSI.c:1022-1057): densities (n,) and
+    velocities (n, 3) of the streams at `point`.  window None: the tree PSI.VDF
+    builds itself, over the cull window mesh.box (zero for an open mesh); else the
+    window of the given tree (tree_window)."""
+    og, ps, keep, box = _meshes(pos, conn, vel, mass, periodic_box)
+    lib = _lib(kind)
+    s = np.ascontiguousarray(point, dtype=np.float64).reshape(3)
+    win = np.ascontiguousarray(box if window is None else window, dtype=np.float64).reshape(2, 3)
+    if kind != "reference":
+        f = lib.oracle_sample_vdf
+        f.restype = C.c_longlong
+        f.argtypes = [C.POINTER(_OgMesh), C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_double, C.c_int,
+                      C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_longlong]
+        n = f(C.byref(og), _dp(win), _dp(s), float(reftol), int(maxlvl), None, None, 0)
+        if n < 0:
+            raise ValueError("oracle_sample_vdf: unsupported element type")
+        rho, v = np.zeros(max(n, 1)), np.zeros((max(n, 1), 3))
+        f(C.byref(og), _dp(win), _dp(s), float(reftol), int(maxlvl), _dp(rho), _dp(v), n)
+        return rho[:n], v[:n]
+    tree = _PsiRtree() if window is not None else None
+    rp, vp, ns = C.POINTER(C.c_double)(), C.POINTER(C.c_double)(), C.c_int()
+    libc = C.CDLL(None)
+    with _quiet_stdout():
+        if tree is not None:
+            lib.psi_rtree_from_mesh(C.byref(tree), C.byref(ps), _dp(win))
+        lib.psi_sample_vdf.argtypes = [_Rvec, C.POINTER(_PsiMesh), C.c_void_p, C.POINTER(C.POINTER(C.c_double)),
+                                       C.POINTER(C.POINTER(C.c_double)), C.POINTER(C.c_int), C.c_double, C.c_int]
+        lib.psi_sample_vdf(_Rvec(*s), C.byref(ps), C.cast(C.byref(tree), C.c_void_p) if tree is not None else None,
+                           C.byref(rp), C.byref(vp), C.byref(ns), float(reftol), int(maxlvl))
+        if tree is not None:
+            lib.psi_rtree_destroy(C.byref(tree))
+    n = ns.value
+    rho = np.ctypeslib.as_array(rp, shape=(n,)).copy() if n else np.zeros(0)
+    v = np.ctypeslib.as_array(vp, shape=(n, 3)).copy() if n else np.zeros((0, 3))
+    libc.free(C.cast(rp, C.c_void_p))
+    libc.free(C.cast(vp, C.c_void_p))
+    return rho, v

@@ -995,3 +995,142 @@ int oracle_annihilation(og_grid *g, const og_mesh *m, double reftol, int max_lvl
     free(tb.mass);
     return rc;
 }
+
+/* ---- element queries and phase-space samples (src/rtree.c:48-125, src/cpsi.c:177-275,
+ *      src/geometry.c:335-389) ----
+ *
+ * The reference indexes the elements that survive the cull against a window
+ * (src/rtree.c:48-73: the periodic box for PSI.RStarTree of a periodic mesh,
+ * +-1e30 for an open one, the mesh's own box for the tree PSI.VDF builds when
+ * given none) by their unwrapped boxes, and answers a query box with every
+ * element whose box it touches (closed intervals).  This restatement scans the
+ * elements in descending index: the order the reference's tree returns while
+ * it is a single leaf (at most 32 elements). */
+
+static int elem_box(const og_mesh *m, const double (*window)[3], int e, double (*rb)[3])
+{
+    og_grid g;
+    memset(&g, 0, sizeof(g));
+    memcpy(g.win, window, sizeof(g.win));
+    double tp[27][3];
+    for (int v = 0; v < m->elemtype; ++v) memcpy(tp[v], &m->pos[3 * (size_t)m->conn[e * m->elemtype + v]], sizeof(tp[v]));
+    return aabb_periodic(tp, m->elemtype, rb, &g, m);
+}
+
+long long oracle_query(const og_mesh *m, const double (*window)[3], const double (*q)[3], int *out, long long cap)
+{
+    long long n = 0;
+    for (int e = m->nelem - 1; e >= 0; --e) {
+        double rb[2][3];
+        if (!elem_box(m, window, e, rb)) continue;
+        int touch = 1;
+        for (int i = 0; i < 3; ++i)
+            if (q[1][i] < rb[0][i] || q[0][i] > rb[1][i]) touch = 0;
+        if (!touch) continue;
+        if (n < cap) out[n] = e;
+        n++;
+    }
+    return n;
+}
+
+/* psi_barycentric (src/geometry.c:335-389): the four barycentric coordinates of
+ * s in the tet v (v[i] opposite coordinate i) as (w_i + s . n_i) / (their sum),
+ * with w_i the signed volume term of the other three vertices -- terms
+ * x_a (b x c).x summed in the reference's order -- and n_i the face normal of
+ * the face opposite v[i], the same edge vectors as its face planes; returns
+ * |sum| / 6, the tet's volume. */
+static ov_real ov_cx(const double *a, const double *b) { return (ov_real)a[1] * b[2] - (ov_real)a[2] * b[1]; }
+
+static void ov_cross(const double *a0, const double *a1, const double *b0, const double *b1, ov_real *n)
+{
+    ov_real A[3], B[3];
+    for (int i = 0; i < 3; ++i) {
+        A[i] = (ov_real)a1[i] - a0[i];
+        B[i] = (ov_real)b1[i] - b0[i];
+    }
+    n[0] = A[1] * B[2] - A[2] * B[1];
+    n[1] = A[2] * B[0] - A[0] * B[2];
+    n[2] = A[0] * B[1] - A[1] * B[0];
+}
+
+static ov_real ov_barycentric(const double (*v)[3], const double *s, ov_real *b)
+{
+    ov_real w[4], n[4][3];
+    w[0] = v[1][0] * ov_cx(v[2], v[3]) + v[2][0] * ov_cx(v[3], v[1]) + v[3][0] * ov_cx(v[1], v[2]);
+    w[1] = v[0][0] * ov_cx(v[3], v[2]) + v[2][0] * ov_cx(v[0], v[3]) + v[3][0] * ov_cx(v[2], v[0]);
+    w[2] = v[0][0] * ov_cx(v[1], v[3]) + v[1][0] * ov_cx(v[3], v[0]) + v[3][0] * ov_cx(v[0], v[1]);
+    w[3] = v[0][0] * ov_cx(v[2], v[1]) + v[1][0] * ov_cx(v[0], v[2]) + v[2][0] * ov_cx(v[1], v[0]);
+    ov_cross(v[1], v[3], v[1], v[2], n[0]);
+    ov_cross(v[0], v[2], v[2], v[3], n[1]);
+    ov_cross(v[3], v[1], v[3], v[0], n[2]);
+    ov_cross(v[2], v[0], v[0], v[1], n[3]);
+    ov_real tot = 0.0;
+    for (int i = 0; i < 4; ++i) {
+        b[i] = w[i];
+        for (int j = 0; j < 3; ++j) b[i] += s[j] * n[i][j];
+        tot += b[i];
+    }
+    for (int i = 0; i < 4; ++i) b[i] /= tot;
+    ov_real vol = ((ov_real)1 / 6) * tot;
+    return vol < 0 ? -vol : vol;
+}
+
+/* psi_sample_vdf (src/cpsi.c:177-275): for every element whose box contains the
+ * point (a query with the degenerate box [s, s]), its tets -- refined from its
+ * vertices as stored, with the tolerance reftol itself -- that contain the
+ * point give one sample each: density mass / volume and the velocity
+ * interpolated at the point.  Returns the number of samples; writes up to cap. */
+long long oracle_sample_vdf(const og_mesh *m, const double (*window)[3], const double *s, double reftol, int max_lvl,
+                            double *rho, double *vel, long long cap)
+{
+    static og_counters unused; /* the element refinement reports errors here */
+    g_cnt = &unused;
+    if (m->elemtype != 4 && m->elemtype != 8) return -1;
+    if (max_lvl > 6) max_lvl = 6;
+    ov_tetbuf tb;
+    memset(&tb, 0, sizeof(tb));
+    tb.max_lvl = max_lvl;
+    tb.ptol2 = reftol * reftol;
+    const double q[2][3] = {{s[0], s[1], s[2]}, {s[0], s[1], s[2]}};
+    long long n = 0;
+    for (int e = m->nelem - 1; e >= 0; --e) {
+        double rb[2][3];
+        if (!elem_box(m, window, e, rb)) continue;
+        int touch = 1;
+        for (int i = 0; i < 3; ++i)
+            if (q[1][i] < rb[0][i] || q[0][i] > rb[1][i]) touch = 0;
+        if (!touch) continue;
+        double tp[8][3], tu[8][3];
+        for (int v = 0; v < m->elemtype; ++v) {
+            int id = m->conn[e * m->elemtype + v];
+            memcpy(tp[v], &m->pos[3 * (size_t)id], sizeof(tp[v]));
+            memcpy(tu[v], &m->vel[3 * (size_t)id], sizeof(tu[v]));
+        }
+        if (element_tets(&tb, (const double(*)[3])tp, (const double(*)[3])tu, m->mass[e], m->elemtype)) {
+            n = -1;
+            break;
+        }
+        for (int t = 0; t < tb.num; ++t) {
+            ov_real b[4];
+            ov_real vol = ov_barycentric((const double(*)[3])tb.pos[4 * t], s, b);
+            if (vol <= 0.0) continue;
+            int inside = 1;
+            for (int i = 0; i < 4; ++i)
+                if (b[i] < 0.0) inside = 0;
+            if (!inside) continue;
+            if (n < cap) {
+                for (int i = 0; i < 3; ++i) {
+                    ov_real u = 0.0;
+                    for (int j = 0; j < 4; ++j) u += b[j] * tb.vel[4 * t + j][i];
+                    vel[3 * n + i] = (double)u;
+                }
+                rho[n] = (double)(tb.mass[t] / vol);
+            }
+            n++;
+        }
+    }
+    free(tb.pos);
+    free(tb.vel);
+    free(tb.mass);
+    return n;
+}

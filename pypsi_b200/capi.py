@@ -55,6 +55,12 @@ lib.psib_voxels_adjoint.restype = C.c_int
 lib.psib_voxels_batch.argtypes = [C.POINTER(Grid), C.POINTER(Mesh), C.c_int, C.c_int, C.c_double, C.c_int,
                                   C.POINTER(Options)]
 lib.psib_voxels_batch.restype = C.c_int
+lib.psib_query_elements.argtypes = [C.POINTER(Mesh), C.c_void_p, C.c_void_p, C.c_longlong, C.c_void_p, C.c_void_p,
+                                    C.c_longlong, C.POINTER(Options)]
+lib.psib_query_elements.restype = C.c_int
+lib.psib_sample_vdf.argtypes = [C.POINTER(Mesh), C.c_void_p, C.c_void_p, C.c_longlong, C.c_double, C.c_int, C.c_void_p,
+                                C.c_void_p, C.c_void_p, C.c_longlong, C.POINTER(Options)]
+lib.psib_sample_vdf.restype = C.c_int
 lib.psib_last_error.restype = C.c_char_p
 lib.psib_release_device_memory.restype = C.c_int
 
@@ -231,3 +237,80 @@ def autotune_batch(cutouts: list, candidates=(8 << 20, 16 << 20, 32 << 20, 64 <<
         for t in c["fields"].values():
             t.zero_()
     return best
+
+
+def tree_window(periodic_box=None):
+    """The cull window of PSI.RStarTree(mesh): the periodic box, or +-1e30."""
+    if periodic_box is not None:
+        return (tuple(float(v) for v in periodic_box[0]), tuple(float(v) for v in periodic_box[1]))
+    return ((-1.0e30,) * 3, (1.0e30,) * 3)
+
+
+def _window_array(window):
+    import numpy as np
+
+    return np.ascontiguousarray(np.array([list(window[0]), list(window[1])], dtype=np.float64))
+
+
+def sample_vdf(points, pos, connectivity=None, vel=None, mass=None, block_dims=None, periodic_box=None, window=None,
+               refine_tolerance=1.0, refine_max_lvl=0):
+    """Phase-space samples at many points at once (psib_sample_vdf): the
+    batched PSI.VDF.  numpy arrays (host memory) or CUDA tensors (device
+    memory, on the current stream).  window: a tree's cull window (default:
+    tree_window(periodic_box), as PSI.RStarTree(mesh) has).  Returns
+    (offsets (npoints + 1,), rho (n,), vel (n, 3)); point p's samples are
+    [offsets[p], offsets[p + 1])."""
+    import numpy as np
+
+    device = hasattr(points, "is_cuda") and points.is_cuda
+    win = _window_array(tree_window(periodic_box) if window is None else window)
+    if device:
+        m = mesh_from_tensors(pos, vel, mass, connectivity, block_dims, periodic_box)
+    else:
+        pos = np.ascontiguousarray(pos, dtype=np.float64)
+        vel = None if vel is None else np.ascontiguousarray(vel, dtype=np.float64)
+        mass = None if mass is None else np.ascontiguousarray(mass, dtype=np.float64)
+        connectivity = None if connectivity is None else np.ascontiguousarray(connectivity, dtype=np.int32)
+        npart = pos.size // 3
+        if connectivity is not None:
+            et, nelem = connectivity.shape[-1], connectivity.size // connectivity.shape[-1]
+        else:
+            et, nelem = 8, int(np.prod([b if periodic_box is not None else b - 1 for b in block_dims]))
+        m = make_mesh(npart, nelem, pos.ctypes.data, None if vel is None else vel.ctypes.data,
+                      None if mass is None else mass.ctypes.data,
+                      None if connectivity is None else connectivity.ctypes.data, et, block_dims, periodic_box)
+    npts = points.shape[0]
+    if device:
+        import torch
+
+        s = torch.cuda.current_stream()
+        o = Options(precision=PSIB_FP64, memory=PSIB_DEVICE, device=-1, stream=C.c_void_p(s.cuda_stream))
+        off = torch.zeros(npts + 1, dtype=torch.int64, device=points.device)
+        rc = lib.psib_sample_vdf(C.byref(m), win.ctypes.data, points.data_ptr(), npts, float(refine_tolerance),
+                                 int(refine_max_lvl), off.data_ptr(), None, None, 0, C.byref(o))
+        if rc != 0:
+            raise PsibError(rc)
+        n = int(off[-1].item())
+        rho = torch.empty(max(n, 1), dtype=torch.float64, device=points.device)
+        v = torch.empty((max(n, 1), 3), dtype=torch.float64, device=points.device)
+        if n:
+            rc = lib.psib_sample_vdf(C.byref(m), win.ctypes.data, points.data_ptr(), npts, float(refine_tolerance),
+                                     int(refine_max_lvl), off.data_ptr(), rho.data_ptr(), v.data_ptr(), n, C.byref(o))
+            if rc != 0:
+                raise PsibError(rc)
+        return off, rho[:n], v[:n]
+    points = np.ascontiguousarray(points, dtype=np.float64)
+    o = Options(precision=PSIB_FP64, memory=PSIB_HOST, device=-1)
+    off = np.zeros(npts + 1, dtype=np.int64)
+    rc = lib.psib_sample_vdf(C.byref(m), win.ctypes.data, points.ctypes.data, npts, float(refine_tolerance),
+                             int(refine_max_lvl), off.ctypes.data, None, None, 0, C.byref(o))
+    if rc != 0:
+        raise PsibError(rc)
+    n = int(off[-1])
+    rho, v = np.zeros(max(n, 1)), np.zeros((max(n, 1), 3))
+    if n:
+        rc = lib.psib_sample_vdf(C.byref(m), win.ctypes.data, points.ctypes.data, npts, float(refine_tolerance),
+                                 int(refine_max_lvl), off.ctypes.data, rho.ctypes.data, v.ctypes.data, n, C.byref(o))
+        if rc != 0:
+            raise PsibError(rc)
+    return off, rho[:n], v[:n]

@@ -307,6 +307,105 @@ cudaError_t launch_ann_chunk_bounds(const long long* tp_excl, long long nslot, l
     return cudaGetLastError();
 }
 
+// ---- queries (PSI.RStarTree.query, PSI.VDF) ----
+
+// Every (box, element) pair: the closed-interval test of the reference's
+// query (src/rtree.c:108-111) against each kept element's box.
+template <bool EMIT>
+__global__ void k_query_boxes(AnnArgs a)
+{
+    const long long total = a.nq * a.nelem;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += stride) {
+        const long long q = i / a.nelem, e = i % a.nelem;
+        if (!kept_elem(a, e)) continue;
+        const double* b = a.qry + 6 * q;
+        bool touch = true;
+        for (int c = 0; c < 3; ++c)
+            if (b[3 + c] < a.ebox[6 * e + c] || b[c] > a.ebox[6 * e + 3 + c]) touch = false;
+        if (!touch) continue;
+        if (EMIT) {
+            const unsigned long long w = atomicAdd(a.q_n, 1ull);
+            a.q_key[w] = ((unsigned long long)q << 32) | (0xFFFFFFFFull - (unsigned long long)e);
+        } else {
+            atomicAdd((unsigned long long*)&a.q_cnt[q], 1ull);
+        }
+    }
+}
+
+cudaError_t launch_query_boxes(const AnnArgs& a, bool emit, cudaStream_t s)
+{
+    if (emit) k_query_boxes<true><<<grid_for(a.nq * a.nelem, 256), 256, 0, s>>>(a);
+    else k_query_boxes<false><<<grid_for(a.nq * a.nelem, 256), 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+// A point against the elements registered in its cell: every element whose
+// box contains the point (the degenerate query box of src/cpsi.c:212-216)
+// is registered there.
+template <bool EMIT>
+__global__ void k_query_points(AnnArgs a)
+{
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < a.nq; q += stride) {
+        const double* s = a.qry + 3 * q;
+        const unsigned long long k =
+            (unsigned long long)((cell_of(a.cg, 0, s[0]) * a.cg.n[1] + cell_of(a.cg, 1, s[1])) * a.cg.n[2] +
+                                 cell_of(a.cg, 2, s[2]));
+        long long lo = 0, hi = a.nruns; // the run whose key is k, if any
+        while (lo < hi) {
+            const long long mid = (lo + hi) >> 1;
+            if (a.run_key[mid] < k) lo = mid + 1;
+            else hi = mid;
+        }
+        long long n = 0, w = EMIT ? a.q_off[q] : 0;
+        if (lo < a.nruns && a.run_key[lo] == k) {
+            for (long long j = a.run_off[lo]; j < a.run_off[lo] + a.run_cnt[lo]; ++j) {
+                const long long e = a.reg_elem[j];
+                bool in = true;
+                for (int c = 0; c < 3; ++c)
+                    if (s[c] < a.ebox[6 * e + c] || s[c] > a.ebox[6 * e + 3 + c]) in = false;
+                if (!in) continue;
+                if (EMIT) a.q_key[w++] = ((unsigned long long)q << 32) | (0xFFFFFFFFull - (unsigned long long)e);
+                n++;
+            }
+        }
+        if (!EMIT) a.q_cnt[q] = n;
+    }
+}
+
+cudaError_t launch_query_points(const AnnArgs& a, bool emit, cudaStream_t s)
+{
+    if (emit) k_query_points<true><<<grid_for(a.nq, 128), 128, 0, s>>>(a);
+    else k_query_points<false><<<grid_for(a.nq, 128), 128, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+__global__ void k_keys_elem(const unsigned long long* keys, long long n, int* out)
+{
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += stride)
+        out[i] = (int)(0xFFFFFFFFull - (keys[i] & 0xFFFFFFFFull));
+}
+
+cudaError_t launch_keys_elem(const unsigned long long* keys, long long n, int* out, cudaStream_t s)
+{
+    k_keys_elem<<<grid_for(n, 256), 256, 0, s>>>(keys, n, out);
+    return cudaGetLastError();
+}
+
+__global__ void k_gather_ll(const long long* src, const long long* idx, long long n, long long* out)
+{
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += stride) out[i] = src[idx[i]];
+}
+
+cudaError_t launch_gather_ll(const long long* src, const long long* idx, long long n, long long* out, cudaStream_t s)
+{
+    k_gather_ll<<<grid_for(n, 256), 256, 0, s>>>(src, idx, n, out);
+    return cudaGetLastError();
+}
+
 // ---- the clip of one tet pair ----
 
 // Face plane n.x + d >= 0 of a tet (src/geometry.c:503-558): n = A x B with

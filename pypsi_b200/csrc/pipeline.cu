@@ -123,6 +123,8 @@ struct Ctx {
     DevBuf a_cnt, a_off, a_ebox, a_tets_a, a_tets_b, a_stats, a_reg_cnt, a_reg_off, a_reg_key, a_reg_elem,
         a_reg_key_s, a_reg_elem_s, a_run_key, a_run_cnt, a_run_off, a_run_lo, a_run_hi, a_pair_cnt, a_pair_off,
         a_pair_key, a_pair_key_s, a_na, a_aoff, a_tp_cnt, a_tp_excl, a_bounds, a_tpairs, a_deep;
+    // element queries and phase-space samples
+    DevBuf q_in, q_cnt, q_off, q_key, q_key_s, q_out, s_cnt, s_off, s_offs, s_rho, s_vel;
     cudaGraphExec_t pass_exec = nullptr; // one breadth-first pass as a CUDA graph
     PassKey pass_key{};                  // the arguments it was recorded with
     std::vector<DevBuf*> all()
@@ -136,7 +138,8 @@ struct Ctx {
                 &qwin[2], &btab, &igrid, &passes, &a_cnt, &a_off, &a_ebox, &a_tets_a, &a_tets_b, &a_stats,
                 &a_reg_cnt, &a_reg_off, &a_reg_key, &a_reg_elem, &a_reg_key_s, &a_reg_elem_s, &a_run_key,
                 &a_run_cnt, &a_run_off, &a_run_lo, &a_run_hi, &a_pair_cnt, &a_pair_off, &a_pair_key,
-                &a_pair_key_s, &a_na, &a_aoff, &a_tp_cnt, &a_tp_excl, &a_bounds, &a_tpairs, &a_deep};
+                &a_pair_key_s, &a_na, &a_aoff, &a_tp_cnt, &a_tp_excl, &a_bounds, &a_tpairs, &a_deep, &q_in, &q_cnt,
+                &q_off, &q_key, &q_key_s, &q_out, &s_cnt, &s_off, &s_offs, &s_rho, &s_vel};
     }
 };
 
@@ -1038,6 +1041,104 @@ double from_ord(unsigned long long o)
     return x;
 }
 
+// The cell index over the kept element boxes (aa.nelem, aa.ebox and the kept
+// flags aa.cnt_a / aa.cnt_b set): a uniform grid of cells about one mean
+// element box wide (at most 1024 per axis); every kept element registered in
+// the cells its box covers, sorted by cell; each registration's cell run
+// (aa.run_lo / run_hi) and the runs themselves (aa.run_key / run_off /
+// run_cnt, aa.nruns).  kept = the number of kept elements (0: no index).
+int build_cells(Ctx& C, AnnArgs& aa, cudaStream_t st, long long& klaunch, long long& kept)
+{
+    const long long ne = aa.nelem;
+    RET(ensure(C.a_stats, 16 * 8));
+    CK(cudaMemsetAsync(C.a_stats.p, 0xFF, 3 * 8, st));
+    CK(cudaMemsetAsync(C.a_stats.as<char>() + 24, 0, 13 * 8, st));
+    unsigned long long* bs = C.a_stats.as<unsigned long long>();
+    CK(launch_ann_box_stats(aa, bs, (double*)(bs + 8), st));
+    klaunch++;
+    unsigned long long hb[16];
+    CK(cudaMemcpyAsync(hb, bs, sizeof(hb), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    kept = (long long)hb[6];
+    if (kept == 0) return PSIB_OK;
+    long long ncell = 1;
+    for (int i = 0; i < 3; ++i) {
+        const double lo = from_ord(hb[i]), hi = from_ord(hb[3 + i]);
+        double ext;
+        memcpy(&ext, &hb[8 + i], 8);
+        const double range = hi - lo;
+        // cells about one mean element box wide, at most 1024 per axis
+        double h = ext / (double)kept;
+        if (!(h >= range / 1024.0)) h = range / 1024.0;
+        if (!(h > 0.0) || !std::isfinite(h)) h = range > 0.0 && std::isfinite(range) ? range : 1.0;
+        aa.cg.o[i] = std::isfinite(lo) ? lo : 0.0;
+        aa.cg.h[i] = h;
+        long long n = std::isfinite(range) ? (long long)(range / h) + 1 : 1;
+        aa.cg.n[i] = n < 1 ? 1 : (n > 1024 ? 1024 : n);
+        ncell *= aa.cg.n[i];
+    }
+
+    // ---- cell registrations, sorted by cell ----
+    RET(ensure(C.a_reg_cnt, (size_t)(ne + 1) * sizeof(long long)));
+    RET(ensure(C.a_reg_off, (size_t)(ne + 1) * sizeof(long long)));
+    aa.reg_cnt = C.a_reg_cnt.as<long long>();
+    CK(launch_ann_cells(aa, false, st));
+    CK(cudaMemsetAsync(aa.reg_cnt + ne, 0, sizeof(long long), st));
+    RET(excl_scan(C, aa.reg_cnt, C.a_reg_off.as<long long>(), ne + 1, st));
+    long long nreg = 0;
+    RET(read_dev(C.a_reg_off.as<long long>() + ne, nreg, st));
+    if (nreg >= (1ll << 31)) return fail(PSIB_ERR_OVERFLOW, "too many cell registrations (%lld)", nreg);
+    RET(ensure(C.a_reg_key, (size_t)nreg * 8));
+    RET(ensure(C.a_reg_elem, (size_t)nreg * 4));
+    RET(ensure(C.a_reg_key_s, (size_t)nreg * 8));
+    RET(ensure(C.a_reg_elem_s, (size_t)nreg * 4));
+    aa.reg_off = C.a_reg_off.as<long long>();
+    aa.reg_key = C.a_reg_key.as<unsigned long long>();
+    aa.reg_elem = C.a_reg_elem.as<int>();
+    CK(launch_ann_cells(aa, true, st));
+    klaunch += 2;
+    {
+        size_t tb = 0;
+        const int cb = bits_for((unsigned long long)ncell);
+        CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, aa.reg_key, C.a_reg_key_s.as<unsigned long long>(), aa.reg_elem,
+                                           C.a_reg_elem_s.as<int>(), (int)nreg, 0, cb, st));
+        RET(ensure(C.cub_tmp, tb));
+        CK(cub::DeviceRadixSort::SortPairs(C.cub_tmp.p, tb, aa.reg_key, C.a_reg_key_s.as<unsigned long long>(),
+                                           aa.reg_elem, C.a_reg_elem_s.as<int>(), (int)nreg, 0, cb, st));
+    }
+    aa.reg_key = C.a_reg_key_s.as<unsigned long long>();
+    aa.reg_elem = C.a_reg_elem_s.as<int>();
+    aa.nreg = nreg;
+    // each registration's cell run
+    RET(ensure(C.a_run_key, (size_t)nreg * 8));
+    RET(ensure(C.a_run_cnt, (size_t)nreg * 4 + 8));
+    RET(ensure(C.a_run_off, (size_t)nreg * 8));
+    RET(ensure(C.a_run_lo, (size_t)nreg * 8));
+    RET(ensure(C.a_run_hi, (size_t)nreg * 8));
+    {
+        int* d_nruns = (int*)(C.a_run_cnt.as<char>() + (size_t)nreg * 4);
+        size_t tb = 0;
+        CK(cub::DeviceRunLengthEncode::Encode(nullptr, tb, aa.reg_key, C.a_run_key.as<unsigned long long>(),
+                                              C.a_run_cnt.as<int>(), d_nruns, (int)nreg, st));
+        RET(ensure(C.cub_tmp, tb));
+        CK(cub::DeviceRunLengthEncode::Encode(C.cub_tmp.p, tb, aa.reg_key, C.a_run_key.as<unsigned long long>(),
+                                              C.a_run_cnt.as<int>(), d_nruns, (int)nreg, st));
+        int nruns = 0;
+        RET(read_dev(d_nruns, nruns, st));
+        RET(excl_scan(C, C.a_run_cnt.as<int>(), C.a_run_off.as<long long>(), nruns, st));
+        CK(launch_ann_runs(C.a_run_cnt.as<unsigned>(), C.a_run_off.as<long long>(), nruns, C.a_run_lo.as<long long>(),
+                           C.a_run_hi.as<long long>(), st));
+        klaunch++;
+        aa.nruns = nruns;
+    }
+    aa.run_key = C.a_run_key.as<unsigned long long>();
+    aa.run_off = C.a_run_off.as<long long>();
+    aa.run_cnt = C.a_run_cnt.as<int>();
+    aa.run_lo = C.a_run_lo.as<long long>();
+    aa.run_hi = C.a_run_hi.as<long long>();
+    return PSIB_OK;
+}
+
 // Annihilation mode (src/cpsi.c:115-158): elements -> tets of both sides ->
 // element pairs from a uniform cell grid -> tet pairs in the reference's order
 // (e, e1 descending, t, t1), streamed in chunks -> one clip thread per tet pair
@@ -1141,88 +1242,10 @@ int run_annihilation(Call& c)
     aa.tets_a = ta.tets_a;
     aa.tets_b = ta.tets_b;
     aa.status = (unsigned*)&sm[S_STATUS];
-    RET(ensure(C.a_stats, 16 * 8));
-    CK(cudaMemsetAsync(C.a_stats.p, 0xFF, 3 * 8, st));
-    CK(cudaMemsetAsync(C.a_stats.as<char>() + 24, 0, 13 * 8, st));
-    unsigned long long* bs = C.a_stats.as<unsigned long long>();
-    CK(launch_ann_box_stats(aa, bs, (double*)(bs + 8), st));
-    klaunch++;
-    unsigned long long hb[16];
-    CK(cudaMemcpyAsync(hb, bs, sizeof(hb), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    const long long kept = (long long)hb[6];
+    long long kept = 0;
+    RET(build_cells(C, aa, st, klaunch, kept));
     if (kept == 0) return finish();
-    long long ncell = 1;
-    for (int i = 0; i < 3; ++i) {
-        const double lo = from_ord(hb[i]), hi = from_ord(hb[3 + i]);
-        double ext;
-        memcpy(&ext, &hb[8 + i], 8);
-        const double range = hi - lo;
-        // cells about one mean element box wide, at most 1024 per axis
-        double h = ext / (double)kept;
-        if (!(h >= range / 1024.0)) h = range / 1024.0;
-        if (!(h > 0.0) || !std::isfinite(h)) h = range > 0.0 && std::isfinite(range) ? range : 1.0;
-        aa.cg.o[i] = std::isfinite(lo) ? lo : 0.0;
-        aa.cg.h[i] = h;
-        long long n = std::isfinite(range) ? (long long)(range / h) + 1 : 1;
-        aa.cg.n[i] = n < 1 ? 1 : (n > 1024 ? 1024 : n);
-        ncell *= aa.cg.n[i];
-    }
-
-    // ---- cell registrations, sorted by cell ----
-    RET(ensure(C.a_reg_cnt, (size_t)(ne + 1) * sizeof(long long)));
-    RET(ensure(C.a_reg_off, (size_t)(ne + 1) * sizeof(long long)));
-    aa.reg_cnt = C.a_reg_cnt.as<long long>();
-    CK(launch_ann_cells(aa, false, st));
-    CK(cudaMemsetAsync(aa.reg_cnt + ne, 0, sizeof(long long), st));
-    RET(excl_scan(C, aa.reg_cnt, C.a_reg_off.as<long long>(), ne + 1, st));
-    long long nreg = 0;
-    RET(read_dev(C.a_reg_off.as<long long>() + ne, nreg, st));
-    if (nreg >= (1ll << 31)) return fail(PSIB_ERR_OVERFLOW, "too many cell registrations (%lld)", nreg);
-    RET(ensure(C.a_reg_key, (size_t)nreg * 8));
-    RET(ensure(C.a_reg_elem, (size_t)nreg * 4));
-    RET(ensure(C.a_reg_key_s, (size_t)nreg * 8));
-    RET(ensure(C.a_reg_elem_s, (size_t)nreg * 4));
-    aa.reg_off = C.a_reg_off.as<long long>();
-    aa.reg_key = C.a_reg_key.as<unsigned long long>();
-    aa.reg_elem = C.a_reg_elem.as<int>();
-    CK(launch_ann_cells(aa, true, st));
-    klaunch += 2;
-    {
-        size_t tb = 0;
-        const int cb = bits_for((unsigned long long)ncell);
-        CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, aa.reg_key, C.a_reg_key_s.as<unsigned long long>(), aa.reg_elem,
-                                           C.a_reg_elem_s.as<int>(), (int)nreg, 0, cb, st));
-        RET(ensure(C.cub_tmp, tb));
-        CK(cub::DeviceRadixSort::SortPairs(C.cub_tmp.p, tb, aa.reg_key, C.a_reg_key_s.as<unsigned long long>(),
-                                           aa.reg_elem, C.a_reg_elem_s.as<int>(), (int)nreg, 0, cb, st));
-    }
-    aa.reg_key = C.a_reg_key_s.as<unsigned long long>();
-    aa.reg_elem = C.a_reg_elem_s.as<int>();
-    aa.nreg = nreg;
-    // each registration's cell run
-    RET(ensure(C.a_run_key, (size_t)nreg * 8));
-    RET(ensure(C.a_run_cnt, (size_t)nreg * 4 + 8));
-    RET(ensure(C.a_run_off, (size_t)nreg * 8));
-    RET(ensure(C.a_run_lo, (size_t)nreg * 8));
-    RET(ensure(C.a_run_hi, (size_t)nreg * 8));
-    {
-        int* d_nruns = (int*)(C.a_run_cnt.as<char>() + (size_t)nreg * 4);
-        size_t tb = 0;
-        CK(cub::DeviceRunLengthEncode::Encode(nullptr, tb, aa.reg_key, C.a_run_key.as<unsigned long long>(),
-                                              C.a_run_cnt.as<int>(), d_nruns, (int)nreg, st));
-        RET(ensure(C.cub_tmp, tb));
-        CK(cub::DeviceRunLengthEncode::Encode(C.cub_tmp.p, tb, aa.reg_key, C.a_run_key.as<unsigned long long>(),
-                                              C.a_run_cnt.as<int>(), d_nruns, (int)nreg, st));
-        int nruns = 0;
-        RET(read_dev(d_nruns, nruns, st));
-        RET(excl_scan(C, C.a_run_cnt.as<int>(), C.a_run_off.as<long long>(), nruns, st));
-        CK(launch_ann_runs(C.a_run_cnt.as<unsigned>(), C.a_run_off.as<long long>(), nruns, C.a_run_lo.as<long long>(),
-                           C.a_run_hi.as<long long>(), st));
-        klaunch++;
-    }
-    aa.run_lo = C.a_run_lo.as<long long>();
-    aa.run_hi = C.a_run_hi.as<long long>();
+    const long long nreg = aa.nreg;
 
     // ---- element pairs, sorted (e ascending, e1 descending) ----
     RET(ensure(C.a_pair_cnt, (size_t)(nreg + 1) * sizeof(long long)));
@@ -1464,6 +1487,28 @@ int copy_mesh_in(Call& c, Ctx& C, const psib_mesh& mesh, cudaStream_t st)
     return PSIB_OK;
 }
 
+int validate_mesh(const psib_mesh* m)
+{
+    if (!m) return fail(PSIB_ERR_ARG, "mesh is required");
+    if (m->elemtype != 4 && m->elemtype != 8 && m->elemtype != 27)
+        return fail(PSIB_ERR_ARG, "elemtype must be 4, 8 or 27");
+    if (m->nelem < 0 || m->npart < 0) return fail(PSIB_ERR_ARG, "negative mesh size");
+    if (m->nelem >= (1ll << 31) || m->npart >= (1ll << 31))
+        return fail(PSIB_ERR_ARG, "meshes of 2^31 elements or particles are not supported");
+    if (m->nelem > 0 && !m->pos) return fail(PSIB_ERR_ARG, "pos is required");
+    if (!m->connectivity) {
+        if (m->elemtype != 8) return fail(PSIB_ERR_ARG, "implicit connectivity needs elemtype 8");
+        long long np = 1, nel = 1;
+        for (int i = 0; i < 3; ++i) {
+            if (m->block_dims[i] <= 0) return fail(PSIB_ERR_ARG, "connectivity or block_dims is required");
+            np *= m->block_dims[i];
+            nel *= m->periodic ? m->block_dims[i] : m->block_dims[i] - 1;
+        }
+        if (np != m->npart || nel != m->nelem) return fail(PSIB_ERR_ARG, "block_dims disagree with npart/nelem");
+    }
+    return PSIB_OK;
+}
+
 int validate(const psib_grid* g, const psib_mesh* m, int mode, const psib_options* o)
 {
     if (!g || !m) return fail(PSIB_ERR_ARG, "grid and mesh are required");
@@ -1481,27 +1526,267 @@ int validate(const psib_grid* g, const psib_mesh* m, int mode, const psib_option
     if (g->fields[PSIB_XV] && !(g->fields[PSIB_X] && g->fields[PSIB_V]))
         return fail(PSIB_ERR_ARG, "field 'xv' requires fields 'x' and 'v'");
     if (g->fields[PSIB_VV] && !g->fields[PSIB_V]) return fail(PSIB_ERR_ARG, "field 'vv' requires field 'v'");
-    if (m->elemtype != 4 && m->elemtype != 8 && m->elemtype != 27)
-        return fail(PSIB_ERR_ARG, "elemtype must be 4, 8 or 27");
-    if (m->nelem < 0 || m->npart < 0) return fail(PSIB_ERR_ARG, "negative mesh size");
-    if (m->nelem >= (1ll << 31) || m->npart >= (1ll << 31))
-        return fail(PSIB_ERR_ARG, "meshes of 2^31 elements or particles are not supported");
-    if (m->nelem > 0 && !m->pos) return fail(PSIB_ERR_ARG, "pos is required");
-    if (!m->connectivity) {
-        if (m->elemtype != 8) return fail(PSIB_ERR_ARG, "implicit connectivity needs elemtype 8");
-        long long np = 1, nel = 1;
-        for (int i = 0; i < 3; ++i) {
-            if (m->block_dims[i] <= 0) return fail(PSIB_ERR_ARG, "connectivity or block_dims is required");
-            np *= m->block_dims[i];
-            nel *= m->periodic ? m->block_dims[i] : m->block_dims[i] - 1;
-        }
-        if (np != m->npart || nel != m->nelem) return fail(PSIB_ERR_ARG, "block_dims disagree with npart/nelem");
-    }
+    RET(validate_mesh(m));
     if (o && o->refine_mode != PSIB_REFINE_MIDPOINT && o->refine_mode != PSIB_REFINE_STRETCH)
         return fail(PSIB_ERR_ARG, "invalid refine_mode %d", o->refine_mode);
     if (o && o->precision != PSIB_FP64 && o->precision != PSIB_MIXED && o->precision != PSIB_FP64_CENTRAL)
         return fail(PSIB_ERR_ARG, "invalid precision %d", o->precision);
     return PSIB_OK;
+}
+
+// ---- element queries and phase-space samples ----
+
+// A query call: device, context, stream and the mesh in device memory (copied
+// in for host-memory calls; device-memory calls run on the library's stream
+// fenced to the caller's).
+struct QueryCall {
+    Call c;
+    Ctx* C = nullptr;
+    bool host = true;
+    cudaStream_t user = nullptr;
+};
+
+int query_begin(QueryCall& q, const psib_mesh* mesh, const psib_options* opt)
+{
+    g_err.clear();
+    RET(validate_mesh(mesh));
+    psib_options o = {};
+    o.memory = PSIB_HOST;
+    o.device = -1;
+    if (opt) o = *opt;
+    if (o.memory != PSIB_HOST && o.memory != PSIB_DEVICE) return fail(PSIB_ERR_ARG, "invalid memory kind %d", o.memory);
+    if (psib_device_count() <= 0) return fail(PSIB_ERR_NODEVICE, "no CUDA device is visible");
+    int dev = o.device;
+    if (o.memory == PSIB_DEVICE || dev < 0) CK(cudaGetDevice(&dev));
+    CK(cudaSetDevice(dev));
+    RET(get_ctx(dev, &q.C));
+    q.host = o.memory == PSIB_HOST;
+    q.c = Call{};
+    q.c.mesh = mesh;
+    q.c.C = q.C;
+    q.c.st = q.C->own;
+    if (q.host) {
+        if (mesh->nelem > 0) RET(copy_mesh_in(q.c, *q.C, *mesh, q.c.st));
+    } else {
+        q.user = (cudaStream_t)o.stream;
+        RET(enter_own_stream(*q.C, q.user));
+        q.c.pos = mesh->pos;
+        q.c.vel = mesh->vel;
+        q.c.mass = mesh->mass;
+        q.c.conn = mesh->connectivity;
+    }
+    return PSIB_OK;
+}
+
+int query_end(QueryCall& q, int rc)
+{
+    if (!q.host && q.C) {
+        const int r = leave_own_stream(*q.C, q.user);
+        if (rc == PSIB_OK) rc = r;
+    }
+    if (rc == PSIB_OK) CK(cudaStreamSynchronize(q.c.st));
+    return rc;
+}
+
+// The kept elements (cull against `window`) and their unwrapped boxes.
+int query_elements_stage(QueryCall& q, const double (*window)[3], double reftol, AnnArgs& aa, unsigned long long* sm)
+{
+    Ctx& C = *q.C;
+    const psib_mesh& m = *q.c.mesh;
+    const long long ne = m.nelem;
+    cudaStream_t st = q.c.st;
+    psib_grid gw = {};
+    for (int i = 0; i < 3; ++i) {
+        gw.n[i] = 1;
+        gw.window[0][i] = window[0][i];
+        gw.window[1][i] = window[1][i];
+        gw.d[i] = 1.0;
+    }
+    MeshDev md = mesh_dev(m, gw, q.c.pos, q.c.vel, q.c.mass, q.c.conn, 1.0, nullptr);
+    md.ptol2 = reftol * reftol; // psi_tet_buffer_init(&tetbuf, reftol, ...): the tolerance itself (src/cpsi.c:198)
+    RET(ensure(C.a_cnt, (size_t)2 * (ne + 1) * sizeof(int)));
+    RET(ensure(C.a_ebox, (size_t)(ne > 0 ? ne : 1) * 6 * sizeof(double)));
+    AnnTessArgs ta = {};
+    ta.m = md;
+    ta.g = grid_dev(gw);
+    ta.cnt_a = C.a_cnt.as<int>();
+    ta.cnt_b = ta.cnt_a + (ne + 1);
+    ta.ebox = C.a_ebox.as<double>();
+    ta.status = (unsigned*)&sm[S_STATUS];
+    if (ne > 0) CK(launch_elem_boxes(ta, st));
+    aa = AnnArgs{};
+    aa.nelem = ne;
+    aa.ebox = ta.ebox;
+    aa.cnt_a = ta.cnt_a;
+    aa.cnt_b = ta.cnt_b;
+    aa.status = ta.status;
+    q.c.reftol = reftol;
+    return PSIB_OK;
+}
+
+// A device buffer of `bytes` holding the caller's array (copied in for host-memory calls).
+int query_input(QueryCall& q, DevBuf& b, const void* src, size_t bytes, const void** dst)
+{
+    if (!q.host) {
+        *dst = src;
+        return PSIB_OK;
+    }
+    RET(ensure(b, bytes > 0 ? bytes : 16));
+    if (bytes) CK(cudaMemcpyAsync(b.p, src, bytes, cudaMemcpyHostToDevice, q.c.st));
+    *dst = b.p;
+    return PSIB_OK;
+}
+
+int query_output(QueryCall& q, void* dst, const void* src, size_t bytes)
+{
+    if (!bytes) return PSIB_OK;
+    CK(cudaMemcpyAsync(dst, src, bytes, q.host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, q.c.st));
+    return PSIB_OK;
+}
+
+int sort_keys(Ctx& C, unsigned long long* in, unsigned long long* out, long long n, int bits, cudaStream_t st)
+{
+    if (n >= (1ll << 31)) return fail(PSIB_ERR_OVERFLOW, "too many query results (%lld)", n);
+    size_t tb = 0;
+    CK(cub::DeviceRadixSort::SortKeys(nullptr, tb, in, out, (int)n, 0, bits, st));
+    RET(ensure(C.cub_tmp, tb));
+    CK(cub::DeviceRadixSort::SortKeys(C.cub_tmp.p, tb, in, out, (int)n, 0, bits, st));
+    return PSIB_OK;
+}
+
+int query_status(QueryCall& q, unsigned long long* sm)
+{
+    unsigned long long h[S_WORDS];
+    CK(cudaMemcpyAsync(h, sm, sizeof(h), cudaMemcpyDeviceToHost, q.c.st));
+    CK(cudaStreamSynchronize(q.c.st));
+    return check_status(q.c, h);
+}
+
+int query_elements_impl(QueryCall& q, const double (*window)[3], const double* boxes, long long nboxes,
+                        long long* offsets, int* elements, long long capacity)
+{
+    Ctx& C = *q.C;
+    cudaStream_t st = q.c.st;
+    RET(ensure(C.small, S_WORDS * 8));
+    unsigned long long* sm = C.small.as<unsigned long long>();
+    CK(cudaMemsetAsync(sm, 0, S_WORDS * 8, st));
+    AnnArgs aa;
+    RET(query_elements_stage(q, window, 1.0, aa, sm));
+    const void* qin = nullptr;
+    RET(query_input(q, C.q_in, boxes, (size_t)nboxes * 6 * sizeof(double), &qin));
+    aa.qry = (const double*)qin;
+    aa.nq = nboxes;
+    RET(ensure(C.q_cnt, (size_t)(nboxes + 1) * sizeof(long long)));
+    RET(ensure(C.q_off, (size_t)(nboxes + 1) * sizeof(long long)));
+    RET(ensure(C.small, S_WORDS * 8));
+    aa.q_cnt = C.q_cnt.as<long long>();
+    CK(cudaMemsetAsync(aa.q_cnt, 0, (size_t)(nboxes + 1) * sizeof(long long), st));
+    if (nboxes > 0 && aa.nelem > 0) CK(launch_query_boxes(aa, false, st));
+    RET(excl_scan(C, aa.q_cnt, C.q_off.as<long long>(), nboxes + 1, st));
+    long long total = 0;
+    RET(read_dev(C.q_off.as<long long>() + nboxes, total, st));
+    RET(query_status(q, sm));
+    RET(query_output(q, offsets, C.q_off.p, (size_t)(nboxes + 1) * sizeof(long long)));
+    if (!elements) return PSIB_OK;
+    if (capacity < total)
+        return fail(PSIB_ERR_OVERFLOW, "the output holds %lld elements, the queries found %lld", capacity, total);
+    if (total == 0) return PSIB_OK;
+    RET(ensure(C.q_key, (size_t)total * 8));
+    RET(ensure(C.q_key_s, (size_t)total * 8));
+    aa.q_key = C.q_key.as<unsigned long long>();
+    aa.q_n = &sm[S_RECN];
+    CK(cudaMemsetAsync(aa.q_n, 0, 8, st));
+    CK(launch_query_boxes(aa, true, st));
+    RET(sort_keys(C, aa.q_key, C.q_key_s.as<unsigned long long>(), total, 32 + bits_for((unsigned long long)nboxes + 1),
+                  st));
+    int* out = elements;
+    if (q.host) {
+        RET(ensure(C.q_out, (size_t)total * sizeof(int)));
+        out = C.q_out.as<int>();
+    }
+    CK(launch_keys_elem(C.q_key_s.as<unsigned long long>(), total, out, st));
+    if (q.host) RET(query_output(q, elements, out, (size_t)total * sizeof(int)));
+    return query_status(q, sm);
+}
+
+int sample_vdf_impl(QueryCall& q, const double (*window)[3], const double* points, long long npoints, double reftol,
+                    int maxlvl, long long* offsets, double* rho, double* vel, long long capacity)
+{
+    Ctx& C = *q.C;
+    cudaStream_t st = q.c.st;
+    const psib_mesh& m = *q.c.mesh;
+    RET(ensure(C.small, S_WORDS * 8));
+    unsigned long long* sm = C.small.as<unsigned long long>();
+    CK(cudaMemsetAsync(sm, 0, S_WORDS * 8, st));
+    AnnArgs aa;
+    RET(query_elements_stage(q, window, reftol, aa, sm));
+    long long klaunch = 0, kept = 0;
+    if (aa.nelem > 0) RET(build_cells(C, aa, st, klaunch, kept));
+    const void* qin = nullptr;
+    RET(query_input(q, C.q_in, points, (size_t)npoints * 3 * sizeof(double), &qin));
+    aa.qry = (const double*)qin;
+    aa.nq = npoints;
+    // (point, element) pairs: every kept element whose box contains the point
+    RET(ensure(C.q_cnt, (size_t)(npoints + 1) * sizeof(long long)));
+    RET(ensure(C.q_off, (size_t)(npoints + 1) * sizeof(long long)));
+    aa.q_cnt = C.q_cnt.as<long long>();
+    CK(cudaMemsetAsync(aa.q_cnt, 0, (size_t)(npoints + 1) * sizeof(long long), st));
+    if (kept > 0 && npoints > 0) CK(launch_query_points(aa, false, st));
+    RET(excl_scan(C, aa.q_cnt, C.q_off.as<long long>(), npoints + 1, st));
+    aa.q_off = C.q_off.as<long long>();
+    long long npair = 0;
+    RET(read_dev(aa.q_off + npoints, npair, st));
+    RET(ensure(C.q_key, (size_t)(npair > 0 ? npair : 1) * 8));
+    RET(ensure(C.q_key_s, (size_t)(npair > 0 ? npair : 1) * 8));
+    if (npair > 0) {
+        aa.q_key = C.q_key.as<unsigned long long>();
+        CK(launch_query_points(aa, true, st));
+        RET(sort_keys(C, aa.q_key, C.q_key_s.as<unsigned long long>(), npair,
+                      32 + bits_for((unsigned long long)npoints + 1), st));
+    }
+    // samples per pair, in pair order (point, element descending, tet)
+    VdfArgs va = {};
+    va.m = mesh_dev(m, psib_grid{}, q.c.pos, q.c.vel, q.c.mass, q.c.conn, 1.0, nullptr);
+    va.m.ptol2 = reftol * reftol;
+    va.max_lvl = maxlvl > 6 ? 6 : (maxlvl < 0 ? 0 : maxlvl);
+    va.quad = m.elemtype == 27;
+    va.points = aa.qry;
+    va.pairs = C.q_key_s.as<unsigned long long>();
+    va.npair = npair;
+    va.status = (unsigned*)&sm[S_STATUS];
+    RET(ensure(C.s_cnt, (size_t)(npair + 1) * sizeof(long long)));
+    RET(ensure(C.s_off, (size_t)(npair + 1) * sizeof(long long)));
+    va.cnt = C.s_cnt.as<long long>();
+    CK(cudaMemsetAsync(va.cnt, 0, (size_t)(npair + 1) * sizeof(long long), st));
+    if (npair > 0) CK(launch_vdf_samples(va, false, st));
+    RET(excl_scan(C, va.cnt, C.s_off.as<long long>(), npair + 1, st));
+    va.off = C.s_off.as<long long>();
+    long long total = 0;
+    RET(read_dev(va.off + npair, total, st));
+    // each point's first sample: the sample offset of its first pair
+    RET(ensure(C.s_offs, (size_t)(npoints + 1) * sizeof(long long)));
+    CK(launch_gather_ll(va.off, aa.q_off, npoints + 1, C.s_offs.as<long long>(), st));
+    RET(query_status(q, sm));
+    RET(query_output(q, offsets, C.s_offs.p, (size_t)(npoints + 1) * sizeof(long long)));
+    if (!rho || !vel) return PSIB_OK;
+    if (capacity < total)
+        return fail(PSIB_ERR_OVERFLOW, "the output holds %lld samples, the points have %lld", capacity, total);
+    if (total == 0) return PSIB_OK;
+    if (q.host) {
+        RET(ensure(C.s_rho, (size_t)total * sizeof(double)));
+        RET(ensure(C.s_vel, (size_t)total * 3 * sizeof(double)));
+        va.rho = C.s_rho.as<double>();
+        va.vel = C.s_vel.as<double>();
+    } else {
+        va.rho = rho;
+        va.vel = vel;
+    }
+    CK(launch_vdf_samples(va, true, st));
+    if (q.host) {
+        RET(query_output(q, rho, va.rho, (size_t)total * sizeof(double)));
+        RET(query_output(q, vel, va.vel, (size_t)total * 3 * sizeof(double)));
+    }
+    return query_status(q, sm);
 }
 
 } // namespace
@@ -1807,6 +2092,30 @@ int psib_voxels_adjoint(const psib_grid* grad, const psib_mesh* mesh, double ref
     CK(cudaEventSynchronize(C->ev[7]));
     if (o.stats) CK(cudaEventElapsedTime(&o.stats->ms_total, C->ev[0], C->ev[7]));
     return PSIB_OK;
+}
+
+int psib_query_elements(const psib_mesh* mesh, const double window[2][3], const double* boxes, long long nboxes,
+                        long long* offsets, int* elements, long long capacity, const psib_options* opt)
+{
+    if (!window || !offsets || nboxes < 0 || (nboxes > 0 && !boxes))
+        return fail(PSIB_ERR_ARG, "window, offsets and nboxes >= 0 boxes are required");
+    if (nboxes >= (1ll << 31)) return fail(PSIB_ERR_ARG, "at most 2^31 - 1 query boxes");
+    QueryCall q;
+    RET(query_begin(q, mesh, opt));
+    return query_end(q, query_elements_impl(q, window, boxes, nboxes, offsets, elements, capacity));
+}
+
+int psib_sample_vdf(const psib_mesh* mesh, const double window[2][3], const double* points, long long npoints,
+                    double refine_tolerance, int refine_max_lvl, long long* offsets, double* rho, double* vel,
+                    long long capacity, const psib_options* opt)
+{
+    if (!window || !offsets || npoints < 0 || (npoints > 0 && !points))
+        return fail(PSIB_ERR_ARG, "window, offsets and npoints >= 0 points are required");
+    if (npoints >= (1ll << 31)) return fail(PSIB_ERR_ARG, "at most 2^31 - 1 sample points");
+    QueryCall q;
+    RET(query_begin(q, mesh, opt));
+    return query_end(q, sample_vdf_impl(q, window, points, npoints, refine_tolerance, refine_max_lvl, offsets, rho,
+                                        vel, capacity));
 }
 
 } // extern "C"

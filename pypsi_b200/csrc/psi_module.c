@@ -13,8 +13,9 @@
  *
  * The 'gadget2' / 'gevolution' loaders read snapshots through
  * psib_load_gadget2 / psib_load_gevolution; mode='annihilation' runs the
- * library's annihilation deposit.  Not provided here: PSI.RStarTree and
- * PSI.VDF (other paths of the reference).
+ * library's annihilation deposit; PSI.RStarTree(mesh).query(box) and
+ * PSI.VDF(mesh, sample_pos, tree, ...) run psib_query_elements and
+ * psib_sample_vdf.
  */
 #define PY_SSIZE_T_CLEAN
 #include <Python.h>
@@ -572,14 +573,35 @@ static PyTypeObject MeshType = {
 
 /* ------------------------------------------------------------ voxels() */
 
-static PyObject *raise_status(int rc)
+static PyObject *raise_status_of(const char *what, int rc)
 {
     PyObject *exc = PyExc_RuntimeError;
     if (rc == PSIB_ERR_ARG) exc = PyExc_ValueError;
     else if (rc == PSIB_ERR_UNSUPPORTED) exc = PyExc_NotImplementedError;
     else if (rc == PSIB_ERR_NOMEM) exc = PyExc_MemoryError;
-    PyErr_Format(exc, "PSI.voxels failed (code %d): %s", rc, psib_last_error());
+    PyErr_Format(exc, "%s failed (code %d): %s", what, rc, psib_last_error());
     return NULL;
+}
+
+static PyObject *raise_status(int rc) { return raise_status_of("PSI.voxels", rc); }
+
+/* The library's view of a Mesh object's arrays. */
+static void mesh_view(Mesh *mesh, psib_mesh *m)
+{
+    memset(m, 0, sizeof(*m));
+    m->elemtype = mesh->elemtype;
+    m->npart = mesh->npart;
+    m->nelem = mesh->nelem;
+    m->pos = (const double *)PyArray_DATA((PyArrayObject *)mesh->pos);
+    m->vel = (const double *)PyArray_DATA((PyArrayObject *)mesh->vel);
+    m->mass = (const double *)PyArray_DATA((PyArrayObject *)mesh->mass);
+    if (mesh->block) {
+        for (int i = 0; i < 3; ++i) m->block_dims[i] = mesh->nside[i];
+    } else {
+        m->connectivity = (const int *)PyArray_DATA((PyArrayObject *)mesh->connectivity);
+    }
+    m->periodic = mesh->periodic;
+    memcpy(m->box, mesh->box, sizeof(m->box));
 }
 
 /* src/PSI.c:974-1018 */
@@ -650,20 +672,7 @@ static PyObject *PSI_voxels(PyObject *self, PyObject *args, PyObject *kwds)
         g.fields[f] = (double *)PyArray_DATA((PyArrayObject *)a);
     }
     psib_mesh m;
-    memset(&m, 0, sizeof(m));
-    m.elemtype = mesh->elemtype;
-    m.npart = mesh->npart;
-    m.nelem = mesh->nelem;
-    m.pos = (const double *)PyArray_DATA((PyArrayObject *)mesh->pos);
-    m.vel = (const double *)PyArray_DATA((PyArrayObject *)mesh->vel);
-    m.mass = (const double *)PyArray_DATA((PyArrayObject *)mesh->mass);
-    if (mesh->block) {
-        for (int i = 0; i < 3; ++i) m.block_dims[i] = mesh->nside[i];
-    } else {
-        m.connectivity = (const int *)PyArray_DATA((PyArrayObject *)mesh->connectivity);
-    }
-    m.periodic = mesh->periodic;
-    memcpy(m.box, mesh->box, sizeof(m.box));
+    mesh_view(mesh, &m);
 
     psib_options o;
     memset(&o, 0, sizeof(o));
@@ -701,8 +710,154 @@ static PyObject *PSI_device_count(PyObject *self, PyObject *noargs)
     return PyLong_FromLong(psib_device_count());
 }
 
+/* ------------------------------------------------------------ RStarTree */
+
+/* PSI.RStarTree(mesh, initial_capacity=1024) (src/PSI.c:809-962): the spatial
+ * index of the mesh's elements.  No tree is built here: the object keeps the
+ * mesh and the cull window of the reference's tree (the periodic box of a
+ * periodic mesh, +-1e30 for an open one, src/PSI.c:877-893), and query() tests
+ * the box against every element on the GPU (psib_query_elements). */
+typedef struct {
+    PyObject_HEAD PyObject *mesh;
+    double window[2][3];
+} RStarTree;
+
+static int RStarTree_init(RStarTree *self, PyObject *args, PyObject *kwds)
+{
+    Mesh *mesh = NULL;
+    int init_cap = 1024;
+    static char *kwlist[] = {"mesh", "initial_capacity", NULL};
+    if (!PyArg_ParseTupleAndKeywords(args, kwds, "O!|i", kwlist, &MeshType, &mesh, &init_cap)) return -1;
+    (void)init_cap;
+    for (int i = 0; i < 3; ++i) {
+        self->window[0][i] = mesh->periodic ? mesh->box[0][i] : -1.0e30;
+        self->window[1][i] = mesh->periodic ? mesh->box[1][i] : 1.0e30;
+    }
+    Py_INCREF(mesh);
+    swap_ref(&self->mesh, (PyObject *)mesh);
+    return 0;
+}
+
+static PyObject *RStarTree_new(PyTypeObject *type, PyObject *args, PyObject *kwds)
+{
+    (void)args;
+    (void)kwds;
+    RStarTree *self = (RStarTree *)type->tp_alloc(type, 0);
+    return (PyObject *)self;
+}
+
+static void RStarTree_dealloc(RStarTree *self)
+{
+    Py_XDECREF(self->mesh);
+    Py_TYPE(self)->tp_free((PyObject *)self);
+}
+
+/* src/PSI.c:817-862: int32 indices of the elements whose box touches `box` */
+static PyObject *RStarTree_query(RStarTree *self, PyObject *args, PyObject *kwds)
+{
+    PyObject *box;
+    double q[6];
+    static char *kwlist[] = {"box", NULL};
+    if (!PyArg_ParseTupleAndKeywords(args, kwds, "O", kwlist, &box)) return NULL;
+    if (!PyArg_ParseTuple(box, "(ddd)(ddd)", &q[0], &q[1], &q[2], &q[3], &q[4], &q[5])) {
+        PyErr_SetString(PyExc_TypeError, "Query box must be a tuple containing two tuples of 3 values each");
+        return NULL;
+    }
+    if (!self->mesh) {
+        PyErr_SetString(PyExc_ValueError, "RStarTree has no mesh");
+        return NULL;
+    }
+    psib_mesh m;
+    mesh_view((Mesh *)self->mesh, &m);
+    long long off[2] = {0, 0};
+    int rc;
+    Py_BEGIN_ALLOW_THREADS rc = psib_query_elements(&m, (const double(*)[3])self->window, q, 1, off, NULL, 0, NULL);
+    Py_END_ALLOW_THREADS if (rc != PSIB_OK) return raise_status_of("PSI.RStarTree.query", rc);
+    npy_intp nd[1] = {(npy_intp)off[1]};
+    PyObject *out = PyArray_SimpleNew(1, nd, NPY_INT32);
+    if (!out) return NULL;
+    if (off[1] > 0) {
+        int *dst = (int *)PyArray_DATA((PyArrayObject *)out);
+        Py_BEGIN_ALLOW_THREADS rc = psib_query_elements(&m, (const double(*)[3])self->window, q, 1, off, dst, off[1], NULL);
+        Py_END_ALLOW_THREADS if (rc != PSIB_OK) {
+            Py_DECREF(out);
+            return raise_status_of("PSI.RStarTree.query", rc);
+        }
+    }
+    return out;
+}
+
+static PyMemberDef RStarTree_members[] = {{"mesh", T_OBJECT_EX, offsetof(RStarTree, mesh), READONLY, "mesh"},
+                                          {NULL, 0, 0, 0, NULL}};
+
+static PyMethodDef RStarTree_methods[] = {
+    {"query", (PyCFunction)(void (*)(void))RStarTree_query, METH_VARARGS | METH_KEYWORDS, "Query the RStarTree."},
+    {NULL, NULL, 0, NULL}};
+
+static PyTypeObject RStarTreeType = {
+    PyVarObject_HEAD_INIT(NULL, 0).tp_name = "PSI.RStarTree",
+    .tp_basicsize = sizeof(RStarTree),
+    .tp_dealloc = (destructor)RStarTree_dealloc,
+    .tp_flags = Py_TPFLAGS_DEFAULT | Py_TPFLAGS_BASETYPE,
+    .tp_doc = "RStarTree",
+    .tp_methods = RStarTree_methods,
+    .tp_members = RStarTree_members,
+    .tp_init = (initproc)RStarTree_init,
+    .tp_new = RStarTree_new,
+};
+
+/* ------------------------------------------------------------ VDF */
+
+/* PSI.VDF(mesh, sample_pos, tree=None, refine_tolerance=1.0, refine_max_lvl=0)
+ * (src/PSI.c:1022-1057): (rho, vel) of every stream at sample_pos.  Without a
+ * tree the elements are culled against the mesh's box, as the reference's own
+ * tree for this call is (src/cpsi.c:206-209); with one, against the tree's
+ * window. */
+static PyObject *PSI_VDF(PyObject *self, PyObject *args, PyObject *kwds)
+{
+    (void)self;
+    Mesh *mesh = NULL;
+    RStarTree *tree = NULL;
+    double s[3], reftol = 1.0;
+    int maxlvl = 0;
+    static char *kwlist[] = {"mesh", "sample_pos", "tree", "refine_tolerance", "refine_max_lvl", NULL};
+    if (!PyArg_ParseTupleAndKeywords(args, kwds, "O!(ddd)|O!di", kwlist, &MeshType, &mesh, &s[0], &s[1], &s[2],
+                                     &RStarTreeType, &tree, &reftol, &maxlvl))
+        return NULL;
+    psib_mesh m;
+    mesh_view(mesh, &m);
+    double win[2][3];
+    memcpy(win, tree ? tree->window : mesh->box, sizeof(win));
+    long long off[2] = {0, 0};
+    int rc;
+    Py_BEGIN_ALLOW_THREADS rc = psib_sample_vdf(&m, (const double(*)[3])win, s, 1, reftol, maxlvl, off, NULL, NULL, 0, NULL);
+    Py_END_ALLOW_THREADS if (rc != PSIB_OK) return raise_status_of("PSI.VDF", rc);
+    npy_intp nd[2] = {(npy_intp)off[1], 3};
+    PyObject *rho = PyArray_SimpleNew(1, nd, NPY_FLOAT64);
+    PyObject *vel = PyArray_SimpleNew(2, nd, NPY_FLOAT64);
+    if (!rho || !vel) {
+        Py_XDECREF(rho);
+        Py_XDECREF(vel);
+        return NULL;
+    }
+    if (off[1] > 0) {
+        double *r = (double *)PyArray_DATA((PyArrayObject *)rho), *v = (double *)PyArray_DATA((PyArrayObject *)vel);
+        Py_BEGIN_ALLOW_THREADS rc = psib_sample_vdf(&m, (const double(*)[3])win, s, 1, reftol, maxlvl, off, r, v, off[1], NULL);
+        Py_END_ALLOW_THREADS if (rc != PSIB_OK) {
+            Py_DECREF(rho);
+            Py_DECREF(vel);
+            return raise_status_of("PSI.VDF", rc);
+        }
+    }
+    PyObject *ret = Py_BuildValue("OO", rho, vel);
+    Py_DECREF(rho);
+    Py_DECREF(vel);
+    return ret;
+}
+
 static PyMethodDef module_methods[] = {
     {"voxels", (PyCFunction)(void (*)(void))PSI_voxels, METH_VARARGS | METH_KEYWORDS, "Voxelizes"},
+    {"VDF", (PyCFunction)(void (*)(void))PSI_VDF, METH_VARARGS | METH_KEYWORDS, "VDF"},
     {"last_stats", PSI_last_stats, METH_NOARGS, "Work counters and device timings of the last voxels() call"},
     {"device_count", PSI_device_count, METH_NOARGS, "Number of visible CUDA devices"},
     {NULL, NULL, 0, NULL}};
@@ -715,9 +870,11 @@ PyMODINIT_FUNC PyInit_PSI(void)
     PyObject *m = PyModule_Create(&PSImodule);
     if (!m) return NULL;
     import_array();
-    if (PyType_Ready(&MeshType) < 0 || PyType_Ready(&GridType) < 0) return NULL;
+    if (PyType_Ready(&MeshType) < 0 || PyType_Ready(&GridType) < 0 || PyType_Ready(&RStarTreeType) < 0) return NULL;
     Py_INCREF(&MeshType);
     PyModule_AddObject(m, "Mesh", (PyObject *)&MeshType);
+    Py_INCREF(&RStarTreeType);
+    PyModule_AddObject(m, "RStarTree", (PyObject *)&RStarTreeType);
     Py_INCREF(&GridType);
     PyModule_AddObject(m, "Grid", (PyObject *)&GridType);
     return m;

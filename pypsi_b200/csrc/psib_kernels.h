@@ -247,6 +247,19 @@ struct AnnArgs {
     long long *tp_cnt;        // per slot (count)
     int2 *tpairs;             // (side-A tet, side-B tet) of every tet pair of the chunk
     unsigned *status;
+    // queries: sorted unique cell keys of the registrations, their runs
+    const unsigned long long *run_key;
+    const long long *run_off;
+    const int *run_cnt;
+    long long nruns;
+    // query boxes (6 doubles: lo, hi) or points (3 doubles), their result counts and keys
+    // (q << 32) | (2^32 - 1 - e), sorted afterwards: q ascending, e descending
+    const double *qry;
+    long long nq;
+    long long *q_cnt;
+    const long long *q_off;
+    unsigned long long *q_key;
+    unsigned long long *q_n;  // brute-force query: emission counter
 };
 // stats of the kept element boxes: 2 x 3 ordered-int min/max, 3 extent sums, kept count
 cudaError_t launch_ann_box_stats(const AnnArgs &a, unsigned long long *out, double *ext, cudaStream_t s);
@@ -260,6 +273,31 @@ cudaError_t launch_ann_tpairs(const AnnArgs &a, bool emit, cudaStream_t s);
 // (bounds[0] = 0, bounds[nb] = nslot); tp_excl holds nslot + 1 offsets
 cudaError_t launch_ann_chunk_bounds(const long long *tp_excl, long long nslot, long long budget, int nb,
                                     long long *bounds, cudaStream_t s);
+
+// the element boxes of a query: cull against a.g's window, kept flag in cnt_a and cnt_b
+cudaError_t launch_elem_boxes(const AnnTessArgs &a, cudaStream_t s);
+// box queries, every (box, element) pair tested (count: q_cnt; emit: q_key via q_n)
+cudaError_t launch_query_boxes(const AnnArgs &a, bool emit, cudaStream_t s);
+// point queries through the cell index (count: q_cnt; emit: q_key at q_off)
+cudaError_t launch_query_points(const AnnArgs &a, bool emit, cudaStream_t s);
+
+// Phase-space samples of (point, element) pairs (psi_sample_vdf, src/cpsi.c:177-275).
+struct VdfArgs {
+    MeshDev m;                // ptol2 = refine_tolerance^2
+    int max_lvl, quad;
+    const double *points;
+    const unsigned long long *pairs; // sorted keys (point << 32) | (2^32 - 1 - element)
+    long long npair;
+    long long *cnt;           // count: samples per pair
+    const long long *off;     // emit: exclusive sample offset per pair
+    double *rho, *vel;
+    unsigned *status;
+};
+cudaError_t launch_vdf_samples(const VdfArgs &a, bool emit, cudaStream_t s);
+// out[i] = the element of sorted query key i
+cudaError_t launch_keys_elem(const unsigned long long *keys, long long n, int *out, cudaStream_t s);
+// out[p] = pair_soff[q_off[p]] for p in [0, np]: each point's first sample
+cudaError_t launch_gather_ll(const long long *src, const long long *idx, long long n, long long *out, cudaStream_t s);
 
 struct AnnClipArgs {
     const int2 *tpairs;

@@ -665,6 +665,167 @@ cudaError_t launch_ann_tess(const AnnTessArgs& a, bool emit, cudaStream_t s)
     return cudaGetLastError();
 }
 
+// ---- element boxes and phase-space samples (queries, PSI.VDF) ----
+
+// One thread per element: the cull against the window a.g (src/rtree.c:63-70,
+// which unwraps the element) and its box; cnt_a[e] = cnt_b[e] = 1 when kept.
+__global__ void __launch_bounds__(128) k_elem_boxes(AnnTessArgs a)
+{
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < a.m.nelem; e += stride) {
+        double p[27][3], u[27][3];
+        int ids[27];
+        if (!gather(a.m, e, p, u, ids)) {
+            atomicOr(a.status, ST_INDEX);
+            a.cnt_a[e] = a.cnt_b[e] = 0;
+            continue;
+        }
+        const bool keep = aabb_periodic(p, a.m.elemtype, a.m, a.g);
+        double rb[2][3];
+        aabb_n(p, a.m.elemtype, rb);
+        for (int i = 0; i < 3; ++i) {
+            a.ebox[6 * e + i] = rb[0][i];
+            a.ebox[6 * e + 3 + i] = rb[1][i];
+        }
+        a.cnt_a[e] = a.cnt_b[e] = keep ? 1 : 0;
+    }
+}
+
+cudaError_t launch_elem_boxes(const AnnTessArgs& a, cudaStream_t s)
+{
+    k_elem_boxes<<<tess_grid(a.m.nelem), 128, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+// psi_barycentric (src/geometry.c:335-389): barycentric coordinates of s in
+// the tet v, (w_i + s . n_i) / sum, where w_i is the volume term of the three
+// vertices other than v[i] -- x_a (b x c).x + ... in the reference's order --
+// and n_i the normal of the face opposite v[i], built from the same edge
+// vectors as the reference's (those of its face planes); returns |sum| / 6.
+__device__ __forceinline__ double cross_x(const double* a, const double* b) { return a[1] * b[2] - a[2] * b[1]; }
+
+__device__ __forceinline__ void edge_cross(const double* a0, const double* a1, const double* b0, const double* b1,
+                                           double* n)
+{
+    double A[3], B[3];
+    for (int i = 0; i < 3; ++i) {
+        A[i] = a1[i] - a0[i];
+        B[i] = b1[i] - b0[i];
+    }
+    n[0] = A[1] * B[2] - A[2] * B[1];
+    n[1] = A[2] * B[0] - A[0] * B[2];
+    n[2] = A[0] * B[1] - A[1] * B[0];
+}
+
+__device__ double barycentric(const double (*v)[3], const double* s, double* b)
+{
+    double w[4], n[4][3];
+    w[0] = v[1][0] * cross_x(v[2], v[3]) + v[2][0] * cross_x(v[3], v[1]) + v[3][0] * cross_x(v[1], v[2]);
+    w[1] = v[0][0] * cross_x(v[3], v[2]) + v[2][0] * cross_x(v[0], v[3]) + v[3][0] * cross_x(v[2], v[0]);
+    w[2] = v[0][0] * cross_x(v[1], v[3]) + v[1][0] * cross_x(v[3], v[0]) + v[3][0] * cross_x(v[0], v[1]);
+    w[3] = v[0][0] * cross_x(v[2], v[1]) + v[1][0] * cross_x(v[0], v[2]) + v[2][0] * cross_x(v[1], v[0]);
+    edge_cross(v[1], v[3], v[1], v[2], n[0]);
+    edge_cross(v[0], v[2], v[2], v[3], n[1]);
+    edge_cross(v[3], v[1], v[3], v[0], n[2]);
+    edge_cross(v[2], v[0], v[0], v[1], n[3]);
+    double tot = 0.0;
+    for (int i = 0; i < 4; ++i) {
+        b[i] = w[i];
+        for (int j = 0; j < 3; ++j) b[i] += s[j] * n[i][j];
+        tot += b[i];
+    }
+    for (int i = 0; i < 4; ++i) b[i] /= tot;
+    return fabs((1.0 / 6.0) * tot);
+}
+
+// A tet that contains the point gives one sample: density mass / volume and
+// the velocity interpolated at the point (src/cpsi.c:237-262).
+struct VdfEmitter {
+    const VdfArgs& a;
+    const double* s;
+    long long pos;
+    int n;
+    bool write;
+    __device__ void tet(const double (*p)[3], const double (*u)[3], double mass, long long, const int*)
+    {
+        double b[4];
+        const double vol = barycentric(p, s, b);
+        if (vol <= 0.0) return;
+        for (int i = 0; i < 4; ++i)
+            if (b[i] < 0.0) return;
+        if (write) {
+            for (int i = 0; i < 3; ++i) {
+                double acc = 0.0;
+                for (int j = 0; j < 4; ++j) acc += b[j] * u[j][i];
+                a.vel[3 * pos + i] = acc;
+            }
+            a.rho[pos] = mass / vol;
+            pos++;
+        }
+        n++;
+    }
+};
+
+// One thread per (point, element) pair: the element refined from its vertices
+// as stored (src/cpsi.c:222-230), every tet tested against the point.
+template <bool REFINE, bool QUAD, bool EMIT>
+__global__ void __launch_bounds__(128) k_vdf_samples(VdfArgs a)
+{
+    constexpr int NV = QUAD ? 27 : 8;
+    RefNode* L = nullptr;
+    RefNode Lbuf[(REFINE || QUAD) ? MAX_REFINE + 1 : 1];
+    if constexpr (REFINE || QUAD) L = Lbuf;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < a.npair; i += stride) {
+        const unsigned long long key = a.pairs[i];
+        const long long pt = (long long)(key >> 32);
+        const long long e = (long long)(0xFFFFFFFFull - (key & 0xFFFFFFFFull));
+        double p[NV][3], u[NV][3];
+        int ids[NV];
+        if ((!QUAD && a.m.elemtype == 27) || !gather(a.m, e, p, u, ids)) {
+            atomicOr(a.status, ST_INDEX);
+            if (!EMIT) a.cnt[i] = 0;
+            continue;
+        }
+        const double me = a.m.mass ? a.m.mass[e] : 1.0;
+        VdfEmitter em{a, a.points + 3 * pt, EMIT ? a.off[i] : 0, 0, EMIT};
+        const int et = a.m.elemtype;
+        if (et == 4) {
+            em.tet(p, u, me, e, nullptr);
+        } else if (QUAD && et == 27) {
+            if constexpr (QUAD)
+                refine_element_quad(em, p, u, me, e, REFINE ? a.max_lvl : 0, a.m.ptol2, 0, 0.0, a.m.lag, L);
+        } else if (!REFINE) {
+            for (int t = 0; t < 6; ++t) {
+                double tp[4][3], tu[4][3];
+                for (int v = 0; v < 4; ++v)
+                    for (int c = 0; c < 3; ++c) {
+                        tp[v][c] = p[c_tet_corners[t][v]][c];
+                        tu[v][c] = u[c_tet_corners[t][v]][c];
+                    }
+                em.tet(tp, tu, me * (1.0 / 6), e, nullptr);
+            }
+        } else {
+            if constexpr (REFINE) refine_element(em, p, u, me, e, a.max_lvl, a.m.ptol2, 0, 0.0, a.m.lag, L);
+        }
+        if (!EMIT) a.cnt[i] = em.n;
+    }
+}
+
+cudaError_t launch_vdf_samples(const VdfArgs& a, bool emit, cudaStream_t s)
+{
+    const int g = tess_grid(a.npair);
+    const bool refine = a.max_lvl > 0 && a.m.elemtype != 4;
+    if (a.quad) {
+        if (refine) emit ? k_vdf_samples<true, true, true><<<g, 128, 0, s>>>(a) : k_vdf_samples<true, true, false><<<g, 128, 0, s>>>(a);
+        else emit ? k_vdf_samples<false, true, true><<<g, 128, 0, s>>>(a) : k_vdf_samples<false, true, false><<<g, 128, 0, s>>>(a);
+    } else {
+        if (refine) emit ? k_vdf_samples<true, false, true><<<g, 128, 0, s>>>(a) : k_vdf_samples<true, false, false><<<g, 128, 0, s>>>(a);
+        else emit ? k_vdf_samples<false, false, true><<<g, 128, 0, s>>>(a) : k_vdf_samples<false, false, false><<<g, 128, 0, s>>>(a);
+    }
+    return cudaGetLastError();
+}
+
 // ---- fragment records applied to the fields, voxel by voxel ----
 
 // Physical moments of one FP32-kernel fragment from its record (m0, q-centroid,
