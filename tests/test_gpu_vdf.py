@@ -74,8 +74,9 @@ def test_vdf_batched_host_and_device(gpu, oracle):
     kw = dict(connectivity=c["conn"], vel=c["vel"], mass=c["mass"], periodic_box=c["periodic_box"],
               refine_tolerance=c["reftol"], refine_max_lvl=c["maxlvl"])
     off, rho, vel = capi.sample_vdf(pts, c["pos"], **kw)
-    assert off[0] == 0 and off[-1] == len(rho) and len(rho) > 500
-    for i in range(0, 500, 7):
+    # the oracle finds 203 samples at these points (stored-position partners leave gaps near the box edge)
+    assert off[0] == 0 and off[-1] == len(rho) == 203
+    for i in range(0, 500, 3):
         w_rho, w_vel = vdf(c, "restatement", pts[i], True)
         assert np.array_equal(rho[off[i]:off[i + 1]], w_rho), i
         assert np.array_equal(vel[off[i]:off[i + 1]], w_vel), i
