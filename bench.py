@@ -54,11 +54,15 @@ def parse():
     ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--ann-n", type=int, default=64, help="ann: particles per side (smaller cases for profiling)")
+    ap.add_argument("--ann-grid", type=int, default=128, help="ann: grid cells per side")
     ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c5", "ann"],
                     help="c2: the headline (128^3 -> 256^3, order 2); c3: 512 uneven cutouts in one batch; "
                          "c5: 256^3 -> 512^3 with stretch refinement; ann: annihilation mode, 64^3 -> 128^3")
     args = ap.parse_args()
     if (args.n_part, args.n_grid) != (N_PART, N_GRID) or args.precision != "both":
+        args.no_cpu_baseline = True
+    if (args.ann_n, args.ann_grid) != (ANN_N, ANN_GRID):
         args.no_cpu_baseline = True
     return args
 
@@ -323,13 +327,14 @@ def run_ann(args):
     rank, world, local = env_rank()
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    pos = zeldovich(ANN_N, ANN_RMS, 4242 + rank, wrap=False)[0]
+    n_part, n_grid = args.ann_n, args.ann_grid
+    pos = zeldovich(n_part, ANN_RMS, 4242 + rank, wrap=False)[0]
     dpos = torch.from_numpy(pos.reshape(-1, 3)).to(dev)
-    m = torch.zeros((ANN_GRID,) * 3, dtype=torch.float64, device=dev)
+    m = torch.zeros((n_grid,) * 3, dtype=torch.float64, device=dev)
     stream = torch.cuda.current_stream()
 
     def step():
-        return capi.voxels_device({"m": m}, (ANN_GRID,) * 3, BOX, dpos, block_dims=(ANN_N,) * 3, mode="annihilation",
+        return capi.voxels_device({"m": m}, (n_grid,) * 3, BOX, dpos, block_dims=(n_part,) * 3, mode="annihilation",
                                   stream=stream)
 
     for _ in range(max(1, args.warmup)):
@@ -349,7 +354,7 @@ def run_ann(args):
     # end to end: PSI.voxels(mode='annihilation') on host arrays (the copies in the timed region)
     e2e = None
     if not args.no_e2e:
-        grid = PSI.Grid(n=(ANN_GRID,) * 3, bounds=BOX)
+        grid = PSI.Grid(n=(n_grid,) * 3, bounds=BOX)
         mesh = PSI.Mesh(loader="block", pos=np.ascontiguousarray(pos))
         PSI.voxels(grid=grid, mesh=mesh, mode="annihilation")
         ts = []
@@ -365,7 +370,9 @@ def run_ann(args):
     line = {"metric": ANN_METRIC, "value": pairs / (ms * 1e-3), "unit": "tet pairs/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": ANN_DATA,
-            "config": {"workload": ANN_WORKLOAD, "l2": "inputs larger than L2 (tet records and fragment records)"},
+            "config": {"workload": ANN_WORKLOAD if (n_part, n_grid) == (ANN_N, ANN_GRID) else
+                       f"{n_part}^3 particles, open lattice, Zel'dovich rms 1.5 cells -> {n_grid}^3 grid, annihilation",
+                       "l2": "inputs larger than L2 (tet records and fragment records)"},
             "work": {"elements_kept": st["elements_kept"], "tets": st["tets"], "tet_pairs": pairs,
                      "fragments": st["fragments"], "splits": st["splits"], "chunks": st["chunks"]},
             "stage_ms": {"elements_pairs_and_tet_pairs": st["ms_tess"], "clip": st["ms_clip"],
