@@ -234,6 +234,28 @@ cudaError_t launch_ann_pair_sides(const AnnArgs& a, long long* na, cudaStream_t 
     return cudaGetLastError();
 }
 
+// Ordering key of a tet pair: the voxel index box of its walk (the two boxes'
+// intersection within the window, as the clip computes it), larger boxes
+// first.  The clip kernel takes tet pairs in this order so that the 32 lanes
+// of a warp walk trees of similar size; the records carry the tet pair's
+// index, so the order changes no result.
+__device__ __forceinline__ uint16_t walk_key(const GridDev& g, const double* b0, const double* b1)
+{
+    long long vol = 1;
+    for (int c = 0; c < 3; ++c) {
+        double cmin = fmax(b0[c], b1[c]), cmax = fmin(b0[3 + c], b1[3 + c]);
+        if (g.w0[c] > cmin) cmin = g.w0[c];
+        if (g.w1[c] < cmax) cmax = g.w1[c];
+        int lo = (int)floor((cmin - g.w0[c]) / g.d[c]);
+        int hi = (int)ceil((cmax - g.w0[c]) / g.d[c]);
+        if (lo < 0) lo = 0;
+        if (hi > g.n[c]) hi = g.n[c];
+        const int sz = hi - lo;
+        if (vol < 0xFFFF) vol *= (sz > 1 ? sz : 1);
+    }
+    return (uint16_t)(0xFFFF - (vol < 0xFFFE ? vol : 0xFFFE));
+}
+
 // Tet pairs: slot u is side-A tet t of element pair p (u = aoff[p] + t); it
 // pairs with every side-B tet of e1 whose box overlaps its own with positive
 // extent on every axis (psi_aabb_ixn, src/cpsi.c:293-306).  Slots are taken
@@ -268,7 +290,10 @@ __global__ void k_ann_tpairs(AnnArgs a)
                 ok = ok && (h > l);
             }
             if (!ok) continue;
-            if (EMIT) a.tpairs[w++] = make_int2((int)ta, (int)(tb0 + t1));
+            if (EMIT) {
+                a.tp_key[w] = walk_key(a.g, b0, rb + TR_BOX);
+                a.tpairs[w++] = make_int2((int)ta, (int)(tb0 + t1));
+            }
             n++;
         }
         if (!EMIT) a.tp_cnt[u] = n;

@@ -122,7 +122,8 @@ struct Ctx {
     // annihilation: element tets and boxes, cell registrations, element and tet pairs
     DevBuf a_cnt, a_off, a_ebox, a_tets_a, a_tets_b, a_stats, a_reg_cnt, a_reg_off, a_reg_key, a_reg_elem,
         a_reg_key_s, a_reg_elem_s, a_run_key, a_run_cnt, a_run_off, a_run_lo, a_run_hi, a_pair_cnt, a_pair_off,
-        a_pair_key, a_pair_key_s, a_na, a_aoff, a_tp_cnt, a_tp_excl, a_bounds, a_tpairs, a_deep;
+        a_pair_key, a_pair_key_s, a_na, a_aoff, a_tp_cnt, a_tp_excl, a_bounds, a_tpairs, a_deep, a_tp_key,
+        a_tp_key_s, a_ord_in, a_ord;
     // element queries and phase-space samples
     DevBuf q_in, q_cnt, q_off, q_key, q_key_s, q_out, s_cnt, s_off, s_offs, s_rho, s_vel;
     cudaGraphExec_t pass_exec = nullptr; // one breadth-first pass as a CUDA graph
@@ -138,7 +139,8 @@ struct Ctx {
                 &qwin[2], &btab, &igrid, &passes, &a_cnt, &a_off, &a_ebox, &a_tets_a, &a_tets_b, &a_stats,
                 &a_reg_cnt, &a_reg_off, &a_reg_key, &a_reg_elem, &a_reg_key_s, &a_reg_elem_s, &a_run_key,
                 &a_run_cnt, &a_run_off, &a_run_lo, &a_run_hi, &a_pair_cnt, &a_pair_off, &a_pair_key,
-                &a_pair_key_s, &a_na, &a_aoff, &a_tp_cnt, &a_tp_excl, &a_bounds, &a_tpairs, &a_deep, &q_in, &q_cnt,
+                &a_pair_key_s, &a_na, &a_aoff, &a_tp_cnt, &a_tp_excl, &a_bounds, &a_tpairs, &a_deep, &a_tp_key,
+                &a_tp_key_s, &a_ord_in, &a_ord, &q_in, &q_cnt,
                 &q_off, &q_key, &q_key_s, &q_out, &s_cnt, &s_off, &s_offs, &s_rho, &s_vel};
     }
 };
@@ -1318,7 +1320,13 @@ int run_annihilation(Call& c)
     if (cap >= (1ll << 31)) return fail(PSIB_ERR_OVERFLOW, "a chunk of %lld tet pairs is too large", cap);
     RET(ensure(C.a_tpairs, (size_t)cap * sizeof(int2)));
     RET(ensure(C.a_deep, (size_t)cap * sizeof(int)));
+    RET(ensure(C.a_tp_key, (size_t)cap * sizeof(uint16_t)));
+    RET(ensure(C.a_tp_key_s, (size_t)cap * sizeof(uint16_t)));
+    RET(ensure(C.a_ord_in, (size_t)cap * sizeof(int)));
+    RET(ensure(C.a_ord, (size_t)cap * sizeof(int)));
     aa.tpairs = C.a_tpairs.as<int2>();
+    aa.tp_key = C.a_tp_key.as<uint16_t>();
+    aa.g = gd;
 
     const int clip_block = 128, big_block = 64;
     const int clip_grid = C.num_sms * ann_blocks_per_sm(false, clip_block);
@@ -1334,7 +1342,18 @@ int run_annihilation(Call& c)
         aa.slot1 = bnd[k + 1];
         aa.tp_base = boff[k];
         CK(launch_ann_tpairs(aa, true, st));
-        klaunch++;
+        // the clip's order: larger walks first (k_ann_tpairs' keys)
+        k_iota<<<C.num_sms * 8, 256, 0, st>>>(C.a_ord_in.as<int>(), ntp);
+        CK(cudaGetLastError());
+        {
+            size_t tb = 0;
+            CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, aa.tp_key, C.a_tp_key_s.as<uint16_t>(),
+                                               C.a_ord_in.as<int>(), C.a_ord.as<int>(), (int)ntp, 0, 16, st));
+            RET(ensure(C.cub_tmp, tb));
+            CK(cub::DeviceRadixSort::SortPairs(C.cub_tmp.p, tb, aa.tp_key, C.a_tp_key_s.as<uint16_t>(),
+                                               C.a_ord_in.as<int>(), C.a_ord.as<int>(), (int)ntp, 0, 16, st));
+        }
+        klaunch += 2;
         const int ibits = bits_for((unsigned long long)ntp);
         if (ibits + vbits > 64) return fail(PSIB_ERR_OVERFLOW, "grid and chunk too large for a 64-bit record key");
         AnnClipArgs ca = {};
@@ -1360,7 +1379,7 @@ int run_annihilation(Call& c)
             CK(cudaMemsetAsync(&sm[S_CNT], 0, 24, st));
             CK(cudaMemsetAsync(&sm[S_HEAD], 0, 16, st));
             ca.n = ntp;
-            ca.list = nullptr;
+            ca.list = C.a_ord.as<int>();
             ca.head = &sm[S_HEAD];
             ca.scratch = C.scratch.p;
             CK(launch_ann_clip(ca, false, clip_grid, clip_block, st));

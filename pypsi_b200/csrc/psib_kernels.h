@@ -246,6 +246,8 @@ struct AnnArgs {
     long long tp_base;
     long long *tp_cnt;        // per slot (count)
     int2 *tpairs;             // (side-A tet, side-B tet) of every tet pair of the chunk
+    uint16_t *tp_key;         // emit: per tet pair, larger voxel boxes of the pair's walk first
+    GridDev g;                // the grid (tet-pair keys)
     unsigned *status;
     // queries: sorted unique cell keys of the registrations, their runs
     const unsigned long long *run_key;
