@@ -19,6 +19,8 @@
 // reference's double-precision operations.
 #include "psib_clip.cuh"
 
+#include <cstdlib>
+
 namespace psib {
 
 // The polyhedron of a tet pair: the intersection of two tets, the window and a
@@ -672,13 +674,32 @@ __device__ __forceinline__ void ann_clip_loop(const AnnClipArgs& a)
     }
 }
 
+// Main kernel variants by the minimum number of resident 128-thread blocks per
+// SM the register allocation must allow (0: no cap); PSIB_ANN_MINB picks one.
+// Measured at 64^3 -> 128^3: 96 registers (no cap) 201 M tet pairs/s, 80
+// (6 blocks) 216 M/s, 64 (8 blocks, a few spills) 227 M/s.
+template <int MINB>
+__global__ void __launch_bounds__(128, MINB) k_ann_clip_b(AnnClipArgs a) { ann_clip_loop<NS_MAIN, false>(a); }
 __global__ void __launch_bounds__(128) k_ann_clip(AnnClipArgs a) { ann_clip_loop<NS_MAIN, false>(a); }
 __global__ void __launch_bounds__(64) k_ann_clip_big(AnnClipArgs a) { ann_clip_loop<NS_BIG, true>(a); }
+
+constexpr int DEFAULT_MINB_ANN = 8;
+
+template <class F>
+static auto ann_variant(F&& f)
+{
+    const char* v = getenv("PSIB_ANN_MINB");
+    switch (v && *v ? atoi(v) : DEFAULT_MINB_ANN) {
+    case 6: return f(k_ann_clip_b<6>);
+    case 8: return f(k_ann_clip_b<8>);
+    default: return f(k_ann_clip);
+    }
+}
 
 cudaError_t launch_ann_clip(const AnnClipArgs& a, bool big, int grid, int block, cudaStream_t s)
 {
     if (big) k_ann_clip_big<<<grid, block, 0, s>>>(a);
-    else k_ann_clip<<<grid, block, 0, s>>>(a);
+    else ann_variant([&](auto k) { k<<<grid, block, 0, s>>>(a); return 0; });
     return cudaGetLastError();
 }
 
@@ -688,7 +709,7 @@ int ann_blocks_per_sm(bool big, int block)
 {
     int n = 0;
     cudaError_t e = big ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_ann_clip_big, block, 0)
-                        : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_ann_clip, block, 0);
+                        : ann_variant([&](auto k) { return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, block, 0); });
     if (e != cudaSuccess) { cudaGetLastError(); return 1; }
     return n > 0 ? n : 1;
 }
