@@ -133,3 +133,45 @@ def test_voxels_fails_loudly_without_gpu(psi):
     with pytest.raises(RuntimeError, match="no CUDA device"):
         psi.voxels(g, m)
     assert not g.fields["m"].any()
+
+
+def test_query_and_vdf_argument_errors(psi):
+    """PSI.RStarTree / PSI.VDF keep the reference's argument checks
+    (src/PSI.c:817-835, :865-876, :1022-1040); the C entry points reject
+    missing arrays before any device work."""
+    import ctypes
+
+    import pypsi_b200
+
+    m = psi.Mesh(loader="block", pos=np.random.default_rng(1).random((3, 3, 3, 3)))
+    with pytest.raises(TypeError):
+        psi.RStarTree("not a mesh")
+    with pytest.raises(TypeError):
+        psi.VDF(m, (0.5, 0.5))
+    with pytest.raises(TypeError):
+        psi.VDF(m, (0.5, 0.5, 0.5), tree="not a tree")
+    tree = psi.RStarTree(m)
+    assert tree.mesh is m
+    with pytest.raises(TypeError, match="two tuples of 3 values"):
+        tree.query(((0, 0), (1, 1)))
+    lib = pypsi_b200.lib
+    lib.psib_last_error.restype = ctypes.c_char_p
+    off = (ctypes.c_longlong * 2)()
+    assert lib.psib_query_elements(None, None, None, ctypes.c_longlong(1), off, None, ctypes.c_longlong(0), None) == 1
+    assert b"window" in lib.psib_last_error()
+    assert lib.psib_sample_vdf(None, None, None, ctypes.c_longlong(1), ctypes.c_double(1.0), 0, off, None, None,
+                               ctypes.c_longlong(0), None) == 1
+    assert b"window" in lib.psib_last_error()
+
+
+def test_query_and_vdf_fail_loudly_without_gpu(psi):
+    if psi.device_count() > 0:
+        pytest.skip("a GPU is present")
+    m = psi.Mesh(loader="block", pos=np.random.default_rng(1).random((3, 3, 3, 3)), periodic_box=((0, 0, 0), (1, 1, 1)))
+    with pytest.raises(RuntimeError, match="no CUDA device"):
+        psi.VDF(m, (0.5, 0.5, 0.5))
+    with pytest.raises(RuntimeError, match="no CUDA device"):
+        psi.RStarTree(m).query(((0, 0, 0), (1, 1, 1)))
+    g = psi.Grid(n=(4, 4, 4))
+    with pytest.raises(RuntimeError, match="no CUDA device"):
+        psi.voxels(g, m, mode="annihilation")
