@@ -56,9 +56,10 @@ def parse():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--ann-n", type=int, default=64, help="ann: particles per side (smaller cases for profiling)")
     ap.add_argument("--ann-grid", type=int, default=128, help="ann: grid cells per side")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c5", "ann"],
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c5", "ann", "loaders"],
                     help="c2: the headline (128^3 -> 256^3, order 2); c3: 512 uneven cutouts in one batch; "
-                         "c5: 256^3 -> 512^3 with stretch refinement; ann: annihilation mode, 64^3 -> 128^3")
+                         "c5: 256^3 -> 512^3 with stretch refinement; ann: annihilation mode, 64^3 -> 128^3; "
+                         "loaders: Gadget-2 / gevolution snapshot loading (host only)")
     args = ap.parse_args()
     if (args.n_part, args.n_grid) != (N_PART, N_GRID) or args.precision != "both":
         args.no_cpu_baseline = True
@@ -397,6 +398,62 @@ def run_ann(args):
         line["cpu_baseline"] = _ann_sample_line(kind, nb, pairs_c, secs, 1, "in all")
     capi.lib.psib_release_device_memory()
     if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- snapshot loaders (--workload loaders)
+def run_loaders(args):
+    """Host code only: PSI.Mesh(loader='gadget2' | 'gevolution') on a synthetic
+    128^3 snapshot (a seeded displaced lattice in shuffled file order, read from
+    the page cache) against the reference's own load_gadget2 / load_gevolution
+    (oracle/_ref), in particles/s; every array is compared."""
+    import numpy as np
+
+    sys.path[:0] = [os.path.join(ROOT, "oracle"), os.path.join(ROOT, "tests")]
+    import oracle as O
+    from snapshots import make_snapshot
+
+    from pypsi_b200 import PSI
+
+    rank, _, _ = env_rank()
+    if rank != 0:
+        return
+    n = 128
+    lines = []
+    with tempfile.TemporaryDirectory() as d:
+        for flav in ("gadget2", "gevolution"):
+            path = os.path.join(d, flav)
+            make_snapshot(path, n, flavour=flav, seed=1)
+            open(path, "rb").read()
+            ours, ref = [], []
+            for _ in range(max(1, args.warmup)):
+                mesh = PSI.Mesh(loader=flav, filename=path)
+            for _ in range(args.steps):
+                t0 = time.perf_counter()
+                mesh = PSI.Mesh(loader=flav, filename=path)
+                ours.append(time.perf_counter() - t0)
+                if O.available("reference"):
+                    t0 = time.perf_counter()
+                    r = O.load_snapshot("reference", path, flav)
+                    ref.append(time.perf_counter() - t0)
+            same = None
+            if ref:
+                same = all(np.array_equal(a, b) for a, b in zip((mesh.pos, mesh.vel, mesh.mass, mesh.connectivity),
+                                                                 r[:4]))
+            t = statistics.median(ours)
+            line = {"metric": f"particles/s loaded, {flav} snapshot of 128^3 particles", "value": n ** 3 / t,
+                    "unit": "particles/s", "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
+                    "ms_per_step": 1000 * t, "higher_is_better": True, "scaling": "none", "vs_baseline": None,
+                    "dtype": "f32->f64", "data": "synthetic: seeded displaced lattice, shuffled file order",
+                    "config": {"workload": f"PSI.Mesh(loader='{flav}') of a {os.path.getsize(path) >> 20} MiB file "
+                                           "in the page cache, host threads " + str(len(os.sched_getaffinity(0)))},
+                    "arrays_equal_reference": same}
+            if ref:
+                tr = statistics.median(ref)
+                line["cpu_baseline"] = {"value": n ** 3 / tr, "unit": "particles/s", "cores": 1, "kind": "reference",
+                                        "sample": "the same file through the reference's own loader"}
+            lines.append(line)
+    for line in lines:
         print(json.dumps(line), flush=True)
 
 
@@ -784,7 +841,9 @@ def run_ours(args):
 
 def main():
     args = parse()
-    if args.impl == "reference" and args.workload == "ann":
+    if args.workload == "loaders":
+        run_loaders(args)
+    elif args.impl == "reference" and args.workload == "ann":
         run_reference_ann(args)
     elif args.impl == "reference":
         run_reference(args)

@@ -23,8 +23,9 @@
  * and a block whose length marker disagrees with npart are errors here.
  *
  * The IDs are read first and the position and velocity blocks are then
- * streamed in chunks straight into their rows, so a load needs no float
- * copy of the particle data.
+ * streamed in chunks straight into their rows, so a load needs no float copy
+ * of the particle data; the scatter of each chunk, the masses and the
+ * connectivity are filled by up to 16 host threads.
  */
 #include <algorithm>
 #include <cmath>
@@ -32,6 +33,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "psi_b200.h"
@@ -116,6 +118,21 @@ inline int tile_cube_to_slot(int i, int j, int k)
     return 8 * gray_inv(o) + gray_inv(in);
 }
 
+// Run f(begin, end) over [0, n) in contiguous ranges on up to 16 host threads.
+template <class F>
+void parallel_for(long long n, F f)
+{
+    const long long hw = std::max(1u, std::thread::hardware_concurrency());
+    const long long nt = std::min<long long>(std::min<long long>(hw, 16), std::max<long long>(1, n / 16384));
+    if (nt <= 1) {
+        f(0, n);
+        return;
+    }
+    std::vector<std::thread> th;
+    for (long long t = 0; t < nt; ++t) th.emplace_back(f, n * t / nt, n * (t + 1) / nt);
+    for (auto& x : th) x.join();
+}
+
 template <typename ID>
 int load(const char* filename, bool tiled, long long npart, double* pos, double* vel, double* mass, int* conn)
 {
@@ -163,8 +180,9 @@ int load(const char* filename, bool tiled, long long npart, double* pos, double*
         if (!marker(fp, id_bytes)) return fail(PSIB_ERR_ARG, "bad particle ID block");
     }
 
-    // positions and velocities, float32 widened to double, scattered to their rows
-    std::vector<float> buf(3u << 16);
+    // positions and velocities, float32 widened to double, scattered to their rows (the
+    // IDs are distinct, so the threads of a chunk write distinct rows)
+    std::vector<float> buf(3u << 20);
     for (int blk = 0; blk < 2; ++blk) {
         double* dst = blk ? vel : pos;
         if (!fp.seek(blk ? vel_at : pos_at) || !marker(fp, vec_bytes))
@@ -172,44 +190,67 @@ int load(const char* filename, bool tiled, long long npart, double* pos, double*
         for (long long p0 = 0; p0 < npart; p0 += (long long)buf.size() / 3) {
             size_t cnt = (size_t)std::min<long long>((long long)buf.size() / 3, npart - p0);
             if (!fp.read(buf.data(), cnt * 12)) return fail(PSIB_ERR_ARG, "truncated particle block");
-            for (size_t q = 0; q < cnt; ++q) {
-                double* d = dst + 3 * (size_t)row[(size_t)(p0 + (long long)q)];
-                d[0] = buf[3 * q];
-                d[1] = buf[3 * q + 1];
-                d[2] = buf[3 * q + 2];
-            }
+            parallel_for((long long)cnt, [&](long long b, long long e) {
+                for (long long q = b; q < e; ++q) {
+                    double* d = dst + 3 * (size_t)row[(size_t)(p0 + q)];
+                    d[0] = buf[3 * q];
+                    d[1] = buf[3 * q + 1];
+                    d[2] = buf[3 * q + 2];
+                }
+            });
         }
         if (!marker(fp, vec_bytes)) return fail(PSIB_ERR_ARG, blk ? "bad velocity block" : "bad position block");
     }
 
     const double m = h.mass1 / (double)npart;
-    for (long long e = 0; e < npart; ++e) mass[e] = m;
+    parallel_for(npart, [&](long long b, long long e) {
+        for (long long i = b; i < e; ++i) mass[i] = m;
+    });
 
     if (!tiled) {
-        for (long long e = 0; e < npart; ++e) {
-            long long i = e / (n * n), j = (e / n) % n, k = e % n;
-            for (int c = 0; c < 8; ++c)
-                conn[8 * e + c] = (int)(n * n * ((i + (c >> 2)) % n) + n * ((j + ((c >> 1) & 1)) % n) + (k + (c & 1)) % n);
-        }
-    } else {
-        const long long tn = n / 4;
-        for (long long p = 0; p < npart; ++p) {
-            long long t = p / 64;
-            long long tile[3] = {t % tn, (t / tn) % tn, t / (tn * tn)};  // (ti, tj, tk), ti fastest
-            int at[3];
-            tile_slot_to_cube((int)(p % 64), at);
-            for (int c = 0; c < 8; ++c) {
-                int q[3];
-                long long dt[3];
-                for (int a = 0; a < 3; ++a) {
-                    q[a] = at[a] + ((c >> (2 - a)) & 1);
-                    dt[a] = q[a] / 4;
-                    q[a] %= 4;
+        // element (i, j, k) joins the lattice points (i + ii, j + jj, k + kk) mod n
+        const long long n2 = n * n;
+        parallel_for(n, [&](long long i0, long long i1) {
+            for (long long i = i0; i < i1; ++i) {
+                const long long a[2] = {n2 * i, n2 * (i + 1 == n ? 0 : i + 1)};
+                for (long long j = 0; j < n; ++j) {
+                    const long long b[2] = {n * j, n * (j + 1 == n ? 0 : j + 1)};
+                    int* c = conn + 8 * (n2 * i + n * j);
+                    for (long long k = 0; k < n; ++k, c += 8) {
+                        const long long kk[2] = {k, k + 1 == n ? 0 : k + 1};
+                        for (int v = 0; v < 8; ++v) c[v] = (int)(a[v >> 2] + b[(v >> 1) & 1] + kk[v & 1]);
+                    }
                 }
-                long long flat = (tile[0] + dt[0]) % tn + tn * ((tile[1] + dt[1]) % tn) + tn * tn * ((tile[2] + dt[2]) % tn);
-                conn[8 * p + c] = (int)(64 * flat + tile_cube_to_slot(q[0], q[1], q[2]));
             }
-        }
+        });
+    } else {
+        // per tile: the flat index of its 8 upper neighbour tiles; per slot: its cube position;
+        // per position in the 5^3 block of a slot and its upper neighbours: the slot inside the tile
+        const long long tn = n / 4;
+        int cube[64][3];
+        for (int sl = 0; sl < 64; ++sl) tile_slot_to_cube(sl, cube[sl]);
+        parallel_for(tn * tn * tn, [&](long long t0, long long t1) {
+            for (long long t = t0; t < t1; ++t) {
+                const long long ti = t % tn, tj = (t / tn) % tn, tk = t / (tn * tn);
+                const long long tip = ti + 1 == tn ? 0 : ti + 1, tjp = tj + 1 == tn ? 0 : tj + 1,
+                                tkp = tk + 1 == tn ? 0 : tk + 1;
+                long long nbt[8]; // neighbour tile (di, dj, dk) at 4 di + 2 dj + dk
+                for (int d = 0; d < 8; ++d)
+                    nbt[d] = ((d >> 2) ? tip : ti) + tn * (((d >> 1) & 1) ? tjp : tj) + tn * tn * ((d & 1) ? tkp : tk);
+                for (int sl = 0; sl < 64; ++sl) {
+                    int* c = conn + 8 * (64 * t + sl);
+                    for (int v = 0; v < 8; ++v) {
+                        int q[3], d = 0;
+                        for (int ax = 0; ax < 3; ++ax) {
+                            q[ax] = cube[sl][ax] + ((v >> (2 - ax)) & 1);
+                            d |= (q[ax] >> 2) << (2 - ax);
+                            q[ax] &= 3;
+                        }
+                        c[v] = (int)(64 * nbt[d] + tile_cube_to_slot(q[0], q[1], q[2]));
+                    }
+                }
+            }
+        });
     }
     return PSIB_OK;
 }
