@@ -56,10 +56,11 @@ def parse():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--ann-n", type=int, default=64, help="ann: particles per side (smaller cases for profiling)")
     ap.add_argument("--ann-grid", type=int, default=128, help="ann: grid cells per side")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c5", "ann", "loaders"],
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c5", "ann", "loaders", "vdf", "quad"],
                     help="c2: the headline (128^3 -> 256^3, order 2); c3: 512 uneven cutouts in one batch; "
                          "c5: 256^3 -> 512^3 with stretch refinement; ann: annihilation mode, 64^3 -> 128^3; "
-                         "loaders: Gadget-2 / gevolution snapshot loading (host only)")
+                         "loaders: Gadget-2 / gevolution snapshot loading (host only); vdf: PSI.VDF at 2^20 points; "
+                         "quad: 27-node elements")
     args = ap.parse_args()
     if (args.n_part, args.n_grid) != (N_PART, N_GRID) or args.precision != "both":
         args.no_cpu_baseline = True
@@ -396,6 +397,175 @@ def run_ann(args):
             if secs > 12.0:
                 break
         line["cpu_baseline"] = _ann_sample_line(kind, nb, pairs_c, secs, 1, "in all")
+    capi.lib.psib_release_device_memory()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- PSI.VDF (--workload vdf)
+VDF_N, VDF_POINTS = 64, 1 << 20
+VDF_METRIC = "sample points/s, PSI.VDF batched at 2^20 random points of a 64³ periodic sheet (rms 2 cells)"
+
+
+def run_vdf(args):
+    """Phase-space samples at 2^20 random points of a periodic 64^3 Zel'dovich
+    sheet (rms 2 cells, box 100, the tree's window = the box), unrefined:
+    psib_sample_vdf on device arrays (CUDA events), the same on host arrays
+    (e2e), and the reference's psi_sample_vdf per point over its own tree."""
+    import numpy as np
+    import torch
+
+    from pypsi_b200 import capi
+    from pypsi_b200.synth import zeldovich
+
+    rank, world, local = env_rank()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pos, vel = zeldovich(VDF_N, 2.0, 777 + rank)
+    pts = np.random.default_rng(5 + rank).uniform(0.0, 100.0, (VDF_POINTS, 3))
+    dpos = torch.from_numpy(pos.reshape(-1, 3)).to(dev)
+    dvel = torch.from_numpy(vel.reshape(-1, 3)).to(dev)
+    dpts = torch.from_numpy(pts).to(dev)
+    kw = dict(block_dims=(VDF_N,) * 3, periodic_box=BOX)
+
+    def step():
+        return capi.sample_vdf(dpts, dpos, vel=dvel, **kw)
+
+    for _ in range(max(1, args.warmup)):
+        off, rho, v = step()
+    torch.cuda.synchronize()
+    nsamp = int(off[-1].item())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ck = Clocks(local)
+    ck.__enter__()
+    e0.record()
+    for _ in range(args.steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    ck.__exit__()
+    ms = e0.elapsed_time(e1) / args.steps
+    line = {"metric": VDF_METRIC, "value": VDF_POINTS / (ms * 1e-3), "unit": "points/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": DATA,
+            "config": {"workload": "64^3 periodic lattice (box 100, rms 2 cells), 2^20 uniform points, no refinement, "
+                                   "tree window = the box", "samples": nsamp},
+            "gpu_launches": None, "clocks": ck.summary()}
+    if not args.no_e2e:
+        capi.sample_vdf(pts, pos.reshape(-1, 3), vel=vel.reshape(-1, 3), **kw)
+        ts = []
+        for _ in range(max(1, args.e2e_steps)):
+            t0 = time.perf_counter()
+            capi.sample_vdf(pts, pos.reshape(-1, 3), vel=vel.reshape(-1, 3), **kw)
+            ts.append(time.perf_counter() - t0)
+        t = statistics.median(ts)
+        line["e2e"] = {"value": VDF_POINTS / t, "unit": "points/s", "h2d_bytes_per_step": int(pts.nbytes + pos.nbytes +
+                       vel.nbytes), "d2h_bytes_per_step": int(8 * (VDF_POINTS + 1) + 32 * nsamp),
+                       "api": "capi.sample_vdf on host numpy arrays (psib_sample_vdf, host memory)",
+                       "ms_per_step": 1000 * t}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sys.path[:0] = [os.path.join(ROOT, "oracle")]
+        import oracle as O
+
+        kind = "reference" if O.available("reference") else "restatement"
+        conn = O.block_connectivity((VDF_N,) * 3, True)
+        n = 1 << 18 if kind == "reference" else 64  # the reference: ~47 K points/s after a ~4 s tree build
+        _, secs = O.sample_vdf_many(kind, pos.reshape(-1, 3), conn, pts[:n], vel=vel.reshape(-1, 3),
+                                    periodic_box=BOX, window=BOX)
+        line["cpu_baseline"] = {"value": n / secs, "unit": "points/s", "cores": 1,
+                                "kind": "reference" if kind == "reference" else "port",
+                                "sample": f"the first {n} points, psi_sample_vdf per point over a tree built once "
+                                          f"({secs:.1f} s)"}
+    capi.lib.psib_release_device_memory()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- triquadratic elements (--workload quad)
+def quad_mesh(ne, seed, box=100.0):
+    """27-node elements: node (a,b,c) of element (i,j,k) is point (2i+a, 2j+b, 2k+c) of an open
+    (2 ne + 1)^3 lattice of the box, displaced by a Zel'dovich field (rms 1 lattice cell)."""
+    import numpy as np
+
+    from pypsi_b200.synth import zeldovich
+
+    nn = 2 * ne + 1
+    pos, vel = zeldovich(nn, 1.0, seed, box=box * nn / (nn - 1), wrap=False)
+    conn = np.empty((ne, ne, ne, 27), dtype=np.int32)
+    i, j, k = np.meshgrid(np.arange(ne), np.arange(ne), np.arange(ne), indexing="ij")
+    for a in range(3):
+        for b in range(3):
+            for c in range(3):
+                conn[..., 9 * a + 3 * b + c] = ((2 * i + a) * nn + (2 * j + b)) * nn + (2 * k + c)
+    return pos.reshape(-1, 3), vel.reshape(-1, 3), conn.reshape(-1, 27)
+
+
+def run_quad(args):
+    """32^3 triquadratic elements (65^3 nodes) on 128^3 voxels, all order-2
+    fields, unrefined: mixed and FP64 tets/s on device arrays, the reference's
+    psi_voxels on 4^3-element sub-blocks (own window at the same voxel size)."""
+    import numpy as np
+    import torch
+
+    from pypsi_b200 import capi
+
+    rank, world, local = env_rank()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    ne, ng = 32, 128
+    pos, vel, conn = quad_mesh(ne, 31 + rank)
+    dpos, dvel = torch.from_numpy(pos).to(dev), torch.from_numpy(vel).to(dev)
+    dconn = torch.from_numpy(conn).to(dev)
+    shapes = {"m": (), "x": (3,), "v": (3,), "xx": (3, 3), "xv": (3, 3), "vv": (3, 3)}
+    fields = {f: torch.zeros((ng,) * 3 + sh, dtype=torch.float64, device=dev) for f, sh in shapes.items()}
+    out = {}
+    for prec in ("mixed", "fp64"):
+        def step():
+            return capi.voxels_device(fields, (ng,) * 3, BOX, dpos, dvel, connectivity=dconn, precision=prec)
+
+        for _ in range(max(1, args.warmup)):
+            st = step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            step()
+        e1.record()
+        torch.cuda.synchronize()
+        out[prec] = (e0.elapsed_time(e1) / args.steps, st)
+    ms, st = out["mixed"]
+    line = {"metric": "tets/s, 27-node elements 32³ (65³ nodes) → 128³, order 2, mixed", "value": st["tets"] / (ms * 1e-3),
+            "unit": "tets/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+            "data": "synthetic: seeded Zel'dovich-displaced open node lattice, element mass 1",
+            "config": {"workload": "32^3 triquadratic elements on a 128^3 grid over the box, fields m,x,v,xx,xv,vv, "
+                                   "no refinement"},
+            "fp64": {"value": out["fp64"][1]["tets"] / (out["fp64"][0] * 1e-3), "ms_per_step": out["fp64"][0]},
+            "work": {"tets": st["tets"], "fragments": st["fragments"]}}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sys.path[:0] = [os.path.join(ROOT, "oracle")]
+        import oracle as O
+
+        if O.available("reference"):
+            d = BOX[1][0] / ng
+            tets, secs, nb = 0, 0.0, 0
+            c4 = conn.reshape(ne, ne, ne, 27)
+            for o in range(0, ne ** 3 // 64):
+                a, b, c = 4 * (o // 64), 4 * ((o // 8) % 8), 4 * (o % 8)
+                sub = np.ascontiguousarray(c4[a:a + 4, b:b + 4, c:c + 4].reshape(-1, 27))
+                p = pos[np.unique(sub)]
+                lo, hi = np.floor(p.min(0) / d) - 1, np.ceil(p.max(0) / d) + 1
+                t0 = time.perf_counter()
+                O.voxelize("reference", n=tuple(int(v) for v in hi - lo), bounds=(tuple(lo * d), tuple(hi * d)),
+                           pos=pos, vel=vel, conn=sub, fields=FIELDS)
+                secs += time.perf_counter() - t0
+                tets += 6 * sub.shape[0]
+                nb += 1
+                if secs > 10.0:
+                    break
+            line["cpu_baseline"] = {"value": tets / secs, "unit": "tets/s", "cores": 1, "kind": "reference",
+                                    "sample": f"{nb} sub-blocks of 4^3 elements ({tets} tets, {secs:.1f} s), each on "
+                                              "a window covering it at the 128^3 voxel size"}
     capi.lib.psib_release_device_memory()
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -849,6 +1019,10 @@ def main():
         run_reference(args)
     elif args.workload == "ann":
         run_ann(args)
+    elif args.workload == "vdf":
+        run_vdf(args)
+    elif args.workload == "quad":
+        run_quad(args)
     elif args.workload == "c5":
         run_c5(args)
     elif args.workload == "c3":

@@ -412,3 +412,39 @@ def sample_vdf(kind, pos, conn, point, vel=None, mass=None, periodic_box=None, w
     libc.free(C.cast(rp, C.c_void_p))
     libc.free(C.cast(vp, C.c_void_p))
     return rho, v
+
+
+def sample_vdf_many(kind, pos, conn, points, vel=None, mass=None, periodic_box=None, window=None, reftol=1.0,
+                    maxlvl=0):
+    """sample_vdf at many points: for the reference, one tree built once (the
+    tree a PSI.RStarTree holds) and psi_sample_vdf per point.  Returns the list
+    of (rho, vel) per point and the seconds spent sampling (tree build excluded)."""
+    import time
+
+    if kind != "reference":
+        t0 = time.perf_counter()
+        res = [sample_vdf(kind, pos, conn, p, vel, mass, periodic_box, window, reftol, maxlvl) for p in points]
+        return res, time.perf_counter() - t0
+    og, ps, keep, box = _meshes(pos, conn, vel, mass, periodic_box)
+    lib = _lib(kind)
+    win = np.ascontiguousarray(box if window is None else window, dtype=np.float64).reshape(2, 3)
+    tree = _PsiRtree()
+    libc = C.CDLL(None)
+    lib.psi_sample_vdf.argtypes = [_Rvec, C.POINTER(_PsiMesh), C.c_void_p, C.POINTER(C.POINTER(C.c_double)),
+                                   C.POINTER(C.POINTER(C.c_double)), C.POINTER(C.c_int), C.c_double, C.c_int]
+    res = []
+    with _quiet_stdout():
+        lib.psi_rtree_from_mesh(C.byref(tree), C.byref(ps), _dp(win))
+        t0 = time.perf_counter()
+        for p in np.asarray(points, dtype=np.float64).reshape(-1, 3):
+            rp, vp, ns = C.POINTER(C.c_double)(), C.POINTER(C.c_double)(), C.c_int()
+            lib.psi_sample_vdf(_Rvec(*p), C.byref(ps), C.cast(C.byref(tree), C.c_void_p), C.byref(rp), C.byref(vp),
+                               C.byref(ns), float(reftol), int(maxlvl))
+            n = ns.value
+            res.append((np.ctypeslib.as_array(rp, shape=(n,)).copy() if n else np.zeros(0),
+                        np.ctypeslib.as_array(vp, shape=(n, 3)).copy() if n else np.zeros((0, 3))))
+            libc.free(C.cast(rp, C.c_void_p))
+            libc.free(C.cast(vp, C.c_void_p))
+        secs = time.perf_counter() - t0
+        lib.psi_rtree_destroy(C.byref(tree))
+    return res, secs
