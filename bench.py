@@ -463,6 +463,21 @@ def run_vdf(args):
                        vel.nbytes), "d2h_bytes_per_step": int(8 * (VDF_POINTS + 1) + 32 * nsamp),
                        "api": "capi.sample_vdf on host numpy arrays (psib_sample_vdf, host memory)",
                        "ms_per_step": 1000 * t}
+    if not args.no_e2e:
+        # the drop-in call one point at a time, as a loop over the reference's PSI.VDF with a tree would run
+        from pypsi_b200 import PSI
+
+        mesh = PSI.Mesh(loader="block", pos=pos, vel=vel, periodic_box=BOX)
+        tree = PSI.RStarTree(mesh)
+        PSI.VDF(mesh, tuple(pts[0]), tree)
+        npt = 2000
+        t0 = time.perf_counter()
+        for p in pts[:npt]:
+            PSI.VDF(mesh, tuple(p), tree)
+        t = time.perf_counter() - t0
+        line["one_point_per_call"] = {"value": npt / t, "unit": "points/s",
+                                      "api": "PSI.VDF(mesh, point, tree) in a Python loop, the tree's device index "
+                                             "built by the first call"}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         sys.path[:0] = [os.path.join(ROOT, "oracle")]
         import oracle as O

@@ -247,6 +247,26 @@ int psib_sample_vdf(const psib_mesh *mesh, const double window[2][3], const doub
                     double refine_tolerance, int refine_max_lvl, long long *offsets, double *rho, double *vel,
                     long long capacity, const psib_options *opt);
 
+/* A persistent element index: what PSI.RStarTree(mesh) builds once and its
+ * queries reuse (src/PSI.c:865-896, src/rtree.c:48-73).  psib_index_create
+ * copies the mesh to the device, culls its elements against `window`, keeps
+ * their boxes and the cell index over them, and returns a handle; the index
+ * holds the mesh as it was then.  psib_index_query and psib_index_sample_vdf
+ * then answer exactly as psib_query_elements and psib_sample_vdf with the same
+ * mesh and window, at the cost of the query alone (no upload, no index build):
+ * the form for many small calls, PSI.VDF(mesh, point, tree) in a loop.  Points,
+ * boxes and outputs follow options->memory (host by default).  An index lives
+ * on the device that was current at its creation until psib_index_destroy. */
+typedef struct psib_index psib_index;
+int psib_index_create(const psib_mesh *mesh, const double window[2][3], psib_index **index,
+                      const psib_options *opt);
+int psib_index_query(psib_index *index, const double *boxes, long long nboxes, long long *offsets, int *elements,
+                     long long capacity, const psib_options *opt);
+int psib_index_sample_vdf(psib_index *index, const double *points, long long npoints, double refine_tolerance,
+                          int refine_max_lvl, long long *offsets, double *rho, double *vel, long long capacity,
+                          const psib_options *opt);
+void psib_index_destroy(psib_index *index);
+
 /* Snapshot readers: a Gadget-2 (format 1) file as the periodic trilinear mesh
  * of PSI.Mesh(loader='gadget2') (src/mesh.c:35-160) or, with 64-bit particle
  * IDs and particles numbered in tiles of 4^3, loader='gevolution'

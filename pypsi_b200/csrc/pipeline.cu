@@ -1681,6 +1681,12 @@ int query_status(QueryCall& q, unsigned long long* sm)
     return check_status(q.c, h);
 }
 
+int query_from_boxes(QueryCall& q, AnnArgs& aa, unsigned long long* sm, const double* boxes, long long nboxes,
+                     long long* offsets, int* elements, long long capacity);
+int vdf_from_index(QueryCall& q, AnnArgs& aa, long long kept, unsigned long long* sm, const double* points,
+                   long long npoints, double reftol, int maxlvl, long long* offsets, double* rho, double* vel,
+                   long long capacity);
+
 int query_elements_impl(QueryCall& q, const double (*window)[3], const double* boxes, long long nboxes,
                         long long* offsets, int* elements, long long capacity)
 {
@@ -1691,6 +1697,15 @@ int query_elements_impl(QueryCall& q, const double (*window)[3], const double* b
     CK(cudaMemsetAsync(sm, 0, S_WORDS * 8, st));
     AnnArgs aa;
     RET(query_elements_stage(q, window, 1.0, aa, sm));
+    return query_from_boxes(q, aa, sm, boxes, nboxes, offsets, elements, capacity);
+}
+
+// Box queries over the kept element boxes of aa (cnt_a flags, ebox).
+int query_from_boxes(QueryCall& q, AnnArgs& aa, unsigned long long* sm, const double* boxes, long long nboxes,
+                     long long* offsets, int* elements, long long capacity)
+{
+    Ctx& C = *q.C;
+    cudaStream_t st = q.c.st;
     const void* qin = nullptr;
     RET(query_input(q, C.q_in, boxes, (size_t)nboxes * 6 * sizeof(double), &qin));
     aa.qry = (const double*)qin;
@@ -1741,6 +1756,18 @@ int sample_vdf_impl(QueryCall& q, const double (*window)[3], const double* point
     RET(query_elements_stage(q, window, reftol, aa, sm));
     long long klaunch = 0, kept = 0;
     if (aa.nelem > 0) RET(build_cells(C, aa, st, klaunch, kept));
+    return vdf_from_index(q, aa, kept, sm, points, npoints, reftol, maxlvl, offsets, rho, vel, capacity);
+}
+
+// Samples at the points through the cell index of aa (kept elements, their
+// boxes, cells and runs), the mesh of q.
+int vdf_from_index(QueryCall& q, AnnArgs& aa, long long kept, unsigned long long* sm, const double* points,
+                   long long npoints, double reftol, int maxlvl, long long* offsets, double* rho, double* vel,
+                   long long capacity)
+{
+    Ctx& C = *q.C;
+    cudaStream_t st = q.c.st;
+    const psib_mesh& m = *q.c.mesh;
     const void* qin = nullptr;
     RET(query_input(q, C.q_in, points, (size_t)npoints * 3 * sizeof(double), &qin));
     aa.qry = (const double*)qin;
@@ -1806,6 +1833,129 @@ int sample_vdf_impl(QueryCall& q, const double (*window)[3], const double* point
         RET(query_output(q, vel, va.vel, (size_t)total * 3 * sizeof(double)));
     }
     return query_status(q, sm);
+}
+
+} // namespace
+
+// ---- a persistent element index (PSI.RStarTree) ----
+
+// The mesh (device copies), its kept elements' boxes and the cell index over
+// them, built once; later queries and samples reuse them.
+struct psib_index {
+    int device = 0;
+    psib_mesh mesh = {}; // device pointers into the buffers below
+    psib::AnnArgs aa = {}; // kept flags, boxes, cells and runs, pointing into the buffers below
+    long long kept = 0;
+    DevBuf pos, vel, mass, conn, ebox, cnt, reg_elem, run_key, run_off, run_cnt;
+};
+
+namespace {
+
+int copy_dev(DevBuf& dst, const void* src, size_t bytes, cudaStream_t st)
+{
+    RET(ensure(dst, bytes));
+    if (bytes && src) CK(cudaMemcpyAsync(dst.p, src, bytes, cudaMemcpyDeviceToDevice, st));
+    return PSIB_OK;
+}
+
+void free_index(psib_index* ix)
+{
+    if (!ix) return;
+    for (DevBuf* b : {&ix->pos, &ix->vel, &ix->mass, &ix->conn, &ix->ebox, &ix->cnt, &ix->reg_elem, &ix->run_key,
+                      &ix->run_off, &ix->run_cnt})
+        if (b->p) cudaFree(b->p);
+    delete ix;
+}
+
+int index_fill(QueryCall& q, const double (*window)[3], psib_index* ix)
+{
+    Ctx& C = *q.C;
+    cudaStream_t st = q.c.st;
+    const psib_mesh& m = *q.c.mesh;
+    RET(ensure(C.small, S_WORDS * 8));
+    unsigned long long* sm = C.small.as<unsigned long long>();
+    CK(cudaMemsetAsync(sm, 0, S_WORDS * 8, st));
+    psib::AnnArgs aa;
+    RET(query_elements_stage(q, window, 1.0, aa, sm));
+    long long klaunch = 0, kept = 0;
+    if (aa.nelem > 0) RET(build_cells(C, aa, st, klaunch, kept));
+    RET(query_status(q, sm));
+    const size_t np = (size_t)m.npart, ne = (size_t)m.nelem;
+    RET(copy_dev(ix->pos, q.c.pos, np * 24, st));
+    if (q.c.vel) RET(copy_dev(ix->vel, q.c.vel, np * 24, st));
+    if (q.c.mass) RET(copy_dev(ix->mass, q.c.mass, ne * 8, st));
+    if (q.c.conn) RET(copy_dev(ix->conn, q.c.conn, ne * (size_t)m.elemtype * 4, st));
+    RET(copy_dev(ix->ebox, aa.ebox, ne * 48, st));
+    RET(copy_dev(ix->cnt, aa.cnt_a, 2 * (ne + 1) * sizeof(int), st));
+    if (kept > 0) {
+        RET(copy_dev(ix->reg_elem, aa.reg_elem, (size_t)aa.nreg * sizeof(int), st));
+        RET(copy_dev(ix->run_key, aa.run_key, (size_t)aa.nruns * 8, st));
+        RET(copy_dev(ix->run_off, aa.run_off, (size_t)aa.nruns * 8, st));
+        RET(copy_dev(ix->run_cnt, aa.run_cnt, (size_t)aa.nruns * sizeof(int), st));
+    }
+    CK(cudaStreamSynchronize(st));
+    ix->device = C.device;
+    ix->kept = kept;
+    ix->mesh = m;
+    ix->mesh.pos = ix->pos.as<double>();
+    ix->mesh.vel = q.c.vel ? ix->vel.as<double>() : nullptr;
+    ix->mesh.mass = q.c.mass ? ix->mass.as<double>() : nullptr;
+    ix->mesh.connectivity = q.c.conn ? ix->conn.as<int>() : nullptr;
+    psib::AnnArgs& a = ix->aa;
+    a = psib::AnnArgs{};
+    a.nelem = aa.nelem;
+    a.cg = aa.cg;
+    a.nreg = aa.nreg;
+    a.nruns = aa.nruns;
+    a.ebox = ix->ebox.as<double>();
+    a.cnt_a = ix->cnt.as<int>();
+    a.cnt_b = ix->cnt.as<int>() + (ne + 1);
+    a.reg_elem = ix->reg_elem.as<int>();
+    a.run_key = ix->run_key.as<unsigned long long>();
+    a.run_off = ix->run_off.as<long long>();
+    a.run_cnt = ix->run_cnt.as<int>();
+    return PSIB_OK;
+}
+
+// A call on an index: its device and mesh, points and outputs in the memory options->memory names.
+int index_begin(QueryCall& q, psib_index* ix, const psib_options* opt)
+{
+    g_err.clear();
+    if (!ix) return fail(PSIB_ERR_ARG, "index is required");
+    psib_options o = {};
+    o.memory = PSIB_HOST;
+    if (opt) o = *opt;
+    if (o.memory != PSIB_HOST && o.memory != PSIB_DEVICE) return fail(PSIB_ERR_ARG, "invalid memory kind %d", o.memory);
+    if (psib_device_count() <= 0) return fail(PSIB_ERR_NODEVICE, "no CUDA device is visible");
+    CK(cudaSetDevice(ix->device));
+    RET(get_ctx(ix->device, &q.C));
+    q.host = o.memory == PSIB_HOST;
+    q.c = Call{};
+    q.c.mesh = &ix->mesh;
+    q.c.C = q.C;
+    q.c.st = q.C->own;
+    q.c.pos = ix->mesh.pos;
+    q.c.vel = ix->mesh.vel;
+    q.c.mass = ix->mesh.mass;
+    q.c.conn = ix->mesh.connectivity;
+    if (!q.host) {
+        q.user = (cudaStream_t)o.stream;
+        RET(enter_own_stream(*q.C, q.user));
+    }
+    return PSIB_OK;
+}
+
+unsigned long long* index_status(QueryCall& q, psib::AnnArgs& aa, int& rc)
+{
+    rc = ensure(q.C->small, S_WORDS * 8);
+    if (rc) return nullptr;
+    unsigned long long* sm = q.C->small.as<unsigned long long>();
+    if (cudaMemsetAsync(sm, 0, S_WORDS * 8, q.c.st) != cudaSuccess) {
+        rc = fail(PSIB_ERR_CUDA, "cudaMemsetAsync failed");
+        return nullptr;
+    }
+    aa.status = (unsigned*)&sm[S_STATUS];
+    return sm;
 }
 
 } // namespace
@@ -2135,6 +2285,66 @@ int psib_sample_vdf(const psib_mesh* mesh, const double window[2][3], const doub
     RET(query_begin(q, mesh, opt));
     return query_end(q, sample_vdf_impl(q, window, points, npoints, refine_tolerance, refine_max_lvl, offsets, rho,
                                         vel, capacity));
+}
+
+int psib_index_create(const psib_mesh* mesh, const double window[2][3], psib_index** index, const psib_options* opt)
+{
+    if (!index || !window) return fail(PSIB_ERR_ARG, "index and window are required");
+    *index = nullptr;
+    QueryCall q;
+    RET(query_begin(q, mesh, opt));
+    psib_index* ix = new psib_index();
+    const int rc = query_end(q, index_fill(q, window, ix));
+    if (rc != PSIB_OK) {
+        free_index(ix);
+        return rc;
+    }
+    *index = ix;
+    return PSIB_OK;
+}
+
+int psib_index_query(psib_index* index, const double* boxes, long long nboxes, long long* offsets, int* elements,
+                     long long capacity, const psib_options* opt)
+{
+    if (!offsets || nboxes < 0 || (nboxes > 0 && !boxes))
+        return fail(PSIB_ERR_ARG, "offsets and nboxes >= 0 boxes are required");
+    if (nboxes >= (1ll << 31)) return fail(PSIB_ERR_ARG, "at most 2^31 - 1 query boxes");
+    QueryCall q;
+    RET(index_begin(q, index, opt));
+    psib::AnnArgs aa = index->aa;
+    int rc = PSIB_OK;
+    unsigned long long* sm = index_status(q, aa, rc);
+    if (rc == PSIB_OK) rc = query_from_boxes(q, aa, sm, boxes, nboxes, offsets, elements, capacity);
+    return query_end(q, rc);
+}
+
+int psib_index_sample_vdf(psib_index* index, const double* points, long long npoints, double refine_tolerance,
+                          int refine_max_lvl, long long* offsets, double* rho, double* vel, long long capacity,
+                          const psib_options* opt)
+{
+    if (!offsets || npoints < 0 || (npoints > 0 && !points))
+        return fail(PSIB_ERR_ARG, "offsets and npoints >= 0 points are required");
+    if (npoints >= (1ll << 31)) return fail(PSIB_ERR_ARG, "at most 2^31 - 1 sample points");
+    QueryCall q;
+    RET(index_begin(q, index, opt));
+    psib::AnnArgs aa = index->aa;
+    int rc = PSIB_OK;
+    unsigned long long* sm = index_status(q, aa, rc);
+    if (rc == PSIB_OK)
+        rc = vdf_from_index(q, aa, index->kept, sm, points, npoints, refine_tolerance, refine_max_lvl, offsets, rho,
+                            vel, capacity);
+    return query_end(q, rc);
+}
+
+void psib_index_destroy(psib_index* index)
+{
+    if (!index) return;
+    int cur = 0;
+    const bool have = cudaGetDevice(&cur) == cudaSuccess;
+    if (cudaSetDevice(index->device) == cudaSuccess) cudaDeviceSynchronize();
+    free_index(index);
+    if (have) cudaSetDevice(cur);
+    cudaGetLastError();
 }
 
 } // extern "C"

@@ -713,13 +713,16 @@ static PyObject *PSI_device_count(PyObject *self, PyObject *noargs)
 /* ------------------------------------------------------------ RStarTree */
 
 /* PSI.RStarTree(mesh, initial_capacity=1024) (src/PSI.c:809-962): the spatial
- * index of the mesh's elements.  No tree is built here: the object keeps the
- * mesh and the cull window of the reference's tree (the periodic box of a
- * periodic mesh, +-1e30 for an open one, src/PSI.c:877-893), and query() tests
- * the box against every element on the GPU (psib_query_elements). */
+ * index of the mesh's elements.  It keeps the mesh and the cull window of the
+ * reference's tree (the periodic box of a periodic mesh, +-1e30 for an open
+ * one, src/PSI.c:877-893); its first query builds the library's device index
+ * (psib_index_create: the mesh, its element boxes and a cell grid over them, as
+ * the mesh is at that moment), which later queries and PSI.VDF(..., tree)
+ * reuse. */
 typedef struct {
     PyObject_HEAD PyObject *mesh;
     double window[2][3];
+    psib_index *ix;
 } RStarTree;
 
 static int RStarTree_init(RStarTree *self, PyObject *args, PyObject *kwds)
@@ -732,6 +735,10 @@ static int RStarTree_init(RStarTree *self, PyObject *args, PyObject *kwds)
     for (int i = 0; i < 3; ++i) {
         self->window[0][i] = mesh->periodic ? mesh->box[0][i] : -1.0e30;
         self->window[1][i] = mesh->periodic ? mesh->box[1][i] : 1.0e30;
+    }
+    if (self->ix) {
+        psib_index_destroy(self->ix);
+        self->ix = NULL;
     }
     Py_INCREF(mesh);
     swap_ref(&self->mesh, (PyObject *)mesh);
@@ -748,8 +755,44 @@ static PyObject *RStarTree_new(PyTypeObject *type, PyObject *args, PyObject *kwd
 
 static void RStarTree_dealloc(RStarTree *self)
 {
+    if (self->ix) psib_index_destroy(self->ix);
     Py_XDECREF(self->mesh);
     Py_TYPE(self)->tp_free((PyObject *)self);
+}
+
+/* The tree's device index, built on first use (0, or -1 with an exception set). */
+static int tree_index(RStarTree *self, const char *what)
+{
+    if (self->ix) return 0;
+    if (!self->mesh) {
+        PyErr_SetString(PyExc_ValueError, "RStarTree has no mesh");
+        return -1;
+    }
+    psib_mesh m;
+    mesh_view((Mesh *)self->mesh, &m);
+    psib_index *ix = NULL;
+    int rc;
+    Py_BEGIN_ALLOW_THREADS rc = psib_index_create(&m, (const double(*)[3])self->window, &ix, NULL);
+    Py_END_ALLOW_THREADS if (rc != PSIB_OK)
+    {
+        raise_status_of(what, rc);
+        return -1;
+    }
+    self->ix = ix;
+    return 0;
+}
+
+/* A float64 / int32 array of the first n entries of `a` (which holds at least n). */
+static PyObject *head_of(PyObject *a, npy_intp n)
+{
+    PyArrayObject *arr = (PyArrayObject *)a;
+    const int nd = PyArray_NDIM(arr);
+    npy_intp dims[2] = {n, nd > 1 ? PyArray_DIMS(arr)[1] : 0};
+    PyObject *out = PyArray_SimpleNew(nd, dims, PyArray_TYPE(arr));
+    if (!out) return NULL;
+    const size_t row = (size_t)PyArray_ITEMSIZE(arr) * (nd > 1 ? (size_t)dims[1] : 1);
+    if (n > 0) memcpy(PyArray_DATA((PyArrayObject *)out), PyArray_DATA(arr), (size_t)n * row);
+    return out;
 }
 
 /* src/PSI.c:817-862: int32 indices of the elements whose box touches `box` */
@@ -763,28 +806,31 @@ static PyObject *RStarTree_query(RStarTree *self, PyObject *args, PyObject *kwds
         PyErr_SetString(PyExc_TypeError, "Query box must be a tuple containing two tuples of 3 values each");
         return NULL;
     }
-    if (!self->mesh) {
-        PyErr_SetString(PyExc_ValueError, "RStarTree has no mesh");
-        return NULL;
-    }
-    psib_mesh m;
-    mesh_view((Mesh *)self->mesh, &m);
+    if (tree_index(self, "PSI.RStarTree.query") < 0) return NULL;
     long long off[2] = {0, 0};
-    int rc;
-    Py_BEGIN_ALLOW_THREADS rc = psib_query_elements(&m, (const double(*)[3])self->window, q, 1, off, NULL, 0, NULL);
-    Py_END_ALLOW_THREADS if (rc != PSIB_OK) return raise_status_of("PSI.RStarTree.query", rc);
-    npy_intp nd[1] = {(npy_intp)off[1]};
-    PyObject *out = PyArray_SimpleNew(1, nd, NPY_INT32);
-    if (!out) return NULL;
-    if (off[1] > 0) {
+    npy_intp cap = 1024;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        PyObject *out = PyArray_SimpleNew(1, &cap, NPY_INT32);
+        if (!out) return NULL;
         int *dst = (int *)PyArray_DATA((PyArrayObject *)out);
-        Py_BEGIN_ALLOW_THREADS rc = psib_query_elements(&m, (const double(*)[3])self->window, q, 1, off, dst, off[1], NULL);
-        Py_END_ALLOW_THREADS if (rc != PSIB_OK) {
+        int rc;
+        Py_BEGIN_ALLOW_THREADS rc = psib_index_query(self->ix, q, 1, off, dst, (long long)cap, NULL);
+        Py_END_ALLOW_THREADS if (rc == PSIB_ERR_OVERFLOW && attempt == 0)
+        {
+            Py_DECREF(out);
+            cap = (npy_intp)off[1];
+            continue;
+        }
+        if (rc != PSIB_OK) {
             Py_DECREF(out);
             return raise_status_of("PSI.RStarTree.query", rc);
         }
+        PyObject *res = head_of(out, (npy_intp)off[1]);
+        Py_DECREF(out);
+        return res;
     }
-    return out;
+    PyErr_SetString(PyExc_RuntimeError, "PSI.RStarTree.query: the result size changed between calls");
+    return NULL;
 }
 
 static PyMemberDef RStarTree_members[] = {{"mesh", T_OBJECT_EX, offsetof(RStarTree, mesh), READONLY, "mesh"},
@@ -811,8 +857,8 @@ static PyTypeObject RStarTreeType = {
 /* PSI.VDF(mesh, sample_pos, tree=None, refine_tolerance=1.0, refine_max_lvl=0)
  * (src/PSI.c:1022-1057): (rho, vel) of every stream at sample_pos.  Without a
  * tree the elements are culled against the mesh's box, as the reference's own
- * tree for this call is (src/cpsi.c:206-209); with one, against the tree's
- * window. */
+ * tree for this call is (src/cpsi.c:206-209); with one, the tree's index (and
+ * so its window) is used. */
 static PyObject *PSI_VDF(PyObject *self, PyObject *args, PyObject *kwds)
 {
     (void)self;
@@ -824,35 +870,54 @@ static PyObject *PSI_VDF(PyObject *self, PyObject *args, PyObject *kwds)
     if (!PyArg_ParseTupleAndKeywords(args, kwds, "O!(ddd)|O!di", kwlist, &MeshType, &mesh, &s[0], &s[1], &s[2],
                                      &RStarTreeType, &tree, &reftol, &maxlvl))
         return NULL;
+    if (tree && tree_index(tree, "PSI.VDF") < 0) return NULL;
     psib_mesh m;
     mesh_view(mesh, &m);
     double win[2][3];
-    memcpy(win, tree ? tree->window : mesh->box, sizeof(win));
+    memcpy(win, mesh->box, sizeof(win));
     long long off[2] = {0, 0};
-    int rc;
-    Py_BEGIN_ALLOW_THREADS rc = psib_sample_vdf(&m, (const double(*)[3])win, s, 1, reftol, maxlvl, off, NULL, NULL, 0, NULL);
-    Py_END_ALLOW_THREADS if (rc != PSIB_OK) return raise_status_of("PSI.VDF", rc);
-    npy_intp nd[2] = {(npy_intp)off[1], 3};
-    PyObject *rho = PyArray_SimpleNew(1, nd, NPY_FLOAT64);
-    PyObject *vel = PyArray_SimpleNew(2, nd, NPY_FLOAT64);
-    if (!rho || !vel) {
-        Py_XDECREF(rho);
-        Py_XDECREF(vel);
-        return NULL;
-    }
-    if (off[1] > 0) {
+    npy_intp cap = 256;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        npy_intp nd[2] = {cap, 3};
+        PyObject *rho = PyArray_SimpleNew(1, nd, NPY_FLOAT64);
+        PyObject *vel = PyArray_SimpleNew(2, nd, NPY_FLOAT64);
+        if (!rho || !vel) {
+            Py_XDECREF(rho);
+            Py_XDECREF(vel);
+            return NULL;
+        }
         double *r = (double *)PyArray_DATA((PyArrayObject *)rho), *v = (double *)PyArray_DATA((PyArrayObject *)vel);
-        Py_BEGIN_ALLOW_THREADS rc = psib_sample_vdf(&m, (const double(*)[3])win, s, 1, reftol, maxlvl, off, r, v, off[1], NULL);
-        Py_END_ALLOW_THREADS if (rc != PSIB_OK) {
+        int rc;
+        Py_BEGIN_ALLOW_THREADS if (tree) rc =
+            psib_index_sample_vdf(tree->ix, s, 1, reftol, maxlvl, off, r, v, (long long)cap, NULL);
+        else rc = psib_sample_vdf(&m, (const double(*)[3])win, s, 1, reftol, maxlvl, off, r, v, (long long)cap, NULL);
+        Py_END_ALLOW_THREADS if (rc == PSIB_ERR_OVERFLOW && attempt == 0)
+        {
+            Py_DECREF(rho);
+            Py_DECREF(vel);
+            cap = (npy_intp)off[1];
+            continue;
+        }
+        if (rc != PSIB_OK) {
             Py_DECREF(rho);
             Py_DECREF(vel);
             return raise_status_of("PSI.VDF", rc);
         }
+        PyObject *rh = head_of(rho, (npy_intp)off[1]), *vh = head_of(vel, (npy_intp)off[1]);
+        Py_DECREF(rho);
+        Py_DECREF(vel);
+        if (!rh || !vh) {
+            Py_XDECREF(rh);
+            Py_XDECREF(vh);
+            return NULL;
+        }
+        PyObject *ret = Py_BuildValue("OO", rh, vh);
+        Py_DECREF(rh);
+        Py_DECREF(vh);
+        return ret;
     }
-    PyObject *ret = Py_BuildValue("OO", rho, vel);
-    Py_DECREF(rho);
-    Py_DECREF(vel);
-    return ret;
+    PyErr_SetString(PyExc_RuntimeError, "PSI.VDF: the result size changed between calls");
+    return NULL;
 }
 
 static PyMethodDef module_methods[] = {

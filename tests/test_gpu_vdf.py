@@ -129,3 +129,54 @@ def test_vdf_from_block_and_snapshot_loaders(gpu, oracle, tmp_path):
         rho, vel = gpu.VDF(bmesh, tuple(p), tree)
         w_rho, w_vel = O.sample_vdf("restatement", c["pos"], c["conn"], p, vel=c["vel"], window=O.tree_window(None))
         assert np.array_equal(rho, w_rho) and np.array_equal(vel, w_vel)
+
+
+def test_index_equals_stateless_calls(gpu, oracle):
+    """psib_index_create / _query / _sample_vdf answer as psib_query_elements and
+    psib_sample_vdf do, over many points and boxes, and the index outlives the
+    caller's arrays (it holds its own copy of the mesh)."""
+    import ctypes as C
+
+    from pypsi_b200 import capi
+
+    c = make("periodic5")
+    pos, conn, vel, mass = (np.ascontiguousarray(c[k]) for k in ("pos", "conn", "vel", "mass"))
+    m = capi.make_mesh(len(pos), len(conn), pos.ctypes.data, vel.ctypes.data, mass.ctypes.data, conn.ctypes.data, 8,
+                       None, c["periodic_box"])
+    win = np.ascontiguousarray(O.tree_window(c["periodic_box"]), dtype=np.float64)
+    lib = capi.lib
+    lib.psib_index_create.argtypes = [C.POINTER(capi.Mesh), C.c_void_p, C.POINTER(C.c_void_p), C.c_void_p]
+    lib.psib_index_query.argtypes = [C.c_void_p, C.c_void_p, C.c_longlong, C.c_void_p, C.c_void_p, C.c_longlong,
+                                     C.c_void_p]
+    lib.psib_index_sample_vdf.argtypes = [C.c_void_p, C.c_void_p, C.c_longlong, C.c_double, C.c_int, C.c_void_p,
+                                          C.c_void_p, C.c_void_p, C.c_longlong, C.c_void_p]
+    lib.psib_index_destroy.argtypes = [C.c_void_p]
+    ix = C.c_void_p()
+    assert lib.psib_index_create(C.byref(m), win.ctypes.data, C.byref(ix), None) == 0
+    try:
+        pos2 = pos.copy()
+        pos[:] = 0.0  # the index keeps the mesh as it was
+        pts = np.random.default_rng(8).uniform(0, 1, (300, 3))
+        want_off, want_rho, want_vel = capi.sample_vdf(pts, pos2, connectivity=conn, vel=vel, mass=mass,
+                                                       periodic_box=c["periodic_box"], refine_tolerance=c["reftol"],
+                                                       refine_max_lvl=c["maxlvl"])
+        off = np.zeros(len(pts) + 1, dtype=np.int64)
+        n = int(want_off[-1])
+        rho, v = np.zeros(max(n, 1)), np.zeros((max(n, 1), 3))
+        assert lib.psib_index_sample_vdf(ix, pts.ctypes.data, len(pts), c["reftol"], c["maxlvl"], off.ctypes.data,
+                                         rho.ctypes.data, v.ctypes.data, n, None) == 0
+        assert np.array_equal(off, want_off)
+        assert np.array_equal(rho[:n], want_rho) and np.array_equal(v[:n], want_vel)
+        lo = np.random.default_rng(2).uniform(-0.1, 0.9, (20, 3))
+        boxes = np.ascontiguousarray(np.concatenate([lo, lo + 0.3], axis=1))
+        qoff = np.zeros(21, dtype=np.int64)
+        assert lib.psib_index_query(ix, boxes.ctypes.data, 20, qoff.ctypes.data, None, 0, None) == 0
+        els = np.zeros(max(int(qoff[-1]), 1), dtype=np.int32)
+        assert lib.psib_index_query(ix, boxes.ctypes.data, 20, qoff.ctypes.data, els.ctypes.data, int(qoff[-1]),
+                                    None) == 0
+        for b in range(20):
+            want = O.query_elements("restatement", pos2, conn, win, (tuple(lo[b]), tuple(lo[b] + 0.3)),
+                                    c["periodic_box"])
+            assert np.array_equal(els[qoff[b]:qoff[b + 1]], want), b
+    finally:
+        lib.psib_index_destroy(ix)
