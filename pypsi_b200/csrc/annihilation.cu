@@ -103,14 +103,6 @@ cudaError_t launch_ann_box_stats(const AnnArgs& a, unsigned long long* out, doub
 
 // ---- cells ----
 
-__device__ __forceinline__ long long cell_of(const CellGrid& cg, int i, double x)
-{
-    double f = floor((x - cg.o[i]) / cg.h[i]);
-    if (!(f >= 0.0)) f = 0.0; // also NaN
-    long long c = f < (double)cg.n[i] ? (long long)f : cg.n[i] - 1;
-    return c;
-}
-
 __device__ __forceinline__ bool kept_elem(const AnnArgs& a, long long e) { return a.cnt_a[e] > 0 || a.cnt_b[e] > 0; }
 
 template <bool EMIT>
@@ -369,25 +361,19 @@ cudaError_t launch_query_boxes(const AnnArgs& a, bool emit, cudaStream_t s)
 
 // A point against the elements registered in its cell: every element whose
 // box contains the point (the degenerate query box of src/cpsi.c:212-216)
-// is registered there.
+// is registered there.  A run lists its elements in ascending order; it is
+// walked backwards, so each point's pairs come out in descending element
+// order -- the keys are written already sorted.
 template <bool EMIT>
 __global__ void k_query_points(AnnArgs a)
 {
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < a.nq; q += stride) {
         const double* s = a.qry + 3 * q;
-        const unsigned long long k =
-            (unsigned long long)((cell_of(a.cg, 0, s[0]) * a.cg.n[1] + cell_of(a.cg, 1, s[1])) * a.cg.n[2] +
-                                 cell_of(a.cg, 2, s[2]));
-        long long lo = 0, hi = a.nruns; // the run whose key is k, if any
-        while (lo < hi) {
-            const long long mid = (lo + hi) >> 1;
-            if (a.run_key[mid] < k) lo = mid + 1;
-            else hi = mid;
-        }
+        const long long r = find_run(a, point_cell(a.cg, s));
         long long n = 0, w = EMIT ? a.q_off[q] : 0;
-        if (lo < a.nruns && a.run_key[lo] == k) {
-            for (long long j = a.run_off[lo]; j < a.run_off[lo] + a.run_cnt[lo]; ++j) {
+        if (r >= 0) {
+            for (long long j = a.run_off[r] + a.run_cnt[r] - 1; j >= a.run_off[r]; --j) {
                 const long long e = a.reg_elem[j];
                 bool in = true;
                 for (int c = 0; c < 3; ++c)

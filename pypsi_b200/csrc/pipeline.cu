@@ -1686,6 +1686,8 @@ int query_from_boxes(QueryCall& q, AnnArgs& aa, unsigned long long* sm, const do
 int vdf_from_index(QueryCall& q, AnnArgs& aa, long long kept, unsigned long long* sm, const double* points,
                    long long npoints, double reftol, int maxlvl, long long* offsets, double* rho, double* vel,
                    long long capacity);
+int vdf_one_point(QueryCall& q, AnnArgs& aa, long long kept, unsigned long long* sm, double reftol, int maxlvl,
+                  long long* offsets, double* rho, double* vel, long long capacity);
 
 int query_elements_impl(QueryCall& q, const double (*window)[3], const double* boxes, long long nboxes,
                         long long* offsets, int* elements, long long capacity)
@@ -1759,6 +1761,46 @@ int sample_vdf_impl(QueryCall& q, const double (*window)[3], const double* point
     return vdf_from_index(q, aa, kept, sm, points, npoints, reftol, maxlvl, offsets, rho, vel, capacity);
 }
 
+// One point in host memory (the drop-in PSI.VDF call): one thread walks the
+// point's cell and writes the samples that fit `capacity`; one copy brings
+// back their number and the samples.
+int vdf_one_point(QueryCall& q, AnnArgs& aa, long long kept, unsigned long long* sm, double reftol, int maxlvl,
+                  long long* offsets, double* rho, double* vel, long long capacity)
+{
+    Ctx& C = *q.C;
+    cudaStream_t st = q.c.st;
+    const psib_mesh& m = *q.c.mesh;
+    VdfArgs va = {};
+    va.m = mesh_dev(m, psib_grid{}, q.c.pos, q.c.vel, q.c.mass, q.c.conn, 1.0, nullptr);
+    va.m.ptol2 = reftol * reftol;
+    va.max_lvl = maxlvl > 6 ? 6 : (maxlvl < 0 ? 0 : maxlvl);
+    va.quad = m.elemtype == 27;
+    va.points = aa.qry;
+    va.status = aa.status;
+    const long long cap = (rho && vel) ? (capacity > 0 ? capacity : 0) : 0;
+    RET(ensure(C.s_rho, (size_t)(cap > 0 ? cap : 1) * sizeof(double)));
+    RET(ensure(C.s_vel, (size_t)(cap > 0 ? cap : 1) * 3 * sizeof(double)));
+    va.rho = C.s_rho.as<double>();
+    va.vel = C.s_vel.as<double>();
+    CK(cudaMemsetAsync(&sm[S_RECN], 0, 8, st));
+    if (kept > 0) CK(launch_vdf_point(va, aa, &sm[S_RECN], cap, st));
+    unsigned long long h[S_WORDS];
+    CK(cudaMemcpyAsync(h, sm, sizeof(h), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    RET(check_status(q.c, h));
+    const long long total = (long long)h[S_RECN];
+    offsets[0] = 0;
+    offsets[1] = total;
+    if (!rho || !vel) return PSIB_OK;
+    if (capacity < total)
+        return fail(PSIB_ERR_OVERFLOW, "the output holds %lld samples, the points have %lld", capacity, total);
+    if (total > 0) {
+        CK(cudaMemcpyAsync(rho, va.rho, (size_t)total * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(vel, va.vel, (size_t)total * 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    }
+    return PSIB_OK;
+}
+
 // Samples at the points through the cell index of aa (kept elements, their
 // boxes, cells and runs), the mesh of q.
 int vdf_from_index(QueryCall& q, AnnArgs& aa, long long kept, unsigned long long* sm, const double* points,
@@ -1772,6 +1814,8 @@ int vdf_from_index(QueryCall& q, AnnArgs& aa, long long kept, unsigned long long
     RET(query_input(q, C.q_in, points, (size_t)npoints * 3 * sizeof(double), &qin));
     aa.qry = (const double*)qin;
     aa.nq = npoints;
+    if (npoints == 1 && q.host)
+        return vdf_one_point(q, aa, kept, sm, reftol, maxlvl, offsets, rho, vel, capacity);
     // (point, element) pairs: every kept element whose box contains the point
     RET(ensure(C.q_cnt, (size_t)(npoints + 1) * sizeof(long long)));
     RET(ensure(C.q_off, (size_t)(npoints + 1) * sizeof(long long)));
@@ -1783,13 +1827,8 @@ int vdf_from_index(QueryCall& q, AnnArgs& aa, long long kept, unsigned long long
     long long npair = 0;
     RET(read_dev(aa.q_off + npoints, npair, st));
     RET(ensure(C.q_key, (size_t)(npair > 0 ? npair : 1) * 8));
-    RET(ensure(C.q_key_s, (size_t)(npair > 0 ? npair : 1) * 8));
-    if (npair > 0) {
-        aa.q_key = C.q_key.as<unsigned long long>();
-        CK(launch_query_points(aa, true, st));
-        RET(sort_keys(C, aa.q_key, C.q_key_s.as<unsigned long long>(), npair,
-                      32 + bits_for((unsigned long long)npoints + 1), st));
-    }
+    aa.q_key = C.q_key.as<unsigned long long>();
+    if (npair > 0) CK(launch_query_points(aa, true, st)); // keys come out sorted: point, element descending
     // samples per pair, in pair order (point, element descending, tet)
     VdfArgs va = {};
     va.m = mesh_dev(m, psib_grid{}, q.c.pos, q.c.vel, q.c.mass, q.c.conn, 1.0, nullptr);
@@ -1797,7 +1836,7 @@ int vdf_from_index(QueryCall& q, AnnArgs& aa, long long kept, unsigned long long
     va.max_lvl = maxlvl > 6 ? 6 : (maxlvl < 0 ? 0 : maxlvl);
     va.quad = m.elemtype == 27;
     va.points = aa.qry;
-    va.pairs = C.q_key_s.as<unsigned long long>();
+    va.pairs = aa.q_key;
     va.npair = npair;
     va.status = (unsigned*)&sm[S_STATUS];
     RET(ensure(C.s_cnt, (size_t)(npair + 1) * sizeof(long long)));

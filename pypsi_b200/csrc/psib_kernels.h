@@ -276,6 +276,29 @@ cudaError_t launch_ann_tpairs(const AnnArgs &a, bool emit, cudaStream_t s);
 cudaError_t launch_ann_chunk_bounds(const long long *tp_excl, long long nslot, long long budget, int nb,
                                     long long *bounds, cudaStream_t s);
 
+// The cell of coordinate x on axis i (clamped to the grid; NaN to cell 0), and
+// the run of the sorted registrations whose cell key is k (-1: none).
+__device__ __forceinline__ long long cell_of(const CellGrid &cg, int i, double x)
+{
+    double f = floor((x - cg.o[i]) / cg.h[i]);
+    if (!(f >= 0.0)) f = 0.0;
+    return f < (double)cg.n[i] ? (long long)f : cg.n[i] - 1;
+}
+__device__ __forceinline__ unsigned long long point_cell(const CellGrid &cg, const double *s)
+{
+    return (unsigned long long)((cell_of(cg, 0, s[0]) * cg.n[1] + cell_of(cg, 1, s[1])) * cg.n[2] + cell_of(cg, 2, s[2]));
+}
+__device__ __forceinline__ long long find_run(const AnnArgs &a, unsigned long long k)
+{
+    long long lo = 0, hi = a.nruns;
+    while (lo < hi) {
+        const long long mid = (lo + hi) >> 1;
+        if (a.run_key[mid] < k) lo = mid + 1;
+        else hi = mid;
+    }
+    return (lo < a.nruns && a.run_key[lo] == k) ? lo : -1;
+}
+
 // the element boxes of a query: cull against a.g's window, kept flag in cnt_a and cnt_b
 cudaError_t launch_elem_boxes(const AnnTessArgs &a, cudaStream_t s);
 // box queries, every (box, element) pair tested (count: q_cnt; emit: q_key via q_n)
@@ -296,6 +319,10 @@ struct VdfArgs {
     unsigned *status;
 };
 cudaError_t launch_vdf_samples(const VdfArgs &a, bool emit, cudaStream_t s);
+// One point (a.points[0]) through the cell index x on one thread: its samples, in the order
+// of the pairs above, written while fewer than cap; their number to *count.
+cudaError_t launch_vdf_point(const VdfArgs &a, const AnnArgs &x, unsigned long long *count, long long cap,
+                             cudaStream_t s);
 // out[i] = the element of sorted query key i
 cudaError_t launch_keys_elem(const unsigned long long *keys, long long n, int *out, cudaStream_t s);
 // out[p] = pair_soff[q_off[p]] for p in [0, np]: each point's first sample

@@ -743,9 +743,10 @@ __device__ double barycentric(const double (*v)[3], const double* s, double* b)
 struct VdfEmitter {
     const VdfArgs& a;
     const double* s;
-    long long pos;
+    long long pos;   // next sample's index
     int n;
     bool write;
+    long long cap;   // samples are written at indices below cap
     __device__ void tet(const double (*p)[3], const double (*u)[3], double mass, long long, const int*)
     {
         double b[4];
@@ -754,24 +755,59 @@ struct VdfEmitter {
         for (int i = 0; i < 4; ++i)
             if (b[i] < 0.0) return;
         if (write) {
-            for (int i = 0; i < 3; ++i) {
-                double acc = 0.0;
-                for (int j = 0; j < 4; ++j) acc += b[j] * u[j][i];
-                a.vel[3 * pos + i] = acc;
+            if (pos < cap) {
+                for (int i = 0; i < 3; ++i) {
+                    double acc = 0.0;
+                    for (int j = 0; j < 4; ++j) acc += b[j] * u[j][i];
+                    a.vel[3 * pos + i] = acc;
+                }
+                a.rho[pos] = mass / vol;
             }
-            a.rho[pos] = mass / vol;
             pos++;
         }
         n++;
     }
 };
 
+// The samples of one element at the emitter's point: the element refined from
+// its vertices as stored (src/cpsi.c:222-230), every tet tested.
+template <bool REFINE, bool QUAD>
+__device__ void vdf_element(const VdfArgs& a, VdfEmitter& em, long long e, RefNode* L)
+{
+    constexpr int NV = QUAD ? 27 : 8;
+    double p[NV][3], u[NV][3];
+    int ids[NV];
+    if ((!QUAD && a.m.elemtype == 27) || !gather(a.m, e, p, u, ids)) {
+        atomicOr(a.status, ST_INDEX);
+        return;
+    }
+    const double me = a.m.mass ? a.m.mass[e] : 1.0;
+    const int et = a.m.elemtype;
+    if (et == 4) {
+        em.tet(p, u, me, e, nullptr);
+    } else if (QUAD && et == 27) {
+        if constexpr (QUAD)
+            refine_element_quad(em, p, u, me, e, REFINE ? a.max_lvl : 0, a.m.ptol2, 0, 0.0, a.m.lag, L);
+    } else if (!REFINE) {
+        for (int t = 0; t < 6; ++t) {
+            double tp[4][3], tu[4][3];
+            for (int v = 0; v < 4; ++v)
+                for (int c = 0; c < 3; ++c) {
+                    tp[v][c] = p[c_tet_corners[t][v]][c];
+                    tu[v][c] = u[c_tet_corners[t][v]][c];
+                }
+            em.tet(tp, tu, me * (1.0 / 6), e, nullptr);
+        }
+    } else {
+        if constexpr (REFINE) refine_element(em, p, u, me, e, a.max_lvl, a.m.ptol2, 0, 0.0, a.m.lag, L);
+    }
+}
+
 // One thread per (point, element) pair: the element refined from its vertices
 // as stored (src/cpsi.c:222-230), every tet tested against the point.
 template <bool REFINE, bool QUAD, bool EMIT>
 __global__ void __launch_bounds__(128) k_vdf_samples(VdfArgs a)
 {
-    constexpr int NV = QUAD ? 27 : 8;
     RefNode* L = nullptr;
     RefNode Lbuf[(REFINE || QUAD) ? MAX_REFINE + 1 : 1];
     if constexpr (REFINE || QUAD) L = Lbuf;
@@ -780,36 +816,47 @@ __global__ void __launch_bounds__(128) k_vdf_samples(VdfArgs a)
         const unsigned long long key = a.pairs[i];
         const long long pt = (long long)(key >> 32);
         const long long e = (long long)(0xFFFFFFFFull - (key & 0xFFFFFFFFull));
-        double p[NV][3], u[NV][3];
-        int ids[NV];
-        if ((!QUAD && a.m.elemtype == 27) || !gather(a.m, e, p, u, ids)) {
-            atomicOr(a.status, ST_INDEX);
-            if (!EMIT) a.cnt[i] = 0;
-            continue;
-        }
-        const double me = a.m.mass ? a.m.mass[e] : 1.0;
-        VdfEmitter em{a, a.points + 3 * pt, EMIT ? a.off[i] : 0, 0, EMIT};
-        const int et = a.m.elemtype;
-        if (et == 4) {
-            em.tet(p, u, me, e, nullptr);
-        } else if (QUAD && et == 27) {
-            if constexpr (QUAD)
-                refine_element_quad(em, p, u, me, e, REFINE ? a.max_lvl : 0, a.m.ptol2, 0, 0.0, a.m.lag, L);
-        } else if (!REFINE) {
-            for (int t = 0; t < 6; ++t) {
-                double tp[4][3], tu[4][3];
-                for (int v = 0; v < 4; ++v)
-                    for (int c = 0; c < 3; ++c) {
-                        tp[v][c] = p[c_tet_corners[t][v]][c];
-                        tu[v][c] = u[c_tet_corners[t][v]][c];
-                    }
-                em.tet(tp, tu, me * (1.0 / 6), e, nullptr);
-            }
-        } else {
-            if constexpr (REFINE) refine_element(em, p, u, me, e, a.max_lvl, a.m.ptol2, 0, 0.0, a.m.lag, L);
-        }
+        VdfEmitter em{a, a.points + 3 * pt, EMIT ? a.off[i] : 0, 0, EMIT, 0x7FFFFFFFFFFFFFFFll};
+        vdf_element<REFINE, QUAD>(a, em, e, L);
         if (!EMIT) a.cnt[i] = em.n;
     }
+}
+
+// One point on one thread: its cell's elements in descending order (the pairs
+// of k_query_points), each containing one sampled as above.
+template <bool REFINE, bool QUAD>
+__global__ void k_vdf_point(VdfArgs a, AnnArgs x, unsigned long long* count, long long cap)
+{
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    RefNode* L = nullptr;
+    RefNode Lbuf[(REFINE || QUAD) ? MAX_REFINE + 1 : 1];
+    if constexpr (REFINE || QUAD) L = Lbuf;
+    const double* s = a.points;
+    VdfEmitter em{a, s, 0, 0, true, cap};
+    const long long r = find_run(x, point_cell(x.cg, s));
+    if (r >= 0)
+        for (long long j = x.run_off[r] + x.run_cnt[r] - 1; j >= x.run_off[r]; --j) {
+            const long long e = x.reg_elem[j];
+            bool in = true;
+            for (int c = 0; c < 3; ++c)
+                if (s[c] < x.ebox[6 * e + c] || s[c] > x.ebox[6 * e + 3 + c]) in = false;
+            if (in) vdf_element<REFINE, QUAD>(a, em, e, L);
+        }
+    *count = (unsigned long long)em.n;
+}
+
+cudaError_t launch_vdf_point(const VdfArgs& a, const AnnArgs& x, unsigned long long* count, long long cap,
+                             cudaStream_t s)
+{
+    const bool refine = a.max_lvl > 0 && a.m.elemtype != 4;
+    if (a.quad) {
+        if (refine) k_vdf_point<true, true><<<1, 32, 0, s>>>(a, x, count, cap);
+        else k_vdf_point<false, true><<<1, 32, 0, s>>>(a, x, count, cap);
+    } else {
+        if (refine) k_vdf_point<true, false><<<1, 32, 0, s>>>(a, x, count, cap);
+        else k_vdf_point<false, false><<<1, 32, 0, s>>>(a, x, count, cap);
+    }
+    return cudaGetLastError();
 }
 
 cudaError_t launch_vdf_samples(const VdfArgs& a, bool emit, cudaStream_t s)
