@@ -45,7 +45,7 @@ typedef struct {
 } og_grid;
 
 typedef struct {
-    int elemtype;            /* 4, 8 (27 is rejected by this oracle) */
+    int elemtype;            /* 4, 8 or 27 */
     int npart, nelem;
     const double *pos, *vel; /* npart x 3 */
     const double *mass;      /* nelem */
@@ -599,6 +599,96 @@ static int refine_trilinear(ov_tetbuf *tb, const double (*p)[3], const double (*
     return tetbuf_push6(tb, p, u, mass);
 }
 
+/* Triquadratic elements (27 nodes, index 9i+3j+k): the 125-node interpolation of
+ * src/refine.c:321-345 -- the corner values at even lattice points, then three
+ * sweeps (x on the even y, z planes; y on the even z planes; z everywhere), each
+ * new node 1/8 (3 near + 6 middle - far) of the three nodes of its line. */
+#define I5(a, b, c) (25 * (a) + 5 * (b) + (c))
+static void quad_fill_line(double (*o)[3], int a0, int s, int ax)
+{
+    /* nodes a0, a0 + s, ..., a0 + 4s of one line: fill 1 and 3 from 0, 2, 4 */
+    const double *n0 = o[a0], *n2 = o[a0 + 2 * s], *n4 = o[a0 + 4 * s];
+    o[a0 + s][ax] = 0.125 * (3.0 * n0[ax] + 6.0 * n2[ax] - n4[ax]);
+    o[a0 + 3 * s][ax] = 0.125 * (3.0 * n4[ax] + 6.0 * n2[ax] - n0[ax]);
+}
+
+static void interp_triquadratic(const double (*in)[3], double (*out)[3])
+{
+    for (int ax = 0; ax < 3; ++ax) {
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j)
+                for (int k = 0; k < 3; ++k) out[I5(2 * i, 2 * j, 2 * k)][ax] = in[I3(i, j, k)][ax];
+        for (int j = 0; j < 5; j += 2)
+            for (int k = 0; k < 5; k += 2) quad_fill_line(out, I5(0, j, k), 25, ax);
+        for (int i = 0; i < 5; ++i)
+            for (int k = 0; k < 5; k += 2) quad_fill_line(out, I5(i, 0, k), 5, ax);
+        for (int i = 0; i < 5; ++i)
+            for (int j = 0; j < 5; ++j) quad_fill_line(out, I5(i, j, 0), 1, ax);
+    }
+}
+
+/* src/refine.c:152-221: refine while the midpoint of one of the 19 tet edges of
+ * the 3x3x3 node cube (end, midpoint, end: the table of src/refine.c:157-161)
+ * deviates from the straight edge by more than the tolerance; child (i,j,k)
+ * takes nodes (2i..2i+2, ...) of the 125-node interpolation; a leaf is the six
+ * tets of its corner nodes. */
+static int refine_triquadratic(ov_tetbuf *tb, const double (*p)[3], const double (*u)[3], double mass, int lvl)
+{
+    static const int edges[19][3] = {{0, 1, 2},    {0, 3, 6},    {0, 9, 18},   {2, 4, 6},    {2, 5, 8},
+                                     {2, 10, 18},  {2, 11, 20},  {6, 7, 8},    {6, 12, 18},  {6, 15, 24},
+                                     {8, 13, 18},  {8, 14, 20},  {8, 16, 24},  {8, 17, 26},  {18, 19, 20},
+                                     {18, 21, 24}, {20, 22, 24}, {20, 23, 26}, {24, 25, 26}};
+    if (lvl < tb->max_lvl)
+        for (int e = 0; e < 19; ++e) {
+            double err2 = 0.0;
+            for (int i = 0; i < 3; ++i) {
+                double mt = 0.5 * (p[edges[e][0]][i] + p[edges[e][2]][i]);
+                double mq = p[edges[e][1]][i];
+                err2 += (mt - mq) * (mt - mq);
+            }
+            if (err2 > tb->ptol2) {
+                double ip[125][3], iu[125][3], cp[27][3], cu[27][3];
+                interp_triquadratic(p, ip);
+                interp_triquadratic(u, iu);
+                for (int i = 0; i < 2; ++i)
+                    for (int j = 0; j < 2; ++j)
+                        for (int k = 0; k < 2; ++k) {
+                            for (int a = 0; a < 3; ++a)
+                                for (int b = 0; b < 3; ++b)
+                                    for (int c = 0; c < 3; ++c) {
+                                        memcpy(cp[I3(a, b, c)], ip[I5(a + 2 * i, b + 2 * j, c + 2 * k)], sizeof(cp[0]));
+                                        memcpy(cu[I3(a, b, c)], iu[I5(a + 2 * i, b + 2 * j, c + 2 * k)], sizeof(cu[0]));
+                                    }
+                            if (refine_triquadratic(tb, (const double(*)[3])cp, (const double(*)[3])cu, 0.125 * mass,
+                                                    lvl + 1))
+                                return -1;
+                        }
+                return 0;
+            }
+        }
+    return tetbuf_push6(tb, p, u, mass);
+}
+
+/* An element's tets into tb (src/refine.c:58-150): a simplex is one tet of the
+ * element's mass, a trilinear or triquadratic element is refined. */
+static int element_tets(ov_tetbuf *tb, const double (*p)[3], const double (*u)[3], double mass, int vpe)
+{
+    tb->num = 0;
+    if (vpe == 4) {
+        if (tetbuf_reserve(tb, 1)) return -1;
+        memcpy(tb->pos[0], p, sizeof(double) * 12);
+        memcpy(tb->vel[0], u, sizeof(double) * 12);
+        tb->mass[0] = mass;
+        tb->num = 1;
+        return 0;
+    }
+    if (vpe == 27) return refine_triquadratic(tb, p, u, mass, 0); /* the 27 nodes as they are (src/refine.c:79-81) */
+    double np_[27][3], nu[27][3];
+    interp_trilinear(p, np_);
+    interp_trilinear(u, nu);
+    return refine_trilinear(tb, (const double(*)[3])np_, (const double(*)[3])nu, mass, 0);
+}
+
 /* ---- element loop helpers (src/cpsi.c:277-373) ---- */
 
 static void aabb(const double (*p)[3], int n, double (*rb)[3])
@@ -693,7 +783,7 @@ static int voxels_impl(og_grid *g, const og_mesh *m, double reftol, int max_lvl,
     og_counters dummy;
     memset(&dummy, 0, sizeof(dummy));
     g_cnt = cnt ? cnt : &dummy;
-    if (m->elemtype != 4 && m->elemtype != 8) return -1;
+    if (m->elemtype != 4 && m->elemtype != 8 && m->elemtype != 27) return -1;
     double dxmin = 1.0e30;
     for (int i = 0; i < 3; ++i)
         if (g->d[i] < dxmin) dxmin = g->d[i];
@@ -710,7 +800,7 @@ static int voxels_impl(og_grid *g, const og_mesh *m, double reftol, int max_lvl,
     int vpe = m->elemtype;
     int rc = 0;
     for (int e = 0; e < m->nelem; ++e) {
-        double tp[8][3], tu[8][3], rb[2][3];
+        double tp[27][3], tu[27][3], rb[2][3];
         for (int v = 0; v < vpe; ++v) {
             int id = m->conn[e * vpe + v];
             memcpy(tp[v], &m->pos[3 * (size_t)id], sizeof(tp[v]));
@@ -718,20 +808,7 @@ static int voxels_impl(og_grid *g, const og_mesh *m, double reftol, int max_lvl,
         }
         if (!aabb_periodic(tp, vpe, rb, g, m)) continue;
         g_cnt->elements_kept++;
-        tb.num = 0;
-        if (vpe == 4) {
-            if (tetbuf_reserve(&tb, 1)) { rc = -1; break; }
-            /* a simplex element is one tet of the element's own mass (src/refine.c:60-66) */
-            memcpy(tb.pos[0], tp, sizeof(double) * 12);
-            memcpy(tb.vel[0], tu, sizeof(double) * 12);
-            tb.mass[0] = m->mass[e];
-            tb.num = 1;
-        } else {
-            double np_[27][3], nu[27][3];
-            interp_trilinear((const double(*)[3])tp, np_);
-            interp_trilinear((const double(*)[3])tu, nu);
-            if (refine_trilinear(&tb, (const double(*)[3])np_, (const double(*)[3])nu, m->mass[e], 0)) { rc = -1; break; }
-        }
+        if (element_tets(&tb, (const double(*)[3])tp, (const double(*)[3])tu, m->mass[e], vpe)) { rc = -1; break; }
         for (int t = 0; t < tb.num; ++t) {
             double gp[32][3], grb[16][3];
             memcpy(gp, tb.pos[4 * t], sizeof(double) * 12);
@@ -890,31 +967,12 @@ static void ov_annihilate(const double (*p0)[3], ov_real vol0, ov_real rho0, con
     }
 }
 
-/* An element's tets into tb (src/refine.c:58-150): a simplex is one tet of the
- * element's mass, a trilinear element is refined. */
-static int element_tets(ov_tetbuf *tb, const double (*p)[3], const double (*u)[3], double mass, int vpe)
-{
-    tb->num = 0;
-    if (vpe == 4) {
-        if (tetbuf_reserve(tb, 1)) return -1;
-        memcpy(tb->pos[0], p, sizeof(double) * 12);
-        memcpy(tb->vel[0], u, sizeof(double) * 12);
-        tb->mass[0] = mass;
-        tb->num = 1;
-        return 0;
-    }
-    double np_[27][3], nu[27][3];
-    interp_trilinear(p, np_);
-    interp_trilinear(u, nu);
-    return refine_trilinear(tb, (const double(*)[3])np_, (const double(*)[3])nu, mass, 0);
-}
-
 int oracle_annihilation(og_grid *g, const og_mesh *m, double reftol, int max_lvl, og_counters *cnt)
 {
     og_counters dummy;
     memset(&dummy, 0, sizeof(dummy));
     g_cnt = cnt ? cnt : &dummy;
-    if (m->elemtype != 4 && m->elemtype != 8) return -1;
+    if (m->elemtype != 4 && m->elemtype != 8 && m->elemtype != 27) return -1;
     const int vpe = m->elemtype;
     double dxmin = 1.0e30;
     for (int i = 0; i < 3; ++i)
@@ -931,14 +989,14 @@ int oracle_annihilation(og_grid *g, const og_mesh *m, double reftol, int max_lvl
     int rc = (box && kept && stack) ? 0 : -1;
     /* element boxes after the unwrap, and the cull (src/rtree.c:48-73) */
     for (int e = 0; rc == 0 && e < m->nelem; ++e) {
-        double tp[8][3];
+        double tp[27][3];
         for (int v = 0; v < vpe; ++v) memcpy(tp[v], &m->pos[3 * (size_t)m->conn[e * vpe + v]], sizeof(tp[v]));
         kept[e] = (char)aabb_periodic(tp, vpe, box[e], g, m);
     }
     for (int e = 0; rc == 0 && e < m->nelem; ++e) {
         if (!kept[e]) continue;
         g_cnt->elements_kept++;
-        double tp[8][3], tu[8][3], rb[2][3];
+        double tp[27][3], tu[27][3], rb[2][3];
         for (int v = 0; v < vpe; ++v) {
             int id = m->conn[e * vpe + v];
             memcpy(tp[v], &m->pos[3 * (size_t)id], sizeof(tp[v]));
@@ -953,7 +1011,7 @@ int oracle_annihilation(og_grid *g, const og_mesh *m, double reftol, int max_lvl
             for (int i = 0; i < 3; ++i)
                 if (box[e][1][i] < box[e1][0][i] || box[e][0][i] > box[e1][1][i]) touch = 0;
             if (!touch) continue;
-            double sp[8][3], su[8][3];
+            double sp[27][3], su[27][3];
             for (int v = 0; v < vpe; ++v) {
                 int id = m->conn[e1 * vpe + v];
                 memcpy(sp[v], &m->pos[3 * (size_t)id], sizeof(sp[v]));
@@ -1085,7 +1143,7 @@ long long oracle_sample_vdf(const og_mesh *m, const double (*window)[3], const d
 {
     static og_counters unused; /* the element refinement reports errors here */
     g_cnt = &unused;
-    if (m->elemtype != 4 && m->elemtype != 8) return -1;
+    if (m->elemtype != 4 && m->elemtype != 8 && m->elemtype != 27) return -1;
     if (max_lvl > 6) max_lvl = 6;
     ov_tetbuf tb;
     memset(&tb, 0, sizeof(tb));
@@ -1100,7 +1158,7 @@ long long oracle_sample_vdf(const og_mesh *m, const double (*window)[3], const d
         for (int i = 0; i < 3; ++i)
             if (q[1][i] < rb[0][i] || q[0][i] > rb[1][i]) touch = 0;
         if (!touch) continue;
-        double tp[8][3], tu[8][3];
+        double tp[27][3], tu[27][3];
         for (int v = 0; v < m->elemtype; ++v) {
             int id = m->conn[e * m->elemtype + v];
             memcpy(tp[v], &m->pos[3 * (size_t)id], sizeof(tp[v]));

@@ -91,9 +91,9 @@ def test_vdf_batched_host_and_device(gpu, oracle):
 
 
 def test_vdf_triquadratic_against_reference(gpu, oracle):
-    if not oracle.available("reference"):
-        pytest.skip("the compiled reference is not built")
     from test_gpu_triquadratic import _quad_case
+
+    kind = "reference" if oracle.available("reference") else "restatement"
 
     q = _quad_case(ne=3, maxlvl=1, reftol=0.01)  # 27 elements: one leaf
     mesh = gpu.Mesh(loader="array", pos=q["pos"], vel=q["vel"], mass=q["mass"], connectivity=q["conn"])
@@ -101,7 +101,7 @@ def test_vdf_triquadratic_against_reference(gpu, oracle):
     n = 0
     for p in np.random.default_rng(4).uniform(0.1, 0.9, (10, 3)):
         rho, vel = gpu.VDF(mesh, tuple(p), tree, refine_tolerance=0.01, refine_max_lvl=1)
-        r_rho, r_vel = O.sample_vdf("reference", q["pos"], q["conn"], p, vel=q["vel"], mass=q["mass"],
+        r_rho, r_vel = O.sample_vdf(kind, q["pos"], q["conn"], p, vel=q["vel"], mass=q["mass"],
                                     window=O.tree_window(None), reftol=0.01, maxlvl=1)
         assert np.array_equal(rho, r_rho) and np.array_equal(vel, r_vel)
         n += len(rho)
