@@ -21,10 +21,10 @@ def _block(pos, vel, n_grid, fields, box=BOX, bounds=None, reftol=1.0, maxlvl=0,
 
 
 def make(name: str) -> dict:
-    if name == "c1_small":  # BASELINE config 1 shape at 16^3 particles
+    if name == "c1_small":  # the 32^3 -> 64^3 density workload's shape at 16^3 particles
         pos, vel = zeldovich(16, 0.3, 101)
         return _block(pos, vel, 32, [])
-    if name == "c2_small":  # config 2 shape: shell-crossed, all order-2 fields
+    if name == "c2_small":  # the 128^3 -> 256^3 workload's shape: shell-crossed, all order-2 fields
         pos, vel = zeldovich(16, 2.0, 102)
         return _block(pos, vel, 32, ALL)
     if name == "c2_order1":

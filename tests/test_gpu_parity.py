@@ -235,7 +235,7 @@ def test_full_size_properties(gpu):
     check_vs_exact_and_reference(outs["mixed"], outs["fp64"], outs["fp64-central"], MIXED_TOL, "full")
 
 
-def test_config1_size_bitwise_against_compiled_reference(gpu, oracle):
+def test_32cube_to_64cube_density_bitwise_against_compiled_reference(gpu, oracle):
     """The reference's CPU-runnable workload at its own size: 32^3 particles
     (rms 0.3 cells) onto a 64^3 grid, density only, against the reference's C
     code compiled from its sources -- bit for bit in FP64, 1e-5 in mixed."""
@@ -249,5 +249,5 @@ def test_config1_size_bitwise_against_compiled_reference(gpu, oracle):
     out, _, _ = run_psi(gpu, c, precision="fp64")
     assert np.array_equal(out["m"], ref["m"])
     out, _, _ = run_psi(gpu, c, precision="mixed")
-    check(field_errors(out, ref), MIXED_TOL, "config 1")
+    check(field_errors(out, ref), MIXED_TOL, "32^3 -> 64^3")
     assert mass_error(out["m"], 32 ** 3) <= MASS_TOL
