@@ -175,3 +175,16 @@ def test_query_and_vdf_fail_loudly_without_gpu(psi):
     g = psi.Grid(n=(4, 4, 4))
     with pytest.raises(RuntimeError, match="no CUDA device"):
         psi.voxels(g, m, mode="annihilation")
+
+
+def test_ctypes_wrappers_fail_loudly_without_gpu(psi):
+    """The device-array wrappers raise the library's error; nothing falls back to the CPU."""
+    if psi.device_count() > 0:
+        pytest.skip("a GPU is present")
+    from pypsi_b200 import capi
+
+    pos = np.random.default_rng(1).random((27, 3))
+    with pytest.raises(capi.PsibError, match="no CUDA device"):
+        capi.sample_vdf(np.zeros((4, 3)), pos, block_dims=(3, 3, 3), periodic_box=((0, 0, 0), (1, 1, 1)))
+    assert capi.tree_window(None) == ((-1.0e30,) * 3, (1.0e30,) * 3)
+    assert capi.tree_window(((0, 0, 0), (2, 3, 4))) == ((0.0, 0.0, 0.0), (2.0, 3.0, 4.0))
