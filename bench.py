@@ -37,7 +37,25 @@ BOX = ((0.0, 0.0, 0.0), (100.0, 100.0, 100.0))
 FIELDS = ["x", "v", "xx", "xv", "vv"]
 WORKLOAD = "128^3 particles -> 256^3 grid, Zel'dovich rms 2 cells, fields m,x,v,xx,xv,vv"
 DATA = "synthetic: seeded Zel'dovich-displaced particle lattice (P(k)~k^-2), element mass 1"
-FP64_FMA_PER_CLK_PER_SM = 64
+# Algorithmic bytes of one fragment: its record of 10 moments and key out of the
+# walk (88 B) and the tet image's 4 positions and 4 velocities read (192 B).
+ALG_BYTES_PER_FRAGMENT = 88 + 192
+
+
+def clip_traffic_bytes(frags):
+    """DRAM bytes the clip walk moves per step: the ncu capture of one
+    64^3 -> 128^3 step (dram__bytes_read.sum + dram__bytes_write.sum over the
+    walk's launches, profiles/clip_walk_traffic_64cube_to_128cube.md) scaled by
+    the fragments of this step; None before a capture is recorded."""
+    if CLIP_TRAFFIC_PER_FRAGMENT is None:
+        return None
+    return {"bytes_per_step": CLIP_TRAFFIC_PER_FRAGMENT * frags,
+            "def": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the walk's launches in one 64^3 -> 128^3 step, "
+                   f"{CLIP_TRAFFIC_PER_FRAGMENT:.0f} B per fragment, times this step's fragments"}
+
+
+# bytes per fragment of the capture above (None: no capture yet)
+CLIP_TRAFFIC_PER_FRAGMENT = None
 
 
 def parse():
@@ -118,54 +136,82 @@ class Clocks:
 
 
 # ---------------------------------------------------------------- reference arm
-def _ref_init(seed):
-    global _W
+def arm_config(n_part=N_PART, n_grid=N_GRID):
+    """The workload's config, printed identically by both arms."""
+    return {"workload": WORKLOAD if (n_part, n_grid) == (N_PART, N_GRID) else
+            f"{n_part}^3 particles -> {n_grid}^3 grid, Zel'dovich rms 2 cells, fields m,x,v,xx,xv,vv",
+            "l2": "inputs larger than L2 (4.6 GB of grid fields, 3 GB of tet images per step)",
+            "per_rank": "each rank deposits its own lattice (seed 1234+rank) on its own GPU"}
+
+
+def slab_window(slab, nslabs, n_grid=N_GRID):
+    """Voxel planes [i0, i1) of the grid along x for one of nslabs window slabs,
+    and that slab's window bounds."""
+    i0, i1 = n_grid * slab // nslabs, n_grid * (slab + 1) // nslabs
+    d = (BOX[1][0] - BOX[0][0]) / n_grid
+    return i0, i1, ((BOX[0][0] + i0 * d, BOX[0][1], BOX[0][2]), (BOX[0][0] + i1 * d, BOX[1][1], BOX[1][2]))
+
+
+def _ref_inputs(seed=1234):
+    """The workload's mesh as the reference takes it: positions, velocities,
+    element masses and the periodic block connectivity (src/PSI.c:636-656)."""
     sys.path[:0] = [ROOT, os.path.join(ROOT, "oracle")]
     import numpy as np
 
-    from pypsi_b200.synth import zeldovich
+    import oracle as O
+    from pypsi_b200.synth import zeldovich  # pure numpy: maps none of the library's native code
 
     pos, vel = zeldovich(N_PART, RMS, seed)
-    _W = (np.ascontiguousarray(pos.reshape(-1, 3)), np.ascontiguousarray(vel.reshape(-1, 3)))
+    conn = O.block_connectivity((N_PART,) * 3, True)
+    return (np.ascontiguousarray(pos.reshape(-1, 3)), np.ascontiguousarray(vel.reshape(-1, 3)),
+            np.ones(conn.shape[0]), conn)
 
 
-def sample_blocks(edge=16):
-    """Lagrangian sub-blocks of the lattice (origin triples) whose tets do not
-    wrap the periodic box; the sample units of the CPU runs."""
-    nb = N_PART // edge
-    return [(i * edge, j * edge, k * edge) for i in range(1, nb - 1) for j in range(1, nb - 1)
-            for k in range(1, nb - 1)]
-
-
-def _ref_block(args):
-    """Deposit one sub-block with the reference's psi_voxels on a window that
-    covers it at the workload's voxel size; returns (tets, seconds)."""
-    origin, edge, kind = args
-    import numpy as np
-
+def _ref_slab(inputs, slab, nslabs, kind, out=None, planes=None):
+    """The reference's psi_voxels over the whole periodic mesh on one window slab
+    of the 256^3 grid (all fields); returns (fields, seconds).  planes limits
+    the slab to its first few voxel planes (the warm-up step)."""
     import oracle as O
 
-    pos, vel = _W
-    n = N_PART
-    i, j, k = np.meshgrid(*(np.arange(o, o + edge) for o in origin), indexing="ij")
-    conn = np.empty(i.shape + (8,), np.int32)
-    for ii in range(2):
-        for jj in range(2):
-            for kk in range(2):
-                conn[..., 4 * ii + 2 * jj + kk] = (n * n * ((i + ii) % n) + n * ((j + jj) % n) + (k + kk) % n)
-    conn = conn.reshape(-1, 8)
-    p = pos[np.unique(conn)]
-    d = BOX[1][0] / N_GRID
-    lo = np.floor(p.min(axis=0) / d) - 1
-    hi = np.ceil(p.max(axis=0) / d) + 1
-    bounds = (tuple(lo * d), tuple(hi * d))
-    ng = tuple(int(v) for v in (hi - lo))
+    pos, vel, mass, conn = inputs
+    i0, i1, bounds = slab_window(slab, nslabs)
+    if planes is not None:
+        i1 = min(i1, i0 + planes)
+        d = (BOX[1][0] - BOX[0][0]) / N_GRID
+        bounds = (bounds[0], (BOX[0][0] + i1 * d, bounds[1][1], bounds[1][2]))
+    n = (i1 - i0, N_GRID, N_GRID)
+    if out is None or out["m"].shape != n:
+        out = O.new_fields(n, FIELDS)
     t0 = time.perf_counter()
-    O.voxelize(kind, n=ng, bounds=bounds, pos=pos, vel=vel, conn=conn, periodic_box=None, fields=FIELDS)
-    return 6 * conn.shape[0], time.perf_counter() - t0
+    O.voxelize(kind, n=n, bounds=bounds, pos=pos, vel=vel, mass=mass, conn=conn, periodic_box=BOX, out=out)
+    return out, time.perf_counter() - t0
+
+
+def _ref_worker(pipe, slab, nslabs, kind):
+    """One process of the reference arm: deposits its window slab of the whole
+    workload at every 'step', a few voxel planes of it at every 'warm'."""
+    inputs = _ref_inputs()
+    out, thin = None, None
+    pipe.send("ready")
+    while True:
+        cmd = pipe.recv()
+        if cmd == "stop":
+            break
+        if cmd == "warm":
+            thin, secs = _ref_slab(inputs, slab, nslabs, kind, thin, planes=1)
+        else:
+            out, secs = _ref_slab(inputs, slab, nslabs, kind, out)
+        pipe.send(secs)
 
 
 def run_reference(args):
+    """The reference's own C path (oracle/_ref, compiled from its sources) on
+    every host core over the whole workload: the 256^3 grid split along x into
+    one window slab per core, each process running psi_voxels over every element
+    of the periodic 128^3 mesh on its slab (periodic images and window clips
+    are the reference's own).  The slabs are disjoint, so together they are the
+    full deposit (to rounding at the slab faces).  A step is the wall time from
+    the start of all slabs to the end of the last."""
     rank, world, _ = env_rank()
     if rank != 0:
         return
@@ -176,53 +222,93 @@ def run_reference(args):
 
     kind = "reference" if O.available("reference") else "restatement"
     cores = len(os.sched_getaffinity(0))
-    blocks = sample_blocks()
-    per_step = blocks[: max(1, min(len(blocks), cores))]
     ctx = mp.get_context("spawn")
-    with ctx.Pool(cores, initializer=_ref_init, initargs=(1234,)) as pool:
-        def step():
+    pipes, procs = [], []
+    for slab in range(cores):
+        a, b = ctx.Pipe()
+        p = ctx.Process(target=_ref_worker, args=(b, slab, cores, kind), daemon=True)
+        p.start()
+        pipes.append(a)
+        procs.append(p)
+    try:
+        for a in pipes:
+            assert a.recv() == "ready"
+
+        def step(cmd):
             t0 = time.perf_counter()
-            res = pool.map(_ref_block, [(b, 16, kind) for b in per_step], chunksize=1)
-            return sum(r[0] for r in res), time.perf_counter() - t0
+            for a in pipes:
+                a.send(cmd)
+            inner = max(a.recv() for a in pipes)
+            return time.perf_counter() - t0, inner
 
         for _ in range(args.warmup):
-            step()
-        tets, secs = 0, 0.0
-        for _ in range(args.steps):
-            t, s = step()
-            tets += t
-            secs += s
+            step("warm")
+        times = [step("step") for _ in range(args.steps)]
+    finally:
+        for a in pipes:
+            try:
+                a.send("stop")
+            except OSError:
+                pass
+        for p in procs:
+            p.join(30)
+    secs = sum(t[0] for t in times)
+    tets = 6 * N_PART ** 3 * args.steps
     value = tets / secs
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "tets/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * secs / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": DATA,
-            "config": {"workload": WORKLOAD, "precision": "fp64 (reference C)"},
+            "config": arm_config(),
+            "precision": "fp64 (the reference's own C code)",
             "cpu_baseline": {"value": value, "unit": "tets/s", "cores": cores,
                              "kind": "reference" if kind == "reference" else "port",
-                             "sample": f"{len(per_step)} Lagrangian 16^3-element sub-blocks of the workload per step, "
-                                       f"one per process, each on a window covering it at the 256^3 voxel size"},
+                             "sample": f"the whole workload every step: the 256^3 grid in {cores} window slabs "
+                                       f"along x, one process per slab, each running psi_voxels over all "
+                                       f"{N_PART ** 3} elements of the periodic mesh (periodic images included)"},
+            "warmup_step": "each process deposits the first voxel plane of its slab",
+            "slowest_slab_ms_per_step": 1000 * sum(t[1] for t in times) / args.steps,
             "e2e": {"value": value, "unit": "tets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
-def cpu_baseline_single(seconds=12.0):
-    """The reference's C path on one host core over a bounded sample."""
+def cpu_baseline_single(nslabs=16, slab=0):
+    """The reference's C path on one host core over a bounded sample: one of
+    nslabs window slabs of the whole workload (slab 0 holds the periodic wrap
+    at x = 0), every element of the mesh given.  Returns the baseline line and
+    the reference's fields on that slab (the parity sample of the GPU arm)."""
     sys.path[:0] = [os.path.join(ROOT, "oracle")]
     import oracle as O
 
     kind = "reference" if O.available("reference") else "restatement"
-    _ref_init(1234)
-    tets, secs, nb = 0, 0.0, 0
-    for b in sample_blocks():
-        t, s = _ref_block((b, 16, kind))
-        tets += t
-        secs += s
-        nb += 1
-        if secs > seconds:
-            break
+    inputs = _ref_inputs()
+    out, secs = _ref_slab(inputs, slab, nslabs, kind)
+    tets = 6 * N_PART ** 3 / nslabs
     return {"value": tets / secs, "unit": "tets/s", "cores": 1, "kind": "reference" if kind == "reference" else "port",
-            "sample": f"{nb} Lagrangian 16^3-element sub-blocks of the workload ({tets} tets, {secs:.1f} s), "
-                      f"each on a window covering it at the 256^3 voxel size"}
+            "sample": f"window slab {slab} of {nslabs} along x of the 256^3 grid (1/{nslabs} of the workload, "
+                      f"{secs:.1f} s), psi_voxels over all {N_PART ** 3} elements of the periodic mesh; tets counted "
+                      f"as 6 n^3 / {nslabs}"}, out
+
+
+def parity_on_slab(ref, deposit, nslabs=16, slab=0):
+    """The GPU's FP64 and mixed fields on the CPU-baseline sample's window
+    against the reference's: FP64 bit for bit; mixed within 1e-5 of the
+    reference plus the reference's own rounding (its distance to the
+    FP64-central result), per field in the voxel-scale normalisation."""
+    import numpy as np
+
+    from pypsi_b200.metrics import error_maps, field_errors
+
+    i0, i1, bounds = slab_window(slab, nslabs)
+    n = (i1 - i0, N_GRID, N_GRID)
+    outs = {p: deposit(n, bounds, p) for p in ("fp64", "mixed", "fp64-central")}
+    e_mr = error_maps(outs["mixed"], ref, scale_from=outs["fp64-central"])
+    e_rc = error_maps(ref, outs["fp64-central"])
+    return {"sample": f"window slab {slab} of {nslabs} along x (the CPU-baseline sample), all fields, against the "
+                      f"reference's own C code",
+            "fp64_bitwise": all(bool(np.array_equal(outs["fp64"][f], ref[f])) for f in ref),
+            "mixed_err_vs_reference": {f: e["norm"] for f, e in field_errors(outs["mixed"], ref).items()
+                                       if f != "dead_m"},
+            "mixed_within_1e5_plus_reference_rounding": all(bool(np.all(e_mr[f] <= 1e-5 + e_rc[f])) for f in e_mr)}
 
 
 # ---------------------------------------------------------------- annihilation (--workload ann)
@@ -833,6 +919,8 @@ def run_ours(args):
 
     n_part, n_grid = args.n_part, args.n_grid
     tets_per_step = 6 * n_part ** 3
+    fp64_peak = capi.measure_fma_peak("fp64")
+    fp32_peak = capi.measure_fma_peak("fp32")
     pos, vel = zeldovich(n_part, RMS, 1234 + rank)
     dev = torch.device("cuda", local)
     dpos = torch.from_numpy(pos.reshape(-1, 3)).to(dev)
@@ -846,8 +934,8 @@ def run_ours(args):
 
     stream = torch.cuda.current_stream()
 
-    def step(fields, prec):
-        return capi.voxels_device(fields, (n_grid,) * 3, BOX, dpos, dvel, block_dims=(n_part,) * 3,
+    def step(fields, prec, n=(n_grid,) * 3, bounds=BOX):
+        return capi.voxels_device(fields, n, bounds, dpos, dvel, block_dims=(n_part,) * 3,
                                   periodic_box=BOX, precision=prec, stream=stream)
 
     def barrier():
@@ -954,21 +1042,23 @@ def run_ours(args):
     if rank != 0:
         return
 
-    # roofline of the clip walk (k_bfs_init/level/leaf plus the small deep-tree
-    # kernel): the algorithmic bytes it moves -- polyhedra read and written
-    # between levels, tet vertices, fragment records -- counted by the kernels
-    # (walk_bytes), over the walk's event time, against the measured HBM copy
-    # bandwidth; beside it the FP64 arithmetic per fragment,
-    # F_2 = 20 V + 132 (2V - 4) + 520 (V = mean vertices per fragment), against
-    # the FP64 issue rate
+    # roofline of the clip walk (its init, level and leaf kernels plus the small
+    # deep-tree kernel), following the per-fragment FP64 work of the
+    # algorithm: F_2 = 20 V + 132 (2V - 4) + 520 flop per fragment (V = mean
+    # vertices per fragment; clip, reduction, projection and accumulation),
+    # over the walk's CUDA-event time, against this GPU's FP64 FMA issue rate
+    # measured live.  The mixed kernel does the clip term (20 V) in FP32: it is
+    # reported against the FP32 rate beside it.  The HBM entry counts the bytes
+    # the walk moves by its own algorithm (walk_bytes).
     s = st_mixed[-1]
     frags = s["fragments"] / s["passes"]
     vbar = s["frag_verts"] / max(1, s["fragments"])
     flops = frags * (20 * vbar + 132 * (2 * vbar - 4) + 520)
+    flops32 = frags * 20 * vbar
     clip_ms = statistics.mean(x["ms_clip"] for x in st_mixed)
     launches = s["clip_launches"]
-    fp64_tflops = flops / (clip_ms * 1e-3) / 1e12
-    fp64_peak = 148 * FP64_FMA_PER_CLK_PER_SM * 2 * 1965e6 / 1e12
+    tflops = flops / (clip_ms * 1e-3) / 1e12
+    tflops32 = flops32 / (clip_ms * 1e-3) / 1e12
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except OSError:
@@ -976,18 +1066,14 @@ def run_ours(args):
     hbm_peak = peaks.get("hbm_gbs") or 6650.0
     walk_gbs = s["walk_bytes"] / (clip_ms * 1e-3) / 1e9
     value = world * tets_per_step / (ms_mixed * 1e-3)
+    traffic = clip_traffic_bytes(frags)
     line = {
         "metric": METRIC, "value": value, "unit": "tets/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64" if head == "fp64" else "f32+f64", "data": DATA,
-        "config": {"workload": WORKLOAD if (n_part, n_grid) == (N_PART, N_GRID) else
-                   f"{n_part}^3 particles -> {n_grid}^3 grid, Zel'dovich rms 2 cells, fields m,x,v,xx,xv,vv",
-                   "precision": "fp64 (reference operation order)" if head == "fp64" else
-                   "mixed (FP32 clip, FP64 moments/accumulation)",
-                   "l2": "inputs larger than L2 (4.6 GB of grid fields, 3 GB of tet images per step)",
-                   "per_rank": "each rank deposits its own lattice (seed 1234+rank) on its own GPU"},
-        "fp64": {"value": world * tets_per_step / (ms_fp64 * 1e-3), "unit": "tets/s", "ms_per_step": ms_fp64},
-        "mixed_over_fp64": ms_fp64 / ms_mixed,
+        "config": arm_config(n_part, n_grid),
+        "precision": "fp64 (reference operation order)" if head == "fp64" else
+                     "mixed (FP32 clip, FP64 moments/accumulation)",
         "voxel_clips_per_s": world * frags / (ms_mixed * 1e-3),
         "mixed_vs_fp64_err": {f: e["norm"] for f, e in errs.items() if f != "dead_m"} if errs else None,
         "mixed_vs_fp64_err_m_rel": errs["m"]["rel"] if errs else None,
@@ -995,32 +1081,52 @@ def run_ours(args):
         "fp64_vs_fp64central_err": {f: e["norm"] for f, e in errs_rx.items() if f != "dead_m"} if errs_rx else None,
         "mixed_within_1e5_plus_reference_rounding": within,
         "mass_err": merr,
-        "fwd_bwd_over_fwd": (adjoint[f"{n_part}^3->{n_grid}^3 rms {RMS:g}"]["ratio"] if adjoint else None),
         "adjoint": adjoint,
         "stage_ms": {"tessellate_and_order": statistics.mean(x["ms_tess"] for x in st_mixed),
                      "clip": statistics.mean(x["ms_clip"] for x in st_mixed),
                      "sort_and_apply": statistics.mean(x["ms_final"] for x in st_mixed)},
         "work": {"tets": tets_per_step, "tet_images": s["tet_images"], "fragments_per_pass": frags,
                  "verts_per_fragment": vbar, "passes": s["passes"], "splits_per_pass": s["splits"] / s["passes"]},
-        "roofline": {"bound": "hbm", "achieved": walk_gbs, "peak": hbm_peak, "unit": "GB/s",
-                     "frac": walk_gbs / hbm_peak, "traffic": None,
-                     "kernel": "clip walk (k_bfs_init, k_bfs_level, k_bfs_leaf, k_clip_mixed_big)",
-                     "achieved_def": "walk_bytes (algorithmic bytes counted by the kernels: polyhedra read and "
-                                     "written, tet vertices, records) / clip event time",
-                     "units": {"walk_bytes_per_step": s["walk_bytes"], "fragments_per_step": frags},
-                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks.get("hbm_gbs")
-                     else "fallback 6650 GB/s",
-                     "fp64": {"achieved": fp64_tflops, "peak": fp64_peak, "unit": "TFLOP/s",
-                              "frac": fp64_tflops / fp64_peak,
-                              "def": "F_2 algorithmic FP64 flops per fragment / clip event time; peak = FP64 FMA "
-                                     "issue rate 64/clk/SM x 148 SMs x 2 flop at 1965 MHz"},
+        "roofline": {"bound": "fp64", "achieved": tflops, "peak": fp64_peak, "unit": "TFLOP/s",
+                     "frac": tflops / fp64_peak,
+                     "traffic": traffic["bytes_per_step"] if traffic else None,
+                     "kernel": "clip walk (its init, level and leaf kernels, and the deep-tree kernel), all launches "
+                               "of one step",
+                     "achieved_def": "F_2 = 20 V + 132 (2V - 4) + 520 algorithmic flop per fragment x fragments per "
+                                     "step / clip CUDA-event time per step",
+                     "units": {"fragments_per_step": frags, "verts_per_fragment": vbar,
+                               "flop_per_fragment": 20 * vbar + 132 * (2 * vbar - 4) + 520},
+                     "peak_source": f"measured live on this GPU: FMA-chain probe (psib_measure_fma_peak), "
+                                    f"{fp64_peak:.1f} TFLOP/s FP64; the measured-peaks file has no FP64 figure",
+                     "traffic_def": traffic["def"] if traffic else "no capture recorded",
+                     "traffic_over_algorithmic": (traffic["bytes_per_step"] / (frags * ALG_BYTES_PER_FRAGMENT)
+                                                  if traffic else None),
+                     "fp32": {"achieved": tflops32, "peak": fp32_peak, "unit": "TFLOP/s", "frac": tflops32 / fp32_peak,
+                              "def": "clip term 20 V flop per fragment (FP32 in the mixed kernel) / clip time; peak "
+                                     "measured live by the same probe in FP32"},
+                     "hbm": {"achieved": walk_gbs, "peak": hbm_peak, "unit": "GB/s", "frac": walk_gbs / hbm_peak,
+                             "def": "walk_bytes (polyhedra read and written between levels, tet vertices, records, "
+                                    "counted by the kernels) / clip time; peak MEASURED_PEAKS.json hbm_gbs"
+                                    + (" (of measured)" if peaks.get("hbm_gbs") else " (fallback)")},
                      "clip_ms_per_step": clip_ms, "clip_launches_per_step": launches},
         "e2e": e2e,
         "gpu_launches": int(sum(x["kernel_launches"] for x in st_mixed)),
         "clocks": clocks,
     }
     if world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline_single()
+        line["cpu_baseline"], ref_slab = cpu_baseline_single()
+
+        def deposit(n, bounds, prec):
+            f = {k: torch.zeros(n + sh[3:], dtype=torch.float64, device=dev) for k, sh in shapes.items()}
+            step(f, prec, n, bounds)
+            return {k: v.cpu().numpy() for k, v in f.items()}
+
+        line["parity_vs_reference"] = parity_on_slab(ref_slab, deposit)
+        capi.lib.psib_release_device_memory()
+    # the comparison the metric names, last so that the tail of the line shows it
+    line["fp64"] = {"value": world * tets_per_step / (ms_fp64 * 1e-3), "unit": "tets/s", "ms_per_step": ms_fp64}
+    line["mixed_over_fp64"] = ms_fp64 / ms_mixed
+    line["fwd_bwd_over_fwd"] = adjoint[f"{n_part}^3->{n_grid}^3 rms {RMS:g}"]["ratio"] if adjoint else None
     print(json.dumps(line), flush=True)
 
 

@@ -81,7 +81,8 @@ typedef struct {
 
 /* Lagrangian mesh.  pos and vel are npart x 3 doubles (vel may be NULL:
  * zeros), mass is one double per element (NULL: ones).  connectivity is
- * nelem x elemtype ints (elemtype 4 or 8).  With connectivity == NULL and
+ * nelem x elemtype ints (elemtype 4: tets, 8: trilinear cubes, 27: triquadratic
+ * cubes, as src/PSI.c:439-443 accepts).  With connectivity == NULL and
  * block_dims set, the trilinear block connectivity of src/PSI.c:636-656 is
  * implied (periodic wrap when periodic != 0), and is never materialised. */
 typedef struct {
@@ -114,13 +115,19 @@ typedef struct {
     long long clip_launches; /* launches of the clip kernels */
     long long kernel_launches; /* launches of this library's own kernels (library scans/sorts excluded) */
     long long walk_bytes;    /* mixed precision: bytes the breadth-first walk reads and writes by its
-                                algorithm (polyhedra, tet vertices, fragment records) */
+                                algorithm (polyhedra, tet vertices, fragment records or sums) */
+    long long corrected_items; /* atomic accumulation: tet images walked a second time to add their mass
+                                  correction (their FP32 walk missed the exact q-volume by more than 1e-14) */
+    int accumulation;        /* 1: fragments were added to per-voxel sums with atomics; 0: sorted records */
 } psib_stats;
 
 typedef struct {
     int precision;     /* PSIB_FP64, PSIB_MIXED or PSIB_FP64_CENTRAL */
-    int deterministic; /* accepted for compatibility: every call is deterministic (fragments are sorted
-                          by voxel and applied in the reference's order; FP64 equals the reference bit for bit) */
+    int deterministic; /* 0 (default): mixed and FP64-central calls add each fragment's moments to
+                          per-voxel sums with FP64 atomics and merge the sums into the fields once (the
+                          last bits may differ between runs); 1: fragments are written as records,
+                          sorted by voxel and applied in a fixed order (bit-reproducible).  PSIB_FP64
+                          always applies the records in the reference's order (bit for bit). */
     int memory;        /* PSIB_HOST or PSIB_DEVICE */
     int device;        /* CUDA device ordinal for PSIB_HOST calls (-1: current) */
     void *stream;      /* cudaStream_t for PSIB_DEVICE calls; NULL: legacy default stream */
@@ -202,13 +209,26 @@ int psib_release_device_memory(void);
  *
  * It calls no cudaMalloc or cudaFree: its scratch is a fixed array of about
  * 7.9 MiB in device memory, held by every GPU that loads the library until
- * the process exits.  Limits: a tet whose voxel index box needs a bisection
- * deeper than 12 levels (roughly more than 16 voxels on every axis) is
- * rejected with PSIB_ERR_ARG.  All calls on a device share that array: calls
- * that overlap on the GPU race.  The first call on a device looks up the
- * array's address and should come before any stream capture. */
+ * the process exits.  Limit: a tet is too large when the bisection of its
+ * voxel index box (clamped to the grid window) is deeper than 12 levels, i.e.
+ * when the sum over the three axes of ceil(log2(box size)) exceeds 12 (so
+ * 16x16x16 voxels is accepted, 16x16x32 rejected).  A first pass checks every
+ * tet: if one is too large the call returns PSIB_ERR_ARG and adds nothing to
+ * m.  Any other failure (PSIB_ERR_OVERFLOW, PSIB_ERR_INDEX) is found while
+ * depositing, so m then holds part of the call's tets.  All calls on a device
+ * share that array: calls that overlap on the GPU race.  Every call looks up
+ * the array's address (an allocation-free lookup); the first call on a device
+ * also loads the library's kernels there and should come before any stream
+ * capture. */
 int psib_voxels_density_noalloc(const psib_grid *grid, const double *tet_pos, const double *tet_mass,
                                 long long ntets, void *stream);
+
+/* The FMA issue rate of the current device in TFLOP/s (2 flop per FMA):
+ * precision PSIB_FP64 for FP64, PSIB_MIXED for FP32.  Eight independent FMA
+ * chains per thread on every SM, best of three timed launches.  It has no
+ * counterpart in the reference: it measures the denominators of the FP64 and
+ * FP32 rooflines of the clip walk.  Allocates and frees one small buffer. */
+int psib_measure_fma_peak(int precision, double *tflops);
 
 /* Element queries: for each of nboxes boxes (6 doubles each: lo xyz, hi xyz)
  * the elements whose box touches it (closed intervals) -- PSI.RStarTree(mesh)

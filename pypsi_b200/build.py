@@ -13,6 +13,7 @@ import os
 import subprocess
 import sys
 import sysconfig
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
@@ -32,6 +33,7 @@ CUDA_UNITS = {  # unit -> extra flags
     "noalloc.cu": ["--fmad=false"],
     "bfs.cu": [],
     "annihilation.cu": ["--fmad=false"],
+    "probe.cu": [],  # the FMA issue-rate probe (explicit fma(), so contraction does not matter)
     "loaders.cpp": [],  # host code only: the snapshot readers
 }
 HEADERS = ["psib_device.cuh", "psib_clip.cuh", "psib_kernels.h"]
@@ -57,14 +59,18 @@ def _run(cmd: list[str], verbose: bool) -> None:
 def build(force: bool = False, verbose: bool = False) -> None:
     os.makedirs(BUILD, exist_ok=True)
     hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, "psi_b200.h")]
-    objs = []
+    objs, jobs = [], []
     for unit, extra in CUDA_UNITS.items():
         src = os.path.join(CSRC, unit)
         obj = os.path.join(BUILD, os.path.splitext(unit)[0] + ".o")
         objs.append(obj)
         if force or _newer(obj, [src, __file__] + hdrs):
-            _run([NVCC, "-std=c++17", "-O3", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC", "-I", INCLUDE, "-I", CSRC,
-                  *extra, "-c", src, "-o", obj], verbose)
+            jobs.append([NVCC, "-std=c++17", "-O3", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC", "-I", INCLUDE, "-I",
+                         CSRC, *extra, "-c", src, "-o", obj])
+    # the translation units are independent: compile them side by side
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        for f in [ex.submit(_run, cmd, verbose) for cmd in jobs]:
+            f.result()
     if force or _newer(LIB, objs):
         _run([NVCC, "-shared", *ARCH, "-o", LIB, *objs], verbose)
     msrc = os.path.join(CSRC, "psi_module.c")

@@ -4,7 +4,8 @@
 live on the GPU (torch CUDA tensors here, raw device pointers in general) and on
 the caller's CUDA stream.  It is also the template of the binding a maintainer
 of the reference would add to call the library from Python without the PSI
-extension.
+extension: one ctypes structure per C struct of the header, one argtypes line
+per entry point, and a status code turned into an exception.
 """
 from __future__ import annotations
 
@@ -35,7 +36,8 @@ class Stats(C.Structure):
                 ("fragments", C.c_longlong), ("frag_verts", C.c_longlong), ("splits", C.c_longlong),
                 ("passes", C.c_int), ("chunks", C.c_int), ("ms_total", C.c_float), ("ms_clip", C.c_float),
                 ("ms_tess", C.c_float), ("ms_final", C.c_float), ("clip_launches", C.c_longlong),
-                ("kernel_launches", C.c_longlong), ("walk_bytes", C.c_longlong)]
+                ("kernel_launches", C.c_longlong), ("walk_bytes", C.c_longlong),
+                ("corrected_items", C.c_longlong), ("accumulation", C.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -61,6 +63,8 @@ lib.psib_query_elements.restype = C.c_int
 lib.psib_sample_vdf.argtypes = [C.POINTER(Mesh), C.c_void_p, C.c_void_p, C.c_longlong, C.c_double, C.c_int, C.c_void_p,
                                 C.c_void_p, C.c_void_p, C.c_longlong, C.POINTER(Options)]
 lib.psib_sample_vdf.restype = C.c_int
+lib.psib_measure_fma_peak.argtypes = [C.c_int, C.POINTER(C.c_double)]
+lib.psib_measure_fma_peak.restype = C.c_int
 lib.psib_last_error.restype = C.c_char_p
 lib.psib_release_device_memory.restype = C.c_int
 
@@ -69,6 +73,15 @@ class PsibError(RuntimeError):
     def __init__(self, code: int):
         self.code = code
         super().__init__(f"psib_voxels failed (code {code}): {lib.psib_last_error().decode()}")
+
+
+def measure_fma_peak(precision="fp64") -> float:
+    """This GPU's FMA issue rate in TFLOP/s, 'fp64' or 'fp32' (psib_measure_fma_peak)."""
+    out = C.c_double(0.0)
+    rc = lib.psib_measure_fma_peak(PSIB_FP64 if precision == "fp64" else PSIB_MIXED, C.byref(out))
+    if rc != 0:
+        raise PsibError(rc)
+    return out.value
 
 
 def make_grid(n, bounds, field_ptrs: dict) -> Grid:
@@ -177,7 +190,8 @@ def adjoint_device(grad_m, n, bounds, pos, grad_pos, mass=None, connectivity=Non
 
 
 def voxels_batch_device(cutouts: list, precision="fp64", refine_tolerance=1.0, refine_max_lvl=0,
-                        refine_criterion="midpoint", refine_cell=None, stream=None, queue_voxels=0) -> dict:
+                        refine_criterion="midpoint", refine_cell=None, stream=None, queue_voxels=0,
+                        deterministic=False) -> dict:
     """Many independent deposits in one pass (psib_voxels_batch).
 
     cutouts: dicts with the arguments of voxels_device -- fields, n, bounds,
@@ -196,9 +210,9 @@ def voxels_batch_device(cutouts: list, precision="fp64", refine_tolerance=1.0, r
                                       c.get("block_dims"), c.get("periodic_box"))
     s = stream if stream is not None else torch.cuda.current_stream()
     st = Stats()
-    o = Options(precision=PRECISIONS[precision], deterministic=0, memory=PSIB_DEVICE, device=-1,
-                stream=C.c_void_p(s.cuda_stream), stats=C.pointer(st), refine_mode=REFINE[refine_criterion],
-                queue_voxels=int(queue_voxels))
+    o = Options(precision=PRECISIONS[precision], deterministic=int(bool(deterministic)), memory=PSIB_DEVICE,
+                device=-1, stream=C.c_void_p(s.cuda_stream), stats=C.pointer(st),
+                refine_mode=REFINE[refine_criterion], queue_voxels=int(queue_voxels))
     if refine_cell is not None:
         o.refine_cell[:] = [float(v) for v in refine_cell]
     rc = lib.psib_voxels_batch(grids, meshes, nb, 0, float(refine_tolerance), int(refine_max_lvl), C.byref(o))

@@ -34,6 +34,7 @@
 // A level queue never holds more polyhedra than the leaves its images will
 // produce, which is at most the sum of their index-box volumes; the host sizes
 // each pass of images by that bound.
+#include "psib_accum.cuh"
 #include "psib_device.cuh"
 #include "psib_kernels.h"
 
@@ -185,10 +186,14 @@ __global__ void __launch_bounds__(BB) k_bfs_init(BfsArgs a)
         const unsigned long long bq = warp_reserve(a.out.count, use && !leaf ? 1u : 0u, oq);
         const unsigned long long bl = warp_reserve(a.leaf.count, leaf ? 1u : 0u, ol);
         if (to_dfs) a.dfs_list[bd + od] = t;
-        if (wbfs && !use) a.c.scale[t] = 1.0; // wholly outside the window: deposits nothing
+        // the correction pass walks images again with their mass factor: their scale stays as it is
+        const bool main_pass = a.c.acc.factor == nullptr;
+        if (wbfs && !use && main_pass) a.c.scale[t] = 1.0; // wholly outside the window: deposits nothing
         if (use) {
-            a.c.scale[t] = -target; // marks a breadth-first image: bfs_finalize sets its mass correction
-            a.vsum[t] = 0.0;
+            if (main_pass) {
+                a.c.scale[t] = -target; // marks a breadth-first image: bfs_finalize sets its mass correction
+                a.vsum[t] = 0.0;
+            }
             const PolyQueue& Q = leaf ? a.leaf : a.out;
             const unsigned long long e = leaf ? bl + ol : bq + oq;
             if (e >= Q.cap) {
@@ -534,7 +539,7 @@ __device__ __forceinline__ unsigned leaf_moments(int nv, const uint32_t* nbs, co
     return 0;
 }
 
-__global__ void __launch_bounds__(BB) k_bfs_leaf(BfsArgs a)
+__global__ void __launch_bounds__(BB, 3) k_bfs_leaf(BfsArgs a)
 {
     extern __shared__ uint32_t smem[];
     uint32_t* nbs = smem;
@@ -600,10 +605,17 @@ __global__ void __launch_bounds__(BB) k_bfs_leaf(BfsArgs a)
                         rec[7] = mom[7] / m0 - u[1] * u[1];
                         rec[8] = mom[8] / m0 - u[1] * u[2];
                         rec[9] = mom[9] / m0 - u[2] * u[2];
-                        has = true;
                         ++frags;
                         verts += nv;
-                        atomicAdd(&a.vsum[t], m0);
+                        if (c.acc.sum) {
+                            // atomic mode: straight into the voxel's sums, no record
+                            const double f = c.acc.factor ? c.acc.factor[t] : 1.0;
+                            accumulate_fragment(c, g, c.grids ? (int)c.it.grid[t] : 0, gi, lo, t, rec, f);
+                            moved += 8ull * c.acc.stride;
+                        } else {
+                            has = true;
+                        }
+                        if (!c.acc.factor) atomicAdd(&a.vsum[t], m0);
                     }
                 }
             }

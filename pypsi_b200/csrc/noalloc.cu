@@ -21,20 +21,29 @@
 //   * The array holds NA_THREADS slot regions of NA_NS polyhedra each,
 //     NA_SCRATCH_BYTES (about 7.9 MiB) in total.  Every GPU that loads the
 //     library keeps it until the process exits.
-//   * A tet whose voxel index box needs a bisection deeper than NA_DMAX levels
-//     (roughly more than 16 voxels along each axis) is rejected: the call
-//     returns PSIB_ERR_ARG and deposits nothing for that tet.
+//   * Depth limit: a tet is too large when the bisection of its voxel index
+//     box (after the clamp to the grid window) is deeper than NA_DMAX = 12
+//     levels, i.e. when sum over the three axes of ceil(log2(size_a)) > 12
+//     (axes of size 1 count 0).  16x16x16 voxels (4 + 4 + 4) is accepted,
+//     16x16x32 (4 + 4 + 5) rejected, 4096x1x1 (12) accepted.  A first kernel
+//     checks every tet; if one is too large the call returns PSIB_ERR_ARG and
+//     deposits nothing at all.
+//   * Any other failure found while depositing (a polyhedron that outgrows
+//     its vertex buffer, a face walk that does not close, a voxel index out of
+//     range) returns PSIB_ERR_OVERFLOW or PSIB_ERR_INDEX after the other tets,
+//     and part of the failing tet, have already been added to m.
 //   * All calls on a device share the array and its queue and status words,
 //     which keep the last call's contents; each call clears the words that
 //     must start at zero.  Calls that overlap on the GPU (on different
 //     streams, or from different host threads) race on them.
-//   * The first call on a device looks up the array's device address
-//     (cudaGetSymbolAddress, with that device current) and caches it; it
-//     should come before any stream capture.
+//   * Every call looks up the array's device address with
+//     cudaGetSymbolAddress (with the caller's device current; it allocates
+//     nothing), so the address stays valid after a cudaDeviceReset.  The first
+//     call on a device also loads the library's kernels there and should come
+//     before any stream capture.
 #include <cuda_runtime.h>
 
 #include <cstdio>
-#include <mutex>
 
 #include "psi_b200.h"
 #include "psib_clip.cuh"
@@ -43,8 +52,8 @@ namespace psib {
 
 namespace {
 
-constexpr int NA_BLOCK = 128;
-constexpr int NA_THREADS = 4 * NA_BLOCK;                  // resident threads of one call
+constexpr int NA_BLOCK = 32;                              // one warp per block: the regions spread over 16 SMs
+constexpr int NA_THREADS = 16 * NA_BLOCK;                 // resident threads of one call
 constexpr int NA_DMAX = 12;                               // deepest bisection served
 constexpr int NA_NS = NA_DMAX + 3;                        // slots per thread
 constexpr size_t NA_REGION = sizeof(Poly<double>) * NA_NS; // bytes per thread
@@ -68,6 +77,31 @@ struct NaArgs {
     unsigned char *scratch; // device address of g_noalloc_scratch
 };
 
+// The tet's voxel index box, clamped to the grid window (src/geometry.c:816-842).
+__device__ __forceinline__ void index_box(const NaArgs& a, const double (*rb)[3], int* lo, int* hi)
+{
+    for (int i = 0; i < 3; ++i) {
+        double cmin = rb[0][i], cmax = rb[1][i];
+        if (a.g.w0[i] > cmin) cmin = a.g.w0[i];
+        if (a.g.w1[i] < cmax) cmax = a.g.w1[i];
+        lo[i] = (int)floor((cmin - a.g.w0[i]) / a.g.d[i]);
+        hi[i] = (int)ceil((cmax - a.g.w0[i]) / a.g.d[i]);
+        if (lo[i] < 0) lo[i] = 0;
+        if (hi[i] > a.g.n[i]) hi[i] = a.g.n[i];
+    }
+}
+
+// Depth of the box's bisection: sum over the axes of ceil(log2(size)).
+__device__ __forceinline__ int box_depth(const int* lo, const int* hi)
+{
+    int depth = 0;
+    for (int i = 0; i < 3; ++i) {
+        const int sz = hi[i] - lo[i];
+        if (sz > 1) depth += 32 - __clz(sz - 1);
+    }
+    return depth;
+}
+
 // Depth-first bisection of one tet with mass deposited by atomics.  Same
 // arithmetic as clip_item<double, ..> up to the fragment's m0.
 __device__ void deposit_tet(const NaArgs& a, long long t, Poly<double>* S, unsigned& st)
@@ -78,7 +112,7 @@ __device__ void deposit_tet(const NaArgs& a, long long t, Poly<double>* S, unsig
     const double mass = a.mass ? a.mass[t] : 1.0;
     double rb[2][3];
     aabb4(p, rb);
-    int pax[6], psg[6], npl = 0, lo[3], hi[3], depth = 0;
+    int pax[6], psg[6], npl = 0, lo[3], hi[3];
     double pdd[6];
     for (int i = 0; i < 3; ++i) {
         double cmin = rb[0][i], cmax = rb[1][i];
@@ -87,15 +121,10 @@ __device__ void deposit_tet(const NaArgs& a, long long t, Poly<double>* S, unsig
         if (chi) cmax = a.g.w1[i];
         if (clo) { pax[npl] = i; psg[npl] = 1; pdd[npl] = -cmin; npl++; }
         if (chi) { pax[npl] = i; psg[npl] = -1; pdd[npl] = cmax; npl++; }
-        lo[i] = (int)floor((cmin - a.g.w0[i]) / a.g.d[i]);
-        hi[i] = (int)ceil((cmax - a.g.w0[i]) / a.g.d[i]);
-        if (lo[i] < 0) lo[i] = 0;
-        if (hi[i] > a.g.n[i]) hi[i] = a.g.n[i];
-        const int sz = hi[i] - lo[i];
-        if (sz > 1) depth += 32 - __clz(sz - 1);
     }
-    if (depth > NA_DMAX) {
-        st |= ST_DEPTH; // too large for the fixed slot pool: rejected, nothing deposited
+    index_box(a, rb, lo, hi);
+    if (box_depth(lo, hi) > NA_DMAX) {
+        st |= ST_DEPTH; // cannot happen after the pre-pass; kept so that no slot pool is overrun
         return;
     }
     uint32_t freem = (1u << NA_NS) - 1u;
@@ -196,9 +225,30 @@ __device__ void deposit_tet(const NaArgs& a, long long t, Poly<double>* S, unsig
     }
 }
 
+// Pre-pass: flags ST_DEPTH when any tet is too deep for the slot pool, so
+// that the deposit kernel, launched next on the same stream, adds nothing.
+__global__ void k_noalloc_depth(NaArgs a)
+{
+    NaState* state = (NaState*)a.scratch;
+    bool deep = false;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < a.ntets;
+         t += (long long)gridDim.x * blockDim.x) {
+        double p[4][3];
+        for (int v = 0; v < 4; ++v)
+            for (int i = 0; i < 3; ++i) p[v][i] = a.pos[12 * t + 3 * v + i];
+        double rb[2][3];
+        aabb4(p, rb);
+        int lo[3], hi[3];
+        index_box(a, rb, lo, hi);
+        deep = deep || box_depth(lo, hi) > NA_DMAX;
+    }
+    if (__any_sync(0xFFFFFFFFu, deep) && (threadIdx.x & 31) == 0) atomicOr(&state->status, ST_DEPTH);
+}
+
 __global__ void __launch_bounds__(NA_BLOCK) k_density_noalloc(NaArgs a)
 {
     NaState* state = (NaState*)a.scratch;
+    if (*(volatile unsigned*)&state->status & ST_DEPTH) return; // the pre-pass rejected the call
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     Poly<double>* S = (Poly<double>*)(a.scratch + NA_STATE + (size_t)tid * NA_REGION);
     const int lane = threadIdx.x & 31;
@@ -214,27 +264,20 @@ __global__ void __launch_bounds__(NA_BLOCK) k_density_noalloc(NaArgs a)
     if (st) atomicOr(&state->status, st);
 }
 
-std::mutex g_na_mu;
-unsigned char* g_na_ptr[64];
-
-// Device address of the scratch array on the current device, looked up once.
-int noalloc_scratch(int dev, unsigned char** out)
+// Device address of the scratch array on the current device.  Looked up on
+// every call (cudaGetSymbolAddress allocates nothing), so that it is right
+// for the device's current context, also after a cudaDeviceReset.
+int noalloc_scratch(unsigned char** out)
 {
-    std::lock_guard<std::mutex> lk(g_na_mu);
-    if (dev < 0 || dev >= 64) return report_error(PSIB_ERR_ARG, "device ordinal out of range");
-    if (!g_na_ptr[dev]) {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p) {
-            cudaGetLastError();
-            char msg[256];
-            snprintf(msg, sizeof(msg), "cudaGetSymbolAddress of the no-alloc scratch failed: %s",
-                     cudaGetErrorString(e));
-            return report_error(PSIB_ERR_CUDA, msg);
-        }
-        g_na_ptr[dev] = (unsigned char*)p;
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+        cudaGetLastError();
+        char msg[256];
+        snprintf(msg, sizeof(msg), "cudaGetSymbolAddress of the no-alloc scratch failed: %s", cudaGetErrorString(e));
+        return report_error(PSIB_ERR_CUDA, msg);
     }
-    *out = g_na_ptr[dev];
+    *out = (unsigned char*)p;
     return PSIB_OK;
 }
 
@@ -259,13 +302,8 @@ extern "C" int psib_voxels_density_noalloc(const psib_grid* grid, const double* 
     }
     if (ntets == 0) return PSIB_OK;
     if (psib_device_count() <= 0) return report_error(PSIB_ERR_NODEVICE, "no CUDA device is visible");
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) {
-        cudaGetLastError();
-        return report_error(PSIB_ERR_CUDA, "cudaGetDevice failed");
-    }
     unsigned char* scratch = nullptr;
-    int rc = noalloc_scratch(dev, &scratch);
+    int rc = noalloc_scratch(&scratch);
     if (rc != PSIB_OK) return rc;
     cudaStream_t st = (cudaStream_t)stream;
     NaArgs a;
@@ -283,6 +321,10 @@ extern "C" int psib_voxels_density_noalloc(const psib_grid* grid, const double* 
     // the queue head and the status word start at zero on every call
     cudaError_t e = cudaMemsetAsync(scratch, 0, NA_STATE, st);
     if (e == cudaSuccess) {
+        k_noalloc_depth<<<64, 256, 0, st>>>(a);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) {
         k_density_noalloc<<<NA_THREADS / NA_BLOCK, NA_BLOCK, 0, st>>>(a);
         e = cudaGetLastError();
     }
@@ -296,8 +338,9 @@ extern "C" int psib_voxels_density_noalloc(const psib_grid* grid, const double* 
         return report_error(PSIB_ERR_CUDA, msg);
     }
     if (h.status & ST_DEPTH)
-        return report_error(PSIB_ERR_ARG, "a tet is too large for psib_voxels_density_noalloc: its voxel index box "
-                                          "needs a bisection deeper than 12 levels (use psib_voxels)");
+        return report_error(PSIB_ERR_ARG, "a tet is too large for psib_voxels_density_noalloc: the bisection of its "
+                                          "voxel index box, sum of ceil(log2(size)) over the axes, is deeper than 12 "
+                                          "levels (use psib_voxels); nothing was deposited");
     if (h.status & ST_INDEX) return report_error(PSIB_ERR_INDEX, "voxel index out of range");
     if (h.status) return report_error(PSIB_ERR_OVERFLOW, "a polyhedron outgrew its vertex buffer or slot pool");
     return PSIB_OK;

@@ -118,6 +118,8 @@ struct Ctx {
     // breadth-first clip: three polyhedron queues, the volume histogram, per-level counters, window list
     DevBuf qx[3], qnb[3], qnv[3], qwin[3], qbox[3], qitem[3], hist, bfs_cnt, dfs_list, vsum;
     DevBuf btab, igrid; // batch tables, image -> cutout
+    // atomic accumulation: per-voxel sums, tile reference velocities, the mass-correction pass
+    DevBuf acc_sum, acc_tsum, acc_vref, acc_toff, fix_list, fix_keys, fix_list_s, fix_keys_s, ifactor;
     DevBuf passes;      // breadth-first pass table
     // annihilation: element tets and boxes, cell registrations, element and tet pairs
     DevBuf a_cnt, a_off, a_ebox, a_tets_a, a_tets_b, a_stats, a_reg_cnt, a_reg_off, a_reg_key, a_reg_elem,
@@ -140,7 +142,8 @@ struct Ctx {
                 &a_reg_cnt, &a_reg_off, &a_reg_key, &a_reg_elem, &a_reg_key_s, &a_reg_elem_s, &a_run_key,
                 &a_run_cnt, &a_run_off, &a_run_lo, &a_run_hi, &a_pair_cnt, &a_pair_off, &a_pair_key,
                 &a_pair_key_s, &a_na, &a_aoff, &a_tp_cnt, &a_tp_excl, &a_bounds, &a_tpairs, &a_deep, &a_tp_key,
-                &a_tp_key_s, &a_ord_in, &a_ord, &q_in, &q_cnt,
+                &a_tp_key_s, &a_ord_in, &a_ord, &q_in, &q_cnt, &acc_sum, &acc_tsum, &acc_vref, &acc_toff,
+                &fix_list, &fix_keys, &fix_list_s, &fix_keys_s, &ifactor,
                 &q_off, &q_key, &q_key_s, &q_out, &s_cnt, &s_off, &s_offs, &s_rho, &s_vel};
     }
 };
@@ -171,7 +174,7 @@ int get_ctx(int dev, Ctx** out)
 
 // small device block layout (unsigned long long words)
 enum { S_STATUS = 0, S_CNT = 1 /* 3 words */, S_TESS = 4 /* 2 */, S_HEAD = 8 /* 4 */, S_RECN = 12, S_NDEEP = 13,
-       S_DFS = 14, S_BYTES = 15, S_PASS = 6, S_WORDS = 16 };
+       S_DFS = 14, S_BYTES = 15, S_PASS = 6, S_FIX = 7, S_WORDS = 16 };
 
 // Histogram of the sorted footprint keys: lanes holding equal keys (most of a
 // warp, as the keys are sorted) add with one atomic.
@@ -280,13 +283,14 @@ int leave_own_stream(Ctx& C, cudaStream_t user)
     return PSIB_OK;
 }
 
+// keys: the footprint keys of the queue positions [0, nmain), ascending.
 int bfs_clip(Ctx& C, ClipArgs& ca, long long nmain, long long nitems, unsigned long long* sm, int clip_grid,
              int clip_block, long long queue_voxels, bool batch, cudaStream_t st, long long& launches,
-             long long& klaunch)
+             long long& klaunch, const uint16_t* keys)
 {
     RET(ensure(C.hist, 65536 * sizeof(unsigned)));
     CK(cudaMemsetAsync(C.hist.p, 0, 65536 * sizeof(unsigned), st));
-    k_key_hist<<<C.num_sms * 4, 256, 0, st>>>(C.key_sorted.as<uint16_t>(), nmain, C.hist.as<unsigned>());
+    k_key_hist<<<C.num_sms * 4, 256, 0, st>>>(keys, nmain, C.hist.as<unsigned>());
     CK(cudaGetLastError());
     klaunch++;
     std::vector<unsigned> hist(65536);
@@ -526,6 +530,46 @@ int stretch_cell(const psib_mesh& m, const double* given, double* lag)
 
 int run_annihilation(Call& c);
 
+// The mass correction of the atomic mode.  A breadth-first image's FP32 walk
+// can miss the exact q-volume by O(1e-7) where a fragment vertex falls back to
+// its FP32 position; the record path scales every fragment of such an image by
+// target / (sum of its fragment volumes) when it applies the records.  Atomic
+// sums are linear in an image's mass, so the same correction is a second walk
+// of just those images with mass factor (scale - 1): bfs_finalize has computed
+// scale for every image; those more than tol from 1 are listed (footprint keys
+// ascending, as the pass planner wants them) and walked again.
+int correct_masses(Ctx& C, const ClipArgs& ca, long long nitems, unsigned long long* sm, int clip_grid,
+                   int clip_block, long long queue_voxels, cudaStream_t st, long long& launches, long long& klaunch,
+                   long long& ncorr)
+{
+    constexpr double tol = 1e-14;
+    RET(ensure(C.fix_list, (size_t)nitems * sizeof(int)));
+    RET(ensure(C.fix_keys, (size_t)nitems * sizeof(uint16_t)));
+    RET(ensure(C.ifactor, (size_t)nitems * sizeof(double)));
+    CK(cudaMemsetAsync(&sm[S_FIX], 0, 8, st));
+    CK(launch_correction_select(ca.it, ca.scale, nitems, tol, C.fix_list.as<int>(), C.fix_keys.as<uint16_t>(),
+                                C.ifactor.as<double>(), &sm[S_FIX], C.num_sms, st));
+    klaunch++;
+    unsigned long long n = 0;
+    CK(cudaMemcpyAsync(&n, &sm[S_FIX], 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    ncorr = (long long)n;
+    if (n == 0) return PSIB_OK;
+    RET(ensure(C.fix_list_s, (size_t)n * sizeof(int)));
+    RET(ensure(C.fix_keys_s, (size_t)n * sizeof(uint16_t)));
+    size_t tb = 0;
+    CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, C.fix_keys.as<uint16_t>(), C.fix_keys_s.as<uint16_t>(),
+                                       C.fix_list.as<int>(), C.fix_list_s.as<int>(), (int)n, 0, 16, st));
+    RET(ensure(C.cub_tmp, tb));
+    CK(cub::DeviceRadixSort::SortPairs(C.cub_tmp.p, tb, C.fix_keys.as<uint16_t>(), C.fix_keys_s.as<uint16_t>(),
+                                       C.fix_list.as<int>(), C.fix_list_s.as<int>(), (int)n, 0, 16, st));
+    ClipArgs cf = ca;
+    cf.order = C.fix_list_s.as<int>();
+    cf.acc.factor = C.ifactor.as<double>();
+    return bfs_clip(C, cf, (long long)n, nitems, sm, clip_grid, clip_block, queue_voxels, false, st, launches,
+                    klaunch, C.fix_keys_s.as<uint16_t>());
+}
+
 int run_device(Call& c)
 {
     if (c.mode == PSIB_MODE_ANNIHILATION) return run_annihilation(c);
@@ -565,6 +609,11 @@ int run_device(Call& c)
             if ((batch ? c.grids[b] : g).n[i] >= 0xFFFF) use_bfs = false; // box bounds are packed in 16 bits
     // 1, 4 or 10 moments per record (FP32 kernel: m0, q-centroid, central second moment)
     const int nmom = order == 2 ? 10 : order == 1 ? 4 : 1;
+    // Fragments added to per-voxel sums with atomics (deterministic == 0): central-form
+    // fragments whose mass correction is 1 or applied by a second walk -- the breadth-first
+    // walk (window images included) and the FP64 walks.  Otherwise records, sorted and applied.
+    const bool window_bfs = env_ll("PSIB_BFS_WINDOW", 1) != 0;
+    const bool atomic = central && !c.deterministic && !c.adjoint && (!mixed || (use_bfs && window_bfs));
 
     const GridDev gd = grid_dev(g);
     const MeshDev md = mesh_dev(m, g, c.pos, c.vel, c.mass, c.conn, c.reftol, c.refine_cell);
@@ -726,7 +775,38 @@ int run_device(Call& c)
         ca.adj_mass_factor = m.elemtype == 8 ? 1.0 / 6.0 : 1.0;
     }
 
+    long long ntiles = 0;
+    if (atomic) {
+        // the per-voxel sums (only those the fields need), zeroed; the tiles' reference velocities
+        int stride = 1, ox = -1, ov = -1, oxx = -1, oxv = -1, ovv = -1;
+        if (flags & (F_X | F_XX | F_XV)) { ox = stride; stride += 3; }
+        if (flags & (F_V | F_VV | F_XV)) { ov = stride; stride += 3; }
+        if (flags & F_XX) { oxx = stride; stride += 6; }
+        if (flags & F_XV) { oxv = stride; stride += 9; }
+        if (flags & F_VV) { ovv = stride; stride += 6; }
+        RET(ensure(C.acc_sum, (size_t)nvox * stride * sizeof(double)));
+        CK(cudaMemsetAsync(C.acc_sum.p, 0, (size_t)nvox * stride * sizeof(double), st));
+        const long long* d_toff = nullptr;
+        if (batch) {
+            std::vector<long long> toff(c.nbatch + 1, 0);
+            for (int b = 0; b < c.nbatch; ++b) toff[b + 1] = toff[b] + acc_tiles(grid_dev(c.grids[b]));
+            ntiles = toff[c.nbatch];
+            RET(ensure(C.acc_toff, toff.size() * sizeof(long long)));
+            CK(cudaMemcpyAsync(C.acc_toff.p, toff.data(), toff.size() * sizeof(long long), cudaMemcpyHostToDevice,
+                               st));
+            CK(cudaStreamSynchronize(st)); // the host table goes out of scope
+            d_toff = C.acc_toff.as<long long>();
+        } else {
+            ntiles = acc_tiles(gd);
+        }
+        RET(ensure(C.acc_tsum, (size_t)ntiles * 4 * sizeof(double)));
+        RET(ensure(C.acc_vref, (size_t)ntiles * 3 * sizeof(double)));
+        ca.acc = AccArgs{C.acc_sum.as<double>(), stride, ox, ov, oxx, oxv, ovv, C.acc_vref.as<double>(), d_toff,
+                         nullptr};
+    }
+
     float ms_clip = 0.f, ms_tess = 0.f, ms_final = 0.f;
+    long long corrected = 0;
     unsigned long long clip_counts[3] = {0, 0, 0}; // fragments, fragment vertices, splits
     unsigned long long walk_bytes = 0;
     long long launches = 0;
@@ -801,6 +881,56 @@ int run_device(Call& c)
             for (int w = 0; w < 3; ++w) clip_counts[w] += h[S_CNT + w];
             continue;
         }
+        if (atomic) {
+            // ---- clip, each fragment added to its voxel's sums ----
+            CK(cudaMemsetAsync(&sm[S_BYTES], 0, 8, st));
+            CK(cudaMemsetAsync(&sm[S_CNT], 0, 24, st));
+            CK(cudaMemsetAsync(&sm[S_HEAD], 0, 16, st));
+            CK(cudaEventRecord(C.ev[4], st));
+            if (k == 0) {
+                // the tiles' reference velocities, fixed before the first fragment is added
+                CK(cudaMemsetAsync(C.acc_tsum.p, 0, (size_t)ntiles * 4 * sizeof(double), st));
+                CK(launch_vref(it, nitems, gd, d_grids, ca.acc, C.acc_tsum.as<double>(), ntiles, C.num_sms, st));
+                klaunch += 2;
+            }
+            if (nmain > 0 && use_bfs) {
+                ca.scratch = C.scratch.p;
+                RET(bfs_clip(C, ca, nmain, nitems, sm, clip_grid, clip_block, c.queue_voxels, batch, st, launches,
+                             klaunch, C.key_sorted.as<uint16_t>()));
+                long long ncorr = 0;
+                RET(correct_masses(C, ca, nitems, sm, clip_grid, clip_block, c.queue_voxels, st, launches, klaunch,
+                                   ncorr));
+                corrected += ncorr;
+            } else if (nmain > 0) {
+                ca.scratch = C.scratch.p;
+                ca.order_base = 0;
+                ca.n = nmain;
+                ca.head = &sm[S_HEAD];
+                CK(launch_clip_mixed(ca, false, !mixed, clip_grid, clip_block, st));
+                launches++;
+            }
+            if (ndeep > 0) {
+                const int big_grid = (int)std::min<long long>(C.num_sms * 2, (ndeep + big_block - 1) / big_block);
+                RET(ensure(C.scratch_big, big_bytes * (size_t)big_grid * big_block));
+                ca.scratch = C.scratch_big.p;
+                ca.order_base = nmain;
+                ca.n = ndeep;
+                ca.head = &sm[S_HEAD + 1];
+                CK(launch_clip_mixed(ca, true, !mixed, big_grid, big_block, st));
+                launches++;
+            }
+            CK(cudaEventRecord(C.ev[5], st));
+            unsigned long long h[S_WORDS];
+            CK(cudaMemcpyAsync(h, sm, sizeof(h), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            float t = 0.f;
+            CK(cudaEventElapsedTime(&t, C.ev[4], C.ev[5]));
+            ms_clip += t;
+            RET(check_status(c, h));
+            for (int w = 0; w < 3; ++w) clip_counts[w] += h[S_CNT + w];
+            walk_bytes += h[S_BYTES];
+            continue;
+        }
         // ---- clip to fragment records; grow the record buffer and redo if it overflowed ----
         int ibits = 1, vbits = 1;
         while ((1ll << ibits) < nitems) ++ibits;
@@ -823,7 +953,7 @@ int run_device(Call& c)
             if (nmain > 0 && use_bfs) {
                 ca.scratch = C.scratch.p;
                 RET(bfs_clip(C, ca, nmain, nitems, sm, clip_grid, clip_block, c.queue_voxels, batch, st, launches,
-                             klaunch));
+                             klaunch, C.key_sorted.as<uint16_t>()));
             } else if (nmain > 0) {
                 ca.scratch = C.scratch.p;
                 ca.order_base = 0;
@@ -981,12 +1111,56 @@ int run_device(Call& c)
             break;
         }
     }
+    if (atomic) {
+        // ---- merge every voxel's sums into its fields; host calls copy each slab back beside the next ----
+        CK(cudaEventRecord(C.ev[6], st));
+        FinalArgs fa = {};
+        fa.ap.M = c.F[0]; fa.ap.X = c.F[1]; fa.ap.V = c.F[2]; fa.ap.XX = c.F[3]; fa.ap.XV = c.F[4]; fa.ap.VV = c.F[5];
+        fa.ap.nbatch = batch ? c.nbatch : 0;
+        fa.ap.voff = d_voff;
+        fa.ap.fptr = d_fptr;
+        fa.acc = ca.acc;
+        fa.g = gd;
+        fa.grids = d_grids;
+        if (c.fields_ready) CK(cudaStreamWaitEvent(st, c.fields_ready, 0));
+        if (c.host_fields && !batch && nvox >= 4 * NOUT) {
+            static const int comps[6] = {1, 3, 3, 9, 9, 9};
+            for (int p = 0; p < NOUT; ++p) {
+                fa.v0 = nvox * p / NOUT;
+                fa.v1 = nvox * (p + 1) / NOUT;
+                CK(launch_acc_finalize(fa, C.num_sms, st));
+                CK(cudaEventRecord(C.ev_out[p], st));
+                CK(cudaStreamWaitEvent(C.copy, C.ev_out[p], 0));
+                for (int f = 0; f < 6; ++f) {
+                    if (!c.F[f]) continue;
+                    const size_t o = (size_t)fa.v0 * comps[f] * sizeof(double);
+                    const size_t n = (size_t)(fa.v1 - fa.v0) * comps[f] * sizeof(double);
+                    CK(cudaMemcpyAsync((char*)c.host_fields[f] + o, (const char*)c.F[f] + o, n,
+                                       cudaMemcpyDeviceToHost, C.copy));
+                }
+            }
+            c.copied_out = true;
+            klaunch += NOUT;
+        } else {
+            fa.v0 = 0;
+            fa.v1 = nvox;
+            CK(launch_acc_finalize(fa, C.num_sms, st));
+            klaunch++;
+        }
+        CK(cudaEventRecord(C.ev[7], st));
+        CK(cudaEventSynchronize(C.ev[7]));
+        float t = 0.f;
+        CK(cudaEventElapsedTime(&t, C.ev[6], C.ev[7]));
+        ms_final += t;
+    }
     unsigned long long h[S_WORDS];
     CK(cudaMemcpyAsync(h, sm, sizeof(h), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     RET(check_status(c, h));
     if (c.stats) {
         psib_stats& s = *c.stats;
+        s.corrected_items = corrected;
+        s.accumulation = atomic ? 1 : 0;
         s.elements_kept = (long long)h[S_TESS];
         s.tets = (long long)h[S_TESS + 1];
         s.tet_images = total;

@@ -695,12 +695,13 @@ static PyObject *PSI_last_stats(PyObject *self, PyObject *noargs)
     (void)self;
     (void)noargs;
     const psib_stats *s = &g_last_stats;
-    return Py_BuildValue("{s:L,s:L,s:L,s:L,s:L,s:L,s:i,s:i,s:f,s:f,s:f,s:f,s:L,s:L}", "elements_kept", s->elements_kept,
-                         "tets", s->tets, "tet_images", s->tet_images, "fragments", s->fragments, "frag_verts",
-                         s->frag_verts, "splits", s->splits, "passes", s->passes, "chunks", s->chunks, "ms_total",
-                         (double)s->ms_total, "ms_clip", (double)s->ms_clip, "ms_tess", (double)s->ms_tess, "ms_final",
-                         (double)s->ms_final, "clip_launches", s->clip_launches, "kernel_launches",
-                         s->kernel_launches);
+    return Py_BuildValue("{s:L,s:L,s:L,s:L,s:L,s:L,s:i,s:i,s:f,s:f,s:f,s:f,s:L,s:L,s:L,s:L,s:i}", "elements_kept",
+                         s->elements_kept, "tets", s->tets, "tet_images", s->tet_images, "fragments", s->fragments,
+                         "frag_verts", s->frag_verts, "splits", s->splits, "passes", s->passes, "chunks", s->chunks,
+                         "ms_total", (double)s->ms_total, "ms_clip", (double)s->ms_clip, "ms_tess", (double)s->ms_tess,
+                         "ms_final", (double)s->ms_final, "clip_launches", s->clip_launches, "kernel_launches",
+                         s->kernel_launches, "walk_bytes", s->walk_bytes, "corrected_items", s->corrected_items,
+                         "accumulation", s->accumulation);
 }
 
 static PyObject *PSI_device_count(PyObject *self, PyObject *noargs)

@@ -24,6 +24,7 @@
 // interleave threads word by word and waste most of each sector as soon as
 // threads index different slots.
 #pragma once
+#include "psib_accum.cuh"
 #include "psib_device.cuh"
 #include "psib_kernels.h"
 
@@ -64,9 +65,16 @@ struct Tally {
     unsigned long long frags = 0, verts = 0, splits = 0;
 };
 
-__device__ __forceinline__ void write_record(const ClipArgs& a, long long gi, long long t, const double* mom,
-                                             unsigned& st)
+// One fragment of image t in voxel lo (global gi) of grid g: a record, or in
+// the atomic mode (central records only) straight into the voxel's sums.
+__device__ __forceinline__ void write_record(const ClipArgs& a, const GridDev& g, long long gi, const int* lo,
+                                             long long t, const double* mom, unsigned& st)
 {
+    if (a.acc.sum) {
+        accumulate_fragment(a, g, a.grids ? (int)a.it.grid[t] : 0, gi, lo, t, mom,
+                            a.acc.factor ? a.acc.factor[t] : 1.0);
+        return;
+    }
     // one atomic per group of lanes that reach this point together: the record
     // counter is a single address that every fragment of the launch hits
     const unsigned act = __activemask();
@@ -291,9 +299,9 @@ __device__ void clip_item(const ClipArgs& a, long long t, Poly<R>* S, QPoly* QL,
                             rec[7] = mom[7] / m0 - u[1] * u[1];
                             rec[8] = mom[8] / m0 - u[1] * u[2];
                             rec[9] = mom[9] / m0 - u[2] * u[2];
-                            write_record(a, gi, t, rec, st);
+                            write_record(a, g, gi, P.lo, t, rec, st);
                         } else {
-                            write_record(a, gi, t, mom, st);
+                            write_record(a, g, gi, P.lo, t, mom, st);
                         }
                     }
                 }

@@ -33,6 +33,38 @@ struct GridDev {
     double w0[3], w1[3], d[3];
 };
 
+// Atomic accumulation of central-form fragments (options deterministic == 0,
+// mixed and FP64-central): instead of writing a record, each fragment adds its
+// mass, first and second moments to per-voxel sums with FP64 atomics (L2), and
+// one pass at the end merges the sums into the fields.  sum holds `stride`
+// doubles per voxel: [0] mass m; [ox + i] m (x_f - c)_i about the voxel's centre
+// c; [ov + i] m (v_f - u)_i about the reference velocity u of the voxel's tile of
+// ACC_TILE^3 voxels; [oxx + k] m (S_xx + dx dx^T) over (xx xy xz yy yz zz);
+// [oxv + 3i + j] m (S_xv + dx dv^T)_ij; [ovv + k] as oxx.  An offset of -1 marks
+// sums not kept.  Taking x about the voxel's centre and v about a reference
+// near the voxel's mean keeps the later E[vv] - E[v]E[v] free of cancellation.
+constexpr int ACC_TILE = 8;
+struct AccArgs {
+    double *sum;              // null: write records
+    int stride, ox, ov, oxx, oxv, ovv;
+    const double *vref;       // 3 per tile
+    const long long *toff;    // batch: first tile of each cutout (null: one grid, tiles from 0)
+    const double *factor;     // correction pass: per image mass factor (null: 1)
+};
+
+// Tile of voxel (i, j, k) of grid g: ACC_TILE^3 voxels, numbered within the grid.
+__host__ __device__ __forceinline__ long long acc_tile(const GridDev &g, int i, int j, int k)
+{
+    const long long ty = (g.n[1] + ACC_TILE - 1) / ACC_TILE, tz = (g.n[2] + ACC_TILE - 1) / ACC_TILE;
+    return ((long long)(i / ACC_TILE) * ty + j / ACC_TILE) * tz + k / ACC_TILE;
+}
+__host__ __device__ __forceinline__ long long acc_tiles(const GridDev &g)
+{
+    long long t = 1;
+    for (int a = 0; a < 3; ++a) t *= (g.n[a] + ACC_TILE - 1) / ACC_TILE;
+    return t;
+}
+
 struct ClipArgs {
     ItemArrays it;
     const int *order;        // queue position -> item (may be null: identity)
@@ -63,6 +95,7 @@ struct ClipArgs {
     long long adj_npart;
     double *adj_gmass;       // dL/dmass per element (accumulated), may be null
     double adj_mass_factor;  // element mass / tet mass
+    AccArgs acc;             // atomic accumulation (acc.sum != null) instead of records
 };
 
 struct MeshDev {
@@ -190,6 +223,28 @@ struct ApplyArgs {
     double *const *fptr;
 };
 cudaError_t launch_apply_records(const ApplyArgs &a, cudaStream_t s);
+
+// The atomic accumulation's sums merged into the fields, voxels [v0, v1) of the
+// call's voxel numbering (fields and batch tables as in ApplyArgs).
+struct FinalArgs {
+    ApplyArgs ap;             // fields (M..VV, nbatch, voff, fptr)
+    AccArgs acc;
+    GridDev g;                // one grid, or
+    const GridDev *grids;     // a batch's grids
+    long long v0, v1;
+};
+cudaError_t launch_acc_finalize(const FinalArgs &a, int num_sms, cudaStream_t s);
+// Reference velocities of the tiles: the mass-weighted mean velocity of the
+// images whose first vertex lies in the tile (0 where none does).  tsum: 4
+// doubles per tile, zeroed by the caller.
+cudaError_t launch_vref(const ItemArrays &it, long long nitems, const GridDev &g, const GridDev *grids,
+                        const AccArgs &acc, double *tsum, long long ntiles, int num_sms, cudaStream_t s);
+// Images whose breadth-first mass correction (scale) differs from 1 by more
+// than tol: appended to list (count in *n), with factor[t] = scale[t] - 1 and
+// their footprint keys gathered into keys.
+cudaError_t launch_correction_select(const ItemArrays &it, const double *scale, long long nitems, double tol,
+                                     int *list, uint16_t *keys, double *factor, unsigned long long *n,
+                                     int num_sms, cudaStream_t s);
 
 // ---- annihilation mode (annihilation.cu; the element stage in tess.cu) ----
 // A tet record: 4 oriented vertices (vertex-major), rho = mass / volume, the

@@ -3,6 +3,9 @@
 // Built with --fmad=false: the element unwrap, the trilinear refinement and
 // the online field update below repeat the reference's double-precision
 // operations in the reference's order.
+#include <algorithm>
+
+#include "psib_accum.cuh"
 #include "psib_device.cuh"
 #include "psib_kernels.h"
 
@@ -875,43 +878,6 @@ cudaError_t launch_vdf_samples(const VdfArgs& a, bool emit, cudaStream_t s)
 
 // ---- fragment records applied to the fields, voxel by voxel ----
 
-// Physical moments of one FP32-kernel fragment from its record (m0, q-centroid,
-// central q second moment): centroid c = x0 + D cq, central moment D C D^T.
-// The x-v moment is brought to the reference's pairing of its cross terms
-// (src/geometry.c:137-146), which equals cov_xv + 2 a b^T - a a^T - b b^T with
-// a = x0 - c_x and b = v0 - c_v.
-__device__ void mixed_fragment(const double* rec, const double* p0, const double (*DX)[3], const double* v0,
-                               const double (*DV)[3], bool x, bool v, bool xx, bool xv, bool vv, double* cm,
-                               double* cv, double (*sxx)[3], double (*sxv)[3], double (*svv)[3])
-{
-    const double* cq = rec + 1;
-    // second moments are only recorded (and only read) when a second-order field is asked for
-    const bool two = xx || xv || vv;
-    const double C[3][3] = {{two ? rec[4] : 0.0, two ? rec[5] : 0.0, two ? rec[6] : 0.0},
-                            {two ? rec[5] : 0.0, two ? rec[7] : 0.0, two ? rec[8] : 0.0},
-                            {two ? rec[6] : 0.0, two ? rec[8] : 0.0, two ? rec[9] : 0.0}};
-    if (x || xx || xv)
-        for (int i = 0; i < 3; ++i) cm[i] = p0[i] + DX[i][0] * cq[0] + DX[i][1] * cq[1] + DX[i][2] * cq[2];
-    if (v || xv || vv)
-        for (int i = 0; i < 3; ++i) cv[i] = v0[i] + DV[i][0] * cq[0] + DV[i][1] * cq[1] + DV[i][2] * cq[2];
-    double TX[3][3], TV[3][3];
-    for (int i = 0; i < 3; ++i)
-        for (int q = 0; q < 3; ++q) {
-            TX[i][q] = (xx || xv) ? DX[i][0] * C[0][q] + DX[i][1] * C[1][q] + DX[i][2] * C[2][q] : 0.0;
-            TV[i][q] = vv ? DV[i][0] * C[0][q] + DV[i][1] * C[1][q] + DV[i][2] * C[2][q] : 0.0;
-        }
-    for (int i = 0; i < 3; ++i)
-        for (int j = 0; j < 3; ++j) {
-            if (xx) sxx[i][j] = TX[i][0] * DX[j][0] + TX[i][1] * DX[j][1] + TX[i][2] * DX[j][2];
-            if (vv) svv[i][j] = TV[i][0] * DV[j][0] + TV[i][1] * DV[j][1] + TV[i][2] * DV[j][2];
-            if (xv) {
-                const double ai = p0[i] - cm[i], aj = p0[j] - cm[j], bi = v0[i] - cv[i], bj = v0[j] - cv[j];
-                sxv[i][j] = TX[i][0] * DV[j][0] + TX[i][1] * DV[j][1] + TX[i][2] * DV[j][2] + 2.0 * ai * bj - ai * aj -
-                            bi * bj;
-            }
-        }
-}
-
 // Sorted records into contiguous arrays: voxel, item, moments.
 __global__ void k_gather_records(GatherArgs a)
 {
@@ -1195,6 +1161,165 @@ cudaError_t launch_apply_records(const ApplyArgs& a, cudaStream_t s)
     } else {
         k_apply_runs<<<(unsigned)((a.nruns + 127) / 128), 128, 0, s>>>(a);
     }
+    return cudaGetLastError();
+}
+
+// ---- the atomic accumulation: reference velocities, mass corrections, finalize ----
+
+__device__ __forceinline__ int cutout_of(const ApplyArgs& a, long long gv)
+{
+    int lo = 0, hi = a.nbatch;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (a.voff[mid] <= (unsigned long long)gv) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// One thread per voxel: the voxel's sums (about its centre and its tile's
+// reference velocity) as one fragment of mass sm, mean xr, vr and central
+// (co)variances, merged once into what the voxel holds -- the update of
+// src/geometry.c:164-186 for one combined fragment, as k_apply_central does.
+__global__ void __launch_bounds__(128) k_acc_finalize(FinalArgs a)
+{
+    const AccArgs& A = a.acc;
+    const bool hx = a.ap.X, hv = a.ap.V, hxx = a.ap.XX, hxv = a.ap.XV, hvv = a.ap.VV;
+    for (long long gv = a.v0 + blockIdx.x * (long long)blockDim.x + threadIdx.x; gv < a.v1;
+         gv += (long long)gridDim.x * blockDim.x) {
+        const double* S = A.sum + gv * A.stride;
+        const double sm = S[0];
+        if (!(sm > 0.0)) continue;
+        const int cut = a.ap.nbatch ? cutout_of(a.ap, gv) : 0;
+        const Fields F = fields_of(a.ap, gv);
+        const long long gi = F.gi;
+        const GridDev& g = a.grids ? a.grids[cut] : a.g;
+        const long long nyz = (long long)g.n[1] * g.n[2];
+        const int ix[3] = {(int)(gi / nyz), (int)((gi / g.n[2]) % g.n[1]), (int)(gi % g.n[2])};
+        double xr[3], vr[3], dxr[3] = {0.0, 0.0, 0.0}, dvr[3] = {0.0, 0.0, 0.0};
+        if (A.ox >= 0)
+            for (int i = 0; i < 3; ++i) {
+                dxr[i] = S[A.ox + i] / sm;
+                xr[i] = (g.w0[i] + g.d[i] * ((double)ix[i] + 0.5)) + dxr[i];
+            }
+        if (A.ov >= 0) {
+            const long long tile = (A.toff ? A.toff[cut] : 0ll) + acc_tile(g, ix[0], ix[1], ix[2]);
+            for (int i = 0; i < 3; ++i) {
+                dvr[i] = S[A.ov + i] / sm;
+                vr[i] = A.vref[3 * tile + i] + dvr[i];
+            }
+        }
+        const double M0 = F.M[gi], Mf = M0 + sm;
+        const double cw = sm / Mf, dw = M0 / Mf;
+        double X0[3] = {0, 0, 0}, V0[3] = {0, 0, 0};
+        for (int i = 0; i < 3; ++i) {
+            if (hx || hxx || hxv) X0[i] = hx ? F.X[3 * gi + i] : 0.0;
+            if (hv || hvv || hxv) V0[i] = hv ? F.V[3 * gi + i] : 0.0;
+        }
+        if (hxx) {
+            int k = 0;
+            double C[3][3];
+            for (int i = 0; i < 3; ++i)
+                for (int j = i; j < 3; ++j, ++k) C[i][j] = C[j][i] = S[A.oxx + k] / sm - dxr[i] * dxr[j];
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) {
+                    double* t = &F.XX[9 * gi + 3 * i + j];
+                    *t = dw * *t + cw * C[i][j] + cw * dw * (xr[i] - X0[i]) * (xr[j] - X0[j]);
+                }
+        }
+        if (hvv) {
+            int k = 0;
+            double C[3][3];
+            for (int i = 0; i < 3; ++i)
+                for (int j = i; j < 3; ++j, ++k) C[i][j] = C[j][i] = S[A.ovv + k] / sm - dvr[i] * dvr[j];
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) {
+                    double* t = &F.VV[9 * gi + 3 * i + j];
+                    *t = dw * *t + cw * C[i][j] + cw * dw * (vr[i] - V0[i]) * (vr[j] - V0[j]);
+                }
+        }
+        if (hxv)
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) {
+                    const double C = S[A.oxv + 3 * i + j] / sm - dxr[i] * dvr[j];
+                    double* t = &F.XV[9 * gi + 3 * i + j];
+                    *t = dw * *t + cw * C + cw * dw * (xr[i] - X0[i]) * (vr[j] - V0[j]);
+                }
+        if (hx)
+            for (int i = 0; i < 3; ++i) F.X[3 * gi + i] = X0[i] + cw * (xr[i] - X0[i]);
+        if (hv)
+            for (int i = 0; i < 3; ++i) F.V[3 * gi + i] = V0[i] + cw * (vr[i] - V0[i]);
+        F.M[gi] = Mf;
+    }
+}
+
+cudaError_t launch_acc_finalize(const FinalArgs& a, int num_sms, cudaStream_t s)
+{
+    if (a.v1 <= a.v0) return cudaSuccess;
+    const long long blocks = std::min<long long>((a.v1 - a.v0 + 127) / 128, (long long)num_sms * 16);
+    k_acc_finalize<<<(unsigned)blocks, 128, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+// Mass and momentum of the images whose first vertex lies in each tile.
+__global__ void k_vref_accum(ItemArrays it, long long n, GridDev g0, const GridDev* grids, const long long* toff,
+                             double* tsum)
+{
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int cut = grids ? (int)it.grid[t] : 0;
+        const GridDev& g = grids ? grids[cut] : g0;
+        const double* fr = it.frame + t * FRAME;
+        int ix[3];
+        for (int a = 0; a < 3; ++a) {
+            double f = floor((fr[a] - g.w0[a]) / g.d[a]);
+            if (!(f >= 0.0)) f = 0.0;
+            ix[a] = f < (double)g.n[a] ? (int)f : g.n[a] - 1;
+        }
+        const long long tile = (toff ? toff[cut] : 0ll) + acc_tile(g, ix[0], ix[1], ix[2]);
+        const double m = fr[FR_MASS];
+        atomicAdd(&tsum[4 * tile], m);
+        for (int a = 0; a < 3; ++a)
+            atomicAdd(&tsum[4 * tile + 1 + a],
+                      m * 0.25 * (fr[FR_U + a] + fr[FR_U + 3 + a] + fr[FR_U + 6 + a] + fr[FR_U + 9 + a]));
+    }
+}
+
+__global__ void k_vref_fix(const double* tsum, long long ntiles, double* vref)
+{
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < ntiles; k += (long long)gridDim.x * blockDim.x)
+        for (int a = 0; a < 3; ++a) vref[3 * k + a] = tsum[4 * k] > 0.0 ? tsum[4 * k + 1 + a] / tsum[4 * k] : 0.0;
+}
+
+cudaError_t launch_vref(const ItemArrays& it, long long nitems, const GridDev& g, const GridDev* grids,
+                        const AccArgs& acc, double* tsum, long long ntiles, int num_sms, cudaStream_t s)
+{
+    if (nitems > 0) k_vref_accum<<<num_sms * 8, 256, 0, s>>>(it, nitems, g, grids, acc.toff, tsum);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_vref_fix<<<num_sms * 4, 256, 0, s>>>(tsum, ntiles, (double*)acc.vref);
+    return cudaGetLastError();
+}
+
+__global__ void k_correction_select(ItemArrays it, const double* scale, long long n, double tol, int* list,
+                                    uint16_t* keys, double* factor, unsigned long long* count)
+{
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const double sc = scale[t];
+        if (sc > 0.0 && fabs(sc - 1.0) > tol) {
+            const unsigned long long i = atomicAdd(count, 1ull);
+            list[i] = (int)t;
+            keys[i] = it.key[t];
+            factor[t] = sc - 1.0;
+        }
+    }
+}
+
+cudaError_t launch_correction_select(const ItemArrays& it, const double* scale, long long nitems, double tol,
+                                     int* list, uint16_t* keys, double* factor, unsigned long long* n, int num_sms,
+                                     cudaStream_t s)
+{
+    if (nitems <= 0) return cudaSuccess;
+    k_correction_select<<<num_sms * 8, 256, 0, s>>>(it, scale, nitems, tol, list, keys, factor, n);
     return cudaGetLastError();
 }
 

@@ -101,26 +101,49 @@ def test_deterministic_is_bitwise_reference(gpu, oracle, name):
         assert np.array_equal(out[f], ref[f]), (name, f, np.abs(out[f] - ref[f]).max())
 
 
+@pytest.mark.parametrize("det", [False, True], ids=["atomic", "sorted"])
 @pytest.mark.parametrize("name", NAMES)
-def test_mixed_within_1e5(gpu, oracle, name):
+def test_mixed_within_1e5(gpu, oracle, name, det):
+    """Mixed precision in both accumulation modes: per-voxel FP64 atomic sums
+    (the default) and sorted records applied in order (deterministic=True)."""
     ref, _ = reference(oracle, name)
     c = make(name)
-    out, _, _ = run_psi(gpu, c, precision="mixed")
+    out, _, _ = run_psi(gpu, c, precision="mixed", deterministic=det)
+    assert gpu.last_stats()["accumulation"] == (0 if det else 1)
     check_vs_exact_and_reference(out, ref, exact(oracle, name), MIXED_TOL, name)
     if name in FULL_BOX:
         assert mass_error(out["m"], total_mass(c)) <= MASS_TOL
 
 
+@pytest.mark.parametrize("det", [False, True], ids=["atomic", "sorted"])
 @pytest.mark.parametrize("name", NAMES)
-def test_fp64_central_near_exact(gpu, oracle, name):
+def test_fp64_central_near_exact(gpu, oracle, name, det):
     """The FP64 walk with central moments: FP64 accuracy where the reference's
-    raw moments lose it."""
+    raw moments lose it, in both accumulation modes."""
     ref, _ = reference(oracle, name)
     c = make(name)
-    out, _, _ = run_psi(gpu, c, precision="fp64-central")
+    out, _, _ = run_psi(gpu, c, precision="fp64-central", deterministic=det)
     check_vs_exact_and_reference(out, ref, exact(oracle, name), 1e-9, name)
     if name in FULL_BOX:
         assert mass_error(out["m"], total_mass(c)) <= MASS_TOL
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_atomic_sums_equal_sorted_records(gpu, name):
+    """The atomic mode adds the same fragments as the sorted mode, about the
+    voxel's centre and a tile velocity instead of the run's first fragment:
+    the two agree to rounding (1e-12 in the voxel-scale norm), and the FP64
+    path ignores the flag (always the reference's order)."""
+    c = make(name)
+    a, _, _ = run_psi(gpu, c, precision="mixed", deterministic=False)
+    b, _, _ = run_psi(gpu, c, precision="mixed", deterministic=True)
+    errs = field_errors(a, b)
+    assert errs["m"]["rel"] <= 1e-12 and errs["dead_m"] == 0.0, (name, errs["m"])
+    for f, e in errs.items():
+        if f != "dead_m":
+            assert e["norm"] <= 1e-12, (name, f, e)
+    run_psi(gpu, c, precision="fp64", deterministic=False)
+    assert gpu.last_stats()["accumulation"] == 0
 
 
 @pytest.mark.parametrize("gname", sorted(load_golden()))
