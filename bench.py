@@ -10,10 +10,12 @@ the FP64 kernel is timed beside it and the mixed result is checked against it.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Under torchrun every rank deposits its own lattice (seed + rank) on its own
-GPU (weak scaling, no collective on the data path); the step time is the max
-over ranks of CUDA-event time.  `--impl reference` times the reference's own C
-implementation (oracle/_ref, compiled from its sources) on all host cores.
+Under torchrun the ranks share out the one lattice by element slabs (strong
+scaling): each deposits its slab into a full grid and one exchange combines
+the grids (pypsi_b200.parallel); the step time is the max over ranks of
+CUDA-event time.  `--impl reference` times the reference's own C
+implementation (oracle/_ref, compiled from its sources) on all host cores over
+the whole workload.
 """
 from __future__ import annotations
 
@@ -136,12 +138,16 @@ class Clocks:
 
 
 # ---------------------------------------------------------------- reference arm
-def arm_config(n_part=N_PART, n_grid=N_GRID):
+def arm_config(n_part=N_PART, n_grid=N_GRID, world=1):
     """The workload's config, printed identically by both arms."""
+    per = ("one GPU deposits the whole lattice (seed 1234)" if world == 1 else
+           f"one lattice (seed 1234) over {world} GPUs: rank r deposits element slab r into a full grid, then one "
+           f"exchange (FP32 all-reduce of reference means, reduce-scatter of 34 FP64 sums per voxel over x-slabs, "
+           f"all-gather)")
     return {"workload": WORKLOAD if (n_part, n_grid) == (N_PART, N_GRID) else
             f"{n_part}^3 particles -> {n_grid}^3 grid, Zel'dovich rms 2 cells, fields m,x,v,xx,xv,vv",
             "l2": "inputs larger than L2 (4.6 GB of grid fields, 3 GB of tet images per step)",
-            "per_rank": "each rank deposits its own lattice (seed 1234+rank) on its own GPU"}
+            "per_rank": per}
 
 
 def slab_window(slab, nslabs, n_grid=N_GRID):
@@ -258,7 +264,7 @@ def run_reference(args):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "tets/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * secs / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": DATA,
-            "config": arm_config(),
+            "config": arm_config(world=world),
             "precision": "fp64 (the reference's own C code)",
             "cpu_baseline": {"value": value, "unit": "tets/s", "cores": cores,
                              "kind": "reference" if kind == "reference" else "port",
@@ -918,10 +924,13 @@ def run_ours(args):
     from pypsi_b200.synth import zeldovich
 
     n_part, n_grid = args.n_part, args.n_grid
+    # one GPU: the whole mesh.  Several: one mesh shared out by element slabs (strong scaling),
+    # every rank depositing its slab and one exchange combining the grids
+    sharded = world > 1
     tets_per_step = 6 * n_part ** 3
     fp64_peak = capi.measure_fma_peak("fp64")
     fp32_peak = capi.measure_fma_peak("fp32")
-    pos, vel = zeldovich(n_part, RMS, 1234 + rank)
+    pos, vel = zeldovich(n_part, RMS, 1234)
     dev = torch.device("cuda", local)
     dpos = torch.from_numpy(pos.reshape(-1, 3)).to(dev)
     dvel = torch.from_numpy(vel.reshape(-1, 3)).to(dev)
@@ -933,10 +942,23 @@ def run_ours(args):
         return {f: torch.zeros(s, dtype=torch.float64, device=dev) for f, s in shapes.items()}
 
     stream = torch.cuda.current_stream()
+    if sharded:
+        from pypsi_b200.parallel import block_slab_connectivity, element_slab, merge_fields
+
+        e0, e1 = element_slab(n_part ** 3, world, rank)
+        slab_conn = block_slab_connectivity((n_part,) * 3, True, e0, e1, device=dev)
 
     def step(fields, prec, n=(n_grid,) * 3, bounds=BOX):
-        return capi.voxels_device(fields, n, bounds, dpos, dvel, block_dims=(n_part,) * 3,
-                                  periodic_box=BOX, precision=prec, stream=stream)
+        if not sharded:
+            return capi.voxels_device(fields, n, bounds, dpos, dvel, block_dims=(n_part,) * 3,
+                                      periodic_box=BOX, precision=prec, stream=stream)
+        # voxels_sharded's steps, keeping the library's stats of this rank's slab
+        for t in fields.values():
+            t.zero_()
+        st = capi.voxels_device(fields, n, bounds, dpos, dvel, connectivity=slab_conn, periodic_box=BOX,
+                                precision=prec, stream=stream)
+        merge_fields(fields)
+        return st
 
     def barrier():
         if dist:
@@ -980,7 +1002,7 @@ def run_ours(args):
     # for the exact result: the reference-order FP64 result carries its own
     # rounding in voxels of tiny fragments.
     errs, errs_x, errs_rx, merr, within = {}, {}, {}, {}, None
-    if args.precision == "both":
+    if args.precision == "both" and not sharded:
         outs = {}
         for prec in ("fp64", "mixed", "fp64-central"):
             f = fresh()
@@ -1000,7 +1022,44 @@ def run_ours(args):
 
     # end to end through the drop-in module: host numpy in, host numpy out
     e2e = None
-    if not args.no_e2e:
+    if not args.no_e2e and sharded:
+        # several GPUs: parallel.voxels_sharded, every step copying the mesh in from pinned host
+        # memory and rank 0 copying the merged fields back
+        from pypsi_b200.parallel import voxels_sharded
+
+        hpos = torch.from_numpy(pos.reshape(-1, 3)).pin_memory()
+        hvel = torch.from_numpy(vel.reshape(-1, 3)).pin_memory()
+        f = fresh()
+        hout = {k: torch.empty(v.shape, dtype=v.dtype).pin_memory() for k, v in f.items()} if rank == 0 else {}
+
+        def e2e_step():
+            xp = hpos.to(dev, non_blocking=True)
+            xv = hvel.to(dev, non_blocking=True)
+            for t in f.values():
+                t.zero_()
+            voxels_sharded(f, (n_grid,) * 3, BOX, xp, xv, block_dims=(n_part,) * 3, periodic_box=BOX,
+                           precision=head)
+            for k, t in hout.items():
+                t.copy_(f[k], non_blocking=True)
+            torch.cuda.synchronize()
+
+        e2e_step()
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            e2e_step()
+        barrier()
+        e2e_s = (time.perf_counter() - t0) / args.e2e_steps
+        t = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+        field_bytes = sum(v.nbytes for v in f.values())
+        e2e = {"value": tets_per_step / e2e_s, "unit": "tets/s", "h2d_bytes_per_step": pos.nbytes + vel.nbytes,
+               "d2h_bytes_per_step": field_bytes, "api": f"pypsi_b200.parallel.voxels_sharded(..., precision="
+               f"'{head}') over {world} GPUs, mesh from pinned host memory, rank 0 reads the fields back",
+               "ms_per_step": e2e_s * 1e3}
+        del f, hout
+    elif not args.no_e2e:
         mesh = PSI.Mesh(loader="block", pos=pos, vel=vel, periodic_box=BOX)
         grid = PSI.Grid(n=(n_grid,) * 3, bounds=BOX, fields=FIELDS)
         PSI.voxels(grid=grid, mesh=mesh, precision=head)
@@ -1023,7 +1082,7 @@ def run_ours(args):
     # forward + backward of a density loss against forward alone (FP64 forward,
     # adjoint kernel backward) at this workload's sizes and at 64^3 -> 128^3
     adjoint = None
-    if not args.no_adjoint:
+    if not args.no_adjoint and not sharded:
         adjoint = {"forward": "FP64 m field (deposit_density)", "loss": "sum((m/dV - rho_target)^2)",
                    "backward": "psib_voxels_adjoint through torch.autograd (dL/dpos)"}
         sizes = [(n_part, n_grid, RMS, dpos)]
@@ -1065,16 +1124,17 @@ def run_ours(args):
         peaks = {}
     hbm_peak = peaks.get("hbm_gbs") or 6650.0
     walk_gbs = s["walk_bytes"] / (clip_ms * 1e-3) / 1e9
-    value = world * tets_per_step / (ms_mixed * 1e-3)
+    value = (1 if sharded else world) * tets_per_step / (ms_mixed * 1e-3)
     traffic = clip_traffic_bytes(frags)
     line = {
         "metric": METRIC, "value": value, "unit": "tets/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": ms_mixed, "higher_is_better": True,
+        "scaling": "strong" if sharded else "weak",
         "vs_baseline": None, "dtype": "f64" if head == "fp64" else "f32+f64", "data": DATA,
-        "config": arm_config(n_part, n_grid),
+        "config": arm_config(n_part, n_grid, world),
         "precision": "fp64 (reference operation order)" if head == "fp64" else
                      "mixed (FP32 clip, FP64 moments/accumulation)",
-        "voxel_clips_per_s": world * frags / (ms_mixed * 1e-3),
+        "voxel_clips_per_s": (1 if sharded else world) * frags / (ms_mixed * 1e-3),
         "mixed_vs_fp64_err": {f: e["norm"] for f, e in errs.items() if f != "dead_m"} if errs else None,
         "mixed_vs_fp64_err_m_rel": errs["m"]["rel"] if errs else None,
         "mixed_vs_fp64central_err": {f: e["norm"] for f, e in errs_x.items() if f != "dead_m"} if errs_x else None,
@@ -1124,7 +1184,8 @@ def run_ours(args):
         line["parity_vs_reference"] = parity_on_slab(ref_slab, deposit)
         capi.lib.psib_release_device_memory()
     # the comparison the metric names, last so that the tail of the line shows it
-    line["fp64"] = {"value": world * tets_per_step / (ms_fp64 * 1e-3), "unit": "tets/s", "ms_per_step": ms_fp64}
+    line["fp64"] = {"value": (1 if sharded else world) * tets_per_step / (ms_fp64 * 1e-3), "unit": "tets/s",
+                    "ms_per_step": ms_fp64}
     line["mixed_over_fp64"] = ms_fp64 / ms_mixed
     line["fwd_bwd_over_fwd"] = adjoint[f"{n_part}^3->{n_grid}^3 rms {RMS:g}"]["ratio"] if adjoint else None
     print(json.dumps(line), flush=True)

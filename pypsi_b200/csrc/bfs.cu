@@ -611,7 +611,6 @@ __global__ void __launch_bounds__(BB, 3) k_bfs_leaf(BfsArgs a)
                             // atomic mode: straight into the voxel's sums, no record
                             const double f = c.acc.factor ? c.acc.factor[t] : 1.0;
                             accumulate_fragment(c, g, c.grids ? (int)c.it.grid[t] : 0, gi, lo, t, rec, f);
-                            moved += 8ull * c.acc.stride;
                         } else {
                             has = true;
                         }

@@ -119,7 +119,7 @@ struct Ctx {
     DevBuf qx[3], qnb[3], qnv[3], qwin[3], qbox[3], qitem[3], hist, bfs_cnt, dfs_list, vsum;
     DevBuf btab, igrid; // batch tables, image -> cutout
     // atomic accumulation: per-voxel sums, tile reference velocities, the mass-correction pass
-    DevBuf acc_sum, acc_tsum, acc_vref, acc_toff, fix_list, fix_keys, fix_list_s, fix_keys_s, ifactor;
+    DevBuf acc_sum, acc_ref, acc_tsum, acc_vref, acc_toff, fix_list, fix_keys, fix_list_s, fix_keys_s, ifactor;
     DevBuf passes;      // breadth-first pass table
     // annihilation: element tets and boxes, cell registrations, element and tet pairs
     DevBuf a_cnt, a_off, a_ebox, a_tets_a, a_tets_b, a_stats, a_reg_cnt, a_reg_off, a_reg_key, a_reg_elem,
@@ -142,7 +142,7 @@ struct Ctx {
                 &a_reg_cnt, &a_reg_off, &a_reg_key, &a_reg_elem, &a_reg_key_s, &a_reg_elem_s, &a_run_key,
                 &a_run_cnt, &a_run_off, &a_run_lo, &a_run_hi, &a_pair_cnt, &a_pair_off, &a_pair_key,
                 &a_pair_key_s, &a_na, &a_aoff, &a_tp_cnt, &a_tp_excl, &a_bounds, &a_tpairs, &a_deep, &a_tp_key,
-                &a_tp_key_s, &a_ord_in, &a_ord, &q_in, &q_cnt, &acc_sum, &acc_tsum, &acc_vref, &acc_toff,
+                &a_tp_key_s, &a_ord_in, &a_ord, &q_in, &q_cnt, &acc_sum, &acc_ref, &acc_tsum, &acc_vref, &acc_toff,
                 &fix_list, &fix_keys, &fix_list_s, &fix_keys_s, &ifactor,
                 &q_off, &q_key, &q_key_s, &q_out, &s_cnt, &s_off, &s_offs, &s_rho, &s_vel};
     }
@@ -194,7 +194,7 @@ __global__ void k_count_deep(const uint16_t* key, long long n, unsigned long lon
 {
     unsigned long long c = 0;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        c += (key[i] == 0xFFFF);
+        c += (key[i] == KEY_DEEP);
     c = __reduce_add_sync(0xFFFFFFFFu, (unsigned)c);
     if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, c);
 }
@@ -315,7 +315,7 @@ int bfs_clip(Ctx& C, ClipArgs& ca, long long nmain, long long nitems, unsigned l
     long long cur = 0, pos = 0;
     for (int k = 0; k < 0xFFFF; ++k) {
         long long cnt = hist[k];
-        const long long vol = std::max(1, 0xFFFE - k);
+        const long long vol = key_volume((unsigned)k);
         while (cnt > 0) {
             const long long take = std::min(cnt, (cap - cur) / vol);
             if (take == 0) {
@@ -336,7 +336,7 @@ int bfs_clip(Ctx& C, ClipArgs& ca, long long nmain, long long nitems, unsigned l
         size_t p = 0;
         long long acc = 0, at = 0;
         for (int k = 0; k < 0xFFFF && p + 1 < qb.size(); ++k) {
-            const long long vol = std::max(1, 0xFFFE - k);
+            const long long vol = key_volume((unsigned)k);
             for (long long cnt = hist[k]; cnt > 0;) {
                 const long long take = std::min(cnt, qb[p + 1] - at);
                 acc += take * vol;
@@ -786,6 +786,9 @@ int run_device(Call& c)
         if (flags & F_VV) { ovv = stride; stride += 6; }
         RET(ensure(C.acc_sum, (size_t)nvox * stride * sizeof(double)));
         CK(cudaMemsetAsync(C.acc_sum.p, 0, (size_t)nvox * stride * sizeof(double), st));
+        // the voxels' reference points (position, velocity), claimed by their first fragments
+        RET(ensure(C.acc_ref, (size_t)nvox * 2 * sizeof(unsigned long long)));
+        CK(cudaMemsetAsync(C.acc_ref.p, 0, (size_t)nvox * 2 * sizeof(unsigned long long), st));
         const long long* d_toff = nullptr;
         if (batch) {
             std::vector<long long> toff(c.nbatch + 1, 0);
@@ -802,7 +805,7 @@ int run_device(Call& c)
         RET(ensure(C.acc_tsum, (size_t)ntiles * 4 * sizeof(double)));
         RET(ensure(C.acc_vref, (size_t)ntiles * 3 * sizeof(double)));
         ca.acc = AccArgs{C.acc_sum.as<double>(), stride, ox, ov, oxx, oxv, ovv, C.acc_vref.as<double>(), d_toff,
-                         nullptr};
+                         nullptr, C.acc_ref.as<unsigned long long>(), C.acc_ref.as<unsigned long long>() + nvox};
     }
 
     float ms_clip = 0.f, ms_tess = 0.f, ms_final = 0.f;
@@ -897,10 +900,6 @@ int run_device(Call& c)
                 ca.scratch = C.scratch.p;
                 RET(bfs_clip(C, ca, nmain, nitems, sm, clip_grid, clip_block, c.queue_voxels, batch, st, launches,
                              klaunch, C.key_sorted.as<uint16_t>()));
-                long long ncorr = 0;
-                RET(correct_masses(C, ca, nitems, sm, clip_grid, clip_block, c.queue_voxels, st, launches, klaunch,
-                                   ncorr));
-                corrected += ncorr;
             } else if (nmain > 0) {
                 ca.scratch = C.scratch.p;
                 ca.order_base = 0;
@@ -918,6 +917,13 @@ int run_device(Call& c)
                 ca.head = &sm[S_HEAD + 1];
                 CK(launch_clip_mixed(ca, true, !mixed, big_grid, big_block, st));
                 launches++;
+            }
+            if (nmain > 0 && use_bfs) {
+                // every image's scale is set now (the deep-tree kernel sets its own to 1)
+                long long ncorr = 0;
+                RET(correct_masses(C, ca, nitems, sm, clip_grid, clip_block, c.queue_voxels, st, launches, klaunch,
+                                   ncorr));
+                corrected += ncorr;
             }
             CK(cudaEventRecord(C.ev[5], st));
             unsigned long long h[S_WORDS];

@@ -5,7 +5,7 @@
 // moment C as xx xy xz yy yz zz).  Through the tet image's frame it becomes the
 // fragment's mass, position and velocity centroids and its central second
 // moments in x and v (src/geometry.c:81-161).  The per-voxel sums about the
-// voxel's centre and its tile's reference velocity are merged into the grid
+// voxel's reference points (claimed by its first fragment) are merged into the grid
 // fields by the finalize kernel (tess.cu), as the reference's online update
 // (src/geometry.c:164-186) merges one combined fragment.
 #pragma once
@@ -51,9 +51,58 @@ __device__ __forceinline__ void mixed_fragment(const double* rec, const double* 
         }
 }
 
+// Reference points of a voxel, claimed by its first fragment.  A reference
+// need not be exact, only near the voxel's means, and the same for every
+// fragment of the voxel and for the finalize pass; so it is packed into one
+// 64-bit word (top bit set: claimed) that a single atomicCAS publishes:
+//   position: 3 x 21-bit fixed point, the offset from the voxel's centre in
+//             units of d / 2^19 (the centroid lies within half a voxel);
+//   velocity: 3 x 21-bit truncated floats (sign, exponent, 12 mantissa bits) of
+//             the offset from the tile's reference velocity.
+constexpr unsigned long long REF_SET = 1ull << 63;
+constexpr double REF_QX = 524288.0; // 2^19 steps per voxel
+
+__device__ __forceinline__ unsigned long long pack_xref(const double* c, const double* cen, const double* d)
+{
+    unsigned long long w = REF_SET;
+    for (int i = 0; i < 3; ++i) {
+        double q = rint((c[i] - cen[i]) / d[i] * REF_QX);
+        q = fmin(fmax(q, -1048575.0), 1048575.0);
+        w |= (unsigned long long)((long long)q + 1048576) << (42 - 21 * i);
+    }
+    return w;
+}
+__device__ __forceinline__ void unpack_xref(unsigned long long w, const double* cen, const double* d, double* r)
+{
+    for (int i = 0; i < 3; ++i)
+        r[i] = cen[i] + (double)((long long)((w >> (42 - 21 * i)) & 0x1FFFFFull) - 1048576) * (d[i] / REF_QX);
+}
+__device__ __forceinline__ unsigned long long pack_vref(const double* off)
+{
+    unsigned long long w = REF_SET;
+    for (int i = 0; i < 3; ++i) {
+        const float f = isfinite(off[i]) ? (float)off[i] : 0.0f;
+        w |= (unsigned long long)(__float_as_uint(f) >> 11) << (42 - 21 * i);
+    }
+    return w;
+}
+__device__ __forceinline__ void unpack_vref(unsigned long long w, const double* u, double* r)
+{
+    for (int i = 0; i < 3; ++i)
+        r[i] = u[i] + (double)__uint_as_float((unsigned)((w >> (42 - 21 * i)) & 0x1FFFFFull) << 11);
+}
+// The word at *slot, claimed with `mine` if it is still 0.
+__device__ __forceinline__ unsigned long long claim_ref(unsigned long long* slot, unsigned long long mine)
+{
+    const unsigned long long w = *(volatile unsigned long long*)slot;
+    if (w) return w;
+    const unsigned long long old = atomicCAS(slot, 0ull, mine);
+    return old ? old : mine;
+}
+
 // Add fragment rec of image t, lying in voxel lo of grid g (global voxel gi,
 // cutout `cut` of a batch, else 0), to the atomic sums, its mass scaled by
-// `factor`.  x is taken about the voxel's centre, v about the tile's reference.
+// `factor`.  x and v are taken about the voxel's reference points.
 // Inlined into the leaf and clip kernels, whose register budgets are capped by
 // their launch bounds.
 __device__ __forceinline__ void accumulate_fragment(const ClipArgs& a, const GridDev& g, int cut, long long gi,
@@ -78,15 +127,23 @@ __device__ __forceinline__ void accumulate_fragment(const ClipArgs& a, const Gri
     double cm[3] = {0.0, 0.0, 0.0}, cv[3] = {0.0, 0.0, 0.0}, sxx[3][3], sxv[3][3], svv[3][3];
     mixed_fragment(rec, p0, DX, v0, DV, hx, hv, hxx, hxv, hvv, cm, cv, sxx, sxv, svv);
     double dx[3] = {0.0, 0.0, 0.0}, dv[3] = {0.0, 0.0, 0.0};
-    if (hx)
+    if (hx) {
+        double cen[3], r[3];
+        for (int i = 0; i < 3; ++i) cen[i] = g.w0[i] + g.d[i] * ((double)lo[i] + 0.5);
+        unpack_xref(claim_ref(A.rx + gi, pack_xref(cm, cen, g.d)), cen, g.d, r);
         for (int i = 0; i < 3; ++i) {
-            dx[i] = cm[i] - (g.w0[i] + g.d[i] * ((double)lo[i] + 0.5));
+            dx[i] = cm[i] - r[i];
             atomicAdd(S + A.ox + i, m * dx[i]);
         }
+    }
     if (hv) {
         const long long tile = (A.toff ? A.toff[cut] : 0ll) + acc_tile(g, lo[0], lo[1], lo[2]);
+        const double* u = A.vref + 3 * tile;
+        const double off[3] = {cv[0] - u[0], cv[1] - u[1], cv[2] - u[2]};
+        double r[3];
+        unpack_vref(claim_ref(A.rv + gi, pack_vref(off)), u, r);
         for (int i = 0; i < 3; ++i) {
-            dv[i] = cv[i] - A.vref[3 * tile + i];
+            dv[i] = cv[i] - r[i];
             atomicAdd(S + A.ov + i, m * dv[i]);
         }
     }

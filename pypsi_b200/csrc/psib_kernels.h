@@ -33,6 +33,22 @@ struct GridDev {
     double w0[3], w1[3], d[3];
 };
 
+// Footprint key of a tet image (ItemArrays.key), sorted ascending to order the
+// clip's work: KEY_DEEP for the deep-tree kernel, else the index-box volume
+// (1..256: a box the main walk takes has a bisection at most 8 deep) in the
+// high bits, larger boxes first, and in the low KEY_CELL_BITS a coarse cell of
+// the grid (8 x 4 x 4 cells) holding the box's low corner, so that images of
+// one volume are walked in spatial order and their fragments' atomic sums stay
+// in L2.
+constexpr unsigned KEY_DEEP = 0xFFFFu;
+constexpr int KEY_CELL_BITS = 7;
+__host__ __device__ __forceinline__ long long key_volume(unsigned k)
+{
+    if (k >= KEY_DEEP) return 1ll << 40;
+    const long long v = 256 - (long long)(k >> KEY_CELL_BITS);
+    return v > 0 ? v : 1;
+}
+
 // Atomic accumulation of central-form fragments (options deterministic == 0,
 // mixed and FP64-central): instead of writing a record, each fragment adds its
 // mass, first and second moments to per-voxel sums with FP64 atomics (L2), and
@@ -41,8 +57,12 @@ struct GridDev {
 // c; [ov + i] m (v_f - u)_i about the reference velocity u of the voxel's tile of
 // ACC_TILE^3 voxels; [oxx + k] m (S_xx + dx dx^T) over (xx xy xz yy yz zz);
 // [oxv + 3i + j] m (S_xv + dx dv^T)_ij; [ovv + k] as oxx.  An offset of -1 marks
-// sums not kept.  Taking x about the voxel's centre and v about a reference
-// near the voxel's mean keeps the later E[vv] - E[v]E[v] free of cancellation.
+// sums not kept.  dx and dv are taken about reference points of the voxel that
+// lie close to its means -- the centroids of the first fragment that reaches
+// the voxel, which claims them with one 64-bit compare-and-swap (rx, rv; see
+// psib_accum.cuh) -- so that the later E[xx] - E[x]E[x] (and vv, xv) does not
+// cancel even in voxels made of tiny fragments.  The velocity reference is
+// stored relative to the mean velocity of the voxel's tile of ACC_TILE^3 voxels.
 constexpr int ACC_TILE = 8;
 struct AccArgs {
     double *sum;              // null: write records
@@ -50,6 +70,8 @@ struct AccArgs {
     const double *vref;       // 3 per tile
     const long long *toff;    // batch: first tile of each cutout (null: one grid, tiles from 0)
     const double *factor;     // correction pass: per image mass factor (null: 1)
+    unsigned long long *rx;   // per voxel: packed position reference (0: not yet claimed)
+    unsigned long long *rv;   // per voxel: packed velocity reference (0: not yet claimed)
 };
 
 // Tile of voxel (i, j, k) of grid g: ACC_TILE^3 voxels, numbered within the grid.

@@ -147,13 +147,14 @@ __device__ unsigned tet_images(const double (*p)[3], const MeshDev& m, const Gri
 }
 
 // Ordering key of an image from its voxel index box (src/geometry.c:838-841):
-// 0xFFFF for images the deep-tree kernel takes -- bisection trees deeper than
-// the main kernel serves (DMAX_MAIN), or boxes longer than SPAN_MAX voxels on
-// an axis, where FP32 coordinates would lose too much precision inside a voxel
-// -- otherwise larger boxes first.
+// KEY_DEEP for images the deep-tree kernel takes -- bisection trees deeper
+// than the main kernel serves (DMAX_MAIN), or boxes longer than SPAN_MAX voxels
+// on an axis, where FP32 coordinates would lose too much precision inside a
+// voxel -- otherwise larger boxes first, then by coarse cell (psib_kernels.h).
 __device__ uint16_t footprint_key(const double (*rb)[3], const GridDev& g)
 {
-    int depth = 0, span = 0;
+    int depth = 0, span = 0, cell = 0;
+    const int cbits[3] = {3, 2, 2};
     long long vol = 1;
     for (int i = 0; i < 3; ++i) {
         double cmin = rb[0][i], cmax = rb[1][i];
@@ -167,9 +168,11 @@ __device__ uint16_t footprint_key(const double (*rb)[3], const GridDev& g)
         if (sz > 1) depth += 32 - __clz(sz - 1);
         if (sz > span) span = sz;
         if (vol < 0xFFFF) vol *= (sz > 1 ? sz : 1);
+        const int ci = g.n[i] > 0 ? (int)(((long long)lo << cbits[i]) / g.n[i]) : 0;
+        cell = (cell << cbits[i]) | (ci < (1 << cbits[i]) ? ci : (1 << cbits[i]) - 1);
     }
-    if (depth > DMAX_MAIN || span > SPAN_MAX) return 0xFFFF;
-    return (uint16_t)(0xFFFE - (vol < 0xFFFE ? vol : 0xFFFE));
+    if (depth > DMAX_MAIN || span > SPAN_MAX) return (uint16_t)KEY_DEEP;
+    return (uint16_t)(((256 - vol) << KEY_CELL_BITS) | cell);
 }
 
 struct Emitter {
@@ -1197,16 +1200,22 @@ __global__ void __launch_bounds__(128) k_acc_finalize(FinalArgs a)
         const long long nyz = (long long)g.n[1] * g.n[2];
         const int ix[3] = {(int)(gi / nyz), (int)((gi / g.n[2]) % g.n[1]), (int)(gi % g.n[2])};
         double xr[3], vr[3], dxr[3] = {0.0, 0.0, 0.0}, dvr[3] = {0.0, 0.0, 0.0};
-        if (A.ox >= 0)
+        if (A.ox >= 0) {
+            double cen[3], r[3];
+            for (int i = 0; i < 3; ++i) cen[i] = g.w0[i] + g.d[i] * ((double)ix[i] + 0.5);
+            unpack_xref(A.rx[gv], cen, g.d, r);
             for (int i = 0; i < 3; ++i) {
                 dxr[i] = S[A.ox + i] / sm;
-                xr[i] = (g.w0[i] + g.d[i] * ((double)ix[i] + 0.5)) + dxr[i];
+                xr[i] = r[i] + dxr[i];
             }
+        }
         if (A.ov >= 0) {
             const long long tile = (A.toff ? A.toff[cut] : 0ll) + acc_tile(g, ix[0], ix[1], ix[2]);
+            double r[3];
+            unpack_vref(A.rv[gv], A.vref + 3 * tile, r);
             for (int i = 0; i < 3; ++i) {
                 dvr[i] = S[A.ov + i] / sm;
-                vr[i] = A.vref[3 * tile + i] + dvr[i];
+                vr[i] = r[i] + dvr[i];
             }
         }
         const double M0 = F.M[gi], Mf = M0 + sm;
@@ -1305,7 +1314,7 @@ __global__ void k_correction_select(ItemArrays it, const double* scale, long lon
 {
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
         const double sc = scale[t];
-        if (sc > 0.0 && fabs(sc - 1.0) > tol) {
+        if (it.key[t] != KEY_DEEP && sc > 0.0 && fabs(sc - 1.0) > tol) { // breadth-first images only
             const unsigned long long i = atomicAdd(count, 1ull);
             list[i] = (int)t;
             keys[i] = it.key[t];

@@ -3,19 +3,33 @@
 Tets are independent, so the deposit shards over the Lagrangian element index
 space: rank r of W voxelizes the contiguous slab of elements
 ``element_slab(nelem, W, r)`` into a full-size grid of its own, and one
-exchange step combines the ranks' grids on every rank.  The combination is the
-merge of the reference's online update (src/geometry.c:164-186) applied to W
-partial results at once:
+exchange step combines the ranks' grids.  The combination is the merge of the
+reference's online update (src/geometry.c:164-186) applied to W partial
+results at once:
 
     M  = sum_r M_r
     X  = sum_r M_r X_r / M                       (V alike)
     XX = sum_r M_r (XX_r + (X_r - X)(X_r - X)^T) / M   (XV with V, VV alike)
 
-taken in two all-reduces (first M, M X, M V; then the second moments about
-the global means, so nothing cancels).  The sums run in a different order
-from a single deposit, so FP64 results agree with it to rounding, not bit for
-bit.  The collectives are torch.distributed all-reduces: NCCL over NVLink for
-CUDA tensors, gloo for CPU tensors.
+The exchange sends raw sums, so that it is one reduction: each rank turns its
+fields into per-voxel sums about reference points c (position) and u
+(velocity) --
+
+    S0 = M_r,  Sx = M_r (X_r - c),  Sv = M_r (V_r - u),
+    Sxx = M_r (XX_r + (X_r - c)(X_r - c)^T),  Sxv, Svv alike --
+
+one reduce-scatter adds them over the ranks, each rank getting a slab of voxel
+planes along the first axis, and each rank turns its slab back into M, X, V
+and (co)variances; an all-gather of the finished slabs gives every rank the
+whole grid.  c and u must be the same on every rank and close to the voxel's
+final means, or Sxx / M - (Sx / M)(Sx / M)^T cancels in voxels made of tiny
+fragments: they are the means to single precision, from one all-reduce of
+M, M X and M V in FP32 (7 floats per voxel, against 34 doubles in the
+reduce-scatter).  The sums run in a different order from a single deposit, so
+FP64 results agree with it to rounding, not bit for bit.  The collectives are
+torch.distributed: NCCL over NVLink for CUDA tensors (reduce_scatter_tensor,
+all_gather_into_tensor), gloo for CPU tensors (which has no reduce-scatter: an
+all-reduce, then the rank's slab).
 """
 from __future__ import annotations
 
@@ -47,34 +61,104 @@ def block_slab_connectivity(block_dims, periodic: bool, e0: int, e1: int, device
     return torch.stack(cols, dim=1).to(torch.int32).contiguous()
 
 
+def _is_nccl(group) -> bool:
+    return dist.get_backend(group) == "nccl"
+
+
+def _reduce_scatter_rows(buf: torch.Tensor, world: int, rank: int, group) -> torch.Tensor:
+    """Sum of buf over the ranks, rank's slab of rows (buf.shape[0] divisible by world)."""
+    rows = buf.shape[0] // world
+    if _is_nccl(group):
+        out = torch.empty((rows,) + tuple(buf.shape[1:]), dtype=buf.dtype, device=buf.device)
+        dist.reduce_scatter_tensor(out, buf.contiguous(), group=group)
+        return out
+    dist.all_reduce(buf, group=group)
+    return buf[rank * rows:(rank + 1) * rows].clone()
+
+
+def _all_gather_rows(part: torch.Tensor, world: int, group) -> torch.Tensor:
+    if _is_nccl(group):
+        out = torch.empty((world * part.shape[0],) + tuple(part.shape[1:]), dtype=part.dtype, device=part.device)
+        dist.all_gather_into_tensor(out, part.contiguous(), group=group)
+        return out
+    parts = [torch.empty_like(part) for _ in range(world)]
+    dist.all_gather(parts, part.contiguous(), group=group)
+    return torch.cat(parts)
+
+
 def merge_fields(fields: dict, group=None) -> dict:
     """Combine every rank's partial fields (m, and any of x, v, xx, xv, vv, in
     the reference's layout) into the fields of the whole mesh, in place, on
     every rank of `group`."""
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
     m = fields["m"]
-    first = [f for f in ("x", "v") if f in fields]
-    # pass 1: M and the mass-weighted first moments
-    buf1 = [m.clone()] + [fields[f] * m.unsqueeze(-1) for f in first]
-    for b in buf1:
-        dist.all_reduce(b, group=group)
-    mt = buf1[0]
-    safe = torch.where(mt > 0, mt, torch.ones_like(mt))
-    means = {f: b / safe.unsqueeze(-1) for f, b in zip(first, buf1[1:])}
-    # pass 2: second moments about the global means
+    n = tuple(m.shape)
+    dev, dt = m.device, m.dtype
+    hx, hv = "x" in fields, "v" in fields
     second = [f for f in ("xx", "xv", "vv") if f in fields]
-    buf2 = []
+    # reference points, equal on every rank: the merged means in single precision
+    c = u = None
+    if hx or hv:
+        parts = [m.unsqueeze(-1)] + [m.unsqueeze(-1) * fields[f] for f in ("x", "v") if f in fields]
+        approx = torch.cat(parts, dim=-1).float()
+        dist.all_reduce(approx, group=group)
+        mt = approx[..., :1]
+        means = (approx[..., 1:] / torch.where(mt > 0, mt, torch.ones_like(mt))).to(dt)
+        if hx:
+            c = means[..., :3]
+        if hv:
+            u = means[..., 3:6] if hx else means[..., :3]
+    # raw sums, (voxel, component), padded to a multiple of `world` voxel planes
+    comps = [m.unsqueeze(-1)]
+    dx = fields["x"] - c if hx else None
+    dv = fields["v"] - u if hv else None
+    if hx:
+        comps.append(m.unsqueeze(-1) * dx)
+    if hv:
+        comps.append(m.unsqueeze(-1) * dv)
     for f in second:
         a, b = SECOND[f]
-        da = fields[a] - means[a]
-        db = fields[b] - means[b]
-        buf2.append((fields[f] + da.unsqueeze(-1) * db.unsqueeze(-2)) * m[..., None, None])
-    for b in buf2:
-        dist.all_reduce(b, group=group)
-    for f, b in zip(second, buf2):
-        fields[f].copy_(torch.where(mt[..., None, None] > 0, b / safe[..., None, None], torch.zeros_like(b)))
-    for f in first:
-        fields[f].copy_(torch.where(mt.unsqueeze(-1) > 0, means[f], torch.zeros_like(means[f])))
-    fields["m"].copy_(mt)
+        da = dx if a == "x" else dv
+        db = dx if b == "x" else dv
+        comps.append((m[..., None, None] * (fields[f] + da.unsqueeze(-1) * db.unsqueeze(-2))).reshape(n + (9,)))
+    raw = torch.cat(comps, dim=-1)
+    rows = (n[0] + world - 1) // world
+    buf = torch.zeros((rows * world,) + n[1:] + (raw.shape[-1],), dtype=dt, device=dev)
+    buf[: n[0]] = raw
+    del raw, comps
+    part = _reduce_scatter_rows(buf, world, rank, group)
+    del buf
+    # this rank's slab of voxel planes back to fields
+    i0 = rank * rows
+    i1 = min(i0 + rows, n[0])
+    S = part[: max(0, i1 - i0)]
+    s0 = S[..., 0]
+    live = s0 > 0
+    safe = torch.where(live, s0, torch.ones_like(s0))
+    out = {"m": s0}
+    k = 1
+    mx = mv = None
+    if hx:
+        mx = S[..., k:k + 3] / safe.unsqueeze(-1)
+        out["x"] = torch.where(live.unsqueeze(-1), c[i0:i1] + mx, torch.zeros_like(mx))
+        k += 3
+    if hv:
+        mv = S[..., k:k + 3] / safe.unsqueeze(-1)
+        out["v"] = torch.where(live.unsqueeze(-1), u[i0:i1] + mv, torch.zeros_like(mv))
+        k += 3
+    for f in second:
+        a, b = SECOND[f]
+        ma = mx if a == "x" else mv
+        mb = mx if b == "x" else mv
+        cov = S[..., k:k + 9].reshape(S.shape[:3] + (3, 3)) / safe[..., None, None] - ma.unsqueeze(-1) * mb.unsqueeze(-2)
+        out[f] = torch.where(live[..., None, None], cov, torch.zeros_like(cov))
+        k += 9
+    # every rank gets the whole grid
+    for f, slab in out.items():
+        pad = torch.zeros((rows,) + tuple(slab.shape[1:]), dtype=dt, device=dev)
+        pad[: slab.shape[0]] = slab
+        fields[f].copy_(_all_gather_rows(pad, world, group)[: n[0]])
     return fields
 
 
