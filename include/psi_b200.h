@@ -177,6 +177,28 @@ int psib_voxels_adjoint(const psib_grid *grad, const psib_mesh *mesh, double ref
                         int refine_max_lvl, double *grad_pos, double *grad_vel, double *grad_mass,
                         const psib_options *opt);
 
+/* Adjoint of every grid field.  The reference has no adjoint; this is the
+ * backward pass of a psib_voxels deposit into zeroed fields, for differentiable
+ * use of all its moments (src/geometry.c:81-186 defines them).
+ *
+ * fwd holds the fields that deposit produced (m, and any of x, v, xx, xv, vv;
+ * a second moment needs its first moments); grad->fields[f] holds dL/d(field f)
+ * on the same grid, or NULL for a field L does not depend on (a gradient needs
+ * its forward field).  The gradients of L with respect to the particle
+ * positions and velocities (npart x 3 doubles each) and the element masses
+ * (nelem doubles) are ADDED to grad_pos, grad_vel and grad_mass (the last two
+ * may be NULL).  The clip is recomputed in FP64; each fragment's moments are
+ * differentiated through the motion of its faces that lie on its tet's faces,
+ * the tet's density and the interpolated velocity field.  The reference's
+ * pairing of the x-v cross terms with the tet's first vertex
+ * (src/geometry.c:137-146) is differentiated as it is.  Gradients are summed with
+ * atomics, so the last bits may vary between runs.  Device memory only, on
+ * options->stream; refine_max_lvl = 0 for trilinear elements, and simplex
+ * elements. */
+int psib_voxels_adjoint_fields(const psib_grid *grad, const psib_grid *fwd, const psib_mesh *mesh,
+                               double refine_tolerance, int refine_max_lvl, double *grad_pos, double *grad_vel,
+                               double *grad_mass, const psib_options *opt);
+
 /* Message for the last failure on this thread ("" if none). */
 const char *psib_last_error(void);
 

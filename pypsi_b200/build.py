@@ -36,7 +36,7 @@ CUDA_UNITS = {  # unit -> extra flags
     "probe.cu": [],  # the FMA issue-rate probe (explicit fma(), so contraction does not matter)
     "loaders.cpp": [],  # host code only: the snapshot readers
 }
-HEADERS = ["psib_device.cuh", "psib_clip.cuh", "psib_kernels.h", "psib_accum.cuh"]
+HEADERS = ["psib_device.cuh", "psib_clip.cuh", "psib_kernels.h", "psib_accum.cuh", "psib_adjoint.cuh"]
 
 
 def _newer(target: str, deps: list[str]) -> bool:

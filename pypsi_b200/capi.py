@@ -63,6 +63,9 @@ lib.psib_query_elements.restype = C.c_int
 lib.psib_sample_vdf.argtypes = [C.POINTER(Mesh), C.c_void_p, C.c_void_p, C.c_longlong, C.c_double, C.c_int, C.c_void_p,
                                 C.c_void_p, C.c_void_p, C.c_longlong, C.POINTER(Options)]
 lib.psib_sample_vdf.restype = C.c_int
+lib.psib_voxels_adjoint_fields.argtypes = [C.POINTER(Grid), C.POINTER(Grid), C.POINTER(Mesh), C.c_double, C.c_int,
+                                           C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(Options)]
+lib.psib_voxels_adjoint_fields.restype = C.c_int
 lib.psib_measure_fma_peak.argtypes = [C.c_int, C.POINTER(C.c_double)]
 lib.psib_measure_fma_peak.restype = C.c_int
 lib.psib_last_error.restype = C.c_char_p
@@ -184,6 +187,33 @@ def adjoint_device(grad_m, n, bounds, pos, grad_pos, mass=None, connectivity=Non
                 stream=C.c_void_p(s.cuda_stream), stats=C.pointer(st))
     rc = lib.psib_voxels_adjoint(C.byref(g), C.byref(m), 1.0, 0, grad_pos.data_ptr(), None,
                                  grad_mass.data_ptr() if grad_mass is not None else None, C.byref(o))
+    if rc != 0:
+        raise PsibError(rc)
+    return st.as_dict()
+
+
+def adjoint_fields_device(grads: dict, fwd: dict, n, bounds, pos, grad_pos, vel=None, mass=None, connectivity=None,
+                          block_dims=None, periodic_box=None, grad_vel=None, grad_mass=None, stream=None) -> dict:
+    """Backward pass of every field (psib_voxels_adjoint_fields) on device tensors.
+
+    fwd: the fields of the forward deposit into zeroed fields ({"m": ..., "x": ...});
+    grads: dL/d(field) for any of them (missing: 0).  Adds dL/dpos to grad_pos and,
+    if given, dL/dvel to grad_vel ((npart,3)) and dL/dmass to grad_mass ((nelem,))."""
+    import torch
+
+    for t in list(grads.values()) + list(fwd.values()) + [pos, grad_pos] + \
+            [t for t in (vel, grad_vel, grad_mass) if t is not None]:
+        assert t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()
+    g = make_grid(n, bounds, {f: t.data_ptr() for f, t in grads.items()})
+    f = make_grid(n, bounds, {k: t.data_ptr() for k, t in fwd.items()})
+    m = mesh_from_tensors(pos, vel, mass, connectivity, block_dims, periodic_box)
+    s = stream if stream is not None else torch.cuda.current_stream()
+    st = Stats()
+    o = Options(precision=PSIB_FP64, deterministic=0, memory=PSIB_DEVICE, device=-1,
+                stream=C.c_void_p(s.cuda_stream), stats=C.pointer(st))
+    rc = lib.psib_voxels_adjoint_fields(C.byref(g), C.byref(f), C.byref(m), 1.0, 0, grad_pos.data_ptr(),
+                                        grad_vel.data_ptr() if grad_vel is not None else None,
+                                        grad_mass.data_ptr() if grad_mass is not None else None, C.byref(o))
     if rc != 0:
         raise PsibError(rc)
     return st.as_dict()

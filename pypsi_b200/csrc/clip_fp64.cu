@@ -41,18 +41,36 @@ __global__ void __launch_bounds__(64) k_clip_fp64_big(ClipArgs a) { clip_loop<do
 __global__ void __launch_bounds__(128, 4) k_adjoint(ClipArgs a) { clip_loop<double, NS_MAIN, false, true>(a); }
 __global__ void __launch_bounds__(64) k_adjoint_big(ClipArgs a) { clip_loop<double, NS_BIG, false, true>(a); }
 
+// the adjoint of every field (adj_coef set): positions, velocities and masses
+__global__ void __launch_bounds__(128) k_adjoint_full(ClipArgs a) { clip_loop<double, NS_MAIN, false, true, true>(a); }
+__global__ void __launch_bounds__(64) k_adjoint_full_big(ClipArgs a)
+{
+    clip_loop<double, NS_BIG, false, true, true>(a);
+}
+
 cudaError_t launch_adjoint(const ClipArgs& a, bool big, int grid, int block, cudaStream_t s)
 {
-    if (big) k_adjoint_big<<<grid, block, 0, s>>>(a);
-    else k_adjoint<<<grid, block, 0, s>>>(a);
+    if (a.adj_coef) {
+        if (big) k_adjoint_full_big<<<grid, block, 0, s>>>(a);
+        else k_adjoint_full<<<grid, block, 0, s>>>(a);
+    } else if (big) {
+        k_adjoint_big<<<grid, block, 0, s>>>(a);
+    } else {
+        k_adjoint<<<grid, block, 0, s>>>(a);
+    }
     return cudaGetLastError();
 }
 
-int adjoint_blocks_per_sm(bool big, int block)
+int adjoint_blocks_per_sm(bool big, int block, bool full)
 {
     int n = 0;
-    cudaError_t e = big ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_adjoint_big, block, 0)
-                        : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_adjoint, block, 0);
+    cudaError_t e;
+    if (full)
+        e = big ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_adjoint_full_big, block, 0)
+                : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_adjoint_full, block, 0);
+    else
+        e = big ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_adjoint_big, block, 0)
+                : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_adjoint, block, 0);
     if (e != cudaSuccess) { cudaGetLastError(); return 1; }
     return n > 0 ? n : 1;
 }

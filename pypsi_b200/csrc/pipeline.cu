@@ -28,6 +28,7 @@
 #include <vector>
 
 #include "psi_b200.h"
+#include "psib_adjoint.cuh"
 #include "psib_device.cuh"
 #include "psib_kernels.h"
 
@@ -118,6 +119,7 @@ struct Ctx {
     // breadth-first clip: three polyhedron queues, the volume histogram, per-level counters, window list
     DevBuf qx[3], qnb[3], qnv[3], qwin[3], qbox[3], qitem[3], hist, bfs_cnt, dfs_list, vsum;
     DevBuf btab, igrid; // batch tables, image -> cutout
+    DevBuf adjcoef;     // full adjoint: per-voxel coefficients
     // atomic accumulation: per-voxel sums, tile reference velocities, the mass-correction pass
     DevBuf acc_sum, acc_ref, acc_tsum, acc_vref, acc_toff, fix_list, fix_keys, fix_list_s, fix_keys_s, ifactor;
     DevBuf passes;      // breadth-first pass table
@@ -142,7 +144,7 @@ struct Ctx {
                 &a_reg_cnt, &a_reg_off, &a_reg_key, &a_reg_elem, &a_reg_key_s, &a_reg_elem_s, &a_run_key,
                 &a_run_cnt, &a_run_off, &a_run_lo, &a_run_hi, &a_pair_cnt, &a_pair_off, &a_pair_key,
                 &a_pair_key_s, &a_na, &a_aoff, &a_tp_cnt, &a_tp_excl, &a_bounds, &a_tpairs, &a_deep, &a_tp_key,
-                &a_tp_key_s, &a_ord_in, &a_ord, &q_in, &q_cnt, &acc_sum, &acc_ref, &acc_tsum, &acc_vref, &acc_toff,
+                &a_tp_key_s, &a_ord_in, &a_ord, &q_in, &q_cnt, &adjcoef, &acc_sum, &acc_ref, &acc_tsum, &acc_vref, &acc_toff,
                 &fix_list, &fix_keys, &fix_list_s, &fix_keys_s, &ifactor,
                 &q_off, &q_key, &q_key_s, &q_out, &s_cnt, &s_off, &s_offs, &s_rho, &s_vel};
     }
@@ -246,9 +248,11 @@ struct Call {
     const psib_grid* grids;
     const psib_mesh* meshes;
     const double* refine_cell_given;
-    // adjoint call: F[0] holds dL/dm; gradients accumulate into these
+    // adjoint call: F[0] holds dL/dm (or adj_coef the full adjoint's per-voxel coefficients);
+    // gradients accumulate into these
     bool adjoint;
-    double *gpos, *gmass;
+    double *gpos, *gmass, *gvel;
+    const double* adj_coef;
 };
 
 int check_status(Call& c, unsigned long long* small_host)
@@ -747,7 +751,7 @@ int run_device(Call& c)
     // persistent clip kernels: one resident wave, each thread with its own scratch region
     const int clip_block = 128, big_block = 64;
     const int clip_grid =
-        C.num_sms * (c.adjoint ? adjoint_blocks_per_sm(false, clip_block)
+        C.num_sms * (c.adjoint ? adjoint_blocks_per_sm(false, clip_block, c.adj_coef != nullptr)
                      : central ? clip_blocks_per_sm_mixed(false, !mixed, clip_block)
                                : clip_blocks_per_sm_fp64(false, clip_block));
     const size_t main_bytes = central ? scratch_bytes_mixed(false, !mixed) : scratch_bytes_fp64(false);
@@ -773,6 +777,8 @@ int run_device(Call& c)
         ca.adj_npart = m.npart;
         ca.adj_gmass = c.gmass;
         ca.adj_mass_factor = m.elemtype == 8 ? 1.0 / 6.0 : 1.0;
+        ca.adj_coef = c.adj_coef;
+        ca.adj_gvel = c.gvel;
     }
 
     long long ntiles = 0;
@@ -864,7 +870,8 @@ int run_device(Call& c)
             }
             if (ndeep > 0) {
                 const int big_grid = (int)std::min<long long>(
-                    (long long)C.num_sms * adjoint_blocks_per_sm(true, big_block), (ndeep + big_block - 1) / big_block);
+                    (long long)C.num_sms * adjoint_blocks_per_sm(true, big_block, c.adj_coef != nullptr),
+                    (ndeep + big_block - 1) / big_block);
                 RET(ensure(C.scratch_big, big_bytes * (size_t)big_grid * big_block));
                 ca.scratch = C.scratch_big.p;
                 ca.order_base = nmain;
@@ -2479,6 +2486,81 @@ int psib_voxels_adjoint(const psib_grid* grad, const psib_mesh* mesh, double ref
     CK(cudaEventRecord(C->ev[7], st));
     CK(cudaEventSynchronize(C->ev[7]));
     if (o.stats) CK(cudaEventElapsedTime(&o.stats->ms_total, C->ev[0], C->ev[7]));
+    return PSIB_OK;
+}
+
+int psib_voxels_adjoint_fields(const psib_grid* grad, const psib_grid* fwd, const psib_mesh* mesh,
+                               double refine_tolerance, int refine_max_lvl, double* grad_pos, double* grad_vel,
+                               double* grad_mass, const psib_options* opt)
+{
+    g_err.clear();
+    psib_options o = {};
+    o.precision = PSIB_FP64;
+    o.memory = PSIB_DEVICE;
+    o.device = -1;
+    if (opt) o = *opt;
+    if (!grad || !fwd) return fail(PSIB_ERR_ARG, "grad and fwd are required");
+    RET(validate(fwd, mesh, PSIB_MODE_DENSITY, &o));
+    for (int i = 0; i < 3; ++i)
+        if (grad->n[i] != fwd->n[i] || grad->window[0][i] != fwd->window[0][i] ||
+            grad->window[1][i] != fwd->window[1][i])
+            return fail(PSIB_ERR_ARG, "grad and fwd must describe the same grid");
+    static const char* names[6] = {"m", "x", "v", "xx", "xv", "vv"};
+    for (int f = 0; f < 6; ++f)
+        if (grad->fields[f] && !fwd->fields[f])
+            return fail(PSIB_ERR_ARG, "the gradient of field %s needs the forward field %s", names[f], names[f]);
+    if ((fwd->fields[PSIB_XX] && !fwd->fields[PSIB_X]) || (fwd->fields[PSIB_VV] && !fwd->fields[PSIB_V]) ||
+        (fwd->fields[PSIB_XV] && !(fwd->fields[PSIB_X] && fwd->fields[PSIB_V])))
+        return fail(PSIB_ERR_ARG, "the forward second moments need their first moments (xx: x, vv: v, xv: x and v)");
+    if (o.memory != PSIB_DEVICE) return fail(PSIB_ERR_UNSUPPORTED, "psib_voxels_adjoint_fields takes device memory");
+    if (refine_max_lvl > 0 && mesh->elemtype == 8)
+        return fail(PSIB_ERR_UNSUPPORTED, "the adjoint supports refine_max_lvl = 0 only");
+    if (mesh->elemtype == 27) return fail(PSIB_ERR_UNSUPPORTED, "the adjoint supports 4- and 8-node elements");
+    if (!grad_pos && mesh->nelem > 0) return fail(PSIB_ERR_ARG, "grad_pos is required");
+    if (psib_device_count() <= 0) return fail(PSIB_ERR_NODEVICE, "no CUDA device is visible");
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    Ctx* C = nullptr;
+    RET(get_ctx(dev, &C));
+    if (o.stats) *o.stats = psib_stats{};
+    if (mesh->nelem == 0) return PSIB_OK;
+    const long long nvox = (long long)fwd->n[0] * fwd->n[1] * fwd->n[2];
+    cudaStream_t st = (cudaStream_t)o.stream;
+    RET(ensure(C->adjcoef, (size_t)nvox * ADJ_NCOEF * sizeof(double)));
+    AdjCoefArgs ac = {};
+    for (int f = 0; f < 6; ++f) {
+        ac.F[f] = fwd->fields[f];
+        ac.G[f] = grad->fields[f];
+    }
+    ac.coef = C->adjcoef.as<double>();
+    ac.nvox = nvox;
+    CK(launch_adj_coeffs(ac, st));
+
+    Call c = {};
+    c.grid = fwd;
+    c.mesh = mesh;
+    c.reftol = refine_tolerance;
+    c.maxlvl = 0;
+    c.precision = PSIB_FP64;
+    c.C = C;
+    c.stats = o.stats;
+    c.adjoint = true;
+    c.adj_coef = C->adjcoef.as<double>();
+    c.st = st;
+    c.pos = mesh->pos;
+    c.vel = mesh->vel;
+    c.mass = mesh->mass;
+    c.conn = mesh->connectivity;
+    c.gpos = grad_pos;
+    c.gvel = grad_vel;
+    c.gmass = grad_mass;
+    CK(cudaEventRecord(C->ev[0], st));
+    RET(run_device(c));
+    if (o.stats) {
+        CK(cudaEventRecord(C->ev[7], st));
+        CK(cudaEventSynchronize(C->ev[7]));
+        CK(cudaEventElapsedTime(&o.stats->ms_total, C->ev[0], C->ev[7]));
+    }
     return PSIB_OK;
 }
 

@@ -25,6 +25,7 @@
 // threads index different slots.
 #pragma once
 #include "psib_accum.cuh"
+#include "psib_adjoint.cuh"
 #include "psib_device.cuh"
 #include "psib_kernels.h"
 
@@ -98,12 +99,15 @@ __device__ __forceinline__ void write_record(const ClipArgs& a, const GridDev& g
 // records (always so in the FP32 kernel; the FP64 kernel does it when it
 // serves the mixed-precision mode).  ADJ (FP64 only): instead of writing
 // records, pull the upstream gradient of the m field back to the positions of
-// the image's four particles (and to its element's mass).
-template <class R, int NS, bool CENTRAL, bool ADJ = false>
+// the image's four particles (and to its element's mass).  FULL (with ADJ):
+// the gradient of every field, through the per-voxel coefficients adj_coef
+// (psib_adjoint.cuh), back to positions, velocities and masses.
+template <class R, int NS, bool CENTRAL, bool ADJ = false, bool FULL = false>
 __device__ void clip_item(const ClipArgs& a, long long t, Poly<R>* S, QPoly* QL, Poly<double>* WC, unsigned& st,
                           Tally& tally)
 {
     static_assert(!ADJ || (sizeof(R) == 8 && !CENTRAL), "the adjoint walks the FP64 fragments");
+    static_assert(!FULL || ADJ, "FULL is a form of the adjoint");
     // the image's grid: its cutout's in a batch, whose voxels start at vbase
     const GridDev& g = a.grids ? a.grids[a.it.grid[t]] : a.g;
     const unsigned long long vbase = a.voff ? a.voff[a.it.grid[t]] : 0ull;
@@ -234,6 +238,21 @@ __device__ void clip_item(const ClipArgs& a, long long t, Poly<R>* S, QPoly* QL,
     // adjoint accumulators: sum over fragments of g dS(P)/dx_i, and of g m0
     double A[4][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
     double B = 0.0;
+    // full adjoint: the image's frame and its accumulators
+    AdjItem T;
+    AdjAcc acc;
+    if constexpr (FULL) {
+        for (int i = 0; i < 3; ++i) {
+            T.x0[i] = p[0][i];
+            T.v0[i] = fr[FR_U + i];
+            for (int j = 0; j < 3; ++j) {
+                T.DX[i][j] = p[j + 1][i] - p[0][i];
+                T.DV[i][j] = fr[FR_U + 3 * (j + 1) + i] - fr[FR_U + i];
+            }
+        }
+        T.mass = fr[FR_MASS];
+        adj_zero(acc);
+    }
     for (;;) {
         Poly<R>& P = S[c];
         bool done_node = true;
@@ -261,12 +280,21 @@ __device__ void clip_item(const ClipArgs& a, long long t, Poly<R>* S, QPoly* QL,
                     for (int i = 0; i < 3; ++i) o[i] = QL->q[0][i];
                 }
                 double gv = 0.0;
+                const double* cf = nullptr;
                 if constexpr (ADJ) {
-                    if (P.lo[0] < g.n[0] && P.lo[1] < g.n[1] && P.lo[2] < g.n[2])
-                        gv = a.adj_gm[((long long)g.n[1] * P.lo[0] + P.lo[1]) * g.n[2] + P.lo[2]];
+                    if (P.lo[0] < g.n[0] && P.lo[1] < g.n[1] && P.lo[2] < g.n[2]) {
+                        const long long vi = ((long long)g.n[1] * P.lo[0] + P.lo[1]) * g.n[2] + P.lo[2];
+                        if constexpr (FULL) {
+                            cf = a.adj_coef + vi * ADJ_NCOEF;
+                            gv = 1.0; // every fragment is walked: the forward's voxels all hold mass
+                        } else {
+                            gv = a.adj_gm[vi];
+                        }
+                    }
                 }
                 unsigned e;
-                if constexpr (ADJ) e = gv != 0.0 ? reduce_poly(P, mom, 0) : 0u;
+                if constexpr (FULL) e = reduce_poly(P, mom, 2);
+                else if constexpr (ADJ) e = gv != 0.0 ? reduce_poly(P, mom, 0) : 0u;
                 else if constexpr (sizeof(R) == 4) e = reduce_about(*QL, o, mom, order);
                 else e = CENTRAL ? reduce_about(P, o, mom, order) : reduce_poly(P, mom, order);
                 if (e) { st |= e; return; }
@@ -280,7 +308,10 @@ __device__ void clip_item(const ClipArgs& a, long long t, Poly<R>* S, QPoly* QL,
                             (long long)vbase + ((long long)g.n[1] * P.lo[0] + P.lo[1]) * g.n[2] + P.lo[2];
                         tally.frags++;
                         tally.verts += P.nv;
-                        if constexpr (ADJ) {
+                        if constexpr (FULL) {
+                            const unsigned e2 = adjoint_fragment(P, mom, cf, T, acc);
+                            if (e2) { st |= e2; return; }
+                        } else if constexpr (ADJ) {
                             const unsigned e2 = adjoint_poly(P, gv, A);
                             if (e2) { st |= e2; return; }
                             B += gv * mom[0];
@@ -347,7 +378,64 @@ __device__ void clip_item(const ClipArgs& a, long long t, Poly<R>* S, QPoly* QL,
         if (top == 0) break;
         c = stk[--top];
     }
-    if constexpr (ADJ) {
+    if constexpr (FULL) {
+        // dL/dp_k = (mass / vol) * surface integrals - (dvol/dp_k / vol) * I0 - (grad v)^T J_k, plus the
+        // quirk's explicit term on the first vertex; dL/du_k = J_k (plus its velocity term); dL/dmass = I0 / mass
+        double e[3][3];
+        for (int v = 0; v < 3; ++v)
+            for (int i = 0; i < 3; ++i) e[v][i] = p[v + 1][i] - p[0][i];
+        double dS[4][3];
+        for (int v = 0; v < 3; ++v) {
+            const double* u = e[(v + 1) % 3];
+            const double* w = e[(v + 2) % 3];
+            dS[v + 1][0] = (u[1] * w[2] - u[2] * w[1]) * (1.0 / 6.0);
+            dS[v + 1][1] = (u[2] * w[0] - u[0] * w[2]) * (1.0 / 6.0);
+            dS[v + 1][2] = (u[0] * w[1] - u[1] * w[0]) * (1.0 / 6.0);
+        }
+        for (int i = 0; i < 3; ++i) dS[0][i] = -(dS[1][i] + dS[2][i] + dS[3][i]);
+        const double sT = e[0][0] * dS[1][0] + e[0][1] * dS[1][1] + e[0][2] * dS[1][2];
+        if (sT != 0.0) {
+            // grad v = DV DX^-1: solve DX^T G^T = DV^T row by row (DX^-1 = adj(DX)^T / det)
+            double inv[3][3];
+            {
+                const double(*D)[3] = T.DX;
+                const double det = D[0][0] * (D[1][1] * D[2][2] - D[1][2] * D[2][1]) -
+                                   D[0][1] * (D[1][0] * D[2][2] - D[1][2] * D[2][0]) +
+                                   D[0][2] * (D[1][0] * D[2][1] - D[1][1] * D[2][0]);
+                const double id = 1.0 / det;
+                inv[0][0] = (D[1][1] * D[2][2] - D[1][2] * D[2][1]) * id;
+                inv[0][1] = (D[0][2] * D[2][1] - D[0][1] * D[2][2]) * id;
+                inv[0][2] = (D[0][1] * D[1][2] - D[0][2] * D[1][1]) * id;
+                inv[1][0] = (D[1][2] * D[2][0] - D[1][0] * D[2][2]) * id;
+                inv[1][1] = (D[0][0] * D[2][2] - D[0][2] * D[2][0]) * id;
+                inv[1][2] = (D[0][2] * D[1][0] - D[0][0] * D[1][2]) * id;
+                inv[2][0] = (D[1][0] * D[2][1] - D[1][1] * D[2][0]) * id;
+                inv[2][1] = (D[0][1] * D[2][0] - D[0][0] * D[2][1]) * id;
+                inv[2][2] = (D[0][0] * D[1][1] - D[0][1] * D[1][0]) * id;
+            }
+            double gvel[3][3]; // d v_c / d x_a
+            for (int c2 = 0; c2 < 3; ++c2)
+                for (int a2 = 0; a2 < 3; ++a2)
+                    gvel[c2][a2] = T.DV[c2][0] * inv[0][a2] + T.DV[c2][1] * inv[1][a2] + T.DV[c2][2] * inv[2][a2];
+            const double rho = T.mass / sT;
+            for (int v = 0; v < 4; ++v) {
+                const int pid = a.it.pid[v * a.it.cap + t];
+                if (pid < 0 || pid >= a.adj_npart) { st |= ST_INDEX; continue; }
+                for (int i = 0; i < 3; ++i) {
+                    double gp = rho * acc.bnd[v][i] - dS[v][i] / sT * acc.I0;
+                    for (int c2 = 0; c2 < 3; ++c2) gp -= gvel[c2][i] * acc.J[v][c2];
+                    double gu = acc.J[v][i];
+                    if (v == 0) {
+                        gp += acc.qa[i];
+                        gu += acc.qb[i];
+                    }
+                    atomicAdd(&a.adj_gpos[3 * (long long)pid + i], gp);
+                    if (a.adj_gvel) atomicAdd(&a.adj_gvel[3 * (long long)pid + i], gu);
+                }
+            }
+            if (a.adj_gmass && T.mass != 0.0) atomicAdd(&a.adj_gmass[a.it.elem[t]], acc.I0 / T.mass * a.adj_mass_factor);
+        }
+    } else if constexpr (ADJ) {
         // d m0 / dx_i = (dS(P)/dx_i - m0 dS(T)/dx_i) / S(T), times the image's mass
         if (B != 0.0 || A[0][0] != 0.0 || A[0][1] != 0.0 || A[0][2] != 0.0 || A[1][0] != 0.0 || A[1][1] != 0.0 ||
             A[1][2] != 0.0 || A[2][0] != 0.0 || A[2][1] != 0.0 || A[2][2] != 0.0 || A[3][0] != 0.0 ||
@@ -389,7 +477,7 @@ __device__ void clip_item(const ClipArgs& a, long long t, Poly<R>* S, QPoly* QL,
 }
 
 // Persistent kernel body: warps take 32 consecutive queue entries at a time.
-template <class R, int NS, bool CENTRAL, bool ADJ = false>
+template <class R, int NS, bool CENTRAL, bool ADJ = false, bool FULL = false>
 __device__ __forceinline__ void clip_loop(const ClipArgs& a)
 {
     const int lane = threadIdx.x & 31;
@@ -408,7 +496,7 @@ __device__ __forceinline__ void clip_loop(const ClipArgs& a)
         const long long i = (long long)base + lane;
         if (i < a.n) {
             const long long t = a.order ? (long long)a.order[a.order_base + i] : a.order_base + i;
-            clip_item<R, NS, CENTRAL, ADJ>(a, t, S, QL, WC, st, tally);
+            clip_item<R, NS, CENTRAL, ADJ, FULL>(a, t, S, QL, WC, st, tally);
         }
     }
     if (st) atomicOr(a.status, st);

@@ -117,6 +117,8 @@ struct ClipArgs {
     long long adj_npart;
     double *adj_gmass;       // dL/dmass per element (accumulated), may be null
     double adj_mass_factor;  // element mass / tet mass
+    const double *adj_coef;  // full adjoint: ADJ_NCOEF coefficients per voxel (null: the m field only, adj_gm)
+    double *adj_gvel;        // full adjoint: dL/dvel per particle (accumulated), may be null
     AccArgs acc;             // atomic accumulation (acc.sum != null) instead of records
 };
 
@@ -167,9 +169,19 @@ size_t scratch_bytes_mixed(bool big, bool fp64_walk);
 // resident blocks per SM of a clip kernel at this block size
 int clip_blocks_per_sm_fp64(bool big, int block);
 int clip_blocks_per_sm_mixed(bool big, bool fp64_walk, int block);
-// adjoint of the density deposit (FP64 walk, no records)
+// adjoint of the density deposit (FP64 walk, no records); full: every field, through adj_coef
 cudaError_t launch_adjoint(const ClipArgs &a, bool big, int grid, int block, cudaStream_t s);
-int adjoint_blocks_per_sm(bool big, int block);
+int adjoint_blocks_per_sm(bool big, int block, bool full = false);
+
+// Per-voxel coefficients of the full adjoint (psib_adjoint.cuh) from the
+// forward fields and their upstream gradients (either may be null per field).
+struct AdjCoefArgs {
+    const double *F[6];      // forward fields m x v xx xv vv
+    const double *G[6];      // dL/d(field), null: 0
+    double *coef;            // ADJ_NCOEF per voxel
+    long long nvox;
+};
+cudaError_t launch_adj_coeffs(const AdjCoefArgs &a, cudaStream_t s);
 
 // Breadth-first clip of the main tet images (mixed precision, bfs.cu).
 // Polyhedra in flight between levels, in 32-wide tiles: element e's vertex v,

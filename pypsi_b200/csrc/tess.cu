@@ -6,6 +6,7 @@
 #include <algorithm>
 
 #include "psib_accum.cuh"
+#include "psib_adjoint.cuh"
 #include "psib_device.cuh"
 #include "psib_kernels.h"
 
@@ -1164,6 +1165,52 @@ cudaError_t launch_apply_records(const ApplyArgs& a, cudaStream_t s)
     } else {
         k_apply_runs<<<(unsigned)((a.nruns + 127) / 128), 128, 0, s>>>(a);
     }
+    return cudaGetLastError();
+}
+
+// ---- coefficients of the full adjoint (psib_adjoint.cuh) ----
+
+// Per voxel: the first variation of L per unit mass at (x, v) as a quadratic
+// about the voxel's means X, V:
+//   c0 = gM - (<gXX, XX> + <gVV, VV> + <gXV, XV>) / M,  cx = gX / M,  cv = gV / M,
+//   A = gXX / M,  B = gVV / M,  C = gXV / M;  then X and V.
+__global__ void k_adj_coeffs(AdjCoefArgs a)
+{
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < a.nvox;
+         v += (long long)gridDim.x * blockDim.x) {
+        double* c = a.coef + v * ADJ_NCOEF;
+        const double M = a.F[0][v];
+        if (!(M > 0.0)) {
+            for (int k = 0; k < ADJ_NCOEF; ++k) c[k] = 0.0;
+            continue;
+        }
+        const double iM = 1.0 / M;
+        double c0 = a.G[0] ? a.G[0][v] : 0.0;
+        const int off[6] = {0, 0, 0, 7, 25, 16}; // where A (xx), C (xv), B (vv) go
+        for (int f = 3; f < 6; ++f) {
+            double dot = 0.0;
+            for (int k = 0; k < 9; ++k) {
+                const double g = a.G[f] ? a.G[f][9 * v + k] : 0.0;
+                if (a.G[f]) dot += g * a.F[f][9 * v + k];
+                c[off[f] + k] = g * iM;
+            }
+            c0 -= dot * iM;
+        }
+        c[0] = c0;
+        for (int i = 0; i < 3; ++i) {
+            c[1 + i] = a.G[1] ? a.G[1][3 * v + i] * iM : 0.0;
+            c[4 + i] = a.G[2] ? a.G[2][3 * v + i] * iM : 0.0;
+            c[34 + i] = a.F[1] ? a.F[1][3 * v + i] : 0.0;
+            c[37 + i] = a.F[2] ? a.F[2][3 * v + i] : 0.0;
+        }
+    }
+}
+
+cudaError_t launch_adj_coeffs(const AdjCoefArgs& a, cudaStream_t s)
+{
+    if (a.nvox <= 0) return cudaSuccess;
+    const long long blocks = std::min<long long>((a.nvox + 255) / 256, 148ll * 32);
+    k_adj_coeffs<<<(unsigned)blocks, 256, 0, s>>>(a);
     return cudaGetLastError();
 }
 

@@ -47,3 +47,44 @@ def test_subset_fd_equals_whole_mesh_fd(oracle, kind):
         pm[p, ax] -= h
         whole = (loss(pp)[0] - loss(pm)[0]) / (2 * h)
         assert abs(sub - whole) <= 1e-6 * max(abs(whole), 1e-3), (p, ax, sub, whole)
+
+
+@pytest.mark.parametrize("kind", ["restatement", "reference"])
+def test_subset_fd_of_every_field_equals_whole_mesh_fd(oracle, kind):
+    """The finite differences of a loss on every field (tests/fd_fields.py):
+    re-depositing the elements around one particle, through per-voxel sums,
+    gives the same central difference as re-depositing the whole mesh, for
+    positions and velocities."""
+    if not oracle.available(kind):
+        pytest.skip(f"{kind} library not built")
+    from fd_fields import fd_grad, loss
+    from pypsi_b200.synth import zeldovich
+
+    pos, vel = zeldovich(6, 1.0, 78)
+    fields = ["x", "v", "xx", "xv", "vv"]
+    case = cases._block(pos, vel, 12, fields)
+    conn = cases.conn_of(case)
+    flat, vflat = pos.reshape(-1, 3), vel.reshape(-1, 3)
+
+    def dep(px, vx):
+        return oracle.voxelize(kind, n=case["n"], bounds=case["bounds"], pos=px, vel=vx, conn=conn,
+                               periodic_box=case["periodic_box"], fields=fields)
+
+    full = dep(flat, vflat)
+    rng = np.random.default_rng(2)
+    live = full["m"] > 0
+    h = 1e-5
+    for f in ["m"] + fields:
+        W = {f: rng.normal(size=full[f].shape) * live.reshape(live.shape + (1,) * (full[f].ndim - 3))}
+        for what, p, ax in [("pos", 5, 0), ("pos", 101, 2), ("vel", 37, 1), ("vel", 200, 0)]:
+            if f in ("m", "x", "xx") and what == "vel":
+                continue
+            sub = fd_grad(oracle, kind, case, conn, full, W, p, ax, block_elements_of(p, (6, 6, 6), True), what, h)
+            a, b = flat.copy(), vflat.copy()
+            (a if what == "pos" else b)[p, ax] += h
+            lp = loss(dep(a, b), W)
+            a, b = flat.copy(), vflat.copy()
+            (a if what == "pos" else b)[p, ax] -= h
+            lm = loss(dep(a, b), W)
+            whole = (lp - lm) / (2 * h)
+            assert abs(sub - whole) <= 1e-5 * max(abs(whole), 1e-3), (f, what, p, ax, sub, whole)
