@@ -74,6 +74,7 @@ def parse():
     ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="skip the compact 512-cutout and 256^3 -> 512^3 keys")
     ap.add_argument("--ann-n", type=int, default=64, help="ann: particles per side (smaller cases for profiling)")
     ap.add_argument("--ann-grid", type=int, default=128, help="ann: grid cells per side")
     ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c5", "ann", "loaders", "vdf", "quad"],
@@ -781,6 +782,10 @@ def time_fwd_bwd(x0, n_part, n_grid, steps, warmup, barrier):
 
 
 def run_c3(args):
+    print(json.dumps(c3_result(args, args.steps, args.warmup)), flush=True)
+
+
+def c3_result(args, steps, warmup):
     """512 independent cutouts, edge n log-uniform in [8, 64], Zel'dovich rms 1.5
     cells in their own periodic box of side 100, density on their own (2n)^3 grid:
     one psib_voxels_batch call against 512 separate psib_voxels calls."""
@@ -816,7 +821,7 @@ def run_c3(args):
                                    periodic_box=c["periodic_box"], precision="mixed", stream=stream) for c in cut]
 
     def timed(fn, steps):
-        for _ in range(args.warmup):
+        for _ in range(warmup):
             fn()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -828,11 +833,11 @@ def run_c3(args):
 
     ck = Clocks(local)
     ck.__enter__()
-    ms_b, st_b = timed(batch, args.steps)
+    ms_b, st_b = timed(batch, steps)
     ck.__exit__()
-    ms_s, _ = timed(separate, max(1, args.steps // 2))
+    ms_s, _ = timed(separate, max(1, steps // 2))
     line = {"metric": "tets/s, 512 uneven cutouts (n in [8,64], (2n)^3 grids, density), one batch call", "value":
-            tets / (ms_b * 1e-3), "unit": "tets/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            tets / (ms_b * 1e-3), "unit": "tets/s", "n_gpus": 1, "steps": steps, "warmup": warmup,
             "ms_per_step": ms_b, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
             "data": "synthetic: 512 seeded Zel'dovich lattices, rms 1.5 cells, element mass 1",
             "config": {"workload": "512 cutouts, edge log-uniform in [8,64], own box of side 100, (2n)^3 grids, m only",
@@ -842,10 +847,14 @@ def run_c3(args):
                                                          "edge_max": max(ns)},
             "gpu_launches": int(st_b[-1]["kernel_launches"]), "clocks": ck.summary()}
     capi.lib.psib_release_device_memory()
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def run_c5(args):
+    print(json.dumps(c5_result(args, args.steps, args.warmup)), flush=True)
+
+
+def c5_result(args, steps, warmup):
     """256^3 particles (rms 3 cells) onto 512^3, fields m and v, mixed precision,
     tets refined up to 2 levels where a (sub)cube's volume or edge stretches
     beyond 8x its Lagrangian value; total mass must be 256^3 to 1e-13."""
@@ -877,21 +886,21 @@ def run_c5(args):
     st = step()
     torch.cuda.synchronize()
     merr = mass_error(fields["m"].cpu().numpy(), n_part ** 3)
-    for _ in range(max(0, args.warmup - 1)):
+    for _ in range(max(0, warmup - 1)):
         step()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ck = Clocks(local)
     ck.__enter__()
     e0.record(stream)
-    stats = [step() for _ in range(args.steps)]
+    stats = [step() for _ in range(steps)]
     e1.record(stream)
     torch.cuda.synchronize()
     ck.__exit__()
-    ms = e0.elapsed_time(e1) / args.steps
+    ms = e0.elapsed_time(e1) / steps
     tets = st["tets"]
     line = {"metric": "tets/s @256³→512³ (stretch refinement 8x, 2 levels), mixed, fields m,v", "value": tets / (ms * 1e-3),
-            "unit": "tets/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "unit": "tets/s", "n_gpus": 1, "steps": steps, "warmup": warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
             "data": "synthetic: seeded Zel'dovich lattice 256^3, rms 3 cells, element mass 1",
             "config": {"workload": "256^3 particles -> 512^3 grid, fields m,v, stretch refinement 8x up to 2 levels",
@@ -901,8 +910,9 @@ def run_c5(args):
             "mass_err_mixed": merr, "stage_ms": {"tessellate_and_order": st["ms_tess"], "clip": st["ms_clip"],
                                                  "sort_and_apply": st["ms_final"]},
             "gpu_launches": int(sum(x["kernel_launches"] for x in stats)), "clocks": ck.summary()}
+    del fields
     capi.lib.psib_release_device_memory()
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def run_ours(args):
@@ -1183,6 +1193,13 @@ def run_ours(args):
 
         line["parity_vs_reference"] = parity_on_slab(ref_slab, deposit)
         capi.lib.psib_release_device_memory()
+    # the other workloads the target names, compact, on one GPU (--no-extra skips them)
+    if world == 1 and not args.no_extra and (n_part, n_grid) == (N_PART, N_GRID):
+        c3 = c3_result(args, 2, 1)
+        line["c3_batch"] = {k: c3[k] for k in ("value", "unit", "ms_per_step", "batch_over_separate",
+                                               "separate_calls", "work")}
+        c5 = c5_result(args, 2, 1)
+        line["c5_refined"] = {k: c5[k] for k in ("value", "unit", "ms_per_step", "mass_err_mixed", "work")}
     # the comparison the metric names, last so that the tail of the line shows it
     line["fp64"] = {"value": (1 if sharded else world) * tets_per_step / (ms_fp64 * 1e-3), "unit": "tets/s",
                     "ms_per_step": ms_fp64}

@@ -241,15 +241,16 @@ __device__ __forceinline__ bool link_cut_shared(uint32_t* nbs, int base, int nv)
     return true;
 }
 
-// Cut the staged polyhedron (positions in xI as [v*3+c][thread], links in
-// nbI; upper side = bits of um, s = cr - x[ax]) into element el of QL (lower
-// side) and eu of QU (upper side), with the vertex order and arithmetic of
-// cut_poly.
-__device__ __forceinline__ unsigned bfs_cut(int nv, uint32_t um, float cr, float sg, int ax, const float* xI,
-                                            const uint32_t* nbI, uint32_t* nbL, uint32_t* nbU, const PolyQueue& QL,
-                                            unsigned long long el, const PolyQueue& QU, unsigned long long eu,
-                                            bool keep_up, uint32_t cut_tag)
+// Cut the polyhedron at element eI of the input queue (positions read from
+// there, links staged in nbI; upper side = bits of um, s = cr - x[ax]) into
+// element el of QL (lower side) and eu of QU (upper side), with the vertex
+// order and arithmetic of cut_poly.
+__device__ __forceinline__ unsigned bfs_cut(int nv, uint32_t um, float cr, float sg, int ax, const PolyQueue& QI,
+                                            unsigned long long eI, const uint32_t* nbI, uint32_t* nbL, uint32_t* nbU,
+                                            const PolyQueue& QL, unsigned long long el, const PolyQueue& QU,
+                                            unsigned long long eu, bool keep_up, uint32_t cut_tag)
 {
+    auto X = [&](int v, int c) { return __ldg(&QI.x[qx(eI, v, c)]); };
     const uint32_t lmask = ((1u << nv) - 1u) & ~um;
     const int nl = __popc(lmask), nu = __popc(um);
     for (int v = 0; v < nv; ++v) {
@@ -259,7 +260,7 @@ __device__ __forceinline__ unsigned bfs_cut(int nv, uint32_t um, float cr, float
         const PolyQueue& Q = u ? QU : QL;
         const unsigned long long d = u ? eu : el;
         if (!u || keep_up)
-            for (int c = 0; c < 3; ++c) Q.x[qx(d, j, c)] = AT(xI, 3 * v + c);
+            for (int c = 0; c < 3; ++c) Q.x[qx(d, j, c)] = X(v, c);
         const uint32_t w = AT(nbI, v);
         uint32_t ow = 0xFFFFFFu | (w & ALL_TAGS);
         for (int k = 0; k < 3; ++k) {
@@ -291,10 +292,10 @@ __device__ __forceinline__ unsigned bfs_cut(int nv, uint32_t um, float cr, float
         {
             const int vn = nbget(w, np);
             if (nl + k >= MAXV || nu + k >= MAXV) return ST_OVERFLOW;
-            const float sc = sg * (cr - AT(xI, 3 * vc + ax)), sn = sg * (cr - AT(xI, 3 * vn + ax));
+            const float sc = sg * (cr - X(vc, ax)), sn = sg * (cr - X(vn, ax));
             const float iw = 1.0f / (sc - sn);
             for (int c = 0; c < 3; ++c) {
-                const float px = iw * (AT(xI, 3 * vn + c) * sc - AT(xI, 3 * vc + c) * sn);
+                const float px = iw * (X(vn, c) * sc - X(vc, c) * sn);
                 QL.x[qx(el, nl + k, c)] = px;
                 if (keep_up) QU.x[qx(eu, nu + k, c)] = px;
             }
@@ -320,13 +321,12 @@ __device__ __forceinline__ unsigned bfs_cut(int nv, uint32_t um, float cr, float
     return 0;
 }
 
-__global__ void __launch_bounds__(BB) k_bfs_level(BfsArgs a)
+__global__ void __launch_bounds__(BB, 7) k_bfs_level(BfsArgs a)
 {
     extern __shared__ uint32_t smem[];
     uint32_t* nbI = smem;
     uint32_t* nbL = smem + MAXV * BB;
     uint32_t* nbU = smem + 2 * MAXV * BB;
-    float* xI = (float*)(smem + 3 * MAXV * BB); // [v * 3 + c][thread]
     const int lane = threadIdx.x & 31;
     const long long warp = (long long)blockIdx.x * (BB / 32) + (threadIdx.x >> 5);
     const long long nwarp = (long long)gridDim.x * (BB / 32);
@@ -351,10 +351,8 @@ __global__ void __launch_bounds__(BB) k_bfs_level(BfsArgs a)
             t = a.in.item[e];
             const GridDev& g = grid_of(a.c, t);
             const double* fr = a.c.it.frame + (size_t)t * FRAME; // vertex 0: the origin of the FP32 positions
-            for (int v = 0; v < nv; ++v) {
-                AT(nbI, v) = a.in.nb[qn(e, v)];
-                for (int c = 0; c < 3; ++c) AT(xI, 3 * v + c) = a.in.x[qx(e, v, c)];
-            }
+            // the links are staged (the cut walks them); positions are read from the queue
+            for (int v = 0; v < nv; ++v) AT(nbI, v) = a.in.nb[qn(e, v)];
             win = a.in.win[e];
             for (int guard = 0; guard < 64; ++guard) {
                 if (win) {
@@ -368,7 +366,7 @@ __global__ void __launch_bounds__(BB) k_bfs_level(BfsArgs a)
                     sg = lo_side ? -1.0f : 1.0f;
                     um = 0;
                     for (int v = 0; v < nv; ++v)
-                        if (sg * (cr - AT(xI, 3 * v + ax)) < 0.0f) um |= 1u << v;
+                        if (sg * (cr - __ldg(&a.in.x[qx(e, v, ax)])) < 0.0f) um |= 1u << v;
                     if (um == 0) continue;                   // wholly inside this plane
                     if (um == (1u << nv) - 1u) { act = false; break; } // wholly outside
                     wcut = true;
@@ -388,7 +386,7 @@ __global__ void __launch_bounds__(BB) k_bfs_level(BfsArgs a)
                 cr = (float)(coord - fr[ax]);
                 um = 0;
                 for (int v = 0; v < nv; ++v)
-                    if (cr - AT(xI, 3 * v + ax) < 0.0f) um |= 1u << v;
+                    if (cr - __ldg(&a.in.x[qx(e, v, ax)]) < 0.0f) um |= 1u << v;
                 nlo = dmax / 2;
                 nup = dmax - nlo;
                 if (um == 0) { hi[ax] -= nup; continue; }
@@ -416,7 +414,7 @@ __global__ void __launch_bounds__(BB) k_bfs_level(BfsArgs a)
                 st |= ST_OVERFLOW;
             } else {
                 for (int v = 0; v < nv; ++v) {
-                    for (int c = 0; c < 3; ++c) a.leaf.x[qx(d, v, c)] = AT(xI, 3 * v + c);
+                    for (int c = 0; c < 3; ++c) a.leaf.x[qx(d, v, c)] = __ldg(&a.in.x[qx(e, v, c)]);
                     a.leaf.nb[qn(d, v)] = AT(nbI, v);
                 }
                 a.leaf.nv[d] = (uint8_t)nv;
@@ -435,7 +433,7 @@ __global__ void __launch_bounds__(BB) k_bfs_level(BfsArgs a)
                 st |= ST_OVERFLOW;
             } else {
                 const unsigned e2 =
-                    bfs_cut(nv, um, cr, 1.0f, ax, xI, nbI, nbL, nbU, QL, el, QU, eu, true, axis_tag(ax));
+                    bfs_cut(nv, um, cr, 1.0f, ax, a.in, e, nbI, nbL, nbU, QL, el, QU, eu, true, axis_tag(ax));
                 if (e2) {
                     st |= e2;
                     QL.nv[el] = 0; // downstream kernels skip these
@@ -458,7 +456,8 @@ __global__ void __launch_bounds__(BB) k_bfs_level(BfsArgs a)
             if (el >= QL.cap) {
                 st |= ST_OVERFLOW;
             } else {
-                const unsigned e2 = bfs_cut(nv, um, cr, sg, ax, xI, nbI, nbL, nbU, QL, el, QL, el, false, axis_tag(ax));
+                const unsigned e2 =
+                    bfs_cut(nv, um, cr, sg, ax, a.in, e, nbI, nbL, nbU, QL, el, QL, el, false, axis_tag(ax));
                 if (e2) {
                     st |= e2;
                     QL.nv[el] = 0;
@@ -670,7 +669,7 @@ cudaError_t launch_bfs_finalize(const BfsArgs& a, long long nitems, int num_sms,
 
 // ---- launchers ----
 
-static constexpr size_t LEVEL_SMEM = 6 * MAXV * BB * sizeof(uint32_t);
+static constexpr size_t LEVEL_SMEM = 3 * MAXV * BB * sizeof(uint32_t); // links of the cut polyhedron and its children
 static constexpr size_t LEAF_SMEM = MAXV * BB * (sizeof(uint32_t) + 3 * sizeof(double));
 
 // resident blocks per SM of each kernel (one full wave of grid-stride blocks)
