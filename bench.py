@@ -810,11 +810,13 @@ def c3_result(args, steps, warmup):
     tets = sum(6 * n ** 3 for n in ns)
     stream = torch.cuda.current_stream()
 
-    # the queue capacity of this batch, picked by timing (the batch is deposited many times)
-    cap = capi.autotune_batch(cut, precision="mixed", repeats=1)
+    # the queue capacity and work-order tile of this batch, picked by timing (the batch is
+    # deposited many times)
+    tune = capi.autotune_batch(cut, precision="mixed", repeats=1)
+    kw = {"queue_voxels": tune["queue_voxels"], "order_cell_bits": tune["order_cell_bits"]}
 
     def batch():
-        return capi.voxels_batch_device(cut, precision="mixed", stream=stream, queue_voxels=cap)
+        return capi.voxels_batch_device(cut, precision="mixed", stream=stream, **kw)
 
     def separate():
         return [capi.voxels_device(c["fields"], c["n"], c["bounds"], c["pos"], block_dims=c["block_dims"],
@@ -836,6 +838,11 @@ def c3_result(args, steps, warmup):
     ms_b, st_b = timed(batch, steps)
     ck.__exit__()
     ms_s, _ = timed(separate, max(1, steps // 2))
+    # the same batch recorded once as a CUDA graph (capture mode: no host synchronisation), replayed
+    graph = capi.capture_batch(cut, precision="mixed", **kw)
+    ms_g, _ = timed(graph.replay, steps)
+    graph_status = capi.capture_status()
+    del graph
     line = {"metric": "tets/s, 512 uneven cutouts (n in [8,64], (2n)^3 grids, density), one batch call", "value":
             tets / (ms_b * 1e-3), "unit": "tets/s", "n_gpus": 1, "steps": steps, "warmup": warmup,
             "ms_per_step": ms_b, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
@@ -843,7 +850,9 @@ def c3_result(args, steps, warmup):
             "config": {"workload": "512 cutouts, edge log-uniform in [8,64], own box of side 100, (2n)^3 grids, m only",
                        "precision": "mixed"},
             "separate_calls": {"value": tets / (ms_s * 1e-3), "ms_per_step": ms_s, "calls": 512},
-            "batch_over_separate": ms_s / ms_b, "queue_voxels_autotuned": cap, "work": {"tets": tets, "cutouts": 512, "edge_min": min(ns),
+            "batch_over_separate": ms_s / ms_b,
+            "graph_replay": {"value": tets / (ms_g * 1e-3), "ms_per_step": ms_g, "status": graph_status},
+            "autotuned": {"queue_voxels": kw["queue_voxels"], "order_cell_bits": kw["order_cell_bits"]}, "work": {"tets": tets, "cutouts": 512, "edge_min": min(ns),
                                                          "edge_max": max(ns)},
             "gpu_launches": int(st_b[-1]["kernel_launches"]), "clocks": ck.summary()}
     capi.lib.psib_release_device_memory()
@@ -1197,7 +1206,7 @@ def run_ours(args):
     if world == 1 and not args.no_extra and (n_part, n_grid) == (N_PART, N_GRID):
         c3 = c3_result(args, 2, 1)
         line["c3_batch"] = {k: c3[k] for k in ("value", "unit", "ms_per_step", "batch_over_separate",
-                                               "separate_calls", "work")}
+                                               "separate_calls", "graph_replay", "autotuned", "work")}
         c5 = c5_result(args, 2, 1)
         line["c5_refined"] = {k: c5[k] for k in ("value", "unit", "ms_per_step", "mass_err_mixed", "work")}
     # the comparison the metric names, last so that the tail of the line shows it

@@ -137,6 +137,19 @@ typedef struct {
     long long queue_voxels; /* mixed precision: tets walked per pass, bounded by the sum of their index-box
                                volumes (the size of every polyhedron queue); 0: automatic (up to 64M, within
                                35% of the free device memory) */
+    int capture;       /* 0: a plain call.  1 (plan): a plain call (mixed precision, deterministic = 0,
+                          device memory) that also sizes every buffer for calls like it, with room for
+                          25% more tet images, and records their launch plan on this device.
+                          2 (capture): such a call with no host synchronisation and no allocation, so
+                          that the caller can record it in a CUDA graph and replay it: counts stay on
+                          the device, a device-side planner lays out the passes of the walk, and
+                          unused passes fall through.  It needs a plan call with the same grids,
+                          meshes and fields before it, returns before the work is done and reports
+                          failures through psib_capture_status; stats are not filled. */
+    int order_cell_bits; /* mixed precision: the tet images of one box volume are walked in the order of a
+                            coarse grid of 2^b cells (b bits split over the axes, x first: 7 gives
+                            8 x 4 x 4 cells), so that the atomic sums of neighbouring fragments stay in
+                            L2; 0: 7, -1: no spatial order, 1..7: b.  capi.autotune_batch picks it. */
 } psib_options;
 
 /* Deposit the mesh's tets on the grid: the density branch of psi_voxels
@@ -198,6 +211,13 @@ int psib_voxels_adjoint(const psib_grid *grad, const psib_mesh *mesh, double ref
 int psib_voxels_adjoint_fields(const psib_grid *grad, const psib_grid *fwd, const psib_mesh *mesh,
                                double refine_tolerance, int refine_max_lvl, double *grad_pos, double *grad_vel,
                                double *grad_mass, const psib_options *opt);
+
+/* The status the work of capture-mode calls (options->capture = 2) left on the
+ * current device, read after their graph has run (this synchronises the
+ * device): PSIB_OK, or the PSIB_ERR_* code of the first failure -- e.g.
+ * PSIB_ERR_OVERFLOW when the tet images outgrew the planned buffers.  Clears
+ * it.  It has no counterpart in the reference. */
+int psib_capture_status(void);
 
 /* Message for the last failure on this thread ("" if none). */
 const char *psib_last_error(void);

@@ -46,7 +46,8 @@ class Stats(C.Structure):
 class Options(C.Structure):
     _fields_ = [("precision", C.c_int), ("deterministic", C.c_int), ("memory", C.c_int), ("device", C.c_int),
                 ("stream", C.c_void_p), ("stats", C.POINTER(Stats)), ("refine_mode", C.c_int),
-                ("refine_cell", C.c_double * 3), ("queue_voxels", C.c_longlong)]
+                ("refine_cell", C.c_double * 3), ("queue_voxels", C.c_longlong), ("capture", C.c_int),
+                ("order_cell_bits", C.c_int)]
 
 
 lib.psib_voxels.argtypes = [C.POINTER(Grid), C.POINTER(Mesh), C.c_int, C.c_double, C.c_int, C.POINTER(Options)]
@@ -68,6 +69,7 @@ lib.psib_voxels_adjoint_fields.argtypes = [C.POINTER(Grid), C.POINTER(Grid), C.P
 lib.psib_voxels_adjoint_fields.restype = C.c_int
 lib.psib_measure_fma_peak.argtypes = [C.c_int, C.POINTER(C.c_double)]
 lib.psib_measure_fma_peak.restype = C.c_int
+lib.psib_capture_status.restype = C.c_int
 lib.psib_last_error.restype = C.c_char_p
 lib.psib_release_device_memory.restype = C.c_int
 
@@ -119,10 +121,11 @@ MODES = {"density": 0, "annihilation": 1}
 
 def voxels(grid: Grid, mesh: Mesh, precision=PSIB_FP64, deterministic=False, memory=PSIB_DEVICE, stream=None,
            refine_tolerance=1.0, refine_max_lvl=0, refine_criterion="midpoint", refine_cell=None,
-           mode="density") -> dict:
+           mode="density", order_cell_bits=0) -> dict:
     st = Stats()
     o = Options(precision=precision, deterministic=int(bool(deterministic)), memory=memory, device=-1,
-                stream=stream, stats=C.pointer(st), refine_mode=REFINE[refine_criterion])
+                stream=stream, stats=C.pointer(st), refine_mode=REFINE[refine_criterion],
+                order_cell_bits=int(order_cell_bits))
     if refine_cell is not None:
         o.refine_cell[:] = [float(v) for v in refine_cell]
     rc = lib.psib_voxels(C.byref(grid), C.byref(mesh), MODES[mode], float(refine_tolerance), int(refine_max_lvl),
@@ -134,7 +137,8 @@ def voxels(grid: Grid, mesh: Mesh, precision=PSIB_FP64, deterministic=False, mem
 
 def voxels_device(fields: dict, n, bounds, pos, vel=None, mass=None, connectivity=None, block_dims=None,
                   periodic_box=None, precision="fp64", deterministic=False, refine_tolerance=1.0, refine_max_lvl=0,
-                  stream=None, refine_criterion="midpoint", refine_cell=None, mode="density") -> dict:
+                  stream=None, refine_criterion="midpoint", refine_cell=None, mode="density",
+                  order_cell_bits=0) -> dict:
     """Deposit on device-resident torch tensors (mode 'density', or
     'annihilation': m gains the integral of rho_0 rho_1 over overlapping tets).
 
@@ -151,7 +155,8 @@ def voxels_device(fields: dict, n, bounds, pos, vel=None, mass=None, connectivit
     m = mesh_from_tensors(pos, vel, mass, connectivity, block_dims, periodic_box)
     s = stream if stream is not None else torch.cuda.current_stream()
     return voxels(g, m, PRECISIONS[precision], deterministic, PSIB_DEVICE,
-                  C.c_void_p(s.cuda_stream), refine_tolerance, refine_max_lvl, refine_criterion, refine_cell, mode)
+                  C.c_void_p(s.cuda_stream), refine_tolerance, refine_max_lvl, refine_criterion, refine_cell, mode,
+                  order_cell_bits)
 
 
 def mesh_from_tensors(pos, vel=None, mass=None, connectivity=None, block_dims=None, periodic_box=None) -> Mesh:
@@ -221,7 +226,7 @@ def adjoint_fields_device(grads: dict, fwd: dict, n, bounds, pos, grad_pos, vel=
 
 def voxels_batch_device(cutouts: list, precision="fp64", refine_tolerance=1.0, refine_max_lvl=0,
                         refine_criterion="midpoint", refine_cell=None, stream=None, queue_voxels=0,
-                        deterministic=False) -> dict:
+                        deterministic=False, capture=0, order_cell_bits=0) -> dict:
     """Many independent deposits in one pass (psib_voxels_batch).
 
     cutouts: dicts with the arguments of voxels_device -- fields, n, bounds,
@@ -242,7 +247,8 @@ def voxels_batch_device(cutouts: list, precision="fp64", refine_tolerance=1.0, r
     st = Stats()
     o = Options(precision=PRECISIONS[precision], deterministic=int(bool(deterministic)), memory=PSIB_DEVICE,
                 device=-1, stream=C.c_void_p(s.cuda_stream), stats=C.pointer(st),
-                refine_mode=REFINE[refine_criterion], queue_voxels=int(queue_voxels))
+                refine_mode=REFINE[refine_criterion], queue_voxels=int(queue_voxels), capture=int(capture),
+                order_cell_bits=int(order_cell_bits))
     if refine_cell is not None:
         o.refine_cell[:] = [float(v) for v in refine_cell]
     rc = lib.psib_voxels_batch(grids, meshes, nb, 0, float(refine_tolerance), int(refine_max_lvl), C.byref(o))
@@ -251,32 +257,58 @@ def voxels_batch_device(cutouts: list, precision="fp64", refine_tolerance=1.0, r
     return st.as_dict()
 
 
-def autotune_batch(cutouts: list, candidates=(8 << 20, 16 << 20, 32 << 20, 64 << 20), precision="mixed",
-                   repeats=2, **kw) -> int:
-    """Pick the queue capacity (psib_options.queue_voxels) for a batch that will
-    be deposited many times (the same cutouts with new positions, say).
+def capture_status() -> int:
+    """psib_capture_status: the status that capture-mode calls left on the current device (0: ok)."""
+    return lib.psib_capture_status()
 
-    Each candidate is timed with CUDA events over `repeats` batch calls after
-    one warm-up call; the fields of the cutouts are zeroed afterwards.  Returns
-    the fastest capacity, to pass as voxels_batch_device(queue_voxels=...)."""
+
+def capture_batch(cutouts: list, precision="mixed", queue_voxels=0, **kw):
+    """A batch call recorded in a torch CUDA graph: one plan call (options.capture = 1,
+    which also deposits once), then one capture-mode call (capture = 2) recorded
+    and returned as a torch.cuda.CUDAGraph.  graph.replay() repeats the deposit on
+    the cutouts' current particle arrays and fields (it adds to the fields, as a
+    call does); check capture_status() after replays."""
     import torch
 
-    best, best_ms = 0, float("inf")
+    voxels_batch_device(cutouts, precision=precision, queue_voxels=queue_voxels, capture=1, **kw)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        voxels_batch_device(cutouts, precision=precision, queue_voxels=queue_voxels, capture=2,
+                            stream=torch.cuda.current_stream(), **kw)
+    return g
+
+
+def autotune_batch(cutouts: list, candidates=(8 << 20, 16 << 20, 32 << 20, 64 << 20), precision="mixed",
+                   repeats=2, tiles=(7, 5, 3, -1), **kw) -> dict:
+    """Pick the launch parameters of a batch that will be deposited many times (the
+    same cutouts with new positions, say): the queue capacity
+    (psib_options.queue_voxels) and the spatial tile of the work order
+    (psib_options.order_cell_bits: 2^b coarse cells over each grid).
+
+    Each pair is timed with CUDA events over `repeats` batch calls after one
+    warm-up call; the fields of the cutouts are zeroed afterwards.  Returns
+    {"queue_voxels": ..., "order_cell_bits": ..., "ms": ...}, whose first two
+    entries go to voxels_batch_device."""
+    import torch
+
+    best = {"queue_voxels": 0, "order_cell_bits": 0, "ms": float("inf")}
     stream = torch.cuda.current_stream()
     for cap in candidates:
-        try:
-            voxels_batch_device(cutouts, precision=precision, queue_voxels=cap, **kw)
-        except PsibError:
-            continue  # e.g. not enough memory for this capacity
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(repeats):
-            voxels_batch_device(cutouts, precision=precision, queue_voxels=cap, **kw)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / repeats
-        if ms < best_ms:
-            best, best_ms = cap, ms
+        for bits in tiles:
+            try:
+                voxels_batch_device(cutouts, precision=precision, queue_voxels=cap, order_cell_bits=bits, **kw)
+            except PsibError:
+                continue  # e.g. not enough memory for this capacity
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(repeats):
+                voxels_batch_device(cutouts, precision=precision, queue_voxels=cap, order_cell_bits=bits, **kw)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / repeats
+            if ms < best["ms"]:
+                best = {"queue_voxels": cap, "order_cell_bits": bits, "ms": ms}
     for c in cutouts:
         for t in c["fields"].values():
             t.zero_()

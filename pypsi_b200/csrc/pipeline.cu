@@ -132,6 +132,16 @@ struct Ctx {
     DevBuf q_in, q_cnt, q_off, q_key, q_key_s, q_out, s_cnt, s_off, s_offs, s_rho, s_vel;
     cudaGraphExec_t pass_exec = nullptr; // one breadth-first pass as a CUDA graph
     PassKey pass_key{};                  // the arguments it was recorded with
+    // the capture mode: the sizes a plan call found, and the page-locked copy of the batch tables
+    struct Plan {
+        bool valid = false;
+        long long nelem = 0, nvox = 0, cap_items = 0, ntiles = 0, tiles = 0, qcap = 0;
+        int nbatch = 0, max_passes = 0, stride = 0, precision = -1;
+        unsigned flags = 0;
+        size_t btab_bytes = 0;
+    } plan;
+    void* btab_host = nullptr;
+    size_t btab_host_n = 0;
     std::vector<DevBuf*> all()
     {
         return {&hpos, &hgpos, &hgmass, &hvel, &hmass, &hconn, &hfield[0], &hfield[1], &hfield[2], &hfield[3], &hfield[4],
@@ -176,7 +186,7 @@ int get_ctx(int dev, Ctx** out)
 
 // small device block layout (unsigned long long words)
 enum { S_STATUS = 0, S_CNT = 1 /* 3 words */, S_TESS = 4 /* 2 */, S_HEAD = 8 /* 4 */, S_RECN = 12, S_NDEEP = 13,
-       S_DFS = 14, S_BYTES = 15, S_PASS = 6, S_FIX = 7, S_WORDS = 16 };
+       S_DFS = 14, S_BYTES = 15, S_PASS = 6, S_FIX = 7, S_NMAIN = 16, S_NITEMS = 17, S_WORDS = 18 };
 
 // Histogram of the sorted footprint keys: lanes holding equal keys (most of a
 // warp, as the keys are sorted) add with one atomic.
@@ -211,6 +221,103 @@ __global__ void k_iota_u(unsigned* o, long long n)
 {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         o[i] = (unsigned)i;
+}
+
+// ---- capture mode: counts and the pass plan on the device ----
+
+// Entries [*total, cap) of a fixed-size item buffer hold no image: their key sorts last.
+__global__ void k_pad_keys(uint16_t* key, const long long* total, long long cap)
+{
+    const long long t0 = *total;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < cap; i += (long long)gridDim.x * blockDim.x)
+        if (i >= t0) key[i] = (uint16_t)KEY_PAD;
+}
+
+// Counts of the main images (key < KEY_DEEP) and the deep-tree kernel's (KEY_DEEP) among cap keys;
+// sorted, they are [0, nmain) and [nmain, nmain + ndeep).  The two words start at zero.
+__global__ void k_key_classes(const uint16_t* key, long long cap, unsigned long long* nmain, unsigned long long* ndeep)
+{
+    unsigned m = 0, d = 0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < cap; i += (long long)gridDim.x * blockDim.x) {
+        const unsigned k = key[i];
+        m += k < KEY_DEEP;
+        d += k == KEY_DEEP;
+    }
+    m = __reduce_add_sync(0xFFFFFFFFu, m);
+    d = __reduce_add_sync(0xFFFFFFFFu, d);
+    if ((threadIdx.x & 31) == 0) {
+        if (m) atomicAdd(nmain, (unsigned long long)m);
+        if (d) atomicAdd(ndeep, (unsigned long long)d);
+    }
+}
+
+// Histogram of the volume classes (key >> KEY_CELL_BITS) of the first *n sorted keys (n on the
+// device).  The keys sort by class first, so the classes give the passes as the keys would.
+__global__ void k_key_hist_dev(const uint16_t* key, const unsigned long long* n_dev, unsigned* hist)
+{
+    const long long n = (long long)*n_dev;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long n32 = (n + 31) / 32 * 32;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n32; i += stride) {
+        const bool act = i < n;
+        const unsigned k = act ? (unsigned)key[i] >> KEY_CELL_BITS : 0x10000u;
+        const unsigned peers = __match_any_sync(0xFFFFFFFFu, k);
+        if (act && (threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&hist[k], (unsigned)__popc(peers));
+    }
+}
+
+// The host planner of bfs_clip on one thread: images in key order, a pass takes images while the
+// sum of their box volumes stays within cap.  hist counts the volume classes of the main images;
+// passes[0..max_passes] (unused passes empty at nmain).
+__global__ void k_plan_passes(const unsigned* hist, long long cap, long long* passes, int max_passes,
+                              const unsigned long long* nmain, unsigned* status)
+{
+    if (blockIdx.x || threadIdx.x) return;
+    const long long n = (long long)*nmain;
+    int p = 0;
+    long long cur = 0, pos = 0;
+    passes[0] = 0;
+    for (int k = 0; k < (int)(KEY_DEEP >> KEY_CELL_BITS); ++k) {
+        long long cnt = hist[k];
+        const long long vol = key_volume((unsigned)k << KEY_CELL_BITS);
+        while (cnt > 0) {
+            long long take = (cap - cur) / vol;
+            if (take > cnt) take = cnt;
+            if (take == 0) {
+                if (cur == 0 || p + 1 >= max_passes) { // one image above the capacity, or too many passes
+                    atomicOr(status, ST_OVERFLOW);
+                    for (int q = p + 1; q <= max_passes; ++q) passes[q] = n;
+                    return;
+                }
+                passes[++p] = pos;
+                cur = 0;
+                continue;
+            }
+            cur += take * vol;
+            pos += take;
+            cnt -= take;
+        }
+    }
+    for (int q = p + 1; q <= max_passes; ++q) passes[q] = n;
+}
+
+// The correction pass: one pass over the listed images, whose box volumes must fit the queues.
+__global__ void k_plan_list(const uint16_t* keys, const unsigned long long* n_dev, long long cap, long long* passes,
+                            int max_passes, unsigned* status)
+{
+    const long long n = (long long)*n_dev;
+    long long vol = 0;
+    for (long long i = threadIdx.x; i < n; i += blockDim.x) vol += key_volume(keys[i]);
+    __shared__ unsigned long long sum;
+    if (threadIdx.x == 0) sum = 0;
+    __syncthreads();
+    atomicAdd(&sum, (unsigned long long)vol);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if ((long long)sum > cap) atomicOr(status, ST_OVERFLOW);
+        passes[0] = 0;
+        for (int q = 1; q <= max_passes; ++q) passes[q] = n;
+    }
 }
 
 size_t round_up(size_t b) { return (b + 15) & ~(size_t)15; }
@@ -248,12 +355,25 @@ struct Call {
     const psib_grid* grids;
     const psib_mesh* meshes;
     const double* refine_cell_given;
+    int capture;              // options.capture: 0 plain, 1 plan, 2 capture (run_capture)
+    int order_cell_bits;      // options.order_cell_bits: coarse cells of the footprint key
     // adjoint call: F[0] holds dL/dm (or adj_coef the full adjoint's per-voxel coefficients);
     // gradients accumulate into these
     bool adjoint;
     double *gpos, *gmass, *gvel;
     const double* adj_coef;
 };
+
+// Bits of the footprint key's coarse cell per axis: b bits shared out x, y, z, x, ...
+// (0 means the default 7 = 8 x 4 x 4 cells; negative means no spatial order).
+void order_cells(int b, int* cb)
+{
+    cb[0] = cb[1] = cb[2] = 0;
+    if (b == 0) b = KEY_CELL_BITS;
+    if (b < 0) return;
+    if (b > KEY_CELL_BITS) b = KEY_CELL_BITS;
+    for (int i = 0; i < b; ++i) ++cb[i % 3];
+}
 
 int check_status(Call& c, unsigned long long* small_host)
 {
@@ -287,10 +407,50 @@ int leave_own_stream(Ctx& C, cudaStream_t user)
     return PSIB_OK;
 }
 
+// levels of one breadth-first pass: the bisection (at most DMAX_MAIN cuts) and up to 6 window planes
+constexpr int NLEV = DMAX_MAIN + 6;
+// per pass: level-queue counts [0, NLEV] and leaf-queue counts [NLEV + 1, 2 NLEV + 1]
+constexpr int NCNT = 2 * NLEV + 2;
+
+// One breadth-first pass: reset the per-level counts, then init, leaf, and NLEV x (level, leaf),
+// then advance the pass counter.  The pass it walks is read from the device pass table.
+cudaError_t bfs_pass(const BfsArgs& ba, const PolyQueue* Q, unsigned long long* cq, int grid, cudaStream_t s)
+{
+    unsigned long long* cl = cq + NLEV + 1;
+    cudaError_t e = cudaMemsetAsync(cq, 0, NCNT * sizeof(unsigned long long), s);
+    BfsArgs b = ba;
+    b.out = Q[0];
+    b.out.count = &cq[0];
+    b.leaf = Q[2];
+    b.leaf.count = &cl[0];
+    if (e == cudaSuccess) e = launch_bfs_init(b, grid, s);
+    if (e == cudaSuccess) e = launch_bfs_leaf(b, grid, s);
+    int ia = 0;
+    for (int lvl = 0; lvl < NLEV && e == cudaSuccess; ++lvl) {
+        b.in = Q[ia];
+        b.in.count = &cq[lvl];
+        b.out = Q[1 - ia];
+        b.out.count = &cq[lvl + 1];
+        b.leaf.count = &cl[lvl + 1];
+        b.last = lvl == NLEV - 1;
+        e = launch_bfs_level(b, grid, s);
+        if (e == cudaSuccess) e = launch_bfs_leaf(b, grid, s);
+        ia = 1 - ia;
+    }
+    if (e == cudaSuccess) e = launch_bfs_advance(b, s);
+    return e;
+}
+
+// The queue capacity (in 32-wide tiles) and pass count a breadth-first walk used; the capture
+// mode sizes its fixed launch sequence from them.
+struct BfsSizes {
+    long long tiles = 0, cap = 0, npass = 0;
+};
+
 // keys: the footprint keys of the queue positions [0, nmain), ascending.
 int bfs_clip(Ctx& C, ClipArgs& ca, long long nmain, long long nitems, unsigned long long* sm, int clip_grid,
              int clip_block, long long queue_voxels, bool batch, cudaStream_t st, long long& launches,
-             long long& klaunch, const uint16_t* keys)
+             long long& klaunch, const uint16_t* keys, BfsSizes* sizes = nullptr)
 {
     RET(ensure(C.hist, 65536 * sizeof(unsigned)));
     CK(cudaMemsetAsync(C.hist.p, 0, 65536 * sizeof(unsigned), st));
@@ -317,7 +477,7 @@ int bfs_clip(Ctx& C, ClipArgs& ca, long long nmain, long long nitems, unsigned l
     cap = std::max<long long>(env_ll("PSIB_BFS_CAP", cap), 1024);
     std::vector<long long> qb{0};
     long long cur = 0, pos = 0;
-    for (int k = 0; k < 0xFFFF; ++k) {
+    for (int k = 0; k < (int)KEY_DEEP; ++k) {
         long long cnt = hist[k];
         const long long vol = key_volume((unsigned)k);
         while (cnt > 0) {
@@ -339,7 +499,7 @@ int bfs_clip(Ctx& C, ClipArgs& ca, long long nmain, long long nitems, unsigned l
     {
         size_t p = 0;
         long long acc = 0, at = 0;
-        for (int k = 0; k < 0xFFFF && p + 1 < qb.size(); ++k) {
+        for (int k = 0; k < (int)KEY_DEEP && p + 1 < qb.size(); ++k) {
             const long long vol = key_volume((unsigned)k);
             for (long long cnt = hist[k]; cnt > 0;) {
                 const long long take = std::min(cnt, qb[p + 1] - at);
@@ -368,13 +528,8 @@ int bfs_clip(Ctx& C, ClipArgs& ca, long long nmain, long long nitems, unsigned l
                          (unsigned long long)tiles * 32};
     }
     RET(ensure(C.dfs_list, (size_t)std::max<long long>(nmain, 1) * sizeof(int)));
-    // levels: the bisection (at most DMAX_MAIN cuts) and up to 6 window planes
-    constexpr int NLEV = DMAX_MAIN + 6;
-    // per pass: level-queue counts [0, NLEV] and leaf-queue counts [NLEV + 1, 2 NLEV + 1]
-    constexpr int NCNT = 2 * NLEV + 2;
     RET(ensure(C.bfs_cnt, NCNT * sizeof(unsigned long long)));
     unsigned long long* cq = C.bfs_cnt.as<unsigned long long>();
-    unsigned long long* cl = cq + NLEV + 1;
     CK(cudaMemsetAsync(&sm[S_DFS], 0, 8, st));
 
     BfsArgs ba = {};
@@ -400,30 +555,7 @@ int bfs_clip(Ctx& C, ClipArgs& ca, long long nmain, long long nitems, unsigned l
     // pass (and in later calls whose arguments are the same); plain launches if the graph cannot
     // be made.  Single calls launch directly: measured at 128^3 -> 256^3 the replay was 3 %
     // slower, and for 512 cutouts no faster (PSIB_BFS_GRAPH=0/1 overrides).
-    auto pass = [&](cudaStream_t s) -> cudaError_t {
-        cudaError_t e = cudaMemsetAsync(cq, 0, NCNT * sizeof(unsigned long long), s);
-        BfsArgs b = ba;
-        b.out = Q[0];
-        b.out.count = &cq[0];
-        b.leaf = Q[2];
-        b.leaf.count = &cl[0];
-        if (e == cudaSuccess) e = launch_bfs_init(b, grid, s);
-        if (e == cudaSuccess) e = launch_bfs_leaf(b, grid, s);
-        int ia = 0;
-        for (int lvl = 0; lvl < NLEV && e == cudaSuccess; ++lvl) {
-            b.in = Q[ia];
-            b.in.count = &cq[lvl];
-            b.out = Q[1 - ia];
-            b.out.count = &cq[lvl + 1];
-            b.leaf.count = &cl[lvl + 1];
-            b.last = lvl == NLEV - 1;
-            e = launch_bfs_level(b, grid, s);
-            if (e == cudaSuccess) e = launch_bfs_leaf(b, grid, s);
-            ia = 1 - ia;
-        }
-        if (e == cudaSuccess) e = launch_bfs_advance(b, s);
-        return e;
-    };
+    auto pass = [&](cudaStream_t s) -> cudaError_t { return bfs_pass(ba, Q, cq, grid, s); };
     bool graphed = false;
     if (env_ll("PSIB_BFS_GRAPH", batch ? 1 : 0) != 0) {
         PassKey key{};
@@ -461,6 +593,11 @@ int bfs_clip(Ctx& C, ClipArgs& ca, long long nmain, long long nitems, unsigned l
         for (long long p = 0; p < npass; ++p) CK(pass(st));
     klaunch += (3 + 2 * NLEV) * npass;
     launches += (2 + 2 * NLEV) * npass;
+    if (sizes) {
+        sizes->tiles = (long long)tiles;
+        sizes->cap = cap;
+        sizes->npass = npass;
+    }
     CK(launch_bfs_finalize(ba, nitems, C.num_sms, st));
     klaunch++;
     unsigned long long ndfs = 0;
@@ -574,6 +711,36 @@ int correct_masses(Ctx& C, const ClipArgs& ca, long long nitems, unsigned long l
                     klaunch, C.fix_keys_s.as<uint16_t>());
 }
 
+// The batch tables a batch call's kernels read: every cutout's mesh and grid, the element and
+// voxel offsets, and the field pointers, laid out in one host buffer.
+struct BatchTables {
+    std::vector<char> h;
+    size_t o_mesh = 0, o_grid = 0, o_eoff = 0, o_voff = 0, o_fptr = 0;
+};
+int batch_tables(const Call& c, const std::vector<long long>& eoff, const std::vector<unsigned long long>& voff,
+                 BatchTables& t)
+{
+    const int nb = c.nbatch;
+    t.o_mesh = 0;
+    t.o_grid = round_up(t.o_mesh + nb * sizeof(MeshDev));
+    t.o_eoff = round_up(t.o_grid + nb * sizeof(GridDev));
+    t.o_voff = round_up(t.o_eoff + (nb + 1) * 8);
+    t.o_fptr = round_up(t.o_voff + (nb + 1) * 8);
+    t.h.assign(round_up(t.o_fptr + 6 * nb * sizeof(double*)), 0);
+    for (int b = 0; b < nb; ++b) {
+        const psib_mesh& mb = c.meshes[b];
+        double lag[3] = {0.0, 0.0, 0.0};
+        if (c.refine_mode == PSIB_REFINE_STRETCH) RET(stretch_cell(mb, c.refine_cell_given, lag));
+        ((MeshDev*)(t.h.data() + t.o_mesh))[b] =
+            mesh_dev(mb, c.grids[b], mb.pos, mb.vel, mb.mass, mb.connectivity, c.reftol, lag);
+        ((GridDev*)(t.h.data() + t.o_grid))[b] = grid_dev(c.grids[b]);
+        for (int f = 0; f < 6; ++f) ((double**)(t.h.data() + t.o_fptr))[6 * b + f] = c.grids[b].fields[f];
+    }
+    memcpy(t.h.data() + t.o_eoff, eoff.data(), (nb + 1) * 8);
+    memcpy(t.h.data() + t.o_voff, voff.data(), (nb + 1) * 8);
+    return PSIB_OK;
+}
+
 int run_device(Call& c)
 {
     if (c.mode == PSIB_MODE_ANNIHILATION) return run_annihilation(c);
@@ -628,30 +795,26 @@ int run_device(Call& c)
     const unsigned long long* d_voff = nullptr;
     double* const* d_fptr = nullptr;
     if (batch) {
-        const int nb = c.nbatch;
-        const size_t o_mesh = 0, o_grid = round_up(o_mesh + nb * sizeof(MeshDev)),
-                     o_eoff = round_up(o_grid + nb * sizeof(GridDev)), o_voff = round_up(o_eoff + (nb + 1) * 8),
-                     o_fptr = round_up(o_voff + (nb + 1) * 8), total = round_up(o_fptr + 6 * nb * sizeof(double*));
-        std::vector<char> h(total, 0);
-        for (int b = 0; b < nb; ++b) {
-            const psib_mesh& mb = c.meshes[b];
-            double lag[3] = {0.0, 0.0, 0.0};
-            if (c.refine_mode == PSIB_REFINE_STRETCH) RET(stretch_cell(mb, c.refine_cell_given, lag));
-            ((MeshDev*)(h.data() + o_mesh))[b] =
-                mesh_dev(mb, c.grids[b], mb.pos, mb.vel, mb.mass, mb.connectivity, c.reftol, lag);
-            ((GridDev*)(h.data() + o_grid))[b] = grid_dev(c.grids[b]);
-            for (int f = 0; f < 6; ++f) ((double**)(h.data() + o_fptr))[6 * b + f] = c.grids[b].fields[f];
-        }
-        memcpy(h.data() + o_eoff, eoff.data(), (nb + 1) * 8);
-        memcpy(h.data() + o_voff, voff.data(), (nb + 1) * 8);
-        RET(ensure(C.btab, total));
-        CK(cudaMemcpyAsync(C.btab.p, h.data(), total, cudaMemcpyHostToDevice, st));
+        BatchTables bt;
+        RET(batch_tables(c, eoff, voff, bt));
+        RET(ensure(C.btab, bt.h.size()));
+        CK(cudaMemcpyAsync(C.btab.p, bt.h.data(), bt.h.size(), cudaMemcpyHostToDevice, st));
         CK(cudaStreamSynchronize(st)); // the host copy goes out of scope
-        d_meshes = (const MeshDev*)(C.btab.as<char>() + o_mesh);
-        d_grids = (const GridDev*)(C.btab.as<char>() + o_grid);
-        d_eoff = (const long long*)(C.btab.as<char>() + o_eoff);
-        d_voff = (const unsigned long long*)(C.btab.as<char>() + o_voff);
-        d_fptr = (double* const*)(C.btab.as<char>() + o_fptr);
+        if (c.capture == 1) {
+            // a page-locked copy for the capture calls, which may not allocate
+            if (C.btab_host_n < bt.h.size()) {
+                if (C.btab_host) cudaFreeHost(C.btab_host);
+                C.btab_host = nullptr;
+                C.btab_host_n = 0;
+                CK(cudaMallocHost(&C.btab_host, bt.h.size()));
+                C.btab_host_n = bt.h.size();
+            }
+        }
+        d_meshes = (const MeshDev*)(C.btab.as<char>() + bt.o_mesh);
+        d_grids = (const GridDev*)(C.btab.as<char>() + bt.o_grid);
+        d_eoff = (const long long*)(C.btab.as<char>() + bt.o_eoff);
+        d_voff = (const unsigned long long*)(C.btab.as<char>() + bt.o_voff);
+        d_fptr = (double* const*)(C.btab.as<char>() + bt.o_fptr);
     }
 
     RET(ensure(C.small, S_WORDS * 8));
@@ -674,6 +837,7 @@ int run_device(Call& c)
     ta.max_lvl = c.maxlvl;
     ta.refine_mode = c.refine_mode;
     ta.stretch = c.reftol;
+    order_cells(c.order_cell_bits, ta.cbits);
     ta.status = (unsigned*)&sm[S_STATUS];
     ta.counters = &sm[S_TESS];
     std::vector<long long> offs_host;
@@ -726,6 +890,13 @@ int run_device(Call& c)
     else
         for (int k = 0; k < nchunks; ++k) cap = std::max(cap, offs_host[cb[k + 1]] - offs_host[cb[k]]);
     if (cap < 1) cap = 1;
+    if (c.capture == 1) {
+        // a plan: the mixed atomic walk in one chunk, with room for 25% more images in later calls
+        if (!(mixed && atomic && use_bfs))
+            return fail(PSIB_ERR_UNSUPPORTED, "a capture plan needs precision = mixed and deterministic = 0");
+        if (nchunks != 1) return fail(PSIB_ERR_UNSUPPORTED, "a capture plan needs the images in one chunk");
+        cap = total + std::max<long long>(total / 4, 4096);
+    }
 
     RET(ensure(C.iframe, (size_t)cap * FRAME * sizeof(double)));
     RET(ensure(C.ielem, (size_t)cap * sizeof(int)));
@@ -816,6 +987,7 @@ int run_device(Call& c)
 
     float ms_clip = 0.f, ms_tess = 0.f, ms_final = 0.f;
     long long corrected = 0;
+    BfsSizes bsz; // the main walk's queue and pass sizes (a capture plan keeps them)
     unsigned long long clip_counts[3] = {0, 0, 0}; // fragments, fragment vertices, splits
     unsigned long long walk_bytes = 0;
     long long launches = 0;
@@ -906,7 +1078,7 @@ int run_device(Call& c)
             if (nmain > 0 && use_bfs) {
                 ca.scratch = C.scratch.p;
                 RET(bfs_clip(C, ca, nmain, nitems, sm, clip_grid, clip_block, c.queue_voxels, batch, st, launches,
-                             klaunch, C.key_sorted.as<uint16_t>()));
+                             klaunch, C.key_sorted.as<uint16_t>(), &bsz));
             } else if (nmain > 0) {
                 ca.scratch = C.scratch.p;
                 ca.order_base = 0;
@@ -1170,6 +1342,38 @@ int run_device(Call& c)
     CK(cudaMemcpyAsync(h, sm, sizeof(h), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     RET(check_status(c, h));
+    if (c.capture == 1) {
+        // the plan of later capture calls: every buffer they use, sized now
+        Ctx::Plan& P = C.plan;
+        P = Ctx::Plan{};
+        P.nelem = ne;
+        P.nbatch = batch ? c.nbatch : 0;
+        P.nvox = nvox;
+        P.cap_items = cap;
+        P.ntiles = ntiles;
+        P.stride = ca.acc.stride;
+        P.flags = flags;
+        P.precision = c.precision;
+        P.tiles = std::max<long long>(bsz.tiles, 1);
+        P.qcap = P.tiles * 32; // the queues as allocated: a capture call's passes must fit them
+        P.max_passes = (int)std::max<long long>(bsz.npass, 1) + 2;
+        P.btab_bytes = batch ? C.btab_host_n : 0;
+        RET(ensure(C.passes, (size_t)(P.max_passes + 1) * sizeof(long long)));
+        RET(ensure(C.fix_list, (size_t)cap * sizeof(int)));
+        RET(ensure(C.fix_keys, (size_t)cap * sizeof(uint16_t)));
+        RET(ensure(C.ifactor, (size_t)cap * sizeof(double)));
+        RET(ensure(C.vsum, (size_t)cap * sizeof(double)));
+        RET(ensure(C.dfs_list, (size_t)cap * sizeof(int)));
+        const int big_grid = C.num_sms * 2;
+        RET(ensure(C.scratch_big, big_bytes * (size_t)big_grid * big_block));
+        size_t tb = 0, t2 = 0;
+        CK(cub::DeviceScan::ExclusiveScan(nullptr, tb, (const int*)C.counts.p, C.offsets.as<long long>(), cub::Sum(),
+                                          (long long)0, (int)(ne + 1), st));
+        CK(cub::DeviceRadixSort::SortPairs(nullptr, t2, it.key, C.key_sorted.as<uint16_t>(), C.order_in.as<int>(),
+                                           C.order.as<int>(), (int)cap, 0, 16, st));
+        RET(ensure(C.cub_tmp, std::max(tb, t2)));
+        P.valid = true;
+    }
     if (c.stats) {
         psib_stats& s = *c.stats;
         s.corrected_items = corrected;
@@ -1190,6 +1394,221 @@ int run_device(Call& c)
         s.walk_bytes = (long long)walk_bytes;
     }
     (void)nvox;
+    return PSIB_OK;
+}
+
+// ---- capture mode: a call without host synchronisation or allocation ----
+
+// The mixed atomic deposit of run_device with every count kept on the device and every buffer
+// taken from the plan call before it (options.capture = 1), so that the caller can record the
+// call in a CUDA graph.  The item buffer has the plan's fixed size: its unused entries get
+// KEY_PAD and sort past the images; the main and deep images are counted on the device; a
+// one-thread kernel lays out the walk's passes (k_plan_passes) and the plan's number of passes is
+// launched, those beyond the need walking nothing; the deep-tree kernel and the mass-correction
+// pass read their sizes from the device.  Failures stay in the device status word
+// (psib_capture_status).
+int run_capture(Call& c)
+{
+    Ctx& C = *c.C;
+    const Ctx::Plan& P = C.plan;
+    const psib_grid& g = *c.grid;
+    const psib_mesh& m = *c.mesh;
+    cudaStream_t st = c.st;
+    const bool batch = c.nbatch > 0;
+    long long nvox = (long long)g.n[0] * g.n[1] * g.n[2];
+    long long ne = m.nelem;
+    std::vector<long long> eoff{0};
+    std::vector<unsigned long long> voff{0};
+    if (batch) {
+        for (int b = 0; b < c.nbatch; ++b) {
+            const psib_grid& gb = c.grids[b];
+            eoff.push_back(eoff.back() + c.meshes[b].nelem);
+            voff.push_back(voff.back() + (unsigned long long)gb.n[0] * gb.n[1] * gb.n[2]);
+        }
+        nvox = (long long)voff.back();
+        ne = eoff.back();
+    }
+    unsigned flags = 0;
+    if (c.F[1]) flags |= F_X;
+    if (c.F[2]) flags |= F_V;
+    if (c.F[3]) flags |= F_XX;
+    if (c.F[4]) flags |= F_XV;
+    if (c.F[5]) flags |= F_VV;
+    if (!P.valid || P.nelem != ne || P.nvox != nvox || P.nbatch != (batch ? c.nbatch : 0) || P.flags != flags ||
+        P.precision != c.precision)
+        return fail(PSIB_ERR_ARG, "a capture call needs a plan call (options.capture = 1) with the same grids, meshes "
+                                  "and fields before it");
+    if (c.precision != PSIB_MIXED || c.deterministic || c.adjoint || c.mode != PSIB_MODE_DENSITY)
+        return fail(PSIB_ERR_UNSUPPORTED, "the capture mode runs the mixed atomic deposit");
+    const int order = (flags & (F_XX | F_XV | F_VV)) ? 2 : (flags & (F_X | F_V)) ? 1 : 0;
+    const long long cap = P.cap_items;
+    const GridDev gd = grid_dev(g);
+    const MeshDev md = mesh_dev(m, g, c.pos, c.vel, c.mass, c.conn, c.reftol, c.refine_cell);
+    const MeshDev* d_meshes = nullptr;
+    const GridDev* d_grids = nullptr;
+    const long long* d_eoff = nullptr;
+    const unsigned long long* d_voff = nullptr;
+    double* const* d_fptr = nullptr;
+    if (batch) {
+        BatchTables bt;
+        RET(batch_tables(c, eoff, voff, bt));
+        if (bt.h.size() > C.btab_host_n || bt.h.size() > C.btab.n)
+            return fail(PSIB_ERR_ARG, "the batch tables outgrew the plan");
+        memcpy(C.btab_host, bt.h.data(), bt.h.size()); // page-locked: read when the copy runs
+        CK(cudaMemcpyAsync(C.btab.p, C.btab_host, bt.h.size(), cudaMemcpyHostToDevice, st));
+        d_meshes = (const MeshDev*)(C.btab.as<char>() + bt.o_mesh);
+        d_grids = (const GridDev*)(C.btab.as<char>() + bt.o_grid);
+        d_eoff = (const long long*)(C.btab.as<char>() + bt.o_eoff);
+        d_voff = (const unsigned long long*)(C.btab.as<char>() + bt.o_voff);
+        d_fptr = (double* const*)(C.btab.as<char>() + bt.o_fptr);
+    }
+    unsigned long long* sm = C.small.as<unsigned long long>();
+    unsigned* status = (unsigned*)&sm[S_STATUS];
+    CK(cudaMemsetAsync(&sm[1], 0, (S_WORDS - 1) * 8, st)); // the status word keeps earlier failures
+
+    // images: count, scan, emit into the fixed buffer, pad, order
+    TessArgs ta = {};
+    ta.m = md;
+    ta.nbatch = batch ? c.nbatch : 0;
+    ta.quad = m.elemtype == 27;
+    for (int b = 0; batch && b < c.nbatch; ++b) ta.quad |= c.meshes[b].elemtype == 27;
+    ta.meshes = d_meshes;
+    ta.grids = d_grids;
+    ta.eoff = d_eoff;
+    ta.g = gd;
+    ta.max_lvl = c.maxlvl;
+    ta.refine_mode = c.refine_mode;
+    ta.stretch = c.reftol;
+    order_cells(c.order_cell_bits, ta.cbits);
+    ta.status = status;
+    ta.counters = &sm[S_TESS];
+    ta.e0 = 0;
+    ta.e1 = ne;
+    ta.count = (int*)C.counts.p;
+    CK(launch_tess_count(ta, st));
+    CK(cudaMemsetAsync((int*)C.counts.p + ne, 0, sizeof(int), st));
+    size_t tb = 0;
+    CK(cub::DeviceScan::ExclusiveScan(nullptr, tb, (const int*)C.counts.p, C.offsets.as<long long>(), cub::Sum(),
+                                      (long long)0, (int)(ne + 1), st));
+    if (tb > C.cub_tmp.n) return fail(PSIB_ERR_ARG, "scan scratch outgrew the plan");
+    CK(cub::DeviceScan::ExclusiveScan(C.cub_tmp.p, tb, (const int*)C.counts.p, C.offsets.as<long long>(),
+                                      cub::Sum(), (long long)0, (int)(ne + 1), st));
+    const long long* total_dev = C.offsets.as<long long>() + ne;
+    ItemArrays it;
+    it.frame = C.iframe.as<double>();
+    it.elem = C.ielem.as<int>();
+    it.pid = C.ipid.as<int>();
+    it.key = C.ikey.as<uint16_t>();
+    it.grid = batch ? C.igrid.as<uint16_t>() : nullptr;
+    it.cap = cap;
+    ta.it = it;
+    ta.offset = C.offsets.as<long long>();
+    ta.offset_base = 0;
+    CK(launch_tess_emit(ta, st));
+    k_pad_keys<<<C.num_sms * 8, 256, 0, st>>>(it.key, total_dev, cap);
+    k_iota<<<C.num_sms * 8, 256, 0, st>>>(C.order_in.as<int>(), cap);
+    CK(cudaGetLastError());
+    tb = 0;
+    CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, it.key, C.key_sorted.as<uint16_t>(), C.order_in.as<int>(),
+                                       C.order.as<int>(), (int)cap, 0, 16, st));
+    if (tb > C.cub_tmp.n) return fail(PSIB_ERR_ARG, "sort scratch outgrew the plan");
+    CK(cub::DeviceRadixSort::SortPairs(C.cub_tmp.p, tb, it.key, C.key_sorted.as<uint16_t>(), C.order_in.as<int>(),
+                                       C.order.as<int>(), (int)cap, 0, 16, st));
+    k_key_classes<<<C.num_sms * 8, 256, 0, st>>>(C.key_sorted.as<uint16_t>(), cap, &sm[S_NMAIN], &sm[S_NDEEP]);
+    CK(cudaGetLastError());
+
+    // the per-voxel sums and the tiles' reference velocities
+    CK(cudaMemsetAsync(C.acc_sum.p, 0, (size_t)nvox * P.stride * sizeof(double), st));
+    CK(cudaMemsetAsync(C.acc_ref.p, 0, (size_t)nvox * 2 * sizeof(unsigned long long), st));
+    ClipArgs ca = {};
+    ca.it = it;
+    ca.order = C.order.as<int>();
+    ca.g = gd;
+    ca.grids = d_grids;
+    ca.voff = d_voff;
+    ca.mom_order = order;
+    ca.status = status;
+    ca.counters = &sm[S_CNT];
+    ca.rec_nmom = order == 2 ? 10 : order == 1 ? 4 : 1;
+    ca.rec_n = &sm[S_RECN];
+    ca.scale = C.iscale.as<double>();
+    {
+        int stride = 1, ox = -1, ov = -1, oxx = -1, oxv = -1, ovv = -1;
+        if (flags & (F_X | F_XX | F_XV)) { ox = stride; stride += 3; }
+        if (flags & (F_V | F_VV | F_XV)) { ov = stride; stride += 3; }
+        if (flags & F_XX) { oxx = stride; stride += 6; }
+        if (flags & F_XV) { oxv = stride; stride += 9; }
+        if (flags & F_VV) { ovv = stride; stride += 6; }
+        ca.acc = AccArgs{C.acc_sum.as<double>(), stride, ox, ov, oxx, oxv, ovv, C.acc_vref.as<double>(),
+                         batch ? C.acc_toff.as<long long>() : nullptr, nullptr, C.acc_ref.as<unsigned long long>(),
+                         C.acc_ref.as<unsigned long long>() + nvox};
+    }
+    CK(cudaMemsetAsync(C.acc_tsum.p, 0, (size_t)P.ntiles * 4 * sizeof(double), st));
+    CK(launch_vref(it, cap, gd, d_grids, ca.acc, C.acc_tsum.as<double>(), P.ntiles, C.num_sms, st, total_dev));
+
+    // the breadth-first walk of the main images, its passes planned on the device
+    PolyQueue Q[3];
+    const size_t tiles = (size_t)P.tiles;
+    for (int i = 0; i < 3; ++i)
+        Q[i] = PolyQueue{C.qx[i].as<float>(), C.qnb[i].as<uint32_t>(), C.qnv[i].as<uint8_t>(),
+                         C.qwin[i].as<uint8_t>(), C.qbox[i].as<uint32_t>(), C.qitem[i].as<uint32_t>(), nullptr,
+                         (unsigned long long)tiles * 32};
+    unsigned long long* cq = C.bfs_cnt.as<unsigned long long>();
+    BfsArgs ba = {};
+    ba.c = ca;
+    ba.dfs_list = C.dfs_list.as<int>();
+    ba.dfs_count = &sm[S_DFS];
+    ba.bytes = &sm[S_BYTES];
+    ba.window_bfs = 1;
+    ba.vsum = C.vsum.as<double>();
+    ba.passes = C.passes.as<long long>();
+    ba.pass_idx = &sm[S_PASS];
+    CK(cudaMemsetAsync(C.hist.p, 0, (65536 >> KEY_CELL_BITS) * sizeof(unsigned), st));
+    k_key_hist_dev<<<C.num_sms * 4, 256, 0, st>>>(C.key_sorted.as<uint16_t>(), &sm[S_NMAIN], C.hist.as<unsigned>());
+    k_plan_passes<<<1, 1, 0, st>>>(C.hist.as<unsigned>(), P.qcap, C.passes.as<long long>(), P.max_passes,
+                                   &sm[S_NMAIN], status);
+    CK(cudaGetLastError());
+    for (int p = 0; p < P.max_passes; ++p) CK(bfs_pass(ba, Q, cq, C.num_sms, st));
+    CK(launch_bfs_finalize(ba, cap, C.num_sms, st));
+
+    // the deep-tree images, their number and first position read on the device
+    {
+        const int big_block = 64, big_grid = C.num_sms * 2;
+        ClipArgs cd = ca;
+        cd.scratch = C.scratch_big.p;
+        cd.n_dev = &sm[S_NDEEP];
+        cd.base_dev = &sm[S_NMAIN];
+        cd.n = 0;
+        cd.head = &sm[S_HEAD + 1];
+        CK(launch_clip_mixed(cd, true, false, big_grid, big_block, st));
+    }
+
+    // images whose FP32 walk missed their exact volume: walked again with their mass factor
+    CK(launch_correction_select(it, ca.scale, cap, 1e-14, C.fix_list.as<int>(), C.fix_keys.as<uint16_t>(),
+                                C.ifactor.as<double>(), &sm[S_FIX], C.num_sms, st, total_dev));
+    k_plan_list<<<1, 256, 0, st>>>(C.fix_keys.as<uint16_t>(), &sm[S_FIX], P.qcap, C.passes.as<long long>(),
+                                   P.max_passes, status);
+    CK(cudaGetLastError());
+    {
+        BfsArgs bf = ba;
+        bf.c.order = C.fix_list.as<int>();
+        bf.c.acc.factor = C.ifactor.as<double>();
+        CK(cudaMemsetAsync(&sm[S_PASS], 0, 8, st));
+        CK(bfs_pass(bf, Q, cq, C.num_sms, st));
+    }
+
+    // every voxel's sums into its fields
+    FinalArgs fa = {};
+    fa.ap.M = c.F[0]; fa.ap.X = c.F[1]; fa.ap.V = c.F[2]; fa.ap.XX = c.F[3]; fa.ap.XV = c.F[4]; fa.ap.VV = c.F[5];
+    fa.ap.nbatch = batch ? c.nbatch : 0;
+    fa.ap.voff = d_voff;
+    fa.ap.fptr = d_fptr;
+    fa.acc = ca.acc;
+    fa.g = gd;
+    fa.grids = d_grids;
+    fa.v0 = 0;
+    fa.v1 = nvox;
+    CK(launch_acc_finalize(fa, C.num_sms, st));
     return PSIB_OK;
 }
 
@@ -2265,6 +2684,9 @@ int psib_voxels(const psib_grid* grid, const psib_mesh* mesh, int mode, double r
     c.deterministic = o.deterministic;
     c.refine_mode = o.refine_mode;
     c.queue_voxels = o.queue_voxels;
+    c.capture = o.capture;
+    c.order_cell_bits = o.order_cell_bits;
+    if (o.capture && o.memory != PSIB_DEVICE) return fail(PSIB_ERR_ARG, "the capture mode takes device memory");
     if (o.refine_mode == PSIB_REFINE_STRETCH) {
         const bool given = o.refine_cell[0] > 0.0 && o.refine_cell[1] > 0.0 && o.refine_cell[2] > 0.0;
         for (int i = 0; i < 3; ++i) {
@@ -2289,6 +2711,12 @@ int psib_voxels(const psib_grid* grid, const psib_mesh* mesh, int mode, double r
         c.vel = mesh->vel;
         c.mass = mesh->mass;
         c.conn = mesh->connectivity;
+        if (o.capture == 2) {
+            c.stats = nullptr;
+            const int r = run_capture(c);
+            RET(leave_own_stream(*C, (cudaStream_t)o.stream));
+            return r;
+        }
         CK(cudaEventRecord(C->ev[0], c.st));
         const int r = run_device(c);
         RET(leave_own_stream(*C, (cudaStream_t)o.stream));
@@ -2384,8 +2812,10 @@ int psib_voxels_batch(const psib_grid* grids, const psib_mesh* meshes, int nbatc
     c.deterministic = o.deterministic;
     c.refine_mode = o.refine_mode;
     c.queue_voxels = o.queue_voxels;
+    c.capture = o.capture;
+    c.order_cell_bits = o.order_cell_bits;
     c.C = C;
-    c.stats = o.stats;
+    c.stats = o.capture == 2 ? nullptr : o.stats;
     if (o.stats) *o.stats = psib_stats{};
     for (int f = 0; f < 6; ++f) c.F[f] = grids[0].fields[f];
     c.pos = meshes[0].pos;
@@ -2395,6 +2825,11 @@ int psib_voxels_batch(const psib_grid* grids, const psib_mesh* meshes, int nbatc
     if (nelem == 0) return PSIB_OK;
     RET(enter_own_stream(*C, (cudaStream_t)o.stream));
     c.st = C->own;
+    if (o.capture == 2) {
+        const int r = run_capture(c);
+        RET(leave_own_stream(*C, (cudaStream_t)o.stream));
+        return r;
+    }
     CK(cudaEventRecord(C->ev[0], c.st));
     const int r = run_device(c);
     RET(leave_own_stream(*C, (cudaStream_t)o.stream));
@@ -2405,6 +2840,24 @@ int psib_voxels_batch(const psib_grid* grids, const psib_mesh* meshes, int nbatc
         CK(cudaEventElapsedTime(&o.stats->ms_total, C->ev[0], C->ev[7]));
     }
     return PSIB_OK;
+}
+
+int psib_capture_status(void)
+{
+    g_err.clear();
+    if (psib_device_count() <= 0) return fail(PSIB_ERR_NODEVICE, "no CUDA device is visible");
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    Ctx* C = nullptr;
+    RET(get_ctx(dev, &C));
+    if (!C->small.p) return PSIB_OK;
+    CK(cudaDeviceSynchronize());
+    unsigned long long h[S_WORDS];
+    CK(cudaMemcpy(h, C->small.p, sizeof(h), cudaMemcpyDeviceToHost));
+    const unsigned zero = 0;
+    CK(cudaMemcpy(C->small.p, &zero, sizeof(zero), cudaMemcpyHostToDevice));
+    Call c = {};
+    return check_status(c, h);
 }
 
 int psib_voxels_adjoint(const psib_grid* grad, const psib_mesh* mesh, double refine_tolerance, int refine_max_lvl,

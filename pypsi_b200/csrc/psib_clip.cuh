@@ -488,14 +488,16 @@ __device__ __forceinline__ void clip_loop(const ClipArgs& a)
     Poly<double>* WC = (Poly<double>*)(region + wclip_offset<R, NS>());
     unsigned st = 0;
     Tally tally;
+    const long long n = a.n_dev ? (long long)*a.n_dev : a.n;
+    const long long ob = a.base_dev ? (long long)*a.base_dev : a.order_base;
     for (;;) {
         unsigned long long base = 0;
         if (lane == 0) base = atomicAdd(a.head, 32ull);
         base = __shfl_sync(0xFFFFFFFFu, base, 0);
-        if (base >= (unsigned long long)a.n) break;
+        if (base >= (unsigned long long)n) break;
         const long long i = (long long)base + lane;
-        if (i < a.n) {
-            const long long t = a.order ? (long long)a.order[a.order_base + i] : a.order_base + i;
+        if (i < n) {
+            const long long t = a.order ? (long long)a.order[ob + i] : ob + i;
             clip_item<R, NS, CENTRAL, ADJ, FULL>(a, t, S, QL, WC, st, tally);
         }
     }

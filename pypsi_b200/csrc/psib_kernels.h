@@ -23,7 +23,7 @@ struct ItemArrays {
     double *frame;   // FRAME x cap
     int *elem;       // cap: element index
     int *pid;        // 4 x cap: particle ids of the 4 vertices (unrefined meshes), else -1
-    uint16_t *key;   // cap: 0xFFFF for images the deep-tree kernel takes, else larger boxes first
+    uint16_t *key;   // cap: footprint key (KEY_DEEP: the deep-tree kernel's; KEY_PAD: no image)
     uint16_t *grid;  // cap: the image's cutout in a batch (null for a single grid)
     long long cap;
 };
@@ -39,8 +39,10 @@ struct GridDev {
 // high bits, larger boxes first, and in the low KEY_CELL_BITS a coarse cell of
 // the grid (8 x 4 x 4 cells) holding the box's low corner, so that images of
 // one volume are walked in spatial order and their fragments' atomic sums stay
-// in L2.
-constexpr unsigned KEY_DEEP = 0xFFFFu;
+// in L2.  KEY_PAD marks the unused entries of a fixed-size item buffer (the
+// capture mode sorts them past every image).
+constexpr unsigned KEY_DEEP = 0xFFFEu;
+constexpr unsigned KEY_PAD = 0xFFFFu;
 constexpr int KEY_CELL_BITS = 7;
 __host__ __device__ __forceinline__ long long key_volume(unsigned k)
 {
@@ -93,6 +95,8 @@ struct ClipArgs {
     long long order_base;    // first queue position of this launch
     long long n;             // queue entries of this launch
     unsigned long long *head;
+    // capture mode: the queue entries and first position of the launch read from device memory
+    const unsigned long long *n_dev, *base_dev;
     GridDev g;
     int mom_order;           // polynomial order of the moments (0, 1, 2)
     unsigned *status;
@@ -143,6 +147,7 @@ struct TessArgs {
     int quad;                  // some element is triquadratic (27 nodes): the kernel variant that holds them
     int refine_mode;           // 0: the reference's midpoint test (m.ptol2); 1: stretch beyond `stretch` x m.lag
     double stretch;
+    int cbits[3];              // bits of the footprint key's coarse cell per axis (0 0 0: no spatial order)
     // a batch of cutouts (nbatch > 0): element E belongs to cutout b with
     // eoff[b] <= E < eoff[b + 1]; its mesh and grid are meshes[b], grids[b]
     int nbatch;
@@ -272,13 +277,15 @@ cudaError_t launch_acc_finalize(const FinalArgs &a, int num_sms, cudaStream_t s)
 // images whose first vertex lies in the tile (0 where none does).  tsum: 4
 // doubles per tile, zeroed by the caller.
 cudaError_t launch_vref(const ItemArrays &it, long long nitems, const GridDev &g, const GridDev *grids,
-                        const AccArgs &acc, double *tsum, long long ntiles, int num_sms, cudaStream_t s);
+                        const AccArgs &acc, double *tsum, long long ntiles, int num_sms, cudaStream_t s,
+                        const long long *n_items = nullptr);
 // Images whose breadth-first mass correction (scale) differs from 1 by more
 // than tol: appended to list (count in *n), with factor[t] = scale[t] - 1 and
-// their footprint keys gathered into keys.
+// their footprint keys gathered into keys.  n_items (may be null): the number
+// of images, read on the device, below nitems.
 cudaError_t launch_correction_select(const ItemArrays &it, const double *scale, long long nitems, double tol,
                                      int *list, uint16_t *keys, double *factor, unsigned long long *n,
-                                     int num_sms, cudaStream_t s);
+                                     int num_sms, cudaStream_t s, const long long *n_items = nullptr);
 
 // ---- annihilation mode (annihilation.cu; the element stage in tess.cu) ----
 // A tet record: 4 oriented vertices (vertex-major), rho = mass / volume, the

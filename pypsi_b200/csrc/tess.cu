@@ -152,10 +152,9 @@ __device__ unsigned tet_images(const double (*p)[3], const MeshDev& m, const Gri
 // than the main kernel serves (DMAX_MAIN), or boxes longer than SPAN_MAX voxels
 // on an axis, where FP32 coordinates would lose too much precision inside a
 // voxel -- otherwise larger boxes first, then by coarse cell (psib_kernels.h).
-__device__ uint16_t footprint_key(const double (*rb)[3], const GridDev& g)
+__device__ uint16_t footprint_key(const double (*rb)[3], const GridDev& g, const int* cbits)
 {
     int depth = 0, span = 0, cell = 0;
-    const int cbits[3] = {3, 2, 2};
     long long vol = 1;
     for (int i = 0; i < 3; ++i) {
         double cmin = rb[0][i], cmax = rb[1][i];
@@ -173,7 +172,7 @@ __device__ uint16_t footprint_key(const double (*rb)[3], const GridDev& g)
         cell = (cell << cbits[i]) | (ci < (1 << cbits[i]) ? ci : (1 << cbits[i]) - 1);
     }
     if (depth > DMAX_MAIN || span > SPAN_MAX) return (uint16_t)KEY_DEEP;
-    return (uint16_t)(((256 - vol) << KEY_CELL_BITS) | cell);
+    return (uint16_t)(((256 - vol) << KEY_CELL_BITS) | (cell << (KEY_CELL_BITS - cbits[0] - cbits[1] - cbits[2])));
 }
 
 struct Emitter {
@@ -195,6 +194,11 @@ struct Emitter {
             if (write) {
                 const long long t = pos++;
                 const long long cap = a.it.cap;
+                if (t >= cap) { // a fixed-size item buffer (capture mode) that the images outgrew
+                    atomicOr(a.status, ST_OVERFLOW);
+                    n++;
+                    continue;
+                }
                 double q[4][3], rq[2][3];
                 double* fr = a.it.frame + t * FRAME;
                 for (int v = 0; v < 4; ++v)
@@ -213,7 +217,7 @@ struct Emitter {
                 fr[FR_MASS + 1] = 0.0;
                 a.it.elem[t] = (int)e;
                 for (int v = 0; v < 4; ++v) a.it.pid[v * cap + t] = pid ? pid[v] : -1;
-                a.it.key[t] = footprint_key(rq, g);
+                a.it.key[t] = footprint_key(rq, g, a.cbits);
                 if (a.it.grid) a.it.grid[t] = (uint16_t)gid;
             }
             n++;
@@ -1319,8 +1323,9 @@ cudaError_t launch_acc_finalize(const FinalArgs& a, int num_sms, cudaStream_t s)
 
 // Mass and momentum of the images whose first vertex lies in each tile.
 __global__ void k_vref_accum(ItemArrays it, long long n, GridDev g0, const GridDev* grids, const long long* toff,
-                             double* tsum)
+                             double* tsum, const long long* n_dev)
 {
+    if (n_dev) n = min(n, *n_dev);
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
         const int cut = grids ? (int)it.grid[t] : 0;
         const GridDev& g = grids ? grids[cut] : g0;
@@ -1347,9 +1352,10 @@ __global__ void k_vref_fix(const double* tsum, long long ntiles, double* vref)
 }
 
 cudaError_t launch_vref(const ItemArrays& it, long long nitems, const GridDev& g, const GridDev* grids,
-                        const AccArgs& acc, double* tsum, long long ntiles, int num_sms, cudaStream_t s)
+                        const AccArgs& acc, double* tsum, long long ntiles, int num_sms, cudaStream_t s,
+                        const long long* n_items)
 {
-    if (nitems > 0) k_vref_accum<<<num_sms * 8, 256, 0, s>>>(it, nitems, g, grids, acc.toff, tsum);
+    if (nitems > 0) k_vref_accum<<<num_sms * 8, 256, 0, s>>>(it, nitems, g, grids, acc.toff, tsum, n_items);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     k_vref_fix<<<num_sms * 4, 256, 0, s>>>(tsum, ntiles, (double*)acc.vref);
@@ -1357,11 +1363,12 @@ cudaError_t launch_vref(const ItemArrays& it, long long nitems, const GridDev& g
 }
 
 __global__ void k_correction_select(ItemArrays it, const double* scale, long long n, double tol, int* list,
-                                    uint16_t* keys, double* factor, unsigned long long* count)
+                                    uint16_t* keys, double* factor, unsigned long long* count, const long long* n_dev)
 {
+    if (n_dev) n = min(n, *n_dev);
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
         const double sc = scale[t];
-        if (it.key[t] != KEY_DEEP && sc > 0.0 && fabs(sc - 1.0) > tol) { // breadth-first images only
+        if (it.key[t] < KEY_DEEP && sc > 0.0 && fabs(sc - 1.0) > tol) { // breadth-first images only
             const unsigned long long i = atomicAdd(count, 1ull);
             list[i] = (int)t;
             keys[i] = it.key[t];
@@ -1372,10 +1379,10 @@ __global__ void k_correction_select(ItemArrays it, const double* scale, long lon
 
 cudaError_t launch_correction_select(const ItemArrays& it, const double* scale, long long nitems, double tol,
                                      int* list, uint16_t* keys, double* factor, unsigned long long* n, int num_sms,
-                                     cudaStream_t s)
+                                     cudaStream_t s, const long long* n_items)
 {
     if (nitems <= 0) return cudaSuccess;
-    k_correction_select<<<num_sms * 8, 256, 0, s>>>(it, scale, nitems, tol, list, keys, factor, n);
+    k_correction_select<<<num_sms * 8, 256, 0, s>>>(it, scale, nitems, tol, list, keys, factor, n, n_items);
     return cudaGetLastError();
 }
 

@@ -109,8 +109,8 @@ def test_autotune_batch_picks_a_candidate_and_clears(gpu):
     for c in cutouts:
         c["fields"] = {f: torch.zeros(sh, dtype=torch.float64, device="cuda") for f, sh in c["shapes"].items()}
     args = [{k: v for k, v in c.items() if k != "shapes"} for c in cutouts]
-    cap = capi.autotune_batch(args, candidates=(4096, 1 << 16), repeats=1)
-    assert cap in (4096, 1 << 16)
+    tune = capi.autotune_batch(args, candidates=(4096, 1 << 16), repeats=1, tiles=(7, -1))
+    assert tune["queue_voxels"] in (4096, 1 << 16) and tune["order_cell_bits"] in (7, -1) and tune["ms"] > 0
     assert all(float(t.abs().max()) == 0.0 for c in cutouts for t in c["fields"].values())
     # a tiny capacity forces many passes and must give the same fields
     ref, _ = _run(cutouts, "mixed", True)
