@@ -34,6 +34,8 @@ class DepositSpec:
     block_dims: tuple | None = None
     periodic_box: tuple | None = None
     precision: str = "fp64"
+    refine_tolerance: float = 1.0
+    refine_max_lvl: int = 0
 
 
 class _DensityDeposit(torch.autograd.Function):
@@ -41,7 +43,8 @@ class _DensityDeposit(torch.autograd.Function):
     def forward(ctx, pos, mass, connectivity, spec: DepositSpec):
         m = torch.zeros(spec.n, dtype=torch.float64, device=pos.device)
         capi.voxels_device({"m": m}, spec.n, spec.bounds, pos, None, mass, connectivity=connectivity,
-                           block_dims=spec.block_dims, periodic_box=spec.periodic_box, precision=spec.precision)
+                           block_dims=spec.block_dims, periodic_box=spec.periodic_box, precision=spec.precision,
+                           refine_tolerance=spec.refine_tolerance, refine_max_lvl=spec.refine_max_lvl)
         ctx.save_for_backward(pos, mass, connectivity)
         ctx.spec = spec
         return m
@@ -54,20 +57,24 @@ class _DensityDeposit(torch.autograd.Function):
         grad_mass = torch.zeros_like(mass) if (mass is not None and ctx.needs_input_grad[1]) else None
         capi.adjoint_device(grad_m.contiguous(), spec.n, spec.bounds, pos, grad_pos, mass=mass,
                             connectivity=connectivity, block_dims=spec.block_dims,
-                            periodic_box=spec.periodic_box, grad_mass=grad_mass)
+                            periodic_box=spec.periodic_box, grad_mass=grad_mass,
+                            refine_tolerance=spec.refine_tolerance, refine_max_lvl=spec.refine_max_lvl)
         return (grad_pos if ctx.needs_input_grad[0] else None), grad_mass, None, None
 
 
 def deposit_density(pos: torch.Tensor, mass: torch.Tensor | None = None, *, n, bounds, block_dims=None,
                     connectivity: torch.Tensor | None = None, periodic_box=None,
-                    precision: str = "fp64") -> torch.Tensor:
+                    precision: str = "fp64", refine_tolerance: float = 1.0,
+                    refine_max_lvl: int = 0) -> torch.Tensor:
     """m field of PSI.voxels(grid, mesh) for particles at `pos`, differentiable.
 
     pos: (npart, 3) float64 CUDA tensor (C-contiguous).  mass: (nelem,) float64
     or None (1 per element).  The mesh is a block lattice (`block_dims`, as
     Mesh(loader='block')) or explicit `connectivity` ((nelem, 4|8) int32), in a
     periodic box when `periodic_box` is given.  `precision` selects the forward
-    kernel ('fp64' or 'mixed'); the backward pass is always FP64."""
+    kernel ('fp64' or 'mixed'); the backward pass is always FP64.  Elements are
+    refined as PSI.voxels refines them (midpoint criterion); the gradient flows
+    through the interpolation of the refined vertices."""
     if not pos.is_cuda:
         raise ValueError("deposit_density runs on the GPU: pos must be a CUDA tensor")
     if pos.dtype != torch.float64 or not pos.is_contiguous():
@@ -79,7 +86,7 @@ def deposit_density(pos: torch.Tensor, mass: torch.Tensor | None = None, *, n, b
     spec = DepositSpec(tuple(int(v) for v in n), tuple(tuple(float(x) for x in b) for b in bounds),
                        tuple(int(v) for v in block_dims) if block_dims is not None else None,
                        tuple(tuple(float(x) for x in b) for b in periodic_box) if periodic_box is not None else None,
-                       precision)
+                       precision, float(refine_tolerance), int(refine_max_lvl))
     return _DensityDeposit.apply(pos, mass, connectivity, spec)
 
 
@@ -93,7 +100,8 @@ class _FieldsDeposit(torch.autograd.Function):
         out = {f: torch.zeros(spec.n + FIELD_SHAPES[f], dtype=torch.float64, device=pos.device) for f in names}
         capi.voxels_device(out, spec.n, spec.bounds, pos, vel, mass, connectivity=connectivity,
                            block_dims=spec.block_dims, periodic_box=spec.periodic_box, precision=spec.precision,
-                           deterministic=True)
+                           deterministic=True, refine_tolerance=spec.refine_tolerance,
+                           refine_max_lvl=spec.refine_max_lvl)
         res = tuple(out[f] for f in names)
         ctx.save_for_backward(pos, vel, mass, connectivity, *res)
         ctx.spec = spec
@@ -112,13 +120,14 @@ class _FieldsDeposit(torch.autograd.Function):
         if g:
             capi.adjoint_fields_device(g, fwd, spec.n, spec.bounds, pos, grad_pos, vel=vel, mass=mass,
                                        connectivity=connectivity, block_dims=spec.block_dims,
-                                       periodic_box=spec.periodic_box, grad_vel=grad_vel, grad_mass=grad_mass)
+                                       periodic_box=spec.periodic_box, grad_vel=grad_vel, grad_mass=grad_mass,
+                                       refine_tolerance=spec.refine_tolerance, refine_max_lvl=spec.refine_max_lvl)
         return (grad_pos if ctx.needs_input_grad[0] else None), grad_vel, grad_mass, None, None, None
 
 
 def deposit_fields(pos: torch.Tensor, vel: torch.Tensor | None = None, mass: torch.Tensor | None = None, *,
                    fields=("m",), n, bounds, block_dims=None, connectivity: torch.Tensor | None = None,
-                   periodic_box=None) -> dict:
+                   periodic_box=None, refine_tolerance: float = 1.0, refine_max_lvl: int = 0) -> dict:
     """The requested fields of PSI.voxels(grid, mesh) in a zeroed grid --
     m (mass), x and v (mass-weighted means), xx, xv, vv ((co)variances, xv with
     the reference's pairing of its cross terms) -- differentiable with respect
@@ -126,7 +135,9 @@ def deposit_fields(pos: torch.Tensor, vel: torch.Tensor | None = None, mass: tor
 
     The forward pass is the FP64 deposit in the reference's order; the
     backward pass recomputes the clip in FP64 (psib_voxels_adjoint_fields).
-    A second moment needs its first moments among `fields`.  Returns
+    A second moment needs its first moments among `fields`.  Elements are refined
+    as PSI.voxels refines them (midpoint criterion, 8- and 27-node elements); the
+    gradient flows through the interpolation of the refined vertices.  Returns
     {name: tensor} for the requested names (m always included)."""
     for t, name in ((pos, "pos"), (vel, "vel"), (mass, "mass")):
         if t is not None and (not t.is_cuda or t.dtype != torch.float64 or not t.is_contiguous()):
@@ -139,6 +150,6 @@ def deposit_fields(pos: torch.Tensor, vel: torch.Tensor | None = None, mass: tor
     spec = DepositSpec(tuple(int(v) for v in n), tuple(tuple(float(x) for x in b) for b in bounds),
                        tuple(int(v) for v in block_dims) if block_dims is not None else None,
                        tuple(tuple(float(x) for x in b) for b in periodic_box) if periodic_box is not None else None,
-                       "fp64")
+                       "fp64", float(refine_tolerance), int(refine_max_lvl))
     res = _FieldsDeposit.apply(pos, vel, mass, connectivity, spec, names)
     return dict(zip(names, res))

@@ -175,11 +175,12 @@ def mesh_from_tensors(pos, vel=None, mass=None, connectivity=None, block_dims=No
 
 
 def adjoint_device(grad_m, n, bounds, pos, grad_pos, mass=None, connectivity=None, block_dims=None,
-                   periodic_box=None, grad_mass=None, stream=None) -> dict:
+                   periodic_box=None, grad_mass=None, stream=None, refine_tolerance=1.0, refine_max_lvl=0) -> dict:
     """Backward pass of the m field on device-resident torch tensors.
 
     grad_m: (nx,ny,nz) float64 CUDA tensor, dL/dm.  Adds dL/dpos to grad_pos
-    ((npart,3) float64) and, if given, dL/dmass to grad_mass ((nelem,))."""
+    ((npart,3) float64) and, if given, dL/dmass to grad_mass ((nelem,)).  The
+    refinement arguments are those of the forward deposit (midpoint criterion)."""
     import torch
 
     for t in (grad_m, pos, grad_pos) + ((grad_mass,) if grad_mass is not None else ()):
@@ -190,7 +191,8 @@ def adjoint_device(grad_m, n, bounds, pos, grad_pos, mass=None, connectivity=Non
     st = Stats()
     o = Options(precision=PSIB_FP64, deterministic=0, memory=PSIB_DEVICE, device=-1,
                 stream=C.c_void_p(s.cuda_stream), stats=C.pointer(st))
-    rc = lib.psib_voxels_adjoint(C.byref(g), C.byref(m), 1.0, 0, grad_pos.data_ptr(), None,
+    rc = lib.psib_voxels_adjoint(C.byref(g), C.byref(m), float(refine_tolerance), int(refine_max_lvl),
+                                 grad_pos.data_ptr(), None,
                                  grad_mass.data_ptr() if grad_mass is not None else None, C.byref(o))
     if rc != 0:
         raise PsibError(rc)
@@ -198,12 +200,14 @@ def adjoint_device(grad_m, n, bounds, pos, grad_pos, mass=None, connectivity=Non
 
 
 def adjoint_fields_device(grads: dict, fwd: dict, n, bounds, pos, grad_pos, vel=None, mass=None, connectivity=None,
-                          block_dims=None, periodic_box=None, grad_vel=None, grad_mass=None, stream=None) -> dict:
+                          block_dims=None, periodic_box=None, grad_vel=None, grad_mass=None, stream=None,
+                          refine_tolerance=1.0, refine_max_lvl=0) -> dict:
     """Backward pass of every field (psib_voxels_adjoint_fields) on device tensors.
 
     fwd: the fields of the forward deposit into zeroed fields ({"m": ..., "x": ...});
     grads: dL/d(field) for any of them (missing: 0).  Adds dL/dpos to grad_pos and,
-    if given, dL/dvel to grad_vel ((npart,3)) and dL/dmass to grad_mass ((nelem,))."""
+    if given, dL/dvel to grad_vel ((npart,3)) and dL/dmass to grad_mass ((nelem,)).
+    The refinement arguments are those of the forward deposit (midpoint criterion)."""
     import torch
 
     for t in list(grads.values()) + list(fwd.values()) + [pos, grad_pos] + \
@@ -216,7 +220,8 @@ def adjoint_fields_device(grads: dict, fwd: dict, n, bounds, pos, grad_pos, vel=
     st = Stats()
     o = Options(precision=PSIB_FP64, deterministic=0, memory=PSIB_DEVICE, device=-1,
                 stream=C.c_void_p(s.cuda_stream), stats=C.pointer(st))
-    rc = lib.psib_voxels_adjoint_fields(C.byref(g), C.byref(f), C.byref(m), 1.0, 0, grad_pos.data_ptr(),
+    rc = lib.psib_voxels_adjoint_fields(C.byref(g), C.byref(f), C.byref(m), float(refine_tolerance),
+                                        int(refine_max_lvl), grad_pos.data_ptr(),
                                         grad_vel.data_ptr() if grad_vel is not None else None,
                                         grad_mass.data_ptr() if grad_mass is not None else None, C.byref(o))
     if rc != 0:

@@ -947,9 +947,10 @@ int run_device(Call& c)
         ca.adj_gpos = c.gpos;
         ca.adj_npart = m.npart;
         ca.adj_gmass = c.gmass;
-        ca.adj_mass_factor = m.elemtype == 8 ? 1.0 / 6.0 : 1.0;
+        ca.adj_mass_factor = m.elemtype == 4 ? 1.0 : 1.0 / 6.0;
         ca.adj_coef = c.adj_coef;
         ca.adj_gvel = c.gvel;
+        ca.adj_mesh = md;
     }
 
     long long ntiles = 0;
@@ -2873,9 +2874,6 @@ int psib_voxels_adjoint(const psib_grid* grad, const psib_mesh* mesh, double ref
     for (int f = 1; f < 6; ++f)
         if (grad->fields[f])
             return fail(PSIB_ERR_UNSUPPORTED, "the adjoint takes the gradient of field m only");
-    if (refine_max_lvl > 0 && mesh->elemtype == 8)
-        return fail(PSIB_ERR_UNSUPPORTED, "the adjoint supports refine_max_lvl = 0 only");
-    if (mesh->elemtype == 27) return fail(PSIB_ERR_UNSUPPORTED, "the adjoint supports 4- and 8-node elements");
     if (!grad_pos && mesh->nelem > 0) return fail(PSIB_ERR_ARG, "grad_pos is required");
     (void)grad_vel; // the density does not depend on the velocities
     if (psib_device_count() <= 0) return fail(PSIB_ERR_NODEVICE, "no CUDA device is visible");
@@ -2889,7 +2887,7 @@ int psib_voxels_adjoint(const psib_grid* grad, const psib_mesh* mesh, double ref
     c.grid = grad;
     c.mesh = mesh;
     c.reftol = refine_tolerance;
-    c.maxlvl = 0;
+    c.maxlvl = refine_max_lvl > 6 ? 6 : (refine_max_lvl < 0 ? 0 : refine_max_lvl);
     c.precision = PSIB_FP64;
     c.C = C;
     c.stats = o.stats;
@@ -2966,9 +2964,6 @@ int psib_voxels_adjoint_fields(const psib_grid* grad, const psib_grid* fwd, cons
         (fwd->fields[PSIB_XV] && !(fwd->fields[PSIB_X] && fwd->fields[PSIB_V])))
         return fail(PSIB_ERR_ARG, "the forward second moments need their first moments (xx: x, vv: v, xv: x and v)");
     if (o.memory != PSIB_DEVICE) return fail(PSIB_ERR_UNSUPPORTED, "psib_voxels_adjoint_fields takes device memory");
-    if (refine_max_lvl > 0 && mesh->elemtype == 8)
-        return fail(PSIB_ERR_UNSUPPORTED, "the adjoint supports refine_max_lvl = 0 only");
-    if (mesh->elemtype == 27) return fail(PSIB_ERR_UNSUPPORTED, "the adjoint supports 4- and 8-node elements");
     if (!grad_pos && mesh->nelem > 0) return fail(PSIB_ERR_ARG, "grad_pos is required");
     if (psib_device_count() <= 0) return fail(PSIB_ERR_NODEVICE, "no CUDA device is visible");
     int dev = 0;
@@ -2993,7 +2988,7 @@ int psib_voxels_adjoint_fields(const psib_grid* grad, const psib_grid* fwd, cons
     c.grid = fwd;
     c.mesh = mesh;
     c.reftol = refine_tolerance;
-    c.maxlvl = 0;
+    c.maxlvl = refine_max_lvl > 6 ? 6 : (refine_max_lvl < 0 ? 0 : refine_max_lvl);
     c.precision = PSIB_FP64;
     c.C = C;
     c.stats = o.stats;

@@ -102,6 +102,76 @@ __device__ __forceinline__ void write_record(const ClipArgs& a, const GridDev& g
 // the image's four particles (and to its element's mass).  FULL (with ADJ):
 // the gradient of every field, through the per-voxel coefficients adj_coef
 // (psib_adjoint.cuh), back to positions, velocities and masses.
+// The particles a tet vertex of image t moves with: its own particle (pid >= 0, weight 1), or for
+// a vertex of a refined element (pid a refine_vertex_code) the element's nodes with their
+// interpolation weights at the vertex's place -- trilinear for 8-node, triquadratic (Lagrange on
+// 0, 1/2, 1 per axis) for 27-node elements, as the refinement interpolates.  f(id, weight) for each
+// with a nonzero weight; false on an id out of range.
+template <class F>
+__device__ bool for_vertex_sources(const ClipArgs& a, int pid, long long e, F&& f)
+{
+    if (pid >= 0) {
+        if (pid >= a.adj_npart) return false;
+        f(pid, 1.0);
+        return true;
+    }
+    if (pid == -1) return false;
+    int x[3], lvl;
+    refine_vertex_decode(pid, x, lvl);
+    const MeshDev& m = a.adj_mesh;
+    const int et = m.elemtype;
+    if ((et != 8 && et != 27) || e < 0 || e >= m.nelem) return false;
+    const int nb = et == 27 ? 3 : 2;
+    double b[3][3];
+    for (int i = 0; i < 3; ++i) {
+        const double u = x[i] * (1.0 / 128);
+        if (et == 27) {
+            b[i][0] = 2.0 * (u - 0.5) * (u - 1.0);
+            b[i][1] = 4.0 * u * (1.0 - u);
+            b[i][2] = 2.0 * u * (u - 0.5);
+        } else {
+            b[i][0] = 1.0 - u;
+            b[i][1] = u;
+        }
+    }
+    long long nyz = 0;
+    int ei = 0, ej = 0, ek = 0;
+    if (!m.conn) {
+        nyz = (long long)m.edim[1] * m.edim[2];
+        ei = (int)(e / nyz);
+        ej = (int)((e / m.edim[2]) % m.edim[1]);
+        ek = (int)(e % m.edim[2]);
+    }
+    for (int i = 0; i < nb; ++i)
+        for (int j = 0; j < nb; ++j)
+            for (int k = 0; k < nb; ++k) {
+                const double w = b[0][i] * b[1][j] * b[2][k];
+                if (w == 0.0) continue;
+                long long id;
+                if (m.conn) {
+                    id = m.conn[e * et + (et == 27 ? 9 * i + 3 * j + k : 4 * i + 2 * j + k)];
+                } else { // implicit block connectivity (src/PSI.c:644-656)
+                    id = (long long)m.bdim[1] * m.bdim[2] * ((ei + i) % m.bdim[0]) +
+                         (long long)m.bdim[2] * ((ej + j) % m.bdim[1]) + ((ek + k) % m.bdim[2]);
+                }
+                if (id < 0 || id >= a.adj_npart) return false;
+                f((int)id, w);
+            }
+    return true;
+}
+
+// Tet mass / element mass of image t: the unrefined factor times 1/8 per refinement level.
+__device__ __forceinline__ double image_mass_factor(const ClipArgs& a, long long t)
+{
+    const int pid = a.it.pid[t];
+    if (pid > -2) return a.adj_mass_factor;
+    int x[3], lvl;
+    refine_vertex_decode(pid, x, lvl);
+    double f = a.adj_mass_factor;
+    for (int l = 0; l < lvl; ++l) f *= 0.125;
+    return f;
+}
+
 template <class R, int NS, bool CENTRAL, bool ADJ = false, bool FULL = false>
 __device__ void clip_item(const ClipArgs& a, long long t, Poly<R>* S, QPoly* QL, Poly<double>* WC, unsigned& st,
                           Tally& tally)
@@ -419,21 +489,26 @@ __device__ void clip_item(const ClipArgs& a, long long t, Poly<R>* S, QPoly* QL,
                     gvel[c2][a2] = T.DV[c2][0] * inv[0][a2] + T.DV[c2][1] * inv[1][a2] + T.DV[c2][2] * inv[2][a2];
             const double rho = T.mass / sT;
             for (int v = 0; v < 4; ++v) {
-                const int pid = a.it.pid[v * a.it.cap + t];
-                if (pid < 0 || pid >= a.adj_npart) { st |= ST_INDEX; continue; }
+                double gp[3], gu[3];
                 for (int i = 0; i < 3; ++i) {
-                    double gp = rho * acc.bnd[v][i] - dS[v][i] / sT * acc.I0;
-                    for (int c2 = 0; c2 < 3; ++c2) gp -= gvel[c2][i] * acc.J[v][c2];
-                    double gu = acc.J[v][i];
+                    gp[i] = rho * acc.bnd[v][i] - dS[v][i] / sT * acc.I0;
+                    for (int c2 = 0; c2 < 3; ++c2) gp[i] -= gvel[c2][i] * acc.J[v][c2];
+                    gu[i] = acc.J[v][i];
                     if (v == 0) {
-                        gp += acc.qa[i];
-                        gu += acc.qb[i];
+                        gp[i] += acc.qa[i];
+                        gu[i] += acc.qb[i];
                     }
-                    atomicAdd(&a.adj_gpos[3 * (long long)pid + i], gp);
-                    if (a.adj_gvel) atomicAdd(&a.adj_gvel[3 * (long long)pid + i], gu);
                 }
+                const bool ok = for_vertex_sources(a, a.it.pid[v * a.it.cap + t], a.it.elem[t], [&](int id, double w) {
+                    for (int i = 0; i < 3; ++i) {
+                        atomicAdd(&a.adj_gpos[3 * (long long)id + i], w * gp[i]);
+                        if (a.adj_gvel) atomicAdd(&a.adj_gvel[3 * (long long)id + i], w * gu[i]);
+                    }
+                });
+                if (!ok) st |= ST_INDEX;
             }
-            if (a.adj_gmass && T.mass != 0.0) atomicAdd(&a.adj_gmass[a.it.elem[t]], acc.I0 / T.mass * a.adj_mass_factor);
+            if (a.adj_gmass && T.mass != 0.0)
+                atomicAdd(&a.adj_gmass[a.it.elem[t]], acc.I0 / T.mass * image_mass_factor(a, t));
         }
     } else if constexpr (ADJ) {
         // d m0 / dx_i = (dS(P)/dx_i - m0 dS(T)/dx_i) / S(T), times the image's mass
@@ -457,12 +532,14 @@ __device__ void clip_item(const ClipArgs& a, long long t, Poly<R>* S, QPoly* QL,
             if (sT != 0.0) {
                 const double f = mass / sT;
                 for (int v = 0; v < 4; ++v) {
-                    const int pid = a.it.pid[v * a.it.cap + t];
-                    if (pid < 0 || pid >= a.adj_npart) { st |= ST_INDEX; continue; }
-                    for (int i = 0; i < 3; ++i) atomicAdd(&a.adj_gpos[3 * (long long)pid + i], f * (A[v][i] - B * dS[v][i]));
+                    const bool ok = for_vertex_sources(a, a.it.pid[v * a.it.cap + t], a.it.elem[t], [&](int id, double w) {
+                        for (int i = 0; i < 3; ++i)
+                            atomicAdd(&a.adj_gpos[3 * (long long)id + i], w * f * (A[v][i] - B * dS[v][i]));
+                    });
+                    if (!ok) st |= ST_INDEX;
                 }
             }
-            if (a.adj_gmass) atomicAdd(&a.adj_gmass[a.it.elem[t]], B * a.adj_mass_factor);
+            if (a.adj_gmass) atomicAdd(&a.adj_gmass[a.it.elem[t]], B * image_mass_factor(a, t));
         }
     }
     if constexpr (sizeof(R) == 4) {

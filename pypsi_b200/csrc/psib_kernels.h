@@ -22,7 +22,8 @@ constexpr int FR_U = 12, FR_MASS = 24;
 struct ItemArrays {
     double *frame;   // FRAME x cap
     int *elem;       // cap: element index
-    int *pid;        // 4 x cap: particle ids of the 4 vertices (unrefined meshes), else -1
+    int *pid;        // 4 x cap: per vertex the particle id (>= 0), or for a vertex of a refined
+                     // element its place in the element, refine_vertex_code (<= -2)
     uint16_t *key;   // cap: footprint key (KEY_DEEP: the deep-tree kernel's; KEY_PAD: no image)
     uint16_t *grid;  // cap: the image's cutout in a batch (null for a single grid)
     long long cap;
@@ -44,6 +45,22 @@ struct GridDev {
 constexpr unsigned KEY_DEEP = 0xFFFEu;
 constexpr unsigned KEY_PAD = 0xFFFFu;
 constexpr int KEY_CELL_BITS = 7;
+// A vertex of a tet of a refined element, as an image's pid entry: its parameter coordinates in
+// the element's unit cube in units of 1/128 (0..128 each; a leaf cube of level d has side
+// 128 >> d) and the level d (0..6); always <= -2, so never a particle id or the -1 of "none".
+__host__ __device__ __forceinline__ int refine_vertex_code(int x, int y, int z, int d)
+{
+    return -2 - (x | (y << 8) | (z << 16) | (d << 24));
+}
+__host__ __device__ __forceinline__ void refine_vertex_decode(int pid, int *xyz, int &d)
+{
+    const int c = -2 - pid;
+    xyz[0] = c & 0xFF;
+    xyz[1] = (c >> 8) & 0xFF;
+    xyz[2] = (c >> 16) & 0xFF;
+    d = (c >> 24) & 0x7;
+}
+
 __host__ __device__ __forceinline__ long long key_volume(unsigned k)
 {
     if (k >= KEY_DEEP) return 1ll << 40;
@@ -89,6 +106,19 @@ __host__ __device__ __forceinline__ long long acc_tiles(const GridDev &g)
     return t;
 }
 
+struct MeshDev {
+    int elemtype;
+    long long npart, nelem;
+    const double *pos, *vel, *mass;
+    const int *conn;
+    int bdim[3];  // particle lattice of an implicit block mesh
+    int edim[3];  // element lattice of an implicit block mesh
+    int periodic;
+    double box0[3], box1[3];
+    double ptol2;   // midpoint refinement: squared tolerance (reftol x the grid's smallest cell)^2
+    double lag[3];  // stretch refinement: the Lagrangian cell
+};
+
 struct ClipArgs {
     ItemArrays it;
     const int *order;        // queue position -> item (may be null: identity)
@@ -120,23 +150,11 @@ struct ClipArgs {
     double *adj_gpos;        // dL/dpos per particle (accumulated)
     long long adj_npart;
     double *adj_gmass;       // dL/dmass per element (accumulated), may be null
-    double adj_mass_factor;  // element mass / tet mass
+    double adj_mass_factor;  // tet mass / element mass of an unrefined element
     const double *adj_coef;  // full adjoint: ADJ_NCOEF coefficients per voxel (null: the m field only, adj_gm)
     double *adj_gvel;        // full adjoint: dL/dvel per particle (accumulated), may be null
+    MeshDev adj_mesh;        // the mesh: corner ids and weights of the vertices of refined images
     AccArgs acc;             // atomic accumulation (acc.sum != null) instead of records
-};
-
-struct MeshDev {
-    int elemtype;
-    long long npart, nelem;
-    const double *pos, *vel, *mass;
-    const int *conn;
-    int bdim[3];  // particle lattice of an implicit block mesh
-    int edim[3];  // element lattice of an implicit block mesh
-    int periodic;
-    double box0[3], box1[3];
-    double ptol2;   // midpoint refinement: squared tolerance (reftol x the grid's smallest cell)^2
-    double lag[3];  // stretch refinement: the Lagrangian cell
 };
 
 struct TessArgs {

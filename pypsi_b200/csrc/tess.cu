@@ -230,7 +230,18 @@ struct RefNode {
     double u[27][3];
     double mass;
     int child;
+    int o[3], side; // the (sub)cube in the element's unit cube, in units of 1/128
 };
+
+// The pid entries of leaf tet t of (sub)cube N at level d: each vertex's place in the element.
+__device__ __forceinline__ void leaf_codes(const RefNode& N, int t, int d, int* pc)
+{
+    const int h = N.side >> 1;
+    for (int v = 0; v < 4; ++v) {
+        const int nd = c_tet_nodes[t][v];
+        pc[v] = refine_vertex_code(N.o[0] + (nd / 9) * h, N.o[1] + ((nd / 3) % 3) * h, N.o[2] + (nd % 3) * h, d);
+    }
+}
 
 // The stretch criterion (PSIB_REFINE_STRETCH; the reference has only the
 // midpoint test): refine a (sub)cube of level lvl whose edge along axis a is
@@ -275,6 +286,8 @@ __device__ void refine_element(EM& em, const double (*cp)[3], const double (*cu)
     interp_trilinear(cu, L[0].u);
     L[0].mass = mass;
     L[0].child = -1;
+    L[0].o[0] = L[0].o[1] = L[0].o[2] = 0;
+    L[0].side = 128;
     int d = 0;
     while (d >= 0) {
         RefNode& N = L[d];
@@ -299,7 +312,9 @@ __device__ void refine_element(EM& em, const double (*cp)[3], const double (*cu)
                             tp[v][i] = N.p[c_tet_nodes[t][v]][i];
                             tu[v][i] = N.u[c_tet_nodes[t][v]][i];
                         }
-                    em.tet(tp, tu, N.mass * (1.0 / 6), e, nullptr);
+                    int pc[4];
+                    leaf_codes(N, t, d, pc);
+                    em.tet(tp, tu, N.mass * (1.0 / 6), e, pc);
                 }
                 d--;
                 continue;
@@ -321,6 +336,10 @@ __device__ void refine_element(EM& em, const double (*cp)[3], const double (*cu)
             interp_trilinear(ku, L[d + 1].u);
             L[d + 1].mass = 0.125 * N.mass;
             L[d + 1].child = -1;
+            L[d + 1].side = N.side >> 1;
+            L[d + 1].o[0] = N.o[0] + ci * L[d + 1].side;
+            L[d + 1].o[1] = N.o[1] + cj * L[d + 1].side;
+            L[d + 1].o[2] = N.o[2] + ck * L[d + 1].side;
             d++;
         } else {
             d--;
@@ -373,6 +392,8 @@ __device__ void refine_element_quad(EM& em, const double (*cp)[3], const double 
         }
     L[0].mass = mass;
     L[0].child = -1;
+    L[0].o[0] = L[0].o[1] = L[0].o[2] = 0;
+    L[0].side = 128;
     int d = 0;
     while (d >= 0) {
         RefNode& N = L[d];
@@ -397,7 +418,9 @@ __device__ void refine_element_quad(EM& em, const double (*cp)[3], const double 
                             tp[v][i] = N.p[c_tet_nodes[t][v]][i];
                             tu[v][i] = N.u[c_tet_nodes[t][v]][i];
                         }
-                    em.tet(tp, tu, N.mass * (1.0 / 6), e, nullptr);
+                    int pc[4];
+                    leaf_codes(N, t, d, pc);
+                    em.tet(tp, tu, N.mass * (1.0 / 6), e, pc);
                 }
                 d--;
                 continue;
@@ -417,6 +440,10 @@ __device__ void refine_element_quad(EM& em, const double (*cp)[3], const double 
                         }
             K.mass = 0.125 * N.mass;
             K.child = -1;
+            K.side = N.side >> 1;
+            K.o[0] = N.o[0] + ci * K.side;
+            K.o[1] = N.o[1] + cj * K.side;
+            K.o[2] = N.o[2] + ck * K.side;
             d++;
         } else {
             d--;

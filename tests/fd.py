@@ -47,7 +47,8 @@ def fd_loss_grad(O, kind, case, conn, rho, rho_t, p, ax, elems, h=1e-6):
 
     def dep(px):
         return O.voxelize(kind, n=n, bounds=bounds, pos=px, conn=sub, mass=mass,
-                          periodic_box=case["periodic_box"], fields=[])["m"] / dv
+                          periodic_box=case["periodic_box"], fields=[], reftol=case.get("reftol", 1.0),
+                          maxlvl=case.get("maxlvl", 0))["m"] / dv
 
     b0 = dep(pos)
     pp, pm = pos.copy(), pos.copy()

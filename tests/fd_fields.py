@@ -80,7 +80,8 @@ def fd_grad(O, kind, case, conn, full: dict, W: dict, p: int, ax: int, elems, wh
 
     def dep(px, vx):
         return O.voxelize(kind, n=case["n"], bounds=case["bounds"], pos=px, vel=vx, conn=sub, mass=mass,
-                          periodic_box=case["periodic_box"], fields=flds)
+                          periodic_box=case["periodic_box"], fields=flds, reftol=case.get("reftol", 1.0),
+                          maxlvl=case.get("maxlvl", 0))
 
     R = raw_sums(full, r, s)
     b0 = raw_sums(dep(pos, vel), r, s)

@@ -49,12 +49,13 @@ def test_subset_fd_equals_whole_mesh_fd(oracle, kind):
         assert abs(sub - whole) <= 1e-6 * max(abs(whole), 1e-3), (p, ax, sub, whole)
 
 
+@pytest.mark.parametrize("refine", [(1.0, 0), (0.2, 2)])
 @pytest.mark.parametrize("kind", ["restatement", "reference"])
-def test_subset_fd_of_every_field_equals_whole_mesh_fd(oracle, kind):
+def test_subset_fd_of_every_field_equals_whole_mesh_fd(oracle, kind, refine):
     """The finite differences of a loss on every field (tests/fd_fields.py):
     re-depositing the elements around one particle, through per-voxel sums,
     gives the same central difference as re-depositing the whole mesh, for
-    positions and velocities."""
+    positions and velocities, with and without refinement of the elements."""
     if not oracle.available(kind):
         pytest.skip(f"{kind} library not built")
     from fd_fields import fd_grad, loss
@@ -62,13 +63,17 @@ def test_subset_fd_of_every_field_equals_whole_mesh_fd(oracle, kind):
 
     pos, vel = zeldovich(6, 1.0, 78)
     fields = ["x", "v", "xx", "xv", "vv"]
-    case = cases._block(pos, vel, 12, fields)
+    case = cases._block(pos, vel, 12, fields, reftol=refine[0], maxlvl=refine[1])
     conn = cases.conn_of(case)
     flat, vflat = pos.reshape(-1, 3), vel.reshape(-1, 3)
 
-    def dep(px, vx):
-        return oracle.voxelize(kind, n=case["n"], bounds=case["bounds"], pos=px, vel=vx, conn=conn,
-                               periodic_box=case["periodic_box"], fields=fields)
+    def dep(px, vx, k=kind, counters=False):
+        return oracle.voxelize(k, n=case["n"], bounds=case["bounds"], pos=px, vel=vx, conn=conn,
+                               periodic_box=case["periodic_box"], fields=fields, reftol=refine[0],
+                               maxlvl=refine[1], counters=counters)
+
+    if refine[1]:  # the tolerance refines some elements (the restatement counts the tets)
+        assert dep(flat, vflat, "restatement", True)[1]["tets"] > 6 * 6 ** 3
 
     full = dep(flat, vflat)
     rng = np.random.default_rng(2)

@@ -38,7 +38,8 @@ def _setup(case, target_sigma_cells=0.05, seed=5):
     rng = np.random.default_rng(seed)
     cell = (bounds[1][0] - bounds[0][0]) / n[0]
     tpos = pos + rng.normal(0.0, target_sigma_cells * cell, pos.shape)
-    kw = dict(n=n, bounds=bounds, periodic_box=case["periodic_box"])
+    kw = dict(n=n, bounds=bounds, periodic_box=case["periodic_box"], refine_tolerance=case.get("reftol", 1.0),
+              refine_max_lvl=case.get("maxlvl", 0))
     if case["kind"] == "block":
         kw["block_dims"] = case["pos"].shape[:3]
     else:
@@ -131,6 +132,15 @@ def test_adjoint_nonperiodic_block_with_masses(gpu, oracle):
     _check_fd(oracle, case, s, [_ref_kind(oracle)], 48)
 
 
+def test_adjoint_refined_block_mesh(gpu, oracle):
+    """Trilinear refinement up to 2 levels (midpoint criterion, tolerance 0.2 cells): the
+    gradient flows to the element corners through the trilinear weights of each refined vertex."""
+    case = cases.make("refine")
+    case["fields"] = []
+    s = _setup(case)
+    _check_fd(oracle, case, s, [_ref_kind(oracle)], 48)
+
+
 def test_adjoint_zero_inside_one_voxel(gpu):
     """A tet strictly inside one voxel deposits its whole mass there whatever its
     shape: the gradient is zero."""
@@ -189,8 +199,11 @@ def test_adjoint_rejects_unsupported(gpu):
     o = capi.Options(precision=0, memory=capi.PSIB_DEVICE, device=-1)
     import ctypes as C
 
-    rc = lib.psib_voxels_adjoint(C.byref(g), C.byref(m), 1.0, 2, gp.data_ptr(), None, None, C.byref(o))
-    assert rc == 6 and b"refine_max_lvl" in lib.psib_last_error()
+    z = torch.zeros((4, 4, 4, 3), dtype=torch.float64, device="cuda")
+    zm = torch.zeros((4, 4, 4), dtype=torch.float64, device="cuda")
+    gx = capi.make_grid((4, 4, 4), ((0.0,) * 3, (1.0,) * 3), {"m": zm.data_ptr(), "x": z.data_ptr()})
+    rc = lib.psib_voxels_adjoint(C.byref(gx), C.byref(m), 1.0, 0, gp.data_ptr(), None, None, C.byref(o))
+    assert rc == 6 and b"field m only" in lib.psib_last_error()
 
 
 def test_adjoint_directional_derivative_64cube_to_128cube(gpu):

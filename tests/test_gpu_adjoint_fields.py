@@ -8,6 +8,8 @@ pinned restatement where it is absent), moving one particle (or its velocity)
 and re-depositing the elements that contain it through per-voxel sums
 (tests/fd_fields.py).  Element-mass gradients are checked against the deposit
 of each element alone scaled (every field's sums are linear in a tet's mass).
+Refined elements (8-node trilinear and 27-node triquadratic, midpoint criterion)
+are checked the same way, the finite differences refining as the reference does.
 """
 import numpy as np
 import pytest
@@ -44,7 +46,8 @@ def _adjoint(case, W, with_mass=False):
     if case["mass"] is not None:
         mass = torch.from_numpy(np.ascontiguousarray(np.asarray(case["mass"], dtype=np.float64).reshape(-1))).cuda()
         mass.requires_grad_(with_mass)
-    kw = dict(n=case["n"], bounds=case["bounds"], periodic_box=case["periodic_box"], fields=ALL)
+    kw = dict(n=case["n"], bounds=case["bounds"], periodic_box=case["periodic_box"], fields=ALL,
+              refine_tolerance=case.get("reftol", 1.0), refine_max_lvl=case.get("maxlvl", 0))
     if case["kind"] == "block":
         kw["block_dims"] = case["pos"].shape[:3]
     else:
@@ -125,6 +128,62 @@ def test_adjoint_fields_simplex_masses(gpu, oracle, field):
         me = float(case["mass"][e])
         b = raw_sums(oracle.voxelize(kind, n=case["n"], bounds=case["bounds"], pos=case["pos"], vel=case["vel"],
                                      conn=conn[[e]], mass=np.array([me]), fields=ALL), r, s)
+        h = 1e-6 * me
+        lp = loss(fields_of({k: R[k] + b[k] * (h / me) for k in R}, r, s), W)
+        lm = loss(fields_of({k: R[k] - b[k] * (h / me) for k in R}, r, s), W)
+        want = (lp - lm) / (2 * h)
+        assert abs(gm[e] - want) <= 1e-5 * max(1.0, np.abs(gm).max()), (e, gm[e], want)
+
+
+def _refined_tets(case):
+    """Tets of the forward deposit (the stats of a psib_voxels call with the case's refinement)."""
+    import torch
+
+    from pypsi_b200 import capi
+
+    f = {"m": torch.zeros(case["n"], dtype=torch.float64, device="cuda")}
+    pos = torch.from_numpy(np.ascontiguousarray(case["pos"].reshape(-1, 3))).cuda()
+    kw = dict(refine_tolerance=case["reftol"], refine_max_lvl=case["maxlvl"], periodic_box=case["periodic_box"])
+    if case["kind"] == "block":
+        kw["block_dims"] = case["pos"].shape[:3]
+    else:
+        kw["connectivity"] = torch.from_numpy(np.ascontiguousarray(case["conn"], dtype=np.int32)).cuda()
+    return capi.voxels_device(f, case["n"], case["bounds"], pos, **kw)["tets"]
+
+
+@pytest.mark.parametrize("field", ["m", "x", "xx", "xv", "vv"])
+def test_adjoint_fields_refined_block_mesh(gpu, oracle, field):
+    """Trilinear refinement up to 2 levels (midpoint criterion, 0.2 cells): each refined
+    vertex passes its gradient to the 8 element corners with its trilinear weights."""
+    from pypsi_b200.synth import zeldovich
+
+    pos, vel = zeldovich(8, 2.0, 106)
+    case = cases._block(pos, vel, 16, ALL, reftol=0.2, maxlvl=2)
+    assert _refined_tets(case) > 6 * 8 ** 3
+    _check(oracle, case, field, 16, 11)
+
+
+@pytest.mark.parametrize("field", ["m", "xx", "vv"])
+def test_adjoint_fields_triquadratic_refined(gpu, oracle, field):
+    """27-node elements refined up to 2 levels: the triquadratic (Lagrange) weights of each
+    vertex on the element's 27 nodes, element masses included."""
+    from test_gpu_triquadratic import _quad_case
+
+    case = _quad_case(ne=4, maxlvl=2, reftol=0.02, seed=5)
+    assert _refined_tets(case) > 6 * 4 ** 3
+    _check(oracle, case, field, 16, 12)
+    kind = _kind(oracle)
+    conn = cases.conn_of(case)
+    ref = cases.run_oracle(oracle, dict(case, fields=ALL), kind=kind)
+    W = _weights(ref, field, 13)
+    _, _, _, gm = _adjoint(case, W, with_mass=True)
+    r, s = ref["x"], ref["v"]
+    R = raw_sums(ref, r, s)
+    for e in np.random.default_rng(4).choice(conn.shape[0], 6, replace=False):
+        me = float(case["mass"][e])
+        b = raw_sums(oracle.voxelize(kind, n=case["n"], bounds=case["bounds"], pos=case["pos"], vel=case["vel"],
+                                     conn=conn[[e]], mass=np.array([me]), fields=ALL, reftol=case["reftol"],
+                                     maxlvl=case["maxlvl"]), r, s)
         h = 1e-6 * me
         lp = loss(fields_of({k: R[k] + b[k] * (h / me) for k in R}, r, s), W)
         lm = loss(fields_of({k: R[k] - b[k] * (h / me) for k in R}, r, s), W)
