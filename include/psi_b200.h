@@ -184,7 +184,11 @@ int psib_voxels_batch(const psib_grid *grids, const psib_mesh *meshes, int nbatc
  * recomputed in FP64 (options->precision is ignored); each fragment's mass
  * fraction is differentiated through the faces it shares with its tet.
  * Gradients are summed with atomics, so the last bits may vary between runs.
- * Supported: refine_max_lvl = 0 for trilinear elements, and simplex elements.
+ * Elements are refined as psib_voxels refines them (refine_tolerance and
+ * refine_max_lvl of the forward call, midpoint criterion): a refined tet vertex
+ * passes its gradient to the element's nodes with the trilinear (8-node) or
+ * triquadratic (27-node) weights of its place in the element; the refinement
+ * decisions are piecewise constant and carry no gradient.
  * Memory and stream follow options as in psib_voxels. */
 int psib_voxels_adjoint(const psib_grid *grad, const psib_mesh *mesh, double refine_tolerance,
                         int refine_max_lvl, double *grad_pos, double *grad_vel, double *grad_mass,
@@ -206,8 +210,7 @@ int psib_voxels_adjoint(const psib_grid *grad, const psib_mesh *mesh, double ref
  * pairing of the x-v cross terms with the tet's first vertex
  * (src/geometry.c:137-146) is differentiated as it is.  Gradients are summed with
  * atomics, so the last bits may vary between runs.  Device memory only, on
- * options->stream; refine_max_lvl = 0 for trilinear elements, and simplex
- * elements. */
+ * options->stream.  Refinement as in psib_voxels_adjoint. */
 int psib_voxels_adjoint_fields(const psib_grid *grad, const psib_grid *fwd, const psib_mesh *mesh,
                                double refine_tolerance, int refine_max_lvl, double *grad_pos, double *grad_vel,
                                double *grad_mass, const psib_options *opt);
