@@ -479,7 +479,10 @@ __global__ void __launch_bounds__(BB, 7) k_bfs_level(BfsArgs a)
 
 // Moments (order 0..2) of the fragment about q-point o (the q of vertex 0),
 // by the fan triangles of reduce_about; the vertices' FP64 q are in qs as
-// [v * 3 + c][thread].
+// [v * 3 + c][thread].  One loop trip per fan triangle: a lane that finishes a
+// face finds the next one (integer work on the links) before the trip's
+// triangle, so the FP64 body runs with every lane that still has a triangle,
+// whatever the face sizes of the lanes' fragments.
 __device__ __forceinline__ unsigned leaf_moments(int nv, const uint32_t* nbs, const double* qs, int order, double* o,
                                                  double* mom)
 {
@@ -488,52 +491,62 @@ __device__ __forceinline__ unsigned leaf_moments(int nv, const uint32_t* nbs, co
     // directed edges not yet walked (3 * MAXV = 60 bits); the lowest first is
     // the face order of reduce_about
     uint64_t todo = (3 * nv >= 64) ? ~0ull : ((1ull << (3 * nv)) - 1ull);
-    while (todo) {
-        {
+    int vs = 0, vc = 0, vn = 0, steps = 0;
+    bool inface = false;
+    double q0x = 0.0, q0y = 0.0, q0z = 0.0;
+    for (;;) {
+        if (!inface) {
+            if (!todo) break;
             const int b0 = __ffsll((long long)todo) - 1;
             todo &= todo - 1ull;
-            const int vs = b0 / 3, ks = b0 - 3 * vs;
-            int vc = vs;
-            int vn = nbget(AT(nbs, vc), ks);
+            vs = b0 / 3;
+            vc = vs;
+            vn = nbget(AT(nbs, vc), b0 - 3 * vs);
             if (vn >= nv) return ST_GRAPH;
-            const double q0x = AT(qs, 3 * vs) - o[0], q0y = AT(qs, 3 * vs + 1) - o[1], q0z = AT(qs, 3 * vs + 2) - o[2];
-            uint32_t w = AT(nbs, vn);
-            int k = (nbget(w, 0) == vc) ? 0 : (nbget(w, 1) == vc) ? 1 : (nbget(w, 2) == vc) ? 2 : 3;
+            q0x = AT(qs, 3 * vs) - o[0];
+            q0y = AT(qs, 3 * vs + 1) - o[1];
+            q0z = AT(qs, 3 * vs + 2) - o[2];
+            const uint32_t w = AT(nbs, vn);
+            const int k = (nbget(w, 0) == vc) ? 0 : (nbget(w, 1) == vc) ? 1 : (nbget(w, 2) == vc) ? 2 : 3;
             if (k == 3) return ST_GRAPH;
             vc = vn;
-            int kn = (k + 1) % 3;
+            const int kn = (k + 1) % 3;
             todo &= ~(1ull << (3 * vc + kn));
             vn = nbget(AT(nbs, vc), kn);
-            int steps = 0;
-            while (vn != vs) {
-                if (++steps > WALK_CAP || vn >= nv) return ST_GRAPH;
-                const double q1x = AT(qs, 3 * vn) - o[0], q1y = AT(qs, 3 * vn + 1) - o[1], q1z = AT(qs, 3 * vn + 2) - o[2];
-                const double q2x = AT(qs, 3 * vc) - o[0], q2y = AT(qs, 3 * vc + 1) - o[1], q2z = AT(qs, 3 * vc + 2) - o[2];
-                const double m = (-q2x * q1y * q0z + q1x * q2y * q0z + q2x * q0y * q1z
-                                  - q0x * q2y * q1z - q1x * q0y * q2z + q0x * q1y * q2z);
-                mom[0] += m;
-                if (order > 0) {
-                    mom[1] += 0.25 * m * (q0x + q1x + q2x);
-                    mom[2] += 0.25 * m * (q0y + q1y + q2y);
-                    mom[3] += 0.25 * m * (q0z + q1z + q2z);
-                }
-                if (order > 1) {
-                    mom[4] += 0.1 * m * (q0x * q0x + q1x * q1x + q2x * q2x + q1x * q2x + q0x * (q1x + q2x));
-                    mom[5] += 0.05 * m * (q2x * q0y + q2x * q1y + 2 * q2x * q2y + q0x * (2 * q0y + q1y + q2y) + q1x * (q0y + 2 * q1y + q2y));
-                    mom[6] += 0.05 * m * (q2x * q0z + q2x * q1z + 2 * q2x * q2z + q0x * (2 * q0z + q1z + q2z) + q1x * (q0z + 2 * q1z + q2z));
-                    mom[7] += 0.1 * m * (q0y * q0y + q1y * q1y + q2y * q2y + q1y * q2y + q0y * (q1y + q2y));
-                    mom[8] += 0.05 * m * (q2y * q0z + q2y * q1z + 2 * q2y * q2z + q0y * (2 * q0z + q1z + q2z) + q1y * (q0z + 2 * q1z + q2z));
-                    mom[9] += 0.1 * m * (q0z * q0z + q1z * q1z + q2z * q2z + q1z * q2z + q0z * (q1z + q2z));
-                }
-                w = AT(nbs, vn);
-                k = (nbget(w, 0) == vc) ? 0 : (nbget(w, 1) == vc) ? 1 : (nbget(w, 2) == vc) ? 2 : 3;
-                if (k == 3) return ST_GRAPH;
-                vc = vn;
-                kn = (k + 1) % 3;
-                todo &= ~(1ull << (3 * vc + kn));
-                vn = nbget(AT(nbs, vc), kn);
+            steps = 0;
+            inface = vn != vs;
+            if (!inface) continue;
+        }
+        if (++steps > WALK_CAP || vn >= nv) return ST_GRAPH;
+        {
+            const double q1x = AT(qs, 3 * vn) - o[0], q1y = AT(qs, 3 * vn + 1) - o[1], q1z = AT(qs, 3 * vn + 2) - o[2];
+            const double q2x = AT(qs, 3 * vc) - o[0], q2y = AT(qs, 3 * vc + 1) - o[1], q2z = AT(qs, 3 * vc + 2) - o[2];
+            const double m = (-q2x * q1y * q0z + q1x * q2y * q0z + q2x * q0y * q1z
+                              - q0x * q2y * q1z - q1x * q0y * q2z + q0x * q1y * q2z);
+            mom[0] += m;
+            if (order > 0) {
+                mom[1] += 0.25 * m * (q0x + q1x + q2x);
+                mom[2] += 0.25 * m * (q0y + q1y + q2y);
+                mom[3] += 0.25 * m * (q0z + q1z + q2z);
+            }
+            if (order > 1) {
+                mom[4] += 0.1 * m * (q0x * q0x + q1x * q1x + q2x * q2x + q1x * q2x + q0x * (q1x + q2x));
+                mom[5] += 0.05 * m * (q2x * q0y + q2x * q1y + 2 * q2x * q2y + q0x * (2 * q0y + q1y + q2y) + q1x * (q0y + 2 * q1y + q2y));
+                mom[6] += 0.05 * m * (q2x * q0z + q2x * q1z + 2 * q2x * q2z + q0x * (2 * q0z + q1z + q2z) + q1x * (q0z + 2 * q1z + q2z));
+                mom[7] += 0.1 * m * (q0y * q0y + q1y * q1y + q2y * q2y + q1y * q2y + q0y * (q1y + q2y));
+                mom[8] += 0.05 * m * (q2y * q0z + q2y * q1z + 2 * q2y * q2z + q0y * (2 * q0z + q1z + q2z) + q1y * (q0z + 2 * q1z + q2z));
+                mom[9] += 0.1 * m * (q0z * q0z + q1z * q1z + q2z * q2z + q1z * q2z + q0z * (q1z + q2z));
             }
         }
+        // the next edge of the face
+        const uint32_t w = AT(nbs, vn);
+        const int k = (nbget(w, 0) == vc) ? 0 : (nbget(w, 1) == vc) ? 1 : (nbget(w, 2) == vc) ? 2 : 3;
+        if (k == 3) return ST_GRAPH;
+        vc = vn;
+        const int kn = (k + 1) % 3;
+        todo &= ~(1ull << (3 * vc + kn));
+        vn = nbget(AT(nbs, vc), kn);
+        inface = vn != vs;
     }
     return 0;
 }

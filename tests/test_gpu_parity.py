@@ -130,20 +130,30 @@ def test_fp64_central_near_exact(gpu, oracle, name, det):
 
 @pytest.mark.parametrize("name", NAMES)
 def test_atomic_sums_equal_sorted_records(gpu, name):
-    """The atomic mode adds the same fragments as the sorted mode, about the
-    voxel's centre and a tile velocity instead of the run's first fragment:
-    the two agree to rounding (1e-12 in the voxel-scale norm), and the FP64
-    path ignores the flag (always the reference's order)."""
+    """The atomic mode adds the same fragments as the sorted mode, about
+    reference points claimed by each voxel's first fragment instead of the
+    run's first fragment: the two agree to rounding, and the FP64 path ignores
+    the flag (always the reference's order).
+
+    Rounding here is the level at which two exact orders of the same FP64
+    fragments already differ: the reference's own order (fp64) against the
+    central merge in sorted order (fp64-central, deterministic).  Second
+    moments of voxels whose velocity spread is small against their mean
+    velocity lose digits in E[vv] - E[v]E[v] in any order (a few 1e-12 of the
+    voxel's scale at these sizes), so the bound is 4x that level, and never
+    below 1e-12."""
     c = make(name)
     a, _, _ = run_psi(gpu, c, precision="mixed", deterministic=False)
     b, _, _ = run_psi(gpu, c, precision="mixed", deterministic=True)
+    r64, _, _ = run_psi(gpu, c, precision="fp64")
+    assert gpu.last_stats()["accumulation"] == 0
+    rc, _, _ = run_psi(gpu, c, precision="fp64-central", deterministic=True)
+    level = field_errors(rc, r64)
     errs = field_errors(a, b)
     assert errs["m"]["rel"] <= 1e-12 and errs["dead_m"] == 0.0, (name, errs["m"])
     for f, e in errs.items():
         if f != "dead_m":
-            assert e["norm"] <= 1e-12, (name, f, e)
-    run_psi(gpu, c, precision="fp64", deterministic=False)
-    assert gpu.last_stats()["accumulation"] == 0
+            assert e["norm"] <= max(1e-12, 4.0 * level[f]["norm"]), (name, f, e, level[f])
 
 
 @pytest.mark.parametrize("gname", sorted(load_golden()))
