@@ -47,8 +47,8 @@ ALG_BYTES_PER_FRAGMENT = 88 + 192
 def clip_traffic_bytes(frags):
     """DRAM bytes the clip walk moves per step: the ncu capture of one
     64^3 -> 128^3 step (dram__bytes_read.sum + dram__bytes_write.sum over the
-    walk's launches, profiles/clip_walk_traffic_64cube_to_128cube.md) scaled by
-    the fragments of this step; None before a capture is recorded."""
+    walk's launches, kept with the other ncu summaries) scaled by the
+    fragments of this step; None before a capture is recorded."""
     if CLIP_TRAFFIC_PER_FRAGMENT is None:
         return None
     return {"bytes_per_step": CLIP_TRAFFIC_PER_FRAGMENT * frags,
@@ -56,8 +56,8 @@ def clip_traffic_bytes(frags):
                    f"{CLIP_TRAFFIC_PER_FRAGMENT:.0f} B per fragment, times this step's fragments"}
 
 
-# bytes per fragment of the capture above (None: no capture yet)
-CLIP_TRAFFIC_PER_FRAGMENT = None
+# bytes per fragment of the capture above (50.8 GB per call over 28.24 M fragments)
+CLIP_TRAFFIC_PER_FRAGMENT = 1800.0
 
 
 def parse():
