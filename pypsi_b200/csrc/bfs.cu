@@ -477,85 +477,123 @@ __global__ void __launch_bounds__(BB, 7) k_bfs_level(BfsArgs a)
 
 // ---- leaf: fragment moments and records ----
 
+struct D3 {
+    double x, y, z;
+};
+
+// The FP64 q of a leaf vertex beyond the shared-memory cache from its FP32
+// position x (relative to the image's vertex 0) and tags w; fr is the image's
+// frame, (d, w0) its grid's cell and origin, lo the fragment's voxel.  Out of
+// line and with plain scalar arguments, so that the rare call neither raises
+// the register count of the loop that makes it nor copies the kernel's
+// arguments to local memory.
+__device__ __noinline__ D3 leaf_q_slow(const double* fr, float x0, float x1, float x2, uint32_t w, double d0,
+                                       double d1, double d2, double o0, double o1, double o2, int l0, int l1, int l2)
+{
+    const double d[3] = {d0, d1, d2}, w0[3] = {o0, o1, o2};
+    const int lo[3] = {l0, l1, l2};
+    double p0[3], DX[3][3], plo[3], phi[3], tol[3];
+    for (int i = 0; i < 3; ++i) p0[i] = fr[i];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) DX[i][j] = fr[3 * (j + 1) + i] - p0[i];
+    for (int i = 0; i < 3; ++i) {
+        plo[i] = d[i] * lo[i] + w0[i];
+        phi[i] = d[i] * (lo[i] + 1) + w0[i];
+        tol[i] = 1.0e-3 * d[i];
+    }
+    const float x[3] = {x0, x1, x2};
+    double q[3];
+    exact_q(x, w, p0, DX, p0, plo, phi, tol, q);
+    return D3{q[0], q[1], q[2]};
+}
+
 // Moments (order 0..2) of the fragment about q-point o (the q of vertex 0),
 // by the fan triangles of reduce_about; the vertices' FP64 q are in qs as
-// [v * 3 + c][thread].  One loop trip per fan triangle: a lane that finishes a
-// face finds the next one (integer work on the links) before the trip's
-// triangle, so the FP64 body runs with every lane that still has a triangle,
-// whatever the face sizes of the lanes' fragments.
+// [v * 3 + c][thread] for v < QC, and solved again where a walk meets a
+// vertex beyond the cache (leaf_q_slow).
+template <int QC>
 __device__ __forceinline__ unsigned leaf_moments(int nv, const uint32_t* nbs, const double* qs, int order, double* o,
-                                                 double* mom)
+                                                 double* mom, const BfsArgs& a, unsigned long long e, uint32_t t,
+                                                 const int* lo)
 {
+    auto Q = [&](int v) -> D3 {
+        if (QC >= MAXV || v < QC) return D3{AT(qs, 3 * v), AT(qs, 3 * v + 1), AT(qs, 3 * v + 2)};
+        const GridDev& g = grid_of(a.c, t);
+        return leaf_q_slow(a.c.it.frame + (size_t)t * FRAME, a.leaf.x[qx(e, v, 0)], a.leaf.x[qx(e, v, 1)],
+                           a.leaf.x[qx(e, v, 2)], AT(nbs, v), g.d[0], g.d[1], g.d[2], g.w0[0], g.w0[1], g.w0[2],
+                           lo[0], lo[1], lo[2]);
+    };
     for (int i = 0; i < 3; ++i) o[i] = AT(qs, i);
     for (int i = 0; i < 10; ++i) mom[i] = 0.0;
     // directed edges not yet walked (3 * MAXV = 60 bits); the lowest first is
     // the face order of reduce_about
     uint64_t todo = (3 * nv >= 64) ? ~0ull : ((1ull << (3 * nv)) - 1ull);
-    int vs = 0, vc = 0, vn = 0, steps = 0;
-    bool inface = false;
-    double q0x = 0.0, q0y = 0.0, q0z = 0.0;
-    for (;;) {
-        if (!inface) {
-            if (!todo) break;
+    while (todo) {
+        {
             const int b0 = __ffsll((long long)todo) - 1;
             todo &= todo - 1ull;
-            vs = b0 / 3;
-            vc = vs;
-            vn = nbget(AT(nbs, vc), b0 - 3 * vs);
+            const int vs = b0 / 3, ks = b0 - 3 * vs;
+            int vc = vs;
+            int vn = nbget(AT(nbs, vc), ks);
             if (vn >= nv) return ST_GRAPH;
-            q0x = AT(qs, 3 * vs) - o[0];
-            q0y = AT(qs, 3 * vs + 1) - o[1];
-            q0z = AT(qs, 3 * vs + 2) - o[2];
-            const uint32_t w = AT(nbs, vn);
-            const int k = (nbget(w, 0) == vc) ? 0 : (nbget(w, 1) == vc) ? 1 : (nbget(w, 2) == vc) ? 2 : 3;
+            const D3 Q0 = Q(vs);
+            const double q0x = Q0.x - o[0], q0y = Q0.y - o[1], q0z = Q0.z - o[2];
+            uint32_t w = AT(nbs, vn);
+            int k = (nbget(w, 0) == vc) ? 0 : (nbget(w, 1) == vc) ? 1 : (nbget(w, 2) == vc) ? 2 : 3;
             if (k == 3) return ST_GRAPH;
             vc = vn;
-            const int kn = (k + 1) % 3;
+            int kn = (k + 1) % 3;
             todo &= ~(1ull << (3 * vc + kn));
             vn = nbget(AT(nbs, vc), kn);
-            steps = 0;
-            inface = vn != vs;
-            if (!inface) continue;
-        }
-        if (++steps > WALK_CAP || vn >= nv) return ST_GRAPH;
-        {
-            const double q1x = AT(qs, 3 * vn) - o[0], q1y = AT(qs, 3 * vn + 1) - o[1], q1z = AT(qs, 3 * vn + 2) - o[2];
-            const double q2x = AT(qs, 3 * vc) - o[0], q2y = AT(qs, 3 * vc + 1) - o[1], q2z = AT(qs, 3 * vc + 2) - o[2];
-            const double m = (-q2x * q1y * q0z + q1x * q2y * q0z + q2x * q0y * q1z
-                              - q0x * q2y * q1z - q1x * q0y * q2z + q0x * q1y * q2z);
-            mom[0] += m;
-            if (order > 0) {
-                mom[1] += 0.25 * m * (q0x + q1x + q2x);
-                mom[2] += 0.25 * m * (q0y + q1y + q2y);
-                mom[3] += 0.25 * m * (q0z + q1z + q2z);
+            int steps = 0;
+            while (vn != vs) {
+                if (++steps > WALK_CAP || vn >= nv) return ST_GRAPH;
+                const D3 Q1 = Q(vn), Q2 = Q(vc);
+                const double q1x = Q1.x - o[0], q1y = Q1.y - o[1], q1z = Q1.z - o[2];
+                const double q2x = Q2.x - o[0], q2y = Q2.y - o[1], q2z = Q2.z - o[2];
+                const double m = (-q2x * q1y * q0z + q1x * q2y * q0z + q2x * q0y * q1z
+                                  - q0x * q2y * q1z - q1x * q0y * q2z + q0x * q1y * q2z);
+                mom[0] += m;
+                if (order > 0) {
+                    mom[1] += 0.25 * m * (q0x + q1x + q2x);
+                    mom[2] += 0.25 * m * (q0y + q1y + q2y);
+                    mom[3] += 0.25 * m * (q0z + q1z + q2z);
+                }
+                if (order > 1) {
+                    mom[4] += 0.1 * m * (q0x * q0x + q1x * q1x + q2x * q2x + q1x * q2x + q0x * (q1x + q2x));
+                    mom[5] += 0.05 * m * (q2x * q0y + q2x * q1y + 2 * q2x * q2y + q0x * (2 * q0y + q1y + q2y) + q1x * (q0y + 2 * q1y + q2y));
+                    mom[6] += 0.05 * m * (q2x * q0z + q2x * q1z + 2 * q2x * q2z + q0x * (2 * q0z + q1z + q2z) + q1x * (q0z + 2 * q1z + q2z));
+                    mom[7] += 0.1 * m * (q0y * q0y + q1y * q1y + q2y * q2y + q1y * q2y + q0y * (q1y + q2y));
+                    mom[8] += 0.05 * m * (q2y * q0z + q2y * q1z + 2 * q2y * q2z + q0y * (2 * q0z + q1z + q2z) + q1y * (q0z + 2 * q1z + q2z));
+                    mom[9] += 0.1 * m * (q0z * q0z + q1z * q1z + q2z * q2z + q1z * q2z + q0z * (q1z + q2z));
+                }
+                w = AT(nbs, vn);
+                k = (nbget(w, 0) == vc) ? 0 : (nbget(w, 1) == vc) ? 1 : (nbget(w, 2) == vc) ? 2 : 3;
+                if (k == 3) return ST_GRAPH;
+                vc = vn;
+                kn = (k + 1) % 3;
+                todo &= ~(1ull << (3 * vc + kn));
+                vn = nbget(AT(nbs, vc), kn);
             }
-            if (order > 1) {
-                mom[4] += 0.1 * m * (q0x * q0x + q1x * q1x + q2x * q2x + q1x * q2x + q0x * (q1x + q2x));
-                mom[5] += 0.05 * m * (q2x * q0y + q2x * q1y + 2 * q2x * q2y + q0x * (2 * q0y + q1y + q2y) + q1x * (q0y + 2 * q1y + q2y));
-                mom[6] += 0.05 * m * (q2x * q0z + q2x * q1z + 2 * q2x * q2z + q0x * (2 * q0z + q1z + q2z) + q1x * (q0z + 2 * q1z + q2z));
-                mom[7] += 0.1 * m * (q0y * q0y + q1y * q1y + q2y * q2y + q1y * q2y + q0y * (q1y + q2y));
-                mom[8] += 0.05 * m * (q2y * q0z + q2y * q1z + 2 * q2y * q2z + q0y * (2 * q0z + q1z + q2z) + q1y * (q0z + 2 * q1z + q2z));
-                mom[9] += 0.1 * m * (q0z * q0z + q1z * q1z + q2z * q2z + q1z * q2z + q0z * (q1z + q2z));
-            }
         }
-        // the next edge of the face
-        const uint32_t w = AT(nbs, vn);
-        const int k = (nbget(w, 0) == vc) ? 0 : (nbget(w, 1) == vc) ? 1 : (nbget(w, 2) == vc) ? 2 : 3;
-        if (k == 3) return ST_GRAPH;
-        vc = vn;
-        const int kn = (k + 1) % 3;
-        todo &= ~(1ull << (3 * vc + kn));
-        vn = nbget(AT(nbs, vc), kn);
-        inface = vn != vs;
     }
     return 0;
 }
 
-__global__ void __launch_bounds__(BB, 3) k_bfs_leaf(BfsArgs a)
+// q-cache sizes of the two leaf kernels: every vertex where the kernel adds its fragments itself
+// (168 registers, three blocks per SM), the first 14 where it writes records (four blocks per SM:
+// tet-voxel fragments have at most 16 vertices and 7.2 on average, so few walks reach past it)
+constexpr int QC_REC = 14;
+
+// INLINE: atomic mode, each fragment added to its voxel's sums here; else a record per fragment
+// (sorted mode: sorted and applied after the walk; atomic mode: added by k_acc_records).
+template <bool INLINE>
+__global__ void __launch_bounds__(BB, INLINE ? 3 : 4) k_bfs_leaf(BfsArgs a)
 {
+    constexpr int QC = INLINE ? MAXV : QC_REC;
     extern __shared__ uint32_t smem[];
     uint32_t* nbs = smem;
-    double* qs = (double*)(smem + MAXV * BB); // [v * 3 + c][thread]
+    double* qs = (double*)(smem + MAXV * BB); // [v * 3 + c][thread], v < QC
     const int lane = threadIdx.x & 31;
     const long long warp = (long long)blockIdx.x * (BB / 32) + (threadIdx.x >> 5);
     const long long nwarp = (long long)gridDim.x * (BB / 32);
@@ -589,6 +627,7 @@ __global__ void __launch_bounds__(BB, 3) k_bfs_leaf(BfsArgs a)
                 for (int v = 0; v < nv; ++v) {
                     const uint32_t w = a.leaf.nb[qn(e, v)];
                     AT(nbs, v) = w;
+                    if (QC < MAXV && v >= QC) continue; // solved where the walk meets it
                     const float x[3] = {a.leaf.x[qx(e, v, 0)], a.leaf.x[qx(e, v, 1)], a.leaf.x[qx(e, v, 2)]};
                     double q[3];
                     exact_q(x, w, p0, DX, p0, plo, phi, tol, q);
@@ -596,7 +635,7 @@ __global__ void __launch_bounds__(BB, 3) k_bfs_leaf(BfsArgs a)
                 }
                 moved += elem_bytes(nv) + 96; // the fragment and its image's vertices
                 double o[3], mom[10];
-                const unsigned e2 = leaf_moments(nv, nbs, qs, c.mom_order, o, mom);
+                const unsigned e2 = leaf_moments<QC>(nv, nbs, qs, c.mom_order, o, mom, a, e, t, lo);
                 if (e2) {
                     st |= e2;
                 } else if (mom[0] > 0.0) {
@@ -619,7 +658,7 @@ __global__ void __launch_bounds__(BB, 3) k_bfs_leaf(BfsArgs a)
                         rec[9] = mom[9] / m0 - u[2] * u[2];
                         ++frags;
                         verts += nv;
-                        if (c.acc.sum) {
+                        if constexpr (INLINE) {
                             // atomic mode: straight into the voxel's sums, no record
                             const double f = c.acc.factor ? c.acc.factor[t] : 1.0;
                             accumulate_fragment(c, g, c.grids ? (int)c.it.grid[t] : 0, gi, lo, t, rec, f);
@@ -655,15 +694,45 @@ __global__ void __launch_bounds__(BB, 3) k_bfs_leaf(BfsArgs a)
     if (a.bytes && moved) atomicAdd(a.bytes, moved);
 }
 
+// Atomic mode through records: every record of the leaf launch before it added to its
+// voxel's sums (the key gives the voxel and the image), as the inline leaf kernel adds its
+// fragments.  Consecutive records come from consecutive leaf-queue entries, so a warp's
+// atomics stay near one another in the grid.
+__global__ void __launch_bounds__(128) k_acc_records(BfsArgs a)
+{
+    const ClipArgs& c = a.c;
+    const unsigned long long n = min(*c.rec_n, c.rec_cap);
+    const unsigned long long imask = (1ull << c.rec_ibits) - 1ull;
+    for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n;
+         i += (unsigned long long)gridDim.x * blockDim.x) {
+        const unsigned long long key = c.rec_key[i];
+        const long long t = (long long)(key & imask) + c.rec_item_base;
+        const long long gi = (long long)(key >> c.rec_ibits);
+        const GridDev& g = grid_of(c, t);
+        const long long local = gi - (long long)(c.voff ? c.voff[c.it.grid[t]] : 0ull);
+        const int lo[3] = {(int)(local / ((long long)g.n[1] * g.n[2])), (int)((local / g.n[2]) % g.n[1]),
+                           (int)(local % g.n[2])};
+        double rec[10];
+        const double* src = c.rec_mom + i * c.rec_nmom;
+#pragma unroll
+        for (int k = 0; k < 10; ++k) rec[k] = k < c.rec_nmom ? src[k] : 0.0;
+        const double f = c.acc.factor ? c.acc.factor[t] : 1.0;
+        accumulate_fragment(c, g, c.grids ? (int)c.it.grid[t] : 0, gi, lo, t, rec, f);
+    }
+}
+
 // FP32 walks can misplace a vertex that falls back to its FP32 position by
 // ~1e-7 of the tet: each breadth-first image's fragment masses are scaled by
 // target / (sum of its fragment q-volumes), so that it deposits exactly its
 // mass inside the window.  init stores -target in scale (1, or the image's
-// exact FP64 q-volume inside the window).
+// exact FP64 q-volume inside the window).  The deep-tree images (key KEY_DEEP)
+// are not the walk's: their kernel, which may run beside this one, sets their
+// scale itself.
 __global__ void k_bfs_finalize(BfsArgs a, long long nitems)
 {
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nitems; t += (long long)gridDim.x * blockDim.x)
-        if (a.c.scale[t] < 0.0) a.c.scale[t] = a.vsum[t] > 0.0 ? -a.c.scale[t] / a.vsum[t] : 1.0;
+        if (a.c.it.key[t] < KEY_DEEP && a.c.scale[t] < 0.0)
+            a.c.scale[t] = a.vsum[t] > 0.0 ? -a.c.scale[t] / a.vsum[t] : 1.0;
 }
 
 __global__ void k_bfs_advance(BfsArgs a) { ++*a.pass_idx; }
@@ -683,23 +752,30 @@ cudaError_t launch_bfs_finalize(const BfsArgs& a, long long nitems, int num_sms,
 // ---- launchers ----
 
 static constexpr size_t LEVEL_SMEM = 3 * MAXV * BB * sizeof(uint32_t); // links of the cut polyhedron and its children
-static constexpr size_t LEAF_SMEM = MAXV * BB * (sizeof(uint32_t) + 3 * sizeof(double));
+// links of every vertex, FP64 q of the cached ones
+static constexpr size_t LEAF_SMEM = MAXV * BB * sizeof(uint32_t) + 3 * MAXV * BB * sizeof(double);
+static constexpr size_t LEAF_REC_SMEM = MAXV * BB * sizeof(uint32_t) + 3 * QC_REC * BB * sizeof(double);
 
 // resident blocks per SM of each kernel (one full wave of grid-stride blocks)
-static int g_blocks[3] = {0, 0, 0};
+static int g_blocks[5] = {0, 0, 0, 0, 0};
 static void occupancy();
 void bfs_prepare() { occupancy(); }
 static void occupancy()
 {
     if (g_blocks[0]) return;
     cudaFuncSetAttribute(k_bfs_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LEVEL_SMEM);
-    cudaFuncSetAttribute(k_bfs_leaf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LEAF_SMEM);
-    int b[3] = {1, 1, 1};
+    cudaFuncSetAttribute(k_bfs_leaf<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LEAF_SMEM);
+    cudaFuncSetAttribute(k_bfs_leaf<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LEAF_REC_SMEM);
+    int b[5] = {1, 1, 1, 1, 1};
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b[0], k_bfs_init, BB, 0) != cudaSuccess) b[0] = 1;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b[1], k_bfs_level, BB, LEVEL_SMEM) != cudaSuccess) b[1] = 1;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b[2], k_bfs_leaf, BB, LEAF_SMEM) != cudaSuccess) b[2] = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b[2], k_bfs_leaf<true>, BB, LEAF_SMEM) != cudaSuccess)
+        b[2] = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b[3], k_bfs_leaf<false>, BB, LEAF_REC_SMEM) != cudaSuccess)
+        b[3] = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b[4], k_acc_records, 128, 0) != cudaSuccess) b[4] = 1;
     cudaGetLastError();
-    for (int i = 0; i < 3; ++i) g_blocks[i] = b[i] > 0 ? b[i] : 1;
+    for (int i = 0; i < 5; ++i) g_blocks[i] = b[i] > 0 ? b[i] : 1;
 }
 
 cudaError_t launch_bfs_init(const BfsArgs& a, int num_sms, cudaStream_t s)
@@ -719,8 +795,17 @@ cudaError_t launch_bfs_level(const BfsArgs& a, int num_sms, cudaStream_t s)
 cudaError_t launch_bfs_leaf(const BfsArgs& a, int num_sms, cudaStream_t s)
 {
     occupancy();
-    k_bfs_leaf<<<num_sms * g_blocks[2], BB, LEAF_SMEM, s>>>(a);
-    return cudaGetLastError();
+    if (a.c.acc.sum && !a.leaf_records) {
+        k_bfs_leaf<true><<<num_sms * g_blocks[2], BB, LEAF_SMEM, s>>>(a);
+        return cudaGetLastError();
+    }
+    k_bfs_leaf<false><<<num_sms * g_blocks[3], BB, LEAF_REC_SMEM, s>>>(a);
+    if (!a.c.acc.sum) return cudaGetLastError(); // sorted mode: the records wait for the sort
+    k_acc_records<<<num_sms * g_blocks[4], 128, 0, s>>>(a);
+    cudaError_t e = cudaGetLastError();
+    // the next leaf launch writes its records from the start of the buffer
+    if (e == cudaSuccess) e = cudaMemsetAsync(a.c.rec_n, 0, sizeof(unsigned long long), s);
+    return e;
 }
 
 } // namespace psib

@@ -104,6 +104,8 @@ struct Ctx {
     cudaStream_t copy = nullptr; // host-memory calls: the field copies, beside the first stages
     cudaEvent_t fields_in = nullptr;
     cudaEvent_t enter = nullptr, leave = nullptr; // device-memory calls: fences with the caller's stream
+    cudaStream_t side = nullptr; // atomic mode: the deep-tree images, beside the breadth-first walk
+    cudaEvent_t fork = nullptr, join = nullptr;
     cudaEvent_t ev_out[NOUT] = {};
     cudaEvent_t ev[8] = {};
     // host-mode copies
@@ -176,6 +178,9 @@ int get_ctx(int dev, Ctx** out)
         CK(cudaEventCreateWithFlags(&c->fields_in, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&c->enter, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&c->leave, cudaEventDisableTiming));
+        CK(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming));
         for (auto& e : c->ev_out) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         for (auto& e : c->ev) CK(cudaEventCreate(&e));
         g_ctx[dev] = c;
@@ -538,6 +543,20 @@ int bfs_clip(Ctx& C, ClipArgs& ca, long long nmain, long long nitems, unsigned l
     ba.dfs_count = &sm[S_DFS];
     ba.bytes = &sm[S_BYTES];
     ba.window_bfs = env_ll("PSIB_BFS_WINDOW", 1) != 0;
+    // Atomic sums: the leaf kernel writes a record per fragment and k_acc_records adds each leaf
+    // launch's records right after it (a leaf launch has at most one record per leaf-queue entry);
+    // the leaf kernel then needs fewer registers and less shared memory than one that adds its
+    // fragments itself (PSIB_LEAF_RECORDS=0).
+    if (ca.acc.sum && ca.rec_ibits > 0 && env_ll("PSIB_LEAF_RECORDS", 1) != 0) {
+        const size_t nrec = tiles * 32;
+        RET(ensure(C.rkey, nrec * sizeof(unsigned long long)));
+        RET(ensure(C.rmom, nrec * ca.rec_nmom * sizeof(double)));
+        ba.c.rec_key = C.rkey.as<unsigned long long>();
+        ba.c.rec_mom = C.rmom.as<double>();
+        ba.c.rec_cap = nrec;
+        CK(cudaMemsetAsync(ba.c.rec_n, 0, sizeof(unsigned long long), st));
+        ba.leaf_records = 1;
+    }
     RET(ensure(C.vsum, (size_t)std::max<long long>(nitems, 1) * sizeof(double)));
     ba.vsum = C.vsum.as<double>();
     // the pass table on the device; a device counter picks the pass, so every pass runs
@@ -591,7 +610,7 @@ int bfs_clip(Ctx& C, ClipArgs& ca, long long nmain, long long nitems, unsigned l
     }
     if (!graphed)
         for (long long p = 0; p < npass; ++p) CK(pass(st));
-    klaunch += (3 + 2 * NLEV) * npass;
+    klaunch += (3 + 2 * NLEV + (ba.leaf_records ? NLEV + 1 : 0)) * npass;
     launches += (2 + 2 * NLEV) * npass;
     if (sizes) {
         sizes->tiles = (long long)tiles;
@@ -867,7 +886,9 @@ int run_device(Call& c)
     }
 
     // ---- chunking: images are streamed in element chunks of at most `budget` ----
-    const long long budget = env_ll("PSIB_ITEM_BUDGET", 16ll << 20);
+    // (a capture plan keeps every image in one chunk, as the capture call has no host loop)
+    long long budget = env_ll("PSIB_ITEM_BUDGET", 16ll << 20);
+    if (c.capture == 1) budget = std::max(budget, total);
     std::vector<long long> cb; // element boundaries
     cb.push_back(0);
     if (total > budget) {
@@ -1066,6 +1087,14 @@ int run_device(Call& c)
         }
         if (atomic) {
             // ---- clip, each fragment added to its voxel's sums ----
+            {
+                // a record key (voxel | image) for the walk's leaf records, when both fit in 64 bits
+                int ib = 1, vb = 1;
+                while ((1ll << ib) < nitems) ++ib;
+                while ((1ll << vb) < nvox) ++vb;
+                ca.rec_ibits = ib + vb <= 64 ? ib : 0;
+                ca.rec_item_base = 0;
+            }
             CK(cudaMemsetAsync(&sm[S_BYTES], 0, 8, st));
             CK(cudaMemsetAsync(&sm[S_CNT], 0, 24, st));
             CK(cudaMemsetAsync(&sm[S_HEAD], 0, 16, st));
@@ -1075,6 +1104,25 @@ int run_device(Call& c)
                 CK(cudaMemsetAsync(C.acc_tsum.p, 0, (size_t)ntiles * 4 * sizeof(double), st));
                 CK(launch_vref(it, nitems, gd, d_grids, ca.acc, C.acc_tsum.as<double>(), ntiles, C.num_sms, st));
                 klaunch += 2;
+            }
+            // The deep-tree images run on a side stream beside the breadth-first walk: both add to the
+            // per-voxel sums with atomics, touch disjoint images and their own scratch, and the mass
+            // correction below waits for both.
+            bool deep_beside = false;
+            if (ndeep > 0 && nmain > 0 && use_bfs) {
+                const int big_grid = (int)std::min<long long>(C.num_sms * 2, (ndeep + big_block - 1) / big_block);
+                RET(ensure(C.scratch_big, big_bytes * (size_t)big_grid * big_block));
+                ClipArgs cd = ca;
+                cd.scratch = C.scratch_big.p;
+                cd.order_base = nmain;
+                cd.n = ndeep;
+                cd.head = &sm[S_HEAD + 1];
+                CK(cudaEventRecord(C.fork, st));
+                CK(cudaStreamWaitEvent(C.side, C.fork, 0));
+                CK(launch_clip_mixed(cd, true, !mixed, big_grid, big_block, C.side));
+                CK(cudaEventRecord(C.join, C.side));
+                launches++;
+                deep_beside = true;
             }
             if (nmain > 0 && use_bfs) {
                 ca.scratch = C.scratch.p;
@@ -1088,7 +1136,9 @@ int run_device(Call& c)
                 CK(launch_clip_mixed(ca, false, !mixed, clip_grid, clip_block, st));
                 launches++;
             }
-            if (ndeep > 0) {
+            if (deep_beside) {
+                CK(cudaStreamWaitEvent(st, C.join, 0));
+            } else if (ndeep > 0) {
                 const int big_grid = (int)std::min<long long>(C.num_sms * 2, (ndeep + big_block - 1) / big_block);
                 RET(ensure(C.scratch_big, big_bytes * (size_t)big_grid * big_block));
                 ca.scratch = C.scratch_big.p;

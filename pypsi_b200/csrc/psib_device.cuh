@@ -501,69 +501,23 @@ __device__ __forceinline__ bool solve3(const double (*n)[3], const double* b, do
     return true;
 }
 
-// Coordinate a of tet vertex j relative to vertex 0 (0 for j = 0): DX[a][j - 1], by selects so
-// that DX stays in registers.
-__device__ __forceinline__ double tet_coord(const double (*DX)[3], int a, int j)
+// Plane idx of a vertex's tags as a row n . q = b: idx 0..3 is the tet face
+// opposite vertex idx (qx + qy + qz = 1, or q_{idx-1} = 0), idx 4..6 the grid
+// plane x_a = pc_a (a = idx - 4), i.e. DX[a] . q = pc_a - p0_a.  Selects by
+// value so that everything stays in registers.
+__device__ __forceinline__ void plane_row(int idx, const double (*DX)[3], const double* pc, const double* p0,
+                                          double* n, double& b)
 {
-    const double r0 = a == 0 ? DX[0][0] : a == 1 ? DX[1][0] : DX[2][0];
-    const double r1 = a == 0 ? DX[0][1] : a == 1 ? DX[1][1] : DX[2][1];
-    const double r2 = a == 0 ? DX[0][2] : a == 1 ? DX[1][2] : DX[2][2];
-    return j == 1 ? r0 : j == 2 ? r1 : j == 3 ? r2 : 0.0;
-}
-
-// q of a point given by three planes, by the shape of its tags (the tet-face tags tf select the
-// vertices j of the tet whose face it does not lie on; q(j) is the unit vector e_{j-1}, q(0) = 0):
-//   3 faces           the tet vertex j itself
-//   2 faces, 1 plane  on the edge (j1, j2): one division along grid axis a
-//   1 face, 2 planes  on the face (j1, j2, j3): a 2 x 2 solve in the face's own coordinates
-//   3 planes          the voxel corner: the 3 x 3 solve of DX q = pc - p0
-// A tet-face tag i is the row q1 + q2 + q3 = 1 (i = 0) or q_i = 0, a grid-plane tag on axis a the
-// row DX[a] . q = pc_a - p0_a; each case solves its three rows for only the unknowns they leave.
-// False when the system is singular.
-__device__ __forceinline__ bool tagged_q(uint32_t tf, uint32_t ap, const double (*DX)[3], const double* pc,
-                                         const double* p0, double* q)
-{
-    const int nf = __popc(tf);
-    const uint32_t fr = ~tf & 0xFu; // tet vertices off the tagged faces
-    if (nf == 3) {
-        const int j = __ffs(fr) - 1;
-        for (int c = 0; c < 3; ++c) q[c] = j == c + 1 ? 1.0 : 0.0;
-        return true;
+    if (idx < 4) {
+        n[0] = (idx == 0 || idx == 1) ? 1.0 : 0.0;
+        n[1] = (idx == 0 || idx == 2) ? 1.0 : 0.0;
+        n[2] = (idx == 0 || idx == 3) ? 1.0 : 0.0;
+        b = idx == 0 ? 1.0 : 0.0;
+    } else {
+        const int a = idx - 4;
+        for (int c = 0; c < 3; ++c) n[c] = a == 0 ? DX[0][c] : a == 1 ? DX[1][c] : DX[2][c];
+        b = a == 0 ? pc[0] - p0[0] : a == 1 ? pc[1] - p0[1] : pc[2] - p0[2];
     }
-    if (nf == 2) {
-        const int j1 = __ffs(fr) - 1, j2 = __ffs(fr & (fr - 1u)) - 1;
-        const int a = __ffs(ap) - 1;
-        const double d1 = tet_coord(DX, a, j1), d2 = tet_coord(DX, a, j2);
-        const double den = d2 - d1;
-        if (!(den != 0.0)) return false;
-        const double t = ((pc[a] - p0[a]) - d1) / den;
-        if (!isfinite(t)) return false;
-        for (int c = 0; c < 3; ++c) q[c] = (j1 == c + 1 ? 1.0 - t : 0.0) + (j2 == c + 1 ? t : 0.0);
-        return true;
-    }
-    if (nf == 1) {
-        uint32_t m = fr;
-        const int j1 = __ffs(m) - 1;
-        m &= m - 1u;
-        const int j2 = __ffs(m) - 1;
-        m &= m - 1u;
-        const int j3 = __ffs(m) - 1;
-        const int a = __ffs(ap) - 1, b = __ffs(ap & (ap - 1u)) - 1;
-        const double a1 = tet_coord(DX, a, j1), b1 = tet_coord(DX, b, j1);
-        const double A00 = tet_coord(DX, a, j2) - a1, A01 = tet_coord(DX, a, j3) - a1;
-        const double A10 = tet_coord(DX, b, j2) - b1, A11 = tet_coord(DX, b, j3) - b1;
-        const double r0 = (pc[a] - p0[a]) - a1, r1 = (pc[b] - p0[b]) - b1;
-        const double det = A00 * A11 - A01 * A10;
-        if (!(det != 0.0) || !isfinite(det)) return false;
-        const double id = 1.0 / det;
-        const double sv = (r0 * A11 - A01 * r1) * id, tv = (A00 * r1 - r0 * A10) * id;
-        const double uv = 1.0 - sv - tv;
-        for (int c = 0; c < 3; ++c)
-            q[c] = (j1 == c + 1 ? uv : 0.0) + (j2 == c + 1 ? sv : 0.0) + (j3 == c + 1 ? tv : 0.0);
-        return true;
-    }
-    const double bb[3] = {pc[0] - p0[0], pc[1] - p0[1], pc[2] - p0[2]};
-    return solve3(DX, bb, q);
 }
 
 // q of one vertex of an FP32 fragment: x is its FP32 position relative to org,
@@ -594,8 +548,22 @@ __device__ __forceinline__ void exact_q(const float* x, uint32_t w, const double
         if (far < 0) break;
         ap &= ~(1u << far);
     }
+    double n0[3], n1[3], n2[3], b0, b1, b2;
     bool ok = __popc(tf) + __popc(ap) == 3;
-    if (ok) ok = tagged_q(tf, ap, DX, pc, p0, q);
+    if (ok) {
+        uint32_t m = tf | (ap << 4);
+        const int i0 = __ffs(m) - 1;
+        m &= m - 1;
+        const int i1 = __ffs(m) - 1;
+        m &= m - 1;
+        const int i2 = __ffs(m) - 1;
+        plane_row(i0, DX, pc, p0, n0, b0);
+        plane_row(i1, DX, pc, p0, n1, b1);
+        plane_row(i2, DX, pc, p0, n2, b2);
+        const double nn[3][3] = {{n0[0], n0[1], n0[2]}, {n1[0], n1[1], n1[2]}, {n2[0], n2[1], n2[2]}};
+        const double bb[3] = {b0, b1, b2};
+        ok = solve3(nn, bb, q);
+    }
     if (!ok) {
         // position -> q through the tet's own map: rows DX[a], right side x_a - x0_a
         const double bb[3] = {((double)x[0] + org[0]) - p0[0], ((double)x[1] + org[1]) - p0[1],

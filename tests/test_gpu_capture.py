@@ -5,7 +5,8 @@ the capture call (capture = 2) then runs with no host synchronisation and no
 allocation, so torch.cuda.graph can record it.  Replays of that graph must
 deposit what plain calls deposit, on the particle arrays as they are at replay
 time -- the mixed atomic path on both sides, so the fields agree to rounding
-(1e-12 in the voxel-scale norm) rather than bit for bit.  The spatial tile of
+(mass to 1e-12, the other fields to NORM_TOL in the voxel-scale norm) rather
+than bit for bit.  The spatial tile of
 the work order (psib_options.order_cell_bits) changes the order of the atomic
 sums only.
 """
@@ -42,6 +43,13 @@ def _plain(cutouts, **kw):
     return _host(cutouts)
 
 
+# Two orders of the same atomic sums differ by rounding; second moments of voxels made of tiny
+# fragments lose digits in E[vv] - E[v]E[v] (the reference's own FP64 order and the central merge
+# of the same fragments differ by ~4e-12 of a voxel's scale at these sizes), so the bound on the
+# voxel-scale norm is a few times that level.
+NORM_TOL = 2e-11
+
+
 def _agree(a, b, what):
     for i, (s, t) in enumerate(zip(a, b)):
         assert s["m"].sum() > 0, (what, i)
@@ -49,7 +57,7 @@ def _agree(a, b, what):
         assert errs["m"]["rel"] <= 1e-12 and errs["dead_m"] == 0.0, (what, i, errs["m"])
         for f, e in errs.items():
             if f != "dead_m":
-                assert e["norm"] <= 1e-12, (what, i, f, e)
+                assert e["norm"] <= NORM_TOL, (what, i, f, e)
 
 
 def test_plan_call_deposits_as_a_plain_call(gpu):
