@@ -248,7 +248,8 @@ __device__ __forceinline__ bool link_cut_shared(uint32_t* nbs, int base, int nv)
 __device__ __forceinline__ unsigned bfs_cut(int nv, uint32_t um, float cr, float sg, int ax, const PolyQueue& QI,
                                             unsigned long long eI, const uint32_t* nbI, uint32_t* nbL, uint32_t* nbU,
                                             const PolyQueue& QL, unsigned long long el, const PolyQueue& QU,
-                                            unsigned long long eu, bool keep_up, uint32_t cut_tag)
+                                            unsigned long long eu, bool keep_up, uint32_t cut_tag, int& cntL,
+                                            int& cntU)
 {
     auto X = [&](int v, int c) { return __ldg(&QI.x[qx(eI, v, c)]); };
     const uint32_t lmask = ((1u << nv) - 1u) & ~um;
@@ -314,16 +315,22 @@ __device__ __forceinline__ unsigned bfs_cut(int nv, uint32_t um, float cr, float
     if (!link_cut_shared(nbL, nl, nl + k) || (keep_up && !link_cut_shared(nbU, nu, nu + k))) return ST_GRAPH;
     for (int v = 0; v < nl + k; ++v) QL.nb[qn(el, v)] = AT(nbL, v);
     QL.nv[el] = (uint8_t)(nl + k);
+    cntL = nl + k;
     if (keep_up) {
         for (int v = 0; v < nu + k; ++v) QU.nb[qn(eu, v)] = AT(nbU, v);
         QU.nv[eu] = (uint8_t)(nu + k);
+        cntU = nu + k;
     }
     return 0;
 }
 
+// sector slots per queue of one warp's outputs (at most 64 children: 8 full sectors and 2 partial)
+constexpr int PAD_SLOTS = 12;
+
 __global__ void __launch_bounds__(BB, 7) k_bfs_level(BfsArgs a)
 {
     extern __shared__ uint32_t smem[];
+    __shared__ int smax[BB / 32][2 * PAD_SLOTS];
     uint32_t* nbI = smem;
     uint32_t* nbL = smem + MAXV * BB;
     uint32_t* nbU = smem + 2 * MAXV * BB;
@@ -408,6 +415,9 @@ __global__ void __launch_bounds__(BB, 7) k_bfs_level(BfsArgs a)
         unsigned oq, ol;
         const unsigned long long bq = warp_reserve(a.out.count, nq, oq);
         const unsigned long long bl = warp_reserve(a.leaf.count, nlf, ol);
+        // the children this lane writes: queue (0 out, 1 leaf), element, vertex count
+        int ncw = 0, cq[2] = {0, 0}, cn[2] = {0, 0};
+        unsigned long long ce[2] = {0ull, 0ull};
         if (toleaf) {
             const unsigned long long d = bl + ol;
             if (d >= a.leaf.cap) {
@@ -421,6 +431,9 @@ __global__ void __launch_bounds__(BB, 7) k_bfs_level(BfsArgs a)
                 moved += elem_bytes(nv);
                 put_box(a.leaf, d, lo, hi);
                 a.leaf.item[d] = t;
+                cq[ncw] = 1;
+                ce[ncw] = d;
+                cn[ncw++] = nv;
             }
         }
         if (cut) {
@@ -432,14 +445,22 @@ __global__ void __launch_bounds__(BB, 7) k_bfs_level(BfsArgs a)
             if (el >= QL.cap || eu >= QU.cap) {
                 st |= ST_OVERFLOW;
             } else {
-                const unsigned e2 =
-                    bfs_cut(nv, um, cr, 1.0f, ax, a.in, e, nbI, nbL, nbU, QL, el, QU, eu, true, axis_tag(ax));
+                int nL = 0, nU = 0;
+                const unsigned e2 = bfs_cut(nv, um, cr, 1.0f, ax, a.in, e, nbI, nbL, nbU, QL, el, QU, eu, true,
+                                            axis_tag(ax), nL, nU);
                 if (e2) {
                     st |= e2;
                     QL.nv[el] = 0; // downstream kernels skip these
                     QU.nv[eu] = 0;
                 } else {
-                    moved += elem_bytes(QL.nv[el]) + elem_bytes(QU.nv[eu]);
+                    moved += elem_bytes(nL) + elem_bytes(nU);
+                    cq[0] = leafL ? 1 : 0;
+                    ce[0] = el;
+                    cn[0] = nL;
+                    cq[1] = leafU ? 1 : 0;
+                    ce[1] = eu;
+                    cn[1] = nU;
+                    ncw = 2;
                 }
                 put_box(QL, el, llo, lhi);
                 put_box(QU, eu, ulo, uhi);
@@ -456,18 +477,54 @@ __global__ void __launch_bounds__(BB, 7) k_bfs_level(BfsArgs a)
             if (el >= QL.cap) {
                 st |= ST_OVERFLOW;
             } else {
-                const unsigned e2 =
-                    bfs_cut(nv, um, cr, sg, ax, a.in, e, nbI, nbL, nbU, QL, el, QL, el, false, axis_tag(ax));
+                int nL = 0, nU = 0;
+                const unsigned e2 = bfs_cut(nv, um, cr, sg, ax, a.in, e, nbI, nbL, nbU, QL, el, QL, el, false,
+                                            axis_tag(ax), nL, nU);
                 if (e2) {
                     st |= e2;
                     QL.nv[el] = 0;
                 } else {
-                    moved += elem_bytes(QL.nv[el]);
+                    moved += elem_bytes(nL);
+                    cq[0] = leafL ? 1 : 0;
+                    ce[0] = el;
+                    cn[0] = nL;
+                    ncw = 1;
                 }
                 put_box(QL, el, lo, hi);
                 QL.item[el] = t;
                 QL.win[el] = (uint8_t)win;
             }
+        }
+        if (a.pad_rows) {
+            // Complete the 32-byte sectors of the vertex rows this warp wrote: a sector holds one
+            // coordinate (or link) of 8 consecutive elements, and a child with fewer vertices than
+            // its neighbours leaves a hole that makes the sector be read back before it is
+            // written to DRAM.  Each element's rows are filled up to the largest vertex count in
+            // its sector, among the sectors of this warp's outputs.
+            const int wq = threadIdx.x >> 5;
+            const unsigned long long s0[2] = {bq >> 3, bl >> 3}; // first sector of each queue's outputs
+            if (lane < 2 * PAD_SLOTS) smax[wq][lane] = 0;
+            __syncwarp();
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+                if (i >= ncw) break;
+                const unsigned long long sl = (ce[i] >> 3) - (cq[i] ? s0[1] : s0[0]);
+                if (sl < PAD_SLOTS) atomicMax(&smax[wq][cq[i] * PAD_SLOTS + (int)sl], cn[i]);
+            }
+            __syncwarp();
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+                if (i >= ncw) break;
+                const unsigned long long sl = (ce[i] >> 3) - (cq[i] ? s0[1] : s0[0]);
+                if (sl >= PAD_SLOTS) continue;
+                const PolyQueue& Q = cq[i] ? a.leaf : a.out;
+                const int m = smax[wq][cq[i] * PAD_SLOTS + (int)sl];
+                for (int v = cn[i]; v < m; ++v) {
+                    for (int c = 0; c < 3; ++c) Q.x[qx(ce[i], v, c)] = 0.0f;
+                    Q.nb[qn(ce[i], v)] = 0u;
+                }
+            }
+            __syncwarp();
         }
     }
     if (st) atomicOr(a.c.status, st);
