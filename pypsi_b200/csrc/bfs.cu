@@ -324,13 +324,9 @@ __device__ __forceinline__ unsigned bfs_cut(int nv, uint32_t um, float cr, float
     return 0;
 }
 
-// sector slots per queue of one warp's outputs (at most 64 children: 8 full sectors and 2 partial)
-constexpr int PAD_SLOTS = 12;
-
 __global__ void __launch_bounds__(BB, 7) k_bfs_level(BfsArgs a)
 {
     extern __shared__ uint32_t smem[];
-    __shared__ int smax[BB / 32][2 * PAD_SLOTS];
     uint32_t* nbI = smem;
     uint32_t* nbL = smem + MAXV * BB;
     uint32_t* nbU = smem + 2 * MAXV * BB;
@@ -415,9 +411,6 @@ __global__ void __launch_bounds__(BB, 7) k_bfs_level(BfsArgs a)
         unsigned oq, ol;
         const unsigned long long bq = warp_reserve(a.out.count, nq, oq);
         const unsigned long long bl = warp_reserve(a.leaf.count, nlf, ol);
-        // the children this lane writes: queue (0 out, 1 leaf), element, vertex count
-        int ncw = 0, cq[2] = {0, 0}, cn[2] = {0, 0};
-        unsigned long long ce[2] = {0ull, 0ull};
         if (toleaf) {
             const unsigned long long d = bl + ol;
             if (d >= a.leaf.cap) {
@@ -431,9 +424,6 @@ __global__ void __launch_bounds__(BB, 7) k_bfs_level(BfsArgs a)
                 moved += elem_bytes(nv);
                 put_box(a.leaf, d, lo, hi);
                 a.leaf.item[d] = t;
-                cq[ncw] = 1;
-                ce[ncw] = d;
-                cn[ncw++] = nv;
             }
         }
         if (cut) {
@@ -454,13 +444,6 @@ __global__ void __launch_bounds__(BB, 7) k_bfs_level(BfsArgs a)
                     QU.nv[eu] = 0;
                 } else {
                     moved += elem_bytes(nL) + elem_bytes(nU);
-                    cq[0] = leafL ? 1 : 0;
-                    ce[0] = el;
-                    cn[0] = nL;
-                    cq[1] = leafU ? 1 : 0;
-                    ce[1] = eu;
-                    cn[1] = nU;
-                    ncw = 2;
                 }
                 put_box(QL, el, llo, lhi);
                 put_box(QU, eu, ulo, uhi);
@@ -485,46 +468,11 @@ __global__ void __launch_bounds__(BB, 7) k_bfs_level(BfsArgs a)
                     QL.nv[el] = 0;
                 } else {
                     moved += elem_bytes(nL);
-                    cq[0] = leafL ? 1 : 0;
-                    ce[0] = el;
-                    cn[0] = nL;
-                    ncw = 1;
                 }
                 put_box(QL, el, lo, hi);
                 QL.item[el] = t;
                 QL.win[el] = (uint8_t)win;
             }
-        }
-        if (a.pad_rows) {
-            // Complete the 32-byte sectors of the vertex rows this warp wrote: a sector holds one
-            // coordinate (or link) of 8 consecutive elements, and a child with fewer vertices than
-            // its neighbours leaves a hole that makes the sector be read back before it is
-            // written to DRAM.  Each element's rows are filled up to the largest vertex count in
-            // its sector, among the sectors of this warp's outputs.
-            const int wq = threadIdx.x >> 5;
-            const unsigned long long s0[2] = {bq >> 3, bl >> 3}; // first sector of each queue's outputs
-            if (lane < 2 * PAD_SLOTS) smax[wq][lane] = 0;
-            __syncwarp();
-#pragma unroll
-            for (int i = 0; i < 2; ++i) {
-                if (i >= ncw) break;
-                const unsigned long long sl = (ce[i] >> 3) - (cq[i] ? s0[1] : s0[0]);
-                if (sl < PAD_SLOTS) atomicMax(&smax[wq][cq[i] * PAD_SLOTS + (int)sl], cn[i]);
-            }
-            __syncwarp();
-#pragma unroll
-            for (int i = 0; i < 2; ++i) {
-                if (i >= ncw) break;
-                const unsigned long long sl = (ce[i] >> 3) - (cq[i] ? s0[1] : s0[0]);
-                if (sl >= PAD_SLOTS) continue;
-                const PolyQueue& Q = cq[i] ? a.leaf : a.out;
-                const int m = smax[wq][cq[i] * PAD_SLOTS + (int)sl];
-                for (int v = cn[i]; v < m; ++v) {
-                    for (int c = 0; c < 3; ++c) Q.x[qx(ce[i], v, c)] = 0.0f;
-                    Q.nb[qn(ce[i], v)] = 0u;
-                }
-            }
-            __syncwarp();
         }
     }
     if (st) atomicOr(a.c.status, st);
@@ -658,73 +606,87 @@ __global__ void __launch_bounds__(BB, INLINE ? 3 : 4) k_bfs_leaf(BfsArgs a)
     const ClipArgs& c = a.c;
     unsigned st = 0;
     unsigned long long frags = 0, verts = 0, moved = 0;
+    // The fragment's steps run as phases -- load and vertex solves, moments, sums -- with the
+    // warp brought back together between them (a.sync_phases): lanes whose fragments have fewer
+    // vertices or triangles would otherwise start the next phase alone and run it again, apart
+    // from the rest of the warp.
+    const bool sync = a.sync_phases != 0;
     for (unsigned long long base = (unsigned long long)warp * 32; base < n; base += (unsigned long long)nwarp * 32) {
         const unsigned long long e = base + lane;
         bool has = false;
         double rec[10];
         unsigned long long key = 0;
-        if (e < n) {
-            const int nv = a.leaf.nv[e];
-            if (nv >= 4 && nv <= MAXV) {
-                int lo[3], hi[3];
-                get_box(a.leaf, e, lo, hi);
-                const uint32_t t = a.leaf.item[e];
-                const GridDev& g = grid_of(c, t);
-                const unsigned long long vbase = c.voff ? c.voff[c.it.grid[t]] : 0ull;
-                const double* fr = c.it.frame + (size_t)t * FRAME;
-                double p0[3], DX[3][3], plo[3], phi[3], tol[3];
-                for (int i = 0; i < 3; ++i) p0[i] = fr[i];
-                for (int i = 0; i < 3; ++i)
-                    for (int j = 0; j < 3; ++j) DX[i][j] = fr[3 * (j + 1) + i] - p0[i];
-                for (int i = 0; i < 3; ++i) {
-                    plo[i] = g.d[i] * lo[i] + g.w0[i];
-                    phi[i] = g.d[i] * (lo[i] + 1) + g.w0[i];
-                    tol[i] = 1.0e-3 * g.d[i];
+        int nv = 0;
+        if (e < n) nv = a.leaf.nv[e];
+        const bool ok = e < n && nv >= 4 && nv <= MAXV;
+        int lo[3] = {0, 0, 0}, hi[3];
+        uint32_t t = 0;
+        long long gi = -1; // the fragment's voxel, -1 when out of range
+        const GridDev* gp = &c.g;
+        if (ok) {
+            get_box(a.leaf, e, lo, hi);
+            t = a.leaf.item[e];
+            gp = &grid_of(c, t);
+            const GridDev& g = *gp;
+            if (lo[0] < g.n[0] && lo[1] < g.n[1] && lo[2] < g.n[2])
+                gi = (long long)(c.voff ? c.voff[c.it.grid[t]] : 0ull) +
+                     ((long long)g.n[1] * lo[0] + lo[1]) * g.n[2] + lo[2];
+            const double* fr = c.it.frame + (size_t)t * FRAME;
+            double p0[3], DX[3][3], plo[3], phi[3], tol[3];
+            for (int i = 0; i < 3; ++i) p0[i] = fr[i];
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) DX[i][j] = fr[3 * (j + 1) + i] - p0[i];
+            for (int i = 0; i < 3; ++i) {
+                plo[i] = g.d[i] * lo[i] + g.w0[i];
+                phi[i] = g.d[i] * (lo[i] + 1) + g.w0[i];
+                tol[i] = 1.0e-3 * g.d[i];
+            }
+            for (int v = 0; v < nv; ++v) {
+                const uint32_t w = a.leaf.nb[qn(e, v)];
+                AT(nbs, v) = w;
+                if (QC < MAXV && v >= QC) continue; // solved where the walk meets it
+                const float x[3] = {a.leaf.x[qx(e, v, 0)], a.leaf.x[qx(e, v, 1)], a.leaf.x[qx(e, v, 2)]};
+                double q[3];
+                exact_q(x, w, p0, DX, p0, plo, phi, tol, q);
+                for (int i = 0; i < 3; ++i) AT(qs, 3 * v + i) = q[i];
+            }
+            moved += elem_bytes(nv) + 96; // the fragment and its image's vertices
+        }
+        if (sync) __syncwarp();
+        double o[3], mom[10];
+        unsigned e2 = 1;
+        if (ok) {
+            e2 = leaf_moments<QC>(nv, nbs, qs, c.mom_order, o, mom, a, e, t, lo);
+            st |= e2;
+        }
+        if (sync) __syncwarp();
+        if (ok && !e2 && mom[0] > 0.0) {
+            const GridDev& g = *gp;
+            if (gi < 0) {
+                st |= ST_INDEX;
+            } else {
+                key = ((unsigned long long)gi << c.rec_ibits) | (unsigned long long)(t - c.rec_item_base);
+                const double m0 = mom[0];
+                double u[3];
+                for (int i = 0; i < 3; ++i) u[i] = mom[1 + i] / m0;
+                rec[0] = m0;
+                for (int i = 0; i < 3; ++i) rec[1 + i] = o[i] + u[i];
+                rec[4] = mom[4] / m0 - u[0] * u[0];
+                rec[5] = mom[5] / m0 - u[0] * u[1];
+                rec[6] = mom[6] / m0 - u[0] * u[2];
+                rec[7] = mom[7] / m0 - u[1] * u[1];
+                rec[8] = mom[8] / m0 - u[1] * u[2];
+                rec[9] = mom[9] / m0 - u[2] * u[2];
+                ++frags;
+                verts += nv;
+                if constexpr (INLINE) {
+                    // atomic mode: straight into the voxel's sums, no record
+                    const double f = c.acc.factor ? c.acc.factor[t] : 1.0;
+                    accumulate_fragment(c, g, c.grids ? (int)c.it.grid[t] : 0, gi, lo, t, rec, f);
+                } else {
+                    has = true;
                 }
-                for (int v = 0; v < nv; ++v) {
-                    const uint32_t w = a.leaf.nb[qn(e, v)];
-                    AT(nbs, v) = w;
-                    if (QC < MAXV && v >= QC) continue; // solved where the walk meets it
-                    const float x[3] = {a.leaf.x[qx(e, v, 0)], a.leaf.x[qx(e, v, 1)], a.leaf.x[qx(e, v, 2)]};
-                    double q[3];
-                    exact_q(x, w, p0, DX, p0, plo, phi, tol, q);
-                    for (int i = 0; i < 3; ++i) AT(qs, 3 * v + i) = q[i];
-                }
-                moved += elem_bytes(nv) + 96; // the fragment and its image's vertices
-                double o[3], mom[10];
-                const unsigned e2 = leaf_moments<QC>(nv, nbs, qs, c.mom_order, o, mom, a, e, t, lo);
-                if (e2) {
-                    st |= e2;
-                } else if (mom[0] > 0.0) {
-                    if (lo[0] >= g.n[0] || lo[1] >= g.n[1] || lo[2] >= g.n[2]) {
-                        st |= ST_INDEX;
-                    } else {
-                        const long long gi =
-                            (long long)vbase + ((long long)g.n[1] * lo[0] + lo[1]) * g.n[2] + lo[2];
-                        key = ((unsigned long long)gi << c.rec_ibits) | (unsigned long long)(t - c.rec_item_base);
-                        const double m0 = mom[0];
-                        double u[3];
-                        for (int i = 0; i < 3; ++i) u[i] = mom[1 + i] / m0;
-                        rec[0] = m0;
-                        for (int i = 0; i < 3; ++i) rec[1 + i] = o[i] + u[i];
-                        rec[4] = mom[4] / m0 - u[0] * u[0];
-                        rec[5] = mom[5] / m0 - u[0] * u[1];
-                        rec[6] = mom[6] / m0 - u[0] * u[2];
-                        rec[7] = mom[7] / m0 - u[1] * u[1];
-                        rec[8] = mom[8] / m0 - u[1] * u[2];
-                        rec[9] = mom[9] / m0 - u[2] * u[2];
-                        ++frags;
-                        verts += nv;
-                        if constexpr (INLINE) {
-                            // atomic mode: straight into the voxel's sums, no record
-                            const double f = c.acc.factor ? c.acc.factor[t] : 1.0;
-                            accumulate_fragment(c, g, c.grids ? (int)c.it.grid[t] : 0, gi, lo, t, rec, f);
-                        } else {
-                            has = true;
-                        }
-                        if (!c.acc.factor) atomicAdd(&a.vsum[t], m0);
-                    }
-                }
+                if (!c.acc.factor) atomicAdd(&a.vsum[t], m0);
             }
         }
         unsigned off;

@@ -234,7 +234,7 @@ struct BfsArgs {
                               // depth-first kernel)
     int leaf_records;         // atomic sums (c.acc.sum): the leaf kernel writes records and a second
                               // kernel adds them (else the leaf kernel adds its fragments itself)
-    int pad_rows;             // level: fill the vertex-row sectors of a warp's children (see k_bfs_level)
+    int sync_phases;          // leaf: reconverge the warp between a fragment's phases (see k_bfs_leaf)
 };
 // each launches one resident wave of grid-stride blocks on num_sms SMs
 cudaError_t launch_bfs_init(const BfsArgs &a, int num_sms, cudaStream_t s);
