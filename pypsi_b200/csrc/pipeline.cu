@@ -544,6 +544,7 @@ int bfs_clip(Ctx& C, ClipArgs& ca, long long nmain, long long nitems, unsigned l
     ba.bytes = &sm[S_BYTES];
     ba.window_bfs = env_ll("PSIB_BFS_WINDOW", 1) != 0;
     ba.sync_phases = env_ll("PSIB_LEAF_SYNC", 0) != 0;
+    ba.leaf_pool = env_ll("PSIB_LEAF_POOL", 0) != 0;
     // Atomic sums: the leaf kernel writes a record per fragment and k_acc_records adds each leaf
     // launch's records right after it (a leaf launch has at most one record per leaf-queue entry);
     // the leaf kernel then needs fewer registers and less shared memory than one that adds its
