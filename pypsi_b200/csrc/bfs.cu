@@ -224,21 +224,31 @@ __global__ void __launch_bounds__(BB) k_bfs_init(BfsArgs a)
 // link_cut_vertices does for a polyhedron in memory).
 __device__ __forceinline__ bool link_cut_shared(uint32_t* nbs, int base, int nv)
 {
-    for (int vs = base; vs < nv; ++vs) {
+    // no return inside the loops: every lane leaves them at the same place, so the warp
+    // runs the code after them together
+    bool ok = true;
+    for (int vs = base; vs < nv && ok; ++vs) {
         int vc = vs, vn = nbget(AT(nbs, vs), 0);
         int steps = 0;
         do {
-            if (vn >= nv) return false;
+            if (vn >= nv) {
+                ok = false;
+                break;
+            }
             const uint32_t w = AT(nbs, vn);
             const int k = (nbget(w, 0) == vc) ? 0 : (nbget(w, 1) == vc) ? 1 : (nbget(w, 2) == vc) ? 2 : 3;
-            if (k == 3 || ++steps > WALK_CAP) return false;
+            if (k == 3 || ++steps > WALK_CAP) {
+                ok = false;
+                break;
+            }
             vc = vn;
             vn = nbget(AT(nbs, vc), (k + 1) % 3);
         } while (vc < base);
+        if (!ok) break;
         AT(nbs, vs) = nbset(AT(nbs, vs), 2, vc);
         AT(nbs, vc) = nbset(AT(nbs, vc), 1, vs);
     }
-    return true;
+    return ok;
 }
 
 // Cut the polyhedron at element eI of the input queue (positions read from
@@ -254,7 +264,10 @@ __device__ __forceinline__ unsigned bfs_cut(int nv, uint32_t um, float cr, float
     auto X = [&](int v, int c) { return __ldg(&QI.x[qx(eI, v, c)]); };
     const uint32_t lmask = ((1u << nv) - 1u) & ~um;
     const int nl = __popc(lmask), nu = __popc(um);
-    for (int v = 0; v < nv; ++v) {
+    // a failure ends the loops through err rather than a return, so that the lanes of a warp
+    // leave every loop at one place and run the next step together
+    unsigned err = 0;
+    for (int v = 0; v < nv && !err; ++v) {
         const bool u = (um >> v) & 1u;
         const uint32_t sm = u ? um : lmask;
         const int j = rank_in(sm, v);
@@ -266,7 +279,10 @@ __device__ __forceinline__ unsigned bfs_cut(int nv, uint32_t um, float cr, float
         uint32_t ow = 0xFFFFFFu | (w & ALL_TAGS);
         for (int k = 0; k < 3; ++k) {
             const int t = nbget(w, k);
-            if (t >= nv) return ST_GRAPH;
+            if (t >= nv) {
+                err = ST_GRAPH;
+                break;
+            }
             if ((((um >> t) & 1u) != 0) == u) ow = nbset(ow, k, rank_in(sm, t));
         }
         if (u) AT(nbU, j) = ow;
@@ -276,7 +292,7 @@ __device__ __forceinline__ unsigned bfs_cut(int nv, uint32_t um, float cr, float
     // bit first creates the cut vertices in cut_poly's order, and every lane
     // runs the loop body on every trip
     uint64_t cm = 0ull;
-    for (int vc = 0; vc < nv; ++vc) {
+    for (int vc = 0; vc < nv && !err; ++vc) {
         const uint32_t w = AT(nbI, vc);
         const bool low = !((um >> vc) & 1u);
 #pragma unroll
@@ -284,7 +300,7 @@ __device__ __forceinline__ unsigned bfs_cut(int nv, uint32_t um, float cr, float
             if (low && ((um >> nbget(w, np)) & 1u)) cm |= 1ull << (3 * vc + np);
     }
     int k = 0;
-    while (cm) {
+    while (cm && !err) {
         const int bit = __ffsll((long long)cm) - 1;
         cm &= cm - 1ull;
         const int vc = bit / 3, np = bit - 3 * vc;
@@ -292,7 +308,10 @@ __device__ __forceinline__ unsigned bfs_cut(int nv, uint32_t um, float cr, float
         const int jc = rank_in(lmask, vc);
         {
             const int vn = nbget(w, np);
-            if (nl + k >= MAXV || nu + k >= MAXV) return ST_OVERFLOW;
+            if (nl + k >= MAXV || nu + k >= MAXV) {
+                err = ST_OVERFLOW;
+                break;
+            }
             const float sc = sg * (cr - X(vc, ax)), sn = sg * (cr - X(vn, ax));
             const float iw = 1.0f / (sc - sn);
             for (int c = 0; c < 3; ++c) {
@@ -307,12 +326,17 @@ __device__ __forceinline__ unsigned bfs_cut(int nv, uint32_t um, float cr, float
             const int jn = rank_in(um, vn);
             AT(nbU, nu + k) = 0xFFFF00u | (uint32_t)jn | tg;
             const int kb = (nbget(wn, 0) == vc) ? 0 : (nbget(wn, 1) == vc) ? 1 : (nbget(wn, 2) == vc) ? 2 : 3;
-            if (kb == 3) return ST_GRAPH;
+            if (kb == 3) {
+                err = ST_GRAPH;
+                break;
+            }
             AT(nbU, jn) = nbset(AT(nbU, jn), kb, nu + k);
             ++k;
         }
     }
-    if (!link_cut_shared(nbL, nl, nl + k) || (keep_up && !link_cut_shared(nbU, nu, nu + k))) return ST_GRAPH;
+    if (!err && (!link_cut_shared(nbL, nl, nl + k) || (keep_up && !link_cut_shared(nbU, nu, nu + k))))
+        err = ST_GRAPH;
+    if (err) return err;
     for (int v = 0; v < nl + k; ++v) QL.nb[qn(el, v)] = AT(nbL, v);
     QL.nv[el] = (uint8_t)(nl + k);
     cntL = nl + k;
@@ -533,56 +557,69 @@ __device__ __forceinline__ unsigned leaf_moments(int nv, const uint32_t* nbs, co
     // directed edges not yet walked (3 * MAXV = 60 bits); the lowest first is
     // the face order of reduce_about
     uint64_t todo = (3 * nv >= 64) ? ~0ull : ((1ull << (3 * nv)) - 1ull);
-    while (todo) {
-        {
-            const int b0 = __ffsll((long long)todo) - 1;
-            todo &= todo - 1ull;
-            const int vs = b0 / 3, ks = b0 - 3 * vs;
-            int vc = vs;
-            int vn = nbget(AT(nbs, vc), ks);
-            if (vn >= nv) return ST_GRAPH;
-            const D3 Q0 = Q(vs);
-            const double q0x = Q0.x - o[0], q0y = Q0.y - o[1], q0z = Q0.z - o[2];
-            uint32_t w = AT(nbs, vn);
-            int k = (nbget(w, 0) == vc) ? 0 : (nbget(w, 1) == vc) ? 1 : (nbget(w, 2) == vc) ? 2 : 3;
-            if (k == 3) return ST_GRAPH;
+    // a broken graph ends the loops through err rather than a return (the lanes of a warp then
+    // leave each loop at one place)
+    unsigned err = 0;
+    while (todo && !err) {
+        const int b0 = __ffsll((long long)todo) - 1;
+        todo &= todo - 1ull;
+        const int vs = b0 / 3, ks = b0 - 3 * vs;
+        int vc = vs;
+        int vn = nbget(AT(nbs, vc), ks);
+        if (vn >= nv) {
+            err = ST_GRAPH;
+            break;
+        }
+        const D3 Q0 = Q(vs);
+        const double q0x = Q0.x - o[0], q0y = Q0.y - o[1], q0z = Q0.z - o[2];
+        uint32_t w = AT(nbs, vn);
+        int k = (nbget(w, 0) == vc) ? 0 : (nbget(w, 1) == vc) ? 1 : (nbget(w, 2) == vc) ? 2 : 3;
+        if (k == 3) {
+            err = ST_GRAPH;
+            break;
+        }
+        vc = vn;
+        int kn = (k + 1) % 3;
+        todo &= ~(1ull << (3 * vc + kn));
+        vn = nbget(AT(nbs, vc), kn);
+        int steps = 0;
+        while (vn != vs) {
+            if (++steps > WALK_CAP || vn >= nv) {
+                err = ST_GRAPH;
+                break;
+            }
+            const D3 Q1 = Q(vn), Q2 = Q(vc);
+            const double q1x = Q1.x - o[0], q1y = Q1.y - o[1], q1z = Q1.z - o[2];
+            const double q2x = Q2.x - o[0], q2y = Q2.y - o[1], q2z = Q2.z - o[2];
+            const double m = (-q2x * q1y * q0z + q1x * q2y * q0z + q2x * q0y * q1z
+                              - q0x * q2y * q1z - q1x * q0y * q2z + q0x * q1y * q2z);
+            mom[0] += m;
+            if (order > 0) {
+                mom[1] += 0.25 * m * (q0x + q1x + q2x);
+                mom[2] += 0.25 * m * (q0y + q1y + q2y);
+                mom[3] += 0.25 * m * (q0z + q1z + q2z);
+            }
+            if (order > 1) {
+                mom[4] += 0.1 * m * (q0x * q0x + q1x * q1x + q2x * q2x + q1x * q2x + q0x * (q1x + q2x));
+                mom[5] += 0.05 * m * (q2x * q0y + q2x * q1y + 2 * q2x * q2y + q0x * (2 * q0y + q1y + q2y) + q1x * (q0y + 2 * q1y + q2y));
+                mom[6] += 0.05 * m * (q2x * q0z + q2x * q1z + 2 * q2x * q2z + q0x * (2 * q0z + q1z + q2z) + q1x * (q0z + 2 * q1z + q2z));
+                mom[7] += 0.1 * m * (q0y * q0y + q1y * q1y + q2y * q2y + q1y * q2y + q0y * (q1y + q2y));
+                mom[8] += 0.05 * m * (q2y * q0z + q2y * q1z + 2 * q2y * q2z + q0y * (2 * q0z + q1z + q2z) + q1y * (q0z + 2 * q1z + q2z));
+                mom[9] += 0.1 * m * (q0z * q0z + q1z * q1z + q2z * q2z + q1z * q2z + q0z * (q1z + q2z));
+            }
+            w = AT(nbs, vn);
+            k = (nbget(w, 0) == vc) ? 0 : (nbget(w, 1) == vc) ? 1 : (nbget(w, 2) == vc) ? 2 : 3;
+            if (k == 3) {
+                err = ST_GRAPH;
+                break;
+            }
             vc = vn;
-            int kn = (k + 1) % 3;
+            kn = (k + 1) % 3;
             todo &= ~(1ull << (3 * vc + kn));
             vn = nbget(AT(nbs, vc), kn);
-            int steps = 0;
-            while (vn != vs) {
-                if (++steps > WALK_CAP || vn >= nv) return ST_GRAPH;
-                const D3 Q1 = Q(vn), Q2 = Q(vc);
-                const double q1x = Q1.x - o[0], q1y = Q1.y - o[1], q1z = Q1.z - o[2];
-                const double q2x = Q2.x - o[0], q2y = Q2.y - o[1], q2z = Q2.z - o[2];
-                const double m = (-q2x * q1y * q0z + q1x * q2y * q0z + q2x * q0y * q1z
-                                  - q0x * q2y * q1z - q1x * q0y * q2z + q0x * q1y * q2z);
-                mom[0] += m;
-                if (order > 0) {
-                    mom[1] += 0.25 * m * (q0x + q1x + q2x);
-                    mom[2] += 0.25 * m * (q0y + q1y + q2y);
-                    mom[3] += 0.25 * m * (q0z + q1z + q2z);
-                }
-                if (order > 1) {
-                    mom[4] += 0.1 * m * (q0x * q0x + q1x * q1x + q2x * q2x + q1x * q2x + q0x * (q1x + q2x));
-                    mom[5] += 0.05 * m * (q2x * q0y + q2x * q1y + 2 * q2x * q2y + q0x * (2 * q0y + q1y + q2y) + q1x * (q0y + 2 * q1y + q2y));
-                    mom[6] += 0.05 * m * (q2x * q0z + q2x * q1z + 2 * q2x * q2z + q0x * (2 * q0z + q1z + q2z) + q1x * (q0z + 2 * q1z + q2z));
-                    mom[7] += 0.1 * m * (q0y * q0y + q1y * q1y + q2y * q2y + q1y * q2y + q0y * (q1y + q2y));
-                    mom[8] += 0.05 * m * (q2y * q0z + q2y * q1z + 2 * q2y * q2z + q0y * (2 * q0z + q1z + q2z) + q1y * (q0z + 2 * q1z + q2z));
-                    mom[9] += 0.1 * m * (q0z * q0z + q1z * q1z + q2z * q2z + q1z * q2z + q0z * (q1z + q2z));
-                }
-                w = AT(nbs, vn);
-                k = (nbget(w, 0) == vc) ? 0 : (nbget(w, 1) == vc) ? 1 : (nbget(w, 2) == vc) ? 2 : 3;
-                if (k == 3) return ST_GRAPH;
-                vc = vn;
-                kn = (k + 1) % 3;
-                todo &= ~(1ull << (3 * vc + kn));
-                vn = nbget(AT(nbs, vc), kn);
-            }
         }
     }
-    return 0;
+    return err;
 }
 
 // q-cache sizes of the two leaf kernels: every vertex where the kernel adds its fragments itself
