@@ -623,12 +623,13 @@ __device__ __forceinline__ unsigned leaf_moments(int nv, const uint32_t* nbs, co
 }
 
 // q-cache sizes of the two leaf kernels: every vertex where the kernel adds its fragments itself
-// (168 registers, three blocks per SM), the first 14 where it writes records (four blocks per SM:
-// tet-voxel fragments have at most 16 vertices and 7.2 on average, so few walks reach past it)
+// (168 registers, three blocks per SM), the first 14 where it writes records (128 registers, four
+// blocks per SM: tet-voxel fragments have at most 16 vertices and 7.2 on average, so few walks
+// reach past it)
 constexpr int QC_REC = 14;
 
 // INLINE: atomic mode, each fragment added to its voxel's sums here; else a record per fragment
-// (sorted mode: sorted and applied after the walk; atomic mode: added by k_acc_records).
+// (sorted mode: sorted and applied after the walk).
 template <bool INLINE>
 __global__ void __launch_bounds__(BB, INLINE ? 3 : 4) k_bfs_leaf(BfsArgs a)
 {
@@ -643,11 +644,10 @@ __global__ void __launch_bounds__(BB, INLINE ? 3 : 4) k_bfs_leaf(BfsArgs a)
     const ClipArgs& c = a.c;
     unsigned st = 0;
     unsigned long long frags = 0, verts = 0, moved = 0;
-    // The fragment's steps run as phases -- load and vertex solves, moments, sums -- with the
-    // warp brought back together between them (a.sync_phases): lanes whose fragments have fewer
-    // vertices or triangles would otherwise start the next phase alone and run it again, apart
-    // from the rest of the warp.
-    const bool sync = a.sync_phases != 0;
+    // The fragment's steps run as separate blocks -- load and vertex solves, moments, sums --
+    // which every lane leaves at one place, so that lanes whose fragments have fewer vertices or
+    // triangles do not start the next step apart from the rest of the warp (run that way, the
+    // 28 atomics of a fragment took two passes per warp; measured 1.47x faster as blocks).
     for (unsigned long long base = (unsigned long long)warp * 32; base < n; base += (unsigned long long)nwarp * 32) {
         const unsigned long long e = base + lane;
         bool has = false;
@@ -689,14 +689,12 @@ __global__ void __launch_bounds__(BB, INLINE ? 3 : 4) k_bfs_leaf(BfsArgs a)
             }
             moved += elem_bytes(nv) + 96; // the fragment and its image's vertices
         }
-        if (sync) __syncwarp();
         double o[3], mom[10];
         unsigned e2 = 1;
         if (ok) {
             e2 = leaf_moments<QC>(nv, nbs, qs, c.mom_order, o, mom, a, e, t, lo);
             st |= e2;
         }
-        if (sync) __syncwarp();
         if (ok && !e2 && mom[0] > 0.0) {
             const GridDev& g = *gp;
             if (gi < 0) {
@@ -750,264 +748,6 @@ __global__ void __launch_bounds__(BB, INLINE ? 3 : 4) k_bfs_leaf(BfsArgs a)
     if (a.bytes && moved) atomicAdd(a.bytes, moved);
 }
 
-// ---- leaf, pooled: the fan triangles of a warp's 32 fragments shared out over its lanes ----
-//
-// One fragment per lane leaves most lanes idle while the lane with the most triangles finishes
-// (10-11 of 32 lanes active on the 128^3 -> 256^3 workload).  Here each lane solves its
-// fragment's vertices and lists its fan triangles (integer work on the links), then the warp
-// takes the list as one pool: lane j computes the moments of a contiguous run of about
-// T/32 triangles, adding runs that end at a fragment's boundary into that fragment's sums in
-// shared memory, and each lane then adds its own fragment to the voxel sums.  Same moments,
-// summed in another order.
-
-constexpr int LB = 64;                // threads per block of the pooled leaf kernel
-constexpr int TRI_CAP = 2 * MAXV - 4; // fan triangles of a simple polyhedron of MAXV vertices
-static_assert(10 * sizeof(double) <= MAXV * sizeof(uint32_t), "the per-fragment sums reuse the links' bytes");
-// per-warp arrays laid out [row][lane]: this lane's entry, and lane o's
-#define ATL(arr, v) (arr)[(v) * 32 + (threadIdx.x & 31)]
-#define ATO(arr, v, o) (arr)[(v) * 32 + (o)]
-
-// The fan triangles of the fragment whose links are in this lane's column, in the order of
-// leaf_moments, as vs | vn << 5 | vc << 10 (moments of q[vs], q[vn], q[vc]); -1 on a broken graph.
-__device__ __forceinline__ int leaf_triangles(int nv, const uint32_t* nbs, uint16_t* tl)
-{
-    uint64_t todo = (3 * nv >= 64) ? ~0ull : ((1ull << (3 * nv)) - 1ull);
-    int n = 0;
-    while (todo) {
-        const int b0 = __ffsll((long long)todo) - 1;
-        todo &= todo - 1ull;
-        const int vs = b0 / 3;
-        int vc = vs;
-        int vn = nbget(ATL(nbs, vc), b0 - 3 * vs);
-        if (vn >= nv) return -1;
-        uint32_t w = ATL(nbs, vn);
-        int k = (nbget(w, 0) == vc) ? 0 : (nbget(w, 1) == vc) ? 1 : (nbget(w, 2) == vc) ? 2 : 3;
-        if (k == 3) return -1;
-        vc = vn;
-        int kn = (k + 1) % 3;
-        todo &= ~(1ull << (3 * vc + kn));
-        vn = nbget(ATL(nbs, vc), kn);
-        int steps = 0;
-        while (vn != vs) {
-            if (++steps > WALK_CAP || vn >= nv || n >= TRI_CAP) return -1;
-            tl[n++] = (uint16_t)(vs | (vn << 5) | (vc << 10));
-            w = ATL(nbs, vn);
-            k = (nbget(w, 0) == vc) ? 0 : (nbget(w, 1) == vc) ? 1 : (nbget(w, 2) == vc) ? 2 : 3;
-            if (k == 3) return -1;
-            vc = vn;
-            kn = (k + 1) % 3;
-            todo &= ~(1ull << (3 * vc + kn));
-            vn = nbget(ATL(nbs, vc), kn);
-        }
-    }
-    return n;
-}
-
-__global__ void __launch_bounds__(LB, 5) k_bfs_leaf_pool(BfsArgs a)
-{
-    extern __shared__ uint32_t smem[];
-    // this warp's arrays: links [MAXV][32], whose bytes then take the moment sums [10][32];
-    // FP64 q [3 MAXV][32]; triangle lists [32][TRI_CAP]; triangle counts [32]
-    const int wib = threadIdx.x >> 5;
-    uint32_t* nbs = smem + wib * (MAXV * 32);
-    double* msum = (double*)nbs;
-    double* qs = (double*)(smem + (LB / 32) * MAXV * 32) + wib * (3 * MAXV * 32);
-    uint16_t* tri = (uint16_t*)((double*)(smem + (LB / 32) * MAXV * 32) + (LB / 32) * 3 * MAXV * 32) +
-                    wib * (32 * TRI_CAP);
-    int* tcnt = (int*)((uint16_t*)((double*)(smem + (LB / 32) * MAXV * 32) + (LB / 32) * 3 * MAXV * 32) +
-                       LB * TRI_CAP) + wib * 32;
-    const int lane = threadIdx.x & 31;
-    const long long warp = (long long)blockIdx.x * (LB / 32) + (threadIdx.x >> 5);
-    const long long nwarp = (long long)gridDim.x * (LB / 32);
-    const unsigned long long n = min(*a.leaf.count, a.leaf.cap);
-    const ClipArgs& c = a.c;
-    const int order = c.mom_order;
-    unsigned st = 0;
-    unsigned long long frags = 0, verts = 0, moved = 0;
-    for (unsigned long long base = (unsigned long long)warp * 32; base < n; base += (unsigned long long)nwarp * 32) {
-        const unsigned long long e = base + lane;
-        int nv = 0;
-        if (e < n) nv = a.leaf.nv[e];
-        bool ok = e < n && nv >= 4 && nv <= MAXV;
-        int lo[3] = {0, 0, 0}, hi[3];
-        uint32_t t = 0;
-        long long gi = -1;
-        const GridDev* gp = &c.g;
-        if (ok) {
-            get_box(a.leaf, e, lo, hi);
-            t = a.leaf.item[e];
-            gp = &grid_of(c, t);
-            const GridDev& g = *gp;
-            if (lo[0] < g.n[0] && lo[1] < g.n[1] && lo[2] < g.n[2])
-                gi = (long long)(c.voff ? c.voff[c.it.grid[t]] : 0ull) +
-                     ((long long)g.n[1] * lo[0] + lo[1]) * g.n[2] + lo[2];
-            const double* fr = c.it.frame + (size_t)t * FRAME;
-            double p0[3], DX[3][3], plo[3], phi[3], tol[3];
-            for (int i = 0; i < 3; ++i) p0[i] = fr[i];
-            for (int i = 0; i < 3; ++i)
-                for (int j = 0; j < 3; ++j) DX[i][j] = fr[3 * (j + 1) + i] - p0[i];
-            for (int i = 0; i < 3; ++i) {
-                plo[i] = g.d[i] * lo[i] + g.w0[i];
-                phi[i] = g.d[i] * (lo[i] + 1) + g.w0[i];
-                tol[i] = 1.0e-3 * g.d[i];
-            }
-            for (int v = 0; v < nv; ++v) {
-                const uint32_t w = a.leaf.nb[qn(e, v)];
-                ATL(nbs, v) = w;
-                const float x[3] = {a.leaf.x[qx(e, v, 0)], a.leaf.x[qx(e, v, 1)], a.leaf.x[qx(e, v, 2)]};
-                double q[3];
-                exact_q(x, w, p0, DX, p0, plo, phi, tol, q);
-                for (int i = 0; i < 3; ++i) ATL(qs, 3 * v + i) = q[i];
-            }
-            moved += elem_bytes(nv) + 96; // the fragment and its image's vertices
-        }
-        // this lane's triangles
-        int nt = 0;
-        if (ok) {
-            nt = leaf_triangles(nv, nbs, tri + lane * TRI_CAP);
-            if (nt < 0) {
-                st |= ST_GRAPH;
-                ok = false;
-                nt = 0;
-            }
-        }
-        tcnt[lane] = nt;
-        __syncwarp();
-        // the links are no longer read: their bytes take the sums
-        for (int i = 0; i < 10; ++i) ATL(msum, i) = 0.0;
-        // the pool: exclusive prefix of the triangle counts, T in all, runs of ceil(T / 32)
-        int pre = nt;
-        for (int d = 1; d < 32; d <<= 1) {
-            const int y = __shfl_up_sync(FULL, pre, d);
-            if (lane >= d) pre += y;
-        }
-        const int T = __shfl_sync(FULL, pre, 31);
-        pre -= nt;
-        const int run = (T + 31) >> 5;
-        const int s0 = min(lane * run, T), s1 = min(s0 + run, T);
-        // the fragment holding triangle s0: the last lane whose prefix is <= s0
-        int o = 0;
-        for (int step = 16; step; step >>= 1) {
-            const int cand = o + step;
-            const int pc = __shfl_sync(FULL, pre, cand & 31);
-            if (cand < 32 && pc <= s0) o = cand;
-        }
-        int k = s0 - __shfl_sync(FULL, pre, o);
-        __syncwarp();
-        double r[10];
-        for (int i = 0; i < 10; ++i) r[i] = 0.0;
-        bool any = false;
-        for (int g2 = s0; g2 < s1; ++g2) {
-            while (o < 31 && k >= tcnt[o]) { // the run crosses into the next fragment
-                if (any) {
-                    for (int i = 0; i < 10; ++i) {
-                        atomicAdd(&ATO(msum, i, o), r[i]);
-                        r[i] = 0.0;
-                    }
-                    any = false;
-                }
-                k -= tcnt[o];
-                ++o;
-            }
-            if (k >= tcnt[o]) break; // cannot happen: the runs cover the T triangles exactly
-            const int ow = o;
-            const unsigned en = tri[ow * TRI_CAP + k];
-            const int vs = en & 31, vn = (en >> 5) & 31, vc = (en >> 10) & 31;
-            const double ox = ATO(qs, 0, ow), oy = ATO(qs, 1, ow), oz = ATO(qs, 2, ow);
-            const double q0x = ATO(qs, 3 * vs, ow) - ox, q0y = ATO(qs, 3 * vs + 1, ow) - oy,
-                         q0z = ATO(qs, 3 * vs + 2, ow) - oz;
-            const double q1x = ATO(qs, 3 * vn, ow) - ox, q1y = ATO(qs, 3 * vn + 1, ow) - oy,
-                         q1z = ATO(qs, 3 * vn + 2, ow) - oz;
-            const double q2x = ATO(qs, 3 * vc, ow) - ox, q2y = ATO(qs, 3 * vc + 1, ow) - oy,
-                         q2z = ATO(qs, 3 * vc + 2, ow) - oz;
-            const double m = (-q2x * q1y * q0z + q1x * q2y * q0z + q2x * q0y * q1z
-                              - q0x * q2y * q1z - q1x * q0y * q2z + q0x * q1y * q2z);
-            r[0] += m;
-            if (order > 0) {
-                r[1] += 0.25 * m * (q0x + q1x + q2x);
-                r[2] += 0.25 * m * (q0y + q1y + q2y);
-                r[3] += 0.25 * m * (q0z + q1z + q2z);
-            }
-            if (order > 1) {
-                r[4] += 0.1 * m * (q0x * q0x + q1x * q1x + q2x * q2x + q1x * q2x + q0x * (q1x + q2x));
-                r[5] += 0.05 * m * (q2x * q0y + q2x * q1y + 2 * q2x * q2y + q0x * (2 * q0y + q1y + q2y) + q1x * (q0y + 2 * q1y + q2y));
-                r[6] += 0.05 * m * (q2x * q0z + q2x * q1z + 2 * q2x * q2z + q0x * (2 * q0z + q1z + q2z) + q1x * (q0z + 2 * q1z + q2z));
-                r[7] += 0.1 * m * (q0y * q0y + q1y * q1y + q2y * q2y + q1y * q2y + q0y * (q1y + q2y));
-                r[8] += 0.05 * m * (q2y * q0z + q2y * q1z + 2 * q2y * q2z + q0y * (2 * q0z + q1z + q2z) + q1y * (q0z + 2 * q1z + q2z));
-                r[9] += 0.1 * m * (q0z * q0z + q1z * q1z + q2z * q2z + q1z * q2z + q0z * (q1z + q2z));
-            }
-            any = true;
-            ++k;
-        }
-        if (any)
-            for (int i = 0; i < 10; ++i) atomicAdd(&ATO(msum, i, o), r[i]);
-        __syncwarp();
-        if (ok) {
-            double mom[10], oq[3];
-            for (int i = 0; i < 10; ++i) mom[i] = ATL(msum, i);
-            for (int i = 0; i < 3; ++i) oq[i] = ATL(qs, i);
-            if (mom[0] > 0.0) {
-                if (gi < 0) {
-                    st |= ST_INDEX;
-                } else {
-                    const double m0 = mom[0];
-                    double u[3], rec[10];
-                    for (int i = 0; i < 3; ++i) u[i] = mom[1 + i] / m0;
-                    rec[0] = m0;
-                    for (int i = 0; i < 3; ++i) rec[1 + i] = oq[i] + u[i];
-                    rec[4] = mom[4] / m0 - u[0] * u[0];
-                    rec[5] = mom[5] / m0 - u[0] * u[1];
-                    rec[6] = mom[6] / m0 - u[0] * u[2];
-                    rec[7] = mom[7] / m0 - u[1] * u[1];
-                    rec[8] = mom[8] / m0 - u[1] * u[2];
-                    rec[9] = mom[9] / m0 - u[2] * u[2];
-                    ++frags;
-                    verts += nv;
-                    const double f = c.acc.factor ? c.acc.factor[t] : 1.0;
-                    accumulate_fragment(c, *gp, c.grids ? (int)c.it.grid[t] : 0, gi, lo, t, rec, f);
-                    if (!c.acc.factor) atomicAdd(&a.vsum[t], m0);
-                }
-            }
-        }
-        __syncwarp(); // the next fragments overwrite the links, sums and q
-    }
-    if (st) atomicOr(c.status, st);
-    if (c.counters && frags) {
-        atomicAdd(&c.counters[0], frags);
-        atomicAdd(&c.counters[1], verts);
-    }
-    if (a.bytes && moved) atomicAdd(a.bytes, moved);
-}
-#undef ATL
-#undef ATO
-
-// Atomic mode through records: every record of the leaf launch before it added to its
-// voxel's sums (the key gives the voxel and the image), as the inline leaf kernel adds its
-// fragments.  Consecutive records come from consecutive leaf-queue entries, so a warp's
-// atomics stay near one another in the grid.
-__global__ void __launch_bounds__(128) k_acc_records(BfsArgs a)
-{
-    const ClipArgs& c = a.c;
-    const unsigned long long n = min(*c.rec_n, c.rec_cap);
-    const unsigned long long imask = (1ull << c.rec_ibits) - 1ull;
-    for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n;
-         i += (unsigned long long)gridDim.x * blockDim.x) {
-        const unsigned long long key = c.rec_key[i];
-        const long long t = (long long)(key & imask) + c.rec_item_base;
-        const long long gi = (long long)(key >> c.rec_ibits);
-        const GridDev& g = grid_of(c, t);
-        const long long local = gi - (long long)(c.voff ? c.voff[c.it.grid[t]] : 0ull);
-        const int lo[3] = {(int)(local / ((long long)g.n[1] * g.n[2])), (int)((local / g.n[2]) % g.n[1]),
-                           (int)(local % g.n[2])};
-        double rec[10];
-        const double* src = c.rec_mom + i * c.rec_nmom;
-#pragma unroll
-        for (int k = 0; k < 10; ++k) rec[k] = k < c.rec_nmom ? src[k] : 0.0;
-        const double f = c.acc.factor ? c.acc.factor[t] : 1.0;
-        accumulate_fragment(c, g, c.grids ? (int)c.it.grid[t] : 0, gi, lo, t, rec, f);
-    }
-}
-
 // FP32 walks can misplace a vertex that falls back to its FP32 position by
 // ~1e-7 of the tet: each breadth-first image's fragment masses are scaled by
 // target / (sum of its fragment q-volumes), so that it deposits exactly its
@@ -1042,11 +782,9 @@ static constexpr size_t LEVEL_SMEM = 3 * MAXV * BB * sizeof(uint32_t); // links 
 // links of every vertex, FP64 q of the cached ones
 static constexpr size_t LEAF_SMEM = MAXV * BB * sizeof(uint32_t) + 3 * MAXV * BB * sizeof(double);
 static constexpr size_t LEAF_REC_SMEM = MAXV * BB * sizeof(uint32_t) + 3 * QC_REC * BB * sizeof(double);
-static constexpr size_t LEAF_POOL_SMEM = MAXV * LB * sizeof(uint32_t) + 3 * MAXV * LB * sizeof(double) +
-                                         LB * TRI_CAP * sizeof(uint16_t) + LB * sizeof(int);
 
 // resident blocks per SM of each kernel (one full wave of grid-stride blocks)
-static int g_blocks[6] = {0, 0, 0, 0, 0, 0};
+static int g_blocks[4] = {0, 0, 0, 0};
 static void occupancy();
 void bfs_prepare() { occupancy(); }
 static void occupancy()
@@ -1055,19 +793,15 @@ static void occupancy()
     cudaFuncSetAttribute(k_bfs_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LEVEL_SMEM);
     cudaFuncSetAttribute(k_bfs_leaf<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LEAF_SMEM);
     cudaFuncSetAttribute(k_bfs_leaf<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LEAF_REC_SMEM);
-    int b[6] = {1, 1, 1, 1, 1, 1};
+    int b[4] = {1, 1, 1, 1};
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b[0], k_bfs_init, BB, 0) != cudaSuccess) b[0] = 1;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b[1], k_bfs_level, BB, LEVEL_SMEM) != cudaSuccess) b[1] = 1;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b[2], k_bfs_leaf<true>, BB, LEAF_SMEM) != cudaSuccess)
         b[2] = 1;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b[3], k_bfs_leaf<false>, BB, LEAF_REC_SMEM) != cudaSuccess)
         b[3] = 1;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b[4], k_acc_records, 128, 0) != cudaSuccess) b[4] = 1;
-    cudaFuncSetAttribute(k_bfs_leaf_pool, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LEAF_POOL_SMEM);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b[5], k_bfs_leaf_pool, LB, LEAF_POOL_SMEM) != cudaSuccess)
-        b[5] = 1;
     cudaGetLastError();
-    for (int i = 0; i < 6; ++i) g_blocks[i] = b[i] > 0 ? b[i] : 1;
+    for (int i = 0; i < 4; ++i) g_blocks[i] = b[i] > 0 ? b[i] : 1;
 }
 
 cudaError_t launch_bfs_init(const BfsArgs& a, int num_sms, cudaStream_t s)
@@ -1087,21 +821,9 @@ cudaError_t launch_bfs_level(const BfsArgs& a, int num_sms, cudaStream_t s)
 cudaError_t launch_bfs_leaf(const BfsArgs& a, int num_sms, cudaStream_t s)
 {
     occupancy();
-    if (a.c.acc.sum && !a.leaf_records && a.leaf_pool) {
-        k_bfs_leaf_pool<<<num_sms * g_blocks[5], LB, LEAF_POOL_SMEM, s>>>(a);
-        return cudaGetLastError();
-    }
-    if (a.c.acc.sum && !a.leaf_records) {
-        k_bfs_leaf<true><<<num_sms * g_blocks[2], BB, LEAF_SMEM, s>>>(a);
-        return cudaGetLastError();
-    }
-    k_bfs_leaf<false><<<num_sms * g_blocks[3], BB, LEAF_REC_SMEM, s>>>(a);
-    if (!a.c.acc.sum) return cudaGetLastError(); // sorted mode: the records wait for the sort
-    k_acc_records<<<num_sms * g_blocks[4], 128, 0, s>>>(a);
-    cudaError_t e = cudaGetLastError();
-    // the next leaf launch writes its records from the start of the buffer
-    if (e == cudaSuccess) e = cudaMemsetAsync(a.c.rec_n, 0, sizeof(unsigned long long), s);
-    return e;
+    if (a.c.acc.sum) k_bfs_leaf<true><<<num_sms * g_blocks[2], BB, LEAF_SMEM, s>>>(a);
+    else k_bfs_leaf<false><<<num_sms * g_blocks[3], BB, LEAF_REC_SMEM, s>>>(a);
+    return cudaGetLastError();
 }
 
 } // namespace psib

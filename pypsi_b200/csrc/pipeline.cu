@@ -543,22 +543,6 @@ int bfs_clip(Ctx& C, ClipArgs& ca, long long nmain, long long nitems, unsigned l
     ba.dfs_count = &sm[S_DFS];
     ba.bytes = &sm[S_BYTES];
     ba.window_bfs = env_ll("PSIB_BFS_WINDOW", 1) != 0;
-    ba.sync_phases = env_ll("PSIB_LEAF_SYNC", 0) != 0;
-    ba.leaf_pool = env_ll("PSIB_LEAF_POOL", 0) != 0;
-    // Atomic sums: the leaf kernel writes a record per fragment and k_acc_records adds each leaf
-    // launch's records right after it (a leaf launch has at most one record per leaf-queue entry);
-    // the leaf kernel then needs fewer registers and less shared memory than one that adds its
-    // fragments itself (PSIB_LEAF_RECORDS=1; measured no faster, so off by default).
-    if (ca.acc.sum && ca.rec_ibits > 0 && env_ll("PSIB_LEAF_RECORDS", 0) != 0) {
-        const size_t nrec = tiles * 32;
-        RET(ensure(C.rkey, nrec * sizeof(unsigned long long)));
-        RET(ensure(C.rmom, nrec * ca.rec_nmom * sizeof(double)));
-        ba.c.rec_key = C.rkey.as<unsigned long long>();
-        ba.c.rec_mom = C.rmom.as<double>();
-        ba.c.rec_cap = nrec;
-        CK(cudaMemsetAsync(ba.c.rec_n, 0, sizeof(unsigned long long), st));
-        ba.leaf_records = 1;
-    }
     RET(ensure(C.vsum, (size_t)std::max<long long>(nitems, 1) * sizeof(double)));
     ba.vsum = C.vsum.as<double>();
     // the pass table on the device; a device counter picks the pass, so every pass runs
@@ -612,7 +596,7 @@ int bfs_clip(Ctx& C, ClipArgs& ca, long long nmain, long long nitems, unsigned l
     }
     if (!graphed)
         for (long long p = 0; p < npass; ++p) CK(pass(st));
-    klaunch += (3 + 2 * NLEV + (ba.leaf_records ? NLEV + 1 : 0)) * npass;
+    klaunch += (3 + 2 * NLEV) * npass;
     launches += (2 + 2 * NLEV) * npass;
     if (sizes) {
         sizes->tiles = (long long)tiles;
@@ -1089,14 +1073,6 @@ int run_device(Call& c)
         }
         if (atomic) {
             // ---- clip, each fragment added to its voxel's sums ----
-            {
-                // a record key (voxel | image) for the walk's leaf records, when both fit in 64 bits
-                int ib = 1, vb = 1;
-                while ((1ll << ib) < nitems) ++ib;
-                while ((1ll << vb) < nvox) ++vb;
-                ca.rec_ibits = ib + vb <= 64 ? ib : 0;
-                ca.rec_item_base = 0;
-            }
             CK(cudaMemsetAsync(&sm[S_BYTES], 0, 8, st));
             CK(cudaMemsetAsync(&sm[S_CNT], 0, 24, st));
             CK(cudaMemsetAsync(&sm[S_HEAD], 0, 16, st));

@@ -232,10 +232,6 @@ struct BfsArgs {
     unsigned long long *bytes; // algorithmic bytes the walk reads and writes (polyhedra, frames, records)
     int window_bfs;           // init: window-clipped images are walked here too (else listed for the
                               // depth-first kernel)
-    int leaf_records;         // atomic sums (c.acc.sum): the leaf kernel writes records and a second
-                              // kernel adds them (else the leaf kernel adds its fragments itself)
-    int sync_phases;          // leaf: reconverge the warp between a fragment's phases (see k_bfs_leaf)
-    int leaf_pool;            // atomic sums: the leaf kernel that pools a warp's fan triangles
 };
 // each launches one resident wave of grid-stride blocks on num_sms SMs
 cudaError_t launch_bfs_init(const BfsArgs &a, int num_sms, cudaStream_t s);
