@@ -450,52 +450,35 @@ __global__ void __launch_bounds__(BB, 7) k_bfs_level(BfsArgs a)
                 a.leaf.item[d] = t;
             }
         }
-        if (cut) {
+        if (cut || wcut) {
+            // a middle-plane cut keeps both children, a window cut only the side with s >= 0; one
+            // call site for both, so that lanes doing either run the cut together
             unsigned qi = 0, li = 0;
             const PolyQueue& QL = leafL ? a.leaf : a.out;
             const unsigned long long el = leafL ? bl + ol + li++ : bq + oq + qi++;
-            const PolyQueue& QU = leafU ? a.leaf : a.out;
-            const unsigned long long eu = leafU ? bl + ol + li++ : bq + oq + qi++;
+            const PolyQueue& QU = !cut ? QL : leafU ? a.leaf : a.out;
+            const unsigned long long eu = !cut ? el : leafU ? bl + ol + li++ : bq + oq + qi++;
             if (el >= QL.cap || eu >= QU.cap) {
                 st |= ST_OVERFLOW;
             } else {
                 int nL = 0, nU = 0;
-                const unsigned e2 = bfs_cut(nv, um, cr, 1.0f, ax, a.in, e, nbI, nbL, nbU, QL, el, QU, eu, true,
-                                            axis_tag(ax), nL, nU);
+                const unsigned e2 = bfs_cut(nv, um, cr, cut ? 1.0f : sg, ax, a.in, e, nbI, nbL, nbU, QL, el, QU, eu,
+                                            cut, axis_tag(ax), nL, nU);
                 if (e2) {
                     st |= e2;
                     QL.nv[el] = 0; // downstream kernels skip these
-                    QU.nv[eu] = 0;
+                    if (cut) QU.nv[eu] = 0;
                 } else {
-                    moved += elem_bytes(nL) + elem_bytes(nU);
+                    moved += elem_bytes(nL) + (cut ? elem_bytes(nU) : 0ull);
                 }
-                put_box(QL, el, llo, lhi);
-                put_box(QU, eu, ulo, uhi);
+                put_box(QL, el, cut ? llo : lo, cut ? lhi : hi);
                 QL.item[el] = t;
-                QU.item[eu] = t;
-                QL.win[el] = 0;
-                QU.win[eu] = 0;
-            }
-        }
-        if (wcut) {
-            // the window cut keeps one child: the side with s >= 0
-            const PolyQueue& QL = leafL ? a.leaf : a.out;
-            const unsigned long long el = leafL ? bl + ol : bq + oq;
-            if (el >= QL.cap) {
-                st |= ST_OVERFLOW;
-            } else {
-                int nL = 0, nU = 0;
-                const unsigned e2 = bfs_cut(nv, um, cr, sg, ax, a.in, e, nbI, nbL, nbU, QL, el, QL, el, false,
-                                            axis_tag(ax), nL, nU);
-                if (e2) {
-                    st |= e2;
-                    QL.nv[el] = 0;
-                } else {
-                    moved += elem_bytes(nL);
+                QL.win[el] = cut ? (uint8_t)0 : (uint8_t)win;
+                if (cut) {
+                    put_box(QU, eu, ulo, uhi);
+                    QU.item[eu] = t;
+                    QU.win[eu] = 0;
                 }
-                put_box(QL, el, lo, hi);
-                QL.item[el] = t;
-                QL.win[el] = (uint8_t)win;
             }
         }
     }
