@@ -242,7 +242,7 @@ __device__ __forceinline__ bool link_cut_shared(uint32_t* nbs, int base, int nv)
                 break;
             }
             vc = vn;
-            vn = nbget(AT(nbs, vc), (k + 1) % 3);
+            vn = nbget(AT(nbs, vc), k == 2 ? 0 : k + 1);
         } while (vc < base);
         if (!ok) break;
         AT(nbs, vs) = nbset(AT(nbs, vs), 2, vc);
@@ -562,7 +562,7 @@ __device__ __forceinline__ unsigned leaf_moments(int nv, const uint32_t* nbs, co
             break;
         }
         vc = vn;
-        int kn = (k + 1) % 3;
+        int kn = k == 2 ? 0 : k + 1;
         todo &= ~(1ull << (3 * vc + kn));
         vn = nbget(AT(nbs, vc), kn);
         int steps = 0;
@@ -577,18 +577,24 @@ __device__ __forceinline__ unsigned leaf_moments(int nv, const uint32_t* nbs, co
             const double m = (-q2x * q1y * q0z + q1x * q2y * q0z + q2x * q0y * q1z
                               - q0x * q2y * q1z - q1x * q0y * q2z + q0x * q1y * q2z);
             mom[0] += m;
+            // the tet (o, q0, q1, q2): first moments m s / 4 and second moments
+            // m (sum_i q_i q_i^T + s s^T) / 20 with s = q0 + q1 + q2 -- the terms of
+            // reduce_about, grouped so that each takes four multiply-adds
+            const double sx = q0x + q1x + q2x, sy = q0y + q1y + q2y, sz = q0z + q1z + q2z;
             if (order > 0) {
-                mom[1] += 0.25 * m * (q0x + q1x + q2x);
-                mom[2] += 0.25 * m * (q0y + q1y + q2y);
-                mom[3] += 0.25 * m * (q0z + q1z + q2z);
+                const double h = 0.25 * m;
+                mom[1] += h * sx;
+                mom[2] += h * sy;
+                mom[3] += h * sz;
             }
             if (order > 1) {
-                mom[4] += 0.1 * m * (q0x * q0x + q1x * q1x + q2x * q2x + q1x * q2x + q0x * (q1x + q2x));
-                mom[5] += 0.05 * m * (q2x * q0y + q2x * q1y + 2 * q2x * q2y + q0x * (2 * q0y + q1y + q2y) + q1x * (q0y + 2 * q1y + q2y));
-                mom[6] += 0.05 * m * (q2x * q0z + q2x * q1z + 2 * q2x * q2z + q0x * (2 * q0z + q1z + q2z) + q1x * (q0z + 2 * q1z + q2z));
-                mom[7] += 0.1 * m * (q0y * q0y + q1y * q1y + q2y * q2y + q1y * q2y + q0y * (q1y + q2y));
-                mom[8] += 0.05 * m * (q2y * q0z + q2y * q1z + 2 * q2y * q2z + q0y * (2 * q0z + q1z + q2z) + q1y * (q0z + 2 * q1z + q2z));
-                mom[9] += 0.1 * m * (q0z * q0z + q1z * q1z + q2z * q2z + q1z * q2z + q0z * (q1z + q2z));
+                const double h = 0.05 * m;
+                mom[4] += h * (q0x * q0x + q1x * q1x + q2x * q2x + sx * sx);
+                mom[5] += h * (q0x * q0y + q1x * q1y + q2x * q2y + sx * sy);
+                mom[6] += h * (q0x * q0z + q1x * q1z + q2x * q2z + sx * sz);
+                mom[7] += h * (q0y * q0y + q1y * q1y + q2y * q2y + sy * sy);
+                mom[8] += h * (q0y * q0z + q1y * q1z + q2y * q2z + sy * sz);
+                mom[9] += h * (q0z * q0z + q1z * q1z + q2z * q2z + sz * sz);
             }
             w = AT(nbs, vn);
             k = (nbget(w, 0) == vc) ? 0 : (nbget(w, 1) == vc) ? 1 : (nbget(w, 2) == vc) ? 2 : 3;
@@ -597,7 +603,7 @@ __device__ __forceinline__ unsigned leaf_moments(int nv, const uint32_t* nbs, co
                 break;
             }
             vc = vn;
-            kn = (k + 1) % 3;
+            kn = k == 2 ? 0 : k + 1;
             todo &= ~(1ull << (3 * vc + kn));
             vn = nbget(AT(nbs, vc), kn);
         }
