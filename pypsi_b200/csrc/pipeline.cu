@@ -543,7 +543,6 @@ int bfs_clip(Ctx& C, ClipArgs& ca, long long nmain, long long nitems, unsigned l
     ba.dfs_count = &sm[S_DFS];
     ba.bytes = &sm[S_BYTES];
     ba.window_bfs = env_ll("PSIB_BFS_WINDOW", 1) != 0;
-    ba.leaf_four = env_ll("PSIB_LEAF_FOUR", 0) != 0;
     RET(ensure(C.vsum, (size_t)std::max<long long>(nitems, 1) * sizeof(double)));
     ba.vsum = C.vsum.as<double>();
     // the pass table on the device; a device counter picks the pass, so every pass runs

@@ -232,7 +232,6 @@ struct BfsArgs {
     unsigned long long *bytes; // algorithmic bytes the walk reads and writes (polyhedra, frames, records)
     int window_bfs;           // init: window-clipped images are walked here too (else listed for the
                               // depth-first kernel)
-    int leaf_four;            // atomic sums: the leaf kernel with the 14-vertex q cache, 4 blocks per SM
 };
 // each launches one resident wave of grid-stride blocks on num_sms SMs
 cudaError_t launch_bfs_init(const BfsArgs &a, int num_sms, cudaStream_t s);
