@@ -776,6 +776,14 @@ static constexpr size_t LEAF_REC_SMEM = MAXV * BB * sizeof(uint32_t) + 3 * QC_RE
 static int g_blocks[4] = {0, 0, 0, 0};
 static void occupancy();
 void bfs_prepare() { occupancy(); }
+void bfs_level_carveout(int percent)
+{
+    static int set = -1;
+    if (percent == set) return;
+    cudaFuncSetAttribute(k_bfs_level, cudaFuncAttributePreferredSharedMemoryCarveout, percent > 0 ? percent : -1);
+    cudaGetLastError();
+    set = percent;
+}
 static void occupancy()
 {
     if (g_blocks[0]) return;
@@ -803,7 +811,10 @@ cudaError_t launch_bfs_init(const BfsArgs& a, int num_sms, cudaStream_t s)
 cudaError_t launch_bfs_level(const BfsArgs& a, int num_sms, cudaStream_t s)
 {
     occupancy();
-    k_bfs_level<<<num_sms * g_blocks[1], BB, LEVEL_SMEM, s>>>(a);
+    // a.level_blocks (< the occupancy limit): fewer resident blocks, with the shared memory they
+    // leave given to L1 (the positions the cut reads through the read-only cache)
+    const int nb = (a.level_blocks > 0 && a.level_blocks < g_blocks[1]) ? a.level_blocks : g_blocks[1];
+    k_bfs_level<<<num_sms * nb, BB, LEVEL_SMEM, s>>>(a);
     return cudaGetLastError();
 }
 

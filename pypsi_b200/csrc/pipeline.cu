@@ -543,6 +543,9 @@ int bfs_clip(Ctx& C, ClipArgs& ca, long long nmain, long long nitems, unsigned l
     ba.dfs_count = &sm[S_DFS];
     ba.bytes = &sm[S_BYTES];
     ba.window_bfs = env_ll("PSIB_BFS_WINDOW", 1) != 0;
+    ba.level_blocks = (int)env_ll("PSIB_LEVEL_BLOCKS", 0);
+    // fewer level blocks leave shared memory unused: give it to L1 (one block is 30 KB of 228)
+    bfs_level_carveout(ba.level_blocks > 0 ? std::min(100, (ba.level_blocks * 31 * 100 + 227) / 228) : 0);
     RET(ensure(C.vsum, (size_t)std::max<long long>(nitems, 1) * sizeof(double)));
     ba.vsum = C.vsum.as<double>();
     // the pass table on the device; a device counter picks the pass, so every pass runs

@@ -232,6 +232,7 @@ struct BfsArgs {
     unsigned long long *bytes; // algorithmic bytes the walk reads and writes (polyhedra, frames, records)
     int window_bfs;           // init: window-clipped images are walked here too (else listed for the
                               // depth-first kernel)
+    int level_blocks;         // level: resident blocks per SM (0: as many as fit)
 };
 // each launches one resident wave of grid-stride blocks on num_sms SMs
 cudaError_t launch_bfs_init(const BfsArgs &a, int num_sms, cudaStream_t s);
@@ -241,6 +242,8 @@ cudaError_t launch_bfs_finalize(const BfsArgs &a, long long nitems, int num_sms,
 cudaError_t launch_bfs_advance(const BfsArgs &a, cudaStream_t s);
 // kernel attributes and occupancy, queried once before any launch or stream capture
 void bfs_prepare();
+// the shared-memory share of the unified L1 of the level kernel, in percent (0: the driver's choice)
+void bfs_level_carveout(int percent);
 
 cudaError_t launch_tess_count(const TessArgs &a, cudaStream_t s);
 cudaError_t launch_tess_emit(const TessArgs &a, cudaStream_t s);
