@@ -251,6 +251,21 @@ __device__ __forceinline__ bool link_cut_shared(uint32_t* nbs, int base, int nv)
     return ok;
 }
 
+// The edges a cut crosses, (lower vertex vc, link np) as bits 3 vc + np: one new vertex each, so
+// a child keeps its side's vertices plus popc of the mask.
+__device__ __forceinline__ uint64_t cut_edges(int nv, uint32_t um, const uint32_t* nbI)
+{
+    uint64_t cm = 0ull;
+    for (int vc = 0; vc < nv; ++vc) {
+        const uint32_t w = AT(nbI, vc);
+        const bool low = !((um >> vc) & 1u);
+#pragma unroll
+        for (int np = 0; np < 3; ++np)
+            if (low && nbget(w, np) < nv && ((um >> nbget(w, np)) & 1u)) cm |= 1ull << (3 * vc + np);
+    }
+    return cm;
+}
+
 // Cut the polyhedron at element eI of the input queue (positions read from
 // there, links staged in nbI; upper side = bits of um, s = cr - x[ax]) into
 // element el of QL (lower side) and eu of QU (upper side), with the vertex
@@ -258,8 +273,8 @@ __device__ __forceinline__ bool link_cut_shared(uint32_t* nbs, int base, int nv)
 __device__ __forceinline__ unsigned bfs_cut(int nv, uint32_t um, float cr, float sg, int ax, const PolyQueue& QI,
                                             unsigned long long eI, const uint32_t* nbI, uint32_t* nbL, uint32_t* nbU,
                                             const PolyQueue& QL, unsigned long long el, const PolyQueue& QU,
-                                            unsigned long long eu, bool keep_up, uint32_t cut_tag, int& cntL,
-                                            int& cntU)
+                                            unsigned long long eu, bool keep_up, uint32_t cut_tag, uint64_t cm,
+                                            int& cntL, int& cntU)
 {
     auto X = [&](int v, int c) { return __ldg(&QI.x[qx(eI, v, c)]); };
     const uint32_t lmask = ((1u << nv) - 1u) & ~um;
@@ -288,17 +303,8 @@ __device__ __forceinline__ unsigned bfs_cut(int nv, uint32_t um, float cr, float
         if (u) AT(nbU, j) = ow;
         else AT(nbL, j) = ow;
     }
-    // the cut edges (lower vertex, link) as bits 3 vc + np: taking the lowest
-    // bit first creates the cut vertices in cut_poly's order, and every lane
-    // runs the loop body on every trip
-    uint64_t cm = 0ull;
-    for (int vc = 0; vc < nv && !err; ++vc) {
-        const uint32_t w = AT(nbI, vc);
-        const bool low = !((um >> vc) & 1u);
-#pragma unroll
-        for (int np = 0; np < 3; ++np)
-            if (low && ((um >> nbget(w, np)) & 1u)) cm |= 1ull << (3 * vc + np);
-    }
+    // cm: the cut edges (cut_edges); taking the lowest bit first creates the cut vertices in
+    // cut_poly's order
     int k = 0;
     while (cm && !err) {
         const int bit = __ffsll((long long)cm) - 1;
@@ -429,15 +435,40 @@ __global__ void __launch_bounds__(BB, 7) k_bfs_level(BfsArgs a)
         if (cut) { lhi[ax] -= nup; ulo[ax] += nlo; }
         const bool leafL = (cut && one_voxel(llo, lhi)) || (wcut && !win && one_voxel(lo, hi));
         const bool leafU = cut && one_voxel(ulo, uhi);
+        // the children's vertex counts, known before the cut: each side's vertices plus one per cut edge
+        uint64_t cm = 0ull;
+        int nvL = nv, nvU = 0;
+        if (cut || wcut) {
+            cm = cut_edges(nv, um, nbI);
+            const int kc = __popcll((long long)cm);
+            nvL = __popc(((1u << nv) - 1u) & ~um) + kc;
+            nvU = __popc(um) + kc;
+        }
+        // leaf children go to the low end (few vertices) or the high end of the leaf queue
+        const bool hiL = a.leaf_split > 0 && nvL > a.leaf_split, hiU = a.leaf_split > 0 && nvU > a.leaf_split;
+        const bool lfL = toleaf || leafL, lfU = cut && leafU; // toleaf: the polyhedron itself, as "L"
         const unsigned nq = cut ? (unsigned)(!leafL) + (unsigned)(!leafU) : wcut ? (unsigned)(!leafL) : 0u;
-        const unsigned nlf = toleaf ? 1u : cut ? (unsigned)leafL + (unsigned)leafU : wcut ? (unsigned)leafL : 0u;
+        const unsigned nleaf_lo = (unsigned)(lfL && !hiL) + (unsigned)(lfU && !hiU);
+        const unsigned nleaf_hi = (unsigned)(lfL && hiL) + (unsigned)(lfU && hiU);
         if (a.last && nq) st |= ST_DEPTH;
-        unsigned oq, ol;
+        unsigned oq, ol, oh;
         const unsigned long long bq = warp_reserve(a.out.count, nq, oq);
-        const unsigned long long bl = warp_reserve(a.leaf.count, nlf, ol);
+        const unsigned long long bl = warp_reserve(a.leaf.count, nleaf_lo, ol);
+        const unsigned long long bh = warp_reserve(a.leaf.count_hi, nleaf_hi, oh);
+        // leaf element of the i-th leaf child of this lane in its end (false: past that end)
+        unsigned li = 0, hj = 0;
+        auto leaf_slot = [&](bool high, unsigned long long& d) -> bool {
+            if (!high) {
+                d = bl + ol + li++;
+                return d < a.leaf.cap;
+            }
+            const unsigned long long j = bh + oh + hj++;
+            d = a.leaf.cap - 1ull - j;
+            return j < a.leaf.cap;
+        };
         if (toleaf) {
-            const unsigned long long d = bl + ol;
-            if (d >= a.leaf.cap) {
+            unsigned long long d = 0;
+            if (!leaf_slot(hiL, d)) {
                 st |= ST_OVERFLOW;
             } else {
                 for (int v = 0; v < nv; ++v) {
@@ -453,17 +484,24 @@ __global__ void __launch_bounds__(BB, 7) k_bfs_level(BfsArgs a)
         if (cut || wcut) {
             // a middle-plane cut keeps both children, a window cut only the side with s >= 0; one
             // call site for both, so that lanes doing either run the cut together
-            unsigned qi = 0, li = 0;
+            unsigned qi = 0;
+            bool fits = true;
             const PolyQueue& QL = leafL ? a.leaf : a.out;
-            const unsigned long long el = leafL ? bl + ol + li++ : bq + oq + qi++;
+            unsigned long long el = 0;
+            if (leafL) fits = leaf_slot(hiL, el);
+            else fits = (el = bq + oq + qi++) < a.out.cap;
             const PolyQueue& QU = !cut ? QL : leafU ? a.leaf : a.out;
-            const unsigned long long eu = !cut ? el : leafU ? bl + ol + li++ : bq + oq + qi++;
-            if (el >= QL.cap || eu >= QU.cap) {
+            unsigned long long eu = el;
+            if (cut) {
+                if (leafU) fits = leaf_slot(hiU, eu) && fits;
+                else fits = (eu = bq + oq + qi++) < a.out.cap && fits;
+            }
+            if (!fits) {
                 st |= ST_OVERFLOW;
             } else {
                 int nL = 0, nU = 0;
                 const unsigned e2 = bfs_cut(nv, um, cr, cut ? 1.0f : sg, ax, a.in, e, nbI, nbL, nbU, QL, el, QU, eu,
-                                            cut, axis_tag(ax), nL, nU);
+                                            cut, axis_tag(ax), cm, nL, nU);
                 if (e2) {
                     st |= e2;
                     QL.nv[el] = 0; // downstream kernels skip these
@@ -629,22 +667,30 @@ __global__ void __launch_bounds__(BB, INLINE ? 3 : 4) k_bfs_leaf(BfsArgs a)
     const int lane = threadIdx.x & 31;
     const long long warp = (long long)blockIdx.x * (BB / 32) + (threadIdx.x >> 5);
     const long long nwarp = (long long)gridDim.x * (BB / 32);
-    const unsigned long long n = min(*a.leaf.count, a.leaf.cap);
+    // the queue's two ends: [0, nlo) and, for polyhedra of more vertices, the last nhi elements
+    const unsigned long long nlo = min(*a.leaf.count, a.leaf.cap);
+    unsigned long long nhi = a.leaf.count_hi ? min(*a.leaf.count_hi, a.leaf.cap) : 0ull;
     const ClipArgs& c = a.c;
     unsigned st = 0;
+    if (nlo + nhi > a.leaf.cap) { // the ends met: more leaves than a pass can hold
+        st |= ST_OVERFLOW;
+        nhi = a.leaf.cap - nlo;
+    }
+    const unsigned long long n = nlo + nhi;
     unsigned long long frags = 0, verts = 0, moved = 0;
     // The fragment's steps run as separate blocks -- load and vertex solves, moments, sums --
     // which every lane leaves at one place, so that lanes whose fragments have fewer vertices or
     // triangles do not start the next step apart from the rest of the warp (run that way, the
     // 28 atomics of a fragment took two passes per warp; measured 1.47x faster as blocks).
     for (unsigned long long base = (unsigned long long)warp * 32; base < n; base += (unsigned long long)nwarp * 32) {
-        const unsigned long long e = base + lane;
+        const unsigned long long i = base + lane;
+        const unsigned long long e = i < nlo ? i : a.leaf.cap - 1ull - (i - nlo);
         bool has = false;
         double rec[10];
         unsigned long long key = 0;
         int nv = 0;
-        if (e < n) nv = a.leaf.nv[e];
-        const bool ok = e < n && nv >= 4 && nv <= MAXV;
+        if (i < n) nv = a.leaf.nv[e];
+        const bool ok = i < n && nv >= 4 && nv <= MAXV;
         int lo[3] = {0, 0, 0}, hi[3];
         uint32_t t = 0;
         long long gi = -1; // the fragment's voxel, -1 when out of range

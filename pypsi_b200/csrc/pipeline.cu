@@ -414,20 +414,23 @@ int leave_own_stream(Ctx& C, cudaStream_t user)
 
 // levels of one breadth-first pass: the bisection (at most DMAX_MAIN cuts) and up to 6 window planes
 constexpr int NLEV = DMAX_MAIN + 6;
-// per pass: level-queue counts [0, NLEV] and leaf-queue counts [NLEV + 1, 2 NLEV + 1]
-constexpr int NCNT = 2 * NLEV + 2;
+// per pass: level-queue counts [0, NLEV], leaf-queue counts [NLEV + 1, 2 NLEV + 1] and the leaf
+// queues' high-end counts [2 NLEV + 2, 3 NLEV + 2]
+constexpr int NCNT = 3 * NLEV + 3;
 
 // One breadth-first pass: reset the per-level counts, then init, leaf, and NLEV x (level, leaf),
 // then advance the pass counter.  The pass it walks is read from the device pass table.
 cudaError_t bfs_pass(const BfsArgs& ba, const PolyQueue* Q, unsigned long long* cq, int grid, cudaStream_t s)
 {
     unsigned long long* cl = cq + NLEV + 1;
+    unsigned long long* ch = cq + 2 * NLEV + 2;
     cudaError_t e = cudaMemsetAsync(cq, 0, NCNT * sizeof(unsigned long long), s);
     BfsArgs b = ba;
     b.out = Q[0];
     b.out.count = &cq[0];
     b.leaf = Q[2];
     b.leaf.count = &cl[0];
+    b.leaf.count_hi = &ch[0];
     if (e == cudaSuccess) e = launch_bfs_init(b, grid, s);
     if (e == cudaSuccess) e = launch_bfs_leaf(b, grid, s);
     int ia = 0;
@@ -437,6 +440,7 @@ cudaError_t bfs_pass(const BfsArgs& ba, const PolyQueue* Q, unsigned long long* 
         b.out = Q[1 - ia];
         b.out.count = &cq[lvl + 1];
         b.leaf.count = &cl[lvl + 1];
+        b.leaf.count_hi = &ch[lvl + 1];
         b.last = lvl == NLEV - 1;
         e = launch_bfs_level(b, grid, s);
         if (e == cudaSuccess) e = launch_bfs_leaf(b, grid, s);
@@ -543,7 +547,11 @@ int bfs_clip(Ctx& C, ClipArgs& ca, long long nmain, long long nitems, unsigned l
     ba.dfs_count = &sm[S_DFS];
     ba.bytes = &sm[S_BYTES];
     ba.window_bfs = env_ll("PSIB_BFS_WINDOW", 1) != 0;
-    ba.level_blocks = (int)env_ll("PSIB_LEVEL_BLOCKS", 0);
+    // Six resident level blocks per SM rather than the seven that fit, the shared memory left to L1:
+    // 4 % faster end to end at 128^3 -> 256^3 (the deep-tree kernel on its side stream finds room
+    // beside the walk), although the level kernel alone is slower so.
+    ba.level_blocks = (int)env_ll("PSIB_LEVEL_BLOCKS", 6);
+    ba.leaf_split = (int)env_ll("PSIB_LEAF_SPLIT", 7);
     // fewer level blocks leave shared memory unused: give it to L1 (one block is 30 KB of 228)
     bfs_level_carveout(ba.level_blocks > 0 ? std::min(100, (ba.level_blocks * 31 * 100 + 227) / 228) : 0);
     RET(ensure(C.vsum, (size_t)std::max<long long>(nitems, 1) * sizeof(double)));
@@ -1592,6 +1600,8 @@ int run_capture(Call& c)
     ba.dfs_count = &sm[S_DFS];
     ba.bytes = &sm[S_BYTES];
     ba.window_bfs = 1;
+    ba.level_blocks = (int)env_ll("PSIB_LEVEL_BLOCKS", 6); // as bfs_clip
+    ba.leaf_split = (int)env_ll("PSIB_LEAF_SPLIT", 7);
     ba.vsum = C.vsum.as<double>();
     ba.passes = C.passes.as<long long>();
     ba.pass_idx = &sm[S_PASS];

@@ -219,6 +219,10 @@ struct PolyQueue {
     uint32_t *item;
     unsigned long long *count;
     unsigned long long cap;
+    // leaf queue: polyhedra of more than BfsArgs::leaf_split vertices are counted here and stored
+    // from the end of the buffer (element cap - 1 - j), so that a leaf warp's lanes mostly hold
+    // fragments of similar vertex counts; the two ends together stay within cap
+    unsigned long long *count_hi;
 };
 struct BfsArgs {
     ClipArgs c;               // frames, queue order, grid, records, status, counters, scale
@@ -233,6 +237,7 @@ struct BfsArgs {
     int window_bfs;           // init: window-clipped images are walked here too (else listed for the
                               // depth-first kernel)
     int level_blocks;         // level: resident blocks per SM (0: as many as fit)
+    int leaf_split;           // level: leaves of more vertices go to the leaf queue's high end (0: none)
 };
 // each launches one resident wave of grid-stride blocks on num_sms SMs
 cudaError_t launch_bfs_init(const BfsArgs &a, int num_sms, cudaStream_t s);
