@@ -124,8 +124,15 @@ __device__ __forceinline__ void accumulate_fragment(const ClipArgs& a, const Gri
             DV[i][k] = fr[FR_U + 3 * (k + 1) + i] - v0[i];
         }
     }
-    double cm[3] = {0.0, 0.0, 0.0}, cv[3] = {0.0, 0.0, 0.0}, sxx[3][3], sxv[3][3], svv[3][3];
-    mixed_fragment(rec, p0, DX, v0, DV, hx, hv, hxx, hxv, hvv, cm, cv, sxx, sxv, svv);
+    // the projection of mixed_fragment, computed where its terms are added so that the matrices
+    // of one field are dead before the next field's are formed (a smaller register peak in the
+    // leaf and clip kernels that inline this)
+    const double* cq = rec + 1;
+    double cm[3] = {0.0, 0.0, 0.0}, cv[3] = {0.0, 0.0, 0.0};
+    if (hx)
+        for (int i = 0; i < 3; ++i) cm[i] = p0[i] + DX[i][0] * cq[0] + DX[i][1] * cq[1] + DX[i][2] * cq[2];
+    if (hv)
+        for (int i = 0; i < 3; ++i) cv[i] = v0[i] + DV[i][0] * cq[0] + DV[i][1] * cq[1] + DV[i][2] * cq[2];
     double dx[3] = {0.0, 0.0, 0.0}, dv[3] = {0.0, 0.0, 0.0};
     if (hx) {
         double cen[3], r[3];
@@ -147,15 +154,43 @@ __device__ __forceinline__ void accumulate_fragment(const ClipArgs& a, const Gri
             atomicAdd(S + A.ov + i, m * dv[i]);
         }
     }
-    int k = 0;
-    for (int i = 0; i < 3; ++i)
-        for (int j = i; j < 3; ++j, ++k) {
-            if (hxx) atomicAdd(S + A.oxx + k, m * (sxx[i][j] + dx[i] * dx[j]));
-            if (hvv) atomicAdd(S + A.ovv + k, m * (svv[i][j] + dv[i] * dv[j]));
-        }
-    if (hxv)
+    if (!(hxx || hxv || hvv)) return;
+    // central q-space second moment C of the fragment
+    const double C[3][3] = {{rec[4], rec[5], rec[6]}, {rec[5], rec[7], rec[8]}, {rec[6], rec[8], rec[9]}};
+    if (hxx || hxv) {
+        double TX[3][3]; // DX C
         for (int i = 0; i < 3; ++i)
-            for (int j = 0; j < 3; ++j) atomicAdd(S + A.oxv + 3 * i + j, m * (sxv[i][j] + dx[i] * dv[j]));
+            for (int q = 0; q < 3; ++q) TX[i][q] = DX[i][0] * C[0][q] + DX[i][1] * C[1][q] + DX[i][2] * C[2][q];
+        if (hxx) {
+            int k = 0;
+            for (int i = 0; i < 3; ++i)
+                for (int j = i; j < 3; ++j, ++k) {
+                    const double sxx = TX[i][0] * DX[j][0] + TX[i][1] * DX[j][1] + TX[i][2] * DX[j][2];
+                    atomicAdd(S + A.oxx + k, m * (sxx + dx[i] * dx[j]));
+                }
+        }
+        if (hxv)
+            // the reference's pairing of the x-v cross terms (src/geometry.c:137-146):
+            // cov_xv + 2 a b^T - a a^T - b b^T with a = x0 - c_x, b = v0 - c_v
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) {
+                    const double ai = p0[i] - cm[i], aj = p0[j] - cm[j], bi = v0[i] - cv[i], bj = v0[j] - cv[j];
+                    const double sxv = TX[i][0] * DV[j][0] + TX[i][1] * DV[j][1] + TX[i][2] * DV[j][2] +
+                                       2.0 * ai * bj - ai * aj - bi * bj;
+                    atomicAdd(S + A.oxv + 3 * i + j, m * (sxv + dx[i] * dv[j]));
+                }
+    }
+    if (hvv) {
+        double TV[3][3]; // DV C
+        for (int i = 0; i < 3; ++i)
+            for (int q = 0; q < 3; ++q) TV[i][q] = DV[i][0] * C[0][q] + DV[i][1] * C[1][q] + DV[i][2] * C[2][q];
+        int k = 0;
+        for (int i = 0; i < 3; ++i)
+            for (int j = i; j < 3; ++j, ++k) {
+                const double svv = TV[i][0] * DV[j][0] + TV[i][1] * DV[j][1] + TV[i][2] * DV[j][2];
+                atomicAdd(S + A.ovv + k, m * (svv + dv[i] * dv[j]));
+            }
+    }
 }
 
 } // namespace psib
