@@ -363,13 +363,21 @@ __global__ void __launch_bounds__(BB, 7) k_bfs_level(BfsArgs a)
     const int lane = threadIdx.x & 31;
     const long long warp = (long long)blockIdx.x * (BB / 32) + (threadIdx.x >> 5);
     const long long nwarp = (long long)gridDim.x * (BB / 32);
-    // a producer reserves before it checks capacity (and flags the overflow), so clamp
-    const unsigned long long n = min(*a.in.count, a.in.cap);
+    // a producer reserves before it checks capacity (and flags the overflow), so clamp; the input
+    // queue's two ends: [0, ilo) and, for polyhedra of more vertices, its last ihi elements
+    const unsigned long long ilo = min(*a.in.count, a.in.cap);
+    unsigned long long ihi = a.in.count_hi ? min(*a.in.count_hi, a.in.cap) : 0ull;
     unsigned st = 0;
+    if (ilo + ihi > a.in.cap) { // the ends met: more polyhedra than a pass can hold
+        st |= ST_OVERFLOW;
+        ihi = a.in.cap - ilo;
+    }
+    const unsigned long long n = ilo + ihi;
     unsigned long long splits = 0, moved = 0;
     for (unsigned long long base = (unsigned long long)warp * 32; base < n; base += (unsigned long long)nwarp * 32) {
-        const unsigned long long e = base + lane;
-        bool act = e < n;
+        const unsigned long long ie = base + lane;
+        const unsigned long long e = ie < ilo ? ie : a.in.cap - 1ull - (ie - ilo);
+        bool act = ie < n;
         int nv = 0, lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0}, ax = 0, nlo = 0, nup = 0;
         uint32_t um = 0, t = 0, win = 0;
         float cr = 0.0f, sg = 1.0f;
@@ -447,24 +455,39 @@ __global__ void __launch_bounds__(BB, 7) k_bfs_level(BfsArgs a)
         // leaf children go to the low end (few vertices) or the high end of the leaf queue
         const bool hiL = a.leaf_split > 0 && nvL > a.leaf_split, hiU = a.leaf_split > 0 && nvU > a.leaf_split;
         const bool lfL = toleaf || leafL, lfU = cut && leafU; // toleaf: the polyhedron itself, as "L"
-        const unsigned nq = cut ? (unsigned)(!leafL) + (unsigned)(!leafU) : wcut ? (unsigned)(!leafL) : 0u;
+        // the next level queue is filled from both ends the same way
+        const bool qL = (cut || wcut) && !leafL, qU = cut && !leafU;
+        const bool two = a.out.count_hi != nullptr && a.level_split > 0; // the level queue's high end
+        const bool qhL = two && nvL > a.level_split, qhU = two && nvU > a.level_split;
+        const unsigned nq = (unsigned)qL + (unsigned)qU;
+        const unsigned nq_lo = (unsigned)(qL && !qhL) + (unsigned)(qU && !qhU);
+        const unsigned nq_hi = nq - nq_lo;
         const unsigned nleaf_lo = (unsigned)(lfL && !hiL) + (unsigned)(lfU && !hiU);
         const unsigned nleaf_hi = (unsigned)(lfL && hiL) + (unsigned)(lfU && hiU);
         if (a.last && nq) st |= ST_DEPTH;
-        unsigned oq, ol, oh;
-        const unsigned long long bq = warp_reserve(a.out.count, nq, oq);
+        unsigned oq, oqh, ol, oh;
+        const unsigned long long bq = warp_reserve(a.out.count, nq_lo, oq);
+        const unsigned long long bqh = two ? warp_reserve(a.out.count_hi, nq_hi, oqh) : 0ull;
+        if (!two) oqh = 0;
         const unsigned long long bl = warp_reserve(a.leaf.count, nleaf_lo, ol);
         const unsigned long long bh = warp_reserve(a.leaf.count_hi, nleaf_hi, oh);
-        // leaf element of the i-th leaf child of this lane in its end (false: past that end)
-        unsigned li = 0, hj = 0;
-        auto leaf_slot = [&](bool high, unsigned long long& d) -> bool {
+        // element of the next child of this lane at the low or high end of queue Q (false: past it)
+        unsigned li = 0, hj = 0, qi = 0, qj = 0;
+        auto end_slot = [](const PolyQueue& Q, bool high, unsigned long long b_lo, unsigned o_lo, unsigned& i_lo,
+                           unsigned long long b_hi, unsigned o_hi, unsigned& i_hi, unsigned long long& d) -> bool {
             if (!high) {
-                d = bl + ol + li++;
-                return d < a.leaf.cap;
+                d = b_lo + o_lo + i_lo++;
+                return d < Q.cap;
             }
-            const unsigned long long j = bh + oh + hj++;
-            d = a.leaf.cap - 1ull - j;
-            return j < a.leaf.cap;
+            const unsigned long long j = b_hi + o_hi + i_hi++;
+            d = Q.cap - 1ull - j;
+            return j < Q.cap;
+        };
+        auto leaf_slot = [&](bool high, unsigned long long& d) -> bool {
+            return end_slot(a.leaf, high, bl, ol, li, bh, oh, hj, d);
+        };
+        auto out_slot = [&](bool high, unsigned long long& d) -> bool {
+            return end_slot(a.out, high, bq, oq, qi, bqh, oqh, qj, d);
         };
         if (toleaf) {
             unsigned long long d = 0;
@@ -484,17 +507,16 @@ __global__ void __launch_bounds__(BB, 7) k_bfs_level(BfsArgs a)
         if (cut || wcut) {
             // a middle-plane cut keeps both children, a window cut only the side with s >= 0; one
             // call site for both, so that lanes doing either run the cut together
-            unsigned qi = 0;
             bool fits = true;
             const PolyQueue& QL = leafL ? a.leaf : a.out;
             unsigned long long el = 0;
             if (leafL) fits = leaf_slot(hiL, el);
-            else fits = (el = bq + oq + qi++) < a.out.cap;
+            else fits = out_slot(qhL, el);
             const PolyQueue& QU = !cut ? QL : leafU ? a.leaf : a.out;
             unsigned long long eu = el;
             if (cut) {
                 if (leafU) fits = leaf_slot(hiU, eu) && fits;
-                else fits = (eu = bq + oq + qi++) < a.out.cap && fits;
+                else fits = out_slot(qhU, eu) && fits;
             }
             if (!fits) {
                 st |= ST_OVERFLOW;

@@ -414,9 +414,9 @@ int leave_own_stream(Ctx& C, cudaStream_t user)
 
 // levels of one breadth-first pass: the bisection (at most DMAX_MAIN cuts) and up to 6 window planes
 constexpr int NLEV = DMAX_MAIN + 6;
-// per pass: level-queue counts [0, NLEV], leaf-queue counts [NLEV + 1, 2 NLEV + 1] and the leaf
-// queues' high-end counts [2 NLEV + 2, 3 NLEV + 2]
-constexpr int NCNT = 3 * NLEV + 3;
+// per pass: level-queue counts [0, NLEV], leaf-queue counts [NLEV + 1, 2 NLEV + 1], the leaf
+// queues' high-end counts [2 NLEV + 2, 3 NLEV + 2] and the level queues' [3 NLEV + 3, 4 NLEV + 3]
+constexpr int NCNT = 4 * NLEV + 4;
 
 // One breadth-first pass: reset the per-level counts, then init, leaf, and NLEV x (level, leaf),
 // then advance the pass counter.  The pass it walks is read from the device pass table.
@@ -424,10 +424,12 @@ cudaError_t bfs_pass(const BfsArgs& ba, const PolyQueue* Q, unsigned long long* 
 {
     unsigned long long* cl = cq + NLEV + 1;
     unsigned long long* ch = cq + 2 * NLEV + 2;
+    unsigned long long* cqh = cq + 3 * NLEV + 3;
     cudaError_t e = cudaMemsetAsync(cq, 0, NCNT * sizeof(unsigned long long), s);
     BfsArgs b = ba;
     b.out = Q[0];
     b.out.count = &cq[0];
+    b.out.count_hi = &cqh[0];
     b.leaf = Q[2];
     b.leaf.count = &cl[0];
     b.leaf.count_hi = &ch[0];
@@ -437,8 +439,10 @@ cudaError_t bfs_pass(const BfsArgs& ba, const PolyQueue* Q, unsigned long long* 
     for (int lvl = 0; lvl < NLEV && e == cudaSuccess; ++lvl) {
         b.in = Q[ia];
         b.in.count = &cq[lvl];
+        b.in.count_hi = &cqh[lvl];
         b.out = Q[1 - ia];
         b.out.count = &cq[lvl + 1];
+        b.out.count_hi = &cqh[lvl + 1];
         b.leaf.count = &cl[lvl + 1];
         b.leaf.count_hi = &ch[lvl + 1];
         b.last = lvl == NLEV - 1;
@@ -552,6 +556,7 @@ int bfs_clip(Ctx& C, ClipArgs& ca, long long nmain, long long nitems, unsigned l
     // beside the walk), although the level kernel alone is slower so.
     ba.level_blocks = (int)env_ll("PSIB_LEVEL_BLOCKS", 6);
     ba.leaf_split = (int)env_ll("PSIB_LEAF_SPLIT", 7);
+    ba.level_split = (int)env_ll("PSIB_LEVEL_SPLIT", 7);
     // fewer level blocks leave shared memory unused: give it to L1 (one block is 30 KB of 228)
     bfs_level_carveout(ba.level_blocks > 0 ? std::min(100, (ba.level_blocks * 31 * 100 + 227) / 228) : 0);
     RET(ensure(C.vsum, (size_t)std::max<long long>(nitems, 1) * sizeof(double)));
@@ -1602,6 +1607,7 @@ int run_capture(Call& c)
     ba.window_bfs = 1;
     ba.level_blocks = (int)env_ll("PSIB_LEVEL_BLOCKS", 6); // as bfs_clip
     ba.leaf_split = (int)env_ll("PSIB_LEAF_SPLIT", 7);
+    ba.level_split = (int)env_ll("PSIB_LEVEL_SPLIT", 7);
     ba.vsum = C.vsum.as<double>();
     ba.passes = C.passes.as<long long>();
     ba.pass_idx = &sm[S_PASS];
