@@ -557,6 +557,7 @@ int bfs_clip(Ctx& C, ClipArgs& ca, long long nmain, long long nitems, unsigned l
     ba.level_blocks = (int)env_ll("PSIB_LEVEL_BLOCKS", 6);
     ba.leaf_split = (int)env_ll("PSIB_LEAF_SPLIT", 7);
     ba.level_split = (int)env_ll("PSIB_LEVEL_SPLIT", 7);
+    ba.leaf_four = env_ll("PSIB_LEAF_FOUR", 0) != 0;
     // fewer level blocks leave shared memory unused: give it to L1 (one block is 30 KB of 228)
     bfs_level_carveout(ba.level_blocks > 0 ? std::min(100, (ba.level_blocks * 31 * 100 + 227) / 228) : 0);
     RET(ensure(C.vsum, (size_t)std::max<long long>(nitems, 1) * sizeof(double)));
