@@ -679,11 +679,10 @@ constexpr int QC_REC = 14;
 
 // INLINE: atomic mode, each fragment added to its voxel's sums here; else a record per fragment
 // (sorted mode: sorted and applied after the walk).
-// FOUR (with INLINE): the 14-vertex q cache and at most 128 registers, four blocks per SM.
-template <bool INLINE, bool FOUR = false>
-__global__ void __launch_bounds__(BB, (INLINE && !FOUR) ? 3 : 4) k_bfs_leaf(BfsArgs a)
+template <bool INLINE>
+__global__ void __launch_bounds__(BB, INLINE ? 3 : 4) k_bfs_leaf(BfsArgs a)
 {
-    constexpr int QC = (INLINE && !FOUR) ? MAXV : QC_REC;
+    constexpr int QC = INLINE ? MAXV : QC_REC;
     extern __shared__ uint32_t smem[];
     uint32_t* nbs = smem;
     double* qs = (double*)(smem + MAXV * BB); // [v * 3 + c][thread], v < QC
@@ -842,7 +841,7 @@ static constexpr size_t LEAF_SMEM = MAXV * BB * sizeof(uint32_t) + 3 * MAXV * BB
 static constexpr size_t LEAF_REC_SMEM = MAXV * BB * sizeof(uint32_t) + 3 * QC_REC * BB * sizeof(double);
 
 // resident blocks per SM of each kernel (one full wave of grid-stride blocks)
-static int g_blocks[5] = {0, 0, 0, 0, 0};
+static int g_blocks[4] = {0, 0, 0, 0};
 static void occupancy();
 void bfs_prepare() { occupancy(); }
 void bfs_level_carveout(int percent)
@@ -859,18 +858,15 @@ static void occupancy()
     cudaFuncSetAttribute(k_bfs_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LEVEL_SMEM);
     cudaFuncSetAttribute(k_bfs_leaf<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LEAF_SMEM);
     cudaFuncSetAttribute(k_bfs_leaf<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LEAF_REC_SMEM);
-    cudaFuncSetAttribute(k_bfs_leaf<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LEAF_REC_SMEM);
-    int b[5] = {1, 1, 1, 1, 1};
+    int b[4] = {1, 1, 1, 1};
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b[0], k_bfs_init, BB, 0) != cudaSuccess) b[0] = 1;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b[1], k_bfs_level, BB, LEVEL_SMEM) != cudaSuccess) b[1] = 1;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b[2], k_bfs_leaf<true>, BB, LEAF_SMEM) != cudaSuccess)
         b[2] = 1;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b[4], k_bfs_leaf<true, true>, BB, LEAF_REC_SMEM) != cudaSuccess)
-        b[4] = 1;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b[3], k_bfs_leaf<false>, BB, LEAF_REC_SMEM) != cudaSuccess)
         b[3] = 1;
     cudaGetLastError();
-    for (int i = 0; i < 5; ++i) g_blocks[i] = b[i] > 0 ? b[i] : 1;
+    for (int i = 0; i < 4; ++i) g_blocks[i] = b[i] > 0 ? b[i] : 1;
 }
 
 cudaError_t launch_bfs_init(const BfsArgs& a, int num_sms, cudaStream_t s)
@@ -893,8 +889,7 @@ cudaError_t launch_bfs_level(const BfsArgs& a, int num_sms, cudaStream_t s)
 cudaError_t launch_bfs_leaf(const BfsArgs& a, int num_sms, cudaStream_t s)
 {
     occupancy();
-    if (a.c.acc.sum && a.leaf_four) k_bfs_leaf<true, true><<<num_sms * g_blocks[4], BB, LEAF_REC_SMEM, s>>>(a);
-    else if (a.c.acc.sum) k_bfs_leaf<true><<<num_sms * g_blocks[2], BB, LEAF_SMEM, s>>>(a);
+    if (a.c.acc.sum) k_bfs_leaf<true><<<num_sms * g_blocks[2], BB, LEAF_SMEM, s>>>(a);
     else k_bfs_leaf<false><<<num_sms * g_blocks[3], BB, LEAF_REC_SMEM, s>>>(a);
     return cudaGetLastError();
 }

@@ -239,7 +239,6 @@ struct BfsArgs {
     int level_blocks;         // level: resident blocks per SM (0: as many as fit)
     int leaf_split;           // level: leaves of more vertices go to the leaf queue's high end (0: none)
     int level_split;          // level: children of more vertices go to the level queue's high end (0: none)
-    int leaf_four;            // atomic sums: the leaf kernel with the 14-vertex q cache, 4 blocks per SM
 };
 // each launches one resident wave of grid-stride blocks on num_sms SMs
 cudaError_t launch_bfs_init(const BfsArgs &a, int num_sms, cudaStream_t s);
