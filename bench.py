@@ -1168,7 +1168,8 @@ def run_ours(args):
                      "clip": statistics.mean(x["ms_clip"] for x in st_mixed),
                      "sort_and_apply": statistics.mean(x["ms_final"] for x in st_mixed)},
         "work": {"tets": tets_per_step, "tet_images": s["tet_images"], "fragments_per_pass": frags,
-                 "verts_per_fragment": vbar, "passes": s["passes"], "splits_per_pass": s["splits"] / s["passes"]},
+                 "verts_per_fragment": vbar, "passes": s["passes"], "splits_per_pass": s["splits"] / s["passes"],
+                 "mass_corrected_images": s.get("corrected_items")},
         "roofline": {"bound": "fp64", "achieved": tflops, "peak": fp64_peak, "unit": "TFLOP/s",
                      "frac": tflops / fp64_peak,
                      "traffic": traffic["bytes_per_step"] if traffic else None,
