@@ -30,13 +30,16 @@ CUDA_UNITS = {  # unit -> extra flags
     "clip_mixed.cu": [],
     "tess.cu": ["--fmad=false"],
     "pipeline.cu": ["--fmad=false"],
+    "annihilation_host.cu": ["--fmad=false"],
+    "query_host.cu": ["--fmad=false"],
     "noalloc.cu": ["--fmad=false"],
     "bfs.cu": [],
     "annihilation.cu": ["--fmad=false"],
     "probe.cu": [],  # the FMA issue-rate probe (explicit fma(), so contraction does not matter)
     "loaders.cpp": [],  # host code only: the snapshot readers
 }
-HEADERS = ["psib_device.cuh", "psib_clip.cuh", "psib_kernels.h", "psib_accum.cuh", "psib_adjoint.cuh"]
+HEADERS = ["psib_device.cuh", "psib_clip.cuh", "psib_kernels.h", "psib_accum.cuh", "psib_adjoint.cuh",
+           "pipeline_host.h"]
 
 
 def _newer(target: str, deps: list[str]) -> bool:

@@ -1,12 +1,16 @@
-// pipeline.cu -- the C ABI (include/psi_b200.h) and the host orchestration of
-// one PSI.voxels call on the GPU:
+// pipeline.cu -- the C ABI (include/psi_b200.h): device contexts, argument
+// checks and the host orchestration of one PSI.voxels density call on the GPU
+// (annihilation mode and the element queries have theirs in
+// annihilation_host.cu and query_host.cu):
 //
 //   count   elements -> tet images per element             (tess.cu)
 //   scan    per-element offsets (CUB)
 //   emit    tet images in the reference's visiting order    (tess.cu)
 //   order   images sorted by footprint key (CUB radix sort) for load balance
-//   clip    persistent clip kernels: one record per fragment (clip_fp64.cu / clip_mixed.cu)
-//   sort    records by (voxel, image) (CUB radix sort)
+//   clip    mixed precision: the breadth-first walk (bfs.cu), each fragment added to
+//           its voxel's sums with FP64 atomics, the sums merged into the fields once;
+//           FP64: the depth-first clip (clip_fp64.cu), one record per fragment,
+//   sort    records by (voxel, image) (CUB radix sort), and
 //   apply   each voxel's records, in image order, with the reference's
 //           online field update (tess.cu)
 //
@@ -32,9 +36,13 @@
 #include "psib_device.cuh"
 #include "psib_kernels.h"
 
-using namespace psib;
+#include "pipeline_host.h"
 
-namespace {
+using namespace psib;
+using namespace psib::host;
+
+namespace psib {
+namespace host {
 
 thread_local std::string g_err;
 
@@ -48,29 +56,6 @@ int fail(int code, const char* fmt, ...)
     g_err = buf;
     return code;
 }
-
-#define CK(x)                                                                                  \
-    do {                                                                                       \
-        cudaError_t _e = (x);                                                                  \
-        if (_e != cudaSuccess)                                                                 \
-            return fail(_e == cudaErrorMemoryAllocation ? PSIB_ERR_NOMEM : PSIB_ERR_CUDA,      \
-                        "%s failed: %s (%s:%d)", #x, cudaGetErrorString(_e), __FILE__, __LINE__); \
-    } while (0)
-
-#define RET(x)                         \
-    do {                               \
-        int _r = (x);                  \
-        if (_r != PSIB_OK) return _r;  \
-    } while (0)
-
-// host-memory calls copy the fields out in this many voxel slabs, each beside the update of the next
-constexpr int NOUT = 4;
-
-struct DevBuf {
-    void* p = nullptr;
-    size_t n = 0;
-    template <class T> T* as() const { return (T*)p; }
-};
 
 int ensure(DevBuf& b, size_t bytes)
 {
@@ -88,79 +73,6 @@ int ensure(DevBuf& b, size_t bytes)
     b.n = bytes;
     return PSIB_OK;
 }
-
-// The arguments a recorded breadth-first pass depends on.
-struct PassKey {
-    BfsArgs ba;
-    PolyQueue q[3];
-    unsigned long long* cq;
-    int grid;
-};
-
-struct Ctx {
-    int device = -1;
-    int num_sms = 0;
-    cudaStream_t own = nullptr;  // stream of host-memory calls
-    cudaStream_t copy = nullptr; // host-memory calls: the field copies, beside the first stages
-    cudaEvent_t fields_in = nullptr;
-    cudaEvent_t enter = nullptr, leave = nullptr; // device-memory calls: fences with the caller's stream
-    cudaStream_t side = nullptr; // atomic mode: the deep-tree images, beside the breadth-first walk
-    cudaEvent_t fork = nullptr, join = nullptr;
-    cudaEvent_t ev_out[NOUT] = {};
-    cudaEvent_t ev[8] = {};
-    // host-mode copies
-    DevBuf hpos, hvel, hmass, hconn, hfield[6], hgpos, hgmass;
-    // items
-    DevBuf iframe, ielem, ipid, ikey;
-    DevBuf key_sorted, order_in, order;
-    DevBuf counts, offsets;
-    DevBuf cub_tmp, scratch, scratch_big, iscale;
-    DevBuf small; // status, counters, queue heads
-    // records
-    DevBuf rkey, rmom, rkey_sorted, rperm_in, rperm, rvox, ritem, rmom_sorted, run_vox, run_cnt, run_off;
-    // breadth-first clip: three polyhedron queues, the volume histogram, per-level counters, window list
-    DevBuf qx[3], qnb[3], qnv[3], qwin[3], qbox[3], qitem[3], hist, bfs_cnt, dfs_list, vsum;
-    DevBuf btab, igrid; // batch tables, image -> cutout
-    DevBuf adjcoef;     // full adjoint: per-voxel coefficients
-    // atomic accumulation: per-voxel sums, tile reference velocities, the mass-correction pass
-    DevBuf acc_sum, acc_ref, acc_tsum, acc_vref, acc_toff, fix_list, fix_keys, fix_list_s, fix_keys_s, ifactor;
-    DevBuf passes;      // breadth-first pass table
-    // annihilation: element tets and boxes, cell registrations, element and tet pairs
-    DevBuf a_cnt, a_off, a_ebox, a_tets_a, a_tets_b, a_stats, a_reg_cnt, a_reg_off, a_reg_key, a_reg_elem,
-        a_reg_key_s, a_reg_elem_s, a_run_key, a_run_cnt, a_run_off, a_run_lo, a_run_hi, a_pair_cnt, a_pair_off,
-        a_pair_key, a_pair_key_s, a_na, a_aoff, a_tp_cnt, a_tp_excl, a_bounds, a_tpairs, a_deep, a_tp_key,
-        a_tp_key_s, a_ord_in, a_ord;
-    // element queries and phase-space samples
-    DevBuf q_in, q_cnt, q_off, q_key, q_key_s, q_out, s_cnt, s_off, s_offs, s_rho, s_vel;
-    cudaGraphExec_t pass_exec = nullptr; // one breadth-first pass as a CUDA graph
-    PassKey pass_key{};                  // the arguments it was recorded with
-    // the capture mode: the sizes a plan call found, and the page-locked copy of the batch tables
-    struct Plan {
-        bool valid = false;
-        long long nelem = 0, nvox = 0, cap_items = 0, ntiles = 0, tiles = 0, qcap = 0;
-        int nbatch = 0, max_passes = 0, stride = 0, precision = -1;
-        unsigned flags = 0;
-        size_t btab_bytes = 0;
-    } plan;
-    void* btab_host = nullptr;
-    size_t btab_host_n = 0;
-    std::vector<DevBuf*> all()
-    {
-        return {&hpos, &hgpos, &hgmass, &hvel, &hmass, &hconn, &hfield[0], &hfield[1], &hfield[2], &hfield[3], &hfield[4],
-                &hfield[5], &iframe, &ielem, &ipid, &ikey,
-                &key_sorted, &order_in, &order, &counts, &offsets, &cub_tmp, &scratch, &scratch_big, &iscale, &small, &rkey, &rmom,
-                &rkey_sorted, &rperm_in, &rperm, &rvox, &ritem, &rmom_sorted, &run_vox, &run_cnt, &run_off,
-                &qx[0], &qx[1], &qx[2], &qnb[0], &qnb[1], &qnb[2], &qnv[0], &qnv[1], &qnv[2], &qbox[0], &qbox[1],
-                &qbox[2], &qitem[0], &qitem[1], &qitem[2], &hist, &bfs_cnt, &dfs_list, &vsum, &qwin[0], &qwin[1],
-                &qwin[2], &btab, &igrid, &passes, &a_cnt, &a_off, &a_ebox, &a_tets_a, &a_tets_b, &a_stats,
-                &a_reg_cnt, &a_reg_off, &a_reg_key, &a_reg_elem, &a_reg_key_s, &a_reg_elem_s, &a_run_key,
-                &a_run_cnt, &a_run_off, &a_run_lo, &a_run_hi, &a_pair_cnt, &a_pair_off, &a_pair_key,
-                &a_pair_key_s, &a_na, &a_aoff, &a_tp_cnt, &a_tp_excl, &a_bounds, &a_tpairs, &a_deep, &a_tp_key,
-                &a_tp_key_s, &a_ord_in, &a_ord, &q_in, &q_cnt, &adjcoef, &acc_sum, &acc_ref, &acc_tsum, &acc_vref, &acc_toff,
-                &fix_list, &fix_keys, &fix_list_s, &fix_keys_s, &ifactor,
-                &q_off, &q_key, &q_key_s, &q_out, &s_cnt, &s_off, &s_offs, &s_rho, &s_vel};
-    }
-};
 
 std::mutex g_mu;
 Ctx* g_ctx[64];
@@ -189,9 +101,159 @@ int get_ctx(int dev, Ctx** out)
     return PSIB_OK;
 }
 
-// small device block layout (unsigned long long words)
-enum { S_STATUS = 0, S_CNT = 1 /* 3 words */, S_TESS = 4 /* 2 */, S_HEAD = 8 /* 4 */, S_RECN = 12, S_NDEEP = 13,
-       S_DFS = 14, S_BYTES = 15, S_PASS = 6, S_FIX = 7, S_NMAIN = 16, S_NITEMS = 17, S_WORDS = 18 };
+long long env_ll(const char* name, long long dflt)
+{
+    const char* s = getenv(name);
+    if (!s || !*s) return dflt;
+    return atoll(s);
+}
+
+int check_status(Call& c, unsigned long long* small_host)
+{
+    unsigned st = (unsigned)small_host[S_STATUS];
+    if (!st) return PSIB_OK;
+    if (st & ST_INDEX) return fail(PSIB_ERR_INDEX, "connectivity or voxel index out of range (status 0x%x)", st);
+    if (st & (ST_OVERFLOW | ST_DEPTH))
+        return fail(PSIB_ERR_OVERFLOW, "a polyhedron outgrew the vertex buffer or slot pool (status 0x%x)", st);
+    if (st & ST_GRAPH) return fail(PSIB_ERR_OVERFLOW, "a polyhedron graph walk did not close (status 0x%x)", st);
+    return fail(PSIB_ERR_CUDA, "kernel status 0x%x", st);
+}
+
+// Device-memory calls run on the library's own non-blocking stream (a CUDA graph cannot be
+// recorded on the legacy default stream), after the work already queued on the caller's stream
+// and before anything the caller queues next.
+int enter_own_stream(Ctx& C, cudaStream_t user)
+{
+    CK(cudaEventRecord(C.enter, user));
+    CK(cudaStreamWaitEvent(C.own, C.enter, 0));
+    return PSIB_OK;
+}
+int leave_own_stream(Ctx& C, cudaStream_t user)
+{
+    CK(cudaEventRecord(C.leave, C.own));
+    CK(cudaStreamWaitEvent(user, C.leave, 0));
+    return PSIB_OK;
+}
+
+GridDev grid_dev(const psib_grid& g)
+{
+    GridDev gd;
+    for (int i = 0; i < 3; ++i) {
+        gd.n[i] = g.n[i];
+        gd.w0[i] = g.window[0][i];
+        gd.w1[i] = g.window[1][i];
+        gd.d[i] = g.d[i];
+    }
+    return gd;
+}
+
+// The device view of a mesh on a grid: arrays, lattice, box, and the
+// refinement parameters that depend on the grid (midpoint tolerance) or the
+// mesh (Lagrangian cell of the stretch criterion).
+MeshDev mesh_dev(const psib_mesh& m, const psib_grid& g, const double* pos, const double* vel, const double* mass,
+                 const int* conn, double reftol, const double* lag)
+{
+    MeshDev md;
+    md.elemtype = m.elemtype;
+    md.npart = m.npart;
+    md.nelem = m.nelem;
+    md.pos = pos;
+    md.vel = vel;
+    md.mass = mass;
+    md.conn = conn;
+    md.periodic = m.periodic ? 1 : 0;
+    for (int i = 0; i < 3; ++i) {
+        md.bdim[i] = m.block_dims[i];
+        md.edim[i] = m.periodic ? m.block_dims[i] : m.block_dims[i] - 1;
+        md.box0[i] = m.box[0][i];
+        md.box1[i] = m.box[1][i];
+        md.lag[i] = lag ? lag[i] : 0.0;
+    }
+    double dxmin = 1.0e30;
+    for (int i = 0; i < 3; ++i)
+        if (g.d[i] < dxmin) dxmin = g.d[i];
+    const double tol = reftol * dxmin;
+    md.ptol2 = tol * tol;
+    return md;
+}
+
+// Host-memory calls: copy the mesh to the context's device buffers.
+int copy_mesh_in(Call& c, Ctx& C, const psib_mesh& mesh, cudaStream_t st)
+{
+    const size_t np3 = (size_t)mesh.npart * 3 * sizeof(double);
+    RET(ensure(C.hpos, np3));
+    CK(cudaMemcpyAsync(C.hpos.p, mesh.pos, np3, cudaMemcpyHostToDevice, st));
+    c.pos = C.hpos.as<double>();
+    if (mesh.vel) {
+        RET(ensure(C.hvel, np3));
+        CK(cudaMemcpyAsync(C.hvel.p, mesh.vel, np3, cudaMemcpyHostToDevice, st));
+        c.vel = C.hvel.as<double>();
+    }
+    if (mesh.mass) {
+        RET(ensure(C.hmass, (size_t)mesh.nelem * sizeof(double)));
+        CK(cudaMemcpyAsync(C.hmass.p, mesh.mass, (size_t)mesh.nelem * sizeof(double), cudaMemcpyHostToDevice, st));
+        c.mass = C.hmass.as<double>();
+    }
+    if (mesh.connectivity) {
+        const size_t cb = (size_t)mesh.nelem * mesh.elemtype * sizeof(int);
+        RET(ensure(C.hconn, cb));
+        CK(cudaMemcpyAsync(C.hconn.p, mesh.connectivity, cb, cudaMemcpyHostToDevice, st));
+        c.conn = C.hconn.as<int>();
+    }
+    return PSIB_OK;
+}
+
+int validate_mesh(const psib_mesh* m)
+{
+    if (!m) return fail(PSIB_ERR_ARG, "mesh is required");
+    if (m->elemtype != 4 && m->elemtype != 8 && m->elemtype != 27)
+        return fail(PSIB_ERR_ARG, "elemtype must be 4, 8 or 27");
+    if (m->nelem < 0 || m->npart < 0) return fail(PSIB_ERR_ARG, "negative mesh size");
+    if (m->nelem >= (1ll << 31) || m->npart >= (1ll << 31))
+        return fail(PSIB_ERR_ARG, "meshes of 2^31 elements or particles are not supported");
+    if (m->nelem > 0 && !m->pos) return fail(PSIB_ERR_ARG, "pos is required");
+    if (!m->connectivity) {
+        if (m->elemtype != 8) return fail(PSIB_ERR_ARG, "implicit connectivity needs elemtype 8");
+        long long np = 1, nel = 1;
+        for (int i = 0; i < 3; ++i) {
+            if (m->block_dims[i] <= 0) return fail(PSIB_ERR_ARG, "connectivity or block_dims is required");
+            np *= m->block_dims[i];
+            nel *= m->periodic ? m->block_dims[i] : m->block_dims[i] - 1;
+        }
+        if (np != m->npart || nel != m->nelem) return fail(PSIB_ERR_ARG, "block_dims disagree with npart/nelem");
+    }
+    return PSIB_OK;
+}
+
+int validate(const psib_grid* g, const psib_mesh* m, int mode, const psib_options* o)
+{
+    if (!g || !m) return fail(PSIB_ERR_ARG, "grid and mesh are required");
+    if (mode != PSIB_MODE_DENSITY && mode != PSIB_MODE_ANNIHILATION) return fail(PSIB_ERR_ARG, "invalid mode %d", mode);
+    if (mode == PSIB_MODE_ANNIHILATION && o && o->refine_mode != PSIB_REFINE_MIDPOINT)
+        return fail(PSIB_ERR_UNSUPPORTED, "annihilation mode refines by the midpoint criterion only");
+    for (int i = 0; i < 3; ++i) {
+        if (g->n[i] <= 0) return fail(PSIB_ERR_ARG, "grid n must be positive");
+        if (!(g->d[i] > 0.0)) return fail(PSIB_ERR_ARG, "grid cell size d must be positive");
+    }
+    if ((long long)g->n[0] * g->n[1] * g->n[2] >= (1ll << 32))
+        return fail(PSIB_ERR_ARG, "grids of 2^32 voxels or more are not supported");
+    if (!g->fields[PSIB_M]) return fail(PSIB_ERR_ARG, "field m is required");
+    if (g->fields[PSIB_XX] && !g->fields[PSIB_X]) return fail(PSIB_ERR_ARG, "field 'xx' requires field 'x'");
+    if (g->fields[PSIB_XV] && !(g->fields[PSIB_X] && g->fields[PSIB_V]))
+        return fail(PSIB_ERR_ARG, "field 'xv' requires fields 'x' and 'v'");
+    if (g->fields[PSIB_VV] && !g->fields[PSIB_V]) return fail(PSIB_ERR_ARG, "field 'vv' requires field 'v'");
+    RET(validate_mesh(m));
+    if (o && o->refine_mode != PSIB_REFINE_MIDPOINT && o->refine_mode != PSIB_REFINE_STRETCH)
+        return fail(PSIB_ERR_ARG, "invalid refine_mode %d", o->refine_mode);
+    if (o && o->precision != PSIB_FP64 && o->precision != PSIB_MIXED && o->precision != PSIB_FP64_CENTRAL)
+        return fail(PSIB_ERR_ARG, "invalid precision %d", o->precision);
+    return PSIB_OK;
+}
+
+} // namespace host
+} // namespace psib
+
+namespace {
 
 // Histogram of the sorted footprint keys: lanes holding equal keys (most of a
 // warp, as the keys are sorted) add with one atomic.
@@ -214,18 +276,6 @@ __global__ void k_count_deep(const uint16_t* key, long long n, unsigned long lon
         c += (key[i] == KEY_DEEP);
     c = __reduce_add_sync(0xFFFFFFFFu, (unsigned)c);
     if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, c);
-}
-
-__global__ void k_iota(int* o, long long n)
-{
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        o[i] = (int)i;
-}
-
-__global__ void k_iota_u(unsigned* o, long long n)
-{
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        o[i] = (unsigned)i;
 }
 
 // ---- capture mode: counts and the pass plan on the device ----
@@ -325,50 +375,6 @@ __global__ void k_plan_list(const uint16_t* keys, const unsigned long long* n_de
     }
 }
 
-size_t round_up(size_t b) { return (b + 15) & ~(size_t)15; }
-
-long long env_ll(const char* name, long long dflt)
-{
-    const char* s = getenv(name);
-    if (!s || !*s) return dflt;
-    return atoll(s);
-}
-
-struct Call {
-    const psib_grid* grid;
-    const psib_mesh* mesh;
-    int mode; // PSIB_MODE_DENSITY or PSIB_MODE_ANNIHILATION
-    double reftol;
-    int maxlvl;
-    int precision;
-    int deterministic;
-    cudaStream_t st;
-    Ctx* C;
-    psib_stats* stats;
-    // device views
-    double* F[6];
-    const double *pos, *vel, *mass;
-    const int* conn;
-    int refine_mode;
-    double refine_cell[3];
-    long long queue_voxels;
-    cudaEvent_t fields_ready; // host-memory calls: recorded when the fields are on the device
-    double* const* host_fields; // host-memory calls: where the fields go back (the caller's arrays)
-    bool copied_out;          // run_device copied the fields back itself
-    // a batch of cutouts (nbatch > 0): host arrays of grids and meshes (device pointers)
-    int nbatch;
-    const psib_grid* grids;
-    const psib_mesh* meshes;
-    const double* refine_cell_given;
-    int capture;              // options.capture: 0 plain, 1 plan, 2 capture (run_capture)
-    int order_cell_bits;      // options.order_cell_bits: coarse cells of the footprint key
-    // adjoint call: F[0] holds dL/dm (or adj_coef the full adjoint's per-voxel coefficients);
-    // gradients accumulate into these
-    bool adjoint;
-    double *gpos, *gmass, *gvel;
-    const double* adj_coef;
-};
-
 // Bits of the footprint key's coarse cell per axis: b bits shared out x, y, z, x, ...
 // (0 means the default 7 = 8 x 4 x 4 cells; negative means no spatial order).
 void order_cells(int b, int* cb)
@@ -378,38 +384,6 @@ void order_cells(int b, int* cb)
     if (b < 0) return;
     if (b > KEY_CELL_BITS) b = KEY_CELL_BITS;
     for (int i = 0; i < b; ++i) ++cb[i % 3];
-}
-
-int check_status(Call& c, unsigned long long* small_host)
-{
-    unsigned st = (unsigned)small_host[S_STATUS];
-    if (!st) return PSIB_OK;
-    if (st & ST_INDEX) return fail(PSIB_ERR_INDEX, "connectivity or voxel index out of range (status 0x%x)", st);
-    if (st & (ST_OVERFLOW | ST_DEPTH))
-        return fail(PSIB_ERR_OVERFLOW, "a polyhedron outgrew the vertex buffer or slot pool (status 0x%x)", st);
-    if (st & ST_GRAPH) return fail(PSIB_ERR_OVERFLOW, "a polyhedron graph walk did not close (status 0x%x)", st);
-    return fail(PSIB_ERR_CUDA, "kernel status 0x%x", st);
-}
-
-// Mixed-precision clip of queue positions [0, nmain) by the breadth-first
-// walk (bfs.cu); images that need the window clip come back in a list and go to
-// the depth-first kernel.  Images are sorted by index-box volume, largest
-// first; a pass takes images while the sum of their box volumes -- a bound on
-// every queue of the pass -- stays within the queue capacity.
-// Device-memory calls run on the library's own non-blocking stream (a CUDA graph cannot be
-// recorded on the legacy default stream), after the work already queued on the caller's stream
-// and before anything the caller queues next.
-int enter_own_stream(Ctx& C, cudaStream_t user)
-{
-    CK(cudaEventRecord(C.enter, user));
-    CK(cudaStreamWaitEvent(C.own, C.enter, 0));
-    return PSIB_OK;
-}
-int leave_own_stream(Ctx& C, cudaStream_t user)
-{
-    CK(cudaEventRecord(C.leave, C.own));
-    CK(cudaStreamWaitEvent(user, C.leave, 0));
-    return PSIB_OK;
 }
 
 // levels of one breadth-first pass: the bisection (at most DMAX_MAIN cuts) and up to 6 window planes
@@ -460,6 +434,11 @@ struct BfsSizes {
     long long tiles = 0, cap = 0, npass = 0;
 };
 
+// Mixed-precision clip of queue positions [0, nmain) by the breadth-first
+// walk (bfs.cu); images that need the window clip come back in a list and go to
+// the depth-first kernel.  Images are sorted by index-box volume, largest
+// first; a pass takes images while the sum of their box volumes -- a bound on
+// every queue of the pass -- stays within the queue capacity.
 // keys: the footprint keys of the queue positions [0, nmain), ascending.
 int bfs_clip(Ctx& C, ClipArgs& ca, long long nmain, long long nitems, unsigned long long* sm, int clip_grid,
              int clip_block, long long queue_voxels, bool batch, cudaStream_t st, long long& launches,
@@ -638,48 +617,6 @@ int bfs_clip(Ctx& C, ClipArgs& ca, long long nmain, long long nitems, unsigned l
     return PSIB_OK;
 }
 
-GridDev grid_dev(const psib_grid& g)
-{
-    GridDev gd;
-    for (int i = 0; i < 3; ++i) {
-        gd.n[i] = g.n[i];
-        gd.w0[i] = g.window[0][i];
-        gd.w1[i] = g.window[1][i];
-        gd.d[i] = g.d[i];
-    }
-    return gd;
-}
-
-// The device view of a mesh on a grid: arrays, lattice, box, and the
-// refinement parameters that depend on the grid (midpoint tolerance) or the
-// mesh (Lagrangian cell of the stretch criterion).
-MeshDev mesh_dev(const psib_mesh& m, const psib_grid& g, const double* pos, const double* vel, const double* mass,
-                 const int* conn, double reftol, const double* lag)
-{
-    MeshDev md;
-    md.elemtype = m.elemtype;
-    md.npart = m.npart;
-    md.nelem = m.nelem;
-    md.pos = pos;
-    md.vel = vel;
-    md.mass = mass;
-    md.conn = conn;
-    md.periodic = m.periodic ? 1 : 0;
-    for (int i = 0; i < 3; ++i) {
-        md.bdim[i] = m.block_dims[i];
-        md.edim[i] = m.periodic ? m.block_dims[i] : m.block_dims[i] - 1;
-        md.box0[i] = m.box[0][i];
-        md.box1[i] = m.box[1][i];
-        md.lag[i] = lag ? lag[i] : 0.0;
-    }
-    double dxmin = 1.0e30;
-    for (int i = 0; i < 3; ++i)
-        if (g.d[i] < dxmin) dxmin = g.d[i];
-    const double tol = reftol * dxmin;
-    md.ptol2 = tol * tol;
-    return md;
-}
-
 // the Lagrangian cell of the stretch criterion: given, or box / block_dims of a periodic block mesh
 int stretch_cell(const psib_mesh& m, const double* given, double* lag)
 {
@@ -691,8 +628,6 @@ int stretch_cell(const psib_mesh& m, const double* given, double* lag)
     }
     return PSIB_OK;
 }
-
-int run_annihilation(Call& c);
 
 // The mass correction of the atomic mode.  A breadth-first image's FP32 walk
 // can miss the exact q-volume by O(1e-7) where a fragment vertex falls back to
@@ -1241,7 +1176,7 @@ int run_device(Call& c)
             RET(ensure(C.run_vox, (size_t)maxruns * 4));
             RET(ensure(C.run_cnt, (size_t)maxruns * 4 + 8));
             RET(ensure(C.run_off, (size_t)maxruns * 8));
-            k_iota_u<<<C.num_sms * 8, 256, 0, st>>>(C.rperm_in.as<unsigned>(), (long long)nrec);
+            k_iota<<<C.num_sms * 8, 256, 0, st>>>(C.rperm_in.as<unsigned>(), (long long)nrec);
             CK(cudaGetLastError());
             tb = 0;
             CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, C.rkey.as<unsigned long long>(),
@@ -1662,997 +1597,6 @@ int run_capture(Call& c)
     return PSIB_OK;
 }
 
-// ---- annihilation mode ----
-
-// Exclusive scan of n counts into n offsets (CUB), on the stream.
-template <class In, class Out>
-int excl_scan(Ctx& C, const In* in, Out* out, long long n, cudaStream_t st)
-{
-    if (n >= (1ll << 31)) return fail(PSIB_ERR_OVERFLOW, "a scan of %lld items is too long", n);
-    size_t tb = 0;
-    CK(cub::DeviceScan::ExclusiveScan(nullptr, tb, in, out, cub::Sum(), (Out)0, (int)n, st));
-    RET(ensure(C.cub_tmp, tb));
-    CK(cub::DeviceScan::ExclusiveScan(C.cub_tmp.p, tb, in, out, cub::Sum(), (Out)0, (int)n, st));
-    return PSIB_OK;
-}
-
-template <class T>
-int read_dev(const T* p, T& out, cudaStream_t st)
-{
-    CK(cudaMemcpyAsync(&out, p, sizeof(T), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    return PSIB_OK;
-}
-
-int bits_for(unsigned long long n)
-{
-    int b = 1;
-    while (b < 64 && (1ull << b) < n) ++b;
-    return b;
-}
-
-double from_ord(unsigned long long o)
-{
-    const unsigned long long b = (o >> 63) ? (o & 0x7FFFFFFFFFFFFFFFull) : ~o;
-    double x;
-    memcpy(&x, &b, 8);
-    return x;
-}
-
-// The cell index over the kept element boxes (aa.nelem, aa.ebox and the kept
-// flags aa.cnt_a / aa.cnt_b set): a uniform grid of cells about one mean
-// element box wide (at most 1024 per axis); every kept element registered in
-// the cells its box covers, sorted by cell; each registration's cell run
-// (aa.run_lo / run_hi) and the runs themselves (aa.run_key / run_off /
-// run_cnt, aa.nruns).  kept = the number of kept elements (0: no index).
-int build_cells(Ctx& C, AnnArgs& aa, cudaStream_t st, long long& klaunch, long long& kept)
-{
-    const long long ne = aa.nelem;
-    RET(ensure(C.a_stats, 16 * 8));
-    CK(cudaMemsetAsync(C.a_stats.p, 0xFF, 3 * 8, st));
-    CK(cudaMemsetAsync(C.a_stats.as<char>() + 24, 0, 13 * 8, st));
-    unsigned long long* bs = C.a_stats.as<unsigned long long>();
-    CK(launch_ann_box_stats(aa, bs, (double*)(bs + 8), st));
-    klaunch++;
-    unsigned long long hb[16];
-    CK(cudaMemcpyAsync(hb, bs, sizeof(hb), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    kept = (long long)hb[6];
-    if (kept == 0) return PSIB_OK;
-    long long ncell = 1;
-    for (int i = 0; i < 3; ++i) {
-        const double lo = from_ord(hb[i]), hi = from_ord(hb[3 + i]);
-        double ext;
-        memcpy(&ext, &hb[8 + i], 8);
-        const double range = hi - lo;
-        // cells about one mean element box wide, at most 1024 per axis
-        double h = ext / (double)kept;
-        if (!(h >= range / 1024.0)) h = range / 1024.0;
-        if (!(h > 0.0) || !std::isfinite(h)) h = range > 0.0 && std::isfinite(range) ? range : 1.0;
-        aa.cg.o[i] = std::isfinite(lo) ? lo : 0.0;
-        aa.cg.h[i] = h;
-        long long n = std::isfinite(range) ? (long long)(range / h) + 1 : 1;
-        aa.cg.n[i] = n < 1 ? 1 : (n > 1024 ? 1024 : n);
-        ncell *= aa.cg.n[i];
-    }
-
-    // ---- cell registrations, sorted by cell ----
-    RET(ensure(C.a_reg_cnt, (size_t)(ne + 1) * sizeof(long long)));
-    RET(ensure(C.a_reg_off, (size_t)(ne + 1) * sizeof(long long)));
-    aa.reg_cnt = C.a_reg_cnt.as<long long>();
-    CK(launch_ann_cells(aa, false, st));
-    CK(cudaMemsetAsync(aa.reg_cnt + ne, 0, sizeof(long long), st));
-    RET(excl_scan(C, aa.reg_cnt, C.a_reg_off.as<long long>(), ne + 1, st));
-    long long nreg = 0;
-    RET(read_dev(C.a_reg_off.as<long long>() + ne, nreg, st));
-    if (nreg >= (1ll << 31)) return fail(PSIB_ERR_OVERFLOW, "too many cell registrations (%lld)", nreg);
-    RET(ensure(C.a_reg_key, (size_t)nreg * 8));
-    RET(ensure(C.a_reg_elem, (size_t)nreg * 4));
-    RET(ensure(C.a_reg_key_s, (size_t)nreg * 8));
-    RET(ensure(C.a_reg_elem_s, (size_t)nreg * 4));
-    aa.reg_off = C.a_reg_off.as<long long>();
-    aa.reg_key = C.a_reg_key.as<unsigned long long>();
-    aa.reg_elem = C.a_reg_elem.as<int>();
-    CK(launch_ann_cells(aa, true, st));
-    klaunch += 2;
-    {
-        size_t tb = 0;
-        const int cb = bits_for((unsigned long long)ncell);
-        CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, aa.reg_key, C.a_reg_key_s.as<unsigned long long>(), aa.reg_elem,
-                                           C.a_reg_elem_s.as<int>(), (int)nreg, 0, cb, st));
-        RET(ensure(C.cub_tmp, tb));
-        CK(cub::DeviceRadixSort::SortPairs(C.cub_tmp.p, tb, aa.reg_key, C.a_reg_key_s.as<unsigned long long>(),
-                                           aa.reg_elem, C.a_reg_elem_s.as<int>(), (int)nreg, 0, cb, st));
-    }
-    aa.reg_key = C.a_reg_key_s.as<unsigned long long>();
-    aa.reg_elem = C.a_reg_elem_s.as<int>();
-    aa.nreg = nreg;
-    // each registration's cell run
-    RET(ensure(C.a_run_key, (size_t)nreg * 8));
-    RET(ensure(C.a_run_cnt, (size_t)nreg * 4 + 8));
-    RET(ensure(C.a_run_off, (size_t)nreg * 8));
-    RET(ensure(C.a_run_lo, (size_t)nreg * 8));
-    RET(ensure(C.a_run_hi, (size_t)nreg * 8));
-    {
-        int* d_nruns = (int*)(C.a_run_cnt.as<char>() + (size_t)nreg * 4);
-        size_t tb = 0;
-        CK(cub::DeviceRunLengthEncode::Encode(nullptr, tb, aa.reg_key, C.a_run_key.as<unsigned long long>(),
-                                              C.a_run_cnt.as<int>(), d_nruns, (int)nreg, st));
-        RET(ensure(C.cub_tmp, tb));
-        CK(cub::DeviceRunLengthEncode::Encode(C.cub_tmp.p, tb, aa.reg_key, C.a_run_key.as<unsigned long long>(),
-                                              C.a_run_cnt.as<int>(), d_nruns, (int)nreg, st));
-        int nruns = 0;
-        RET(read_dev(d_nruns, nruns, st));
-        RET(excl_scan(C, C.a_run_cnt.as<int>(), C.a_run_off.as<long long>(), nruns, st));
-        CK(launch_ann_runs(C.a_run_cnt.as<unsigned>(), C.a_run_off.as<long long>(), nruns, C.a_run_lo.as<long long>(),
-                           C.a_run_hi.as<long long>(), st));
-        klaunch++;
-        aa.nruns = nruns;
-    }
-    aa.run_key = C.a_run_key.as<unsigned long long>();
-    aa.run_off = C.a_run_off.as<long long>();
-    aa.run_cnt = C.a_run_cnt.as<int>();
-    aa.run_lo = C.a_run_lo.as<long long>();
-    aa.run_hi = C.a_run_hi.as<long long>();
-    return PSIB_OK;
-}
-
-// Annihilation mode (src/cpsi.c:115-158): elements -> tets of both sides ->
-// element pairs from a uniform cell grid -> tet pairs in the reference's order
-// (e, e1 descending, t, t1), streamed in chunks -> one clip thread per tet pair
-// -> records sorted by (voxel, tet pair) and summed into m.
-int run_annihilation(Call& c)
-{
-    Ctx& C = *c.C;
-    const psib_grid& g = *c.grid;
-    const psib_mesh& m = *c.mesh;
-    cudaStream_t st = c.st;
-    const long long ne = m.nelem;
-    const long long nvox = (long long)g.n[0] * g.n[1] * g.n[2];
-    const GridDev gd = grid_dev(g);
-    const MeshDev md = mesh_dev(m, g, c.pos, c.vel, c.mass, c.conn, c.reftol, nullptr);
-    RET(ensure(C.small, S_WORDS * 8));
-    unsigned long long* sm = C.small.as<unsigned long long>();
-    CK(cudaMemsetAsync(sm, 0, S_WORDS * 8, st));
-    long long klaunch = 0, launches = 0;
-    float ms_tess = 0.f, ms_clip = 0.f, ms_final = 0.f;
-    unsigned long long counts[3] = {0, 0, 0};
-    long long ntp_total = 0;
-    int nchunks = 0;
-    auto fill_stats = [&](const unsigned long long* h) {
-        if (!c.stats) return;
-        psib_stats& s = *c.stats;
-        s.elements_kept = (long long)h[S_TESS];
-        s.tets = (long long)h[S_TESS + 1];
-        s.tet_images = ntp_total;
-        s.fragments = (long long)counts[0];
-        s.frag_verts = (long long)counts[1];
-        s.splits = (long long)counts[2];
-        s.passes = 1;
-        s.chunks = nchunks;
-        s.ms_tess = ms_tess;
-        s.ms_clip = ms_clip;
-        s.ms_final = ms_final;
-        s.clip_launches = launches;
-        s.kernel_launches = klaunch + launches;
-    };
-    auto finish = [&]() -> int {
-        unsigned long long h[S_WORDS];
-        CK(cudaMemcpyAsync(h, sm, sizeof(h), cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
-        RET(check_status(c, h));
-        fill_stats(h);
-        return PSIB_OK;
-    };
-    CK(cudaEventRecord(C.ev[2], st));
-
-    // ---- elements: cull, side A and side B tets ----
-    RET(ensure(C.a_cnt, (size_t)2 * (ne + 1) * sizeof(int)));
-    RET(ensure(C.a_off, (size_t)2 * (ne + 1) * sizeof(long long)));
-    RET(ensure(C.a_ebox, (size_t)(ne > 0 ? ne : 1) * 6 * sizeof(double)));
-    int* cnt_a = C.a_cnt.as<int>();
-    int* cnt_b = cnt_a + (ne + 1);
-    long long* off_a = C.a_off.as<long long>();
-    long long* off_b = off_a + (ne + 1);
-    AnnTessArgs ta = {};
-    ta.m = md;
-    ta.g = gd;
-    ta.max_lvl = c.maxlvl;
-    ta.quad = m.elemtype == 27;
-    ta.cnt_a = cnt_a;
-    ta.cnt_b = cnt_b;
-    ta.ebox = C.a_ebox.as<double>();
-    ta.status = (unsigned*)&sm[S_STATUS];
-    ta.counters = &sm[S_TESS];
-    CK(launch_ann_tess(ta, false, st));
-    klaunch++;
-    CK(cudaMemsetAsync(cnt_a + ne, 0, sizeof(int), st));
-    CK(cudaMemsetAsync(cnt_b + ne, 0, sizeof(int), st));
-    RET(excl_scan(C, cnt_a, off_a, ne + 1, st));
-    RET(excl_scan(C, cnt_b, off_b, ne + 1, st));
-    long long na_tot = 0, nb_tot = 0;
-    RET(read_dev(off_a + ne, na_tot, st));
-    RET(read_dev(off_b + ne, nb_tot, st));
-    {
-        unsigned long long h[S_WORDS];
-        CK(cudaMemcpy(h, sm, sizeof(h), cudaMemcpyDeviceToHost));
-        RET(check_status(c, h));
-    }
-    if (na_tot >= (1ll << 31) || nb_tot >= (1ll << 31)) return fail(PSIB_ERR_OVERFLOW, "2^31 tets or more");
-    if (na_tot == 0 || nb_tot == 0) return finish();
-    RET(ensure(C.a_tets_a, (size_t)na_tot * TREC * sizeof(double)));
-    RET(ensure(C.a_tets_b, (size_t)nb_tot * TREC * sizeof(double)));
-    ta.off_a = off_a;
-    ta.off_b = off_b;
-    ta.tets_a = C.a_tets_a.as<double>();
-    ta.tets_b = C.a_tets_b.as<double>();
-    CK(launch_ann_tess(ta, true, st));
-    klaunch++;
-
-    // ---- the cell grid over the kept element boxes ----
-    AnnArgs aa = {};
-    aa.nelem = ne;
-    aa.ebox = C.a_ebox.as<double>();
-    aa.cnt_a = cnt_a;
-    aa.cnt_b = cnt_b;
-    aa.off_a = off_a;
-    aa.off_b = off_b;
-    aa.tets_a = ta.tets_a;
-    aa.tets_b = ta.tets_b;
-    aa.status = (unsigned*)&sm[S_STATUS];
-    long long kept = 0;
-    RET(build_cells(C, aa, st, klaunch, kept));
-    if (kept == 0) return finish();
-    const long long nreg = aa.nreg;
-
-    // ---- element pairs, sorted (e ascending, e1 descending) ----
-    RET(ensure(C.a_pair_cnt, (size_t)(nreg + 1) * sizeof(long long)));
-    RET(ensure(C.a_pair_off, (size_t)(nreg + 1) * sizeof(long long)));
-    aa.pair_cnt = C.a_pair_cnt.as<long long>();
-    CK(launch_ann_pairs(aa, false, st));
-    CK(cudaMemsetAsync(aa.pair_cnt + nreg, 0, sizeof(long long), st));
-    RET(excl_scan(C, aa.pair_cnt, C.a_pair_off.as<long long>(), nreg + 1, st));
-    long long npair = 0;
-    RET(read_dev(C.a_pair_off.as<long long>() + nreg, npair, st));
-    if (npair >= (1ll << 31)) return fail(PSIB_ERR_OVERFLOW, "too many element pairs (%lld)", npair);
-    RET(ensure(C.a_pair_key, (size_t)(npair > 0 ? npair : 1) * 8));
-    RET(ensure(C.a_pair_key_s, (size_t)(npair > 0 ? npair : 1) * 8));
-    aa.pair_off = C.a_pair_off.as<long long>();
-    aa.pair_key = C.a_pair_key.as<unsigned long long>();
-    CK(launch_ann_pairs(aa, true, st));
-    klaunch += 2;
-    {
-        size_t tb = 0;
-        const int kb = 32 + bits_for((unsigned long long)ne);
-        CK(cub::DeviceRadixSort::SortKeys(nullptr, tb, aa.pair_key, C.a_pair_key_s.as<unsigned long long>(), (int)npair,
-                                          0, kb, st));
-        RET(ensure(C.cub_tmp, tb));
-        CK(cub::DeviceRadixSort::SortKeys(C.cub_tmp.p, tb, aa.pair_key, C.a_pair_key_s.as<unsigned long long>(),
-                                          (int)npair, 0, kb, st));
-    }
-    aa.pair_key = C.a_pair_key_s.as<unsigned long long>();
-    aa.npair = npair;
-
-    // ---- tet-pair slots: side-A tets of each element pair; tet pairs per slot ----
-    RET(ensure(C.a_na, (size_t)(npair + 1) * sizeof(long long)));
-    RET(ensure(C.a_aoff, (size_t)(npair + 1) * sizeof(long long)));
-    CK(launch_ann_pair_sides(aa, C.a_na.as<long long>(), st));
-    CK(cudaMemsetAsync(C.a_na.as<long long>() + npair, 0, sizeof(long long), st));
-    RET(excl_scan(C, C.a_na.as<long long>(), C.a_aoff.as<long long>(), npair + 1, st));
-    long long nslot = 0;
-    RET(read_dev(C.a_aoff.as<long long>() + npair, nslot, st));
-    if (nslot >= (1ll << 31)) return fail(PSIB_ERR_OVERFLOW, "too many tet slots (%lld)", nslot);
-    aa.aoff = C.a_aoff.as<long long>();
-    aa.nslot = nslot;
-    RET(ensure(C.a_tp_cnt, (size_t)(nslot + 1) * sizeof(long long)));
-    RET(ensure(C.a_tp_excl, (size_t)(nslot + 1) * sizeof(long long)));
-    aa.tp_cnt = C.a_tp_cnt.as<long long>();
-    aa.slot0 = 0;
-    aa.slot1 = nslot;
-    CK(launch_ann_tpairs(aa, false, st));
-    CK(cudaMemsetAsync(aa.tp_cnt + nslot, 0, sizeof(long long), st));
-    RET(excl_scan(C, aa.tp_cnt, C.a_tp_excl.as<long long>(), nslot + 1, st));
-    RET(read_dev(C.a_tp_excl.as<long long>() + nslot, ntp_total, st));
-    aa.tp_excl = C.a_tp_excl.as<long long>();
-    klaunch += 3;
-    CK(cudaEventRecord(C.ev[3], st));
-    CK(cudaEventSynchronize(C.ev[3]));
-    CK(cudaEventElapsedTime(&ms_tess, C.ev[2], C.ev[3]));
-    if (ntp_total == 0) return finish();
-
-    // ---- chunks of about `budget` tet pairs, on slot boundaries ----
-    const long long budget = std::max<long long>(env_ll("PSIB_ANN_BUDGET", 1ll << 24), 1);
-    const int nb = (int)std::min<long long>((ntp_total + budget - 1) / budget, 1 << 20);
-    RET(ensure(C.a_bounds, (size_t)(nb + 1) * sizeof(long long)));
-    CK(launch_ann_chunk_bounds(aa.tp_excl, nslot, budget, nb, C.a_bounds.as<long long>(), st));
-    std::vector<long long> bnd(nb + 1), boff(nb + 1);
-    CK(cudaMemcpyAsync(bnd.data(), C.a_bounds.p, (nb + 1) * sizeof(long long), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    for (int k = 0; k <= nb; ++k)
-        CK(cudaMemcpyAsync(&boff[k], aa.tp_excl + bnd[k], sizeof(long long), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    long long cap = 1;
-    for (int k = 0; k < nb; ++k) cap = std::max(cap, boff[k + 1] - boff[k]);
-    if (cap >= (1ll << 31)) return fail(PSIB_ERR_OVERFLOW, "a chunk of %lld tet pairs is too large", cap);
-    RET(ensure(C.a_tpairs, (size_t)cap * sizeof(int2)));
-    RET(ensure(C.a_deep, (size_t)cap * sizeof(int)));
-    RET(ensure(C.a_tp_key, (size_t)cap * sizeof(uint16_t)));
-    RET(ensure(C.a_tp_key_s, (size_t)cap * sizeof(uint16_t)));
-    RET(ensure(C.a_ord_in, (size_t)cap * sizeof(int)));
-    RET(ensure(C.a_ord, (size_t)cap * sizeof(int)));
-    aa.tpairs = C.a_tpairs.as<int2>();
-    aa.tp_key = C.a_tp_key.as<uint16_t>();
-    aa.g = gd;
-
-    const int clip_block = 128, big_block = 64;
-    const int clip_grid = C.num_sms * ann_blocks_per_sm(false, clip_block);
-    RET(ensure(C.scratch, ann_scratch_bytes(false) * (size_t)clip_grid * clip_block));
-    const int vbits = bits_for((unsigned long long)nvox);
-    if (c.fields_ready) CK(cudaStreamWaitEvent(st, c.fields_ready, 0));
-    for (int k = 0; k < nb; ++k) {
-        const long long ntp = boff[k + 1] - boff[k];
-        if (ntp == 0) continue;
-        nchunks++;
-        CK(cudaEventRecord(C.ev[4], st));
-        aa.slot0 = bnd[k];
-        aa.slot1 = bnd[k + 1];
-        aa.tp_base = boff[k];
-        CK(launch_ann_tpairs(aa, true, st));
-        // the clip's order: larger walks first (k_ann_tpairs' keys)
-        k_iota<<<C.num_sms * 8, 256, 0, st>>>(C.a_ord_in.as<int>(), ntp);
-        CK(cudaGetLastError());
-        {
-            size_t tb = 0;
-            CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, aa.tp_key, C.a_tp_key_s.as<uint16_t>(),
-                                               C.a_ord_in.as<int>(), C.a_ord.as<int>(), (int)ntp, 0, 16, st));
-            RET(ensure(C.cub_tmp, tb));
-            CK(cub::DeviceRadixSort::SortPairs(C.cub_tmp.p, tb, aa.tp_key, C.a_tp_key_s.as<uint16_t>(),
-                                               C.a_ord_in.as<int>(), C.a_ord.as<int>(), (int)ntp, 0, 16, st));
-        }
-        klaunch += 2;
-        const int ibits = bits_for((unsigned long long)ntp);
-        if (ibits + vbits > 64) return fail(PSIB_ERR_OVERFLOW, "grid and chunk too large for a 64-bit record key");
-        AnnClipArgs ca = {};
-        ca.tpairs = aa.tpairs;
-        ca.tets_a = ta.tets_a;
-        ca.tets_b = ta.tets_b;
-        ca.g = gd;
-        ca.deep = C.a_deep.as<int>();
-        ca.ndeep = &sm[S_NDEEP];
-        ca.rec_n = &sm[S_RECN];
-        ca.rec_ibits = ibits;
-        ca.status = (unsigned*)&sm[S_STATUS];
-        ca.counters = &sm[S_CNT];
-        unsigned long long nrec = 0;
-        for (int attempt = 0;; ++attempt) {
-            const unsigned long long want = (unsigned long long)std::max<long long>(ntp * 4, 1 << 16);
-            RET(ensure(C.rkey, std::max<size_t>(C.rkey.n, want * 8)));
-            RET(ensure(C.rmom, std::max<size_t>(C.rmom.n, C.rkey.n)));
-            ca.rec_key = C.rkey.as<unsigned long long>();
-            ca.rec_val = C.rmom.as<double>();
-            ca.rec_cap = std::min<unsigned long long>(C.rkey.n / 8, C.rmom.n / 8);
-            CK(cudaMemsetAsync(&sm[S_RECN], 0, 16, st)); // records, deep list
-            CK(cudaMemsetAsync(&sm[S_CNT], 0, 24, st));
-            CK(cudaMemsetAsync(&sm[S_HEAD], 0, 16, st));
-            ca.n = ntp;
-            ca.list = C.a_ord.as<int>();
-            ca.head = &sm[S_HEAD];
-            ca.scratch = C.scratch.p;
-            CK(launch_ann_clip(ca, false, clip_grid, clip_block, st));
-            launches++;
-            unsigned long long ndeep = 0;
-            RET(read_dev(&sm[S_NDEEP], ndeep, st));
-            if (ndeep > 0) {
-                const int big_grid =
-                    (int)std::min<long long>((long long)C.num_sms * ann_blocks_per_sm(true, big_block),
-                                             ((long long)ndeep + big_block - 1) / big_block);
-                RET(ensure(C.scratch_big, ann_scratch_bytes(true) * (size_t)big_grid * big_block));
-                ca.n = (long long)ndeep;
-                ca.list = C.a_deep.as<int>();
-                ca.head = &sm[S_HEAD + 1];
-                ca.scratch = C.scratch_big.p;
-                CK(launch_ann_clip(ca, true, big_grid, big_block, st));
-                launches++;
-            }
-            unsigned long long h[S_WORDS];
-            CK(cudaMemcpyAsync(h, sm, sizeof(h), cudaMemcpyDeviceToHost, st));
-            CK(cudaStreamSynchronize(st));
-            nrec = h[S_RECN];
-            if (nrec > ca.rec_cap && attempt == 0) {
-                RET(ensure(C.rkey, nrec * 8));
-                RET(ensure(C.rmom, nrec * 8));
-                unsigned clr = 0;
-                CK(cudaMemcpy(&sm[S_STATUS], &clr, sizeof(clr), cudaMemcpyHostToDevice));
-                continue;
-            }
-            RET(check_status(c, h));
-            for (int w = 0; w < 3; ++w) counts[w] += h[S_CNT + w];
-            break;
-        }
-        CK(cudaEventRecord(C.ev[5], st));
-        if (nrec >= (1ull << 32)) return fail(PSIB_ERR_OVERFLOW, "too many fragments in one chunk");
-        if (nrec > 0) {
-            // ---- records sorted by (voxel, tet pair), each voxel's run summed in that order ----
-            RET(ensure(C.rkey_sorted, nrec * 8));
-            RET(ensure(C.rperm_in, nrec * 4));
-            RET(ensure(C.rperm, nrec * 4));
-            RET(ensure(C.rvox, nrec * 4));
-            RET(ensure(C.ritem, nrec * 4));
-            RET(ensure(C.rmom_sorted, nrec * 8));
-            const long long maxruns = std::min<long long>((long long)nrec, nvox);
-            RET(ensure(C.run_vox, (size_t)maxruns * 4));
-            RET(ensure(C.run_cnt, (size_t)maxruns * 4 + 8));
-            RET(ensure(C.run_off, (size_t)maxruns * 8));
-            k_iota_u<<<C.num_sms * 8, 256, 0, st>>>(C.rperm_in.as<unsigned>(), (long long)nrec);
-            CK(cudaGetLastError());
-            size_t tb = 0;
-            CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, C.rkey.as<unsigned long long>(),
-                                               C.rkey_sorted.as<unsigned long long>(), C.rperm_in.as<unsigned>(),
-                                               C.rperm.as<unsigned>(), (int)nrec, 0, ibits + vbits, st));
-            RET(ensure(C.cub_tmp, tb));
-            CK(cub::DeviceRadixSort::SortPairs(C.cub_tmp.p, tb, C.rkey.as<unsigned long long>(),
-                                               C.rkey_sorted.as<unsigned long long>(), C.rperm_in.as<unsigned>(),
-                                               C.rperm.as<unsigned>(), (int)nrec, 0, ibits + vbits, st));
-            GatherArgs ga = {};
-            ga.key = C.rkey_sorted.as<unsigned long long>();
-            ga.perm = C.rperm.as<unsigned>();
-            ga.mom = C.rmom.as<double>();
-            ga.nrec = (long long)nrec;
-            ga.nmom = 1;
-            ga.ibits = ibits;
-            ga.vox = C.rvox.as<unsigned>();
-            ga.item = C.ritem.as<unsigned>();
-            ga.mom_sorted = C.rmom_sorted.as<double>();
-            CK(launch_gather_records(ga, st));
-            int* d_nruns = (int*)(C.run_cnt.as<char>() + (size_t)maxruns * 4);
-            tb = 0;
-            CK(cub::DeviceRunLengthEncode::Encode(nullptr, tb, C.rvox.as<unsigned>(), C.run_vox.as<unsigned>(),
-                                                  C.run_cnt.as<int>(), d_nruns, (int)nrec, st));
-            RET(ensure(C.cub_tmp, tb));
-            CK(cub::DeviceRunLengthEncode::Encode(C.cub_tmp.p, tb, C.rvox.as<unsigned>(), C.run_vox.as<unsigned>(),
-                                                  C.run_cnt.as<int>(), d_nruns, (int)nrec, st));
-            int nruns = 0;
-            RET(read_dev(d_nruns, nruns, st));
-            RET(excl_scan(C, C.run_cnt.as<int>(), C.run_off.as<long long>(), nruns, st));
-            ApplyArgs ap = {};
-            ap.run_vox = C.run_vox.as<unsigned>();
-            ap.run_cnt = C.run_cnt.as<int>();
-            ap.run_off = C.run_off.as<long long>();
-            ap.nruns = nruns;
-            ap.mom = C.rmom_sorted.as<double>();
-            ap.nmom = 1;
-            ap.M = c.F[0];
-            CK(launch_ann_apply(ap, st));
-            klaunch += 3;
-        }
-        CK(cudaEventRecord(C.ev[6], st));
-        CK(cudaEventSynchronize(C.ev[6]));
-        float t = 0.f;
-        CK(cudaEventElapsedTime(&t, C.ev[4], C.ev[5]));
-        ms_clip += t;
-        CK(cudaEventElapsedTime(&t, C.ev[5], C.ev[6]));
-        ms_final += t;
-    }
-    return finish();
-}
-
-// Host-memory calls: copy the mesh to the context's device buffers.
-int copy_mesh_in(Call& c, Ctx& C, const psib_mesh& mesh, cudaStream_t st)
-{
-    const size_t np3 = (size_t)mesh.npart * 3 * sizeof(double);
-    RET(ensure(C.hpos, np3));
-    CK(cudaMemcpyAsync(C.hpos.p, mesh.pos, np3, cudaMemcpyHostToDevice, st));
-    c.pos = C.hpos.as<double>();
-    if (mesh.vel) {
-        RET(ensure(C.hvel, np3));
-        CK(cudaMemcpyAsync(C.hvel.p, mesh.vel, np3, cudaMemcpyHostToDevice, st));
-        c.vel = C.hvel.as<double>();
-    }
-    if (mesh.mass) {
-        RET(ensure(C.hmass, (size_t)mesh.nelem * sizeof(double)));
-        CK(cudaMemcpyAsync(C.hmass.p, mesh.mass, (size_t)mesh.nelem * sizeof(double), cudaMemcpyHostToDevice, st));
-        c.mass = C.hmass.as<double>();
-    }
-    if (mesh.connectivity) {
-        const size_t cb = (size_t)mesh.nelem * mesh.elemtype * sizeof(int);
-        RET(ensure(C.hconn, cb));
-        CK(cudaMemcpyAsync(C.hconn.p, mesh.connectivity, cb, cudaMemcpyHostToDevice, st));
-        c.conn = C.hconn.as<int>();
-    }
-    return PSIB_OK;
-}
-
-int validate_mesh(const psib_mesh* m)
-{
-    if (!m) return fail(PSIB_ERR_ARG, "mesh is required");
-    if (m->elemtype != 4 && m->elemtype != 8 && m->elemtype != 27)
-        return fail(PSIB_ERR_ARG, "elemtype must be 4, 8 or 27");
-    if (m->nelem < 0 || m->npart < 0) return fail(PSIB_ERR_ARG, "negative mesh size");
-    if (m->nelem >= (1ll << 31) || m->npart >= (1ll << 31))
-        return fail(PSIB_ERR_ARG, "meshes of 2^31 elements or particles are not supported");
-    if (m->nelem > 0 && !m->pos) return fail(PSIB_ERR_ARG, "pos is required");
-    if (!m->connectivity) {
-        if (m->elemtype != 8) return fail(PSIB_ERR_ARG, "implicit connectivity needs elemtype 8");
-        long long np = 1, nel = 1;
-        for (int i = 0; i < 3; ++i) {
-            if (m->block_dims[i] <= 0) return fail(PSIB_ERR_ARG, "connectivity or block_dims is required");
-            np *= m->block_dims[i];
-            nel *= m->periodic ? m->block_dims[i] : m->block_dims[i] - 1;
-        }
-        if (np != m->npart || nel != m->nelem) return fail(PSIB_ERR_ARG, "block_dims disagree with npart/nelem");
-    }
-    return PSIB_OK;
-}
-
-int validate(const psib_grid* g, const psib_mesh* m, int mode, const psib_options* o)
-{
-    if (!g || !m) return fail(PSIB_ERR_ARG, "grid and mesh are required");
-    if (mode != PSIB_MODE_DENSITY && mode != PSIB_MODE_ANNIHILATION) return fail(PSIB_ERR_ARG, "invalid mode %d", mode);
-    if (mode == PSIB_MODE_ANNIHILATION && o && o->refine_mode != PSIB_REFINE_MIDPOINT)
-        return fail(PSIB_ERR_UNSUPPORTED, "annihilation mode refines by the midpoint criterion only");
-    for (int i = 0; i < 3; ++i) {
-        if (g->n[i] <= 0) return fail(PSIB_ERR_ARG, "grid n must be positive");
-        if (!(g->d[i] > 0.0)) return fail(PSIB_ERR_ARG, "grid cell size d must be positive");
-    }
-    if ((long long)g->n[0] * g->n[1] * g->n[2] >= (1ll << 32))
-        return fail(PSIB_ERR_ARG, "grids of 2^32 voxels or more are not supported");
-    if (!g->fields[PSIB_M]) return fail(PSIB_ERR_ARG, "field m is required");
-    if (g->fields[PSIB_XX] && !g->fields[PSIB_X]) return fail(PSIB_ERR_ARG, "field 'xx' requires field 'x'");
-    if (g->fields[PSIB_XV] && !(g->fields[PSIB_X] && g->fields[PSIB_V]))
-        return fail(PSIB_ERR_ARG, "field 'xv' requires fields 'x' and 'v'");
-    if (g->fields[PSIB_VV] && !g->fields[PSIB_V]) return fail(PSIB_ERR_ARG, "field 'vv' requires field 'v'");
-    RET(validate_mesh(m));
-    if (o && o->refine_mode != PSIB_REFINE_MIDPOINT && o->refine_mode != PSIB_REFINE_STRETCH)
-        return fail(PSIB_ERR_ARG, "invalid refine_mode %d", o->refine_mode);
-    if (o && o->precision != PSIB_FP64 && o->precision != PSIB_MIXED && o->precision != PSIB_FP64_CENTRAL)
-        return fail(PSIB_ERR_ARG, "invalid precision %d", o->precision);
-    return PSIB_OK;
-}
-
-// ---- element queries and phase-space samples ----
-
-// A query call: device, context, stream and the mesh in device memory (copied
-// in for host-memory calls; device-memory calls run on the library's stream
-// fenced to the caller's).
-struct QueryCall {
-    Call c;
-    Ctx* C = nullptr;
-    bool host = true;
-    cudaStream_t user = nullptr;
-};
-
-int query_begin(QueryCall& q, const psib_mesh* mesh, const psib_options* opt)
-{
-    g_err.clear();
-    RET(validate_mesh(mesh));
-    psib_options o = {};
-    o.memory = PSIB_HOST;
-    o.device = -1;
-    if (opt) o = *opt;
-    if (o.memory != PSIB_HOST && o.memory != PSIB_DEVICE) return fail(PSIB_ERR_ARG, "invalid memory kind %d", o.memory);
-    if (psib_device_count() <= 0) return fail(PSIB_ERR_NODEVICE, "no CUDA device is visible");
-    int dev = o.device;
-    if (o.memory == PSIB_DEVICE || dev < 0) CK(cudaGetDevice(&dev));
-    CK(cudaSetDevice(dev));
-    RET(get_ctx(dev, &q.C));
-    q.host = o.memory == PSIB_HOST;
-    q.c = Call{};
-    q.c.mesh = mesh;
-    q.c.C = q.C;
-    q.c.st = q.C->own;
-    if (q.host) {
-        if (mesh->nelem > 0) RET(copy_mesh_in(q.c, *q.C, *mesh, q.c.st));
-    } else {
-        q.user = (cudaStream_t)o.stream;
-        RET(enter_own_stream(*q.C, q.user));
-        q.c.pos = mesh->pos;
-        q.c.vel = mesh->vel;
-        q.c.mass = mesh->mass;
-        q.c.conn = mesh->connectivity;
-    }
-    return PSIB_OK;
-}
-
-int query_end(QueryCall& q, int rc)
-{
-    if (!q.host && q.C) {
-        const int r = leave_own_stream(*q.C, q.user);
-        if (rc == PSIB_OK) rc = r;
-    }
-    if (rc == PSIB_OK) CK(cudaStreamSynchronize(q.c.st));
-    return rc;
-}
-
-// The kept elements (cull against `window`) and their unwrapped boxes.
-int query_elements_stage(QueryCall& q, const double (*window)[3], double reftol, AnnArgs& aa, unsigned long long* sm)
-{
-    Ctx& C = *q.C;
-    const psib_mesh& m = *q.c.mesh;
-    const long long ne = m.nelem;
-    cudaStream_t st = q.c.st;
-    psib_grid gw = {};
-    for (int i = 0; i < 3; ++i) {
-        gw.n[i] = 1;
-        gw.window[0][i] = window[0][i];
-        gw.window[1][i] = window[1][i];
-        gw.d[i] = 1.0;
-    }
-    MeshDev md = mesh_dev(m, gw, q.c.pos, q.c.vel, q.c.mass, q.c.conn, 1.0, nullptr);
-    md.ptol2 = reftol * reftol; // psi_tet_buffer_init(&tetbuf, reftol, ...): the tolerance itself (src/cpsi.c:198)
-    RET(ensure(C.a_cnt, (size_t)2 * (ne + 1) * sizeof(int)));
-    RET(ensure(C.a_ebox, (size_t)(ne > 0 ? ne : 1) * 6 * sizeof(double)));
-    AnnTessArgs ta = {};
-    ta.m = md;
-    ta.g = grid_dev(gw);
-    ta.cnt_a = C.a_cnt.as<int>();
-    ta.cnt_b = ta.cnt_a + (ne + 1);
-    ta.ebox = C.a_ebox.as<double>();
-    ta.status = (unsigned*)&sm[S_STATUS];
-    if (ne > 0) CK(launch_elem_boxes(ta, st));
-    aa = AnnArgs{};
-    aa.nelem = ne;
-    aa.ebox = ta.ebox;
-    aa.cnt_a = ta.cnt_a;
-    aa.cnt_b = ta.cnt_b;
-    aa.status = ta.status;
-    q.c.reftol = reftol;
-    return PSIB_OK;
-}
-
-// A device buffer of `bytes` holding the caller's array (copied in for host-memory calls).
-int query_input(QueryCall& q, DevBuf& b, const void* src, size_t bytes, const void** dst)
-{
-    if (!q.host) {
-        *dst = src;
-        return PSIB_OK;
-    }
-    RET(ensure(b, bytes > 0 ? bytes : 16));
-    if (bytes) CK(cudaMemcpyAsync(b.p, src, bytes, cudaMemcpyHostToDevice, q.c.st));
-    *dst = b.p;
-    return PSIB_OK;
-}
-
-int query_output(QueryCall& q, void* dst, const void* src, size_t bytes)
-{
-    if (!bytes) return PSIB_OK;
-    CK(cudaMemcpyAsync(dst, src, bytes, q.host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, q.c.st));
-    return PSIB_OK;
-}
-
-int sort_keys(Ctx& C, unsigned long long* in, unsigned long long* out, long long n, int bits, cudaStream_t st)
-{
-    if (n >= (1ll << 31)) return fail(PSIB_ERR_OVERFLOW, "too many query results (%lld)", n);
-    size_t tb = 0;
-    CK(cub::DeviceRadixSort::SortKeys(nullptr, tb, in, out, (int)n, 0, bits, st));
-    RET(ensure(C.cub_tmp, tb));
-    CK(cub::DeviceRadixSort::SortKeys(C.cub_tmp.p, tb, in, out, (int)n, 0, bits, st));
-    return PSIB_OK;
-}
-
-int query_status(QueryCall& q, unsigned long long* sm)
-{
-    unsigned long long h[S_WORDS];
-    CK(cudaMemcpyAsync(h, sm, sizeof(h), cudaMemcpyDeviceToHost, q.c.st));
-    CK(cudaStreamSynchronize(q.c.st));
-    return check_status(q.c, h);
-}
-
-int query_from_boxes(QueryCall& q, AnnArgs& aa, unsigned long long* sm, const double* boxes, long long nboxes,
-                     long long* offsets, int* elements, long long capacity);
-int vdf_from_index(QueryCall& q, AnnArgs& aa, long long kept, unsigned long long* sm, const double* points,
-                   long long npoints, double reftol, int maxlvl, long long* offsets, double* rho, double* vel,
-                   long long capacity);
-int vdf_one_point(QueryCall& q, AnnArgs& aa, long long kept, unsigned long long* sm, double reftol, int maxlvl,
-                  long long* offsets, double* rho, double* vel, long long capacity);
-
-int query_elements_impl(QueryCall& q, const double (*window)[3], const double* boxes, long long nboxes,
-                        long long* offsets, int* elements, long long capacity)
-{
-    Ctx& C = *q.C;
-    cudaStream_t st = q.c.st;
-    RET(ensure(C.small, S_WORDS * 8));
-    unsigned long long* sm = C.small.as<unsigned long long>();
-    CK(cudaMemsetAsync(sm, 0, S_WORDS * 8, st));
-    AnnArgs aa;
-    RET(query_elements_stage(q, window, 1.0, aa, sm));
-    return query_from_boxes(q, aa, sm, boxes, nboxes, offsets, elements, capacity);
-}
-
-// Box queries over the kept element boxes of aa (cnt_a flags, ebox).
-int query_from_boxes(QueryCall& q, AnnArgs& aa, unsigned long long* sm, const double* boxes, long long nboxes,
-                     long long* offsets, int* elements, long long capacity)
-{
-    Ctx& C = *q.C;
-    cudaStream_t st = q.c.st;
-    const void* qin = nullptr;
-    RET(query_input(q, C.q_in, boxes, (size_t)nboxes * 6 * sizeof(double), &qin));
-    aa.qry = (const double*)qin;
-    aa.nq = nboxes;
-    RET(ensure(C.q_cnt, (size_t)(nboxes + 1) * sizeof(long long)));
-    RET(ensure(C.q_off, (size_t)(nboxes + 1) * sizeof(long long)));
-    RET(ensure(C.small, S_WORDS * 8));
-    aa.q_cnt = C.q_cnt.as<long long>();
-    CK(cudaMemsetAsync(aa.q_cnt, 0, (size_t)(nboxes + 1) * sizeof(long long), st));
-    if (nboxes > 0 && aa.nelem > 0) CK(launch_query_boxes(aa, false, st));
-    RET(excl_scan(C, aa.q_cnt, C.q_off.as<long long>(), nboxes + 1, st));
-    long long total = 0;
-    RET(read_dev(C.q_off.as<long long>() + nboxes, total, st));
-    RET(query_status(q, sm));
-    RET(query_output(q, offsets, C.q_off.p, (size_t)(nboxes + 1) * sizeof(long long)));
-    if (!elements) return PSIB_OK;
-    if (capacity < total)
-        return fail(PSIB_ERR_OVERFLOW, "the output holds %lld elements, the queries found %lld", capacity, total);
-    if (total == 0) return PSIB_OK;
-    RET(ensure(C.q_key, (size_t)total * 8));
-    RET(ensure(C.q_key_s, (size_t)total * 8));
-    aa.q_key = C.q_key.as<unsigned long long>();
-    aa.q_n = &sm[S_RECN];
-    CK(cudaMemsetAsync(aa.q_n, 0, 8, st));
-    CK(launch_query_boxes(aa, true, st));
-    RET(sort_keys(C, aa.q_key, C.q_key_s.as<unsigned long long>(), total, 32 + bits_for((unsigned long long)nboxes + 1),
-                  st));
-    int* out = elements;
-    if (q.host) {
-        RET(ensure(C.q_out, (size_t)total * sizeof(int)));
-        out = C.q_out.as<int>();
-    }
-    CK(launch_keys_elem(C.q_key_s.as<unsigned long long>(), total, out, st));
-    if (q.host) RET(query_output(q, elements, out, (size_t)total * sizeof(int)));
-    return query_status(q, sm);
-}
-
-int sample_vdf_impl(QueryCall& q, const double (*window)[3], const double* points, long long npoints, double reftol,
-                    int maxlvl, long long* offsets, double* rho, double* vel, long long capacity)
-{
-    Ctx& C = *q.C;
-    cudaStream_t st = q.c.st;
-    const psib_mesh& m = *q.c.mesh;
-    RET(ensure(C.small, S_WORDS * 8));
-    unsigned long long* sm = C.small.as<unsigned long long>();
-    CK(cudaMemsetAsync(sm, 0, S_WORDS * 8, st));
-    AnnArgs aa;
-    RET(query_elements_stage(q, window, reftol, aa, sm));
-    long long klaunch = 0, kept = 0;
-    if (aa.nelem > 0) RET(build_cells(C, aa, st, klaunch, kept));
-    return vdf_from_index(q, aa, kept, sm, points, npoints, reftol, maxlvl, offsets, rho, vel, capacity);
-}
-
-// One point in host memory (the drop-in PSI.VDF call): one thread walks the
-// point's cell and writes the samples that fit `capacity`; one copy brings
-// back their number and the samples.
-int vdf_one_point(QueryCall& q, AnnArgs& aa, long long kept, unsigned long long* sm, double reftol, int maxlvl,
-                  long long* offsets, double* rho, double* vel, long long capacity)
-{
-    Ctx& C = *q.C;
-    cudaStream_t st = q.c.st;
-    const psib_mesh& m = *q.c.mesh;
-    VdfArgs va = {};
-    va.m = mesh_dev(m, psib_grid{}, q.c.pos, q.c.vel, q.c.mass, q.c.conn, 1.0, nullptr);
-    va.m.ptol2 = reftol * reftol;
-    va.max_lvl = maxlvl > 6 ? 6 : (maxlvl < 0 ? 0 : maxlvl);
-    va.quad = m.elemtype == 27;
-    va.points = aa.qry;
-    va.status = aa.status;
-    const long long cap = (rho && vel) ? (capacity > 0 ? capacity : 0) : 0;
-    RET(ensure(C.s_rho, (size_t)(cap > 0 ? cap : 1) * sizeof(double)));
-    RET(ensure(C.s_vel, (size_t)(cap > 0 ? cap : 1) * 3 * sizeof(double)));
-    va.rho = C.s_rho.as<double>();
-    va.vel = C.s_vel.as<double>();
-    CK(cudaMemsetAsync(&sm[S_RECN], 0, 8, st));
-    if (kept > 0) CK(launch_vdf_point(va, aa, &sm[S_RECN], cap, st));
-    unsigned long long h[S_WORDS];
-    CK(cudaMemcpyAsync(h, sm, sizeof(h), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    RET(check_status(q.c, h));
-    const long long total = (long long)h[S_RECN];
-    offsets[0] = 0;
-    offsets[1] = total;
-    if (!rho || !vel) return PSIB_OK;
-    if (capacity < total)
-        return fail(PSIB_ERR_OVERFLOW, "the output holds %lld samples, the points have %lld", capacity, total);
-    if (total > 0) {
-        CK(cudaMemcpyAsync(rho, va.rho, (size_t)total * sizeof(double), cudaMemcpyDeviceToHost, st));
-        CK(cudaMemcpyAsync(vel, va.vel, (size_t)total * 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
-    }
-    return PSIB_OK;
-}
-
-// Samples at the points through the cell index of aa (kept elements, their
-// boxes, cells and runs), the mesh of q.
-int vdf_from_index(QueryCall& q, AnnArgs& aa, long long kept, unsigned long long* sm, const double* points,
-                   long long npoints, double reftol, int maxlvl, long long* offsets, double* rho, double* vel,
-                   long long capacity)
-{
-    Ctx& C = *q.C;
-    cudaStream_t st = q.c.st;
-    const psib_mesh& m = *q.c.mesh;
-    const void* qin = nullptr;
-    RET(query_input(q, C.q_in, points, (size_t)npoints * 3 * sizeof(double), &qin));
-    aa.qry = (const double*)qin;
-    aa.nq = npoints;
-    if (npoints == 1 && q.host)
-        return vdf_one_point(q, aa, kept, sm, reftol, maxlvl, offsets, rho, vel, capacity);
-    // (point, element) pairs: every kept element whose box contains the point
-    RET(ensure(C.q_cnt, (size_t)(npoints + 1) * sizeof(long long)));
-    RET(ensure(C.q_off, (size_t)(npoints + 1) * sizeof(long long)));
-    aa.q_cnt = C.q_cnt.as<long long>();
-    CK(cudaMemsetAsync(aa.q_cnt, 0, (size_t)(npoints + 1) * sizeof(long long), st));
-    if (kept > 0 && npoints > 0) CK(launch_query_points(aa, false, st));
-    RET(excl_scan(C, aa.q_cnt, C.q_off.as<long long>(), npoints + 1, st));
-    aa.q_off = C.q_off.as<long long>();
-    long long npair = 0;
-    RET(read_dev(aa.q_off + npoints, npair, st));
-    RET(ensure(C.q_key, (size_t)(npair > 0 ? npair : 1) * 8));
-    aa.q_key = C.q_key.as<unsigned long long>();
-    if (npair > 0) CK(launch_query_points(aa, true, st)); // keys come out sorted: point, element descending
-    // samples per pair, in pair order (point, element descending, tet)
-    VdfArgs va = {};
-    va.m = mesh_dev(m, psib_grid{}, q.c.pos, q.c.vel, q.c.mass, q.c.conn, 1.0, nullptr);
-    va.m.ptol2 = reftol * reftol;
-    va.max_lvl = maxlvl > 6 ? 6 : (maxlvl < 0 ? 0 : maxlvl);
-    va.quad = m.elemtype == 27;
-    va.points = aa.qry;
-    va.pairs = aa.q_key;
-    va.npair = npair;
-    va.status = (unsigned*)&sm[S_STATUS];
-    RET(ensure(C.s_cnt, (size_t)(npair + 1) * sizeof(long long)));
-    RET(ensure(C.s_off, (size_t)(npair + 1) * sizeof(long long)));
-    va.cnt = C.s_cnt.as<long long>();
-    CK(cudaMemsetAsync(va.cnt, 0, (size_t)(npair + 1) * sizeof(long long), st));
-    if (npair > 0) CK(launch_vdf_samples(va, false, st));
-    RET(excl_scan(C, va.cnt, C.s_off.as<long long>(), npair + 1, st));
-    va.off = C.s_off.as<long long>();
-    long long total = 0;
-    RET(read_dev(va.off + npair, total, st));
-    // each point's first sample: the sample offset of its first pair
-    RET(ensure(C.s_offs, (size_t)(npoints + 1) * sizeof(long long)));
-    CK(launch_gather_ll(va.off, aa.q_off, npoints + 1, C.s_offs.as<long long>(), st));
-    RET(query_status(q, sm));
-    RET(query_output(q, offsets, C.s_offs.p, (size_t)(npoints + 1) * sizeof(long long)));
-    if (!rho || !vel) return PSIB_OK;
-    if (capacity < total)
-        return fail(PSIB_ERR_OVERFLOW, "the output holds %lld samples, the points have %lld", capacity, total);
-    if (total == 0) return PSIB_OK;
-    if (q.host) {
-        RET(ensure(C.s_rho, (size_t)total * sizeof(double)));
-        RET(ensure(C.s_vel, (size_t)total * 3 * sizeof(double)));
-        va.rho = C.s_rho.as<double>();
-        va.vel = C.s_vel.as<double>();
-    } else {
-        va.rho = rho;
-        va.vel = vel;
-    }
-    CK(launch_vdf_samples(va, true, st));
-    if (q.host) {
-        RET(query_output(q, rho, va.rho, (size_t)total * sizeof(double)));
-        RET(query_output(q, vel, va.vel, (size_t)total * 3 * sizeof(double)));
-    }
-    return query_status(q, sm);
-}
-
-} // namespace
-
-// ---- a persistent element index (PSI.RStarTree) ----
-
-// The mesh (device copies), its kept elements' boxes and the cell index over
-// them, built once; later queries and samples reuse them.
-struct psib_index {
-    int device = 0;
-    psib_mesh mesh = {}; // device pointers into the buffers below
-    psib::AnnArgs aa = {}; // kept flags, boxes, cells and runs, pointing into the buffers below
-    long long kept = 0;
-    DevBuf pos, vel, mass, conn, ebox, cnt, reg_elem, run_key, run_off, run_cnt;
-};
-
-namespace {
-
-int copy_dev(DevBuf& dst, const void* src, size_t bytes, cudaStream_t st)
-{
-    RET(ensure(dst, bytes));
-    if (bytes && src) CK(cudaMemcpyAsync(dst.p, src, bytes, cudaMemcpyDeviceToDevice, st));
-    return PSIB_OK;
-}
-
-void free_index(psib_index* ix)
-{
-    if (!ix) return;
-    for (DevBuf* b : {&ix->pos, &ix->vel, &ix->mass, &ix->conn, &ix->ebox, &ix->cnt, &ix->reg_elem, &ix->run_key,
-                      &ix->run_off, &ix->run_cnt})
-        if (b->p) cudaFree(b->p);
-    delete ix;
-}
-
-int index_fill(QueryCall& q, const double (*window)[3], psib_index* ix)
-{
-    Ctx& C = *q.C;
-    cudaStream_t st = q.c.st;
-    const psib_mesh& m = *q.c.mesh;
-    RET(ensure(C.small, S_WORDS * 8));
-    unsigned long long* sm = C.small.as<unsigned long long>();
-    CK(cudaMemsetAsync(sm, 0, S_WORDS * 8, st));
-    psib::AnnArgs aa;
-    RET(query_elements_stage(q, window, 1.0, aa, sm));
-    long long klaunch = 0, kept = 0;
-    if (aa.nelem > 0) RET(build_cells(C, aa, st, klaunch, kept));
-    RET(query_status(q, sm));
-    const size_t np = (size_t)m.npart, ne = (size_t)m.nelem;
-    RET(copy_dev(ix->pos, q.c.pos, np * 24, st));
-    if (q.c.vel) RET(copy_dev(ix->vel, q.c.vel, np * 24, st));
-    if (q.c.mass) RET(copy_dev(ix->mass, q.c.mass, ne * 8, st));
-    if (q.c.conn) RET(copy_dev(ix->conn, q.c.conn, ne * (size_t)m.elemtype * 4, st));
-    RET(copy_dev(ix->ebox, aa.ebox, ne * 48, st));
-    RET(copy_dev(ix->cnt, aa.cnt_a, 2 * (ne + 1) * sizeof(int), st));
-    if (kept > 0) {
-        RET(copy_dev(ix->reg_elem, aa.reg_elem, (size_t)aa.nreg * sizeof(int), st));
-        RET(copy_dev(ix->run_key, aa.run_key, (size_t)aa.nruns * 8, st));
-        RET(copy_dev(ix->run_off, aa.run_off, (size_t)aa.nruns * 8, st));
-        RET(copy_dev(ix->run_cnt, aa.run_cnt, (size_t)aa.nruns * sizeof(int), st));
-    }
-    CK(cudaStreamSynchronize(st));
-    ix->device = C.device;
-    ix->kept = kept;
-    ix->mesh = m;
-    ix->mesh.pos = ix->pos.as<double>();
-    ix->mesh.vel = q.c.vel ? ix->vel.as<double>() : nullptr;
-    ix->mesh.mass = q.c.mass ? ix->mass.as<double>() : nullptr;
-    ix->mesh.connectivity = q.c.conn ? ix->conn.as<int>() : nullptr;
-    psib::AnnArgs& a = ix->aa;
-    a = psib::AnnArgs{};
-    a.nelem = aa.nelem;
-    a.cg = aa.cg;
-    a.nreg = aa.nreg;
-    a.nruns = aa.nruns;
-    a.ebox = ix->ebox.as<double>();
-    a.cnt_a = ix->cnt.as<int>();
-    a.cnt_b = ix->cnt.as<int>() + (ne + 1);
-    a.reg_elem = ix->reg_elem.as<int>();
-    a.run_key = ix->run_key.as<unsigned long long>();
-    a.run_off = ix->run_off.as<long long>();
-    a.run_cnt = ix->run_cnt.as<int>();
-    return PSIB_OK;
-}
-
-// A call on an index: its device and mesh, points and outputs in the memory options->memory names.
-int index_begin(QueryCall& q, psib_index* ix, const psib_options* opt)
-{
-    g_err.clear();
-    if (!ix) return fail(PSIB_ERR_ARG, "index is required");
-    psib_options o = {};
-    o.memory = PSIB_HOST;
-    if (opt) o = *opt;
-    if (o.memory != PSIB_HOST && o.memory != PSIB_DEVICE) return fail(PSIB_ERR_ARG, "invalid memory kind %d", o.memory);
-    if (psib_device_count() <= 0) return fail(PSIB_ERR_NODEVICE, "no CUDA device is visible");
-    CK(cudaSetDevice(ix->device));
-    RET(get_ctx(ix->device, &q.C));
-    q.host = o.memory == PSIB_HOST;
-    q.c = Call{};
-    q.c.mesh = &ix->mesh;
-    q.c.C = q.C;
-    q.c.st = q.C->own;
-    q.c.pos = ix->mesh.pos;
-    q.c.vel = ix->mesh.vel;
-    q.c.mass = ix->mesh.mass;
-    q.c.conn = ix->mesh.connectivity;
-    if (!q.host) {
-        q.user = (cudaStream_t)o.stream;
-        RET(enter_own_stream(*q.C, q.user));
-    }
-    return PSIB_OK;
-}
-
-unsigned long long* index_status(QueryCall& q, psib::AnnArgs& aa, int& rc)
-{
-    rc = ensure(q.C->small, S_WORDS * 8);
-    if (rc) return nullptr;
-    unsigned long long* sm = q.C->small.as<unsigned long long>();
-    if (cudaMemsetAsync(sm, 0, S_WORDS * 8, q.c.st) != cudaSuccess) {
-        rc = fail(PSIB_ERR_CUDA, "cudaMemsetAsync failed");
-        return nullptr;
-    }
-    aa.status = (unsigned*)&sm[S_STATUS];
-    return sm;
-}
-
 } // namespace
 
 int psib::report_error(int code, const char* msg) { return fail(code, "%s", msg); }
@@ -3059,90 +2003,6 @@ int psib_voxels_adjoint_fields(const psib_grid* grad, const psib_grid* fwd, cons
         CK(cudaEventElapsedTime(&o.stats->ms_total, C->ev[0], C->ev[7]));
     }
     return PSIB_OK;
-}
-
-int psib_query_elements(const psib_mesh* mesh, const double window[2][3], const double* boxes, long long nboxes,
-                        long long* offsets, int* elements, long long capacity, const psib_options* opt)
-{
-    if (!window || !offsets || nboxes < 0 || (nboxes > 0 && !boxes))
-        return fail(PSIB_ERR_ARG, "window, offsets and nboxes >= 0 boxes are required");
-    if (nboxes >= (1ll << 31)) return fail(PSIB_ERR_ARG, "at most 2^31 - 1 query boxes");
-    QueryCall q;
-    RET(query_begin(q, mesh, opt));
-    return query_end(q, query_elements_impl(q, window, boxes, nboxes, offsets, elements, capacity));
-}
-
-int psib_sample_vdf(const psib_mesh* mesh, const double window[2][3], const double* points, long long npoints,
-                    double refine_tolerance, int refine_max_lvl, long long* offsets, double* rho, double* vel,
-                    long long capacity, const psib_options* opt)
-{
-    if (!window || !offsets || npoints < 0 || (npoints > 0 && !points))
-        return fail(PSIB_ERR_ARG, "window, offsets and npoints >= 0 points are required");
-    if (npoints >= (1ll << 31)) return fail(PSIB_ERR_ARG, "at most 2^31 - 1 sample points");
-    QueryCall q;
-    RET(query_begin(q, mesh, opt));
-    return query_end(q, sample_vdf_impl(q, window, points, npoints, refine_tolerance, refine_max_lvl, offsets, rho,
-                                        vel, capacity));
-}
-
-int psib_index_create(const psib_mesh* mesh, const double window[2][3], psib_index** index, const psib_options* opt)
-{
-    if (!index || !window) return fail(PSIB_ERR_ARG, "index and window are required");
-    *index = nullptr;
-    QueryCall q;
-    RET(query_begin(q, mesh, opt));
-    psib_index* ix = new psib_index();
-    const int rc = query_end(q, index_fill(q, window, ix));
-    if (rc != PSIB_OK) {
-        free_index(ix);
-        return rc;
-    }
-    *index = ix;
-    return PSIB_OK;
-}
-
-int psib_index_query(psib_index* index, const double* boxes, long long nboxes, long long* offsets, int* elements,
-                     long long capacity, const psib_options* opt)
-{
-    if (!offsets || nboxes < 0 || (nboxes > 0 && !boxes))
-        return fail(PSIB_ERR_ARG, "offsets and nboxes >= 0 boxes are required");
-    if (nboxes >= (1ll << 31)) return fail(PSIB_ERR_ARG, "at most 2^31 - 1 query boxes");
-    QueryCall q;
-    RET(index_begin(q, index, opt));
-    psib::AnnArgs aa = index->aa;
-    int rc = PSIB_OK;
-    unsigned long long* sm = index_status(q, aa, rc);
-    if (rc == PSIB_OK) rc = query_from_boxes(q, aa, sm, boxes, nboxes, offsets, elements, capacity);
-    return query_end(q, rc);
-}
-
-int psib_index_sample_vdf(psib_index* index, const double* points, long long npoints, double refine_tolerance,
-                          int refine_max_lvl, long long* offsets, double* rho, double* vel, long long capacity,
-                          const psib_options* opt)
-{
-    if (!offsets || npoints < 0 || (npoints > 0 && !points))
-        return fail(PSIB_ERR_ARG, "offsets and npoints >= 0 points are required");
-    if (npoints >= (1ll << 31)) return fail(PSIB_ERR_ARG, "at most 2^31 - 1 sample points");
-    QueryCall q;
-    RET(index_begin(q, index, opt));
-    psib::AnnArgs aa = index->aa;
-    int rc = PSIB_OK;
-    unsigned long long* sm = index_status(q, aa, rc);
-    if (rc == PSIB_OK)
-        rc = vdf_from_index(q, aa, index->kept, sm, points, npoints, refine_tolerance, refine_max_lvl, offsets, rho,
-                            vel, capacity);
-    return query_end(q, rc);
-}
-
-void psib_index_destroy(psib_index* index)
-{
-    if (!index) return;
-    int cur = 0;
-    const bool have = cudaGetDevice(&cur) == cudaSuccess;
-    if (cudaSetDevice(index->device) == cudaSuccess) cudaDeviceSynchronize();
-    free_index(index);
-    if (have) cudaSetDevice(cur);
-    cudaGetLastError();
 }
 
 } // extern "C"
