@@ -530,13 +530,9 @@ int bfs_clip(Ctx& C, ClipArgs& ca, long long nmain, long long nitems, unsigned l
     ba.dfs_count = &sm[S_DFS];
     ba.bytes = &sm[S_BYTES];
     ba.window_bfs = env_ll("PSIB_BFS_WINDOW", 1) != 0;
-    // Six resident level blocks per SM rather than the seven that fit (72 registers x 128 threads
-    // each): the seventh would fill the register file, and the deep-tree kernel on its side stream
-    // (128 registers x 64 threads a block) then finds no room beside the walk.  The level kernel
-    // alone is slower so; whole steps are as fast or faster (the same at 128^3 -> 256^3 in one
-    // comparison, 4 % faster in another), and at 64^3 -> 128^3, where the deep-tree images are a
-    // fifth of the work, the difference is larger.  The freed shared memory goes to L1.
-    ba.level_blocks = (int)env_ll("PSIB_LEVEL_BLOCKS", 6);
+    // Fewer resident level blocks than fit (PSIB_LEVEL_BLOCKS=6, the freed shared memory given to L1)
+    // measured within noise of all that fit (64^3 -> 128^3 clip 43.5 against 42.6 ms, three runs each)
+    ba.level_blocks = (int)env_ll("PSIB_LEVEL_BLOCKS", 0);
     ba.leaf_split = (int)env_ll("PSIB_LEAF_SPLIT", 7);
     // the level queues filled from both ends too (PSIB_LEVEL_SPLIT=7): the level launches alone
     // 10 % faster, but whole steps measured 4 % slower and more variable, so off by default
@@ -1545,7 +1541,7 @@ int run_capture(Call& c)
     ba.dfs_count = &sm[S_DFS];
     ba.bytes = &sm[S_BYTES];
     ba.window_bfs = 1;
-    ba.level_blocks = (int)env_ll("PSIB_LEVEL_BLOCKS", 6); // as bfs_clip
+    ba.level_blocks = (int)env_ll("PSIB_LEVEL_BLOCKS", 0); // as bfs_clip
     ba.leaf_split = (int)env_ll("PSIB_LEAF_SPLIT", 7);
     ba.level_split = (int)env_ll("PSIB_LEVEL_SPLIT", 0);
     ba.vsum = C.vsum.as<double>();
