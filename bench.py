@@ -56,8 +56,8 @@ def clip_traffic_bytes(frags):
                    f"{CLIP_TRAFFIC_PER_FRAGMENT:.0f} B per fragment, times this step's fragments"}
 
 
-# bytes per fragment of the capture above (51.1 GB per call over 28.24 M fragments)
-CLIP_TRAFFIC_PER_FRAGMENT = 1810.0
+# bytes per fragment of the capture above (47.9 GB per call over 28.24 M fragments)
+CLIP_TRAFFIC_PER_FRAGMENT = 1697.0
 
 
 def parse():
