@@ -114,8 +114,9 @@ typedef struct {
     float ms_final;          /* device time of the record sort and the field update */
     long long clip_launches; /* launches of the clip kernels */
     long long kernel_launches; /* launches of this library's own kernels (library scans/sorts excluded) */
-    long long walk_bytes;    /* mixed precision: bytes the breadth-first walk reads and writes by its
-                                algorithm (polyhedra, tet vertices, fragment records or sums) */
+    long long walk_bytes;    /* bytes the breadth-first walk (mixed, and FP64 unless PSIB_BFS64=0) reads
+                                and writes by its algorithm (polyhedra, tet vertices, fragment records
+                                or sums); 0 when every tet was walked depth first */
     long long corrected_items; /* atomic accumulation: tet images walked a second time to add their mass
                                   correction (their FP32 walk missed the exact q-volume by more than 1e-14) */
     int accumulation;        /* 1: fragments were added to per-voxel sums with atomics; 0: sorted records */

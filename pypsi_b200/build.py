@@ -4,8 +4,8 @@
 
 Objects go to pypsi_b200/_build/; the two shared libraries land next to this
 file so they travel with the source tree.  FMA contraction is disabled in every
-translation unit except clip_mixed.cu: the FP64 path repeats the reference's
-double-precision operation order.
+translation unit except clip_mixed.cu and bfs.cu (the mixed walks): the FP64
+path repeats the reference's double-precision operation order.
 """
 from __future__ import annotations
 
@@ -34,12 +34,13 @@ CUDA_UNITS = {  # unit -> extra flags
     "query_host.cu": ["--fmad=false"],
     "noalloc.cu": ["--fmad=false"],
     "bfs.cu": [],
+    "bfs_fp64.cu": ["--fmad=false"],
     "annihilation.cu": ["--fmad=false"],
     "probe.cu": [],  # the FMA issue-rate probe (explicit fma(), so contraction does not matter)
     "loaders.cpp": [],  # host code only: the snapshot readers
 }
 HEADERS = ["psib_device.cuh", "psib_clip.cuh", "psib_kernels.h", "psib_accum.cuh", "psib_adjoint.cuh",
-           "pipeline_host.h"]
+           "psib_bfs.cuh", "pipeline_host.h"]
 
 
 def _newer(target: str, deps: list[str]) -> bool:

@@ -407,8 +407,11 @@ cudaError_t bfs_pass(const BfsArgs& ba, const PolyQueue* Q, unsigned long long* 
     b.leaf = Q[2];
     b.leaf.count = &cl[0];
     b.leaf.count_hi = &ch[0];
-    if (e == cudaSuccess) e = launch_bfs_init(b, grid, s);
-    if (e == cudaSuccess) e = launch_bfs_leaf(b, grid, s);
+    auto init = ba.fp64 ? launch_bfs64_init : launch_bfs_init;
+    auto level = ba.fp64 ? launch_bfs64_level : launch_bfs_level;
+    auto leaf = ba.fp64 ? launch_bfs64_leaf : launch_bfs_leaf;
+    if (e == cudaSuccess) e = init(b, grid, s);
+    if (e == cudaSuccess) e = leaf(b, grid, s);
     int ia = 0;
     for (int lvl = 0; lvl < NLEV && e == cudaSuccess; ++lvl) {
         b.in = Q[ia];
@@ -420,8 +423,8 @@ cudaError_t bfs_pass(const BfsArgs& ba, const PolyQueue* Q, unsigned long long* 
         b.leaf.count = &cl[lvl + 1];
         b.leaf.count_hi = &ch[lvl + 1];
         b.last = lvl == NLEV - 1;
-        e = launch_bfs_level(b, grid, s);
-        if (e == cudaSuccess) e = launch_bfs_leaf(b, grid, s);
+        e = level(b, grid, s);
+        if (e == cudaSuccess) e = leaf(b, grid, s);
         ia = 1 - ia;
     }
     if (e == cudaSuccess) e = launch_bfs_advance(b, s);
@@ -434,16 +437,19 @@ struct BfsSizes {
     long long tiles = 0, cap = 0, npass = 0;
 };
 
-// Mixed-precision clip of queue positions [0, nmain) by the breadth-first
-// walk (bfs.cu); images that need the window clip come back in a list and go to
-// the depth-first kernel.  Images are sorted by index-box volume, largest
-// first; a pass takes images while the sum of their box volumes -- a bound on
-// every queue of the pass -- stays within the queue capacity.
+// Clip of queue positions [0, nmain) by the breadth-first walk: mixed precision (bfs.cu; images
+// that need the window clip come back in a list for the depth-first kernel when PSIB_BFS_WINDOW=0)
+// or, with fp64, the bit-exact FP64 walk (bfs_fp64.cu, raw records; window planes cut in the walk).
+// Images are sorted by index-box volume, largest first; a pass takes images while the sum of
+// their box volumes -- a bound on every queue of the pass -- stays within the queue capacity.
 // keys: the footprint keys of the queue positions [0, nmain), ascending.
 int bfs_clip(Ctx& C, ClipArgs& ca, long long nmain, long long nitems, unsigned long long* sm, int clip_grid,
              int clip_block, long long queue_voxels, bool batch, cudaStream_t st, long long& launches,
-             long long& klaunch, const uint16_t* keys, BfsSizes* sizes = nullptr)
+             long long& klaunch, const uint16_t* keys, BfsSizes* sizes = nullptr, bool fp64 = false)
 {
+    // bytes of one queue element's positions (FP32, or FP64 position and q)
+    const size_t xbytes = fp64 ? (size_t)MAXV * 6 * sizeof(double) : (size_t)MAXV * 3 * sizeof(float);
+    DevBuf* qxb = fp64 ? C.qxd : C.qx;
     RET(ensure(C.hist, 65536 * sizeof(unsigned)));
     CK(cudaMemsetAsync(C.hist.p, 0, 65536 * sizeof(unsigned), st));
     k_key_hist<<<C.num_sms * 4, 256, 0, st>>>(keys, nmain, C.hist.as<unsigned>());
@@ -456,13 +462,13 @@ int bfs_clip(Ctx& C, ClipArgs& ca, long long nmain, long long nitems, unsigned l
     // (three queues of bytes_per_elem each)
     long long cap = queue_voxels;
     if (cap <= 0) {
-        const long long bytes_per_elem = MAXV * 3 * 4 + MAXV * 4 + 1 + 1 + 12 + 4;
+        const long long bytes_per_elem = (long long)xbytes + MAXV * 4 + 1 + 1 + 12 + 4;
         size_t freeb = 0, totalb = 0;
         if (cudaMemGetInfo(&freeb, &totalb) != cudaSuccess) {
             cudaGetLastError();
             freeb = 0;
         }
-        long long have = (long long)(C.qx[0].n / (MAXV * 3 * 4)); // queues already allocated count as free
+        long long have = (long long)(qxb[0].n / xbytes); // queues already allocated count as free
         cap = std::max<long long>(have, (long long)(0.35 * (double)freeb) / (3 * bytes_per_elem));
         cap = std::min<long long>(cap, 64ll << 20);
     }
@@ -509,15 +515,16 @@ int bfs_clip(Ctx& C, ClipArgs& ca, long long nmain, long long nitems, unsigned l
     const size_t tiles = (size_t)(std::max<long long>(std::min(need, cap), 32) + 31) / 32;
     PolyQueue Q[3];
     for (int i = 0; i < 3; ++i) {
-        RET(ensure(C.qx[i], tiles * 32 * MAXV * 3 * sizeof(float)));
+        RET(ensure(qxb[i], tiles * 32 * xbytes));
         RET(ensure(C.qnb[i], tiles * 32 * MAXV * sizeof(uint32_t)));
         RET(ensure(C.qnv[i], tiles * 32));
         RET(ensure(C.qwin[i], tiles * 32));
         RET(ensure(C.qbox[i], tiles * 32 * 3 * sizeof(uint32_t)));
         RET(ensure(C.qitem[i], tiles * 32 * sizeof(uint32_t)));
-        Q[i] = PolyQueue{C.qx[i].as<float>(), C.qnb[i].as<uint32_t>(), C.qnv[i].as<uint8_t>(),
+        Q[i] = PolyQueue{fp64 ? nullptr : C.qx[i].as<float>(), C.qnb[i].as<uint32_t>(), C.qnv[i].as<uint8_t>(),
                          C.qwin[i].as<uint8_t>(), C.qbox[i].as<uint32_t>(), C.qitem[i].as<uint32_t>(), nullptr,
                          (unsigned long long)tiles * 32};
+        Q[i].xq = fp64 ? C.qxd[i].as<double>() : nullptr;
     }
     RET(ensure(C.dfs_list, (size_t)std::max<long long>(nmain, 1) * sizeof(int)));
     RET(ensure(C.bfs_cnt, NCNT * sizeof(unsigned long long)));
@@ -530,15 +537,16 @@ int bfs_clip(Ctx& C, ClipArgs& ca, long long nmain, long long nitems, unsigned l
     ba.dfs_count = &sm[S_DFS];
     ba.bytes = &sm[S_BYTES];
     ba.window_bfs = env_ll("PSIB_BFS_WINDOW", 1) != 0;
+    ba.fp64 = fp64 ? 1 : 0;
     // Fewer resident level blocks than fit (PSIB_LEVEL_BLOCKS=6, the freed shared memory given to L1)
     // measured within noise of all that fit (64^3 -> 128^3 clip 43.5 against 42.6 ms, three runs each)
     ba.level_blocks = (int)env_ll("PSIB_LEVEL_BLOCKS", 0);
-    ba.leaf_split = (int)env_ll("PSIB_LEAF_SPLIT", 7);
+    ba.leaf_split = fp64 ? 0 : (int)env_ll("PSIB_LEAF_SPLIT", 7);
     // the level queues filled from both ends too (PSIB_LEVEL_SPLIT=7): the level launches alone
     // 10 % faster, but whole steps measured 4 % slower and more variable, so off by default
-    ba.level_split = (int)env_ll("PSIB_LEVEL_SPLIT", 0);
+    ba.level_split = fp64 ? 0 : (int)env_ll("PSIB_LEVEL_SPLIT", 0);
     // fewer level blocks leave shared memory unused: give it to L1 (one block is 30 KB of 228)
-    bfs_level_carveout(ba.level_blocks > 0 ? std::min(100, (ba.level_blocks * 31 * 100 + 227) / 228) : 0);
+    if (!fp64) bfs_level_carveout(ba.level_blocks > 0 ? std::min(100, (ba.level_blocks * 31 * 100 + 227) / 228) : 0);
     RET(ensure(C.vsum, (size_t)std::max<long long>(nitems, 1) * sizeof(double)));
     ba.vsum = C.vsum.as<double>();
     // the pass table on the device; a device counter picks the pass, so every pass runs
@@ -551,6 +559,7 @@ int bfs_clip(Ctx& C, ClipArgs& ca, long long nmain, long long nitems, unsigned l
     ba.pass_idx = &sm[S_PASS];
     const int grid = C.num_sms;
     bfs_prepare();
+    bfs64_prepare();
     // One pass: reset the per-level counts, then init, leaf, and NLEV x (level, leaf), then
     // advance the pass counter.  Batches record it once as a CUDA graph and replay it for every
     // pass (and in later calls whose arguments are the same); plain launches if the graph cannot
@@ -599,8 +608,10 @@ int bfs_clip(Ctx& C, ClipArgs& ca, long long nmain, long long nitems, unsigned l
         sizes->cap = cap;
         sizes->npass = npass;
     }
-    CK(launch_bfs_finalize(ba, nitems, C.num_sms, st));
-    klaunch++;
+    if (!fp64) { // the FP64 walk's images need no mass correction
+        CK(launch_bfs_finalize(ba, nitems, C.num_sms, st));
+        klaunch++;
+    }
     unsigned long long ndfs = 0;
     CK(cudaMemcpyAsync(&ndfs, &sm[S_DFS], 8, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
@@ -610,7 +621,8 @@ int bfs_clip(Ctx& C, ClipArgs& ca, long long nmain, long long nitems, unsigned l
         cw.order_base = 0;
         cw.n = (long long)ndfs;
         cw.head = &sm[S_HEAD];
-        CK(launch_clip_mixed(cw, false, false, clip_grid, clip_block, st));
+        if (fp64) CK(launch_clip_fp64(cw, false, clip_grid, clip_block, st));
+        else CK(launch_clip_mixed(cw, false, false, clip_grid, clip_block, st));
         launches++;
     }
     return PSIB_OK;
@@ -732,9 +744,11 @@ int run_device(Call& c)
     const bool central = (mixed || c.precision == PSIB_FP64_CENTRAL) && !c.adjoint;
     // the mixed kernel walks the main images breadth first (PSIB_BFS=0: depth first)
     bool use_bfs = mixed && env_ll("PSIB_BFS", 1) != 0;
+    // the bit-exact FP64 mode walks them breadth first too (PSIB_BFS64=0: depth first)
+    bool use_bfs64 = c.precision == PSIB_FP64 && !c.adjoint && env_ll("PSIB_BFS64", 1) != 0;
     for (int b = 0; b < (batch ? c.nbatch : 1); ++b)
         for (int i = 0; i < 3; ++i)
-            if ((batch ? c.grids[b] : g).n[i] >= 0xFFFF) use_bfs = false; // box bounds are packed in 16 bits
+            if ((batch ? c.grids[b] : g).n[i] >= 0xFFFF) use_bfs = use_bfs64 = false; // box bounds: 16 bits
     // 1, 4 or 10 moments per record (FP32 kernel: m0, q-centroid, central second moment)
     const int nmom = order == 2 ? 10 : order == 1 ? 4 : 1;
     // Fragments added to per-voxel sums with atomics (deterministic == 0): central-form
@@ -1116,10 +1130,28 @@ int run_device(Call& c)
             CK(cudaMemsetAsync(&sm[S_CNT], 0, 24, st)); // this attempt's counters
             CK(cudaMemsetAsync(&sm[S_HEAD], 0, 16, st));
             CK(cudaEventRecord(C.ev[4], st));
-            if (nmain > 0 && use_bfs) {
+            // Beside the FP64 walk, the deep-tree images run on the side stream: both reserve record
+            // slots with atomics (the sort puts them in order) and use their own scratch and queue heads.
+            bool deep_beside = false;
+            if (ndeep > 0 && nmain > 0 && use_bfs64) {
+                const int big_grid = (int)std::min<long long>(C.num_sms * 2, (ndeep + big_block - 1) / big_block);
+                RET(ensure(C.scratch_big, big_bytes * (size_t)big_grid * big_block));
+                ClipArgs cd = ca;
+                cd.scratch = C.scratch_big.p;
+                cd.order_base = nmain;
+                cd.n = ndeep;
+                cd.head = &sm[S_HEAD + 1];
+                CK(cudaEventRecord(C.fork, st));
+                CK(cudaStreamWaitEvent(C.side, C.fork, 0));
+                CK(launch_clip_fp64(cd, true, big_grid, big_block, C.side));
+                CK(cudaEventRecord(C.join, C.side));
+                launches++;
+                deep_beside = true;
+            }
+            if (nmain > 0 && (use_bfs || use_bfs64)) {
                 ca.scratch = C.scratch.p;
                 RET(bfs_clip(C, ca, nmain, nitems, sm, clip_grid, clip_block, c.queue_voxels, batch, st, launches,
-                             klaunch, C.key_sorted.as<uint16_t>()));
+                             klaunch, C.key_sorted.as<uint16_t>(), nullptr, use_bfs64));
             } else if (nmain > 0) {
                 ca.scratch = C.scratch.p;
                 ca.order_base = 0;
@@ -1129,7 +1161,9 @@ int run_device(Call& c)
                 else CK(launch_clip_fp64(ca, false, clip_grid, clip_block, st));
                 launches++;
             }
-            if (ndeep > 0) {
+            if (deep_beside) {
+                CK(cudaStreamWaitEvent(st, C.join, 0));
+            } else if (ndeep > 0) {
                 const int big_grid = (int)std::min<long long>(C.num_sms * 2, (ndeep + big_block - 1) / big_block);
                 RET(ensure(C.scratch_big, big_bytes * (size_t)big_grid * big_block));
                 ca.scratch = C.scratch_big.p;

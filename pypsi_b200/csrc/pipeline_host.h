@@ -79,6 +79,7 @@ struct Ctx {
     DevBuf rkey, rmom, rkey_sorted, rperm_in, rperm, rvox, ritem, rmom_sorted, run_vox, run_cnt, run_off;
     // breadth-first clip: three polyhedron queues, the volume histogram, per-level counters, window list
     DevBuf qx[3], qnb[3], qnv[3], qwin[3], qbox[3], qitem[3], hist, bfs_cnt, dfs_list, vsum;
+    DevBuf qxd[3]; // the FP64 walk's positions and q
     DevBuf btab, igrid; // batch tables, image -> cutout
     DevBuf adjcoef;     // full adjoint: per-voxel coefficients
     // atomic accumulation: per-voxel sums, tile reference velocities, the mass-correction pass
@@ -109,7 +110,7 @@ struct Ctx {
                 &hfield[5], &iframe, &ielem, &ipid, &ikey,
                 &key_sorted, &order_in, &order, &counts, &offsets, &cub_tmp, &scratch, &scratch_big, &iscale, &small, &rkey, &rmom,
                 &rkey_sorted, &rperm_in, &rperm, &rvox, &ritem, &rmom_sorted, &run_vox, &run_cnt, &run_off,
-                &qx[0], &qx[1], &qx[2], &qnb[0], &qnb[1], &qnb[2], &qnv[0], &qnv[1], &qnv[2], &qbox[0], &qbox[1],
+                &qx[0], &qx[1], &qx[2], &qxd[0], &qxd[1], &qxd[2], &qnb[0], &qnb[1], &qnb[2], &qnv[0], &qnv[1], &qnv[2], &qbox[0], &qbox[1],
                 &qbox[2], &qitem[0], &qitem[1], &qitem[2], &hist, &bfs_cnt, &dfs_list, &vsum, &qwin[0], &qwin[1],
                 &qwin[2], &btab, &igrid, &passes, &a_cnt, &a_off, &a_ebox, &a_tets_a, &a_tets_b, &a_stats,
                 &a_reg_cnt, &a_reg_off, &a_reg_key, &a_reg_elem, &a_reg_key_s, &a_reg_elem_s, &a_run_key,

@@ -223,6 +223,9 @@ struct PolyQueue {
     // from the end of the buffer (element cap - 1 - j), so that a leaf warp's lanes mostly hold
     // fragments of similar vertex counts; the two ends together stay within cap
     unsigned long long *count_hi;
+    // FP64 walk (x null): element e's vertex v holds position then q, c = 0..5, at
+    // xq[((e/32 * MAXV + v) * 6 + c) * 32 + e%32]
+    double *xq;
 };
 struct BfsArgs {
     ClipArgs c;               // frames, queue order, grid, records, status, counters, scale
@@ -239,6 +242,7 @@ struct BfsArgs {
     int level_blocks;         // level: resident blocks per SM (0: as many as fit)
     int leaf_split;           // level: leaves of more vertices go to the leaf queue's high end (0: none)
     int level_split;          // level: children of more vertices go to the level queue's high end (0: none)
+    int fp64;                 // the FP64 walk (bfs_fp64.cu): queues of FP64 positions and q, raw records
 };
 // each launches one resident wave of grid-stride blocks on num_sms SMs
 cudaError_t launch_bfs_init(const BfsArgs &a, int num_sms, cudaStream_t s);
@@ -246,8 +250,13 @@ cudaError_t launch_bfs_level(const BfsArgs &a, int num_sms, cudaStream_t s);
 cudaError_t launch_bfs_leaf(const BfsArgs &a, int num_sms, cudaStream_t s);
 cudaError_t launch_bfs_finalize(const BfsArgs &a, long long nitems, int num_sms, cudaStream_t s);
 cudaError_t launch_bfs_advance(const BfsArgs &a, cudaStream_t s);
+// the FP64 walk's init, level and leaf kernels (the pass table, finalize and advance are shared)
+cudaError_t launch_bfs64_init(const BfsArgs &a, int num_sms, cudaStream_t s);
+cudaError_t launch_bfs64_level(const BfsArgs &a, int num_sms, cudaStream_t s);
+cudaError_t launch_bfs64_leaf(const BfsArgs &a, int num_sms, cudaStream_t s);
 // kernel attributes and occupancy, queried once before any launch or stream capture
 void bfs_prepare();
+void bfs64_prepare();
 // the shared-memory share of the unified L1 of the level kernel, in percent (0: the driver's choice)
 void bfs_level_carveout(int percent);
 

@@ -284,3 +284,45 @@ def test_32cube_to_64cube_density_bitwise_against_compiled_reference(gpu, oracle
     out, _, _ = run_psi(gpu, c, precision="mixed")
     check(field_errors(out, ref), MIXED_TOL, "32^3 -> 64^3")
     assert mass_error(out["m"], 32 ** 3) <= MASS_TOL
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_fp64_breadth_first_equals_depth_first(gpu, name, monkeypatch):
+    """The FP64 walk runs breadth first (the mixed walk's level launches, FP64 positions and q);
+    its fields, fragments and splits equal the depth-first FP64 kernel's bit for bit."""
+    c = make(name)
+    monkeypatch.setenv("PSIB_BFS64", "0")
+    want, _, _ = run_psi(gpu, c, precision="fp64")
+    st0 = gpu.last_stats()
+    assert st0["walk_bytes"] == 0
+    monkeypatch.setenv("PSIB_BFS64", "1")
+    got, _, _ = run_psi(gpu, c, precision="fp64")
+    st1 = gpu.last_stats()
+    if name != "big_tet":  # a tree deeper than the walk's levels goes to the depth-first kernel
+        assert st1["walk_bytes"] > 0
+    for f in want:
+        assert np.array_equal(got[f], want[f]), (name, f, np.abs(got[f] - want[f]).max())
+    assert st1["fragments"] == st0["fragments"]
+    assert st1["splits"] == st0["splits"]
+
+
+def test_fp64_breadth_first_many_passes(gpu, monkeypatch):
+    """64^3 particles (rms 2 cells) onto 128^3 with every field, the walk's queues held to
+    2^18 box voxels so that it takes many passes, and in element chunks: bit for bit the
+    depth-first FP64 kernel, and the mass to 1e-13."""
+    from pypsi_b200.synth import zeldovich
+
+    pos, vel = zeldovich(64, 2.0, 2042, box=50.0)
+    c = {"kind": "block", "pos": pos, "vel": vel, "mass": None, "periodic_box": ((0.0,) * 3, (50.0,) * 3),
+         "n": (128, 128, 128), "bounds": ((0.0,) * 3, (50.0,) * 3), "fields": ["x", "v", "xx", "xv", "vv"],
+         "reftol": 1.0, "maxlvl": 0}
+    monkeypatch.setenv("PSIB_BFS64", "0")
+    want, _, _ = run_psi(gpu, c, precision="fp64")
+    monkeypatch.setenv("PSIB_BFS64", "1")
+    monkeypatch.setenv("PSIB_BFS_CAP", str(1 << 18))
+    monkeypatch.setenv("PSIB_ITEM_BUDGET", str(400000))
+    got, _, _ = run_psi(gpu, c, precision="fp64")
+    assert gpu.last_stats()["chunks"] > 1
+    for f in want:
+        assert np.array_equal(got[f], want[f]), (f, np.abs(got[f] - want[f]).max())
+    assert mass_error(got["m"], 64 ** 3) <= MASS_TOL
