@@ -1215,7 +1215,8 @@ def run_ours(args):
         line["c5_refined"] = {k: c5[k] for k in ("value", "unit", "ms_per_step", "mass_err_mixed", "work")}
     # the comparison the metric names, last so that the tail of the line shows it
     line["fp64"] = {"value": (1 if sharded else world) * tets_per_step / (ms_fp64 * 1e-3), "unit": "tets/s",
-                    "ms_per_step": ms_fp64}
+                    "ms_per_step": ms_fp64,
+                    "walk": "breadth-first" if st_fp64 and st_fp64[-1]["walk_bytes"] > 0 else "depth-first"}
     line["mixed_over_fp64"] = ms_fp64 / ms_mixed
     line["fwd_bwd_over_fwd"] = adjoint[f"{n_part}^3->{n_grid}^3 rms {RMS:g}"]["ratio"] if adjoint else None
     print(json.dumps(line), flush=True)
