@@ -41,8 +41,8 @@ __global__ void __launch_bounds__(BB) k_bfs64_init(BfsArgs a)
     const int lane = threadIdx.x & 31;
     const long long warp = (long long)blockIdx.x * (BB / 32) + (threadIdx.x >> 5);
     const long long nwarp = (long long)gridDim.x * (BB / 32);
-    const unsigned long long p = *a.pass_idx;
-    const long long q0 = a.passes[p], q1 = a.passes[p + 1];
+    const unsigned long long pass = *a.pass_idx;
+    const long long q0 = a.passes[pass], q1 = a.passes[pass + 1];
     unsigned st = 0;
     unsigned long long moved = 0;
     for (long long base = q0 + warp * 32; base < q1; base += nwarp * 32) {
