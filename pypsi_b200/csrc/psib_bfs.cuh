@@ -52,7 +52,7 @@ __device__ __forceinline__ void put_box(const PolyQueue& Q, unsigned long long e
 {
     for (int a = 0; a < 3; ++a) Q.box[3 * e + a] = (uint32_t)lo[a] | ((uint32_t)hi[a] << 16);
 }
-// queue element bytes: positions and links of nv vertices, nv, window mask, box, image
+// the mixed walk's queue element bytes: FP32 positions and links of nv vertices, nv, window mask, box, image
 __device__ __forceinline__ unsigned long long elem_bytes(int nv) { return 16ull * nv + 18ull; }
 
 __device__ __forceinline__ bool one_voxel(const int* lo, const int* hi)
