@@ -135,9 +135,9 @@ typedef struct {
     psib_stats *stats; /* optional */
     int refine_mode;   /* PSIB_REFINE_MIDPOINT (0) or PSIB_REFINE_STRETCH */
     double refine_cell[3]; /* stretch: the Lagrangian cell; all <= 0: box / block_dims of a periodic block mesh */
-    long long queue_voxels; /* mixed precision: tets walked per pass, bounded by the sum of their index-box
-                               volumes (the size of every polyhedron queue); 0: automatic (up to 64M, within
-                               35% of the free device memory) */
+    long long queue_voxels; /* the breadth-first walks (mixed and FP64): tets walked per pass, bounded by the
+                               sum of their index-box volumes (the size of every polyhedron queue); 0:
+                               automatic (up to 64M, within 35% of the free device memory) */
     int capture;       /* 0: a plain call.  1 (plan): a plain call (mixed precision, deterministic = 0,
                           device memory) that also sizes every buffer for calls like it, with room for
                           25% more tet images, and records their launch plan on this device.
